@@ -1,0 +1,231 @@
+/*
+ * sifv.h -- C ABI of the B200 (sm_100a) finite-volume time step.
+ *
+ * This is the drop-in boundary between a host code written against the
+ * SemiImplicitFV interfaces (SimulationConfig, RiemannSolverType,
+ * PressureSolver, IGRSolver) and the CUDA kernels of this library.  Every
+ * entry point takes plain pointers, sizes and PODs; no C++ or torch types
+ * cross it.  All calls return an int status (SIFV_OK == 0, >0 warning,
+ * <0 error); sifv_last_error() gives the message.  A context is not
+ * thread safe: use one host thread per context.  Distinct contexts are
+ * independent.
+ *
+ * Reference interfaces replaced (paths relative to the SemiImplicitFV
+ * repository):
+ *   sifv_config_t      <- SimulationConfig         include/SimulationConfig.hpp:72-210
+ *   sifv_mesh_t        <- RectilinearMesh ctor     include/RectilinearMesh.hpp:35-38
+ *                         + setBoundaryCondition   include/RectilinearMesh.hpp:117
+ *   sifv_set/get_field <- SolutionState SoA        include/SolutionState.hpp:73-113
+ *   sifv_step          <- ExplicitSolver::step     include/ExplicitSolver.hpp:33-36
+ *                         SemiImplicitSolver::step include/SemiImplicitSolver.hpp:36
+ *   sifv_pressure_solve<- PressureSolver::solve    include/PressureSolver.hpp:17-38
+ *                         (JacobiPressureSolver     src/JacobiPressureSolver.cpp:57-108)
+ *   sifv_igr_solve     <- IGRSolver::solveEntropicPressure include/IGR.hpp:42-51
+ *   sifv_acoustic_dt   <- computeAcousticTimeStep  src/RKTimeStepping.cpp:43-123,148-159
+ *   sifv_advective_dt  <- computeAdvectiveTimeStep src/RKTimeStepping.cpp:15-41,125-134
+ *   sifv_convert_cons_to_prim
+ *                      <- SolutionState::convertConservativeToPrimitiveVariables
+ *                         src/SolutionState.cpp:187-205 and
+ *                         MixtureEOS::convertConservativeToPrimitive src/MixtureEOS.cpp:99-143
+ *   sifv_apply_bc      <- RectilinearMesh::applyBoundaryConditions(state, PRIM, halo)
+ *                         src/RectilinearMesh.cpp:498-524
+ */
+#ifndef SIFV_H
+#define SIFV_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SIFV_ABI_VERSION 1
+#define SIFV_MAX_PHASES 8
+
+/* ---- status codes ---------------------------------------------------- */
+#define SIFV_OK                 0
+#define SIFV_NOT_CONVERGED      1   /* pressure solve reached maxIter (the reference returns maxIter silently) */
+#define SIFV_ERR_BAD_CONFIG    -1   /* SimulationConfig::validate() would throw std::invalid_argument */
+#define SIFV_ERR_BAD_ARG       -2
+#define SIFV_ERR_CUDA          -3
+#define SIFV_ERR_NAN           -4
+#define SIFV_ERR_UNSUPPORTED   -5
+#define SIFV_ERR_TIMEOUT       -6   /* a bounded device wait ran out; the context stays usable */
+#define SIFV_ERR_NO_DEVICE     -7
+
+/* ---- enums mirrored from the reference -------------------------------- */
+/* ReconstructionOrder, include/SimulationConfig.hpp:13-20 */
+#define SIFV_WENO1   0
+#define SIFV_WENO3   1
+#define SIFV_WENO5   2
+#define SIFV_UPWIND1 3
+#define SIFV_UPWIND3 4
+#define SIFV_UPWIND5 5
+/* RiemannSolverType, include/RiemannSolver.hpp:16 */
+#define SIFV_LF      0
+#define SIFV_RUSANOV 1
+#define SIFV_HLLC    2
+/* BoundaryCondition, include/RectilinearMesh.hpp:14-20 */
+#define SIFV_BC_SYMMETRY   0
+#define SIFV_BC_OUTFLOW    1
+#define SIFV_BC_PERIODIC   2
+#define SIFV_BC_SLIPWALL   3
+#define SIFV_BC_NOSLIPWALL 4
+/* single-phase EOS: IdealGasEOS (src/IdealGasEOS.cpp) or StiffenedGasEOS (src/StiffenedGasEOS.cpp) */
+#define SIFV_EOS_IDEAL     0
+#define SIFV_EOS_STIFFENED 1
+/* arithmetic of the reconstruction/flux bulk */
+#define SIFV_PREC_FP64  0   /* every operation in FP64 */
+#define SIFV_PREC_MIXED 1   /* FP32 reconstruction/flux bulk; FP64 state, pressure recovery and residuals */
+
+/* ---- field identifiers (SolutionState members) ------------------------ */
+#define SIFV_F_RHO    0
+#define SIFV_F_RHOU   1
+#define SIFV_F_RHOV   2
+#define SIFV_F_RHOW   3
+#define SIFV_F_RHOE   4
+#define SIFV_F_VELU   5
+#define SIFV_F_VELV   6
+#define SIFV_F_VELW   7
+#define SIFV_F_PRES   8
+#define SIFV_F_SIGMA  9
+#define SIFV_F_ALPHARHO(ph) (16 + (ph))   /* alphaRho[ph] */
+#define SIFV_F_ALPHA(ph)    (32 + (ph))   /* alpha[ph]    */
+
+/* Flat mirror of SimulationConfig (include/SimulationConfig.hpp:72-210) plus
+ * the EOS / Riemann-solver choice that the reference passes as objects. */
+typedef struct sifv_config {
+    int    dim;                 /* 1, 2 or 3 */
+    int    nGhost;
+    int    RKOrder;             /* 1, 2 or 3 (Shu-Osher SSP) */
+    int    useIGR;
+    int    semiImplicit;
+    int    reconOrder;          /* SIFV_WENO* / SIFV_UPWIND* */
+    double wenoEps;
+    int    riemannSolver;       /* SIFV_LF / SIFV_RUSANOV / SIFV_HLLC */
+    int    eosKind;             /* SIFV_EOS_IDEAL / SIFV_EOS_STIFFENED */
+    double gamma;
+    double pInf;
+    /* ExplicitParams */
+    double cfl, constDt, maxDt, minDt;
+    /* SemiImplicitParams */
+    double siCfl, siMaxDt, siMinDt;
+    int    maxPressureIters;
+    double pressureTol;
+    /* IGRParams */
+    double alphaCoeff;
+    int    IGRIters;
+    int    IGRWarmStartIters;
+    /* MultiPhaseParams (nPhases == 0: single phase) */
+    int    nPhases;
+    double phaseGamma[SIFV_MAX_PHASES];
+    double phasePInf[SIFV_MAX_PHASES];
+    double alphaMin;
+    /* BodyForceParams: accel_d(t) = a_d + b_d cos(c_d t + d_d) */
+    double bfA[3], bfB[3], bfC[3], bfD[3];
+    /* SIFV_PREC_* */
+    int    precision;
+} sifv_config_t;
+
+/* Mesh: physical node coordinates per axis (n+1 entries; NULL for an
+ * inactive axis means {0, 1}) and the six face boundary conditions
+ * (XLow, XHigh, YLow, YHigh, ZLow, ZHigh).  Periodic axes must be periodic
+ * on both faces. */
+typedef struct sifv_mesh {
+    int nx, ny, nz;
+    const double* xNodes;
+    const double* yNodes;
+    const double* zNodes;
+    int bc[6];
+} sifv_mesh_t;
+
+typedef struct sifv_ctx sifv_ctx_t;
+
+/* Fill a config with the reference's defaults (SimulationConfig members'
+ * initialisers, include/SimulationConfig.hpp:22-92). */
+void sifv_config_defaults(sifv_config_t* cfg);
+
+/* Validate exactly as SimulationConfig::validate()
+ * (include/SimulationConfig.hpp:123-209); message via sifv_last_error(NULL). */
+int sifv_config_validate(const sifv_config_t* cfg);
+
+/* Create a context on CUDA device `device`: allocates the device SoA state
+ * (totalCells doubles per field, ghosts included) and scratch. */
+int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device,
+                sifv_ctx_t** out);
+int sifv_destroy(sifv_ctx_t* ctx);
+
+/* Message of the last error on this context (ctx == NULL: last
+ * context-free error of the calling thread). */
+const char* sifv_last_error(const sifv_ctx_t* ctx);
+
+/* Extents including ghosts (RectilinearMesh::nxTotal/nyTotal/nzTotal). */
+int sifv_extents(const sifv_ctx_t* ctx, int* nxTot, int* nyTot, int* nzTot);
+size_t sifv_total_cells(const sifv_ctx_t* ctx);
+
+/* Copy a whole field (totalCells doubles, x fastest, ghosts included) in or
+ * out.  onDevice != 0: the pointer is device memory on the context's
+ * device.  Copies are ordered on the context's stream and complete before
+ * return. */
+int sifv_set_field(sifv_ctx_t* ctx, int field, const double* src, int onDevice);
+int sifv_get_field(sifv_ctx_t* ctx, int field, double* dst, int onDevice);
+/* Device address of a field (zero-copy access for device-resident callers). */
+int sifv_field_device_ptr(sifv_ctx_t* ctx, int field, double** dptr);
+
+/* Use a caller-owned cudaStream_t (NULL: the context's own stream). */
+int sifv_set_stream(sifv_ctx_t* ctx, void* stream);
+int sifv_synchronize(sifv_ctx_t* ctx);
+
+/* One time step, ExplicitSolver::step or SemiImplicitSolver::step by
+ * cfg->semiImplicit.  `step` and `time` are SimulationConfig::step/time
+ * (IGR warm start on step 0; body-force phase).  targetDt > 0 caps dt as
+ * in the reference.  *dtOut receives the dt taken.  Returns
+ * SIFV_NOT_CONVERGED (still a completed step) when any pressure solve of
+ * the step reached maxPressureIters. */
+int sifv_step(sifv_ctx_t* ctx, int step, double time, double targetDt, double* dtOut);
+
+/* nSteps steps back to back with no host round trip between them: dt is
+ * reduced and applied on the device, and each step's dt is capped by
+ * tEnd - t (tEnd <= 0: no cap).  Explicit path only.  On return
+ * *timeOut = time after the last step.  Steps after t reaches tEnd are
+ * skipped on the device. */
+int sifv_advance(sifv_ctx_t* ctx, int step0, double time0, double tEnd, int nSteps,
+                 double* timeOut, int* stepsTaken);
+
+/* Jacobi iterations of the last pressure solve (SemiImplicitSolver::
+ * lastPressureIterations, include/SemiImplicitSolver.hpp:46). */
+int sifv_last_pressure_iterations(const sifv_ctx_t* ctx, int* iters);
+
+/* PressureSolver::solve (include/PressureSolver.hpp:17-38) for the Jacobi
+ * solver: (1 + rhoc2 dt^2 L) p = rhs + rhoc2 dt^2 offdiag(p), iterated
+ * until max|p_new - p| < tol or maxIter.  All arrays are totalCells long;
+ * `pressure` is the initial guess on entry and the solution on return
+ * (interior cells; ghosts are not written).  onDevice != 0: device
+ * pointers.  *iters as the reference's return value. */
+int sifv_pressure_solve(sifv_ctx_t* ctx, const double* rho, const double* rhoc2,
+                        const double* rhs, double* pressure, double dt, double tol,
+                        int maxIter, int onDevice, int* iters);
+
+/* IGRSolver::solveEntropicPressure on the context's state: velocity
+ * gradients from the current primitive fields (ghosts must be filled, see
+ * sifv_apply_bc), then the lexicographic Gauss-Seidel sweeps of the
+ * reference (IGRWarmStartIters on step 0, else IGRIters) updating sigma. */
+int sifv_igr_solve(sifv_ctx_t* ctx, int step);
+
+/* Time-step reductions on the context's state (interior cells). */
+int sifv_acoustic_dt(sifv_ctx_t* ctx, double cfl, double maxDt, double* dt);
+int sifv_advective_dt(sifv_ctx_t* ctx, double cfl, double maxDt, double* dt);
+
+/* Conservative -> primitive on interior cells, and the PRIM ghost fill. */
+int sifv_convert_cons_to_prim(sifv_ctx_t* ctx);
+int sifv_apply_bc(sifv_ctx_t* ctx);
+
+/* Device time of the kernels launched by the last sifv_step / sifv_advance
+ * call, and the number of kernel launches it made. */
+int sifv_last_step_stats(const sifv_ctx_t* ctx, double* deviceMs, int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIFV_H */

@@ -1,0 +1,303 @@
+"""ctypes mirror of the C ABI in ``include/sifv.h``.
+
+The same structs and call shapes serve every library that implements the
+ABI: the CUDA library of this package (symbol prefix ``sifv_``) and, in the
+tests only, the CPU oracles (``sifvo_`` for the C restatement, ``sifvr_``
+for the reference build).  ``Config`` mirrors ``SimulationConfig``
+(include/SimulationConfig.hpp:72-210 of SemiImplicitFV) field for field and
+``config_defaults`` reproduces its member initialisers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+MAX_PHASES = 8
+
+# status codes
+OK, NOT_CONVERGED = 0, 1
+ERR_BAD_CONFIG, ERR_BAD_ARG, ERR_CUDA, ERR_NAN = -1, -2, -3, -4
+ERR_UNSUPPORTED, ERR_TIMEOUT, ERR_NO_DEVICE = -5, -6, -7
+
+# ReconstructionOrder (include/SimulationConfig.hpp:13-20)
+WENO1, WENO3, WENO5, UPWIND1, UPWIND3, UPWIND5 = range(6)
+# RiemannSolverType (include/RiemannSolver.hpp:16)
+LF, RUSANOV, HLLC = range(3)
+# BoundaryCondition (include/RectilinearMesh.hpp:14-20)
+BC_SYMMETRY, BC_OUTFLOW, BC_PERIODIC, BC_SLIPWALL, BC_NOSLIPWALL = range(5)
+EOS_IDEAL, EOS_STIFFENED = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+# field identifiers (SolutionState members, include/SolutionState.hpp:73-113)
+F_RHO, F_RHOU, F_RHOV, F_RHOW, F_RHOE = 0, 1, 2, 3, 4
+F_VELU, F_VELV, F_VELW, F_PRES, F_SIGMA = 5, 6, 7, 8, 9
+
+
+def F_ALPHARHO(ph: int) -> int:
+    return 16 + ph
+
+
+def F_ALPHA(ph: int) -> int:
+    return 32 + ph
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("nGhost", C.c_int), ("RKOrder", C.c_int),
+        ("useIGR", C.c_int), ("semiImplicit", C.c_int), ("reconOrder", C.c_int),
+        ("wenoEps", C.c_double),
+        ("riemannSolver", C.c_int), ("eosKind", C.c_int),
+        ("gamma", C.c_double), ("pInf", C.c_double),
+        ("cfl", C.c_double), ("constDt", C.c_double), ("maxDt", C.c_double), ("minDt", C.c_double),
+        ("siCfl", C.c_double), ("siMaxDt", C.c_double), ("siMinDt", C.c_double),
+        ("maxPressureIters", C.c_int), ("pressureTol", C.c_double),
+        ("alphaCoeff", C.c_double), ("IGRIters", C.c_int), ("IGRWarmStartIters", C.c_int),
+        ("nPhases", C.c_int),
+        ("phaseGamma", C.c_double * MAX_PHASES), ("phasePInf", C.c_double * MAX_PHASES),
+        ("alphaMin", C.c_double),
+        ("bfA", C.c_double * 3), ("bfB", C.c_double * 3), ("bfC", C.c_double * 3), ("bfD", C.c_double * 3),
+        ("precision", C.c_int),
+    ]
+
+
+class Mesh(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("xNodes", C.POINTER(C.c_double)), ("yNodes", C.POINTER(C.c_double)),
+        ("zNodes", C.POINTER(C.c_double)),
+        ("bc", C.c_int * 6),
+    ]
+
+
+def config_defaults(**overrides) -> Config:
+    """SimulationConfig defaults (include/SimulationConfig.hpp:22-92), IdealGasEOS(1.4)."""
+    c = Config()
+    c.dim, c.nGhost, c.RKOrder = 3, 2, 1
+    c.useIGR, c.semiImplicit = 0, 0
+    c.reconOrder, c.wenoEps = WENO1, 1e-6
+    c.riemannSolver, c.eosKind, c.gamma, c.pInf = HLLC, EOS_IDEAL, 1.4, 0.0
+    c.cfl, c.constDt, c.maxDt, c.minDt = 0.8, -1.0, 1e-2, 1e-12
+    c.siCfl, c.siMaxDt, c.siMinDt = 0.8, 1e-2, 1e-12
+    c.maxPressureIters, c.pressureTol = 100, 1e-8
+    c.alphaCoeff, c.IGRIters, c.IGRWarmStartIters = 1.0, 5, 50
+    c.nPhases, c.alphaMin = 0, 1e-8
+    c.precision = PREC_FP64
+    for k, v in overrides.items():
+        if k in ("phaseGamma", "phasePInf"):
+            arr = getattr(c, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        elif k in ("bfA", "bfB", "bfC", "bfD"):
+            arr = getattr(c, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            if not hasattr(c, k):
+                raise AttributeError(f"unknown config field {k}")
+            setattr(c, k, v)
+    return c
+
+
+def linspace_nodes(n: int, lo: float, hi: float) -> np.ndarray:
+    """Global node array of Runtime::createUniformMesh: a + (b - a) * i / (n - 1)
+    with n = cells + 1 points (src/Runtime.cpp:12-17), evaluated in the same order."""
+    npts = n + 1
+    i = np.arange(npts, dtype=np.float64)
+    return lo + ((hi - lo) * i) / float(npts - 1)
+
+
+class MeshSpec:
+    """Node arrays + boundary conditions; keeps the numpy buffers alive."""
+
+    def __init__(self, x: np.ndarray, y: Optional[np.ndarray] = None, z: Optional[np.ndarray] = None,
+                 bc: Sequence[int] = (BC_OUTFLOW,) * 6):
+        self.x = np.ascontiguousarray(x, dtype=np.float64)
+        self.y = None if y is None else np.ascontiguousarray(y, dtype=np.float64)
+        self.z = None if z is None else np.ascontiguousarray(z, dtype=np.float64)
+        self.bc = list(bc)
+
+    def cstruct(self) -> Mesh:
+        m = Mesh()
+        dp = C.POINTER(C.c_double)
+        m.nx = len(self.x) - 1
+        m.ny = 1 if self.y is None else len(self.y) - 1
+        m.nz = 1 if self.z is None else len(self.z) - 1
+        m.xNodes = self.x.ctypes.data_as(dp)
+        m.yNodes = self.y.ctypes.data_as(dp) if self.y is not None else dp()
+        m.zNodes = self.z.ctypes.data_as(dp) if self.z is not None else dp()
+        for f in range(6):
+            m.bc[f] = self.bc[f]
+        return m
+
+
+class AbiError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"status {status}: {msg}")
+        self.status = status
+
+
+_SIGS = {
+    "create": (C.c_int, [C.POINTER(Config), C.POINTER(Mesh), C.c_int, C.POINTER(C.c_void_p)]),
+    "destroy": (C.c_int, [C.c_void_p]),
+    "last_error": (C.c_char_p, [C.c_void_p]),
+    "extents": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "total_cells": (C.c_size_t, [C.c_void_p]),
+    "set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "last_pressure_iterations": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "pressure_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "igr_solve": (C.c_int, [C.c_void_p, C.c_int]),
+    "acoustic_dt": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "advective_dt": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "convert_cons_to_prim": (C.c_int, [C.c_void_p]),
+    "apply_bc": (C.c_int, [C.c_void_p]),
+}
+
+_OPTIONAL_SIGS = {
+    "advance": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
+                          C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "synchronize": (C.c_int, [C.c_void_p]),
+    "set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "field_device_ptr": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "last_step_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "set_pressure_solver": (C.c_int, [C.c_void_p, C.c_int]),
+    "config_validate": (C.c_int, [C.POINTER(Config)]),
+}
+
+
+class Backend:
+    """A loaded library implementing the ABI under ``prefix``."""
+
+    def __init__(self, lib: C.CDLL, prefix: str, name: str = ""):
+        self.lib = lib
+        self.prefix = prefix
+        self.name = name or prefix
+        self.fn = {}
+        for k, (res, args) in _SIGS.items():
+            f = getattr(lib, prefix + k)
+            f.restype, f.argtypes = res, args
+            self.fn[k] = f
+        for k, (res, args) in _OPTIONAL_SIGS.items():
+            f = getattr(lib, prefix + k, None)
+            if f is not None:
+                f.restype, f.argtypes = res, args
+                self.fn[k] = f
+
+    def error(self, ctx=None) -> str:
+        m = self.fn["last_error"](ctx)
+        return m.decode() if m else ""
+
+    def create(self, cfg: Config, mesh: MeshSpec, device: int = 0) -> "Context":
+        h = C.c_void_p()
+        ms = mesh.cstruct()
+        st = self.fn["create"](C.byref(cfg), C.byref(ms), device, C.byref(h))
+        if st != OK:
+            raise AbiError(st, self.error(None))
+        return Context(self, h, cfg, mesh)
+
+
+class Context:
+    """One solver instance (a SolutionState + solver) in a backend."""
+
+    def __init__(self, be: Backend, handle: C.c_void_p, cfg: Config, mesh: MeshSpec):
+        self.be, self.h, self.cfg, self.mesh = be, handle, cfg, mesh
+        nx, ny, nz = C.c_int(), C.c_int(), C.c_int()
+        self._check(be.fn["extents"](handle, C.byref(nx), C.byref(ny), C.byref(nz)))
+        self.shape = (nz.value, ny.value, nx.value)       # numpy (k, j, i), x fastest
+        self.ncells = nx.value * ny.value * nz.value
+        self.ng = cfg.nGhost
+
+    def _check(self, st: int) -> int:
+        if st < 0:
+            raise AbiError(st, self.be.error(self.h))
+        return st
+
+    def close(self):
+        if self.h:
+            self.be.fn["destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_field(self, fid: int, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        assert a.size == self.ncells, (a.size, self.ncells)
+        self._check(self.be.fn["set_field"](self.h, fid, a.ctypes.data_as(C.c_void_p), 0))
+
+    def get_field(self, fid: int) -> np.ndarray:
+        out = np.empty(self.ncells, dtype=np.float64)
+        self._check(self.be.fn["get_field"](self.h, fid, out.ctypes.data_as(C.c_void_p), 0))
+        return out.reshape(self.shape)
+
+    def set_state(self, fields: dict):
+        for fid, arr in fields.items():
+            self.set_field(fid, arr)
+
+    def step(self, step: int, time: float, target_dt: float = -1.0) -> float:
+        dt = C.c_double()
+        self._check(self.be.fn["step"](self.h, step, time, target_dt, C.byref(dt)))
+        return dt.value
+
+    def advance(self, step0: int, time0: float, t_end: float, n_steps: int):
+        t, n = C.c_double(), C.c_int()
+        self._check(self.be.fn["advance"](self.h, step0, time0, t_end, n_steps, C.byref(t), C.byref(n)))
+        return t.value, n.value
+
+    def last_pressure_iterations(self) -> int:
+        it = C.c_int()
+        self._check(self.be.fn["last_pressure_iterations"](self.h, C.byref(it)))
+        return it.value
+
+    def pressure_solve(self, rho, rhoc2, rhs, p, dt, tol, max_iter):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (rho, rhoc2, rhs)]
+        pp = np.array(p, dtype=np.float64).reshape(-1)
+        it = C.c_int()
+        st = self._check(self.be.fn["pressure_solve"](
+            self.h, *[a.ctypes.data_as(C.c_void_p) for a in arrs], pp.ctypes.data_as(C.c_void_p),
+            dt, tol, max_iter, 0, C.byref(it)))
+        return pp.reshape(self.shape), it.value, st
+
+    def igr_solve(self, step: int):
+        self._check(self.be.fn["igr_solve"](self.h, step))
+
+    def acoustic_dt(self, cfl: float, max_dt: float) -> float:
+        d = C.c_double()
+        self._check(self.be.fn["acoustic_dt"](self.h, cfl, max_dt, C.byref(d)))
+        return d.value
+
+    def advective_dt(self, cfl: float, max_dt: float) -> float:
+        d = C.c_double()
+        self._check(self.be.fn["advective_dt"](self.h, cfl, max_dt, C.byref(d)))
+        return d.value
+
+    def convert_cons_to_prim(self):
+        self._check(self.be.fn["convert_cons_to_prim"](self.h))
+
+    def apply_bc(self):
+        self._check(self.be.fn["apply_bc"](self.h))
+
+    def set_pressure_solver(self, kind: int):
+        self._check(self.be.fn["set_pressure_solver"](self.h, kind))
+
+    def last_step_stats(self):
+        ms, n = C.c_double(), C.c_int()
+        self._check(self.be.fn["last_step_stats"](self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def interior(self, arr: np.ndarray) -> np.ndarray:
+        """Slice the physical cells out of a (k, j, i) field."""
+        d = self.cfg.dim
+        g = self.ng
+        gi = g
+        gj = g if d >= 2 else 0
+        gk = g if d >= 3 else 0
+        nz, ny, nx = self.shape
+        return arr[gk:nz - gk, gj:ny - gj, gi:nx - gi]

@@ -1,0 +1,215 @@
+"""Initial conditions of the parity cases, restated from the reference's
+example drivers and the configurations the benchmark is quoted on.
+
+Each builder returns ``(cfg, mesh, fields)`` where ``fields`` maps a field
+id to a full (ghosts included, ghosts zero) float64 array, so that every
+backend receives bit-identical inputs.  Conservative fields are computed the
+way the examples compute them (EOS toConservative / mixtureTotalEnergy),
+operation for operation, in float64 numpy.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from semiimplicitfv_b200 import abi
+from semiimplicitfv_b200.abi import (BC_OUTFLOW, BC_PERIODIC, F_ALPHA, F_ALPHARHO, F_PRES, F_RHO, F_RHOE,
+                                     F_RHOU, F_RHOV, F_RHOW, F_SIGMA, F_VELU, F_VELV, F_VELW)
+
+
+def _ext_shape(cfg, nx, ny, nz):
+    g = cfg.nGhost
+    return (nz + 2 * g if cfg.dim >= 3 else 1, ny + 2 * g if cfg.dim >= 2 else 1, nx + 2 * g)
+
+
+def _interior_slices(cfg):
+    g = cfg.nGhost
+    sk = slice(g, -g) if cfg.dim >= 3 else slice(0, 1)
+    sj = slice(g, -g) if cfg.dim >= 2 else slice(0, 1)
+    return sk, sj, slice(g, -g)
+
+
+def _centroids(nodes):
+    return 0.5 * (nodes[:-1] + nodes[1:])
+
+
+def _single_phase_fields(cfg, shape, rho, u, v, w, p, eos_gamma, eos_pinf=0.0, stiffened=False):
+    """setPrimitiveState + setConservativeState(eos.toConservative(W)) on the
+    interior (IdealGasEOS::toConservative src/IdealGasEOS.cpp:66-82,
+    StiffenedGasEOS::toConservative src/StiffenedGasEOS.cpp:66-82)."""
+    dim = cfg.dim
+    sl = _interior_slices(cfg)
+    f = {}
+    z = lambda: np.zeros(shape)
+    for fid in (F_RHO, F_RHOU, F_RHOE, F_VELU, F_PRES, F_SIGMA):
+        f[fid] = z()
+    if dim >= 2:
+        f[F_RHOV], f[F_VELV] = z(), z()
+    if dim >= 3:
+        f[F_RHOW], f[F_VELW] = z(), z()
+    f[F_RHO][sl] = rho
+    f[F_VELU][sl] = u
+    f[F_PRES][sl] = p
+    f[F_RHOU][sl] = rho * u
+    ke = 0.0 + u * u
+    if dim >= 2:
+        f[F_VELV][sl] = v
+        f[F_RHOV][sl] = rho * v
+        ke = ke + v * v
+    if dim >= 3:
+        f[F_VELW][sl] = w
+        f[F_RHOW][sl] = rho * w
+        ke = ke + w * w
+    ke = ke * (0.5 * rho)
+    if stiffened:
+        e = (p + eos_gamma * eos_pinf) / (eos_gamma - 1.0)
+    else:
+        e = p / (eos_gamma - 1.0)
+    f[F_RHOE][sl] = e + ke
+    return f
+
+
+def sod(n=1000, cfl=0.6, recon=abi.WENO5, riemann=abi.HLLC, ng=3, rk=3):
+    """1D Sod shock tube (examples/1D_sod_shocktube/1D_sod_shocktube.cpp:24-50):
+    x in [0,1], (rho,u,p) = (1,0,1) for x_c < 0.5 else (0.125,0,0.1)."""
+    cfg = abi.config_defaults(dim=1, nGhost=ng, RKOrder=rk, reconOrder=recon, riemannSolver=riemann, cfl=cfl)
+    x = abi.linspace_nodes(n, 0.0, 1.0)
+    xc = _centroids(x)
+    left = xc < 0.5
+    rho = np.where(left, 1.0, 0.125)
+    p = np.where(left, 1.0, 0.1)
+    u = np.zeros(n)
+    shape = _ext_shape(cfg, n, 1, 1)
+    fields = _single_phase_fields(cfg, shape, rho[None, None, :], u[None, None, :], None, None,
+                                  p[None, None, :], 1.4)
+    return cfg, abi.MeshSpec(x, bc=[BC_OUTFLOW] * 6), fields
+
+
+RIEMANN2D_STATES = {  # (rho, u, v, p) per quadrant, split at (0.8, 0.8)
+    "q1": (1.5, 0.0, 0.0, 1.5),
+    "q2": (0.5323, 1.206, 0.0, 0.3),
+    "q3": (0.138, 1.206, 1.206, 0.029),
+    "q4": (0.5323, 0.0, 1.206, 0.3),
+}
+
+
+def riemann2d(n=64, cfl=0.6, recon=abi.WENO5, riemann=abi.HLLC, ng=3, weno_eps=1e-6, bc=BC_OUTFLOW, rk=3):
+    """2D four-quadrant Riemann problem (examples/2D_riemann/2D_riemann.cpp:24-76
+    with the 0.5323 states of the benchmark configuration)."""
+    cfg = abi.config_defaults(dim=2, nGhost=ng, RKOrder=rk, reconOrder=recon, riemannSolver=riemann, cfl=cfl,
+                              wenoEps=weno_eps)
+    x = abi.linspace_nodes(n, 0.0, 1.0)
+    y = abi.linspace_nodes(n, 0.0, 1.0)
+    X, Y = np.meshgrid(_centroids(x), _centroids(y), indexing="xy")
+    q = np.empty(X.shape, dtype=object)
+    rho = np.empty(X.shape); u = np.empty(X.shape); v = np.empty(X.shape); p = np.empty(X.shape)
+    for name, mask in (("q1", (X >= 0.8) & (Y >= 0.8)), ("q2", (X < 0.8) & (Y >= 0.8)),
+                       ("q3", (X < 0.8) & (Y < 0.8)), ("q4", (X >= 0.8) & (Y < 0.8))):
+        r_, u_, v_, p_ = RIEMANN2D_STATES[name]
+        rho[mask], u[mask], v[mask], p[mask] = r_, u_, v_, p_
+    shape = _ext_shape(cfg, n, n, 1)
+    fields = _single_phase_fields(cfg, shape, rho[None], u[None], v[None], None, p[None], 1.4)
+    return cfg, abi.MeshSpec(x, y, bc=[bc] * 6), fields
+
+
+def acoustic3d(n=16, semi=True, igr=True, rk=1, recon=abi.WENO5, riemann=abi.HLLC, ng=3, tol=1e-6,
+               max_iter=1000, alpha_coeff=10.0, igr_iters=5, warm=50):
+    """3D low-Mach acoustic pulse on the periodic unit cube:
+    rho = 1, u = (0.1, 0.05, 0), p = 1 + 1e-3 exp(-|x - 0.5|^2 / 0.01)."""
+    cfg = abi.config_defaults(dim=3, nGhost=ng, RKOrder=rk, reconOrder=recon, riemannSolver=riemann,
+                              semiImplicit=int(semi), useIGR=int(igr), siCfl=0.8, pressureTol=tol,
+                              maxPressureIters=max_iter, alphaCoeff=alpha_coeff, IGRIters=igr_iters,
+                              IGRWarmStartIters=warm)
+    x = abi.linspace_nodes(n, 0.0, 1.0)
+    c = _centroids(x)
+    Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+    r2 = (X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2
+    p = 1.0 + 1e-3 * np.exp(-r2 / 0.01)
+    rho = np.ones_like(p)
+    u = np.full_like(p, 0.1); v = np.full_like(p, 0.05); w = np.zeros_like(p)
+    shape = _ext_shape(cfg, n, n, n)
+    fields = _single_phase_fields(cfg, shape, rho, u, v, w, p, 1.4)
+    return cfg, abi.MeshSpec(x, x, x, bc=[BC_PERIODIC] * 6), fields
+
+
+def water_air(n=256, x_interface=0.5, p_left=5e8, rho_air=1.0, cfl=0.5, recon=abi.WENO5, riemann=abi.HLLC,
+              ng=3, alpha_min=1e-8, rk=3):
+    """1D two-phase water-air shock tube (examples/1D_liquid_gas_shocktube/
+    1D_liquid_gas_shocktube.cpp:34-77): water gamma 4.4, pInf 6e8, rho 1000 at
+    p_left left of the interface; air gamma 1.4, rho_air, p 1e5 right."""
+    cfg = abi.config_defaults(dim=1, nGhost=ng, RKOrder=rk, reconOrder=recon, riemannSolver=riemann, cfl=cfl,
+                              nPhases=2, phaseGamma=[4.4, 1.4], phasePInf=[6.0e8, 0.0], alphaMin=alpha_min)
+    x = abi.linspace_nodes(n, 0.0, 1.0)
+    xc = _centroids(x)
+    left = xc < x_interface
+    rho = np.where(left, 1000.0, rho_air)
+    p = np.where(left, p_left, 1.0e5)
+    aw = np.where(left, 1.0 - alpha_min, alpha_min)
+    aa = 1.0 - aw
+    shape = _ext_shape(cfg, n, 1, 1)
+    sl = _interior_slices(cfg)
+    f = {fid: np.zeros(shape) for fid in (F_RHO, F_RHOU, F_RHOE, F_VELU, F_PRES, F_SIGMA,
+                                          F_ALPHARHO(0), F_ALPHARHO(1), F_ALPHA(0), F_ALPHA(1))}
+    ar0, ar1 = aw * rho, aa * rho
+    f[F_ALPHARHO(0)][sl] = ar0
+    f[F_ALPHARHO(1)][sl] = ar1
+    f[F_ALPHA(0)][sl] = aw
+    f[F_ALPHA(1)][sl] = aa
+    f[F_RHO][sl] = ar0 + ar1
+    f[F_PRES][sl] = p
+    # mixtureTotalEnergy(rho, p, alphas, ke=0) (src/MixtureEOS.cpp:65-76)
+    e = 0.0 + aw * (p + 4.4 * 6.0e8) / (4.4 - 1.0)
+    e = e + aa * (p + 1.4 * 0.0) / (1.4 - 1.0)
+    f[F_RHOE][sl] = e
+    return cfg, abi.MeshSpec(x, bc=[BC_OUTFLOW] * 6), f
+
+
+def advection1d(n=128, semi=False, riemann=abi.LF, cfl=0.8, rk=3):
+    """1D periodic density-pulse advection (examples/1D_advection/1D_advection.cpp:36-67,
+    85-99): rho0 = 1.225 (1 + 0.01 exp(-d^2 / 0.05^2)), u = 10, p = 101325."""
+    rho0, p0, u0, amp, xcen, sig = 1.225, 101325.0, 10.0, 0.01, 0.5, 0.05
+    if semi:
+        cfg = abi.config_defaults(dim=1, nGhost=3, RKOrder=rk, reconOrder=abi.WENO5, riemannSolver=riemann,
+                                  semiImplicit=1, siCfl=cfl, siMaxDt=1e-2, pressureTol=1e-9, maxPressureIters=200,
+                                  alphaCoeff=10.0, IGRIters=5)
+    else:
+        cfg = abi.config_defaults(dim=1, nGhost=3, RKOrder=rk, reconOrder=abi.WENO5, riemannSolver=riemann, cfl=cfl,
+                                  maxDt=1e-2)
+    x = abi.linspace_nodes(n, 0.0, 1.0)
+    xc = _centroids(x)
+    d = xc - xcen
+    d = d - 1.0 * np.round(d / 1.0)
+    rho = rho0 * (1.0 + amp * np.exp(-(d * d) / (sig * sig)))
+    shape = _ext_shape(cfg, n, 1, 1)
+    fields = _single_phase_fields(cfg, shape, rho[None, None, :], np.full((1, 1, n), u0), None, None,
+                                  np.full((1, 1, n), p0), 1.4)
+    return cfg, abi.MeshSpec(x, bc=[BC_PERIODIC] * 6), fields
+
+
+def run_steps(ctx, nsteps, t_end=None, step0=0, time0=0.0):
+    """Drive ctx.step like the reference drivers: targetDt = t_end - t when
+    given.  Returns (time, steps, dts)."""
+    t, s, dts = time0, step0, []
+    while s - step0 < nsteps and (t_end is None or t < t_end):
+        target = (t_end - t) if t_end is not None else -1.0
+        dt = ctx.step(s, t, target)
+        dts.append(dt)
+        t += dt
+        s += 1
+    return t, s, dts
+
+
+def run_time_loop(ctx, t_end, output_interval):
+    """runTimeLoop's dt sequence (src/RKTimeStepping.cpp:241-275): targetDt is
+    clamped to the next output time; config.step increments per step."""
+    time, step = 0.0, 0
+    next_out = output_interval
+    while time < t_end:
+        target = t_end - time
+        if next_out < t_end:
+            target = min(target, next_out - time)
+        dt = ctx.step(step, time, target)
+        time += dt
+        step += 1
+        if time >= next_out - 1e-12 * output_interval:
+            next_out += output_interval
+    return time, step
