@@ -1,0 +1,272 @@
+"""Benchmark: cell-updates/s of the SSP-RK3 WENO5-HLLC step on the 2D
+four-quadrant Riemann problem, 4096 x 4096 cells, FP64.
+
+One "step" is one full time step (three RK stages, dt reduction, ghost
+fills) over the whole grid.  `value` times K steps queued back to back with
+the state resident in HBM (sifv_advance); `e2e` times K calls of the drop-in
+entry point sifv_step through the C ABI, each returning dt to the host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+Multi-GPU: one process per GPU (torchrun), every rank advances its own
+4096^2 instance (weak scaling, replicas: the single-GPU path needs no
+exchange); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "cell-updates/s per RK3 step (2D Riemann 4096^2, WENO5+HLLC, FP64)"
+UNIT = "cell-updates/s"
+BYTES_PER_CELL_UPDATE = 256   # algorithmic: 64 B x 4 conserved variables per RK3 step
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def _peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_rate(kind: str, n: int, steps: int) -> float:
+    """Reference (or oracle) CPU path on one core: cell-updates/s on an n x n
+    instance of the same problem, `steps` steps after one warm-up step."""
+    import backends
+    import cases
+    be = backends.reference(release=True) if kind == "reference" else backends.oracle()
+    ctx = backends.make(be, cases.riemann2d(n))
+    ctx.step(0, 0.0, -1.0)
+    t0 = time.perf_counter()
+    t = 0.0
+    for s in range(steps):
+        t += ctx.step(1 + s, t, -1.0)
+    dt = time.perf_counter() - t0
+    return n * n * steps / dt
+
+
+def _cpu_worker(args):
+    kind, n, steps = args
+    return cpu_rate(kind, n, steps)
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    import backends
+    kind = "reference" if backends.reference(release=True) is not None else "port"
+    procs = os.cpu_count() or 1
+    n = 512
+    steps = max(args.steps, 1)
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(procs) as pool:
+        rates = pool.map(_cpu_worker, [(kind, n, steps)] * procs)
+    wall = time.perf_counter() - t0
+    value = float(sum(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 4096 * 4096 / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "2D four-quadrant Riemann 4096x4096 (sampled as independent 512x512 instances)",
+                   "scheme": "WENO5+HLLC SSP-RK3 CFL0.6"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
+                         "sample": f"{procs} concurrent single-thread processes, each {steps} steps of a "
+                                   f"{n}x{n} instance (reference is single-threaded per rank); wall {wall:.1f}s"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_cuda(args):
+    import numpy as np
+    import torch
+
+    ws, rank, local = _dist()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+
+    import backends
+    import cases
+    from semiimplicitfv_b200 import abi
+    n = args.n
+    case = cases.riemann2d(n)
+    ctx = backends.cuda().create(case[0], case[1], local)
+    # inputs uploaded from pinned host memory
+    for fid, arr in case[2].items():
+        pinned = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
+        ctx.be.fn["set_field"](ctx.h, fid, ctypes.c_void_p(pinned.data_ptr()), 0)
+    stream = torch.cuda.current_stream()
+    ctx.be.fn["set_stream"](ctx.h, ctypes.c_void_p(stream.cuda_stream))
+    cells = n * n
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws > 1:
+            t = torch.tensor([x], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    # warm-up
+    t_sim, s_sim = ctx.advance(0, 0.0, -1.0, args.warmup)
+    step_idx = args.warmup
+
+    # ---- device-resident timed region -------------------------------------
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        t_sim, _ = ctx.advance(step_idx, t_sim, -1.0, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    step_idx += args.steps
+    _, launches = ctx.last_step_stats()
+    value = ws * cells * args.steps / (ms / 1e3)
+
+    # ---- end-to-end through sifv_step --------------------------------------
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for q in range(args.steps):
+        t_sim += ctx.step(step_idx + q, t_sim, -1.0)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = ws * cells * args.steps / e2e_s
+
+    peak, peak_kind = _peaks()
+    achieved = BYTES_PER_CELL_UPDATE * cells * args.steps / (ms / 1e3) / 1e9
+    result = None
+    if rank == 0:
+        kind = "reference" if backends.reference(release=True) is not None else "port"
+        cpu_n, cpu_steps = 768, 3
+        cpu = cpu_rate(kind, cpu_n, cpu_steps)
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"2D four-quadrant Riemann {n}x{n} (+3 ghosts), WENO5+HLLC SSP-RK3 CFL0.6, "
+                                   "outflow, FP64, state resident in HBM",
+                       "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (4 x 134 MB state)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "whole RK3 step (256 B algorithmic per cell-update)",
+                         "peak_source": peak_kind},
+            "cpu_baseline": {"value": cpu, "unit": UNIT, "cores": 1, "kind": kind,
+                             "sample": f"{cpu_n}x{cpu_n} instance, {cpu_steps} steps, 1 thread"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
+                    "api": "sifv_step (returns dt to the host every step)"},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(result), flush=True)
+    ctx.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--n", type=int, default=4096)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cuda(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,768 @@
+// sifv_capi.cu -- the C ABI of include/sifv.h: context, device allocation,
+// the step orchestration (ExplicitSolver::step / SemiImplicitSolver::step)
+// and the standalone PressureSolver / IGR / dt entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sifv.h"
+#include "sifv_kernels.cuh"
+
+using namespace sifv;
+
+namespace {
+
+thread_local std::string g_err;
+
+constexpr int kCellThreads = 256;
+constexpr int kFaceThreads = 128;
+
+}  // namespace
+
+struct sifv_ctx {
+    sifv_config_t cfg{};
+    Params P{};
+    Fields F{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t ownStream = nullptr;
+    std::vector<void*> allocs;
+    Ctl* ctl = nullptr;        // device control block
+    Ctl* ctlHost = nullptr;    // pinned mirror
+    int resCap = 0;
+    std::string err;
+    int lastIters = 0;
+    float lastMs = 0.f;
+    int lastLaunches = 0;
+    int launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    size_t ncells = 0, nint = 0;
+    double alphaIGR = 0.0;
+    int nphT = 0;   // NPH template bucket (0, 2 or 8)
+    int W = 5;      // stencil width
+    // scratch for the standalone pressure solve with host arrays
+    double *sRho = nullptr, *sRhoc2 = nullptr, *sRhs = nullptr, *sP = nullptr;
+};
+
+namespace {
+
+int fail(sifv_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                     \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return fail(ctx, SIFV_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define LAUNCH_CHECK(ctx)                                                                                  \
+    do {                                                                                                   \
+        cudaError_t e_ = cudaGetLastError();                                                               \
+        if (e_ != cudaSuccess) return fail(ctx, SIFV_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+unsigned blocks(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+// RectilinearMesh::buildExtendedNodes, src/RectilinearMesh.cpp:91-114
+std::vector<double> build_ext(const double* phys, int nCells, int ng) {
+    std::vector<double> ext(nCells + 2 * ng + 1);
+    for (int i = 0; i <= nCells; ++i) ext[ng + i] = phys[i];
+    for (int g = 1; g <= ng; ++g) {
+        int mirror = std::min(g - 1, nCells - 1);
+        double width = phys[mirror + 1] - phys[mirror];
+        ext[ng - g] = ext[ng - g + 1] - width;
+    }
+    for (int g = 1; g <= ng; ++g) {
+        int mirror = std::max(nCells - g, 0);
+        double width = phys[mirror + 1] - phys[mirror];
+        ext[ng + nCells + g] = ext[ng + nCells + g - 1] + width;
+    }
+    return ext;
+}
+
+int validate(const sifv_config_t* c, std::string& msg) {
+    // SimulationConfig::validate, include/SimulationConfig.hpp:123-209
+    auto bad = [&](const char* m) { msg = m; return SIFV_ERR_BAD_CONFIG; };
+    if (c->dim < 1 || c->dim > 3) return bad("dim must be 1, 2, or 3");
+    if (c->RKOrder < 1 || c->RKOrder > 3) return bad("RKOrder must be 1, 2, or 3");
+    if (c->reconOrder < SIFV_WENO1 || c->reconOrder > SIFV_UPWIND5) return bad("unknown reconOrder");
+    int req = (c->reconOrder == SIFV_WENO1 || c->reconOrder == SIFV_UPWIND1) ? 1
+            : (c->reconOrder == SIFV_WENO3 || c->reconOrder == SIFV_UPWIND3) ? 2 : 3;
+    if (c->nGhost < req) return bad("nGhost is too small for chosen reconOrder");
+    if (c->semiImplicit) {
+        if (c->siCfl <= 0) return bad("semiImplicitParams.cfl must be > 0");
+        if (c->siMinDt <= 0) return bad("semiImplicitParams.minDt must be > 0");
+        if (c->siMaxDt <= c->siMinDt) return bad("semiImplicitParams.maxDt must be > minDt");
+        if (c->pressureTol <= 0) return bad("semiImplicitParams.pressureTol must be > 0");
+        if (c->maxPressureIters <= 0) return bad("semiImplicitParams.maxPressureIters must be > 0");
+    } else {
+        if (c->cfl <= 0) return bad("explicitParams.cfl must be > 0");
+        if (c->minDt <= 0) return bad("explicitParams.minDt must be > 0");
+        if (c->maxDt <= c->minDt) return bad("explicitParams.maxDt must be > minDt");
+    }
+    if (c->useIGR) {
+        if (c->alphaCoeff <= 0) return bad("igrParams.alphaCoeff must be > 0");
+        if (c->IGRIters <= 0) return bad("igrParams.IGRIters must be > 0");
+        if (c->IGRWarmStartIters < 0) return bad("igrParams.IGRWarmStartIters must be >= 0");
+    }
+    if (c->nPhases < 0 || c->nPhases > SIFV_MAX_PHASES) return bad("nPhases must be in [0, 8]");
+    for (int p = 0; p < c->nPhases; ++p) {
+        if (c->phaseGamma[p] <= 1.0) return bad("multiPhaseParams.phases[].gamma must be > 1");
+        if (c->phasePInf[p] < 0.0) return bad("multiPhaseParams.phases[].pInf must be >= 0");
+    }
+    if (c->nPhases > 0 && c->alphaMin <= 0.0) return bad("multiPhaseParams.alphaMin must be > 0");
+    if (c->riemannSolver < SIFV_LF || c->riemannSolver > SIFV_HLLC) return bad("unknown riemannSolver");
+    if (c->precision != SIFV_PREC_FP64 && c->precision != SIFV_PREC_MIXED) return bad("unknown precision");
+    return SIFV_OK;
+}
+
+double* dalloc(sifv_ctx* c, size_t n, int& st) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(double));
+    if (e != cudaSuccess) {
+        st = fail(c, SIFV_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        return nullptr;
+    }
+    cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(double), c->stream);
+    c->allocs.push_back(p);
+    return static_cast<double*>(p);
+}
+
+double* field_ptr(sifv_ctx* c, int f) {
+    Fields& F = c->F;
+    switch (f) {
+        case SIFV_F_RHO: return F.rho;
+        case SIFV_F_RHOU: return F.rhoU;
+        case SIFV_F_RHOV: return F.rhoV;
+        case SIFV_F_RHOW: return F.rhoW;
+        case SIFV_F_RHOE: return F.rhoE;
+        case SIFV_F_VELU: return F.velU;
+        case SIFV_F_VELV: return F.velV;
+        case SIFV_F_VELW: return F.velW;
+        case SIFV_F_PRES: return F.pres;
+        case SIFV_F_SIGMA: return F.sigma;
+        default: break;
+    }
+    if (f >= 16 && f < 16 + c->cfg.nPhases) return F.alphaRho[f - 16];
+    if (f >= 32 && f < 32 + c->cfg.nPhases) return F.alpha[f - 32];
+    return nullptr;
+}
+
+int ensure_res(sifv_ctx* c, int n) {
+    if (n <= c->resCap) return SIFV_OK;
+    if (c->ctl) cudaFree(c->ctl);
+    if (c->ctlHost) cudaFreeHost(c->ctlHost);
+    c->ctl = nullptr;
+    c->ctlHost = nullptr;
+    size_t bytes = sizeof(Ctl) + sizeof(unsigned long long) * (size_t)(n + 1);
+    CUDA_TRY(c, cudaMalloc(&c->ctl, bytes));
+    CUDA_TRY(c, cudaMallocHost(&c->ctlHost, bytes));
+    CUDA_TRY(c, cudaMemsetAsync(c->ctl, 0, bytes, c->stream));
+    c->resCap = n;
+    return SIFV_OK;
+}
+
+// ---- launchers ------------------------------------------------------------
+
+template <int NPH>
+void launch_face_nph(sifv_ctx* c, int dir) {
+    const Params& P = c->P;
+    long long nf = (long long)(P.nx + (dir == 0)) * (P.ny + (dir == 1)) * (P.nz + (dir == 2));
+    unsigned g = blocks(nf, kFaceThreads);
+    cudaStream_t s = c->stream;
+#define FACE_CASE(D, Wd) k_face<D, Wd, NPH><<<g, kFaceThreads, 0, s>>>(c->P, c->F, c->ctl)
+    if (dir == 0) {
+        if (c->W == 1) FACE_CASE(0, 1); else if (c->W == 3) FACE_CASE(0, 3); else FACE_CASE(0, 5);
+    } else if (dir == 1) {
+        if (c->W == 1) FACE_CASE(1, 1); else if (c->W == 3) FACE_CASE(1, 3); else FACE_CASE(1, 5);
+    } else {
+        if (c->W == 1) FACE_CASE(2, 1); else if (c->W == 3) FACE_CASE(2, 3); else FACE_CASE(2, 5);
+    }
+#undef FACE_CASE
+    c->launches++;
+}
+
+void launch_face(sifv_ctx* c, int dir) {
+    if (c->nphT == 0) launch_face_nph<0>(c, dir);
+    else if (c->nphT == 2) launch_face_nph<2>(c, dir);
+    else launch_face_nph<8>(c, dir);
+}
+
+#define NPH_DISPATCH(c, KERNEL_CALL)                 \
+    do {                                             \
+        if ((c)->nphT == 0) { constexpr int NPHV = 0; KERNEL_CALL; } \
+        else if ((c)->nphT == 2) { constexpr int NPHV = 2; KERNEL_CALL; } \
+        else { constexpr int NPHV = 8; KERNEL_CALL; } \
+    } while (0)
+
+void launch_prim_bc(sifv_ctx* c, bool interiorOnly = false) {
+    long long n = (long long)c->ncells;
+    NPH_DISPATCH(c, (k_prim_bc<NPHV><<<blocks(n, kCellThreads), kCellThreads, 0, c->stream>>>(
+                         c->P, c->F, c->ctl, interiorOnly ? 1 : 0)));
+    c->launches++;
+}
+
+void launch_bc_prim(sifv_ctx* c) {
+    long long n = (long long)c->ncells;
+    NPH_DISPATCH(c, (k_bc_prim<NPHV><<<blocks(n, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, c->F)));
+    c->launches++;
+}
+
+void launch_scalar_ghosts(sifv_ctx* c, double* f) {
+    k_scalar_ghosts<<<blocks((long long)c->ncells, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, f);
+    c->launches++;
+}
+
+int igr_solve(sifv_ctx* c, int step) {
+    const Params& P = c->P;
+    k_igr_setup<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(P, c->F, c->alphaIGR);
+    c->launches++;
+    int iters = (step == 0) ? c->cfg.IGRWarmStartIters : c->cfg.IGRIters;
+    int nplanes = P.nx + P.ny + P.nz - 2;
+    long long lanes = (P.dim == 2) ? P.ny : (long long)P.ny * P.nz;
+    for (int it = 0; it < iters; ++it) {
+        if (P.dim == 1) {
+            k_igr_sweep_1d<<<1, 32, 0, c->stream>>>(P, c->F);
+            c->launches++;
+        } else {
+            for (int pl = 0; pl < nplanes; ++pl) {
+                k_igr_plane<<<blocks(lanes, kCellThreads), kCellThreads, 0, c->stream>>>(P, c->F, pl);
+            }
+            c->launches += nplanes;
+        }
+        launch_scalar_ghosts(c, c->F.sigma);
+    }
+    LAUNCH_CHECK(c);
+    return SIFV_OK;
+}
+
+// Jacobi iterations on (rho, rhoc2, rhs) with initial guess in F.pA;
+// returns the number of iterations as JacobiPressureSolver::solve does and
+// the buffer holding the result.
+int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rhs, double tol, int maxIter,
+               int& iters, const double*& result) {
+    int st = ensure_res(c, maxIter);
+    if (st != SIFV_OK) return st;
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->jacobiDone, 0, sizeof(int), c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->ctl->res, 0, sizeof(unsigned long long) * (size_t)maxIter, c->stream));
+    unsigned g = blocks((long long)c->nint, kCellThreads);
+    int it = 0, batch = 4;
+    int done = 0;
+    while (it < maxIter) {
+        int nb = std::min(batch, maxIter - it);
+        for (int q = 0; q < nb; ++q, ++it) {
+            const double* pin = (it & 1) ? c->F.pB : c->F.pA;
+            double* pout = (it & 1) ? c->F.pA : c->F.pB;
+            k_jacobi<<<g, kCellThreads, 0, c->stream>>>(c->P, rho, rhoc2, rhs, pin, pout, c->F, c->ctl, it, tol);
+        }
+        c->launches += nb;
+        LAUNCH_CHECK(c);
+        CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl) + sizeof(unsigned long long) * (size_t)it,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        if (c->ctlHost->jacobiDone) {
+            done = c->ctlHost->jacobiDone;
+            break;
+        }
+        double last;
+        unsigned long long b = c->ctlHost->res[it - 1];
+        std::memcpy(&last, &b, sizeof(double));
+        if (last < tol) {
+            done = it;
+            break;
+        }
+        batch = std::min(batch * 2, 32);
+    }
+    iters = done ? done : maxIter;
+    result = (iters & 1) ? c->F.pB : c->F.pA;
+    return SIFV_OK;
+}
+
+void rk_coef(int order, int s, StageCoef& K) {
+    // src/ExplicitSolver.cpp:92-103
+    static const double t1[1][4] = {{1.0, 0.0, 1.0, 1.0}};
+    static const double t2[2][4] = {{1.0, 0.0, 1.0, 1.0}, {1.0, 1.0, 1.0, 2.0}};
+    static const double t3[3][4] = {{1.0, 0.0, 1.0, 1.0}, {1.0, 3.0, 1.0, 4.0}, {2.0, 1.0, 2.0, 3.0}};
+    const double* r = (order == 1) ? t1[s] : (order == 2) ? t2[s] : t3[s];
+    K.c1 = r[0]; K.c2 = r[1]; K.c3 = r[2]; K.c4 = r[3];
+    K.s = s;
+}
+
+bool has_body_force(const sifv_config_t& c) {
+    for (int d = 0; d < 3; ++d)
+        if (c.bfA[d] != 0.0 || c.bfB[d] != 0.0) return true;
+    return false;
+}
+
+void body_force(const sifv_config_t& c, double time, StageCoef& K) {
+    K.hasBodyForce = has_body_force(c) ? 1 : 0;
+    for (int d = 0; d < 3; ++d) K.accel[d] = c.bfA[d] + c.bfB[d] * std::cos(c.bfC[d] * time + c.bfD[d]);
+}
+
+// dt reduction + finalisation on the device.
+void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
+    const sifv_config_t& cfg = c->cfg;
+    unsigned g = blocks((long long)c->nint, kCellThreads);
+    if (cfg.semiImplicit) {
+        k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, cfg.siMaxDt);
+        k_dt_advective<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.siCfl);
+        k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, -1.0, targetDt, 1, cfg.siMinDt, cfg.siMaxDt, useEnd ? 1 : 0);
+        c->launches += 3;
+    } else {
+        if (cfg.constDt <= 0) {
+            k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, cfg.maxDt);
+            NPH_DISPATCH(c, (k_dt_acoustic<NPHV><<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.cfl)));
+            c->launches += 2;
+        }
+        k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, cfg.constDt, targetDt, 0, 0.0, 0.0, useEnd ? 1 : 0);
+        c->launches += 1;
+    }
+}
+
+// One step, everything enqueued on the stream; semi-implicit steps
+// synchronise once per Jacobi batch.
+int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEnd, int& status) {
+    const sifv_config_t& cfg = c->cfg;
+    const Params& P = c->P;
+    status = SIFV_OK;
+    enqueue_dt(c, targetDt, useEnd);
+    unsigned gc = blocks((long long)c->nint, kCellThreads);
+    for (int s = 0; s < cfg.RKOrder; ++s) {
+        StageCoef K{};
+        rk_coef(cfg.RKOrder, s, K);
+        body_force(cfg, time, K);
+        launch_prim_bc(c);
+        if (cfg.useIGR) {
+            int st = igr_solve(c, step);
+            if (st != SIFV_OK) return st;
+        }
+        for (int d = 0; d < P.dim; ++d) launch_face(c, d);
+        if (!cfg.semiImplicit) {
+            NPH_DISPATCH(c, (k_assemble<NPHV, 0><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, K)));
+            c->launches++;
+            LAUNCH_CHECK(c);
+        } else {
+            NPH_DISPATCH(c, (k_assemble<NPHV, 1><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, K)));
+            c->launches++;
+            launch_bc_prim(c);
+            NPH_DISPATCH(c, (k_pressure_setup<NPHV><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl)));
+            c->launches++;
+            LAUNCH_CHECK(c);
+            int iters = 0;
+            const double* pres = nullptr;
+            int st = jacobi_run(c, c->F.rho, c->F.rhoc2, c->F.pRhs, cfg.pressureTol, cfg.maxPressureIters, iters,
+                                pres);
+            if (st != SIFV_OK) return st;
+            c->lastIters = iters;
+            if (iters >= cfg.maxPressureIters) {
+                double last;
+                unsigned long long b = c->ctlHost->res[iters - 1];
+                std::memcpy(&last, &b, sizeof(double));
+                if (!(last < cfg.pressureTol)) status = SIFV_NOT_CONVERGED;
+            }
+            NPH_DISPATCH(c, (k_correction<NPHV><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, pres, c->ctl)));
+            c->launches++;
+            launch_bc_prim(c);
+            LAUNCH_CHECK(c);
+        }
+    }
+    if (!cfg.semiImplicit) launch_prim_bc(c);   // finalize: src/ExplicitSolver.cpp:192-200
+    LAUNCH_CHECK(c);
+    return SIFV_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+void sifv_config_defaults(sifv_config_t* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->dim = 3; c->nGhost = 2; c->RKOrder = 1; c->useIGR = 0; c->semiImplicit = 0;
+    c->reconOrder = SIFV_WENO1; c->wenoEps = 1e-6;
+    c->riemannSolver = SIFV_HLLC; c->eosKind = SIFV_EOS_IDEAL; c->gamma = 1.4; c->pInf = 0.0;
+    c->cfl = 0.8; c->constDt = -1.0; c->maxDt = 1e-2; c->minDt = 1e-12;
+    c->siCfl = 0.8; c->siMaxDt = 1e-2; c->siMinDt = 1e-12; c->maxPressureIters = 100; c->pressureTol = 1e-8;
+    c->alphaCoeff = 1.0; c->IGRIters = 5; c->IGRWarmStartIters = 50;
+    c->nPhases = 0; c->alphaMin = 1e-8;
+    c->precision = SIFV_PREC_FP64;
+}
+
+int sifv_config_validate(const sifv_config_t* cfg) {
+    std::string m;
+    int st = validate(cfg, m);
+    if (st != SIFV_OK) g_err = m;
+    return st;
+}
+
+const char* sifv_last_error(const sifv_ctx_t* ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, sifv_ctx_t** out) {
+    if (!out || !cfg || !mesh) return fail(nullptr, SIFV_ERR_BAD_ARG, "null argument");
+    *out = nullptr;
+    std::string m;
+    int st = validate(cfg, m);
+    if (st != SIFV_OK) return fail(nullptr, st, m);
+    if (cfg->precision != SIFV_PREC_FP64)
+        return fail(nullptr, SIFV_ERR_UNSUPPORTED, "this build implements precision SIFV_PREC_FP64 only");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, SIFV_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(nullptr, SIFV_ERR_BAD_ARG, "device index out of range");
+
+    const int dim = cfg->dim;
+    int nx = mesh->nx, ny = (dim >= 2) ? mesh->ny : 1, nz = (dim >= 3) ? mesh->nz : 1;
+    int ng = cfg->nGhost;
+    if (nx < 1 || ny < 1 || nz < 1) return fail(nullptr, SIFV_ERR_BAD_ARG, "mesh must have at least one cell per axis");
+    if (nx < ng || (dim >= 2 && ny < ng) || (dim >= 3 && nz < ng))
+        return fail(nullptr, SIFV_ERR_UNSUPPORTED, "every active axis needs at least nGhost cells");
+    if (!mesh->xNodes || (dim >= 2 && !mesh->yNodes) || (dim >= 3 && !mesh->zNodes))
+        return fail(nullptr, SIFV_ERR_BAD_ARG, "node arrays of the active axes are required");
+    for (int f = 0; f < 6; ++f)
+        if (mesh->bc[f] < SIFV_BC_SYMMETRY || mesh->bc[f] > SIFV_BC_NOSLIPWALL)
+            return fail(nullptr, SIFV_ERR_BAD_ARG, "unknown boundary condition");
+
+    sifv_ctx* c = new sifv_ctx();
+    c->cfg = *cfg;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return fail(nullptr, SIFV_ERR_CUDA, "cudaSetDevice failed"); }
+    if (cudaStreamCreateWithFlags(&c->ownStream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return fail(nullptr, SIFV_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    c->stream = c->ownStream;
+    cudaEventCreate(&c->ev0);
+    cudaEventCreate(&c->ev1);
+
+    Params& P = c->P;
+    P.dim = dim;
+    P.nx = nx; P.ny = ny; P.nz = nz;
+    P.ngx = ng; P.ngy = (dim >= 2) ? ng : 0; P.ngz = (dim >= 3) ? ng : 0;
+    P.nxT = nx + 2 * P.ngx; P.nyT = ny + 2 * P.ngy; P.nzT = nz + 2 * P.ngz;
+    for (int f = 0; f < 6; ++f) P.bc[f] = mesh->bc[f];
+    P.nPh = cfg->nPhases;
+    P.reconOrder = cfg->reconOrder;
+    P.riemann = cfg->riemannSolver;
+    P.includePressure = cfg->semiImplicit ? 0 : 1;
+    P.useIGR = cfg->useIGR;
+    P.reconSigma = (cfg->useIGR && cfg->riemannSolver == SIFV_LF) ? 1 : 0;
+    P.eosStiffened = (cfg->eosKind == SIFV_EOS_STIFFENED) ? 1 : 0;
+    P.RKOrder = cfg->RKOrder;
+    P.wenoEps = cfg->wenoEps;
+    P.gamma = cfg->gamma;
+    P.pInf = (cfg->eosKind == SIFV_EOS_STIFFENED) ? cfg->pInf : 0.0;
+    for (int p = 0; p < SIFV_MAX_PHASES; ++p) {
+        P.phaseGamma[p] = cfg->phaseGamma[p];
+        P.phasePInf[p] = cfg->phasePInf[p];
+    }
+    P.alphaMin = cfg->alphaMin;
+    c->nphT = (cfg->nPhases == 0) ? 0 : (cfg->nPhases <= 2) ? 2 : 8;
+    c->W = (cfg->reconOrder == SIFV_WENO1 || cfg->reconOrder == SIFV_UPWIND1) ? 1
+         : (cfg->reconOrder == SIFV_WENO3 || cfg->reconOrder == SIFV_UPWIND3) ? 3 : 5;
+    c->ncells = (size_t)P.nxT * P.nyT * P.nzT;
+    c->nint = (size_t)nx * ny * nz;
+
+    st = SIFV_OK;
+    const size_t n = c->ncells;
+    Fields& F = c->F;
+    F.rho = dalloc(c, n, st); F.rhoU = dalloc(c, n, st); F.rhoE = dalloc(c, n, st);
+    F.velU = dalloc(c, n, st); F.pres = dalloc(c, n, st); F.sigma = dalloc(c, n, st);
+    if (dim >= 2) { F.rhoV = dalloc(c, n, st); F.velV = dalloc(c, n, st); }
+    if (dim >= 3) { F.rhoW = dalloc(c, n, st); F.velW = dalloc(c, n, st); }
+    for (int p = 0; p < cfg->nPhases; ++p) { F.alphaRho[p] = dalloc(c, n, st); F.alpha[p] = dalloc(c, n, st); }
+    if (cfg->RKOrder > 1) {
+        F.rho0 = dalloc(c, n, st); F.rhoU0 = dalloc(c, n, st); F.rhoE0 = dalloc(c, n, st); F.pres0 = dalloc(c, n, st);
+        if (dim >= 2) F.rhoV0 = dalloc(c, n, st);
+        if (dim >= 3) F.rhoW0 = dalloc(c, n, st);
+        for (int p = 0; p < cfg->nPhases; ++p) { F.alphaRho0[p] = dalloc(c, n, st); F.alpha0[p] = dalloc(c, n, st); }
+    }
+    if (cfg->semiImplicit) {
+        F.rhoUStar = dalloc(c, n, st); F.rhoEstar = dalloc(c, n, st); F.pAdvected = dalloc(c, n, st);
+        F.rhoc2 = dalloc(c, n, st);
+        if (dim >= 2) F.rhoVStar = dalloc(c, n, st);
+        if (dim >= 3) F.rhoWStar = dalloc(c, n, st);
+        F.pRhs = dalloc(c, n, st); F.divUstar = dalloc(c, n, st);
+    }
+    F.pA = dalloc(c, n, st); F.pB = dalloc(c, n, st);
+    if (cfg->useIGR) { F.igrRhs = dalloc(c, n, st); F.igrDiag = dalloc(c, n, st); }
+    for (int d = 0; d < dim; ++d) {
+        size_t nf = (size_t)(nx + (d == 0)) * (ny + (d == 1)) * (nz + (d == 2));
+        F.flux[d][FS_MASS] = dalloc(c, nf, st);
+        F.flux[d][FS_MOMX] = dalloc(c, nf, st);
+        if (dim >= 2) F.flux[d][FS_MOMY] = dalloc(c, nf, st);
+        if (dim >= 3) F.flux[d][FS_MOMZ] = dalloc(c, nf, st);
+        F.flux[d][FS_ENERGY] = dalloc(c, nf, st);
+        if (cfg->semiImplicit) F.flux[d][FS_PFLUX] = dalloc(c, nf, st);
+        if (cfg->semiImplicit || cfg->nPhases > 0) F.flux[d][FS_FVEL] = dalloc(c, nf, st);
+        for (int p = 0; p < cfg->nPhases; ++p) {
+            F.flux[d][FS_ALPHA + p] = dalloc(c, nf, st);
+            F.flux[d][FS_AR + p] = dalloc(c, nf, st);
+        }
+    }
+    // geometry: per-cell widths incl. ghosts, and IGR alpha/d^2
+    static const double unit[2] = {0.0, 1.0};
+    std::vector<double> xe = build_ext(mesh->xNodes, nx, P.ngx);
+    std::vector<double> ye = build_ext((dim >= 2) ? mesh->yNodes : unit, ny, P.ngy);
+    std::vector<double> ze = build_ext((dim >= 3) ? mesh->zNodes : unit, nz, P.ngz);
+    auto widths = [](const std::vector<double>& e) {
+        std::vector<double> w(e.size() - 1);
+        for (size_t i = 0; i + 1 < e.size(); ++i) w[i] = e[i + 1] - e[i];
+        return w;
+    };
+    std::vector<double> dxv = widths(xe), dyv = widths(ye), dzv = widths(ze);
+    double dx0 = dxv[P.ngx];
+    c->alphaIGR = cfg->alphaCoeff * dx0 * dx0;   // src/IGR.cpp:108
+    auto a2 = [&](const std::vector<double>& w) {
+        std::vector<double> r(w.size());
+        for (size_t i = 0; i < w.size(); ++i) r[i] = c->alphaIGR * (1.0 / (w[i] * w[i]));
+        return r;
+    };
+    std::vector<double> adx = a2(dxv), ady = a2(dyv), adz = a2(dzv);
+    double* g[6];
+    const std::vector<double>* src[6] = {&dxv, &dyv, &dzv, &adx, &ady, &adz};
+    for (int q = 0; q < 6; ++q) {
+        g[q] = dalloc(c, src[q]->size(), st);
+        if (st == SIFV_OK)
+            cudaMemcpyAsync(g[q], src[q]->data(), src[q]->size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    }
+    F.dx = g[0]; F.dy = g[1]; F.dz = g[2]; F.adx2 = g[3]; F.ady2 = g[4]; F.adz2 = g[5];
+    if (st == SIFV_OK) st = ensure_res(c, std::max(cfg->maxPressureIters, 1));
+    if (st == SIFV_OK) {
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) st = fail(c, SIFV_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (st != SIFV_OK) {
+        g_err = c->err;
+        sifv_destroy(c);
+        return st;
+    }
+    *out = c;
+    return SIFV_OK;
+}
+
+int sifv_destroy(sifv_ctx_t* c) {
+    if (!c) return SIFV_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void* p : c->allocs) cudaFree(p);
+    if (c->ctl) cudaFree(c->ctl);
+    if (c->ctlHost) cudaFreeHost(c->ctlHost);
+    if (c->sRho) { cudaFree(c->sRho); cudaFree(c->sRhoc2); cudaFree(c->sRhs); cudaFree(c->sP); }
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->ownStream) cudaStreamDestroy(c->ownStream);
+    delete c;
+    return SIFV_OK;
+}
+
+int sifv_extents(const sifv_ctx_t* c, int* nx, int* ny, int* nz) {
+    if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
+    *nx = c->P.nxT; *ny = c->P.nyT; *nz = c->P.nzT;
+    return SIFV_OK;
+}
+
+size_t sifv_total_cells(const sifv_ctx_t* c) { return c ? c->ncells : 0; }
+
+int sifv_set_stream(sifv_ctx_t* c, void* stream) {
+    c->stream = stream ? static_cast<cudaStream_t>(stream) : c->ownStream;
+    return SIFV_OK;
+}
+
+int sifv_synchronize(sifv_ctx_t* c) {
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SIFV_OK;
+}
+
+int sifv_field_device_ptr(sifv_ctx_t* c, int field, double** dptr) {
+    double* p = field_ptr(c, field);
+    if (!p) return fail(c, SIFV_ERR_BAD_ARG, "field not allocated for this configuration");
+    *dptr = p;
+    return SIFV_OK;
+}
+
+int sifv_set_field(sifv_ctx_t* c, int field, const double* src, int onDevice) {
+    double* p = field_ptr(c, field);
+    if (!p) return fail(c, SIFV_ERR_BAD_ARG, "field not allocated for this configuration");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaMemcpyAsync(p, src, c->ncells * sizeof(double),
+                                onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SIFV_OK;
+}
+
+int sifv_get_field(sifv_ctx_t* c, int field, double* dst, int onDevice) {
+    double* p = field_ptr(c, field);
+    if (!p) return fail(c, SIFV_ERR_BAD_ARG, "field not allocated for this configuration");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaMemcpyAsync(dst, p, c->ncells * sizeof(double),
+                                onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SIFV_OK;
+}
+
+int sifv_step(sifv_ctx_t* c, int step, double time, double targetDt, double* dtOut) {
+    if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
+    cudaSetDevice(c->device);
+    c->launches = 0;
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+    int status = SIFV_OK;
+    int st = enqueue_step(c, step, time, targetDt, false, status);
+    if (st != SIFV_OK) return st;
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    cudaEventElapsedTime(&c->lastMs, c->ev0, c->ev1);
+    c->lastLaunches = c->launches;
+    if (dtOut) *dtOut = c->ctlHost->dt;
+    return status;
+}
+
+int sifv_advance(sifv_ctx_t* c, int step0, double time0, double tEnd, int nSteps, double* timeOut, int* stepsTaken) {
+    if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
+    if (c->cfg.semiImplicit) return fail(c, SIFV_ERR_UNSUPPORTED, "sifv_advance runs the explicit step only");
+    if (c->cfg.useIGR) return fail(c, SIFV_ERR_UNSUPPORTED, "sifv_advance does not run IGR; use sifv_step");
+    if (has_body_force(c->cfg)) return fail(c, SIFV_ERR_UNSUPPORTED, "sifv_advance does not run body forces");
+    cudaSetDevice(c->device);
+    c->launches = 0;
+    Ctl h{};
+    h.time = time0;
+    h.tEnd = (tEnd > 0) ? tEnd : INFINITY;
+    CUDA_TRY(c, cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+    int status = SIFV_OK;
+    for (int q = 0; q < nSteps; ++q) {
+        int st = enqueue_step(c, step0 + q, time0, -1.0, true, status);
+        if (st != SIFV_OK) return st;
+        k_time_advance<<<1, 1, 0, c->stream>>>(c->ctl);
+        c->launches++;
+    }
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    cudaEventElapsedTime(&c->lastMs, c->ev0, c->ev1);
+    c->lastLaunches = c->launches;
+    if (timeOut) *timeOut = c->ctlHost->time;
+    if (stepsTaken) *stepsTaken = c->ctlHost->stepsTaken;
+    return SIFV_OK;
+}
+
+int sifv_last_pressure_iterations(const sifv_ctx_t* c, int* iters) {
+    *iters = c->lastIters;
+    return SIFV_OK;
+}
+
+int sifv_last_step_stats(const sifv_ctx_t* c, double* ms, int* launches) {
+    *ms = c->lastMs;
+    *launches = c->lastLaunches;
+    return SIFV_OK;
+}
+
+int sifv_pressure_solve(sifv_ctx_t* c, const double* rho, const double* rhoc2, const double* rhs, double* pressure,
+                        double dt, double tol, int maxIter, int onDevice, int* iters) {
+    if (!c || !rho || !rhoc2 || !rhs || !pressure || !iters) return fail(c, SIFV_ERR_BAD_ARG, "null argument");
+    if (maxIter <= 0) return fail(c, SIFV_ERR_BAD_ARG, "maxIter must be > 0");
+    cudaSetDevice(c->device);
+    const size_t bytes = c->ncells * sizeof(double);
+    const double *dRho = rho, *dRhoc2 = rhoc2, *dRhs = rhs;
+    double* dP = pressure;
+    if (!onDevice) {
+        if (!c->sRho) {
+            CUDA_TRY(c, cudaMalloc(&c->sRho, bytes));
+            CUDA_TRY(c, cudaMalloc(&c->sRhoc2, bytes));
+            CUDA_TRY(c, cudaMalloc(&c->sRhs, bytes));
+            CUDA_TRY(c, cudaMalloc(&c->sP, bytes));
+        }
+        CUDA_TRY(c, cudaMemcpyAsync(c->sRho, rho, bytes, cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->sRhoc2, rhoc2, bytes, cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->sRhs, rhs, bytes, cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(c->sP, pressure, bytes, cudaMemcpyHostToDevice, c->stream));
+        dRho = c->sRho; dRhoc2 = c->sRhoc2; dRhs = c->sRhs; dP = c->sP;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->F.pA, dP, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(&c->ctl->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    int n = 0;
+    const double* res = nullptr;
+    int st = jacobi_run(c, dRho, dRhoc2, dRhs, tol, maxIter, n, res);
+    if (st != SIFV_OK) return st;
+    k_jacobi_finish<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, c->F.pA, c->F.pB,
+                                                                                             dP, c->ctl, maxIter);
+    LAUNCH_CHECK(c);
+    if (!onDevice) CUDA_TRY(c, cudaMemcpyAsync(pressure, dP, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    *iters = n;
+    if (n >= maxIter) {
+        double last;
+        unsigned long long b = c->ctlHost->res[n - 1];
+        std::memcpy(&last, &b, sizeof(double));
+        if (!(last < tol)) return SIFV_NOT_CONVERGED;
+    }
+    return SIFV_OK;
+}
+
+int sifv_igr_solve(sifv_ctx_t* c, int step) {
+    if (!c->cfg.useIGR) return fail(c, SIFV_ERR_BAD_ARG, "useIGR is off in this configuration");
+    cudaSetDevice(c->device);
+    int st = igr_solve(c, step);
+    if (st != SIFV_OK) return st;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SIFV_OK;
+}
+
+int sifv_acoustic_dt(sifv_ctx_t* c, double cfl, double maxDt, double* dt) {
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
+    k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, maxDt);
+    NPH_DISPATCH(c, (k_dt_acoustic<NPHV><<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(
+                         c->P, c->F, c->ctl, cfl)));
+    LAUNCH_CHECK(c);
+    CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    unsigned long long b = c->ctlHost->dtBits;
+    std::memcpy(dt, &b, sizeof(double));
+    return SIFV_OK;
+}
+
+int sifv_advective_dt(sifv_ctx_t* c, double cfl, double maxDt, double* dt) {
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
+    k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, maxDt);
+    k_dt_advective<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfl);
+    LAUNCH_CHECK(c);
+    CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    unsigned long long b = c->ctlHost->dtBits;
+    std::memcpy(dt, &b, sizeof(double));
+    return SIFV_OK;
+}
+
+int sifv_convert_cons_to_prim(sifv_ctx_t* c) {
+    // interior cells only, ghosts untouched (as the reference)
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
+    launch_prim_bc(c, true);
+    LAUNCH_CHECK(c);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SIFV_OK;
+}
+
+int sifv_apply_bc(sifv_ctx_t* c) {
+    cudaSetDevice(c->device);
+    launch_bc_prim(c);
+    LAUNCH_CHECK(c);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SIFV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,563 @@
+// sifv_device.cuh -- device-side data layout and the per-cell / per-face
+// physics of the SemiImplicitFV finite-volume step, for sm_100a.
+//
+// Layout in HBM: structure of arrays, one FP64 array of totalCells per
+// field, x fastest, ghosts included (the reference's SolutionState layout,
+// include/SolutionState.hpp:73-113, indexed as RectilinearMesh::index,
+// include/RectilinearMesh.hpp:70-73).  Face fluxes are SoA per direction
+// with the reference's face indexing (src/Reconstruction.cpp:71-81).
+//
+// Arithmetic: every expression is evaluated in the order the reference
+// writes it.  The parity build compiles this header with --fmad=false so a
+// kernel's output is bit-identical to the reference compiled without FMA
+// contraction.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "sifv.h"
+
+// Loop over the active axes 0..dim-1, unrolled to 3 with a uniform guard so
+// per-axis arrays stay in registers.
+#define DIMLOOP(v) _Pragma("unroll") for (int v = 0; v < 3; ++v) if (v < dim)
+
+namespace sifv {
+
+constexpr int MAXPH = SIFV_MAX_PHASES;
+
+// Flux component slots of one face (per direction).
+enum FluxSlot : int {
+    FS_MASS = 0,
+    FS_MOMX = 1,
+    FS_MOMY = 2,
+    FS_MOMZ = 3,
+    FS_ENERGY = 4,
+    FS_PFLUX = 5,   // pressureFlux (semi-implicit)
+    FS_FVEL = 6,    // faceVelocity (semi-implicit, multi-phase)
+    FS_ALPHA = 7,   // alphaFlux[ph]         7 .. 7+MAXPH-1
+    FS_AR = 7 + MAXPH,  // upwinded alphaRho flux[ph]
+    FS_COUNT = 7 + 2 * MAXPH
+};
+
+struct Params {
+    int dim;
+    int nx, ny, nz;          // physical cells
+    int ngx, ngy, ngz;       // ghosts per axis (0 on inactive axes)
+    int nxT, nyT, nzT;       // extents incl. ghosts
+    int bc[6];
+    int nPh;
+    int reconOrder;          // SIFV_WENO* / SIFV_UPWIND*
+    int riemann;             // SIFV_LF / SIFV_RUSANOV / SIFV_HLLC
+    int includePressure;     // !semiImplicit
+    int useIGR;
+    int reconSigma;          // sigma affects the flux (LF with IGR)
+    int eosStiffened;
+    int RKOrder;
+    double wenoEps;
+    double gamma, pInf;
+    double phaseGamma[MAXPH], phasePInf[MAXPH];
+    double alphaMin;
+};
+
+struct Fields {
+    double *rho, *rhoU, *rhoV, *rhoW, *rhoE;
+    double *velU, *velV, *velW, *pres, *sigma;
+    double* alphaRho[MAXPH];
+    double* alpha[MAXPH];
+    double *rho0, *rhoU0, *rhoV0, *rhoW0, *rhoE0, *pres0;
+    double* alphaRho0[MAXPH];
+    double* alpha0[MAXPH];
+    double *rhoUStar, *rhoVStar, *rhoWStar, *rhoEstar, *pAdvected, *rhoc2;
+    double* flux[3][FS_COUNT];   // per direction, per slot (nullptr when unused)
+    double *pA, *pB, *pRhs, *divUstar;
+    double *igrRhs, *igrDiag;
+    const double *dx, *dy, *dz;     // per cell incl. ghosts (dx(i) at [i + ngx])
+    const double *adx2, *ady2, *adz2;  // alpha / (d*d) per cell (IGR)
+};
+
+// Step control block in device memory.
+struct Ctl {
+    unsigned long long dtBits;   // reduction accumulator (non-negative doubles order as integers)
+    double dt;                   // dt of the current step
+    double time;                 // physical time (device-resident loops)
+    double tEnd;
+    int skip;                    // nonzero: remaining work of this step is a no-op
+    int jacobiDone;              // iterations taken when converged, else 0
+    int stepsTaken;
+    int errFlag;
+    unsigned long long res[1];   // per-iteration max residual bits (sized at allocation)
+};
+
+// std::max / std::min / std::clamp semantics.
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+
+__device__ __forceinline__ size_t cidx(const Params& P, int i, int j, int k) {
+    return (size_t)(i + P.ngx) + (size_t)P.nxT * ((size_t)(j + P.ngy) + (size_t)P.nyT * (size_t)(k + P.ngz));
+}
+
+// Ghost source along one axis for the PRIM fill (the BoundaryCondition
+// switch of fillGhostX/Y/Z, src/RectilinearMesh.cpp:147-166, 188-207).
+// Returns the interior index; sn multiplies the normal velocity, sa all
+// velocity components.  Requires n >= nGhost.
+__device__ __forceinline__ int prim_src(int i, int n, int bcLo, int bcHi, double& sn, double& sa) {
+    sn = 1.0;
+    sa = 1.0;
+    if (i < 0) {
+        int g = -i;
+        switch (bcLo) {
+            case SIFV_BC_SYMMETRY: return g - 1;
+            case SIFV_BC_PERIODIC: return n - g;
+            case SIFV_BC_SLIPWALL: sn = -1.0; return g - 1;
+            case SIFV_BC_NOSLIPWALL: sa = -1.0; return g - 1;
+            default: return 0;
+        }
+    }
+    if (i >= n) {
+        int g = i - n + 1;
+        switch (bcHi) {
+            case SIFV_BC_SYMMETRY: return n - g;
+            case SIFV_BC_PERIODIC: return g - 1;
+            case SIFV_BC_SLIPWALL: sn = -1.0; return n - g;
+            case SIFV_BC_NOSLIPWALL: sa = -1.0; return n - g;
+            default: return n - 1;
+        }
+    }
+    return i;
+}
+
+// Ghost source along one axis for the scalar fill
+// (RectilinearMesh::fillScalarGhosts, src/RectilinearMesh.cpp:424-492):
+// periodic wrap, otherwise zero gradient.
+__device__ __forceinline__ int scalar_src(int i, int n, int bcLo, int bcHi) {
+    if (i < 0) return (bcLo == SIFV_BC_PERIODIC) ? n + i : 0;
+    if (i >= n) return (bcHi == SIFV_BC_PERIODIC) ? i - n : n - 1;
+    return i;
+}
+
+__device__ __forceinline__ size_t scalar_idx(const Params& P, int i, int j, int k) {
+    return cidx(P, scalar_src(i, P.nx, P.bc[0], P.bc[1]), (P.dim >= 2) ? scalar_src(j, P.ny, P.bc[2], P.bc[3]) : j,
+                (P.dim >= 3) ? scalar_src(k, P.nz, P.bc[4], P.bc[5]) : k);
+}
+
+// ---------------------------------------------------------------------------
+// EOS
+// ---------------------------------------------------------------------------
+
+// MixtureEOS::effectiveGammaAndPiInf, src/MixtureEOS.cpp:18-31
+template <int NPH>
+__device__ __forceinline__ void eff_gamma_piinf(const Params& P, const double* a, double& gEff, double& piEff) {
+    double sumInvGm1 = 0.0, sumPi = 0.0;
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            double gk = P.phaseGamma[ph];
+            double gm1 = gk - 1.0;
+            sumInvGm1 += a[ph] / gm1;
+            sumPi += a[ph] * gk * P.phasePInf[ph] / gm1;
+        }
+    }
+    gEff = 1.0 + 1.0 / sumInvGm1;
+    piEff = (gEff - 1.0) / gEff * sumPi;
+}
+
+// MixtureEOS::mixtureSoundSpeed (Wood), src/MixtureEOS.cpp:48-63
+template <int NPH>
+__device__ __forceinline__ double mixture_sound_speed(const Params& P, double rho, double p, const double* a,
+                                                      const double* ar) {
+    double sumInv = 0.0;
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            double rho_k = smax(ar[ph], 1e-14) / smax(a[ph], 1e-14);
+            double ck2 = P.phaseGamma[ph] * (p + P.phasePInf[ph]) / rho_k;
+            sumInv += a[ph] / (rho_k * smax(ck2, 1e-14));
+        }
+    }
+    double c2 = 1.0 / (rho * smax(sumInv, 1e-30));
+    return sqrt(smax(c2, 0.0));
+}
+
+// MixtureEOS::mixturePressure, src/MixtureEOS.cpp:35-46
+template <int NPH>
+__device__ __forceinline__ double mixture_pressure(const Params& P, double rhoEint, const double* a) {
+    double sumInvGm1 = 0.0, sumPi = 0.0;
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            double gm1 = P.phaseGamma[ph] - 1.0;
+            sumInvGm1 += a[ph] / gm1;
+            sumPi += a[ph] * P.phaseGamma[ph] * P.phasePInf[ph] / gm1;
+        }
+    }
+    return (rhoEint - sumPi) / sumInvGm1;
+}
+
+// MixtureEOS::mixtureTotalEnergy, src/MixtureEOS.cpp:65-76
+template <int NPH>
+__device__ __forceinline__ double mixture_total_energy(const Params& P, double p, const double* a, double ke) {
+    double r = ke;
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            double gm1 = P.phaseGamma[ph] - 1.0;
+            r += a[ph] * (p + P.phaseGamma[ph] * P.phasePInf[ph]) / gm1;
+        }
+    }
+    return r;
+}
+
+// Single-phase sound speed used by computeAcousticTimeStep
+// (src/RKTimeStepping.cpp:61-62) and solvePressure (src/SemiImplicitSolver.cpp:553-554).
+__device__ __forceinline__ double single_sound_speed(const Params& P, double rho, double p) {
+    return sqrt(P.gamma * smax(p + P.pInf, 1e-14) / smax(rho, 1e-14));
+}
+
+// ---------------------------------------------------------------------------
+// Reconstruction kernels, src/Reconstruction.cpp:83-200
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double weno5L(double v0, double v1, double v2, double v3, double v4, double eps) {
+    double p0 = (1.0 / 3.0) * v0 - (7.0 / 6.0) * v1 + (11.0 / 6.0) * v2;
+    double p1 = -(1.0 / 6.0) * v1 + (5.0 / 6.0) * v2 + (1.0 / 3.0) * v3;
+    double p2 = (1.0 / 3.0) * v2 + (5.0 / 6.0) * v3 - (1.0 / 6.0) * v4;
+    double t0 = v0 - 2.0 * v1 + v2, s0 = v0 - 4.0 * v1 + 3.0 * v2;
+    double t1 = v1 - 2.0 * v2 + v3, s1 = v1 - v3;
+    double t2 = v2 - 2.0 * v3 + v4, s2 = 3.0 * v2 - 4.0 * v3 + v4;
+    double b0 = (13.0 / 12.0) * t0 * t0 + (1.0 / 4.0) * s0 * s0;
+    double b1 = (13.0 / 12.0) * t1 * t1 + (1.0 / 4.0) * s1 * s1;
+    double b2 = (13.0 / 12.0) * t2 * t2 + (1.0 / 4.0) * s2 * s2;
+    double e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+    double a0 = (1.0 / 10.0) / (e0 * e0);
+    double a1 = (6.0 / 10.0) / (e1 * e1);
+    double a2 = (3.0 / 10.0) / (e2 * e2);
+    double aSum = a0 + a1 + a2;
+    return (a0 * p0 + a1 * p1 + a2 * p2) / aSum;
+}
+
+__device__ __forceinline__ double weno5R(double v0, double v1, double v2, double v3, double v4, double eps) {
+    double p0 = (1.0 / 3.0) * v4 - (7.0 / 6.0) * v3 + (11.0 / 6.0) * v2;
+    double p1 = -(1.0 / 6.0) * v3 + (5.0 / 6.0) * v2 + (1.0 / 3.0) * v1;
+    double p2 = (1.0 / 3.0) * v2 + (5.0 / 6.0) * v1 - (1.0 / 6.0) * v0;
+    double t0 = v4 - 2.0 * v3 + v2, s0 = v4 - 4.0 * v3 + 3.0 * v2;
+    double t1 = v3 - 2.0 * v2 + v1, s1 = v3 - v1;
+    double t2 = v2 - 2.0 * v1 + v0, s2 = 3.0 * v2 - 4.0 * v1 + v0;
+    double b0 = (13.0 / 12.0) * t0 * t0 + (1.0 / 4.0) * s0 * s0;
+    double b1 = (13.0 / 12.0) * t1 * t1 + (1.0 / 4.0) * s1 * s1;
+    double b2 = (13.0 / 12.0) * t2 * t2 + (1.0 / 4.0) * s2 * s2;
+    double e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+    double a0 = (1.0 / 10.0) / (e0 * e0);
+    double a1 = (6.0 / 10.0) / (e1 * e1);
+    double a2 = (3.0 / 10.0) / (e2 * e2);
+    double aSum = a0 + a1 + a2;
+    return (a0 * p0 + a1 * p1 + a2 * p2) / aSum;
+}
+
+__device__ __forceinline__ double upwind5L(double v0, double v1, double v2, double v3, double v4) {
+    double p0 = (1.0 / 3.0) * v0 - (7.0 / 6.0) * v1 + (11.0 / 6.0) * v2;
+    double p1 = -(1.0 / 6.0) * v1 + (5.0 / 6.0) * v2 + (1.0 / 3.0) * v3;
+    double p2 = (1.0 / 3.0) * v2 + (5.0 / 6.0) * v3 - (1.0 / 6.0) * v4;
+    return (1.0 / 10.0) * p0 + (6.0 / 10.0) * p1 + (3.0 / 10.0) * p2;
+}
+
+__device__ __forceinline__ double upwind5R(double v0, double v1, double v2, double v3, double v4) {
+    double p0 = (1.0 / 3.0) * v4 - (7.0 / 6.0) * v3 + (11.0 / 6.0) * v2;
+    double p1 = -(1.0 / 6.0) * v3 + (5.0 / 6.0) * v2 + (1.0 / 3.0) * v1;
+    double p2 = (1.0 / 3.0) * v2 + (5.0 / 6.0) * v1 - (1.0 / 6.0) * v0;
+    return (1.0 / 10.0) * p0 + (6.0 / 10.0) * p1 + (3.0 / 10.0) * p2;
+}
+
+__device__ __forceinline__ double weno3L(double v0, double v1, double v2, double eps) {
+    double p0 = -0.5 * v0 + 1.5 * v1;
+    double p1 = 0.5 * v1 + 0.5 * v2;
+    double b0 = (v1 - v0) * (v1 - v0);
+    double b1 = (v2 - v1) * (v2 - v1);
+    double e0 = eps + b0, e1 = eps + b1;
+    double a0 = (1.0 / 3.0) / (e0 * e0);
+    double a1 = (2.0 / 3.0) / (e1 * e1);
+    double aSum = a0 + a1;
+    return (a0 * p0 + a1 * p1) / aSum;
+}
+
+__device__ __forceinline__ double weno3R(double v0, double v1, double v2, double eps) {
+    double p0 = 0.5 * v0 + 0.5 * v1;
+    double p1 = 1.5 * v1 - 0.5 * v2;
+    double b0 = (v1 - v0) * (v1 - v0);
+    double b1 = (v2 - v1) * (v2 - v1);
+    double e0 = eps + b0, e1 = eps + b1;
+    double a0 = (2.0 / 3.0) / (e0 * e0);
+    double a1 = (1.0 / 3.0) / (e1 * e1);
+    double aSum = a0 + a1;
+    return (a0 * p0 + a1 * p1) / aSum;
+}
+
+__device__ __forceinline__ double upwind3L(double v0, double v1, double v2) {
+    double p0 = -0.5 * v0 + 1.5 * v1;
+    double p1 = 0.5 * v1 + 0.5 * v2;
+    return (1.0 / 3.0) * p0 + (2.0 / 3.0) * p1;
+}
+
+__device__ __forceinline__ double upwind3R(double v0, double v1, double v2) {
+    double p0 = 0.5 * v0 + 0.5 * v1;
+    double p1 = 1.5 * v1 - 0.5 * v2;
+    return (2.0 / 3.0) * p0 + (1.0 / 3.0) * p1;
+}
+
+// Left and right face values of one field at the face whose right cell is
+// `base`, cells strided by `st` along the sweep direction
+// (reconstructScalar, src/Reconstruction.cpp:11-28: the left state uses
+// cells -3..+1, the right state -2..+2 for WENO5).
+template <int W>
+__device__ __forceinline__ void recon_pair(const double* __restrict__ f, size_t base, long st, bool weno, double eps,
+                                           double& L, double& R) {
+    if (W == 1) {
+        L = f[base - st];
+        R = f[base];
+    } else if (W == 3) {
+        double v0 = f[base - 2 * st], v1 = f[base - st], v2 = f[base], v3 = f[base + st];
+        if (weno) {
+            L = weno3L(v0, v1, v2, eps);
+            R = weno3R(v1, v2, v3, eps);
+        } else {
+            L = upwind3L(v0, v1, v2);
+            R = upwind3R(v1, v2, v3);
+        }
+    } else {
+        double v0 = f[base - 3 * st], v1 = f[base - 2 * st], v2 = f[base - st], v3 = f[base], v4 = f[base + st],
+               v5 = f[base + 2 * st];
+        if (weno) {
+            L = weno5L(v0, v1, v2, v3, v4, eps);
+            R = weno5R(v1, v2, v3, v4, v5, eps);
+        } else {
+            L = upwind5L(v0, v1, v2, v3, v4);
+            R = upwind5R(v1, v2, v3, v4, v5);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Riemann solvers
+// ---------------------------------------------------------------------------
+template <int NPH>
+struct FaceState {
+    double rho, u[3], p, sigma, gEff, piEff;
+    double alpha[NPH > 0 ? NPH : 1];
+};
+
+template <int NPH>
+struct FaceFlux {
+    double mass, mom[3], energy, pflux, fvel;
+    double alpha[NPH > 0 ? NPH : 1];
+};
+
+// soundSpeedDirect / rhoEFromState, include/RiemannSolver.hpp:70-78
+template <int NPH>
+__device__ __forceinline__ double sound_speed_direct(const FaceState<NPH>& W) {
+    return sqrt(W.gEff * smax(W.p + W.piEff, 1e-14) / smax(W.rho, 1e-14));
+}
+template <int NPH>
+__device__ __forceinline__ double rhoE_from_state(const FaceState<NPH>& W) {
+    double ke = 0.5 * W.rho * (W.u[0] * W.u[0] + W.u[1] * W.u[1] + W.u[2] * W.u[2]);
+    return (W.p + W.gEff * W.piEff) / (W.gEff - 1.0) + ke;
+}
+
+// normalVelocity (include/RiemannSolver.hpp:59-64) for the unit normal of
+// axis D: 0 + u_D*1 + sum of u_d*0 over the other active axes.
+template <int D, int NPH>
+__device__ __forceinline__ double normal_velocity(const FaceState<NPH>& W, int dim) {
+    double vn = 0.0;
+    DIMLOOP(d) vn += W.u[d] * ((d == D) ? 1.0 : 0.0);
+    return vn;
+}
+
+// computeHLLCFlux, src/HLLCSolver.cpp:7-161
+template <int D, int NPH>
+__device__ __forceinline__ void hllc_flux(const Params& P, const FaceState<NPH>& L, const FaceState<NPH>& R,
+                                          FaceFlux<NPH>& F) {
+    const int dim = P.dim;
+    const bool incP = P.includePressure;
+    const double n[3] = {D == 0 ? 1.0 : 0.0, D == 1 ? 1.0 : 0.0, D == 2 ? 1.0 : 0.0};
+    F.mass = 0.0; F.mom[0] = F.mom[1] = F.mom[2] = 0.0; F.energy = 0.0; F.pflux = 0.0; F.fvel = 0.0;
+    double uL = normal_velocity<D>(L, dim), uR = normal_velocity<D>(R, dim);
+    double rhoEL = rhoE_from_state(L), rhoER = rhoE_from_state(R);
+    double sL, sR, sStar;
+    if (incP) {
+        double cL = sound_speed_direct(L), cR = sound_speed_direct(R);
+        sL = smin(uL - cL, uR - cR);
+        sR = smax(uL + cL, uR + cR);
+        sStar = (R.p - L.p + L.rho * uL * (sL - uL) - R.rho * uR * (sR - uR)) /
+                (L.rho * (sL - uL) - R.rho * (sR - uR));
+    } else {
+        sL = smin(uL, uR);
+        sR = smax(uL, uR);
+        sStar = 0.5 * (uL + uR);
+    }
+    if (sL >= 0) {
+        F.mass = L.rho * uL;
+        DIMLOOP(i) F.mom[i] = L.rho * L.u[i] * uL;
+        F.energy = rhoEL * uL;
+        if (incP) {
+            DIMLOOP(i) F.mom[i] += L.p * n[i];
+            F.energy += L.p * uL;
+        }
+    } else if (sR <= 0) {
+        F.mass = R.rho * uR;
+        DIMLOOP(i) F.mom[i] = R.rho * R.u[i] * uR;
+        F.energy = rhoER * uR;
+        if (incP) {
+            DIMLOOP(i) F.mom[i] += R.p * n[i];
+            F.energy += R.p * uR;
+        }
+    } else if (sStar >= 0) {
+        double rhoStarL = L.rho * (sL - uL) / (sL - sStar);
+        F.mass = L.rho * uL + sL * (rhoStarL - L.rho);
+        if (incP) {
+            DIMLOOP(i) {
+                double rhoUStarL = rhoStarL * (L.u[i] + (sStar - uL) * n[i]);
+                F.mom[i] = L.rho * L.u[i] * uL + L.p * n[i] + sL * (rhoUStarL - L.rho * L.u[i]);
+            }
+            double eL = rhoEL / L.rho;
+            double EStarL = rhoStarL * (eL + (sStar - uL) * (sStar + L.p / (L.rho * (sL - uL))));
+            F.energy = (rhoEL + L.p) * uL + sL * (EStarL - rhoEL);
+        } else {
+            DIMLOOP(i) {
+                double rhoUStarL = rhoStarL * (L.u[i] + (sStar - uL) * n[i]);
+                F.mom[i] = L.rho * L.u[i] * uL + sL * (rhoUStarL - L.rho * L.u[i]);
+            }
+            double eL = rhoEL / L.rho;
+            double EStarL = rhoStarL * (eL + (sStar - uL) * sStar);
+            F.energy = rhoEL * uL + sL * (EStarL - rhoEL);
+        }
+    } else {
+        double rhoStarR = R.rho * (sR - uR) / (sR - sStar);
+        F.mass = R.rho * uR + sR * (rhoStarR - R.rho);
+        if (incP) {
+            DIMLOOP(i) {
+                double rhoUStarR = rhoStarR * (R.u[i] + (sStar - uR) * n[i]);
+                F.mom[i] = R.rho * R.u[i] * uR + R.p * n[i] + sR * (rhoUStarR - R.rho * R.u[i]);
+            }
+            double eR = rhoER / R.rho;
+            double EStarR = rhoStarR * (eR + (sStar - uR) * (sStar + R.p / (R.rho * (sR - uR))));
+            F.energy = (rhoER + R.p) * uR + sR * (EStarR - rhoER);
+        } else {
+            DIMLOOP(i) {
+                double rhoUStarR = rhoStarR * (R.u[i] + (sStar - uR) * n[i]);
+                F.mom[i] = R.rho * R.u[i] * uR + sR * (rhoUStarR - R.rho * R.u[i]);
+            }
+            double eR = rhoER / R.rho;
+            double EStarR = rhoStarR * (eR + (sStar - uR) * sStar);
+            F.energy = rhoER * uR + sR * (EStarR - rhoER);
+        }
+    }
+    if (sL >= 0) {
+        F.fvel = uL;
+        F.pflux = L.p * uL;
+#pragma unroll
+        for (int ph = 0; ph < NPH; ++ph) F.alpha[ph] = L.alpha[ph] * uL;
+    } else if (sR <= 0) {
+        F.fvel = uR;
+        F.pflux = R.p * uR;
+#pragma unroll
+        for (int ph = 0; ph < NPH; ++ph) F.alpha[ph] = R.alpha[ph] * uR;
+    } else {
+        F.fvel = sStar;
+        if (sStar >= 0) {
+            F.pflux = L.p * sStar;
+#pragma unroll
+            for (int ph = 0; ph < NPH; ++ph) F.alpha[ph] = L.alpha[ph] * sStar;
+        } else {
+            F.pflux = R.p * sStar;
+#pragma unroll
+            for (int ph = 0; ph < NPH; ++ph) F.alpha[ph] = R.alpha[ph] * sStar;
+        }
+    }
+}
+
+// computeRusanovFlux, src/RusanovSolver.cpp:7-83
+template <int D, int NPH>
+__device__ __forceinline__ void rusanov_flux(const Params& P, const FaceState<NPH>& L, const FaceState<NPH>& R,
+                                             FaceFlux<NPH>& F) {
+    const int dim = P.dim;
+    const bool incP = P.includePressure;
+    const double n[3] = {D == 0 ? 1.0 : 0.0, D == 1 ? 1.0 : 0.0, D == 2 ? 1.0 : 0.0};
+    F.mom[0] = F.mom[1] = F.mom[2] = 0.0;
+    double uL = normal_velocity<D>(L, dim), uR = normal_velocity<D>(R, dim);
+    double absUL = fabs(uL), absUR = fabs(uR);
+    double sMax;
+    if (incP) {
+        double cL = sound_speed_direct(L), cR = sound_speed_direct(R);
+        sMax = smax(absUL + cL, absUR + cR);
+    } else {
+        sMax = smax(absUL, absUR);
+    }
+    double rhoEL = rhoE_from_state(L), rhoER = rhoE_from_state(R);
+    double mL = L.rho * uL, mR = R.rho * uR;
+    double momL[3] = {0.0, 0.0, 0.0}, momR[3] = {0.0, 0.0, 0.0};
+    DIMLOOP(i) {
+        momL[i] = L.rho * L.u[i] * uL;
+        momR[i] = R.rho * R.u[i] * uR;
+    }
+    double eL = rhoEL * uL, eR = rhoER * uR;
+    if (incP) {
+        DIMLOOP(i) {
+            momL[i] += L.p * n[i];
+            momR[i] += R.p * n[i];
+        }
+        eL += L.p * uL;
+        eR += R.p * uR;
+    }
+    F.mass = 0.5 * (mL + mR) - 0.5 * sMax * (R.rho - L.rho);
+    DIMLOOP(i)
+        F.mom[i] = 0.5 * (momL[i] + momR[i]) - 0.5 * sMax * (R.rho * R.u[i] - L.rho * L.u[i]);
+    F.energy = 0.5 * (eL + eR) - 0.5 * sMax * (rhoER - rhoEL);
+    F.fvel = 0.5 * (uL + uR);
+    F.pflux = 0.5 * (L.p * uL + R.p * uR) - 0.5 * sMax * (R.p - L.p);
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph)
+        F.alpha[ph] = 0.5 * (L.alpha[ph] * uL + R.alpha[ph] * uR) - 0.5 * sMax * (R.alpha[ph] - L.alpha[ph]);
+}
+
+// computeLFFlux, src/LFSolver.cpp:8-75
+template <int D, int NPH>
+__device__ __forceinline__ void lf_flux(const Params& P, const FaceState<NPH>& L, const FaceState<NPH>& R,
+                                        FaceFlux<NPH>& F) {
+    const int dim = P.dim;
+    const bool incP = P.includePressure;
+    const double n[3] = {D == 0 ? 1.0 : 0.0, D == 1 ? 1.0 : 0.0, D == 2 ? 1.0 : 0.0};
+    F.mom[0] = F.mom[1] = F.mom[2] = 0.0;
+    double uL = normal_velocity<D>(L, dim), uR = normal_velocity<D>(R, dim);
+    double uLS = 0.0, uRS = 0.0;
+    DIMLOOP(i) {
+        uLS += L.u[i] * L.u[i];
+        uRS += R.u[i] * R.u[i];
+    }
+    uLS = sqrt(uLS);
+    uRS = sqrt(uRS);
+    double C;
+    if (incP) {
+        double cL = sound_speed_direct(L), cR = sound_speed_direct(R);
+        C = smax(uLS, uRS) + smax(cL, cR);
+    } else {
+        C = smax(uLS, uRS);
+    }
+    F.mass = 0.5 * (L.rho * uL + R.rho * uR) - 0.5 * C * (R.rho - L.rho);
+    DIMLOOP(i)
+        F.mom[i] = 0.5 * (L.rho * L.u[i] * uL + R.rho * R.u[i] * uR) - 0.5 * C * (R.rho * R.u[i] - L.rho * L.u[i]);
+    double rhoEL = rhoE_from_state(L), rhoER = rhoE_from_state(R);
+    F.energy = 0.5 * (rhoEL * uL + rhoER * uR) - 0.5 * C * (rhoER - rhoEL);
+    if (incP) {
+        DIMLOOP(i) F.mom[i] += 0.5 * (L.p + R.p) * n[i];
+        F.energy += 0.5 * (L.p * uL + R.p * uR);
+    }
+    if (P.useIGR) {
+        DIMLOOP(i) F.mom[i] += 0.5 * (L.sigma + R.sigma) * n[i];
+        F.energy += 0.5 * (L.sigma * uL + R.sigma * uR);
+    }
+    F.fvel = 0.5 * (uL + uR);
+    F.pflux = 0.5 * (L.p * uL + R.p * uR) - 0.5 * C * (R.p - L.p);
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph)
+        F.alpha[ph] = 0.5 * (L.alpha[ph] * uL + R.alpha[ph] * uR) - 0.5 * C * (R.alpha[ph] - L.alpha[ph]);
+}
+
+}  // namespace sifv

@@ -1,0 +1,906 @@
+// sifv_kernels.cuh -- CUDA kernels of the finite-volume step (sm_100a).
+//
+// One stage of the explicit step (ExplicitSolver::step,
+// src/ExplicitSolver.cpp:109-190) is:
+//   k_prim_bc      cons -> prim on interior cells, PRIM ghost fill composed
+//                  into one pass (every ghost cell computes the primitive of
+//                  its interior source itself, so no ordering is needed)
+//   k_face<DIR>    per face: reconstruction of both sides + Riemann flux
+//                  (+ upwinded partial-density flux), written SoA
+//   k_assemble     per cell: flux divergence in the reference's accumulation
+//                  order, sources, and the SSP-RK update (or the
+//                  semi-implicit star update), fused
+// The semi-implicit stage adds k_bc_prim, k_pressure_setup, the Jacobi
+// iterations (k_jacobi) and k_correction.  IGR runs k_igr_setup and one
+// k_igr_plane launch per anti-diagonal plane of the lexicographic
+// Gauss-Seidel sweep (the dependency order of src/IGR.cpp:110-156).
+#pragma once
+
+#include "sifv_device.cuh"
+
+namespace sifv {
+
+__device__ __forceinline__ double bits2d(unsigned long long b) { return __longlong_as_double((long long)b); }
+__device__ __forceinline__ unsigned long long d2bits(double d) { return (unsigned long long)__double_as_longlong(d); }
+
+// Decode a linear id over the extended grid into (i, j, k) with ghosts
+// (i in [-ngx, nx+ngx), ...).  Returns false past the end.
+__device__ __forceinline__ bool ext_coords(const Params& P, long long t, int& i, int& j, int& k) {
+    long long tot = (long long)P.nxT * P.nyT * P.nzT;
+    if (t >= tot) return false;
+    int ii = (int)(t % P.nxT);
+    long long r = t / P.nxT;
+    int jj = (int)(r % P.nyT);
+    int kk = (int)(r / P.nyT);
+    i = ii - P.ngx;
+    j = jj - P.ngy;
+    k = kk - P.ngz;
+    return true;
+}
+
+__device__ __forceinline__ bool int_coords(const Params& P, long long t, int& i, int& j, int& k) {
+    long long tot = (long long)P.nx * P.ny * P.nz;
+    if (t >= tot) return false;
+    i = (int)(t % P.nx);
+    long long r = t / P.nx;
+    j = (int)(r % P.ny);
+    k = (int)(r / P.ny);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Conservative -> primitive of one cell.
+// SolutionState::convertConservativeToPrimitiveVariables with
+// IdealGasEOS / StiffenedGasEOS::toPrimitive (src/SolutionState.cpp:187-205,
+// src/IdealGasEOS.cpp:46-64, src/StiffenedGasEOS.cpp:47-64), or
+// MixtureEOS::convertConservativeToPrimitive (src/MixtureEOS.cpp:99-143).
+// ---------------------------------------------------------------------------
+template <int NPH>
+__device__ __forceinline__ void cons_to_prim_cell(const Params& P, const Fields& F, size_t s, double& rhoOut,
+                                                  double u[3], double& p) {
+    const int dim = P.dim;
+    if (NPH == 0) {
+        double U[3] = {F.rhoU[s], (dim >= 2) ? F.rhoV[s] : 0.0, (dim >= 3) ? F.rhoW[s] : 0.0};
+        double rho = smax(F.rho[s], 1e-14);
+        u[0] = u[1] = u[2] = 0.0;
+        DIMLOOP(d) u[d] = U[d] / rho;
+        double ke = 0.0;
+        DIMLOOP(d) ke += u[d] * u[d];
+        ke *= 0.5 * rho;
+        double e = F.rhoE[s] - ke;
+        p = P.eosStiffened ? (P.gamma - 1.0) * e - P.gamma * P.pInf : smax((P.gamma - 1.0) * e, 1e-14);
+        rhoOut = F.rho[s];
+    } else {
+        double rho = 0.0;
+#pragma unroll
+        for (int ph = 0; ph < NPH; ++ph)
+            if (ph < P.nPh) rho += F.alphaRho[ph][s];
+        double rs = smax(rho, 1e-14);
+        u[0] = F.rhoU[s] / rs;
+        u[1] = (dim >= 2) ? F.rhoV[s] / rs : 0.0;
+        u[2] = (dim >= 3) ? F.rhoW[s] / rs : 0.0;
+        double ke = 0.5 * rs * u[0] * u[0];
+        if (dim >= 2) ke += 0.5 * rs * u[1] * u[1];
+        if (dim >= 3) ke += 0.5 * rs * u[2] * u[2];
+        double a[NPH > 0 ? NPH : 1];
+#pragma unroll
+        for (int ph = 0; ph < NPH; ++ph) a[ph] = (ph < P.nPh) ? F.alpha[ph][s] : 0.0;
+        p = mixture_pressure<NPH>(P, F.rhoE[s] - ke, a);
+        rhoOut = rs;
+    }
+}
+
+// Composed ghost source of cell (i,j,k) for the PRIM fill (onion peel
+// x -> y -> z, src/RectilinearMesh.cpp:127-131) and the velocity signs.
+__device__ __forceinline__ size_t prim_source(const Params& P, int i, int j, int k, double sg[3]) {
+    double sn, sa;
+    sg[0] = sg[1] = sg[2] = 1.0;
+    int si = prim_src(i, P.nx, P.bc[0], P.bc[1], sn, sa);
+    if (si != i) { sg[0] *= sn * sa; sg[1] *= sa; sg[2] *= sa; }
+    int sj = j, sk = k;
+    if (P.dim >= 2) {
+        sj = prim_src(j, P.ny, P.bc[2], P.bc[3], sn, sa);
+        if (sj != j) { sg[0] *= sa; sg[1] *= sn * sa; sg[2] *= sa; }
+    }
+    if (P.dim >= 3) {
+        sk = prim_src(k, P.nz, P.bc[4], P.bc[5], sn, sa);
+        if (sk != k) { sg[0] *= sa; sg[1] *= sa; sg[2] *= sn * sa; }
+    }
+    return cidx(P, si, sj, sk);
+}
+
+__device__ __forceinline__ bool is_interior(const Params& P, int i, int j, int k) {
+    return i >= 0 && i < P.nx && j >= 0 && j < P.ny && k >= 0 && k < P.nz;
+}
+
+// Stage entry: cons -> prim (interior) + PRIM ghost fill, one pass.
+template <int NPH>
+__global__ void k_prim_bc(Params P, Fields F, const Ctl* __restrict__ ctl, int interiorOnly) {
+    if (ctl && ctl->skip) return;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!ext_coords(P, t, i, j, k)) return;
+    const int dim = P.dim;
+    size_t d = cidx(P, i, j, k);
+    if (is_interior(P, i, j, k)) {
+        double rho, u[3], p;
+        cons_to_prim_cell<NPH>(P, F, d, rho, u, p);
+        F.velU[d] = u[0];
+        if (dim >= 2) F.velV[d] = u[1];
+        if (dim >= 3) F.velW[d] = u[2];
+        F.pres[d] = p;
+        if (NPH > 0) F.rho[d] = rho;
+        return;
+    }
+    if (interiorOnly) return;
+    double sg[3];
+    size_t s = prim_source(P, i, j, k, sg);
+    double rho, u[3], p;
+    cons_to_prim_cell<NPH>(P, F, s, rho, u, p);
+    F.rho[d] = rho;
+    F.velU[d] = sg[0] * u[0];
+    if (dim >= 2) F.velV[d] = sg[1] * u[1];
+    if (dim >= 3) F.velW[d] = sg[2] * u[2];
+    F.pres[d] = p;
+    F.sigma[d] = F.sigma[s];
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            F.alphaRho[ph][d] = F.alphaRho[ph][s];
+            F.alpha[ph][d] = F.alpha[ph][s];
+        }
+    }
+}
+
+// PRIM ghost fill from the primitive fields as they stand
+// (RectilinearMesh::applyBoundaryConditions(state, PRIM, halo),
+// src/RectilinearMesh.cpp:498-524 with SolutionState::copyCell_P).
+template <int NPH>
+__global__ void k_bc_prim(Params P, Fields F) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!ext_coords(P, t, i, j, k)) return;
+    if (is_interior(P, i, j, k)) return;
+    const int dim = P.dim;
+    size_t d = cidx(P, i, j, k);
+    double sg[3];
+    size_t s = prim_source(P, i, j, k, sg);
+    F.rho[d] = F.rho[s];
+    F.velU[d] = sg[0] * F.velU[s];
+    if (dim >= 2) F.velV[d] = sg[1] * F.velV[s];
+    if (dim >= 3) F.velW[d] = sg[2] * F.velW[s];
+    F.pres[d] = F.pres[s];
+    F.sigma[d] = F.sigma[s];
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            F.alphaRho[ph][d] = F.alphaRho[ph][s];
+            F.alpha[ph][d] = F.alpha[ph][s];
+        }
+    }
+}
+
+// Scalar ghost fill (RectilinearMesh::fillScalarGhosts, src/RectilinearMesh.cpp:424-492).
+__global__ void k_scalar_ghosts(Params P, double* __restrict__ f) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!ext_coords(P, t, i, j, k)) return;
+    if (is_interior(P, i, j, k)) return;
+    f[cidx(P, i, j, k)] = f[scalar_idx(P, i, j, k)];
+}
+
+// ---------------------------------------------------------------------------
+// Face flux: Reconstructor::reconstructX/Y/Z (src/Reconstruction.cpp:204-541)
+// then computeFluxDirect (include/RiemannSolver.hpp:91-100) and, for
+// multi-phase, the upwinded partial-density flux of computeRHS
+// (src/ExplicitSolver.cpp:307-326).
+// ---------------------------------------------------------------------------
+template <int DIR, int W, int NPH>
+__global__ void __launch_bounds__(128) k_face(Params P, Fields F, const Ctl* __restrict__ ctl) {
+    if (ctl && ctl->skip) return;
+    const int dim = P.dim;
+    // face grid: (nx + [DIR==0]) x (ny + [DIR==1]) x (nz + [DIR==2])
+    const int fnx = P.nx + (DIR == 0), fny = P.ny + (DIR == 1), fnz = P.nz + (DIR == 2);
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long tot = (long long)fnx * fny * fnz;
+    if (t >= tot) return;
+    int i = (int)(t % fnx);
+    long long r = t / fnx;
+    int j = (int)(r % fny);
+    int k = (int)(r / fny);
+    const size_t base = cidx(P, i, j, k);  // right cell of the face
+    const long st = (DIR == 0) ? 1L : (DIR == 1) ? (long)P.nxT : (long)P.nxT * P.nyT;
+    const bool weno = (P.reconOrder == SIFV_WENO1 || P.reconOrder == SIFV_WENO3 || P.reconOrder == SIFV_WENO5);
+    const double eps = P.wenoEps;
+
+    FaceState<NPH> L, R;
+    L.u[0] = L.u[1] = L.u[2] = 0.0;
+    R.u[0] = R.u[1] = R.u[2] = 0.0;
+    L.sigma = R.sigma = 0.0;
+    recon_pair<W>(F.rho, base, st, weno, eps, L.rho, R.rho);
+    recon_pair<W>(F.velU, base, st, weno, eps, L.u[0], R.u[0]);
+    if (dim >= 2) recon_pair<W>(F.velV, base, st, weno, eps, L.u[1], R.u[1]);
+    if (dim >= 3) recon_pair<W>(F.velW, base, st, weno, eps, L.u[2], R.u[2]);
+    recon_pair<W>(F.pres, base, st, weno, eps, L.p, R.p);
+    if (P.reconSigma) recon_pair<W>(F.sigma, base, st, weno, eps, L.sigma, R.sigma);
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        L.alpha[ph] = R.alpha[ph] = 0.0;
+        if (ph < P.nPh) recon_pair<W>(F.alpha[ph], base, st, weno, eps, L.alpha[ph], R.alpha[ph]);
+    }
+    if (NPH > 0) {
+        eff_gamma_piinf<NPH>(P, L.alpha, L.gEff, L.piEff);
+        eff_gamma_piinf<NPH>(P, R.alpha, R.gEff, R.piEff);
+    } else {
+        L.gEff = R.gEff = P.gamma;
+        L.piEff = R.piEff = P.pInf;
+    }
+
+    FaceFlux<NPH> Fx;
+    switch (P.riemann) {
+        case SIFV_HLLC: hllc_flux<DIR, NPH>(P, L, R, Fx); break;
+        case SIFV_RUSANOV: rusanov_flux<DIR, NPH>(P, L, R, Fx); break;
+        default: lf_flux<DIR, NPH>(P, L, R, Fx); break;
+    }
+
+    // reference face index (src/Reconstruction.cpp:71-81) == t
+    double* const* out = F.flux[DIR];
+    out[FS_MASS][t] = Fx.mass;
+    out[FS_MOMX][t] = Fx.mom[0];
+    if (dim >= 2) out[FS_MOMY][t] = Fx.mom[1];
+    if (dim >= 3) out[FS_MOMZ][t] = Fx.mom[2];
+    out[FS_ENERGY][t] = Fx.energy;
+    if (!P.includePressure) out[FS_PFLUX][t] = Fx.pflux;
+    if (!P.includePressure || NPH > 0) out[FS_FVEL][t] = Fx.fvel;
+    if (NPH > 0) {
+        size_t upw = (Fx.mass >= 0) ? base - st : base;
+        double rhoUpw = smax(F.rho[upw], 1e-14);
+#pragma unroll
+        for (int ph = 0; ph < NPH; ++ph) {
+            if (ph < P.nPh) {
+                out[FS_ALPHA + ph][t] = Fx.alpha[ph];
+                out[FS_AR + ph][t] = (F.alphaRho[ph][upw] / rhoUpw) * Fx.mass;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Assemble + update.  The flux divergence reproduces the accumulation order
+// of computeRHS (src/ExplicitSolver.cpp:294-483, src/SemiImplicitSolver.cpp:
+// 263-457): per direction x, y, z, the cell's low face adds coeff*F, its
+// high face subtracts it (divU: the opposite signs), starting from 0.
+// ---------------------------------------------------------------------------
+struct StageCoef {
+    double c1, c2, c3, c4;
+    int s;
+    double accel[3];   // body force accelerations (host-evaluated), or 0
+    int hasBodyForce;
+};
+
+struct CellFaces {
+    long long lo[3];
+    long long hiOff[3];
+    double coeff[3];
+};
+
+__device__ __forceinline__ void cell_faces(const Params& P, const Fields& F, int i, int j, int k, CellFaces& cf) {
+    double dxi = F.dx[i + P.ngx], dyj = F.dy[j + P.ngy], dzk = F.dz[k + P.ngz];
+    double vol = dxi * dyj * dzk;
+    cf.coeff[0] = (dyj * dzk) / vol;
+    cf.coeff[1] = (dxi * dzk) / vol;
+    cf.coeff[2] = (dxi * dyj) / vol;
+    cf.lo[0] = (long long)i + (long long)(P.nx + 1) * ((long long)j + (long long)P.ny * k);
+    cf.hiOff[0] = 1;
+    cf.lo[1] = (long long)i + (long long)P.nx * ((long long)j + (long long)(P.ny + 1) * k);
+    cf.hiOff[1] = P.nx;
+    cf.lo[2] = (long long)i + (long long)P.nx * ((long long)j + (long long)P.ny * k);
+    cf.hiOff[2] = (long long)P.nx * P.ny;
+}
+
+// divergence of one flux slot: ((0 + c F_lo) - c F_hi) per direction
+__device__ __forceinline__ double div_slot(const Params& P, const Fields& F, const CellFaces& cf, int slot) {
+    const int dim = P.dim;
+    double r = 0.0;
+    DIMLOOP(d) {
+        const double* f = F.flux[d][slot];
+        double c = cf.coeff[d];
+        r += c * f[cf.lo[d]];
+        r -= c * f[cf.lo[d] + cf.hiOff[d]];
+    }
+    return r;
+}
+
+__device__ __forceinline__ double div_fvel(const Params& P, const Fields& F, const CellFaces& cf) {
+    const int dim = P.dim;
+    double r = 0.0;
+    DIMLOOP(d) {
+        const double* f = F.flux[d][FS_FVEL];
+        double c = cf.coeff[d];
+        r -= c * f[cf.lo[d]];
+        r += c * f[cf.lo[d] + cf.hiOff[d]];
+    }
+    return r;
+}
+
+template <int NPH>
+__device__ __forceinline__ void mp_post(const Params& P, const Fields& F, size_t c) {
+    double rhoSum = 0.0;
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            double v = smax(F.alphaRho[ph][c], 1e-14);
+            F.alphaRho[ph][c] = v;
+            rhoSum += v;
+        }
+    }
+    F.rho[c] = rhoSum;
+    double a[NPH > 0 ? NPH : 1];
+    double aSum = 0.0;
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            a[ph] = smax(F.alpha[ph][c], P.alphaMin);
+        }
+    }
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph)
+        if (ph < P.nPh) aSum += a[ph];
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph)
+        if (ph < P.nPh) F.alpha[ph][c] = a[ph] / aSum;
+}
+
+// MODE 0: explicit SSP-RK update (src/ExplicitSolver.cpp:127-188).
+// MODE 1: semi-implicit star update (src/SemiImplicitSolver.cpp:159-223).
+template <int NPH, int MODE>
+__global__ void __launch_bounds__(256) k_assemble(Params P, Fields F, const Ctl* __restrict__ ctl, StageCoef K) {
+    if (ctl->skip) return;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(P, t, i, j, k)) return;
+    const int dim = P.dim;
+    const size_t c = cidx(P, i, j, k);
+    CellFaces cf;
+    cell_faces(P, F, i, j, k, cf);
+
+    double rR = div_slot(P, F, cf, FS_MASS);
+    double rU = div_slot(P, F, cf, FS_MOMX);
+    double rV = (dim >= 2) ? div_slot(P, F, cf, FS_MOMY) : 0.0;
+    double rW = (dim >= 3) ? div_slot(P, F, cf, FS_MOMZ) : 0.0;
+    double rE = div_slot(P, F, cf, FS_ENERGY);
+    double rP = 0.0, divU = 0.0;
+    if (MODE == 1) rP = div_slot(P, F, cf, FS_PFLUX);
+    if (MODE == 1 || NPH > 0) divU = div_fvel(P, F, cf);
+    double rAR[NPH > 0 ? NPH : 1], rA[NPH > 0 ? NPH : 1];
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            rAR[ph] = div_slot(P, F, cf, FS_AR + ph);
+            rA[ph] = div_slot(P, F, cf, FS_ALPHA + ph);
+            rA[ph] += F.alpha[ph][c] * divU;   // alpha div(u) source
+        }
+    }
+    if (MODE == 1) rP += F.pres[c] * divU;     // p div(u) source
+    if (K.hasBodyForce) {                      // src/ExplicitSolver.cpp:498-521
+        double rho = F.rho[c];
+        rU += rho * K.accel[0];
+        if (dim >= 2) rV += rho * K.accel[1];
+        if (dim >= 3) rW += rho * K.accel[2];
+        double work = F.velU[c] * K.accel[0];
+        if (dim >= 2) work += F.velV[c] * K.accel[1];
+        if (dim >= 3) work += F.velW[c] * K.accel[2];
+        rE += rho * work;
+    }
+
+    const double dt = ctl->dt;
+    const double c1 = K.c1, c2 = K.c2, c3 = K.c3, c4 = K.c4;
+    const int RK = P.RKOrder;
+    if (K.s == 0 && RK > 1) {   // SolutionState::saveConservativeCell, src/SolutionState.cpp:228-240
+        F.rho0[c] = F.rho[c];
+        F.rhoU0[c] = F.rhoU[c];
+        if (dim >= 2) F.rhoV0[c] = F.rhoV[c];
+        if (dim >= 3) F.rhoW0[c] = F.rhoW[c];
+        F.rhoE0[c] = F.rhoE[c];
+        F.pres0[c] = F.pres[c];
+#pragma unroll
+        for (int ph = 0; ph < NPH; ++ph) {
+            if (ph < P.nPh) {
+                F.alphaRho0[ph][c] = F.alphaRho[ph][c];
+                F.alpha0[ph][c] = F.alpha[ph][c];
+            }
+        }
+    }
+    if (MODE == 0) {
+        if (RK == 1) {
+            F.rho[c] += dt * rR;
+            F.rhoU[c] += dt * rU;
+            if (dim >= 2) F.rhoV[c] += dt * rV;
+            if (dim >= 3) F.rhoW[c] += dt * rW;
+            F.rhoE[c] += dt * rE;
+#pragma unroll
+            for (int ph = 0; ph < NPH; ++ph)
+                if (ph < P.nPh) F.alphaRho[ph][c] += dt * rAR[ph];
+#pragma unroll
+            for (int ph = 0; ph < NPH; ++ph)
+                if (ph < P.nPh) F.alpha[ph][c] += dt * rA[ph];
+        } else {
+            F.rho[c] = (c1 * F.rho[c] + c2 * F.rho0[c] + c3 * dt * rR) / c4;
+            F.rhoU[c] = (c1 * F.rhoU[c] + c2 * F.rhoU0[c] + c3 * dt * rU) / c4;
+            if (dim >= 2) F.rhoV[c] = (c1 * F.rhoV[c] + c2 * F.rhoV0[c] + c3 * dt * rV) / c4;
+            if (dim >= 3) F.rhoW[c] = (c1 * F.rhoW[c] + c2 * F.rhoW0[c] + c3 * dt * rW) / c4;
+            F.rhoE[c] = (c1 * F.rhoE[c] + c2 * F.rhoE0[c] + c3 * dt * rE) / c4;
+#pragma unroll
+            for (int ph = 0; ph < NPH; ++ph)
+                if (ph < P.nPh)
+                    F.alphaRho[ph][c] = (c1 * F.alphaRho[ph][c] + c2 * F.alphaRho0[ph][c] + c3 * dt * rAR[ph]) / c4;
+#pragma unroll
+            for (int ph = 0; ph < NPH; ++ph)
+                if (ph < P.nPh) F.alpha[ph][c] = (c1 * F.alpha[ph][c] + c2 * F.alpha0[ph][c] + c3 * dt * rA[ph]) / c4;
+        }
+        if (NPH > 0) mp_post<NPH>(P, F, c);
+    } else {
+        double pAdv = F.pres[c];
+        double r0 = (RK > 1) ? F.rho0[c] : 0.0;
+        double ru0 = (RK > 1) ? F.rhoU0[c] : 0.0;
+        double re0 = (RK > 1) ? F.rhoE0[c] : 0.0;
+        F.rho[c] = (c1 * F.rho[c] + c2 * r0 + c3 * dt * rR) / c4;
+        F.rhoUStar[c] = (c1 * F.rhoU[c] + c2 * ru0 + c3 * dt * rU) / c4;
+        if (dim >= 2) {
+            double rv0 = (RK > 1) ? F.rhoV0[c] : 0.0;
+            F.rhoVStar[c] = (c1 * F.rhoV[c] + c2 * rv0 + c3 * dt * rV) / c4;
+        }
+        if (dim >= 3) {
+            double rw0 = (RK > 1) ? F.rhoW0[c] : 0.0;
+            F.rhoWStar[c] = (c1 * F.rhoW[c] + c2 * rw0 + c3 * dt * rW) / c4;
+        }
+        F.rhoEstar[c] = (c1 * F.rhoE[c] + c2 * re0 + c3 * dt * rE) / c4;
+        double p0 = (RK > 1) ? F.pres0[c] : 0.0;
+        F.pAdvected[c] = (c1 * pAdv + c2 * p0 + c3 * dt * rP) / c4;
+        if (NPH > 0) {
+            if (RK == 1) {
+#pragma unroll
+                for (int ph = 0; ph < NPH; ++ph)
+                    if (ph < P.nPh) F.alphaRho[ph][c] += dt * rAR[ph];
+#pragma unroll
+                for (int ph = 0; ph < NPH; ++ph)
+                    if (ph < P.nPh) F.alpha[ph][c] += dt * rA[ph];
+            } else {
+#pragma unroll
+                for (int ph = 0; ph < NPH; ++ph)
+                    if (ph < P.nPh)
+                        F.alphaRho[ph][c] =
+                            (c1 * F.alphaRho[ph][c] + c2 * F.alphaRho0[ph][c] + c3 * dt * rAR[ph]) / c4;
+#pragma unroll
+                for (int ph = 0; ph < NPH; ++ph)
+                    if (ph < P.nPh)
+                        F.alpha[ph][c] = (c1 * F.alpha[ph][c] + c2 * F.alpha0[ph][c] + c3 * dt * rA[ph]) / c4;
+            }
+            mp_post<NPH>(P, F, c);
+        }
+        double rs = smax(F.rho[c], 1e-14);
+        F.velU[c] = F.rhoUStar[c] / rs;
+        if (dim >= 2) F.velV[c] = F.rhoVStar[c] / rs;
+        if (dim >= 3) F.velW[c] = F.rhoWStar[c] / rs;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------
+// Block-wide minimum of non-negative doubles, NaN ignored (std::min(dt, x)
+// keeps dt when x is NaN), folded into *acc with an integer atomicMin on the
+// bit pattern (order-preserving for non-negative doubles).
+__device__ __forceinline__ void block_min_to(double v, unsigned long long* acc) {
+    __shared__ double sm[32];
+    // v may be NaN: replace by +inf so it cannot win
+    if (!(v == v)) v = __longlong_as_double(0x7ff0000000000000LL);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        v = (lane < nw) ? sm[lane] : __longlong_as_double(0x7ff0000000000000LL);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) atomicMin(acc, d2bits(v));
+    }
+}
+
+// Block-wide maximum of non-negative doubles, NaN ignored (std::max(m, x)
+// keeps m when x is NaN), folded into *acc with atomicMax on the bits.
+__device__ __forceinline__ void block_max_to(double v, unsigned long long* acc) {
+    __shared__ double sm[32];
+    if (!(v == v)) v = 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = smax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sm[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        v = (lane < nw) ? sm[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = smax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) atomicMax(acc, d2bits(v));
+    }
+}
+
+// computeAcousticTimeStep (src/RKTimeStepping.cpp:43-123): min over
+// interior cells of cfl * min_d d_d / (|u_d| + c).
+template <int NPH>
+__global__ void __launch_bounds__(256) k_dt_acoustic(Params P, Fields F, Ctl* ctl, double cfl) {
+    if (ctl->skip) return;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    double v = __longlong_as_double(0x7ff0000000000000LL);
+    if (int_coords(P, t, i, j, k)) {
+        const int dim = P.dim;
+        size_t c = cidx(P, i, j, k);
+        double cs;
+        if (NPH > 0) {
+            double a[NPH > 0 ? NPH : 1], ar[NPH > 0 ? NPH : 1];
+#pragma unroll
+            for (int ph = 0; ph < NPH; ++ph) {
+                a[ph] = (ph < P.nPh) ? F.alpha[ph][c] : 0.0;
+                ar[ph] = (ph < P.nPh) ? F.alphaRho[ph][c] : 0.0;
+            }
+            cs = mixture_sound_speed<NPH>(P, F.rho[c], F.pres[c], a, ar);
+        } else {
+            cs = single_sound_speed(P, F.rho[c], F.pres[c]);
+        }
+        double dtCell = F.dx[i + P.ngx] / (fabs(F.velU[c]) + cs);
+        if (dim >= 2) dtCell = smin(dtCell, F.dy[j + P.ngy] / (fabs(F.velV[c]) + cs));
+        if (dim >= 3) dtCell = smin(dtCell, F.dz[k + P.ngz] / (fabs(F.velW[c]) + cs));
+        v = cfl * dtCell;
+    }
+    block_min_to(v, &ctl->dtBits);
+}
+
+// computeAdvectiveTimeStep (src/RKTimeStepping.cpp:15-41).
+__global__ void __launch_bounds__(256) k_dt_advective(Params P, Fields F, Ctl* ctl, double cfl) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    double v = __longlong_as_double(0x7ff0000000000000LL);
+    if (int_coords(P, t, i, j, k)) {
+        const int dim = P.dim;
+        size_t c = cidx(P, i, j, k);
+        double dtCell = F.dx[i + P.ngx] / smax(fabs(F.velU[c]), 1e-14);
+        if (dim >= 2) dtCell = smin(dtCell, F.dy[j + P.ngy] / smax(fabs(F.velV[c]), 1e-14));
+        if (dim >= 3) dtCell = smin(dtCell, F.dz[k + P.ngz] / smax(fabs(F.velW[c]), 1e-14));
+        v = cfl * dtCell;
+    }
+    block_min_to(v, &ctl->dtBits);
+}
+
+// Reset the dt accumulator to maxDt (dt starts at maxDt in the reference).
+__global__ void k_dt_init(Ctl* ctl, double maxDt) {
+    if (ctl->skip) return;
+    ctl->dtBits = d2bits(maxDt);
+}
+
+// dt = min(maxDt, reduction); constDt; min with targetDt; semi-implicit
+// clamp (src/ExplicitSolver.cpp:72-90, src/SemiImplicitSolver.cpp:110-123).
+// useEnd: device-resident loop, targetDt = tEnd - time and steps past tEnd
+// are skipped.
+__global__ void k_dt_finalize(Ctl* ctl, double constDt, double targetDt, int clampSemi, double minDt, double maxDt,
+                              int useEnd) {
+    if (useEnd) {
+        if (!(ctl->time < ctl->tEnd)) {
+            ctl->skip = 1;
+            return;
+        }
+        ctl->skip = 0;
+        targetDt = ctl->tEnd - ctl->time;
+    }
+    double dt = (constDt > 0) ? constDt : bits2d(ctl->dtBits);
+    if (targetDt > 0) dt = smin(dt, targetDt);
+    if (clampSemi) dt = (dt < minDt) ? minDt : (maxDt < dt) ? maxDt : dt;
+    ctl->dt = dt;
+}
+
+__global__ void k_time_advance(Ctl* ctl) {
+    if (ctl->skip) return;
+    ctl->time += ctl->dt;
+    ctl->stepsTaken += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Semi-implicit pressure: SemiImplicitSolver::solvePressure
+// (src/SemiImplicitSolver.cpp:533-588) and computeDivergence (680-717).
+// ---------------------------------------------------------------------------
+template <int NPH>
+__global__ void __launch_bounds__(256) k_pressure_setup(Params P, Fields F, const Ctl* __restrict__ ctl) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(P, t, i, j, k)) return;
+    const int dim = P.dim;
+    size_t c = cidx(P, i, j, k);
+    double cs;
+    if (NPH > 0) {
+        double a[NPH > 0 ? NPH : 1], ar[NPH > 0 ? NPH : 1];
+#pragma unroll
+        for (int ph = 0; ph < NPH; ++ph) {
+            a[ph] = (ph < P.nPh) ? F.alpha[ph][c] : 0.0;
+            ar[ph] = (ph < P.nPh) ? F.alphaRho[ph][c] : 0.0;
+        }
+        cs = mixture_sound_speed<NPH>(P, F.rho[c], F.pres[c], a, ar);
+    } else {
+        cs = single_sound_speed(P, F.rho[c], F.pres[c]);
+    }
+    double rhoc2 = F.rho[c] * cs * cs;
+    F.rhoc2[c] = rhoc2;
+    double div = 0.0;
+    {
+        size_t xm = c - 1, xp = c + 1;
+        double fl = 0.5 * (F.velU[xm] + F.velU[c]);
+        double fr = 0.5 * (F.velU[c] + F.velU[xp]);
+        div += (fr - fl) / F.dx[i + P.ngx];
+    }
+    if (dim >= 2) {
+        size_t s = (size_t)P.nxT;
+        double fl = 0.5 * (F.velV[c - s] + F.velV[c]);
+        double fr = 0.5 * (F.velV[c] + F.velV[c + s]);
+        div += (fr - fl) / F.dy[j + P.ngy];
+    }
+    if (dim >= 3) {
+        size_t s = (size_t)P.nxT * P.nyT;
+        double fl = 0.5 * (F.velW[c - s] + F.velW[c]);
+        double fr = 0.5 * (F.velW[c] + F.velW[c + s]);
+        div += (fr - fl) / F.dz[k + P.ngz];
+    }
+    F.divUstar[c] = div;
+    F.pRhs[c] = F.pAdvected[c] - rhoc2 * ctl->dt * div;
+    F.pA[c] = F.pres[c];
+}
+
+// One Jacobi iteration of JacobiPressureSolver::solve
+// (src/JacobiPressureSolver.cpp:57-108) with pressureLaplacian
+// (src/PressureLaplacian.cpp:6-60).  Ghost pressures are read through the
+// scalar ghost map (fillScalarGhosts at the top of every iteration); rho
+// ghosts are the stored PRIM ghosts.  Iteration `it` first checks whether
+// iteration it-1 converged (max |dp| < tol) and then does nothing, so
+// batches of iterations can be queued without a host round trip.
+__global__ void __launch_bounds__(256) k_jacobi(Params P, const double* __restrict__ rho,
+                                                const double* __restrict__ rhoc2, const double* __restrict__ rhs,
+                                                const double* __restrict__ pin, double* __restrict__ pout, Fields F,
+                                                Ctl* ctl, int it, double tol) {
+    if (ctl->jacobiDone) return;
+    if (it > 0 && bits2d(ctl->res[it - 1]) < tol) {
+        if (threadIdx.x == 0) ctl->jacobiDone = it;
+        return;
+    }
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    double res = 0.0;
+    if (int_coords(P, t, i, j, k)) {
+        const int dim = P.dim;
+        const double dt = ctl->dt;
+        const double dt2 = dt * dt;
+        size_t c = cidx(P, i, j, k);
+        double coeff = rhoc2[c] * dt2;
+        double od = 0.0, diag = 0.0;
+        {
+            size_t xm = c - 1, xp = c + 1;
+            size_t pxm = scalar_idx(P, i - 1, j, k), pxp = scalar_idx(P, i + 1, j, k);
+            double rL = 0.5 * (rho[c] + rho[xm]), rR = 0.5 * (rho[c] + rho[xp]);
+            double dm = F.dx[i - 1 + P.ngx], d0 = F.dx[i + P.ngx], dp = F.dx[i + 1 + P.ngx];
+            double dL = 0.5 * (dm + d0), dR = 0.5 * (d0 + dp);
+            double cL = 1.0 / (smax(rL, 1e-14) * dL * d0);
+            double cR = 1.0 / (smax(rR, 1e-14) * dR * d0);
+            od += cL * pin[pxm] + cR * pin[pxp];
+            diag += cL + cR;
+        }
+        if (dim >= 2) {
+            size_t s = (size_t)P.nxT;
+            size_t pym = scalar_idx(P, i, j - 1, k), pyp = scalar_idx(P, i, j + 1, k);
+            double rL = 0.5 * (rho[c] + rho[c - s]), rR = 0.5 * (rho[c] + rho[c + s]);
+            double dm = F.dy[j - 1 + P.ngy], d0 = F.dy[j + P.ngy], dp = F.dy[j + 1 + P.ngy];
+            double dL = 0.5 * (dm + d0), dR = 0.5 * (d0 + dp);
+            double cL = 1.0 / (smax(rL, 1e-14) * dL * d0);
+            double cR = 1.0 / (smax(rR, 1e-14) * dR * d0);
+            od += cL * pin[pym] + cR * pin[pyp];
+            diag += cL + cR;
+        }
+        if (dim >= 3) {
+            size_t s = (size_t)P.nxT * P.nyT;
+            size_t pzm = scalar_idx(P, i, j, k - 1), pzp = scalar_idx(P, i, j, k + 1);
+            double rL = 0.5 * (rho[c] + rho[c - s]), rR = 0.5 * (rho[c] + rho[c + s]);
+            double dm = F.dz[k - 1 + P.ngz], d0 = F.dz[k + P.ngz], dp = F.dz[k + 1 + P.ngz];
+            double dL = 0.5 * (dm + d0), dR = 0.5 * (d0 + dp);
+            double cL = 1.0 / (smax(rL, 1e-14) * dL * d0);
+            double cR = 1.0 / (smax(rR, 1e-14) * dR * d0);
+            od += cL * pin[pzm] + cR * pin[pzp];
+            diag += cL + cR;
+        }
+        double denom = 1.0 + coeff * diag;
+        double pn = (rhs[c] + coeff * od) / denom;
+        pout[c] = pn;
+        res = fabs(pn - pin[c]);
+    }
+    block_max_to(res, &ctl->res[it]);
+}
+
+// Copy the converged Jacobi iterate (in pA or pB by parity) to dst.
+__global__ void k_jacobi_finish(Params P, const double* __restrict__ pA, const double* __restrict__ pB,
+                                double* __restrict__ dst, const Ctl* __restrict__ ctl, int maxIter) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(P, t, i, j, k)) return;
+    int n = ctl->jacobiDone ? ctl->jacobiDone : maxIter;
+    const double* src = (n & 1) ? pB : pA;
+    size_t c = cidx(P, i, j, k);
+    dst[c] = src[c];
+}
+
+// SemiImplicitSolver::correctionStep (src/SemiImplicitSolver.cpp:590-678),
+// all per-cell parts fused: momentum from the face-averaged gradient of
+// p + sigma (scalar-ghost-filled), velocities, pres = p, and total energy
+// from the EOS.  The PRIM ghost fill that follows is k_bc_prim.
+template <int NPH>
+__global__ void __launch_bounds__(256) k_correction(Params P, Fields F, const double* __restrict__ Pn,
+                                                    const Ctl* __restrict__ ctl) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(P, t, i, j, k)) return;
+    const int dim = P.dim;
+    const double dt = ctl->dt;
+    size_t c = cidx(P, i, j, k);
+    const double* S = F.sigma;
+    double pc = Pn[c] + S[c];
+    {
+        size_t m = scalar_idx(P, i - 1, j, k), p = scalar_idx(P, i + 1, j, k);
+        double pTotL = 0.5 * ((Pn[m] + S[m]) + pc);
+        double pTotR = 0.5 * (pc + (Pn[p] + S[p]));
+        F.rhoU[c] = F.rhoUStar[c] - dt * (pTotR - pTotL) / F.dx[i + P.ngx];
+    }
+    if (dim >= 2) {
+        size_t m = scalar_idx(P, i, j - 1, k), p = scalar_idx(P, i, j + 1, k);
+        double pTotL = 0.5 * ((Pn[m] + S[m]) + pc);
+        double pTotR = 0.5 * (pc + (Pn[p] + S[p]));
+        F.rhoV[c] = F.rhoVStar[c] - dt * (pTotR - pTotL) / F.dy[j + P.ngy];
+    }
+    if (dim >= 3) {
+        size_t m = scalar_idx(P, i, j, k - 1), p = scalar_idx(P, i, j, k + 1);
+        double pTotL = 0.5 * ((Pn[m] + S[m]) + pc);
+        double pTotR = 0.5 * (pc + (Pn[p] + S[p]));
+        F.rhoW[c] = F.rhoWStar[c] - dt * (pTotR - pTotL) / F.dz[k + P.ngz];
+    }
+    double rho = F.rho[c];
+    double rs = smax(rho, 1e-14);
+    double u = F.rhoU[c] / rs;
+    double v = (dim >= 2) ? F.rhoV[c] / rs : 0.0;
+    double w = (dim >= 3) ? F.rhoW[c] / rs : 0.0;
+    F.velU[c] = u;
+    if (dim >= 2) F.velV[c] = v;
+    if (dim >= 3) F.velW[c] = w;
+    double pn = Pn[c];
+    F.pres[c] = pn;
+    double ke = 0.5 * rho * u * u;
+    if (dim >= 2) ke += 0.5 * rho * v * v;
+    if (dim >= 3) ke += 0.5 * rho * w * w;
+    if (NPH > 0) {
+        double a[NPH > 0 ? NPH : 1];
+#pragma unroll
+        for (int ph = 0; ph < NPH; ++ph) a[ph] = (ph < P.nPh) ? F.alpha[ph][c] : 0.0;
+        F.rhoE[c] = mixture_total_energy<NPH>(P, pn, a, ke);
+    } else {
+        F.rhoE[c] = (pn + P.gamma * P.pInf) / (P.gamma - 1.0) + ke;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// IGR (src/IGR.cpp)
+// ---------------------------------------------------------------------------
+// Velocity gradient (IGRSolver::computeVelocityGradient, src/IGR.cpp:160-200),
+// RHS alpha (tr(gu gu) + tr(gu)^2) (computeIGRRhs, 18-35) and the diagonal
+// 1/rho + sum alpha/d^2 (1/rho_fl + 1/rho_fr) of the sweep (114-142), which
+// do not change across sweeps.
+__global__ void __launch_bounds__(256) k_igr_setup(Params P, Fields F, double alpha) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(P, t, i, j, k)) return;
+    const int dim = P.dim;
+    size_t c = cidx(P, i, j, k);
+    const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+    double g[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) g[q] = 0.0;
+    double invDx = 0.5 / F.dx[i + P.ngx];
+    double invDy = 0.5 / ((dim >= 2) ? F.dy[j + P.ngy] : 1.0);
+    double invDz = 0.5 / ((dim >= 3) ? F.dz[k + P.ngz] : 1.0);
+    g[0] = (F.velU[c + 1] - F.velU[c - 1]) * invDx;
+    if (dim >= 2) {
+        g[3] = (F.velV[c + 1] - F.velV[c - 1]) * invDx;
+        g[1] = (F.velU[c + sy] - F.velU[c - sy]) * invDy;
+        g[4] = (F.velV[c + sy] - F.velV[c - sy]) * invDy;
+        if (dim >= 3) {
+            g[7] = (F.velW[c + sy] - F.velW[c - sy]) * invDy;
+            g[6] = (F.velW[c + 1] - F.velW[c - 1]) * invDx;
+            g[2] = (F.velU[c + sz] - F.velU[c - sz]) * invDz;
+            g[5] = (F.velV[c + sz] - F.velV[c - sz]) * invDz;
+            g[8] = (F.velW[c + sz] - F.velW[c - sz]) * invDz;
+        }
+    }
+    double trSq = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            if (a < dim && b < dim) trSq += g[3 * a + b] * g[3 * b + a];
+    double tr = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        if (a < dim) tr += g[4 * a];
+    tr *= tr;
+    F.igrRhs[c] = alpha * (trSq + tr);
+
+    double rho_i = F.rho[c];
+    double diag = 1.0 / rho_i;
+    {
+        double rfl = 0.5 * (rho_i + F.rho[c - 1]), rfr = 0.5 * (rho_i + F.rho[c + 1]);
+        diag += F.adx2[i + P.ngx] * (1.0 / rfl + 1.0 / rfr);
+    }
+    if (dim >= 2) {
+        double rfl = 0.5 * (rho_i + F.rho[c - sy]), rfr = 0.5 * (rho_i + F.rho[c + sy]);
+        diag += F.ady2[j + P.ngy] * (1.0 / rfl + 1.0 / rfr);
+    }
+    if (dim >= 3) {
+        double rfl = 0.5 * (rho_i + F.rho[c - sz]), rfr = 0.5 * (rho_i + F.rho[c + sz]);
+        diag += F.adz2[k + P.ngz] * (1.0 / rfl + 1.0 / rfr);
+    }
+    F.igrDiag[c] = diag;
+}
+
+__device__ __forceinline__ void igr_cell(const Params& P, const Fields& F, int i, int j, int k) {
+    const int dim = P.dim;
+    size_t c = cidx(P, i, j, k);
+    const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+    double* S = F.sigma;
+    double rho_i = F.rho[c];
+    double off = 0.0;
+    {
+        double rfl = 0.5 * (rho_i + F.rho[c - 1]), rfr = 0.5 * (rho_i + F.rho[c + 1]);
+        off += F.adx2[i + P.ngx] * (S[c - 1] / rfl + S[c + 1] / rfr);
+    }
+    if (dim >= 2) {
+        double rfl = 0.5 * (rho_i + F.rho[c - sy]), rfr = 0.5 * (rho_i + F.rho[c + sy]);
+        off += F.ady2[j + P.ngy] * (S[c - sy] / rfl + S[c + sy] / rfr);
+    }
+    if (dim >= 3) {
+        double rfl = 0.5 * (rho_i + F.rho[c - sz]), rfr = 0.5 * (rho_i + F.rho[c + sz]);
+        off += F.adz2[k + P.ngz] * (S[c - sz] / rfl + S[c + sz] / rfr);
+    }
+    S[c] = (F.igrRhs[c] + off) / F.igrDiag[c];
+}
+
+// All cells of anti-diagonal plane i + j + k = plane.  Cells of one plane
+// only depend on planes plane-1 (already updated in this sweep) and plane+1
+// (not yet updated), which is the dependency order of the lexicographic
+// in-place sweep.
+__global__ void __launch_bounds__(256) k_igr_plane(Params P, Fields F, int plane) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int j, k;
+    if (P.dim == 2) {
+        if (t >= P.ny) return;
+        j = (int)t;
+        k = 0;
+    } else {
+        if (t >= (long long)P.ny * P.nz) return;
+        j = (int)(t % P.ny);
+        k = (int)(t / P.ny);
+    }
+    int i = plane - j - k;
+    if (i < 0 || i >= P.nx) return;
+    igr_cell(P, F, i, j, k);
+}
+
+// 1D sweep: a single thread walks the line in order.
+__global__ void k_igr_sweep_1d(Params P, Fields F) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int i = 0; i < P.nx; ++i) igr_cell(P, F, i, 0, 0);
+}
+
+}  // namespace sifv

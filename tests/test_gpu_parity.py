@@ -1,0 +1,167 @@
+"""Parity of the CUDA library (through the C ABI) against the C oracle.
+
+The FP64 build evaluates every expression in the reference's order without
+FMA contraction, so the expected result is bit-identical fields; the
+acceptance bar (relative L-infinity <= 1e-10 per variable, the pressure
+solve to pressureTol) is asserted as well and reported separately."""
+import numpy as np
+import pytest
+
+import backends
+import cases
+from semiimplicitfv_b200 import abi
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10   # relative L-infinity per conserved variable
+
+
+def _fields(cfg):
+    f = [abi.F_RHO, abi.F_RHOU, abi.F_RHOE, abi.F_VELU, abi.F_PRES, abi.F_SIGMA]
+    if cfg.dim >= 2:
+        f += [abi.F_RHOV, abi.F_VELV]
+    if cfg.dim >= 3:
+        f += [abi.F_RHOW, abi.F_VELW]
+    for p in range(cfg.nPhases):
+        f += [abi.F_ALPHARHO(p), abi.F_ALPHA(p)]
+    return f
+
+
+def run_pair(case, nsteps, t_end=None):
+    cg = backends.make(backends.cuda(), case)
+    co = backends.make(backends.oracle(), case)
+    tg, sg, dtg = cases.run_steps(cg, nsteps, t_end)
+    to, so, dto = cases.run_steps(co, nsteps, t_end)
+    return cg, co, dtg, dto
+
+
+def check(case, nsteps, t_end=None, bitwise=True):
+    cg, co, dtg, dto = run_pair(case, nsteps, t_end)
+    assert len(dtg) == len(dto)
+    np.testing.assert_allclose(dtg, dto, rtol=TOL, atol=0)
+    worst = {}
+    for fid in _fields(case[0]):
+        a, b = cg.get_field(fid), co.get_field(fid)
+        ia, ib = cg.interior(a), co.interior(b)
+        scale = max(np.abs(ib).max(), 1e-300)
+        rel = np.abs(ia - ib).max() / scale
+        worst[fid] = rel
+        assert rel <= TOL, f"field {fid}: relative L-inf {rel:.3e} > {TOL}"
+        if bitwise:
+            assert np.array_equal(a.view(np.int64), b.view(np.int64)), \
+                f"field {fid} not bit-identical (rel {rel:.3e})"
+    if case[0].semiImplicit:
+        assert cg.last_pressure_iterations() == co.last_pressure_iterations()
+    return worst
+
+
+def test_sod_full_config():
+    """Config 1 in full: 1000 cells, WENO5 + HLLC, RK3, CFL 0.6, to t = 0.2."""
+    check(cases.sod(1000), 100000, t_end=0.2)
+
+
+@pytest.mark.parametrize("recon", [abi.WENO1, abi.WENO3, abi.WENO5, abi.UPWIND1, abi.UPWIND3, abi.UPWIND5])
+@pytest.mark.parametrize("riemann", [abi.LF, abi.RUSANOV, abi.HLLC])
+def test_sod_orders_solvers(recon, riemann):
+    check(cases.sod(120, recon=recon, riemann=riemann), 30)
+
+
+@pytest.mark.parametrize("bc", [abi.BC_OUTFLOW, abi.BC_PERIODIC, abi.BC_SLIPWALL, abi.BC_NOSLIPWALL,
+                                abi.BC_SYMMETRY])
+def test_riemann2d_boundaries(bc):
+    check(cases.riemann2d(40, bc=bc), 8)
+
+
+def test_riemann2d_many_steps():
+    check(cases.riemann2d(96), 60)
+
+
+def test_riemann2d_weno_eps_example():
+    check(cases.riemann2d(64, weno_eps=1e-16), 20)
+
+
+@pytest.mark.parametrize("rk", [1, 2, 3])
+def test_water_air(rk):
+    check(cases.water_air(200, rk=rk), 40)
+
+
+def test_water_air_config5_instance():
+    check(cases.water_air(1024, x_interface=0.43, p_left=7.3e8), 300, t_end=1e-4)
+
+
+@pytest.mark.parametrize("rk,igr", [(1, True), (3, True), (2, False)])
+def test_acoustic3d_semi_implicit(rk, igr):
+    check(cases.acoustic3d(16, rk=rk, igr=igr), 3)
+
+
+def test_explicit_3d_igr_lf():
+    case = cases.acoustic3d(12, semi=False, igr=True, rk=3, riemann=abi.LF)
+    case[0].cfl = 0.5
+    check(case, 3)
+
+
+def test_stiffened_and_body_force():
+    case = cases.riemann2d(32, rk=2)
+    case[0].eosKind = abi.EOS_STIFFENED
+    case[0].pInf = 0.3
+    case[0].bfA[0], case[0].bfB[0], case[0].bfC[0] = 0.1, 0.05, 3.0
+    case[0].bfA[1] = -0.2
+    check(case, 6)
+
+
+def test_semi_implicit_multiphase():
+    case = cases.water_air(64, p_left=2e5, rk=1)
+    case[0].semiImplicit = 1
+    case[0].siCfl = 0.5
+    case[0].siMaxDt = 1e-5
+    check(case, 4)
+
+
+def test_standalone_pressure_solve_dt_and_igr():
+    case = cases.acoustic3d(12)
+    cg = backends.make(backends.cuda(), case)
+    co = backends.make(backends.oracle(), case)
+    rng = np.random.default_rng(11)
+    n = cg.ncells
+    rho = 1.0 + 0.1 * rng.random(n)
+    rhoc2 = 1.4 + 0.2 * rng.random(n)
+    rhs = rng.random(n)
+    p0 = rng.random(n)
+    pg, ig, _ = cg.pressure_solve(rho, rhoc2, rhs, p0, 1e-2, 1e-12, 60)
+    po, io, _ = co.pressure_solve(rho, rhoc2, rhs, p0, 1e-2, 1e-12, 60)
+    assert ig == io
+    assert np.array_equal(cg.interior(pg), co.interior(po))
+    assert cg.acoustic_dt(0.6, 1.0) == co.acoustic_dt(0.6, 1.0)
+    assert cg.advective_dt(0.8, 1.0) == co.advective_dt(0.8, 1.0)
+    for c in (cg, co):
+        c.convert_cons_to_prim()
+        c.apply_bc()
+        c.igr_solve(0)
+    assert np.array_equal(cg.get_field(abi.F_SIGMA), co.get_field(abi.F_SIGMA))
+
+
+def test_not_converged_status():
+    case = cases.acoustic3d(8)
+    cg = backends.make(backends.cuda(), case)
+    n = cg.ncells
+    _, iters, st = cg.pressure_solve(np.ones(n), np.ones(n), np.ones(n), np.zeros(n), 1.0, 1e-30, 1)
+    assert iters == 1 and st == abi.NOT_CONVERGED
+
+
+def test_bad_config_rejected():
+    cfg, mesh, _ = cases.sod(50)
+    cfg.nGhost = 1
+    with pytest.raises(abi.AbiError) as e:
+        backends.cuda().create(cfg, mesh)
+    assert e.value.status == abi.ERR_BAD_CONFIG
+
+
+def test_advance_matches_step():
+    case = cases.riemann2d(48)
+    c1 = backends.make(backends.cuda(), case)
+    c2 = backends.make(backends.cuda(), case)
+    t1, s1, _ = cases.run_steps(c1, 7, t_end=0.05)
+    t2, s2 = c2.advance(0, 0.0, 0.05, 7)
+    assert s1 == s2 and t1 == t2
+    for fid in (abi.F_RHO, abi.F_RHOU, abi.F_RHOV, abi.F_RHOE, abi.F_PRES):
+        assert np.array_equal(c1.get_field(fid), c2.get_field(fid))
