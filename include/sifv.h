@@ -224,6 +224,37 @@ int sifv_apply_bc(sifv_ctx_t* ctx);
  * call, and the number of kernel launches it made. */
 int sifv_last_step_stats(const sifv_ctx_t* ctx, double* deviceMs, int* launches);
 
+/* ---- allocation-free pressure solve ----------------------------------- */
+/* Sizes of the static device scratch behind sifv_pressure_solve_noalloc
+ * (reserved on every GPU that loads the library, about 32 MB). */
+#define SIFV_NOALLOC_MAX_CELLS 2097152   /* cells per solve, ghosts included */
+#define SIFV_NOALLOC_MAX_ITERS 4096      /* maxIter */
+#define SIFV_NOALLOC_MAX_AXIS  8192      /* cells along one axis, ghosts included */
+
+/* The Jacobi pressure solve of sifv_pressure_solve for callers that cannot
+ * allocate device memory -- hosts whose GPU memory belongs to their own
+ * pool allocator, or code that must not call cudaMalloc/cudaFree between
+ * stream operations because those calls can synchronise the device.  It
+ * needs no context and allocates nothing: the two Jacobi iterates, the
+ * residual slots and the cell widths live in one file-scope static device
+ * array (the sizes above).  This entry point has no counterpart in the
+ * reference.
+ *
+ * rho, rhoc2, rhs and pressure are DEVICE arrays of the mesh's totalCells
+ * (ghosts included, x fastest) on the current device; pressure holds the
+ * initial guess and receives the solution in its interior cells (ghosts
+ * untouched).  Work is queued on `stream` (NULL: the legacy default
+ * stream).  Meshes or maxIter above the SIFV_NOALLOC_* limits are rejected
+ * with SIFV_ERR_BAD_ARG.  The first call on a device looks up the static
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls on a device
+ * share the one array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Errors: sifv_noalloc_last_error(). */
+int sifv_pressure_solve_noalloc(const sifv_mesh_t* mesh, int dim, int nGhost, const double* rho,
+                                const double* rhoc2, const double* rhs, double* pressure, double dt,
+                                double tol, int maxIter, void* stream, int* iters);
+const char* sifv_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

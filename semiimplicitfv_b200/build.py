@@ -14,7 +14,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libsifv_b200.so")
-SOURCES = ["sifv_capi.cu"]
+SOURCES = ["sifv_capi.cu", "sifv_noalloc.cu"]
 HEADERS = ["sifv_device.cuh", "sifv_kernels.cuh"]
 
 NVCC_FLAGS = [
