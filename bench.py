@@ -30,8 +30,19 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 METRIC = "cell-updates/s per RK3 step (2D Riemann 4096^2, WENO5+HLLC, FP64)"
+PREC_NAMES = {0: "fp64-reference-order", 1: "mixed-fp32-bulk", 2: "fp64-fast"}
 UNIT = "cell-updates/s"
 BYTES_PER_CELL_UPDATE = 256   # algorithmic: 64 B x 4 conserved variables per RK3 step
+# Algorithmic bytes per cell of one launch of each kernel family of the 2D
+# fused-sweep step (FP64 arrays, 8 B per value):
+#   sweep_x  reads rho, rhoU, rhoV, rhoE; writes velU, velV, pres and the
+#            4-array rhs                                        11 x 8 = 88
+#   sweep_y  reads rho, velU, velV, pres, 4 rhs, 4 U and 4 U0 (stage 0:
+#            pres and U, writes U0 + pres0); writes 4 U     avg 20.67 x 8 = 165.3
+#   dt       reads rho, velU, velV, pres                         4 x 8 = 32
+#   finish_prim reads 4 U, writes velU, velV, pres              7 x 8 = 56
+KERNEL_BYTES_PER_CELL_2D = {"sweep_x": 88.0, "sweep_y": 165.33, "dt": 32.0, "finish_prim": 56.0,
+                            "face_x": 64.0, "face_y": 64.0, "assemble": 229.3, "prim_bc": 56.0}
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -47,29 +58,36 @@ def _peaks():
 class ClockSampler:
     """nvidia-smi clocks + throttle reasons sampled during the timed region."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.lines = []          # (host time, csv line)
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0:   # wait for the sampler to run
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t_start: float, t_end: float):
+        self.window = (t_start, t_end)
 
     def __exit__(self, *a):
         if self.proc:
@@ -82,16 +100,20 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines
+        if self.window:   # samples taken while the timed region ran (0.1 s slack for pipe latency)
+            inside = [x for x in lines if self.window[0] - 0.1 <= x[0] <= self.window[1] + 0.1]
+            lines = inside or lines
+        for _, ln in lines:
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 8:
+            if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
             except ValueError:
                 continue
-            for n, v in zip(names, parts[4:8]):
+            for n, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
@@ -171,15 +193,8 @@ def run_cuda(args):
     import cases
     from semiimplicitfv_b200 import abi
     n = args.n
-    case = cases.riemann2d(n)
-    ctx = backends.cuda().create(case[0], case[1], local)
-    # inputs uploaded from pinned host memory
-    for fid, arr in case[2].items():
-        pinned = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
-        ctx.be.fn["set_field"](ctx.h, fid, ctypes.c_void_p(pinned.data_ptr()), 0)
-    stream = torch.cuda.current_stream()
-    ctx.be.fn["set_stream"](ctx.h, ctypes.c_void_p(stream.cuda_stream))
     cells = n * n
+    stream = torch.cuda.current_stream()
 
     def barrier():
         if ws > 1:
@@ -192,37 +207,85 @@ def run_cuda(args):
             return float(t.item())
         return x
 
-    # warm-up
-    t_sim, s_sim = ctx.advance(0, 0.0, -1.0, args.warmup)
-    step_idx = args.warmup
+    def make_ctx(precision):
+        case = cases.riemann2d(n)
+        case[0].precision = precision
+        ctx = backends.cuda().create(case[0], case[1], local)
+        for fid, arr in case[2].items():   # inputs uploaded from pinned host memory
+            pinned = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
+            ctx.be.fn["set_field"](ctx.h, fid, ctypes.c_void_p(pinned.data_ptr()), 0)
+        ctx.be.fn["set_stream"](ctx.h, ctypes.c_void_p(stream.cuda_stream))
+        return ctx
 
-    # ---- device-resident timed region -------------------------------------
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    def measure(precision, with_clocks=False, with_e2e=False):
+        ctx = make_ctx(precision)
+        clk = ClockSampler(local) if with_clocks else None
+        if clk:
+            clk.__enter__()
+        t_sim, _ = ctx.advance(0, 0.0, -1.0, args.warmup)
+        step_idx = args.warmup
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        w0 = time.time()
         e0.record(stream)
         t_sim, _ = ctx.advance(step_idx, t_sim, -1.0, args.steps)
         e1.record(stream)
         torch.cuda.synchronize()
-    barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1))
-    step_idx += args.steps
-    _, launches = ctx.last_step_stats()
-    value = ws * cells * args.steps / (ms / 1e3)
+        if clk:
+            clk.mark(w0, time.time())
+            clk.__exit__(None, None, None)
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        step_idx += args.steps
+        _, launches = ctx.last_step_stats()
+        out = {"ms": ms, "value": ws * cells * args.steps / (ms / 1e3), "launches": launches,
+               "clocks": clk.summary() if clk else None}
+        if with_clocks:
+            # per-kernel-family device time of two more steps (CUDA events on the launch stream)
+            fam = {}
+            for q in range(2):
+                for k, (fms, cnt) in ctx.profile_step(step_idx + q, t_sim, -1.0).items():
+                    a = fam.setdefault(k, [0.0, 0])
+                    a[0] += fms
+                    a[1] += cnt
+            step_idx += 2
+            out["families"] = fam
+        if with_e2e:
+            # end to end through the drop-in entry point sifv_step (dt back to the host each step)
+            torch.cuda.synchronize()
+            barrier()
+            t0 = time.perf_counter()
+            for q in range(args.steps):
+                t_sim += ctx.step(step_idx + q, t_sim, -1.0)
+            torch.cuda.synchronize()
+            e2e_s = max_over_ranks(time.perf_counter() - t0)
+            out["e2e"] = ws * cells * args.steps / e2e_s
+        ctx.close()
+        return out
 
-    # ---- end-to-end through sifv_step --------------------------------------
-    torch.cuda.synchronize()
-    barrier()
-    t0 = time.perf_counter()
-    for q in range(args.steps):
-        t_sim += ctx.step(step_idx + q, t_sim, -1.0)
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = ws * cells * args.steps / e2e_s
+    main = measure(args.precision, with_clocks=True, with_e2e=True)
+    extra = {}
+    for p in (0, 1, 2):
+        if p != args.precision and not args.quick:
+            extra[PREC_NAMES[p]] = measure(p)
+    ms = main["ms"]
+    value = main["value"]
+    launches = main["launches"]
+    e2e_value = main["e2e"]
+
+    class _Clk:
+        def summary(self):
+            return main["clocks"]
+    clk = _Clk()
 
     peak, peak_kind = _peaks()
-    achieved = BYTES_PER_CELL_UPDATE * cells * args.steps / (ms / 1e3) / 1e9
+    step_achieved = BYTES_PER_CELL_UPDATE * cells * args.steps / (ms / 1e3) / 1e9
+    fam = main["families"]
+    dom = max(fam, key=lambda k: fam[k][0])
+    dom_ms = fam[dom][0] / fam[dom][1]
+    dom_bytes = KERNEL_BYTES_PER_CELL_2D.get(dom, float("nan")) * cells
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     result = None
     if rank == 0:
         kind = "reference" if backends.reference(release=True) is not None else "port"
@@ -231,23 +294,30 @@ def run_cuda(args):
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64" if args.precision != 1 else "f32-bulk/f64-state",
+            "data": "synthetic",
             "config": {"workload": f"2D four-quadrant Riemann {n}x{n} (+3 ghosts), WENO5+HLLC SSP-RK3 CFL0.6, "
-                                   "outflow, FP64, state resident in HBM",
+                                   "outflow, state resident in HBM",
+                       "precision": PREC_NAMES[args.precision],
                        "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (4 x 134 MB state)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
-                         "kernel": "whole RK3 step (256 B algorithmic per cell-update)",
-                         "peak_source": peak_kind},
+                         "kernel": dom, "bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
+                         "peak_source": peak_kind,
+                         "step": {"achieved": step_achieved, "frac": step_achieved / peak,
+                                  "bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
+                         "kernel_ms_per_step": {k: v[0] / 2 for k, v in fam.items()}},
             "cpu_baseline": {"value": cpu, "unit": UNIT, "cores": 1, "kind": kind,
                              "sample": f"{cpu_n}x{cpu_n} instance, {cpu_steps} steps, 1 thread"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
                     "api": "sifv_step (returns dt to the host every step)"},
             "gpu_launches": launches,
             "clocks": clk.summary(),
+            "other_precisions": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
+                                     "roofline_frac": BYTES_PER_CELL_UPDATE * v["value"] / 1e9 / peak}
+                                 for k, v in extra.items()},
         }
         print(json.dumps(result), flush=True)
-    ctx.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
 
@@ -255,10 +325,13 @@ def run_cuda(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--precision", type=int, default=2, choices=[0, 1, 2],
+                    help="0 reference-ordered FP64, 1 mixed (FP32 bulk), 2 fast FP64 (default)")
+    ap.add_argument("--quick", action="store_true", help="skip the other precisions")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

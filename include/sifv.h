@@ -75,8 +75,12 @@ extern "C" {
 #define SIFV_EOS_IDEAL     0
 #define SIFV_EOS_STIFFENED 1
 /* arithmetic of the reconstruction/flux bulk */
-#define SIFV_PREC_FP64  0   /* every operation in FP64 */
-#define SIFV_PREC_MIXED 1   /* FP32 reconstruction/flux bulk; FP64 state, pressure recovery and residuals */
+#define SIFV_PREC_FP64      0   /* FP64 in the reference's operation order: bit-identical results */
+#define SIFV_PREC_MIXED     1   /* FP32 reconstruction/flux bulk; FP64 state, primitive recovery, divergence, RK update */
+#define SIFV_PREC_FP64_FAST 2   /* FP64, fused sweeps with reassociated arithmetic (FMA, shared WENO indicators) */
+/* SIFV_PREC_MIXED and SIFV_PREC_FP64_FAST run the explicit single-phase
+ * WENO5 step (any dim, any Riemann solver, no IGR, no body force); other
+ * configurations are rejected by sifv_create with SIFV_ERR_UNSUPPORTED. */
 
 /* ---- field identifiers (SolutionState members) ------------------------ */
 #define SIFV_F_RHO    0
@@ -219,6 +223,13 @@ int sifv_advective_dt(sifv_ctx_t* ctx, double cfl, double maxDt, double* dt);
 /* Conservative -> primitive on interior cells, and the PRIM ghost fill. */
 int sifv_convert_cons_to_prim(sifv_ctx_t* ctx);
 int sifv_apply_bc(sifv_ctx_t* ctx);
+
+/* One step as sifv_step, with a CUDA event after every kernel family:
+ * per family (in launch order of first appearance) the summed device
+ * milliseconds and the number of launches.  `names` receives the family
+ * names separated by newlines (truncated to namesCap bytes). */
+int sifv_profile_step(sifv_ctx_t* ctx, int step, double time, double targetDt, char* names, int namesCap,
+                      double* ms, int* counts, int maxFamilies, int* nFamilies);
 
 /* Device time of the kernels launched by the last sifv_step / sifv_advance
  * call, and the number of kernel launches it made. */

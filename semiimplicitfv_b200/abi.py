@@ -28,7 +28,7 @@ LF, RUSANOV, HLLC = range(3)
 # BoundaryCondition (include/RectilinearMesh.hpp:14-20)
 BC_SYMMETRY, BC_OUTFLOW, BC_PERIODIC, BC_SLIPWALL, BC_NOSLIPWALL = range(5)
 EOS_IDEAL, EOS_STIFFENED = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP64_FAST = 0, 1, 2
 
 # field identifiers (SolutionState members, include/SolutionState.hpp:73-113)
 F_RHO, F_RHOU, F_RHOV, F_RHOW, F_RHOE = 0, 1, 2, 3, 4
@@ -166,6 +166,8 @@ _OPTIONAL_SIGS = {
     "last_step_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "set_pressure_solver": (C.c_int, [C.c_void_p, C.c_int]),
     "config_validate": (C.c_int, [C.POINTER(Config)]),
+    "profile_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_char_p, C.c_int,
+                               C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
 }
 
 
@@ -291,6 +293,17 @@ class Context:
         ms, n = C.c_double(), C.c_int()
         self._check(self.be.fn["last_step_stats"](self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def profile_step(self, step: int, time: float, target_dt: float = -1.0):
+        """Per-kernel-family device time of one step: {family: (ms, launches)}."""
+        names = C.create_string_buffer(4096)
+        ms = (C.c_double * 64)()
+        cnt = (C.c_int * 64)()
+        n = C.c_int()
+        self._check(self.be.fn["profile_step"](self.h, step, time, target_dt, names, 4096, ms, cnt, 64,
+                                               C.byref(n)))
+        fams = names.value.decode().split("\n") if n.value else []
+        return {f: (ms[k], cnt[k]) for k, f in enumerate(fams)}
 
     def interior(self, arr: np.ndarray) -> np.ndarray:
         """Slice the physical cells out of a (k, j, i) field."""

@@ -14,13 +14,16 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libsifv_b200.so")
-SOURCES = ["sifv_capi.cu", "sifv_noalloc.cu"]
-HEADERS = ["sifv_device.cuh", "sifv_kernels.cuh"]
+# (source, extra flags): the reference-ordered kernels are compiled without
+# FMA contraction; the fused sweep path (sifv_fast.cu) with it.
+SOURCES = [("sifv_capi.cu", ["--fmad=false"]), ("sifv_noalloc.cu", ["--fmad=false"]),
+           ("sifv_fast.cu", ["--fmad=true"])]
+HEADERS = ["sifv_device.cuh", "sifv_common.cuh", "sifv_kernels.cuh", "sifv_sweep.cuh", "sifv_sweep_api.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-lineinfo", "-O3", "-std=c++17", "--fmad=false",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-lineinfo", "-O3", "-std=c++17",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -35,18 +38,32 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "sifv.h")]
+    deps = [os.path.join(CSRC, f) for f, _ in SOURCES] + [os.path.join(CSRC, f) for f in HEADERS] + \
+        [os.path.join(ROOT, "include", "sifv.h"), os.path.abspath(__file__)]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
-    cmd = [_nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           "-o", LIB, *[os.path.join(CSRC, s) for s in SOURCES], "-lcudart"]
+    import concurrent.futures as cf
+    objdir = os.path.join(ROOT, "_build", "csrc")
+    os.makedirs(objdir, exist_ok=True)
+    inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
+    cmds, objs = [], []
+    for src, extra in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        objs.append(obj)
+        cmds.append([_nvcc(), *NVCC_FLAGS, *extra, *inc, "-c", os.path.join(CSRC, src), "-o", obj])
+    with cf.ThreadPoolExecutor(len(cmds)) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd), flush=True)
+        list(ex.map(lambda c: subprocess.run(c, check=True), cmds))
+    link = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs, "-lcudart"]
     if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+        print(" ".join(link), flush=True)
+    subprocess.run(link, check=True)
     return LIB
 
 

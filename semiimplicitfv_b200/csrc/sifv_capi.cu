@@ -12,6 +12,7 @@
 
 #include "sifv.h"
 #include "sifv_kernels.cuh"
+#include "sifv_sweep_api.h"
 
 using namespace sifv;
 
@@ -47,6 +48,13 @@ struct sifv_ctx {
     int W = 5;      // stencil width
     // scratch for the standalone pressure solve with host arrays
     double *sRho = nullptr, *sRhoc2 = nullptr, *sRhs = nullptr, *sP = nullptr;
+    // per-kernel-family timing (sifv_profile_step)
+    bool profiling = false;
+    std::vector<std::pair<std::string, cudaEvent_t>> marks;
+    // fused sweep path (SIFV_PREC_MIXED / SIFV_PREC_FP64_FAST)
+    bool sweep = false;
+    double* rhsBuf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double* invW[3] = {nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -71,6 +79,17 @@ int fail(sifv_ctx* c, int code, const std::string& msg) {
     } while (0)
 
 unsigned blocks(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+// Record an event after a kernel family when profiling.
+void mark(sifv_ctx* c, const char* family) {
+    if (!c->profiling) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, c->stream);
+    c->marks.emplace_back(family, e);
+}
+
+void mark_cb(void* user, const char* family) { mark(static_cast<sifv_ctx*>(user), family); }
 
 // RectilinearMesh::buildExtendedNodes, src/RectilinearMesh.cpp:91-114
 std::vector<double> build_ext(const double* phys, int nCells, int ng) {
@@ -121,7 +140,8 @@ int validate(const sifv_config_t* c, std::string& msg) {
     }
     if (c->nPhases > 0 && c->alphaMin <= 0.0) return bad("multiPhaseParams.alphaMin must be > 0");
     if (c->riemannSolver < SIFV_LF || c->riemannSolver > SIFV_HLLC) return bad("unknown riemannSolver");
-    if (c->precision != SIFV_PREC_FP64 && c->precision != SIFV_PREC_MIXED) return bad("unknown precision");
+    if (c->precision != SIFV_PREC_FP64 && c->precision != SIFV_PREC_MIXED && c->precision != SIFV_PREC_FP64_FAST)
+        return bad("unknown precision");
     return SIFV_OK;
 }
 
@@ -189,6 +209,7 @@ void launch_face_nph(sifv_ctx* c, int dir) {
     }
 #undef FACE_CASE
     c->launches++;
+    mark(c, dir == 0 ? "face_x" : dir == 1 ? "face_y" : "face_z");
 }
 
 void launch_face(sifv_ctx* c, int dir) {
@@ -209,12 +230,14 @@ void launch_prim_bc(sifv_ctx* c, bool interiorOnly = false) {
     NPH_DISPATCH(c, (k_prim_bc<NPHV><<<blocks(n, kCellThreads), kCellThreads, 0, c->stream>>>(
                          c->P, c->F, c->ctl, interiorOnly ? 1 : 0)));
     c->launches++;
+    mark(c, "prim_bc");
 }
 
 void launch_bc_prim(sifv_ctx* c) {
     long long n = (long long)c->ncells;
     NPH_DISPATCH(c, (k_bc_prim<NPHV><<<blocks(n, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, c->F)));
     c->launches++;
+    mark(c, "bc_prim");
 }
 
 void launch_scalar_ghosts(sifv_ctx* c, double* f) {
@@ -241,6 +264,7 @@ int igr_solve(sifv_ctx* c, int step) {
         }
         launch_scalar_ghosts(c, c->F.sigma);
     }
+    mark(c, "igr");
     LAUNCH_CHECK(c);
     return SIFV_OK;
 }
@@ -284,6 +308,7 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
     }
     iters = done ? done : maxIter;
     result = (iters & 1) ? c->F.pB : c->F.pA;
+    mark(c, "jacobi");
     return SIFV_OK;
 }
 
@@ -326,6 +351,7 @@ void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
         k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, cfg.constDt, targetDt, 0, 0.0, 0.0, useEnd ? 1 : 0);
         c->launches += 1;
     }
+    mark(c, "dt");
 }
 
 // One step, everything enqueued on the stream; semi-implicit steps
@@ -336,6 +362,39 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
     status = SIFV_OK;
     enqueue_dt(c, targetDt, useEnd);
     unsigned gc = blocks((long long)c->nint, kCellThreads);
+    if (c->sweep) {
+        SweepArgs A{};
+        A.P = c->P;
+        A.F = c->F;
+        A.ctl = c->ctl;
+        A.C.gamma = c->P.gamma;
+        A.C.pInf = c->P.pInf;
+        A.C.invGm1 = 1.0 / (c->P.gamma - 1.0);
+        A.C.gPinf = c->P.gamma * c->P.pInf;
+        A.eps = cfg.wenoEps;
+        for (int q = 0; q < 5; ++q) A.rhs[q] = c->rhsBuf[q];
+        for (int a = 0; a < 3; ++a) A.inv[a] = c->invW[a];
+        for (int s = 0; s < cfg.RKOrder; ++s) {
+            StageCoef K{};
+            rk_coef(cfg.RKOrder, s, K);
+            A.K.a1 = K.c1 / K.c4;
+            A.K.a2 = K.c2 / K.c4;
+            A.K.a3 = K.c3 / K.c4;
+            A.K.save = (s == 0 && cfg.RKOrder > 1) ? 1 : 0;
+            A.K.useU0 = (K.c2 != 0.0) ? 1 : 0;
+            if (sweep_stage(A, c->stream, cfg.precision == SIFV_PREC_MIXED, c->launches,
+                            c->profiling ? mark_cb : nullptr, c) != 0) {
+                LAUNCH_CHECK(c);
+                return fail(c, SIFV_ERR_CUDA, "sweep launch failed");
+            }
+        }
+        if (sweep_finish_prim(c->P, c->F, c->ctl, c->stream, c->launches) != 0)
+            return fail(c, SIFV_ERR_CUDA, "sweep launch failed");
+        mark(c, "finish_prim");
+        launch_bc_prim(c);
+        LAUNCH_CHECK(c);
+        return SIFV_OK;
+    }
     for (int s = 0; s < cfg.RKOrder; ++s) {
         StageCoef K{};
         rk_coef(cfg.RKOrder, s, K);
@@ -349,13 +408,16 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
         if (!cfg.semiImplicit) {
             NPH_DISPATCH(c, (k_assemble<NPHV, 0><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, K)));
             c->launches++;
+            mark(c, "assemble");
             LAUNCH_CHECK(c);
         } else {
             NPH_DISPATCH(c, (k_assemble<NPHV, 1><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, K)));
             c->launches++;
+            mark(c, "assemble");
             launch_bc_prim(c);
             NPH_DISPATCH(c, (k_pressure_setup<NPHV><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl)));
             c->launches++;
+            mark(c, "pressure_setup");
             LAUNCH_CHECK(c);
             int iters = 0;
             const double* pres = nullptr;
@@ -371,6 +433,7 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
             }
             NPH_DISPATCH(c, (k_correction<NPHV><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, pres, c->ctl)));
             c->launches++;
+            mark(c, "correction");
             launch_bc_prim(c);
             LAUNCH_CHECK(c);
         }
@@ -414,8 +477,14 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     std::string m;
     int st = validate(cfg, m);
     if (st != SIFV_OK) return fail(nullptr, st, m);
-    if (cfg->precision != SIFV_PREC_FP64)
-        return fail(nullptr, SIFV_ERR_UNSUPPORTED, "this build implements precision SIFV_PREC_FP64 only");
+    if (cfg->precision != SIFV_PREC_FP64) {
+        bool bf = false;
+        for (int d = 0; d < 3; ++d) bf = bf || cfg->bfA[d] != 0.0 || cfg->bfB[d] != 0.0;
+        if (cfg->semiImplicit || cfg->nPhases > 0 || cfg->useIGR || cfg->reconOrder != SIFV_WENO5 || bf)
+            return fail(nullptr, SIFV_ERR_UNSUPPORTED,
+                        "SIFV_PREC_MIXED / SIFV_PREC_FP64_FAST run the explicit single-phase WENO5 step without "
+                        "IGR or body force; use SIFV_PREC_FP64 for this configuration");
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(nullptr, SIFV_ERR_NO_DEVICE, "no CUDA device");
@@ -537,6 +606,24 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
             cudaMemcpyAsync(g[q], src[q]->data(), src[q]->size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     }
     F.dx = g[0]; F.dy = g[1]; F.dz = g[2]; F.adx2 = g[3]; F.ady2 = g[4]; F.adz2 = g[5];
+    if (cfg->precision != SIFV_PREC_FP64) {
+        c->sweep = true;
+        c->rhsBuf[0] = dalloc(c, n, st);
+        c->rhsBuf[1] = dalloc(c, n, st);
+        if (dim >= 2) c->rhsBuf[2] = dalloc(c, n, st);
+        if (dim >= 3) c->rhsBuf[3] = dalloc(c, n, st);
+        c->rhsBuf[4] = dalloc(c, n, st);
+        const std::vector<double>* w[3] = {&dxv, &dyv, &dzv};
+        for (int a = 0; a < 3; ++a) {
+            std::vector<double> inv(w[a]->size());
+            for (size_t q = 0; q < inv.size(); ++q) inv[q] = 1.0 / (*w[a])[q];
+            c->invW[a] = dalloc(c, inv.size(), st);
+            if (st == SIFV_OK)
+                cudaMemcpyAsync(c->invW[a], inv.data(), inv.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream);
+        }
+        if (st == SIFV_OK) cudaStreamSynchronize(c->stream);   // host vectors above go out of scope
+    }
     if (st == SIFV_OK) st = ensure_res(c, std::max(cfg->maxPressureIters, 1));
     if (st == SIFV_OK) {
         cudaError_t e = cudaStreamSynchronize(c->stream);
@@ -656,6 +743,53 @@ int sifv_advance(sifv_ctx_t* c, int step0, double time0, double tEnd, int nSteps
     if (timeOut) *timeOut = c->ctlHost->time;
     if (stepsTaken) *stepsTaken = c->ctlHost->stepsTaken;
     return SIFV_OK;
+}
+
+int sifv_profile_step(sifv_ctx_t* c, int step, double time, double targetDt, char* names, int namesCap,
+                      double* ms, int* counts, int maxFamilies, int* nFamilies) {
+    if (!c || !names || !ms || !counts || !nFamilies) return fail(c, SIFV_ERR_BAD_ARG, "null argument");
+    cudaSetDevice(c->device);
+    c->launches = 0;
+    c->marks.clear();
+    c->profiling = true;
+    cudaEvent_t start;
+    cudaEventCreate(&start);
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
+    cudaEventRecord(start, c->stream);
+    int status = SIFV_OK;
+    int st = enqueue_step(c, step, time, targetDt, false, status);
+    c->profiling = false;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    std::vector<std::string> fam;
+    std::vector<double> tot;
+    std::vector<int> cnt;
+    cudaEvent_t prev = start;
+    for (auto& m : c->marks) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, prev, m.second);
+        size_t k = 0;
+        while (k < fam.size() && fam[k] != m.first) ++k;
+        if (k == fam.size()) { fam.push_back(m.first); tot.push_back(0.0); cnt.push_back(0); }
+        tot[k] += t;
+        cnt[k] += 1;
+        prev = m.second;
+    }
+    for (auto& m : c->marks) cudaEventDestroy(m.second);
+    c->marks.clear();
+    cudaEventDestroy(start);
+    if (st != SIFV_OK) return st;
+    if (e != cudaSuccess) return fail(c, SIFV_ERR_CUDA, cudaGetErrorString(e));
+    std::string joined;
+    int n = std::min<int>((int)fam.size(), maxFamilies);
+    for (int k = 0; k < n; ++k) {
+        ms[k] = tot[k];
+        counts[k] = cnt[k];
+        joined += fam[k];
+        if (k + 1 < n) joined += "\n";
+    }
+    std::snprintf(names, (size_t)namesCap, "%s", joined.c_str());
+    *nFamilies = n;
+    return status;
 }
 
 int sifv_last_pressure_iterations(const sifv_ctx_t* c, int* iters) {

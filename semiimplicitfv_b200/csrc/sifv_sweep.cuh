@@ -1,0 +1,477 @@
+// sifv_sweep.cuh -- fused dimension-sweep kernels of the explicit step for
+// the fast-FP64 and mixed-precision paths (T = double or float for the
+// reconstruction / Riemann bulk; state, primitive recovery, flux
+// divergence and the RK update stay FP64).
+//
+// Per RK stage, one kernel per direction:
+//   x sweep  (k_sweep_x): conservative -> primitive (FP64, written back as
+//            the stage's primitive state), WENO5 + Riemann flux along x,
+//            x flux divergence; a warp marches along one row, 32 cells per
+//            step, neighbours exchanged by warp shuffles.
+//   y / z    (k_sweep_line): primitive stencil from the x sweep's output,
+//            flux divergence along y or z; each thread marches along one
+//            line segment keeping a 5-cell register window, lanes are
+//            consecutive x so every load is coalesced.
+// The last direction adds the divergence of the earlier ones and applies
+// the SSP-RK stage update in place (ExplicitSolver::step,
+// src/ExplicitSolver.cpp:127-188); earlier directions write / accumulate
+// the FP64 rhs buffer.
+//
+// Each cell's reconstruction yields both its right-face value (from the
+// left, weno5Left) and its left-face value (from the right, weno5Right)
+// from one set of smoothness indicators: the indicators of the two
+// reconstructions of a 5-cell stencil are the same three numbers in mirror
+// order (src/Reconstruction.cpp:119-168).
+#pragma once
+
+#include "sifv_common.cuh"
+#include "sifv_sweep_api.h"
+
+namespace sifv {
+
+template <typename T>
+struct Prim5 {
+    T rho, u, v, w, p;
+};
+
+template <typename T>
+__device__ __forceinline__ T tmax(T a, T b) { return (a < b) ? b : a; }
+template <typename T>
+__device__ __forceinline__ T tmin(T a, T b) { return (b < a) ? b : a; }
+
+// Both WENO5 face values of the cell whose 5-cell stencil is v0..v4
+// (v2 = the cell): L = value at its right face from the left,
+// R = value at its left face from the right.
+__device__ __forceinline__ void weno5_pair(double v0, double v1, double v2, double v3, double v4, double eps,
+                                           double& L, double& R) {
+    double t0 = v0 - 2.0 * v1 + v2, s0 = v0 - 4.0 * v1 + 3.0 * v2;
+    double t1 = v1 - 2.0 * v2 + v3, s1 = v1 - v3;
+    double t2 = v2 - 2.0 * v3 + v4, s2 = 3.0 * v2 - 4.0 * v3 + v4;
+    double q0 = eps + ((13.0 / 12.0) * t0 * t0 + 0.25 * s0 * s0);
+    double q1 = eps + ((13.0 / 12.0) * t1 * t1 + 0.25 * s1 * s1);
+    double q2 = eps + ((13.0 / 12.0) * t2 * t2 + 0.25 * s2 * s2);
+    q0 *= q0; q1 *= q1; q2 *= q2;
+    // a_k = d_k / q_k; multiplying through by q0 q1 q2 leaves one division per side
+    double m01 = q0 * q1, m02 = q0 * q2, m12 = q1 * q2;
+    double pL0 = (2.0 * v0 - 7.0 * v1 + 11.0 * v2) * (1.0 / 6.0);
+    double pL1 = (-v1 + 5.0 * v2 + 2.0 * v3) * (1.0 / 6.0);
+    double pL2 = (2.0 * v2 + 5.0 * v3 - v4) * (1.0 / 6.0);
+    double pR0 = (2.0 * v4 - 7.0 * v3 + 11.0 * v2) * (1.0 / 6.0);
+    double pR1 = (-v3 + 5.0 * v2 + 2.0 * v1) * (1.0 / 6.0);
+    double pR2 = (2.0 * v2 + 5.0 * v1 - v0) * (1.0 / 6.0);
+    double wL0 = 0.1 * m12, wL1 = 0.6 * m02, wL2 = 0.3 * m01;   // L: d = (.1,.6,.3) on (b0,b1,b2)
+    double wR0 = 0.1 * m01, wR1 = 0.6 * m02, wR2 = 0.3 * m12;   // R: d = (.1,.6,.3) on (b2,b1,b0)
+    L = (wL0 * pL0 + wL1 * pL1 + wL2 * pL2) / (wL0 + wL1 + wL2);
+    R = (wR0 * pR0 + wR1 * pR1 + wR2 * pR2) / (wR0 + wR1 + wR2);
+}
+
+// FP32 version: the product form would overflow single precision for
+// large-valued fields (q ~ (dp^2)^2), so the weights use reciprocals.
+__device__ __forceinline__ void weno5_pair(float v0, float v1, float v2, float v3, float v4, float eps, float& L,
+                                           float& R) {
+    float t0 = v0 - 2.0f * v1 + v2, s0 = v0 - 4.0f * v1 + 3.0f * v2;
+    float t1 = v1 - 2.0f * v2 + v3, s1 = v1 - v3;
+    float t2 = v2 - 2.0f * v3 + v4, s2 = 3.0f * v2 - 4.0f * v3 + v4;
+    float q0 = eps + ((13.0f / 12.0f) * t0 * t0 + 0.25f * s0 * s0);
+    float q1 = eps + ((13.0f / 12.0f) * t1 * t1 + 0.25f * s1 * s1);
+    float q2 = eps + ((13.0f / 12.0f) * t2 * t2 + 0.25f * s2 * s2);
+    float r0 = __frcp_rn(q0 * q0), r1 = __frcp_rn(q1 * q1), r2 = __frcp_rn(q2 * q2);
+    float pL0 = (2.0f * v0 - 7.0f * v1 + 11.0f * v2) * (1.0f / 6.0f);
+    float pL1 = (-v1 + 5.0f * v2 + 2.0f * v3) * (1.0f / 6.0f);
+    float pL2 = (2.0f * v2 + 5.0f * v3 - v4) * (1.0f / 6.0f);
+    float pR0 = (2.0f * v4 - 7.0f * v3 + 11.0f * v2) * (1.0f / 6.0f);
+    float pR1 = (-v3 + 5.0f * v2 + 2.0f * v1) * (1.0f / 6.0f);
+    float pR2 = (2.0f * v2 + 5.0f * v1 - v0) * (1.0f / 6.0f);
+    float aL0 = 0.1f * r0, aL1 = 0.6f * r1, aL2 = 0.3f * r2;
+    float aR0 = 0.1f * r2, aR1 = 0.6f * r1, aR2 = 0.3f * r0;
+    L = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) * __frcp_rn(aL0 + aL1 + aL2);
+    R = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) * __frcp_rn(aR0 + aR1 + aR2);
+}
+
+template <typename T>
+__device__ __forceinline__ T trcp(T x);
+template <>
+__device__ __forceinline__ double trcp<double>(double x) { return 1.0 / x; }
+template <>
+__device__ __forceinline__ float trcp<float>(float x) { return __frcp_rn(x); }
+
+template <typename T>
+struct Flux4 {
+    T mass, m0, m1, m2, energy;
+};
+
+// Single-phase face flux on the normal axis D: HLLC (src/HLLCSolver.cpp:7-161)
+// with the reciprocals shared, Rusanov (src/RusanovSolver.cpp:7-83) or LF
+// (src/LFSolver.cpp:8-75), with pressure (explicit step).
+template <int D, int DIM, typename T>
+__device__ __forceinline__ void face_flux(int riemann, const FluxConsts& C, const Prim5<T>& L, const Prim5<T>& R,
+                                          Flux4<T>& F) {
+    const T g = (T)C.gamma, pinf = (T)C.pInf, invGm1 = (T)C.invGm1, gPinf = (T)C.gPinf;
+    const T tiny = (T)1e-14;
+    T uL[3] = {L.u, L.v, L.w}, uR[3] = {R.u, R.v, R.w};
+    T unL = uL[D], unR = uR[D];
+    T q2L = L.u * L.u, q2R = R.u * R.u;
+    if (DIM >= 2) { q2L += L.v * L.v; q2R += R.v * R.v; }
+    if (DIM >= 3) { q2L += L.w * L.w; q2R += R.w * R.w; }
+    T rhoEL = (L.p + gPinf) * invGm1 + (T)0.5 * L.rho * q2L;
+    T rhoER = (R.p + gPinf) * invGm1 + (T)0.5 * R.rho * q2R;
+    T irL = trcp(tmax(L.rho, tiny)), irR = trcp(tmax(R.rho, tiny));
+    T cL = sqrt(g * tmax(L.p + pinf, tiny) * irL), cR = sqrt(g * tmax(R.p + pinf, tiny) * irR);
+    if (riemann == SIFV_HLLC) {
+        T sL = tmin(unL - cL, unR - cR);
+        T sR = tmax(unL + cL, unR + cR);
+        T aL = L.rho * (sL - unL), aR = R.rho * (sR - unR);
+        T sStar = (R.p - L.p + aL * unL - aR * unR) / (aL - aR);
+        if (sL >= (T)0) {
+            F.mass = L.rho * unL;
+            F.m0 = F.mass * L.u; F.m1 = F.mass * L.v; F.m2 = F.mass * L.w;
+            F.energy = (rhoEL + L.p) * unL;
+            if (D == 0) F.m0 += L.p; else if (D == 1) F.m1 += L.p; else F.m2 += L.p;
+        } else if (sR <= (T)0) {
+            F.mass = R.rho * unR;
+            F.m0 = F.mass * R.u; F.m1 = F.mass * R.v; F.m2 = F.mass * R.w;
+            F.energy = (rhoER + R.p) * unR;
+            if (D == 0) F.m0 += R.p; else if (D == 1) F.m1 += R.p; else F.m2 += R.p;
+        } else {
+            const bool left = sStar >= (T)0;
+            const Prim5<T>& W = left ? L : R;
+            T s = left ? sL : sR, un = left ? unL : unR, rhoE = left ? rhoEL : rhoER, a = left ? aL : aR;
+            T ir = left ? irL : irR;
+            T inv = trcp(s - sStar);
+            T rhoStar = a * inv;                    // rho (s - u) / (s - s*)
+            T fm = W.rho * un;
+            F.mass = fm + s * (rhoStar - W.rho);
+            T du = sStar - un;
+            T w0 = W.u, w1 = W.v, w2 = W.w;
+            T ws[3] = {w0, w1, w2};
+            ws[D] += du;
+            F.m0 = fm * w0 + s * (rhoStar * ws[0] - W.rho * w0);
+            F.m1 = fm * w1 + s * (rhoStar * ws[1] - W.rho * w1);
+            F.m2 = fm * w2 + s * (rhoStar * ws[2] - W.rho * w2);
+            if (D == 0) F.m0 += W.p; else if (D == 1) F.m1 += W.p; else F.m2 += W.p;
+            T e = rhoE * ir;                         // rhoE / rho
+            T EStar = rhoStar * (e + du * (sStar + W.p * trcp(a)));
+            F.energy = (rhoE + W.p) * un + s * (EStar - rhoE);
+        }
+    } else {
+        T sMax;
+        if (riemann == SIFV_RUSANOV) {
+            sMax = tmax(fabs(unL) + cL, fabs(unR) + cR);
+        } else {
+            T sL2 = sqrt(q2L), sR2 = sqrt(q2R);
+            sMax = tmax(sL2, sR2) + tmax(cL, cR);
+        }
+        T fmL = L.rho * unL, fmR = R.rho * unR;
+        T h = (T)0.5, hs = (T)0.5 * sMax;
+        F.mass = h * (fmL + fmR) - hs * (R.rho - L.rho);
+        F.m0 = h * (fmL * L.u + fmR * R.u) - hs * (R.rho * R.u - L.rho * L.u);
+        F.m1 = h * (fmL * L.v + fmR * R.v) - hs * (R.rho * R.v - L.rho * L.v);
+        F.m2 = h * (fmL * L.w + fmR * R.w) - hs * (R.rho * R.w - L.rho * L.w);
+        T pm = h * (L.p + R.p);
+        if (D == 0) F.m0 += pm; else if (D == 1) F.m1 += pm; else F.m2 += pm;
+        F.energy = h * ((rhoEL + L.p) * unL + (rhoER + R.p) * unR) - hs * (rhoER - rhoEL);
+    }
+}
+
+// Conservative -> primitive of one cell in FP64 with velocity signs of its
+// ghost mapping (1 for interior cells).
+__device__ __forceinline__ Prim5<double> load_cons_prim(const Params& P, const Fields& F, size_t src,
+                                                        const double sg[3]) {
+    double rho, u[3], p;
+    cons_to_prim_cell<0>(P, F, src, rho, u, p);
+    Prim5<double> r;
+    r.rho = rho;
+    r.u = sg[0] * u[0];
+    r.v = sg[1] * u[1];
+    r.w = sg[2] * u[2];
+    r.p = p;
+    return r;
+}
+
+template <int DIM>
+__device__ __forceinline__ Prim5<double> load_prim(const Fields& F, size_t src, const double sg[3]) {
+    Prim5<double> r;
+    r.rho = F.rho[src];
+    r.u = sg[0] * F.velU[src];
+    r.v = (DIM >= 2) ? sg[1] * F.velV[src] : 0.0;
+    r.w = (DIM >= 3) ? sg[2] * F.velW[src] : 0.0;
+    r.p = F.pres[src];
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ Prim5<T> to_t(const Prim5<double>& a) {
+    return Prim5<T>{(T)a.rho, (T)a.u, (T)a.v, (T)a.w, (T)a.p};
+}
+
+template <int DIM, typename T>
+__device__ __forceinline__ void recon_cell(const Prim5<T>& a, const Prim5<T>& b, const Prim5<T>& c,
+                                           const Prim5<T>& d, const Prim5<T>& e, T eps, Prim5<T>& L, Prim5<T>& R) {
+    weno5_pair(a.rho, b.rho, c.rho, d.rho, e.rho, eps, L.rho, R.rho);
+    weno5_pair(a.u, b.u, c.u, d.u, e.u, eps, L.u, R.u);
+    if (DIM >= 2) weno5_pair(a.v, b.v, c.v, d.v, e.v, eps, L.v, R.v);
+    else { L.v = R.v = (T)0; }
+    if (DIM >= 3) weno5_pair(a.w, b.w, c.w, d.w, e.w, eps, L.w, R.w);
+    else { L.w = R.w = (T)0; }
+    weno5_pair(a.p, b.p, c.p, d.p, e.p, eps, L.p, R.p);
+}
+
+template <int DIM>
+__device__ __forceinline__ void rk_apply(const Fields& F, size_t c, const RKUpdate& K, double dt, double rR,
+                                         double rU, double rV, double rW, double rE) {
+    const double a3 = K.a3 * dt;
+    double r = F.rho[c], ru = F.rhoU[c], re = F.rhoE[c];
+    double rv = (DIM >= 2) ? F.rhoV[c] : 0.0, rw = (DIM >= 3) ? F.rhoW[c] : 0.0;
+    if (K.save) {
+        F.rho0[c] = r; F.rhoU0[c] = ru; F.rhoE0[c] = re;
+        if (DIM >= 2) F.rhoV0[c] = rv;
+        if (DIM >= 3) F.rhoW0[c] = rw;
+        F.pres0[c] = F.pres[c];
+    }
+    double nr = K.a1 * r + a3 * rR, nu = K.a1 * ru + a3 * rU, ne = K.a1 * re + a3 * rE;
+    double nv = K.a1 * rv + a3 * rV, nw = K.a1 * rw + a3 * rW;
+    if (K.useU0) {
+        nr += K.a2 * F.rho0[c]; nu += K.a2 * F.rhoU0[c]; ne += K.a2 * F.rhoE0[c];
+        if (DIM >= 2) nv += K.a2 * F.rhoV0[c];
+        if (DIM >= 3) nw += K.a2 * F.rhoW0[c];
+    }
+    F.rho[c] = nr; F.rhoU[c] = nu; F.rhoE[c] = ne;
+    if (DIM >= 2) F.rhoV[c] = nv;
+    if (DIM >= 3) F.rhoW[c] = nw;
+}
+
+// x sweep: one warp per row; lane l handles position q = 32 t - 1 + l at
+// step t, q in [-1, nx] (the cells whose face values are needed).  Writes
+// the stage's primitive state and the x flux divergence (rhs buffer); it
+// never updates the conservative state, so periodic ghosts read at the end
+// of a row still see the stage-start values.
+template <int DIM, typename T>
+__global__ void __launch_bounds__(128) k_sweep_x(SweepArgs A) {
+    const Params& P = A.P;
+    const Fields& F = A.F;
+    if (A.ctl->skip) return;
+    const int lane = threadIdx.x & 31;
+    const long long row = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= (long long)P.ny * P.nz) return;
+    const int j = (int)(row % P.ny), k = (int)(row / P.ny);
+    const size_t rowBase = cidx(P, 0, j, k);   // cell (0, j, k)
+    const T eps = (T)A.eps;
+    const int nx = P.nx;
+
+    // load the primitive state of position q (ghosts via the x ghost map), FP64
+    auto loadq = [&](int q, Prim5<double>& out) {
+        if (q < -P.ngx || q >= nx + P.ngx) {
+            out = Prim5<double>{0.0, 0.0, 0.0, 0.0, 0.0};
+            return;
+        }
+        double sn, sa;
+        int s = prim_src(q, nx, P.bc[0], P.bc[1], sn, sa);
+        double sg[3] = {1.0, 1.0, 1.0};
+        if (s != q) { sg[0] = sn * sa; sg[1] = sa; sg[2] = sa; }
+        out = load_cons_prim(P, F, rowBase + (size_t)s, sg);
+    };
+
+    const int nsteps = (nx + 2 + 31) / 32;
+    Prim5<double> prevD, curD, nextD;
+    loadq(-33 + lane, prevD);
+    loadq(-1 + lane, curD);
+    loadq(31 + lane, nextD);
+    Prim5<T> prev = to_t<T>(prevD), cur = to_t<T>(curD), next = to_t<T>(nextD);
+    Prim5<T> Lprev31;                 // L of position q - 1 for lane 0 (previous step's lane 31)
+    Flux4<T> Fprev31;                 // flux of face q - 1 for lane 0
+    Lprev31 = Prim5<T>{(T)0, (T)0, (T)0, (T)0, (T)0};
+    Fprev31 = Flux4<T>{(T)0, (T)0, (T)0, (T)0, (T)0};
+    for (int t = 0; t < nsteps; ++t) {
+        const int q = 32 * t - 1 + lane;
+        // stage primitive write-back of the cells this lane holds (FIRST sweep)
+        if (q >= 0 && q < nx) {
+            size_t c = rowBase + q;
+            F.velU[c] = curD.u;
+            if (DIM >= 2) F.velV[c] = curD.v;
+            if (DIM >= 3) F.velW[c] = curD.w;
+            F.pres[c] = curD.p;
+        }
+        // stencil q-2 .. q+2
+        Prim5<T> sm2, sm1, sp1, sp2;
+#define SHUF_FIELD(fld)                                                                      \
+        {                                                                                    \
+            T a2 = __shfl_sync(0xffffffffu, cur.fld, (lane + 30) & 31);                       \
+            T b2 = __shfl_sync(0xffffffffu, prev.fld, (lane + 30) & 31);                      \
+            sm2.fld = (lane >= 2) ? a2 : b2;                                                 \
+            T a1 = __shfl_sync(0xffffffffu, cur.fld, (lane + 31) & 31);                       \
+            T b1 = __shfl_sync(0xffffffffu, prev.fld, (lane + 31) & 31);                      \
+            sm1.fld = (lane >= 1) ? a1 : b1;                                                 \
+            T c1 = __shfl_sync(0xffffffffu, cur.fld, (lane + 1) & 31);                        \
+            T d1 = __shfl_sync(0xffffffffu, next.fld, (lane + 1) & 31);                       \
+            sp1.fld = (lane <= 30) ? c1 : d1;                                                \
+            T c2 = __shfl_sync(0xffffffffu, cur.fld, (lane + 2) & 31);                        \
+            T d2 = __shfl_sync(0xffffffffu, next.fld, (lane + 2) & 31);                       \
+            sp2.fld = (lane <= 29) ? c2 : d2;                                                \
+        }
+        SHUF_FIELD(rho)
+        SHUF_FIELD(u)
+        if (DIM >= 2) SHUF_FIELD(v)
+        if (DIM >= 3) SHUF_FIELD(w)
+        SHUF_FIELD(p)
+#undef SHUF_FIELD
+        if (DIM < 2) { sm2.v = sm1.v = sp1.v = sp2.v = (T)0; }
+        if (DIM < 3) { sm2.w = sm1.w = sp1.w = sp2.w = (T)0; }
+        Prim5<T> L, R;
+        recon_cell<DIM, T>(sm2, sm1, cur, sp1, sp2, eps, L, R);
+        // face q: left state L(q-1), right state R(q)
+        Prim5<T> Lm;
+        Lm.rho = __shfl_sync(0xffffffffu, L.rho, (lane + 31) & 31);
+        Lm.u = __shfl_sync(0xffffffffu, L.u, (lane + 31) & 31);
+        Lm.v = __shfl_sync(0xffffffffu, L.v, (lane + 31) & 31);
+        Lm.w = __shfl_sync(0xffffffffu, L.w, (lane + 31) & 31);
+        Lm.p = __shfl_sync(0xffffffffu, L.p, (lane + 31) & 31);
+        if (lane == 0) Lm = Lprev31;
+        Flux4<T> Fq;
+        face_flux<0, DIM, T>(P.riemann, A.C, Lm, R, Fq);
+        // divergence of cell q-1: faces q-1 and q
+        Flux4<T> Fm;
+        Fm.mass = __shfl_sync(0xffffffffu, Fq.mass, (lane + 31) & 31);
+        Fm.m0 = __shfl_sync(0xffffffffu, Fq.m0, (lane + 31) & 31);
+        Fm.m1 = __shfl_sync(0xffffffffu, Fq.m1, (lane + 31) & 31);
+        Fm.m2 = __shfl_sync(0xffffffffu, Fq.m2, (lane + 31) & 31);
+        Fm.energy = __shfl_sync(0xffffffffu, Fq.energy, (lane + 31) & 31);
+        if (lane == 0) Fm = Fprev31;
+        const int cq = q - 1;
+        if (cq >= 0 && cq < nx) {
+            size_t c = rowBase + cq;
+            double ci = A.inv[0][cq + P.ngx];
+            double rR = ci * ((double)Fm.mass - (double)Fq.mass);
+            double rU = ci * ((double)Fm.m0 - (double)Fq.m0);
+            double rV = ci * ((double)Fm.m1 - (double)Fq.m1);
+            double rW = ci * ((double)Fm.m2 - (double)Fq.m2);
+            double rE = ci * ((double)Fm.energy - (double)Fq.energy);
+            A.rhs[0][c] = rR;
+            A.rhs[1][c] = rU;
+            if (DIM >= 2) A.rhs[2][c] = rV;
+            if (DIM >= 3) A.rhs[3][c] = rW;
+            A.rhs[4][c] = rE;
+        }
+        // carry lane 31's L and flux to the next step's lane 0
+        Lprev31.rho = __shfl_sync(0xffffffffu, L.rho, 31);
+        Lprev31.u = __shfl_sync(0xffffffffu, L.u, 31);
+        Lprev31.v = __shfl_sync(0xffffffffu, L.v, 31);
+        Lprev31.w = __shfl_sync(0xffffffffu, L.w, 31);
+        Lprev31.p = __shfl_sync(0xffffffffu, L.p, 31);
+        Fprev31.mass = __shfl_sync(0xffffffffu, Fq.mass, 31);
+        Fprev31.m0 = __shfl_sync(0xffffffffu, Fq.m0, 31);
+        Fprev31.m1 = __shfl_sync(0xffffffffu, Fq.m1, 31);
+        Fprev31.m2 = __shfl_sync(0xffffffffu, Fq.m2, 31);
+        Fprev31.energy = __shfl_sync(0xffffffffu, Fq.energy, 31);
+        // advance the window by 32 positions
+        prev = cur;
+        cur = next;
+        curD = nextD;
+        loadq(32 * (t + 2) - 1 + lane, nextD);
+        next = to_t<T>(nextD);
+    }
+}
+
+// y or z sweep: each thread marches along one line segment [s0, s0 + seg)
+// of axis DIR at fixed x = i (consecutive lanes, coalesced) keeping the
+// 5-cell window of positions q-2 .. q+2 in registers.
+template <int DIR, int DIM, typename T, bool LAST>
+__global__ void __launch_bounds__(128) k_sweep_line(SweepArgs A) {
+    const Params& P = A.P;
+    const Fields& F = A.F;
+    if (A.ctl->skip) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.nx) return;
+    const int nLine = (DIR == 1) ? P.ny : P.nz;
+    const int other = blockIdx.z;   // k for DIR == 1, j for DIR == 2
+    const int s0 = blockIdx.y * A.seg;
+    if (s0 >= nLine) return;
+    const int s1 = min(s0 + A.seg, nLine);
+    const long st = (DIR == 1) ? (long)P.nxT : (long)P.nxT * P.nyT;
+    const size_t lineBase = (DIR == 1) ? cidx(P, i, 0, other) : cidx(P, i, other, 0);
+    const int ng = (DIR == 1) ? P.ngy : P.ngz;
+    const int bcLo = P.bc[2 * DIR], bcHi = P.bc[2 * DIR + 1];
+    const T eps = (T)A.eps;
+
+    auto loadq = [&](int q) -> Prim5<T> {
+        if (q < -ng || q >= nLine + ng) return Prim5<T>{(T)0, (T)0, (T)0, (T)0, (T)0};
+        double sn, sa;
+        int s = prim_src(q, nLine, bcLo, bcHi, sn, sa);
+        double sg[3] = {1.0, 1.0, 1.0};
+        if (s != q) { sg[0] = sa; sg[1] = sa; sg[2] = sa; sg[DIR] = sn * sa; }
+        return to_t<T>(load_prim<DIM>(F, lineBase + (long)s * st, sg));
+    };
+
+    Prim5<T> w0 = loadq(s0 - 3), w1 = loadq(s0 - 2), w2 = loadq(s0 - 1), w3 = loadq(s0), w4 = loadq(s0 + 1);
+    Prim5<T> Lm;
+    Flux4<T> Fm;
+    // position s0 - 1: only its right-face value is needed
+    {
+        Prim5<T> R;
+        recon_cell<DIM, T>(w0, w1, w2, w3, w4, eps, Lm, R);
+    }
+    for (int q = s0; q <= s1; ++q) {
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4;
+        w4 = loadq(q + 2);
+        Prim5<T> L, R;
+        recon_cell<DIM, T>(w0, w1, w2, w3, w4, eps, L, R);
+        Flux4<T> Fq;
+        face_flux<DIR, DIM, T>(P.riemann, A.C, Lm, R, Fq);
+        if (q > s0) {
+            const int cq = q - 1;
+            const size_t c = lineBase + (long)cq * st;
+            double ci = A.inv[DIR][cq + ng];
+            double rR = ci * ((double)Fm.mass - (double)Fq.mass);
+            double rU = ci * ((double)Fm.m0 - (double)Fq.m0);
+            double rV = ci * ((double)Fm.m1 - (double)Fq.m1);
+            double rW = ci * ((double)Fm.m2 - (double)Fq.m2);
+            double rE = ci * ((double)Fm.energy - (double)Fq.energy);
+            rR += A.rhs[0][c];
+            rU += A.rhs[1][c];
+            if (DIM >= 2) rV += A.rhs[2][c];
+            if (DIM >= 3) rW += A.rhs[3][c];
+            rE += A.rhs[4][c];
+            if (LAST) {
+                rk_apply<DIM>(F, c, A.K, A.ctl->dt, rR, rU, rV, rW, rE);
+            } else {
+                A.rhs[0][c] = rR;
+                A.rhs[1][c] = rU;
+                if (DIM >= 2) A.rhs[2][c] = rV;
+                if (DIM >= 3) A.rhs[3][c] = rW;
+                A.rhs[4][c] = rE;
+            }
+        }
+        Lm = L;
+        Fm = Fq;
+    }
+}
+
+// Stage update from the complete rhs buffer (1D, where the x sweep is the
+// only direction).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_rk_update(SweepArgs A) {
+    if (A.ctl->skip) return;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(A.P, t, i, j, k)) return;
+    size_t c = cidx(A.P, i, j, k);
+    rk_apply<DIM>(A.F, c, A.K, A.ctl->dt, A.rhs[0][c], A.rhs[1][c], (DIM >= 2) ? A.rhs[2][c] : 0.0,
+                  (DIM >= 3) ? A.rhs[3][c] : 0.0, A.rhs[4][c]);
+}
+
+// End of step: primitive state of the updated cells (interior), as the
+// reference's final convertConservativeToPrimitiveVariables.
+__global__ void __launch_bounds__(256) k_cons_to_prim_interior(Params P, Fields F, const Ctl* ctl) {
+    if (ctl->skip) return;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(P, t, i, j, k)) return;
+    size_t c = cidx(P, i, j, k);
+    double rho, u[3], p;
+    cons_to_prim_cell<0>(P, F, c, rho, u, p);
+    F.velU[c] = u[0];
+    if (P.dim >= 2) F.velV[c] = u[1];
+    if (P.dim >= 3) F.velW[c] = u[2];
+    F.pres[c] = p;
+}
+
+}  // namespace sifv

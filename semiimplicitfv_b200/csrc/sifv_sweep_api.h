@@ -1,0 +1,50 @@
+// sifv_sweep_api.h -- host entry points and argument block of the fused
+// sweep path, shared by the C ABI translation unit and the sweep
+// translation unit.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sifv_device.cuh"
+
+namespace sifv {
+
+// EOS constants of the single-phase face flux.
+struct FluxConsts {
+    double gamma, pInf, invGm1, gPinf;
+};
+
+// Stage update of one interior cell from its complete flux divergence
+// (src/ExplicitSolver.cpp:127-188) as U = a1 U + a2 U0 + a3 dt R with
+// (a1, a2, a3) = (c1, c2, c3) / c4; dt is read from device memory.
+struct RKUpdate {
+    double a1, a2, a3;
+    int save;     // stage 0 of a multi-stage scheme: back up U into U0
+    int useU0;
+};
+
+struct SweepArgs {
+    Params P;
+    Fields F;
+    const Ctl* ctl;
+    FluxConsts C;
+    RKUpdate K;
+    double eps;
+    int seg;       // cells per thread segment (line sweeps)
+    double* rhs[5];  // FP64 rhs buffer (rho, rhoU, rhoV, rhoW, rhoE)
+    const double* inv[3];   // 1 / d per cell (ghosts included)
+};
+
+// Called after each kernel launch with the kernel family's name (per-kernel
+// timing); may be null.
+typedef void (*LaunchMark)(void* user, const char* family);
+
+// One RK stage of the explicit step on the fused sweep kernels
+// (mixed: FP32 reconstruction / Riemann bulk).  Returns 0 on success.
+int sweep_stage(SweepArgs A, cudaStream_t s, bool mixed, int& launches, LaunchMark mark = nullptr,
+                void* user = nullptr);
+
+// End-of-step conservative -> primitive on interior cells.
+int sweep_finish_prim(const Params& P, const Fields& F, const Ctl* ctl, cudaStream_t s, int& launches);
+
+}  // namespace sifv

@@ -1,0 +1,143 @@
+"""The fused-sweep paths on the GPU.
+
+SIFV_PREC_FP64_FAST is FP64 with reassociated arithmetic: it must stay
+within 1e-10 relative L-infinity per conserved variable of the
+reference-ordered path (itself bit-identical to the reference), also over
+long runs.  SIFV_PREC_MIXED runs the reconstruction / Riemann bulk in FP32:
+it is judged by its L1 error against the exact solution (Sod) and against
+the FP64 discretisation error."""
+import numpy as np
+import pytest
+
+import backends
+import cases
+import exact_riemann
+from semiimplicitfv_b200 import abi
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+CONS = (abi.F_RHO, abi.F_RHOU, abi.F_RHOE)
+
+
+def _run(case, precision, nsteps, t_end=None, backend=None):
+    case[0].precision = precision
+    c = backends.make(backend or backends.cuda(), case)
+    t, s, dts = cases.run_steps(c, nsteps, t_end)
+    return c, dts
+
+
+def _cons(cfg):
+    f = list(CONS)
+    if cfg.dim >= 2:
+        f.append(abi.F_RHOV)
+    if cfg.dim >= 3:
+        f.append(abi.F_RHOW)
+    return f
+
+
+def _max_rel(ca, cb, cfg):
+    worst = 0.0
+    for fid in _cons(cfg):
+        a, b = ca.interior(ca.get_field(fid)), cb.interior(cb.get_field(fid))
+        worst = max(worst, np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    return worst
+
+
+def test_fast_sod_full_config_vs_oracle():
+    cf, dtf = _run(cases.sod(1000), abi.PREC_FP64_FAST, 10 ** 6, 0.2)
+    co, dto = _run(cases.sod(1000), abi.PREC_FP64, 10 ** 6, 0.2, backends.oracle())
+    assert len(dtf) == len(dto)
+    assert _max_rel(cf, co, cf.cfg) <= TOL
+
+
+@pytest.mark.parametrize("bc", [abi.BC_OUTFLOW, abi.BC_PERIODIC, abi.BC_SLIPWALL, abi.BC_NOSLIPWALL,
+                                abi.BC_SYMMETRY])
+@pytest.mark.parametrize("riemann", [abi.HLLC, abi.RUSANOV, abi.LF])
+def test_fast_riemann2d(bc, riemann):
+    cf, _ = _run(cases.riemann2d(48, bc=bc, riemann=riemann), abi.PREC_FP64_FAST, 20)
+    co, _ = _run(cases.riemann2d(48, bc=bc, riemann=riemann), abi.PREC_FP64, 20, backend=backends.oracle())
+    assert _max_rel(cf, co, cf.cfg) <= TOL
+
+
+def test_fast_riemann2d_long_run_stays_within_tolerance():
+    """256^2 to t = 0.8 (the benchmark problem's full time at reduced size):
+    round-off differences must not grow past the parity bar."""
+    cf, dtf = _run(cases.riemann2d(256), abi.PREC_FP64_FAST, 10 ** 6, 0.8)
+    ce, dte = _run(cases.riemann2d(256), abi.PREC_FP64, 10 ** 6, 0.8)
+    assert len(dtf) == len(dte)
+    rel = _max_rel(cf, ce, cf.cfg)
+    assert rel <= TOL, rel
+
+
+def test_fast_3d_explicit():
+    case = lambda: cases.acoustic3d(16, semi=False, igr=False, rk=3)
+    cf, _ = _run(case(), abi.PREC_FP64_FAST, 6)
+    co, _ = _run(case(), abi.PREC_FP64, 6, backend=backends.oracle())
+    assert _max_rel(cf, co, cf.cfg) <= TOL
+
+
+def test_fast_stiffened_and_rk2():
+    def case():
+        c = cases.riemann2d(32, rk=2)
+        c[0].eosKind = abi.EOS_STIFFENED
+        c[0].pInf = 0.3
+        return c
+    cf, _ = _run(case(), abi.PREC_FP64_FAST, 10)
+    co, _ = _run(case(), abi.PREC_FP64, 10, backend=backends.oracle())
+    assert _max_rel(cf, co, cf.cfg) <= TOL
+
+
+def test_fast_advance_matches_step():
+    case = cases.riemann2d(64)
+    case[0].precision = abi.PREC_FP64_FAST
+    c1 = backends.make(backends.cuda(), case)
+    c2 = backends.make(backends.cuda(), case)
+    t1, s1, _ = cases.run_steps(c1, 9, t_end=0.05)
+    t2, s2 = c2.advance(0, 0.0, 0.05, 9)
+    assert (t1, s1) == (t2, s2)
+    for fid in _cons(case[0]):
+        assert np.array_equal(c1.get_field(fid), c2.get_field(fid))
+
+
+def test_unsupported_configs_rejected():
+    case = cases.water_air(32)
+    case[0].precision = abi.PREC_MIXED
+    with pytest.raises(abi.AbiError) as e:
+        backends.cuda().create(case[0], case[1])
+    assert e.value.status == abi.ERR_UNSUPPORTED
+
+
+def _sod_l1(precision, n):
+    case = cases.sod(n)
+    c, _ = _run(case, precision, 10 ** 6, 0.2)
+    x = 0.5 * (case[1].x[:-1] + case[1].x[1:])
+    rho_e, _, _ = exact_riemann.sod_exact(x, 0.2)
+    return np.abs(c.interior(c.get_field(abi.F_RHO)).ravel() - rho_e).mean()
+
+
+@pytest.mark.parametrize("n", [1000, 4000])
+def test_mixed_sod_error_within_bound(n):
+    """Mixed-precision L1 error against the exact solution within 1.5x of the
+    FP64 discretisation error."""
+    e64 = _sod_l1(abi.PREC_FP64, n)
+    emx = _sod_l1(abi.PREC_MIXED, n)
+    assert emx <= 1.5 * e64, (emx, e64)
+
+
+def test_mixed_riemann2d_error_within_bound():
+    """2D Riemann 256^2 to t = 0.25: the mixed-vs-FP64 difference is well
+    below the FP64 discretisation error (FP64 256^2 vs FP64 512^2 averaged
+    onto 256^2)."""
+    t_end = 0.25
+    c64, _ = _run(cases.riemann2d(256), abi.PREC_FP64_FAST, 10 ** 6, t_end)
+    cmx, _ = _run(cases.riemann2d(256), abi.PREC_MIXED, 10 ** 6, t_end)
+    cfine, _ = _run(cases.riemann2d(512), abi.PREC_FP64_FAST, 10 ** 6, t_end)
+    r64 = c64.interior(c64.get_field(abi.F_RHO))[0]
+    rmx = cmx.interior(cmx.get_field(abi.F_RHO))[0]
+    rf = cfine.interior(cfine.get_field(abi.F_RHO))[0]
+    rf = 0.25 * (rf[0::2, 0::2] + rf[1::2, 0::2] + rf[0::2, 1::2] + rf[1::2, 1::2])
+    disc = np.abs(r64 - rf).mean()
+    mixed_vs_fp64 = np.abs(rmx - r64).mean()
+    err_mx = np.abs(rmx - rf).mean()
+    assert err_mx <= 1.5 * disc, (err_mx, disc)
+    assert mixed_vs_fp64 < 0.1 * disc, (mixed_vs_fp64, disc)
