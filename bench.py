@@ -35,13 +35,13 @@ UNIT = "cell-updates/s"
 BYTES_PER_CELL_UPDATE = 256   # algorithmic: 64 B x 4 conserved variables per RK3 step
 # Algorithmic bytes per cell of one launch of each kernel family of the 2D
 # fused-sweep step (FP64 arrays, 8 B per value):
-#   sweep_x  reads rho, rhoU, rhoV, rhoE; writes velU, velV, pres and the
-#            4-array rhs                                        11 x 8 = 88
+#   sweep_x  reads rho, rhoU, rhoV, rhoE; writes the stage density copy,
+#            velU, velV, pres and the 4-array rhs              12 x 8 = 96
 #   sweep_y  reads rho, velU, velV, pres, 4 rhs, 4 U and 4 U0 (stage 0:
 #            pres and U, writes U0 + pres0); writes 4 U     avg 20.67 x 8 = 165.3
 #   dt       reads rho, velU, velV, pres                         4 x 8 = 32
 #   finish_prim reads 4 U, writes velU, velV, pres              7 x 8 = 56
-KERNEL_BYTES_PER_CELL_2D = {"sweep_x": 88.0, "sweep_y": 165.33, "dt": 32.0, "finish_prim": 56.0,
+KERNEL_BYTES_PER_CELL_2D = {"sweep_x": 96.0, "sweep_y": 165.33, "dt": 32.0, "finish_prim": 56.0,
                             "face_x": 64.0, "face_y": 64.0, "assemble": 229.3, "prim_bc": 56.0}
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 

@@ -55,6 +55,7 @@ struct sifv_ctx {
     bool sweep = false;
     double* rhsBuf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* invW[3] = {nullptr, nullptr, nullptr};
+    double* rhoP = nullptr;
 };
 
 namespace {
@@ -373,6 +374,7 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
         A.C.gPinf = c->P.gamma * c->P.pInf;
         A.eps = cfg.wenoEps;
         for (int q = 0; q < 5; ++q) A.rhs[q] = c->rhsBuf[q];
+        A.rhoP = c->rhoP;
         for (int a = 0; a < 3; ++a) A.inv[a] = c->invW[a];
         for (int s = 0; s < cfg.RKOrder; ++s) {
             StageCoef K{};
@@ -608,6 +610,7 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     F.dx = g[0]; F.dy = g[1]; F.dz = g[2]; F.adx2 = g[3]; F.ady2 = g[4]; F.adz2 = g[5];
     if (cfg->precision != SIFV_PREC_FP64) {
         c->sweep = true;
+        c->rhoP = dalloc(c, n, st);
         c->rhsBuf[0] = dalloc(c, n, st);
         c->rhsBuf[1] = dalloc(c, n, st);
         if (dim >= 2) c->rhsBuf[2] = dalloc(c, n, st);

@@ -189,9 +189,10 @@ __device__ __forceinline__ Prim5<double> load_cons_prim(const Params& P, const F
 }
 
 template <int DIM>
-__device__ __forceinline__ Prim5<double> load_prim(const Fields& F, size_t src, const double sg[3]) {
+__device__ __forceinline__ Prim5<double> load_prim(const Fields& F, const double* rhoP, size_t src,
+                                                   const double sg[3]) {
     Prim5<double> r;
-    r.rho = F.rho[src];
+    r.rho = rhoP[src];
     r.u = sg[0] * F.velU[src];
     r.v = (DIM >= 2) ? sg[1] * F.velV[src] : 0.0;
     r.w = (DIM >= 3) ? sg[2] * F.velW[src] : 0.0;
@@ -286,6 +287,7 @@ __global__ void __launch_bounds__(128) k_sweep_x(SweepArgs A) {
         // stage primitive write-back of the cells this lane holds (FIRST sweep)
         if (q >= 0 && q < nx) {
             size_t c = rowBase + q;
+            A.rhoP[c] = curD.rho;
             F.velU[c] = curD.u;
             if (DIM >= 2) F.velV[c] = curD.v;
             if (DIM >= 3) F.velW[c] = curD.w;
@@ -398,7 +400,7 @@ __global__ void __launch_bounds__(128) k_sweep_line(SweepArgs A) {
         int s = prim_src(q, nLine, bcLo, bcHi, sn, sa);
         double sg[3] = {1.0, 1.0, 1.0};
         if (s != q) { sg[0] = sa; sg[1] = sa; sg[2] = sa; sg[DIR] = sn * sa; }
-        return to_t<T>(load_prim<DIM>(F, lineBase + (long)s * st, sg));
+        return to_t<T>(load_prim<DIM>(F, A.rhoP, lineBase + (long)s * st, sg));
     };
 
     Prim5<T> w0 = loadq(s0 - 3), w1 = loadq(s0 - 2), w2 = loadq(s0 - 1), w3 = loadq(s0), w4 = loadq(s0 + 1);

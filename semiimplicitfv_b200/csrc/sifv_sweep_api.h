@@ -32,6 +32,8 @@ struct SweepArgs {
     double eps;
     int seg;       // cells per thread segment (line sweeps)
     double* rhs[5];  // FP64 rhs buffer (rho, rhoU, rhoV, rhoW, rhoE)
+    double* rhoP;    // stage primitive density: the conservative rho is updated in place by the
+                     // last sweep while neighbouring stencils still need the stage-start value
     const double* inv[3];   // 1 / d per cell (ghosts included)
 };
 
