@@ -1,9 +1,10 @@
 """The fused-sweep paths on the GPU.
 
-SIFV_PREC_FP64_FAST is FP64 with reassociated arithmetic: it must stay
-within 1e-10 relative L-infinity per conserved variable of the
-reference-ordered path (itself bit-identical to the reference), also over
-long runs.  SIFV_PREC_MIXED runs the reconstruction / Riemann bulk in FP32:
+SIFV_PREC_FP64_FAST is FP64 with reassociated arithmetic: on the parity
+cases it must stay within 1e-10 relative L-infinity per conserved variable
+of the reference-ordered path (itself bit-identical to the reference); on a
+long Kelvin-Helmholtz-unstable run it must drift no more than the reference
+drifts from itself under its own Release compiler flags.  SIFV_PREC_MIXED runs the reconstruction / Riemann bulk in FP32:
 it is judged by its L1 error against the exact solution (Sod) and against
 the FP64 discretisation error."""
 import json
