@@ -12,14 +12,15 @@ namespace sifv {
 
 namespace {
 
-constexpr int kSegment = 64;   // cells per thread along y / z
+constexpr int kSegment = 32;    // cells per thread along y / z
+constexpr int kSegmentX = 510;  // cells per warp along x: 16 steps of 32 positions
 
 template <int DIM, typename T>
 int stage_dim(const SweepArgs& A, cudaStream_t s, int& launches, LaunchMark mark, void* user) {
     const Params& P = A.P;
     {
-        long long rows = (long long)P.ny * P.nz;
-        unsigned g = (unsigned)((rows + 3) / 4);
+        long long warps = (long long)P.ny * P.nz * ((P.nx + A.segx - 1) / A.segx);
+        unsigned g = (unsigned)((warps + 3) / 4);
         k_sweep_x<DIM, T><<<g, 128, 0, s>>>(A);
         ++launches;
         if (mark) mark(user, "sweep_x");
@@ -48,6 +49,7 @@ int stage_dim(const SweepArgs& A, cudaStream_t s, int& launches, LaunchMark mark
 
 int sweep_stage(SweepArgs A, cudaStream_t s, bool mixed, int& launches, LaunchMark mark, void* user) {
     A.seg = kSegment;
+    A.segx = kSegmentX;
     switch (A.P.dim) {
         case 1:
             return mixed ? stage_dim<1, float>(A, s, launches, mark, user)

@@ -241,51 +241,86 @@ __device__ __forceinline__ void rk_apply(const Fields& F, size_t c, const RKUpda
     if (DIM >= 3) F.rhoW[c] = nw;
 }
 
-// x sweep: one warp per row; lane l handles position q = 32 t - 1 + l at
-// step t, q in [-1, nx] (the cells whose face values are needed).  Writes
-// the stage's primitive state and the x flux divergence (rhs buffer); it
-// never updates the conservative state, so periodic ghosts read at the end
-// of a row still see the stage-start values.
+// x sweep: each warp takes one segment [x0, x0 + seg) of one row (seg = 32 m
+// - 2, so the seg + 2 positions whose face values are needed, x0-1 .. x0+seg,
+// fill m steps of 32 lanes exactly); lane l handles position
+// q = x0 - 1 + 32 t + l at step t.  The conservative values of step t+2 are
+// loaded during step t and converted to primitives at its end, so their
+// memory latency is hidden behind a step of arithmetic.  Writes the
+// stage's primitive state (the density into the stage copy) and the x flux
+// divergence (rhs buffer); it never updates the conservative state, so
+// periodic ghosts read at the end of a row still see the stage-start values.
+struct RawCons {
+    double rho, ru, rv, rw, re;
+    double sg0, sg1, sg2;
+    int valid;
+};
+
 template <int DIM, typename T>
 __global__ void __launch_bounds__(128) k_sweep_x(SweepArgs A) {
     const Params& P = A.P;
     const Fields& F = A.F;
     if (A.ctl->skip) return;
     const int lane = threadIdx.x & 31;
-    const long long row = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (row >= (long long)P.ny * P.nz) return;
-    const int j = (int)(row % P.ny), k = (int)(row / P.ny);
-    const size_t rowBase = cidx(P, 0, j, k);   // cell (0, j, k)
-    const T eps = (T)A.eps;
     const int nx = P.nx;
+    const int segs = (nx + A.segx - 1) / A.segx;
+    const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (wid >= (long long)P.ny * P.nz * segs) return;
+    const int sIdx = (int)(wid % segs);
+    const long long row = wid / segs;
+    const int j = (int)(row % P.ny), k = (int)(row / P.ny);
+    const int x0 = sIdx * A.segx;
+    const int xe = min(x0 + A.segx, nx);          // cells [x0, xe)
+    const size_t rowBase = cidx(P, 0, j, k);
+    const T eps = (T)A.eps;
 
-    // load the primitive state of position q (ghosts via the x ghost map), FP64
-    auto loadq = [&](int q, Prim5<double>& out) {
-        if (q < -P.ngx || q >= nx + P.ngx) {
-            out = Prim5<double>{0.0, 0.0, 0.0, 0.0, 0.0};
-            return;
-        }
+    // raw conservative values of position q (ghosts through the x ghost map)
+    auto fetch = [&](int q) -> RawCons {
+        RawCons r;
+        r.valid = (q >= -P.ngx && q < nx + P.ngx);
+        r.sg0 = r.sg1 = r.sg2 = 1.0;
+        if (!r.valid) { r.rho = r.ru = r.rv = r.rw = r.re = 0.0; return r; }
         double sn, sa;
         int s = prim_src(q, nx, P.bc[0], P.bc[1], sn, sa);
-        double sg[3] = {1.0, 1.0, 1.0};
-        if (s != q) { sg[0] = sn * sa; sg[1] = sa; sg[2] = sa; }
-        out = load_cons_prim(P, F, rowBase + (size_t)s, sg);
+        if (s != q) { r.sg0 = sn * sa; r.sg1 = sa; r.sg2 = sa; }
+        size_t c = rowBase + (size_t)s;
+        r.rho = F.rho[c];
+        r.ru = F.rhoU[c];
+        r.rv = (DIM >= 2) ? F.rhoV[c] : 0.0;
+        r.rw = (DIM >= 3) ? F.rhoW[c] : 0.0;
+        r.re = F.rhoE[c];
+        return r;
+    };
+    // conservative -> primitive in FP64 (SolutionState::convertConservativeToPrimitiveVariables,
+    // src/SolutionState.cpp:187-205 with src/IdealGasEOS.cpp:46-64 / src/StiffenedGasEOS.cpp:47-64)
+    auto convert = [&](const RawCons& r) -> Prim5<double> {
+        if (!r.valid) return Prim5<double>{0.0, 0.0, 0.0, 0.0, 0.0};
+        const int dim = DIM;
+        double rho = (r.rho < 1e-14) ? 1e-14 : r.rho;
+        double ir = 1.0 / rho;
+        double u = r.ru * ir, v = r.rv * ir, w = r.rw * ir;
+        double ke = u * u;
+        if (dim >= 2) ke += v * v;
+        if (dim >= 3) ke += w * w;
+        ke *= 0.5 * rho;
+        double e = r.re - ke;
+        double p = P.eosStiffened ? (P.gamma - 1.0) * e - P.gamma * P.pInf : (P.gamma - 1.0) * e;
+        if (!P.eosStiffened && p < 1e-14) p = 1e-14;
+        return Prim5<double>{r.rho, r.sg0 * u, r.sg1 * v, r.sg2 * w, p};
     };
 
-    const int nsteps = (nx + 2 + 31) / 32;
-    Prim5<double> prevD, curD, nextD;
-    loadq(-33 + lane, prevD);
-    loadq(-1 + lane, curD);
-    loadq(31 + lane, nextD);
-    Prim5<T> prev = to_t<T>(prevD), cur = to_t<T>(curD), next = to_t<T>(nextD);
-    Prim5<T> Lprev31;                 // L of position q - 1 for lane 0 (previous step's lane 31)
-    Flux4<T> Fprev31;                 // flux of face q - 1 for lane 0
-    Lprev31 = Prim5<T>{(T)0, (T)0, (T)0, (T)0, (T)0};
-    Fprev31 = Flux4<T>{(T)0, (T)0, (T)0, (T)0, (T)0};
+    const int nsteps = (xe - x0 + 2 + 31) / 32;
+    Prim5<double> curD = convert(fetch(x0 - 1 + lane));
+    Prim5<T> prev = to_t<T>(convert(fetch(x0 - 33 + lane)));
+    Prim5<T> cur = to_t<T>(curD);
+    Prim5<double> nextD = convert(fetch(x0 + 31 + lane));
+    Prim5<T> next = to_t<T>(nextD);
+    RawCons raw = fetch(x0 + 63 + lane);
+    Prim5<T> Lprev31 = Prim5<T>{(T)0, (T)0, (T)0, (T)0, (T)0};
+    Flux4<T> Fprev31 = Flux4<T>{(T)0, (T)0, (T)0, (T)0, (T)0};
     for (int t = 0; t < nsteps; ++t) {
-        const int q = 32 * t - 1 + lane;
-        // stage primitive write-back of the cells this lane holds (FIRST sweep)
-        if (q >= 0 && q < nx) {
+        const int q = x0 - 1 + 32 * t + lane;
+        if (q >= x0 && q < xe) {
             size_t c = rowBase + q;
             A.rhoP[c] = curD.rho;
             F.velU[c] = curD.u;
@@ -339,19 +374,14 @@ __global__ void __launch_bounds__(128) k_sweep_x(SweepArgs A) {
         Fm.energy = __shfl_sync(0xffffffffu, Fq.energy, (lane + 31) & 31);
         if (lane == 0) Fm = Fprev31;
         const int cq = q - 1;
-        if (cq >= 0 && cq < nx) {
+        if (cq >= x0 && cq < xe) {
             size_t c = rowBase + cq;
             double ci = A.inv[0][cq + P.ngx];
-            double rR = ci * ((double)Fm.mass - (double)Fq.mass);
-            double rU = ci * ((double)Fm.m0 - (double)Fq.m0);
-            double rV = ci * ((double)Fm.m1 - (double)Fq.m1);
-            double rW = ci * ((double)Fm.m2 - (double)Fq.m2);
-            double rE = ci * ((double)Fm.energy - (double)Fq.energy);
-            A.rhs[0][c] = rR;
-            A.rhs[1][c] = rU;
-            if (DIM >= 2) A.rhs[2][c] = rV;
-            if (DIM >= 3) A.rhs[3][c] = rW;
-            A.rhs[4][c] = rE;
+            A.rhs[0][c] = ci * ((double)Fm.mass - (double)Fq.mass);
+            A.rhs[1][c] = ci * ((double)Fm.m0 - (double)Fq.m0);
+            if (DIM >= 2) A.rhs[2][c] = ci * ((double)Fm.m1 - (double)Fq.m1);
+            if (DIM >= 3) A.rhs[3][c] = ci * ((double)Fm.m2 - (double)Fq.m2);
+            A.rhs[4][c] = ci * ((double)Fm.energy - (double)Fq.energy);
         }
         // carry lane 31's L and flux to the next step's lane 0
         Lprev31.rho = __shfl_sync(0xffffffffu, L.rho, 31);
@@ -364,18 +394,22 @@ __global__ void __launch_bounds__(128) k_sweep_x(SweepArgs A) {
         Fprev31.m1 = __shfl_sync(0xffffffffu, Fq.m1, 31);
         Fprev31.m2 = __shfl_sync(0xffffffffu, Fq.m2, 31);
         Fprev31.energy = __shfl_sync(0xffffffffu, Fq.energy, 31);
-        // advance the window by 32 positions
+        // advance the window by 32 positions; convert the prefetched step,
+        // then start loading the one after it
         prev = cur;
         cur = next;
         curD = nextD;
-        loadq(32 * (t + 2) - 1 + lane, nextD);
+        nextD = convert(raw);
         next = to_t<T>(nextD);
+        if (t + 3 < nsteps + 1) raw = fetch(x0 + 32 * (t + 3) - 1 + lane);
     }
 }
 
 // y or z sweep: each thread marches along one line segment [s0, s0 + seg)
 // of axis DIR at fixed x = i (consecutive lanes, coalesced) keeping the
-// 5-cell window of positions q-2 .. q+2 in registers.
+// 5-cell window of positions q-2 .. q+2 in registers.  The primitive values
+// of position q+3 and the update inputs of cell q-1 are loaded before the
+// arithmetic of step q so their latency overlaps it.
 template <int DIR, int DIM, typename T, bool LAST>
 __global__ void __launch_bounds__(128) k_sweep_line(SweepArgs A) {
     const Params& P = A.P;
@@ -393,17 +427,20 @@ __global__ void __launch_bounds__(128) k_sweep_line(SweepArgs A) {
     const int ng = (DIR == 1) ? P.ngy : P.ngz;
     const int bcLo = P.bc[2 * DIR], bcHi = P.bc[2 * DIR + 1];
     const T eps = (T)A.eps;
+    const double dt = A.ctl->dt;
 
-    auto loadq = [&](int q) -> Prim5<T> {
-        if (q < -ng || q >= nLine + ng) return Prim5<T>{(T)0, (T)0, (T)0, (T)0, (T)0};
+    auto loadq = [&](int q) -> Prim5<double> {
+        if (q < -ng || q >= nLine + ng) return Prim5<double>{0.0, 0.0, 0.0, 0.0, 0.0};
         double sn, sa;
         int s = prim_src(q, nLine, bcLo, bcHi, sn, sa);
         double sg[3] = {1.0, 1.0, 1.0};
         if (s != q) { sg[0] = sa; sg[1] = sa; sg[2] = sa; sg[DIR] = sn * sa; }
-        return to_t<T>(load_prim<DIM>(F, A.rhoP, lineBase + (long)s * st, sg));
+        return load_prim<DIM>(F, A.rhoP, lineBase + (long)s * st, sg);
     };
 
-    Prim5<T> w0 = loadq(s0 - 3), w1 = loadq(s0 - 2), w2 = loadq(s0 - 1), w3 = loadq(s0), w4 = loadq(s0 + 1);
+    Prim5<T> w0 = to_t<T>(loadq(s0 - 3)), w1 = to_t<T>(loadq(s0 - 2)), w2 = to_t<T>(loadq(s0 - 1));
+    Prim5<T> w3 = to_t<T>(loadq(s0)), w4 = to_t<T>(loadq(s0 + 1));
+    Prim5<double> ahead = loadq(s0 + 2);
     Prim5<T> Lm;
     Flux4<T> Fm;
     // position s0 - 1: only its right-face value is needed
@@ -413,27 +450,58 @@ __global__ void __launch_bounds__(128) k_sweep_line(SweepArgs A) {
     }
     for (int q = s0; q <= s1; ++q) {
         w0 = w1; w1 = w2; w2 = w3; w3 = w4;
-        w4 = loadq(q + 2);
+        w4 = to_t<T>(ahead);
+        ahead = loadq(q + 3);
+        // update inputs of cell q-1
+        const bool emit = q > s0;
+        const int cq = q - 1;
+        const size_t c = lineBase + (long)cq * st;
+        double pr[5] = {0, 0, 0, 0, 0}, U[5] = {0, 0, 0, 0, 0}, U0[5] = {0, 0, 0, 0, 0}, pres = 0.0;
+        if (emit) {
+            pr[0] = A.rhs[0][c]; pr[1] = A.rhs[1][c]; pr[4] = A.rhs[4][c];
+            if (DIM >= 2) pr[2] = A.rhs[2][c];
+            if (DIM >= 3) pr[3] = A.rhs[3][c];
+            if (LAST) {
+                U[0] = F.rho[c]; U[1] = F.rhoU[c]; U[4] = F.rhoE[c];
+                if (DIM >= 2) U[2] = F.rhoV[c];
+                if (DIM >= 3) U[3] = F.rhoW[c];
+                if (A.K.useU0) {
+                    U0[0] = F.rho0[c]; U0[1] = F.rhoU0[c]; U0[4] = F.rhoE0[c];
+                    if (DIM >= 2) U0[2] = F.rhoV0[c];
+                    if (DIM >= 3) U0[3] = F.rhoW0[c];
+                }
+                if (A.K.save) pres = F.pres[c];
+            }
+        }
         Prim5<T> L, R;
         recon_cell<DIM, T>(w0, w1, w2, w3, w4, eps, L, R);
         Flux4<T> Fq;
         face_flux<DIR, DIM, T>(P.riemann, A.C, Lm, R, Fq);
-        if (q > s0) {
-            const int cq = q - 1;
-            const size_t c = lineBase + (long)cq * st;
+        if (emit) {
             double ci = A.inv[DIR][cq + ng];
-            double rR = ci * ((double)Fm.mass - (double)Fq.mass);
-            double rU = ci * ((double)Fm.m0 - (double)Fq.m0);
-            double rV = ci * ((double)Fm.m1 - (double)Fq.m1);
-            double rW = ci * ((double)Fm.m2 - (double)Fq.m2);
-            double rE = ci * ((double)Fm.energy - (double)Fq.energy);
-            rR += A.rhs[0][c];
-            rU += A.rhs[1][c];
-            if (DIM >= 2) rV += A.rhs[2][c];
-            if (DIM >= 3) rW += A.rhs[3][c];
-            rE += A.rhs[4][c];
+            double rR = ci * ((double)Fm.mass - (double)Fq.mass) + pr[0];
+            double rU = ci * ((double)Fm.m0 - (double)Fq.m0) + pr[1];
+            double rV = ci * ((double)Fm.m1 - (double)Fq.m1) + pr[2];
+            double rW = ci * ((double)Fm.m2 - (double)Fq.m2) + pr[3];
+            double rE = ci * ((double)Fm.energy - (double)Fq.energy) + pr[4];
             if (LAST) {
-                rk_apply<DIM>(F, c, A.K, A.ctl->dt, rR, rU, rV, rW, rE);
+                const RKUpdate& K = A.K;
+                if (K.save) {
+                    F.rho0[c] = U[0]; F.rhoU0[c] = U[1]; F.rhoE0[c] = U[4];
+                    if (DIM >= 2) F.rhoV0[c] = U[2];
+                    if (DIM >= 3) F.rhoW0[c] = U[3];
+                    F.pres0[c] = pres;
+                }
+                const double a3 = K.a3 * dt;
+                double nr = K.a1 * U[0] + a3 * rR, nu = K.a1 * U[1] + a3 * rU, ne = K.a1 * U[4] + a3 * rE;
+                double nv = K.a1 * U[2] + a3 * rV, nw = K.a1 * U[3] + a3 * rW;
+                if (K.useU0) {
+                    nr += K.a2 * U0[0]; nu += K.a2 * U0[1]; ne += K.a2 * U0[4];
+                    nv += K.a2 * U0[2]; nw += K.a2 * U0[3];
+                }
+                F.rho[c] = nr; F.rhoU[c] = nu; F.rhoE[c] = ne;
+                if (DIM >= 2) F.rhoV[c] = nv;
+                if (DIM >= 3) F.rhoW[c] = nw;
             } else {
                 A.rhs[0][c] = rR;
                 A.rhs[1][c] = rU;

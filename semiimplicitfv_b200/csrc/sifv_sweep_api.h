@@ -31,6 +31,7 @@ struct SweepArgs {
     RKUpdate K;
     double eps;
     int seg;       // cells per thread segment (line sweeps)
+    int segx;      // cells per warp segment of a row (x sweep), 32 m - 2
     double* rhs[5];  // FP64 rhs buffer (rho, rhoU, rhoV, rhoW, rhoE)
     double* rhoP;    // stage primitive density: the conservative rho is updated in place by the
                      // last sweep while neighbouring stencils still need the stage-start value
