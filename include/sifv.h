@@ -235,6 +235,40 @@ int sifv_profile_step(sifv_ctx_t* ctx, int step, double time, double targetDt, c
  * call, and the number of kernel launches it made. */
 int sifv_last_step_stats(const sifv_ctx_t* ctx, double* deviceMs, int* launches);
 
+/* ---- batched ensembles -------------------------------------------------- */
+/* Many independent 1D problems of different sizes (same configuration and
+ * boundary conditions, own mesh [xLo[k], xHi[k]] with nCells[k] cells)
+ * advanced to a common end time by ONE kernel launch: one CTA per instance
+ * runs the instance's whole time loop (own dt, targetDt = tEnd - t as the
+ * reference's time loop caps it, src/RKTimeStepping.cpp:258-266).  Explicit
+ * 1D WENO5 / UPWIND5, single- or multi-phase, any Riemann solver;
+ * SIFV_PREC_FP64 (bit-identical to running each instance alone) or
+ * SIFV_PREC_MIXED (FP32 reconstruction / Riemann bulk; the primitive
+ * recovery, including the mixture pressure from total energy, the carried
+ * state and the update stay FP64).  Fields are packed instance after instance, each
+ * with its ghosts, x fastest (sifv_ensemble_layout gives the nInst + 1
+ * offsets). */
+typedef struct sifv_ensemble sifv_ensemble_t;
+int sifv_ensemble_create(const sifv_config_t* cfg, int nInst, const int* nCells, const double* xLo,
+                         const double* xHi, const int bc[2], int device, sifv_ensemble_t** out);
+int sifv_ensemble_destroy(sifv_ensemble_t* e);
+const char* sifv_ensemble_last_error(const sifv_ensemble_t* e);
+int sifv_ensemble_layout(const sifv_ensemble_t* e, long long* offsets);
+int sifv_ensemble_set_field(sifv_ensemble_t* e, int field, const double* packed, int onDevice);
+int sifv_ensemble_get_field(sifv_ensemble_t* e, int field, double* packed, int onDevice);
+/* Advance every instance until its time reaches tEnd or it has taken
+ * maxSteps steps in total (<= 0: no step limit).  blockSize 0: the
+ * autotuned (or default 256) threads per instance.  timesOut / stepsOut
+ * (nInst entries each, may be NULL) receive each instance's time and step
+ * count; *deviceMs the launch's device time.  An instance whose time step
+ * comes out non-positive (a blown-up state) stops there and the call
+ * returns SIFV_ERR_NAN; tEnd must be finite unless maxSteps > 0. */
+int sifv_ensemble_run(sifv_ensemble_t* e, double tEnd, int maxSteps, int blockSize, double* timesOut,
+                      int* stepsOut, double* deviceMs);
+/* Time probeSteps steps of every instance at 128 / 256 / 512 threads per
+ * instance, keep the fastest for later runs, restore the state. */
+int sifv_ensemble_autotune(sifv_ensemble_t* e, int probeSteps, int* blockSizeOut);
+
 /* ---- allocation-free pressure solve ----------------------------------- */
 /* Sizes of the static device scratch behind sifv_pressure_solve_noalloc
  * (reserved on every GPU that loads the library, about 32 MB). */

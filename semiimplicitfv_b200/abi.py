@@ -168,6 +168,16 @@ _OPTIONAL_SIGS = {
     "config_validate": (C.c_int, [C.POINTER(Config)]),
     "profile_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_char_p, C.c_int,
                                C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
+    "ensemble_create": (C.c_int, [C.POINTER(Config), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_void_p)]),
+    "ensemble_destroy": (C.c_int, [C.c_void_p]),
+    "ensemble_last_error": (C.c_char_p, [C.c_void_p]),
+    "ensemble_layout": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "ensemble_set_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "ensemble_get_field": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "ensemble_run": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_double),
+                               C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "ensemble_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
 }
 
 
@@ -200,6 +210,85 @@ class Backend:
         if st != OK:
             raise AbiError(st, self.error(None))
         return Context(self, h, cfg, mesh)
+
+    def create_ensemble(self, cfg: Config, n_cells: Sequence[int], x_lo: Sequence[float],
+                        x_hi: Sequence[float], bc=(BC_OUTFLOW, BC_OUTFLOW), device: int = 0) -> "Ensemble":
+        if "ensemble_create" not in self.fn:
+            raise AbiError(ERR_UNSUPPORTED, f"{self.name} has no ensemble entry points")
+        k = len(n_cells)
+        nc = (C.c_int * k)(*[int(v) for v in n_cells])
+        lo = (C.c_double * k)(*[float(v) for v in x_lo])
+        hi = (C.c_double * k)(*[float(v) for v in x_hi])
+        b = (C.c_int * 2)(int(bc[0]), int(bc[1]))
+        h = C.c_void_p()
+        st = self.fn["ensemble_create"](C.byref(cfg), k, nc, lo, hi, b, device, C.byref(h))
+        if st != OK:
+            raise AbiError(st, self.fn["ensemble_last_error"](None).decode())
+        return Ensemble(self, h, cfg, list(n_cells))
+
+
+class Ensemble:
+    """Independent 1D problems of different sizes advanced together
+    (sifv_ensemble_*).  Fields are packed instance after instance with
+    ghosts; ``offsets[k]:offsets[k + 1]`` is instance k's slice."""
+
+    def __init__(self, be: "Backend", handle: C.c_void_p, cfg: Config, n_cells):
+        self.be, self.h, self.cfg, self.n_cells = be, handle, cfg, n_cells
+        k = len(n_cells)
+        off = (C.c_longlong * (k + 1))()
+        self._check(be.fn["ensemble_layout"](handle, off))
+        self.offsets = np.array(off[:], dtype=np.int64)
+        self.ncells = int(self.offsets[-1])
+        self.ng = cfg.nGhost
+
+    def _check(self, st: int) -> int:
+        if st < 0:
+            raise AbiError(st, self.be.fn["ensemble_last_error"](self.h).decode())
+        return st
+
+    def close(self):
+        if self.h:
+            self.be.fn["ensemble_destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def pack(self, per_instance) -> np.ndarray:
+        """Concatenate per-instance arrays (each n + 2 nGhost long)."""
+        out = np.concatenate([np.asarray(a, dtype=np.float64).reshape(-1) for a in per_instance])
+        assert out.size == self.ncells, (out.size, self.ncells)
+        return out
+
+    def unpack(self, packed: np.ndarray):
+        return [packed[self.offsets[k]:self.offsets[k + 1]] for k in range(len(self.n_cells))]
+
+    def set_field(self, fid: int, packed: np.ndarray):
+        a = np.ascontiguousarray(packed, dtype=np.float64).reshape(-1)
+        assert a.size == self.ncells
+        self._check(self.be.fn["ensemble_set_field"](self.h, fid, a.ctypes.data, 0))
+
+    def get_field(self, fid: int) -> np.ndarray:
+        a = np.empty(self.ncells)
+        self._check(self.be.fn["ensemble_get_field"](self.h, fid, a.ctypes.data, 0))
+        return a
+
+    def run(self, t_end: float, max_steps: int = 0, block_size: int = 0):
+        """Returns (times, steps, device_ms)."""
+        k = len(self.n_cells)
+        t = (C.c_double * k)()
+        s = (C.c_int * k)()
+        ms = C.c_double()
+        self._check(self.be.fn["ensemble_run"](self.h, t_end, max_steps, block_size, t, s, C.byref(ms)))
+        return np.array(t[:]), np.array(s[:]), ms.value
+
+    def autotune(self, probe_steps: int = 20) -> int:
+        bs = C.c_int()
+        self._check(self.be.fn["ensemble_autotune"](self.h, probe_steps, C.byref(bs)))
+        return bs.value
 
 
 class Context:

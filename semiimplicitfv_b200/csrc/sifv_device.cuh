@@ -89,9 +89,12 @@ struct Ctl {
     unsigned long long res[1];   // per-iteration max residual bits (sized at allocation)
 };
 
-// std::max / std::min / std::clamp semantics.
-__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
-__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+// std::max / std::min semantics (the first argument unless the comparison
+// says otherwise; NaN handling follows from that).
+template <typename T>
+__device__ __forceinline__ T smax(T a, T b) { return (a < b) ? b : a; }
+template <typename T>
+__device__ __forceinline__ T smin(T a, T b) { return (b < a) ? b : a; }
 
 __device__ __forceinline__ size_t cidx(const Params& P, int i, int j, int k) {
     return (size_t)(i + P.ngx) + (size_t)P.nxT * ((size_t)(j + P.ngy) + (size_t)P.nyT * (size_t)(k + P.ngz));
@@ -146,20 +149,20 @@ __device__ __forceinline__ size_t scalar_idx(const Params& P, int i, int j, int 
 // ---------------------------------------------------------------------------
 
 // MixtureEOS::effectiveGammaAndPiInf, src/MixtureEOS.cpp:18-31
-template <int NPH>
-__device__ __forceinline__ void eff_gamma_piinf(const Params& P, const double* a, double& gEff, double& piEff) {
-    double sumInvGm1 = 0.0, sumPi = 0.0;
+template <int NPH, typename T = double>
+__device__ __forceinline__ void eff_gamma_piinf(const Params& P, const T* a, T& gEff, T& piEff) {
+    T sumInvGm1 = T(0.0), sumPi = T(0.0);
 #pragma unroll
     for (int ph = 0; ph < NPH; ++ph) {
         if (ph < P.nPh) {
-            double gk = P.phaseGamma[ph];
-            double gm1 = gk - 1.0;
+            T gk = T(P.phaseGamma[ph]);
+            T gm1 = gk - T(1.0);
             sumInvGm1 += a[ph] / gm1;
-            sumPi += a[ph] * gk * P.phasePInf[ph] / gm1;
+            sumPi += a[ph] * gk * T(P.phasePInf[ph]) / gm1;
         }
     }
-    gEff = 1.0 + 1.0 / sumInvGm1;
-    piEff = (gEff - 1.0) / gEff * sumPi;
+    gEff = T(1.0) + T(1.0) / sumInvGm1;
+    piEff = (gEff - T(1.0)) / gEff * sumPi;
 }
 
 // MixtureEOS::mixtureSoundSpeed (Wood), src/MixtureEOS.cpp:48-63
@@ -217,104 +220,112 @@ __device__ __forceinline__ double single_sound_speed(const Params& P, double rho
 // ---------------------------------------------------------------------------
 // Reconstruction kernels, src/Reconstruction.cpp:83-200
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double weno5L(double v0, double v1, double v2, double v3, double v4, double eps) {
-    double p0 = (1.0 / 3.0) * v0 - (7.0 / 6.0) * v1 + (11.0 / 6.0) * v2;
-    double p1 = -(1.0 / 6.0) * v1 + (5.0 / 6.0) * v2 + (1.0 / 3.0) * v3;
-    double p2 = (1.0 / 3.0) * v2 + (5.0 / 6.0) * v3 - (1.0 / 6.0) * v4;
-    double t0 = v0 - 2.0 * v1 + v2, s0 = v0 - 4.0 * v1 + 3.0 * v2;
-    double t1 = v1 - 2.0 * v2 + v3, s1 = v1 - v3;
-    double t2 = v2 - 2.0 * v3 + v4, s2 = 3.0 * v2 - 4.0 * v3 + v4;
-    double b0 = (13.0 / 12.0) * t0 * t0 + (1.0 / 4.0) * s0 * s0;
-    double b1 = (13.0 / 12.0) * t1 * t1 + (1.0 / 4.0) * s1 * s1;
-    double b2 = (13.0 / 12.0) * t2 * t2 + (1.0 / 4.0) * s2 * s2;
-    double e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
-    double a0 = (1.0 / 10.0) / (e0 * e0);
-    double a1 = (6.0 / 10.0) / (e1 * e1);
-    double a2 = (3.0 / 10.0) / (e2 * e2);
-    double aSum = a0 + a1 + a2;
+template <typename T>
+__device__ __forceinline__ T weno5L(T v0, T v1, T v2, T v3, T v4, T eps) {
+    T p0 = (T(1.0) / T(3.0)) * v0 - (T(7.0) / T(6.0)) * v1 + (T(11.0) / T(6.0)) * v2;
+    T p1 = -(T(1.0) / T(6.0)) * v1 + (T(5.0) / T(6.0)) * v2 + (T(1.0) / T(3.0)) * v3;
+    T p2 = (T(1.0) / T(3.0)) * v2 + (T(5.0) / T(6.0)) * v3 - (T(1.0) / T(6.0)) * v4;
+    T t0 = v0 - T(2.0) * v1 + v2, s0 = v0 - T(4.0) * v1 + T(3.0) * v2;
+    T t1 = v1 - T(2.0) * v2 + v3, s1 = v1 - v3;
+    T t2 = v2 - T(2.0) * v3 + v4, s2 = T(3.0) * v2 - T(4.0) * v3 + v4;
+    T b0 = (T(13.0) / T(12.0)) * t0 * t0 + (T(1.0) / T(4.0)) * s0 * s0;
+    T b1 = (T(13.0) / T(12.0)) * t1 * t1 + (T(1.0) / T(4.0)) * s1 * s1;
+    T b2 = (T(13.0) / T(12.0)) * t2 * t2 + (T(1.0) / T(4.0)) * s2 * s2;
+    T e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+    T a0 = (T(1.0) / T(10.0)) / (e0 * e0);
+    T a1 = (T(6.0) / T(10.0)) / (e1 * e1);
+    T a2 = (T(3.0) / T(10.0)) / (e2 * e2);
+    T aSum = a0 + a1 + a2;
     return (a0 * p0 + a1 * p1 + a2 * p2) / aSum;
 }
 
-__device__ __forceinline__ double weno5R(double v0, double v1, double v2, double v3, double v4, double eps) {
-    double p0 = (1.0 / 3.0) * v4 - (7.0 / 6.0) * v3 + (11.0 / 6.0) * v2;
-    double p1 = -(1.0 / 6.0) * v3 + (5.0 / 6.0) * v2 + (1.0 / 3.0) * v1;
-    double p2 = (1.0 / 3.0) * v2 + (5.0 / 6.0) * v1 - (1.0 / 6.0) * v0;
-    double t0 = v4 - 2.0 * v3 + v2, s0 = v4 - 4.0 * v3 + 3.0 * v2;
-    double t1 = v3 - 2.0 * v2 + v1, s1 = v3 - v1;
-    double t2 = v2 - 2.0 * v1 + v0, s2 = 3.0 * v2 - 4.0 * v1 + v0;
-    double b0 = (13.0 / 12.0) * t0 * t0 + (1.0 / 4.0) * s0 * s0;
-    double b1 = (13.0 / 12.0) * t1 * t1 + (1.0 / 4.0) * s1 * s1;
-    double b2 = (13.0 / 12.0) * t2 * t2 + (1.0 / 4.0) * s2 * s2;
-    double e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
-    double a0 = (1.0 / 10.0) / (e0 * e0);
-    double a1 = (6.0 / 10.0) / (e1 * e1);
-    double a2 = (3.0 / 10.0) / (e2 * e2);
-    double aSum = a0 + a1 + a2;
+template <typename T>
+__device__ __forceinline__ T weno5R(T v0, T v1, T v2, T v3, T v4, T eps) {
+    T p0 = (T(1.0) / T(3.0)) * v4 - (T(7.0) / T(6.0)) * v3 + (T(11.0) / T(6.0)) * v2;
+    T p1 = -(T(1.0) / T(6.0)) * v3 + (T(5.0) / T(6.0)) * v2 + (T(1.0) / T(3.0)) * v1;
+    T p2 = (T(1.0) / T(3.0)) * v2 + (T(5.0) / T(6.0)) * v1 - (T(1.0) / T(6.0)) * v0;
+    T t0 = v4 - T(2.0) * v3 + v2, s0 = v4 - T(4.0) * v3 + T(3.0) * v2;
+    T t1 = v3 - T(2.0) * v2 + v1, s1 = v3 - v1;
+    T t2 = v2 - T(2.0) * v1 + v0, s2 = T(3.0) * v2 - T(4.0) * v1 + v0;
+    T b0 = (T(13.0) / T(12.0)) * t0 * t0 + (T(1.0) / T(4.0)) * s0 * s0;
+    T b1 = (T(13.0) / T(12.0)) * t1 * t1 + (T(1.0) / T(4.0)) * s1 * s1;
+    T b2 = (T(13.0) / T(12.0)) * t2 * t2 + (T(1.0) / T(4.0)) * s2 * s2;
+    T e0 = eps + b0, e1 = eps + b1, e2 = eps + b2;
+    T a0 = (T(1.0) / T(10.0)) / (e0 * e0);
+    T a1 = (T(6.0) / T(10.0)) / (e1 * e1);
+    T a2 = (T(3.0) / T(10.0)) / (e2 * e2);
+    T aSum = a0 + a1 + a2;
     return (a0 * p0 + a1 * p1 + a2 * p2) / aSum;
 }
 
-__device__ __forceinline__ double upwind5L(double v0, double v1, double v2, double v3, double v4) {
-    double p0 = (1.0 / 3.0) * v0 - (7.0 / 6.0) * v1 + (11.0 / 6.0) * v2;
-    double p1 = -(1.0 / 6.0) * v1 + (5.0 / 6.0) * v2 + (1.0 / 3.0) * v3;
-    double p2 = (1.0 / 3.0) * v2 + (5.0 / 6.0) * v3 - (1.0 / 6.0) * v4;
-    return (1.0 / 10.0) * p0 + (6.0 / 10.0) * p1 + (3.0 / 10.0) * p2;
+template <typename T>
+__device__ __forceinline__ T upwind5L(T v0, T v1, T v2, T v3, T v4) {
+    T p0 = (T(1.0) / T(3.0)) * v0 - (T(7.0) / T(6.0)) * v1 + (T(11.0) / T(6.0)) * v2;
+    T p1 = -(T(1.0) / T(6.0)) * v1 + (T(5.0) / T(6.0)) * v2 + (T(1.0) / T(3.0)) * v3;
+    T p2 = (T(1.0) / T(3.0)) * v2 + (T(5.0) / T(6.0)) * v3 - (T(1.0) / T(6.0)) * v4;
+    return (T(1.0) / T(10.0)) * p0 + (T(6.0) / T(10.0)) * p1 + (T(3.0) / T(10.0)) * p2;
 }
 
-__device__ __forceinline__ double upwind5R(double v0, double v1, double v2, double v3, double v4) {
-    double p0 = (1.0 / 3.0) * v4 - (7.0 / 6.0) * v3 + (11.0 / 6.0) * v2;
-    double p1 = -(1.0 / 6.0) * v3 + (5.0 / 6.0) * v2 + (1.0 / 3.0) * v1;
-    double p2 = (1.0 / 3.0) * v2 + (5.0 / 6.0) * v1 - (1.0 / 6.0) * v0;
-    return (1.0 / 10.0) * p0 + (6.0 / 10.0) * p1 + (3.0 / 10.0) * p2;
+template <typename T>
+__device__ __forceinline__ T upwind5R(T v0, T v1, T v2, T v3, T v4) {
+    T p0 = (T(1.0) / T(3.0)) * v4 - (T(7.0) / T(6.0)) * v3 + (T(11.0) / T(6.0)) * v2;
+    T p1 = -(T(1.0) / T(6.0)) * v3 + (T(5.0) / T(6.0)) * v2 + (T(1.0) / T(3.0)) * v1;
+    T p2 = (T(1.0) / T(3.0)) * v2 + (T(5.0) / T(6.0)) * v1 - (T(1.0) / T(6.0)) * v0;
+    return (T(1.0) / T(10.0)) * p0 + (T(6.0) / T(10.0)) * p1 + (T(3.0) / T(10.0)) * p2;
 }
 
-__device__ __forceinline__ double weno3L(double v0, double v1, double v2, double eps) {
-    double p0 = -0.5 * v0 + 1.5 * v1;
-    double p1 = 0.5 * v1 + 0.5 * v2;
-    double b0 = (v1 - v0) * (v1 - v0);
-    double b1 = (v2 - v1) * (v2 - v1);
-    double e0 = eps + b0, e1 = eps + b1;
-    double a0 = (1.0 / 3.0) / (e0 * e0);
-    double a1 = (2.0 / 3.0) / (e1 * e1);
-    double aSum = a0 + a1;
+template <typename T>
+__device__ __forceinline__ T weno3L(T v0, T v1, T v2, T eps) {
+    T p0 = -T(0.5) * v0 + T(1.5) * v1;
+    T p1 = T(0.5) * v1 + T(0.5) * v2;
+    T b0 = (v1 - v0) * (v1 - v0);
+    T b1 = (v2 - v1) * (v2 - v1);
+    T e0 = eps + b0, e1 = eps + b1;
+    T a0 = (T(1.0) / T(3.0)) / (e0 * e0);
+    T a1 = (T(2.0) / T(3.0)) / (e1 * e1);
+    T aSum = a0 + a1;
     return (a0 * p0 + a1 * p1) / aSum;
 }
 
-__device__ __forceinline__ double weno3R(double v0, double v1, double v2, double eps) {
-    double p0 = 0.5 * v0 + 0.5 * v1;
-    double p1 = 1.5 * v1 - 0.5 * v2;
-    double b0 = (v1 - v0) * (v1 - v0);
-    double b1 = (v2 - v1) * (v2 - v1);
-    double e0 = eps + b0, e1 = eps + b1;
-    double a0 = (2.0 / 3.0) / (e0 * e0);
-    double a1 = (1.0 / 3.0) / (e1 * e1);
-    double aSum = a0 + a1;
+template <typename T>
+__device__ __forceinline__ T weno3R(T v0, T v1, T v2, T eps) {
+    T p0 = T(0.5) * v0 + T(0.5) * v1;
+    T p1 = T(1.5) * v1 - T(0.5) * v2;
+    T b0 = (v1 - v0) * (v1 - v0);
+    T b1 = (v2 - v1) * (v2 - v1);
+    T e0 = eps + b0, e1 = eps + b1;
+    T a0 = (T(2.0) / T(3.0)) / (e0 * e0);
+    T a1 = (T(1.0) / T(3.0)) / (e1 * e1);
+    T aSum = a0 + a1;
     return (a0 * p0 + a1 * p1) / aSum;
 }
 
-__device__ __forceinline__ double upwind3L(double v0, double v1, double v2) {
-    double p0 = -0.5 * v0 + 1.5 * v1;
-    double p1 = 0.5 * v1 + 0.5 * v2;
-    return (1.0 / 3.0) * p0 + (2.0 / 3.0) * p1;
+template <typename T>
+__device__ __forceinline__ T upwind3L(T v0, T v1, T v2) {
+    T p0 = -T(0.5) * v0 + T(1.5) * v1;
+    T p1 = T(0.5) * v1 + T(0.5) * v2;
+    return (T(1.0) / T(3.0)) * p0 + (T(2.0) / T(3.0)) * p1;
 }
 
-__device__ __forceinline__ double upwind3R(double v0, double v1, double v2) {
-    double p0 = 0.5 * v0 + 0.5 * v1;
-    double p1 = 1.5 * v1 - 0.5 * v2;
-    return (2.0 / 3.0) * p0 + (1.0 / 3.0) * p1;
+template <typename T>
+__device__ __forceinline__ T upwind3R(T v0, T v1, T v2) {
+    T p0 = T(0.5) * v0 + T(0.5) * v1;
+    T p1 = T(1.5) * v1 - T(0.5) * v2;
+    return (T(2.0) / T(3.0)) * p0 + (T(1.0) / T(3.0)) * p1;
 }
 
 // Left and right face values of one field at the face whose right cell is
 // `base`, cells strided by `st` along the sweep direction
 // (reconstructScalar, src/Reconstruction.cpp:11-28: the left state uses
 // cells -3..+1, the right state -2..+2 for WENO5).
-template <int W>
-__device__ __forceinline__ void recon_pair(const double* __restrict__ f, size_t base, long st, bool weno, double eps,
-                                           double& L, double& R) {
+template <int W, typename T>
+__device__ __forceinline__ void recon_pair(const T* __restrict__ f, size_t base, long st, bool weno, T eps,
+                                           T& L, T& R) {
     if (W == 1) {
         L = f[base - st];
         R = f[base];
     } else if (W == 3) {
-        double v0 = f[base - 2 * st], v1 = f[base - st], v2 = f[base], v3 = f[base + st];
+        T v0 = f[base - 2 * st], v1 = f[base - st], v2 = f[base], v3 = f[base + st];
         if (weno) {
             L = weno3L(v0, v1, v2, eps);
             R = weno3R(v1, v2, v3, eps);
@@ -323,7 +334,7 @@ __device__ __forceinline__ void recon_pair(const double* __restrict__ f, size_t 
             R = upwind3R(v1, v2, v3);
         }
     } else {
-        double v0 = f[base - 3 * st], v1 = f[base - 2 * st], v2 = f[base - st], v3 = f[base], v4 = f[base + st],
+        T v0 = f[base - 3 * st], v1 = f[base - 2 * st], v2 = f[base - st], v3 = f[base], v4 = f[base + st],
                v5 = f[base + 2 * st];
         if (weno) {
             L = weno5L(v0, v1, v2, v3, v4, eps);
@@ -338,51 +349,51 @@ __device__ __forceinline__ void recon_pair(const double* __restrict__ f, size_t 
 // ---------------------------------------------------------------------------
 // Riemann solvers
 // ---------------------------------------------------------------------------
-template <int NPH>
+template <int NPH, typename T = double>
 struct FaceState {
-    double rho, u[3], p, sigma, gEff, piEff;
-    double alpha[NPH > 0 ? NPH : 1];
+    T rho, u[3], p, sigma, gEff, piEff;
+    T alpha[NPH > 0 ? NPH : 1];
 };
 
-template <int NPH>
+template <int NPH, typename T = double>
 struct FaceFlux {
-    double mass, mom[3], energy, pflux, fvel;
-    double alpha[NPH > 0 ? NPH : 1];
+    T mass, mom[3], energy, pflux, fvel;
+    T alpha[NPH > 0 ? NPH : 1];
 };
 
 // soundSpeedDirect / rhoEFromState, include/RiemannSolver.hpp:70-78
-template <int NPH>
-__device__ __forceinline__ double sound_speed_direct(const FaceState<NPH>& W) {
-    return sqrt(W.gEff * smax(W.p + W.piEff, 1e-14) / smax(W.rho, 1e-14));
+template <int NPH, typename T>
+__device__ __forceinline__ T sound_speed_direct(const FaceState<NPH, T>& W) {
+    return sqrt(W.gEff * smax(W.p + W.piEff, T(1e-14)) / smax(W.rho, T(1e-14)));
 }
-template <int NPH>
-__device__ __forceinline__ double rhoE_from_state(const FaceState<NPH>& W) {
-    double ke = 0.5 * W.rho * (W.u[0] * W.u[0] + W.u[1] * W.u[1] + W.u[2] * W.u[2]);
-    return (W.p + W.gEff * W.piEff) / (W.gEff - 1.0) + ke;
+template <int NPH, typename T>
+__device__ __forceinline__ T rhoE_from_state(const FaceState<NPH, T>& W) {
+    T ke = T(0.5) * W.rho * (W.u[0] * W.u[0] + W.u[1] * W.u[1] + W.u[2] * W.u[2]);
+    return (W.p + W.gEff * W.piEff) / (W.gEff - T(1.0)) + ke;
 }
 
 // normalVelocity (include/RiemannSolver.hpp:59-64) for the unit normal of
 // axis D: 0 + u_D*1 + sum of u_d*0 over the other active axes.
-template <int D, int NPH>
-__device__ __forceinline__ double normal_velocity(const FaceState<NPH>& W, int dim) {
-    double vn = 0.0;
-    DIMLOOP(d) vn += W.u[d] * ((d == D) ? 1.0 : 0.0);
+template <int D, int NPH, typename T>
+__device__ __forceinline__ T normal_velocity(const FaceState<NPH, T>& W, int dim) {
+    T vn = T(0.0);
+    DIMLOOP(d) vn += W.u[d] * ((d == D) ? T(1.0) : T(0.0));
     return vn;
 }
 
 // computeHLLCFlux, src/HLLCSolver.cpp:7-161
-template <int D, int NPH>
-__device__ __forceinline__ void hllc_flux(const Params& P, const FaceState<NPH>& L, const FaceState<NPH>& R,
-                                          FaceFlux<NPH>& F) {
+template <int D, int NPH, typename T>
+__device__ __forceinline__ void hllc_flux(const Params& P, const FaceState<NPH, T>& L, const FaceState<NPH, T>& R,
+                                          FaceFlux<NPH, T>& F) {
     const int dim = P.dim;
     const bool incP = P.includePressure;
-    const double n[3] = {D == 0 ? 1.0 : 0.0, D == 1 ? 1.0 : 0.0, D == 2 ? 1.0 : 0.0};
-    F.mass = 0.0; F.mom[0] = F.mom[1] = F.mom[2] = 0.0; F.energy = 0.0; F.pflux = 0.0; F.fvel = 0.0;
-    double uL = normal_velocity<D>(L, dim), uR = normal_velocity<D>(R, dim);
-    double rhoEL = rhoE_from_state(L), rhoER = rhoE_from_state(R);
-    double sL, sR, sStar;
+    const T n[3] = {D == 0 ? T(1.0) : T(0.0), D == 1 ? T(1.0) : T(0.0), D == 2 ? T(1.0) : T(0.0)};
+    F.mass = T(0.0); F.mom[0] = F.mom[1] = F.mom[2] = T(0.0); F.energy = T(0.0); F.pflux = T(0.0); F.fvel = T(0.0);
+    T uL = normal_velocity<D>(L, dim), uR = normal_velocity<D>(R, dim);
+    T rhoEL = rhoE_from_state(L), rhoER = rhoE_from_state(R);
+    T sL, sR, sStar;
     if (incP) {
-        double cL = sound_speed_direct(L), cR = sound_speed_direct(R);
+        T cL = sound_speed_direct(L), cR = sound_speed_direct(R);
         sL = smin(uL - cL, uR - cR);
         sR = smax(uL + cL, uR + cR);
         sStar = (R.p - L.p + L.rho * uL * (sL - uL) - R.rho * uR * (sR - uR)) /
@@ -390,7 +401,7 @@ __device__ __forceinline__ void hllc_flux(const Params& P, const FaceState<NPH>&
     } else {
         sL = smin(uL, uR);
         sR = smax(uL, uR);
-        sStar = 0.5 * (uL + uR);
+        sStar = T(0.5) * (uL + uR);
     }
     if (sL >= 0) {
         F.mass = L.rho * uL;
@@ -409,43 +420,43 @@ __device__ __forceinline__ void hllc_flux(const Params& P, const FaceState<NPH>&
             F.energy += R.p * uR;
         }
     } else if (sStar >= 0) {
-        double rhoStarL = L.rho * (sL - uL) / (sL - sStar);
+        T rhoStarL = L.rho * (sL - uL) / (sL - sStar);
         F.mass = L.rho * uL + sL * (rhoStarL - L.rho);
         if (incP) {
             DIMLOOP(i) {
-                double rhoUStarL = rhoStarL * (L.u[i] + (sStar - uL) * n[i]);
+                T rhoUStarL = rhoStarL * (L.u[i] + (sStar - uL) * n[i]);
                 F.mom[i] = L.rho * L.u[i] * uL + L.p * n[i] + sL * (rhoUStarL - L.rho * L.u[i]);
             }
-            double eL = rhoEL / L.rho;
-            double EStarL = rhoStarL * (eL + (sStar - uL) * (sStar + L.p / (L.rho * (sL - uL))));
+            T eL = rhoEL / L.rho;
+            T EStarL = rhoStarL * (eL + (sStar - uL) * (sStar + L.p / (L.rho * (sL - uL))));
             F.energy = (rhoEL + L.p) * uL + sL * (EStarL - rhoEL);
         } else {
             DIMLOOP(i) {
-                double rhoUStarL = rhoStarL * (L.u[i] + (sStar - uL) * n[i]);
+                T rhoUStarL = rhoStarL * (L.u[i] + (sStar - uL) * n[i]);
                 F.mom[i] = L.rho * L.u[i] * uL + sL * (rhoUStarL - L.rho * L.u[i]);
             }
-            double eL = rhoEL / L.rho;
-            double EStarL = rhoStarL * (eL + (sStar - uL) * sStar);
+            T eL = rhoEL / L.rho;
+            T EStarL = rhoStarL * (eL + (sStar - uL) * sStar);
             F.energy = rhoEL * uL + sL * (EStarL - rhoEL);
         }
     } else {
-        double rhoStarR = R.rho * (sR - uR) / (sR - sStar);
+        T rhoStarR = R.rho * (sR - uR) / (sR - sStar);
         F.mass = R.rho * uR + sR * (rhoStarR - R.rho);
         if (incP) {
             DIMLOOP(i) {
-                double rhoUStarR = rhoStarR * (R.u[i] + (sStar - uR) * n[i]);
+                T rhoUStarR = rhoStarR * (R.u[i] + (sStar - uR) * n[i]);
                 F.mom[i] = R.rho * R.u[i] * uR + R.p * n[i] + sR * (rhoUStarR - R.rho * R.u[i]);
             }
-            double eR = rhoER / R.rho;
-            double EStarR = rhoStarR * (eR + (sStar - uR) * (sStar + R.p / (R.rho * (sR - uR))));
+            T eR = rhoER / R.rho;
+            T EStarR = rhoStarR * (eR + (sStar - uR) * (sStar + R.p / (R.rho * (sR - uR))));
             F.energy = (rhoER + R.p) * uR + sR * (EStarR - rhoER);
         } else {
             DIMLOOP(i) {
-                double rhoUStarR = rhoStarR * (R.u[i] + (sStar - uR) * n[i]);
+                T rhoUStarR = rhoStarR * (R.u[i] + (sStar - uR) * n[i]);
                 F.mom[i] = R.rho * R.u[i] * uR + sR * (rhoUStarR - R.rho * R.u[i]);
             }
-            double eR = rhoER / R.rho;
-            double EStarR = rhoStarR * (eR + (sStar - uR) * sStar);
+            T eR = rhoER / R.rho;
+            T EStarR = rhoStarR * (eR + (sStar - uR) * sStar);
             F.energy = rhoER * uR + sR * (EStarR - rhoER);
         }
     }
@@ -474,30 +485,30 @@ __device__ __forceinline__ void hllc_flux(const Params& P, const FaceState<NPH>&
 }
 
 // computeRusanovFlux, src/RusanovSolver.cpp:7-83
-template <int D, int NPH>
-__device__ __forceinline__ void rusanov_flux(const Params& P, const FaceState<NPH>& L, const FaceState<NPH>& R,
-                                             FaceFlux<NPH>& F) {
+template <int D, int NPH, typename T>
+__device__ __forceinline__ void rusanov_flux(const Params& P, const FaceState<NPH, T>& L, const FaceState<NPH, T>& R,
+                                             FaceFlux<NPH, T>& F) {
     const int dim = P.dim;
     const bool incP = P.includePressure;
-    const double n[3] = {D == 0 ? 1.0 : 0.0, D == 1 ? 1.0 : 0.0, D == 2 ? 1.0 : 0.0};
-    F.mom[0] = F.mom[1] = F.mom[2] = 0.0;
-    double uL = normal_velocity<D>(L, dim), uR = normal_velocity<D>(R, dim);
-    double absUL = fabs(uL), absUR = fabs(uR);
-    double sMax;
+    const T n[3] = {D == 0 ? T(1.0) : T(0.0), D == 1 ? T(1.0) : T(0.0), D == 2 ? T(1.0) : T(0.0)};
+    F.mom[0] = F.mom[1] = F.mom[2] = T(0.0);
+    T uL = normal_velocity<D>(L, dim), uR = normal_velocity<D>(R, dim);
+    T absUL = fabs(uL), absUR = fabs(uR);
+    T sMax;
     if (incP) {
-        double cL = sound_speed_direct(L), cR = sound_speed_direct(R);
+        T cL = sound_speed_direct(L), cR = sound_speed_direct(R);
         sMax = smax(absUL + cL, absUR + cR);
     } else {
         sMax = smax(absUL, absUR);
     }
-    double rhoEL = rhoE_from_state(L), rhoER = rhoE_from_state(R);
-    double mL = L.rho * uL, mR = R.rho * uR;
-    double momL[3] = {0.0, 0.0, 0.0}, momR[3] = {0.0, 0.0, 0.0};
+    T rhoEL = rhoE_from_state(L), rhoER = rhoE_from_state(R);
+    T mL = L.rho * uL, mR = R.rho * uR;
+    T momL[3] = {T(0.0), T(0.0), T(0.0)}, momR[3] = {T(0.0), T(0.0), T(0.0)};
     DIMLOOP(i) {
         momL[i] = L.rho * L.u[i] * uL;
         momR[i] = R.rho * R.u[i] * uR;
     }
-    double eL = rhoEL * uL, eR = rhoER * uR;
+    T eL = rhoEL * uL, eR = rhoER * uR;
     if (incP) {
         DIMLOOP(i) {
             momL[i] += L.p * n[i];
@@ -506,58 +517,58 @@ __device__ __forceinline__ void rusanov_flux(const Params& P, const FaceState<NP
         eL += L.p * uL;
         eR += R.p * uR;
     }
-    F.mass = 0.5 * (mL + mR) - 0.5 * sMax * (R.rho - L.rho);
+    F.mass = T(0.5) * (mL + mR) - T(0.5) * sMax * (R.rho - L.rho);
     DIMLOOP(i)
-        F.mom[i] = 0.5 * (momL[i] + momR[i]) - 0.5 * sMax * (R.rho * R.u[i] - L.rho * L.u[i]);
-    F.energy = 0.5 * (eL + eR) - 0.5 * sMax * (rhoER - rhoEL);
-    F.fvel = 0.5 * (uL + uR);
-    F.pflux = 0.5 * (L.p * uL + R.p * uR) - 0.5 * sMax * (R.p - L.p);
+        F.mom[i] = T(0.5) * (momL[i] + momR[i]) - T(0.5) * sMax * (R.rho * R.u[i] - L.rho * L.u[i]);
+    F.energy = T(0.5) * (eL + eR) - T(0.5) * sMax * (rhoER - rhoEL);
+    F.fvel = T(0.5) * (uL + uR);
+    F.pflux = T(0.5) * (L.p * uL + R.p * uR) - T(0.5) * sMax * (R.p - L.p);
 #pragma unroll
     for (int ph = 0; ph < NPH; ++ph)
-        F.alpha[ph] = 0.5 * (L.alpha[ph] * uL + R.alpha[ph] * uR) - 0.5 * sMax * (R.alpha[ph] - L.alpha[ph]);
+        F.alpha[ph] = T(0.5) * (L.alpha[ph] * uL + R.alpha[ph] * uR) - T(0.5) * sMax * (R.alpha[ph] - L.alpha[ph]);
 }
 
 // computeLFFlux, src/LFSolver.cpp:8-75
-template <int D, int NPH>
-__device__ __forceinline__ void lf_flux(const Params& P, const FaceState<NPH>& L, const FaceState<NPH>& R,
-                                        FaceFlux<NPH>& F) {
+template <int D, int NPH, typename T>
+__device__ __forceinline__ void lf_flux(const Params& P, const FaceState<NPH, T>& L, const FaceState<NPH, T>& R,
+                                        FaceFlux<NPH, T>& F) {
     const int dim = P.dim;
     const bool incP = P.includePressure;
-    const double n[3] = {D == 0 ? 1.0 : 0.0, D == 1 ? 1.0 : 0.0, D == 2 ? 1.0 : 0.0};
-    F.mom[0] = F.mom[1] = F.mom[2] = 0.0;
-    double uL = normal_velocity<D>(L, dim), uR = normal_velocity<D>(R, dim);
-    double uLS = 0.0, uRS = 0.0;
+    const T n[3] = {D == 0 ? T(1.0) : T(0.0), D == 1 ? T(1.0) : T(0.0), D == 2 ? T(1.0) : T(0.0)};
+    F.mom[0] = F.mom[1] = F.mom[2] = T(0.0);
+    T uL = normal_velocity<D>(L, dim), uR = normal_velocity<D>(R, dim);
+    T uLS = T(0.0), uRS = T(0.0);
     DIMLOOP(i) {
         uLS += L.u[i] * L.u[i];
         uRS += R.u[i] * R.u[i];
     }
     uLS = sqrt(uLS);
     uRS = sqrt(uRS);
-    double C;
+    T C;
     if (incP) {
-        double cL = sound_speed_direct(L), cR = sound_speed_direct(R);
+        T cL = sound_speed_direct(L), cR = sound_speed_direct(R);
         C = smax(uLS, uRS) + smax(cL, cR);
     } else {
         C = smax(uLS, uRS);
     }
-    F.mass = 0.5 * (L.rho * uL + R.rho * uR) - 0.5 * C * (R.rho - L.rho);
+    F.mass = T(0.5) * (L.rho * uL + R.rho * uR) - T(0.5) * C * (R.rho - L.rho);
     DIMLOOP(i)
-        F.mom[i] = 0.5 * (L.rho * L.u[i] * uL + R.rho * R.u[i] * uR) - 0.5 * C * (R.rho * R.u[i] - L.rho * L.u[i]);
-    double rhoEL = rhoE_from_state(L), rhoER = rhoE_from_state(R);
-    F.energy = 0.5 * (rhoEL * uL + rhoER * uR) - 0.5 * C * (rhoER - rhoEL);
+        F.mom[i] = T(0.5) * (L.rho * L.u[i] * uL + R.rho * R.u[i] * uR) - T(0.5) * C * (R.rho * R.u[i] - L.rho * L.u[i]);
+    T rhoEL = rhoE_from_state(L), rhoER = rhoE_from_state(R);
+    F.energy = T(0.5) * (rhoEL * uL + rhoER * uR) - T(0.5) * C * (rhoER - rhoEL);
     if (incP) {
-        DIMLOOP(i) F.mom[i] += 0.5 * (L.p + R.p) * n[i];
-        F.energy += 0.5 * (L.p * uL + R.p * uR);
+        DIMLOOP(i) F.mom[i] += T(0.5) * (L.p + R.p) * n[i];
+        F.energy += T(0.5) * (L.p * uL + R.p * uR);
     }
     if (P.useIGR) {
-        DIMLOOP(i) F.mom[i] += 0.5 * (L.sigma + R.sigma) * n[i];
-        F.energy += 0.5 * (L.sigma * uL + R.sigma * uR);
+        DIMLOOP(i) F.mom[i] += T(0.5) * (L.sigma + R.sigma) * n[i];
+        F.energy += T(0.5) * (L.sigma * uL + R.sigma * uR);
     }
-    F.fvel = 0.5 * (uL + uR);
-    F.pflux = 0.5 * (L.p * uL + R.p * uR) - 0.5 * C * (R.p - L.p);
+    F.fvel = T(0.5) * (uL + uR);
+    F.pflux = T(0.5) * (L.p * uL + R.p * uR) - T(0.5) * C * (R.p - L.p);
 #pragma unroll
     for (int ph = 0; ph < NPH; ++ph)
-        F.alpha[ph] = 0.5 * (L.alpha[ph] * uL + R.alpha[ph] * uR) - 0.5 * C * (R.alpha[ph] - L.alpha[ph]);
+        F.alpha[ph] = T(0.5) * (L.alpha[ph] * uL + R.alpha[ph] * uR) - T(0.5) * C * (R.alpha[ph] - L.alpha[ph]);
 }
 
 }  // namespace sifv

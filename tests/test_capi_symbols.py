@@ -57,3 +57,25 @@ def test_create_without_gpu_fails_cleanly():
         assert e.status in (abi.ERR_NO_DEVICE, abi.ERR_CUDA)
     else:
         raise AssertionError("create succeeded without a GPU")
+
+
+def test_ensemble_create_without_gpu_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        return
+    be = abi.Backend(_lib.load(), "sifv_", "cuda")
+    cfg = abi.config_defaults(dim=1, nGhost=3, reconOrder=abi.WENO5)
+    try:
+        be.create_ensemble(cfg, [16, 32], [0.0, 0.0], [1.0, 2.0])
+    except abi.AbiError as e:
+        assert e.status in (abi.ERR_NO_DEVICE, abi.ERR_CUDA)
+    else:
+        raise AssertionError("ensemble create succeeded without a GPU")
+    # configuration checks come first and need no device
+    bad = abi.config_defaults(dim=2, nGhost=3, reconOrder=abi.WENO5)
+    try:
+        be.create_ensemble(bad, [16], [0.0], [1.0])
+    except abi.AbiError as e:
+        assert e.status == abi.ERR_UNSUPPORTED
+    else:
+        raise AssertionError("2D ensemble accepted")
