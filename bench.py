@@ -3,8 +3,12 @@ four-quadrant Riemann problem, 4096 x 4096 cells, FP64.
 
 One "step" is one full time step (three RK stages, dt reduction, ghost
 fills) over the whole grid.  `value` times K steps queued back to back with
-the state resident in HBM (sifv_advance); `e2e` times K calls of the drop-in
-entry point sifv_step through the C ABI, each returning dt to the host.
+the state resident in HBM (sifv_advance); `e2e` times K steps the way the
+drop-in solver with host-authoritative state runs them: per step the state
+fields the step reads are copied from pinned host buffers (sifv_set_field),
+sifv_step runs and returns dt, and the fields it writes are copied back
+(sifv_get_field).  The `ensemble` object times the batched-ensemble
+workload (2048 two-phase water-air tubes, one launch).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 
@@ -43,6 +47,16 @@ BYTES_PER_CELL_UPDATE = 256   # algorithmic: 64 B x 4 conserved variables per RK
 #   finish_prim reads 4 U, writes velU, velV, pres              7 x 8 = 56
 KERNEL_BYTES_PER_CELL_2D = {"sweep_x": 96.0, "sweep_y": 165.33, "dt": 32.0, "finish_prim": 56.0,
                             "face_x": 64.0, "face_y": 64.0, "assemble": 229.3, "prim_bc": 56.0}
+# DRAM bytes per cell of one launch, measured by ncu on the 2048^2 case of the
+# same workload (dram__bytes_read.sum + dram__bytes_write.sum over 2048^2 cells)
+# and scaled by the cell count for the benchmark size.
+NCU_DRAM_BYTES_PER_CELL = {(2, "sweep_y"): 164.8, (2, "sweep_x"): 84.5, (1, "sweep_y"): 164.7,
+                           (1, "sweep_x"): 86.2, (0, "assemble"): 166.2}
+# Fields a 2D step reads and writes (host-authoritative drop-in round trip).
+E2E_FIELDS_2D = ("F_RHO", "F_RHOU", "F_RHOV", "F_RHOE", "F_VELU", "F_VELV", "F_PRES")
+# Batched ensemble of two-phase water-air tubes: count, cell range, end time.
+ENS_COUNT, ENS_NMIN, ENS_NMAX, ENS_TEND, ENS_SEED = 2048, 256, 16384, 1e-4, 0
+ENS_BYTES_PER_CELL_UPDATE = 384   # state alphaRho0, alphaRho1, rhoU, rhoE, alpha0, alpha1: 64 B x 6
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -118,6 +132,54 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def ensemble_instances(count=ENS_COUNT, seed=ENS_SEED, nmin=ENS_NMIN, nmax=ENS_NMAX):
+    """Seeded two-phase water-air tubes on [0, 1]: cells log-uniform in
+    [nmin, nmax], interface uniform in [0.3, 0.7], water pressure uniform in
+    [1e8, 1e9] (water gamma 4.4, pInf 6e8, rho 1000; air gamma 1.4, rho 1,
+    p 1e5; alphaMin 1e-8), WENO5 + mixture HLLC, SSP-RK3, CFL 0.5."""
+    import numpy as np
+    import cases
+    rng = np.random.default_rng(seed)
+    ns = np.round(np.exp(rng.uniform(np.log(nmin), np.log(nmax), count))).astype(int)
+    xi = rng.uniform(0.3, 0.7, count)
+    pl = rng.uniform(1e8, 1e9, count)
+    return [cases.water_air(int(n), x_interface=float(a), p_left=float(b)) for n, a, b in zip(ns, xi, pl)]
+
+
+def _ens_cpu_worker(args):
+    """One process: the reference (or oracle) runs its share of tubes alone,
+    each to the end time; returns (cell-updates, seconds)."""
+    kind, idx = args
+    import backends
+    import cases
+    be = backends.reference(release=True) if kind == "reference" else backends.oracle()
+    inst = ensemble_instances()
+    cu, sec = 0.0, 0.0
+    for k in idx:
+        case = inst[k]
+        ctx = backends.make(be, case)
+        t0 = time.perf_counter()
+        _, steps, _ = cases.run_steps(ctx, 10 ** 9, t_end=ENS_TEND)
+        sec += time.perf_counter() - t0
+        cu += (len(case[1].x) - 1) * steps
+    return cu, sec
+
+
+def ensemble_cpu_rate(kind, procs, budget_cells=1500):
+    """Aggregate cell-updates/s of `procs` concurrent single-thread processes,
+    each running seeded tubes of the ensemble whose cell count is at most
+    `budget_cells` (a bounded sample: cost per cell-update does not depend
+    on the tube length)."""
+    inst = ensemble_instances()
+    small = [k for k, c in enumerate(inst) if len(c[1].x) - 1 <= budget_cells]
+    per = max(1, min(len(small) // max(procs, 1), 4))
+    shares = [small[(p * per) % len(small):(p * per) % len(small) + per] for p in range(procs)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        out = pool.map(_ens_cpu_worker, [(kind, sh) for sh in shares])
+    rate = sum(cu / sec for cu, sec in out if sec > 0)
+    return rate, f"{procs} concurrent single-thread processes x {per} seeded tubes of <= {budget_cells} cells each"
 
 
 def _dist():
@@ -252,23 +314,99 @@ def run_cuda(args):
             step_idx += 2
             out["families"] = fam
         if with_e2e:
-            # end to end through the drop-in entry point sifv_step (dt back to the host each step)
+            # (1) device-resident drop-in (state stays on the GPU, dt back to the host each step)
             torch.cuda.synchronize()
             barrier()
             t0 = time.perf_counter()
             for q in range(args.steps):
                 t_sim += ctx.step(step_idx + q, t_sim, -1.0)
             torch.cuda.synchronize()
-            e2e_s = max_over_ranks(time.perf_counter() - t0)
-            out["e2e"] = ws * cells * args.steps / e2e_s
+            out["e2e_resident"] = ws * cells * args.steps / max_over_ranks(time.perf_counter() - t0)
+            step_idx += args.steps
+            # (2) host-authoritative drop-in: per step the fields the step reads go up
+            # from pinned host buffers, sifv_step runs, the fields it writes come back
+            fids = [getattr(abi, f) for f in E2E_FIELDS_2D]
+            host = {f: torch.from_numpy(ctx.get_field(f).reshape(-1).copy()).pin_memory() for f in fids}
+            set_f, get_f, step_f = ctx.be.fn["set_field"], ctx.be.fn["get_field"], ctx.be.fn["step"]
+            dtv = ctypes.c_double()
+            torch.cuda.synchronize()
+            barrier()
+            t0 = time.perf_counter()
+            for q in range(args.steps):
+                for f in fids:
+                    assert set_f(ctx.h, f, ctypes.c_void_p(host[f].data_ptr()), 0) == 0
+                assert step_f(ctx.h, step_idx + q, t_sim, -1.0, ctypes.byref(dtv)) == 0
+                t_sim += dtv.value
+                for f in fids:
+                    assert get_f(ctx.h, f, ctypes.c_void_p(host[f].data_ptr()), 0) == 0
+            torch.cuda.synchronize()
+            out["e2e"] = ws * cells * args.steps / max_over_ranks(time.perf_counter() - t0)
+            out["e2e_bytes"] = len(fids) * ctx.ncells * 8
         ctx.close()
         return out
+
+    def measure_ensemble(precision, with_clocks=False, with_e2e=False):
+        """The batched-ensemble workload in one launch; returns timing and the
+        per-tube densities (for the mixed-vs-FP64 error)."""
+        inst = ensemble_instances()
+        ns = [len(c[1].x) - 1 for c in inst]
+        cfg = inst[0][0]
+        cfg.precision = precision
+        ens = backends.cuda().create_ensemble(cfg, ns, [0.0] * len(ns), [1.0] * len(ns), device=local)
+        fids = [f for f in inst[0][2] if f != abi.F_SIGMA]
+        packed = {f: torch.from_numpy(ens.pack([c[2][f] for c in inst])).pin_memory() for f in fids}
+        for f in fids:
+            ens.set_field(f, packed[f].numpy())
+        bs = ens.autotune(10)          # also the warm-up launches
+        clk = ClockSampler(local) if with_clocks else None
+        if clk:
+            clk.__enter__()
+        w0 = time.time()
+        times, steps, ms = ens.run(ENS_TEND)
+        if clk:
+            clk.mark(w0, time.time())
+            clk.__exit__(None, None, None)
+        cu = float(np.dot(np.array(ns, dtype=np.float64), steps))
+        rho = [r[ens.ng:-ens.ng].copy() for r in ens.unpack(ens.get_field(abi.F_RHO))]
+        out = {"ms": ms, "value": cu / (ms / 1e3), "cell_updates": cu, "block_size": bs, "rho": rho,
+               "steps_min": int(steps.min()), "steps_max": int(steps.max()), "ncells": sum(ns),
+               "e2e_bytes": len(fids) * ens.ncells * 8, "clocks": clk.summary() if clk else None}
+        ens.close()
+        if with_e2e:
+            # end to end from host buffers: upload the state, run, download it
+            ens2 = backends.cuda().create_ensemble(cfg, ns, [0.0] * len(ns), [1.0] * len(ns), device=local)
+            t0 = time.perf_counter()
+            for f in fids:
+                assert ens2.be.fn["ensemble_set_field"](ens2.h, f, ctypes.c_void_p(packed[f].data_ptr()), 0) == 0
+            ens2.run(ENS_TEND, block_size=bs)
+            for f in fids:
+                assert ens2.be.fn["ensemble_get_field"](ens2.h, f, ctypes.c_void_p(packed[f].data_ptr()), 0) == 0
+            out["e2e"] = cu / (time.perf_counter() - t0)
+            ens2.close()
+        return out
+
+    if args.kernels_only:
+        r = measure(args.precision)
+        if rank == 0:
+            print(json.dumps({"kernels_only": True, "n": n, "precision": PREC_NAMES[args.precision],
+                              "ms_per_step": r["ms"] / args.steps, "value": r["value"]}), flush=True)
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return
 
     main = measure(args.precision, with_clocks=True, with_e2e=True)
     extra = {}
     for p in (0, 1, 2):
         if p != args.precision and not args.quick:
             extra[PREC_NAMES[p]] = measure(p)
+    ens = None
+    if ws == 1 and not args.quick and not args.no_ensemble:
+        emx = measure_ensemble(abi.PREC_MIXED, with_clocks=True, with_e2e=True)
+        e64 = measure_ensemble(abi.PREC_FP64)
+        rel = [np.abs(a - b).mean() / np.abs(b).mean() for a, b in zip(emx["rho"], e64["rho"])]
+        linf = [np.abs(a - b).max() / np.abs(b).max() for a, b in zip(emx["rho"], e64["rho"])]
+        ens = {"mixed": emx, "fp64": e64, "l1_rel_max": float(max(rel)), "l1_rel_mean": float(np.mean(rel)),
+               "linf_rel_max": float(max(linf))}
     ms = main["ms"]
     value = main["value"]
     launches = main["launches"]
@@ -286,6 +424,8 @@ def run_cuda(args):
     dom_ms = fam[dom][0] / fam[dom][1]
     dom_bytes = KERNEL_BYTES_PER_CELL_2D.get(dom, float("nan")) * cells
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    tpc = NCU_DRAM_BYTES_PER_CELL.get((args.precision, dom))
+    traffic = tpc * cells if tpc is not None else None
     result = None
     if rank == 0:
         kind = "reference" if backends.reference(release=True) is not None else "port"
@@ -301,7 +441,8 @@ def run_cuda(args):
                        "precision": PREC_NAMES[args.precision],
                        "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (4 x 134 MB state)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": "ncu dram bytes per cell on the 2048^2 case x cells",
                          "kernel": dom, "bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
                          "peak_source": peak_kind,
                          "step": {"achieved": step_achieved, "frac": step_achieved / peak,
@@ -309,14 +450,40 @@ def run_cuda(args):
                          "kernel_ms_per_step": {k: v[0] / 2 for k, v in fam.items()}},
             "cpu_baseline": {"value": cpu, "unit": UNIT, "cores": 1, "kind": kind,
                              "sample": f"{cpu_n}x{cpu_n} instance, {cpu_steps} steps, 1 thread"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8,
-                    "api": "sifv_step (returns dt to the host every step)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": main["e2e_bytes"],
+                    "d2h_bytes_per_step": main["e2e_bytes"] + 8,
+                    "api": "per step: sifv_set_field x7 from pinned host buffers, sifv_step (dt to the host), "
+                           "sifv_get_field x7 (host-authoritative drop-in)",
+                    "resident_value": main["e2e_resident"],
+                    "resident_api": "sifv_step only, state resident on the GPU (dt to the host each step)"},
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "other_precisions": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
                                      "roofline_frac": BYTES_PER_CELL_UPDATE * v["value"] / 1e9 / peak}
                                  for k, v in extra.items()},
         }
+        if ens is not None:
+            mx, f64 = ens["mixed"], ens["fp64"]
+            ens_cpu, ens_sample = ensemble_cpu_rate(kind, os.cpu_count() or 1)
+            result["ensemble"] = {
+                "workload": f"{ENS_COUNT} two-phase water-air tubes, cells log-uniform [{ENS_NMIN},{ENS_NMAX}] "
+                            f"(seed {ENS_SEED}, {mx['ncells']} cells), WENO5 + mixture HLLC, SSP-RK3 CFL0.5, "
+                            f"t_end={ENS_TEND}, one launch",
+                "metric": "cell-updates/s", "value": mx["value"], "precision": "mixed-fp32-bulk",
+                "seconds": mx["ms"] / 1e3, "cell_updates": mx["cell_updates"],
+                "steps_min_max": [mx["steps_min"], mx["steps_max"]], "threads_per_tube": mx["block_size"],
+                "fp64": {"value": f64["value"], "seconds": f64["ms"] / 1e3, "threads_per_tube": f64["block_size"]},
+                "mixed_vs_fp64_rho": {"l1_rel_max": ens["l1_rel_max"], "l1_rel_mean": ens["l1_rel_mean"],
+                                      "linf_rel_max": ens["linf_rel_max"]},
+                "roofline": {"bound": "hbm", "bytes_per_cell_update": ENS_BYTES_PER_CELL_UPDATE,
+                             "achieved": ENS_BYTES_PER_CELL_UPDATE * mx["value"] / 1e9, "peak": peak,
+                             "unit": "GB/s", "frac": ENS_BYTES_PER_CELL_UPDATE * mx["value"] / 1e9 / peak},
+                "e2e": {"value": mx["e2e"], "h2d_bytes": mx["e2e_bytes"], "d2h_bytes": mx["e2e_bytes"],
+                        "api": "sifv_ensemble_set_field x9, sifv_ensemble_run, sifv_ensemble_get_field x9"},
+                "cpu_baseline": {"value": ens_cpu, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": kind,
+                                 "sample": ens_sample},
+                "clocks": mx["clocks"],
+            }
         print(json.dumps(result), flush=True)
     if ws > 1:
         torch.distributed.destroy_process_group()
@@ -331,7 +498,10 @@ def main():
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--precision", type=int, default=2, choices=[0, 1, 2],
                     help="0 reference-ordered FP64, 1 mixed (FP32 bulk), 2 fast FP64 (default)")
-    ap.add_argument("--quick", action="store_true", help="skip the other precisions")
+    ap.add_argument("--quick", action="store_true", help="skip the other precisions and the ensemble")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble workload")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only the device-timed step loop (no clocks, e2e, CPU baseline): a small case to profile")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
