@@ -235,6 +235,36 @@ int sifv_profile_step(sifv_ctx_t* ctx, int step, double time, double targetDt, c
  * call, and the number of kernel launches it made. */
 int sifv_last_step_stats(const sifv_ctx_t* ctx, double* deviceMs, int* launches);
 
+/* ---- discrete adjoint and tangent of the explicit step ------------------ */
+/* Reverse- and forward-mode derivatives of the map U(t0) -> U(tEnd) that
+ * sifv_step iterates (ExplicitSolver::step, src/ExplicitSolver.cpp:68-203:
+ * cons -> prim, PRIM ghost fill, WENO5 / UPWIND5 reconstruction, Riemann
+ * flux, flux divergence, SSP-RK stages), single-phase, SIFV_PREC_FP64, no
+ * IGR or body force.  The time-step sequence is held fixed (the CFL minimum
+ * is not differentiable); every branch (HLLC wave pattern, wave-speed
+ * estimates, clamps) is the one the forward pass took.
+ *
+ * sifv_adjoint_forward runs the forward from the context's state, with the
+ * CFL dt and targetDt = tEnd - t (as the reference's time loop) or with the
+ * given dt sequence, records the sequence and a checkpoint of the
+ * conservative state every checkpointEvery steps.  sifv_adjoint_set_seed
+ * sets dJ/dU(tEnd) (interior cells; ghosts ignored); sifv_adjoint_backward
+ * recomputes each checkpoint segment (storing its stage states) and sweeps
+ * it in reverse; sifv_adjoint_get_gradient then returns dJ/dU(t0) (ghost
+ * entries zero) and the context's state is the forward end state again.
+ * sifv_tangent_forward advances the state and the direction set by
+ * sifv_tangent_set_direction together (dU(tEnd) by sifv_tangent_get). */
+int sifv_adjoint_forward(sifv_ctx_t* ctx, int step0, double time0, double tEnd, int maxSteps, int checkpointEvery,
+                         const double* dtSchedule, int nSchedule, double* timeOut, int* stepsOut);
+int sifv_adjoint_schedule(const sifv_ctx_t* ctx, double* dts, int cap, int* n);
+int sifv_adjoint_set_seed(sifv_ctx_t* ctx, int field, const double* seed, int onDevice);
+int sifv_adjoint_backward(sifv_ctx_t* ctx, double* deviceMs);
+int sifv_adjoint_get_gradient(sifv_ctx_t* ctx, int field, double* grad, int onDevice);
+int sifv_tangent_set_direction(sifv_ctx_t* ctx, int field, const double* dir, int onDevice);
+int sifv_tangent_forward(sifv_ctx_t* ctx, int step0, double time0, double tEnd, int maxSteps,
+                         const double* dtSchedule, int nSchedule, double* timeOut, int* stepsOut);
+int sifv_tangent_get(sifv_ctx_t* ctx, int field, double* out, int onDevice);
+
 /* ---- batched ensembles -------------------------------------------------- */
 /* Many independent 1D problems of different sizes (same configuration and
  * boundary conditions, own mesh [xLo[k], xHi[k]] with nCells[k] cells)

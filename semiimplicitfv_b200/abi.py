@@ -168,6 +168,16 @@ _OPTIONAL_SIGS = {
     "config_validate": (C.c_int, [C.POINTER(Config)]),
     "profile_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_char_p, C.c_int,
                                C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
+    "adjoint_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
+                                  C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "adjoint_schedule": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_int)]),
+    "adjoint_set_seed": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "adjoint_backward": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "adjoint_get_gradient": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "tangent_set_direction": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "tangent_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
+                                  C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "tangent_get": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "ensemble_create": (C.c_int, [C.POINTER(Config), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                   C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_void_p)]),
     "ensemble_destroy": (C.c_int, [C.c_void_p]),
@@ -341,6 +351,63 @@ class Context:
         t, n = C.c_double(), C.c_int()
         self._check(self.be.fn["advance"](self.h, step0, time0, t_end, n_steps, C.byref(t), C.byref(n)))
         return t.value, n.value
+
+    # ---- discrete adjoint / tangent (explicit single-phase FP64 step) ----
+    @staticmethod
+    def _sched(schedule):
+        if schedule is None:
+            return None, 0, None
+        a = np.ascontiguousarray(schedule, dtype=np.float64)
+        return a.ctypes.data_as(C.POINTER(C.c_double)), a.size, a
+
+    def adjoint_forward(self, step0: int, time0: float, t_end: float, max_steps: int = 0, every: int = 32,
+                        schedule=None):
+        """Forward run recording the dt sequence and checkpoints; returns (time, steps)."""
+        p, n, keep = self._sched(schedule)
+        t, k = C.c_double(), C.c_int()
+        self._check(self.be.fn["adjoint_forward"](self.h, step0, time0, t_end, max_steps, every, p, n,
+                                                  C.byref(t), C.byref(k)))
+        return t.value, k.value
+
+    def adjoint_schedule(self) -> np.ndarray:
+        n = C.c_int()
+        self._check(self.be.fn["adjoint_schedule"](self.h, None, 0, C.byref(n)))
+        out = np.empty(n.value)
+        self._check(self.be.fn["adjoint_schedule"](self.h, out.ctypes.data_as(C.POINTER(C.c_double)), n.value,
+                                                   C.byref(n)))
+        return out
+
+    def adjoint_set_seed(self, fid: int, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        assert a.size == self.ncells
+        self._check(self.be.fn["adjoint_set_seed"](self.h, fid, a.ctypes.data, 0))
+
+    def adjoint_backward(self) -> float:
+        ms = C.c_double()
+        self._check(self.be.fn["adjoint_backward"](self.h, C.byref(ms)))
+        return ms.value
+
+    def adjoint_get_gradient(self, fid: int) -> np.ndarray:
+        out = np.empty(self.ncells)
+        self._check(self.be.fn["adjoint_get_gradient"](self.h, fid, out.ctypes.data, 0))
+        return out.reshape(self.shape)
+
+    def tangent_set_direction(self, fid: int, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        assert a.size == self.ncells
+        self._check(self.be.fn["tangent_set_direction"](self.h, fid, a.ctypes.data, 0))
+
+    def tangent_forward(self, step0: int, time0: float, t_end: float, max_steps: int = 0, schedule=None):
+        p, n, keep = self._sched(schedule)
+        t, k = C.c_double(), C.c_int()
+        self._check(self.be.fn["tangent_forward"](self.h, step0, time0, t_end, max_steps, p, n,
+                                                  C.byref(t), C.byref(k)))
+        return t.value, k.value
+
+    def tangent_get(self, fid: int) -> np.ndarray:
+        out = np.empty(self.ncells)
+        self._check(self.be.fn["tangent_get"](self.h, fid, out.ctypes.data, 0))
+        return out.reshape(self.shape)
 
     def last_pressure_iterations(self) -> int:
         it = C.c_int()

@@ -7,10 +7,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
 #include "sifv.h"
+#include "sifv_adjoint_api.h"
 #include "sifv_kernels.cuh"
 #include "sifv_sweep_api.h"
 
@@ -56,6 +58,22 @@ struct sifv_ctx {
     double* rhsBuf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* invW[3] = {nullptr, nullptr, nullptr};
     double* rhoP = nullptr;
+    // discrete adjoint / tangent (sifv_adjoint_*, sifv_tangent_*)
+    double forcedDt = -1.0;                   // > 0: the steps use this dt (no CFL reduction)
+    std::function<int(int, int)> stageHook;   // (stage, phase): 0 before the prim fill, 1 before the update, 2 after
+    int adjEvery = 0;
+    std::vector<double> adjDts;               // time-step sequence of the recorded forward run
+    std::vector<double*> adjCkpt;             // (dim + 2) arrays per checkpoint, then the final state
+    double* adjStage = nullptr;               // stage inputs of one segment
+    size_t adjStageCap = 0;
+    bool adjReady = false;
+    double* lam[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double* acc0[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double* share[3] = {nullptr, nullptr, nullptr};
+    double* tan[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double* tan0[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double* tanW[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double* tanF[3][5] = {};
 };
 
 namespace {
@@ -343,6 +361,9 @@ void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
         k_dt_advective<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.siCfl);
         k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, -1.0, targetDt, 1, cfg.siMinDt, cfg.siMaxDt, useEnd ? 1 : 0);
         c->launches += 3;
+    } else if (c->forcedDt > 0) {
+        k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, c->forcedDt, -1.0, 0, 0.0, 0.0, 0);
+        c->launches += 1;
     } else {
         if (cfg.constDt <= 0) {
             k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, cfg.maxDt);
@@ -401,6 +422,7 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
         StageCoef K{};
         rk_coef(cfg.RKOrder, s, K);
         body_force(cfg, time, K);
+        if (c->stageHook && c->stageHook(s, 0) != 0) return SIFV_ERR_CUDA;
         launch_prim_bc(c);
         if (cfg.useIGR) {
             int st = igr_solve(c, step);
@@ -408,10 +430,12 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
         }
         for (int d = 0; d < P.dim; ++d) launch_face(c, d);
         if (!cfg.semiImplicit) {
+            if (c->stageHook && c->stageHook(s, 1) != 0) return SIFV_ERR_CUDA;
             NPH_DISPATCH(c, (k_assemble<NPHV, 0><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, K)));
             c->launches++;
             mark(c, "assemble");
             LAUNCH_CHECK(c);
+            if (c->stageHook && c->stageHook(s, 2) != 0) return SIFV_ERR_CUDA;
         } else {
             NPH_DISPATCH(c, (k_assemble<NPHV, 1><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, K)));
             c->launches++;
@@ -652,6 +676,8 @@ int sifv_destroy(sifv_ctx_t* c) {
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->ownStream) cudaStreamDestroy(c->ownStream);
+    for (double* p : c->adjCkpt) cudaFree(p);
+    if (c->adjStage) cudaFree(c->adjStage);
     delete c;
     return SIFV_OK;
 }
@@ -903,3 +929,384 @@ int sifv_apply_bc(sifv_ctx_t* c) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Discrete adjoint and tangent of the explicit step
+// ===========================================================================
+namespace {
+
+int nv_of(const sifv_ctx* c) { return c->cfg.dim + 2; }
+
+// slot q of the conservative state: 0 rho, 1..dim momenta, dim + 1 energy
+double* cons_field(sifv_ctx* c, int q) {
+    const int dim = c->cfg.dim;
+    if (q == 0) return c->F.rho;
+    if (q == dim + 1) return c->F.rhoE;
+    return (q == 1) ? c->F.rhoU : (q == 2) ? c->F.rhoV : c->F.rhoW;
+}
+
+int cons_slot(const sifv_ctx* c, int field) {
+    const int dim = c->cfg.dim;
+    switch (field) {
+        case SIFV_F_RHO: return 0;
+        case SIFV_F_RHOU: return 1;
+        case SIFV_F_RHOV: return dim >= 2 ? 2 : -1;
+        case SIFV_F_RHOW: return dim >= 3 ? 3 : -1;
+        case SIFV_F_RHOE: return dim + 1;
+        default: return -1;
+    }
+}
+
+int adjoint_supported(sifv_ctx* c) {
+    const sifv_config_t& g = c->cfg;
+    if (g.semiImplicit || g.useIGR || g.nPhases > 0 || has_body_force(g) || g.precision != SIFV_PREC_FP64 ||
+        (g.reconOrder != SIFV_WENO5 && g.reconOrder != SIFV_UPWIND5) || g.nGhost > 7)
+        return fail(c, SIFV_ERR_UNSUPPORTED,
+                    "the adjoint / tangent covers the explicit single-phase WENO5 / UPWIND5 step in SIFV_PREC_FP64 "
+                    "without IGR or body force (nGhost <= 7)");
+    return SIFV_OK;
+}
+
+size_t face_count(const Params& P, int d) {
+    return (size_t)(P.nx + (d == 0)) * (P.ny + (d == 1)) * (P.nz + (d == 2));
+}
+
+int ensure_adj_arrays(sifv_ctx* c, bool tangent) {
+    int st = SIFV_OK;
+    const int nv = nv_of(c), dim = c->cfg.dim;
+    if (!tangent && !c->lam[0]) {
+        for (int q = 0; q < nv; ++q) {
+            c->lam[q] = dalloc(c, c->ncells, st);
+            c->acc0[q] = dalloc(c, c->ncells, st);
+        }
+        for (int d = 0; d < dim; ++d) c->share[d] = dalloc(c, face_count(c->P, d) * 10 * nv, st);
+    }
+    if (tangent && !c->tan[0]) {
+        for (int q = 0; q < nv; ++q) {
+            c->tan[q] = dalloc(c, c->ncells, st);
+            c->tan0[q] = dalloc(c, c->ncells, st);
+            c->tanW[q] = dalloc(c, c->ncells, st);
+        }
+        for (int d = 0; d < dim; ++d)
+            for (int q = 0; q < nv; ++q) c->tanF[d][q] = dalloc(c, face_count(c->P, d), st);
+    }
+    return st;
+}
+
+AdjArgs adj_args(sifv_ctx* c) {
+    AdjArgs A{};
+    A.P = c->P;
+    A.F = c->F;
+    for (int q = 0; q < 5; ++q) {
+        A.lam[q] = c->lam[q];
+        A.acc0[q] = c->acc0[q];
+        A.tan[q] = c->tan[q];
+        A.tan0[q] = c->tan0[q];
+        A.tanW[q] = c->tanW[q];
+    }
+    for (int d = 0; d < 3; ++d) {
+        A.share[d] = c->share[d];
+        for (int q = 0; q < 5; ++q) A.tanF[d][q] = c->tanF[d][q];
+    }
+    return A;
+}
+
+void set_stage_coef(AdjArgs& A, int order, int s) {
+    StageCoef K{};
+    rk_coef(order, s, K);
+    A.a1 = K.c1 / K.c4;
+    A.a2 = K.c2 / K.c4;
+    A.a3 = K.c3 / K.c4;
+}
+
+void free_checkpoints(sifv_ctx* c) {
+    for (double* p : c->adjCkpt) cudaFree(p);
+    c->adjCkpt.clear();
+    c->adjDts.clear();
+    c->adjReady = false;
+}
+
+// copy of the conservative state appended to the checkpoint list
+int push_checkpoint(sifv_ctx* c) {
+    for (int q = 0; q < nv_of(c); ++q) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, c->ncells * sizeof(double)) != cudaSuccess)
+            return fail(c, SIFV_ERR_CUDA, "cudaMalloc for an adjoint checkpoint failed");
+        c->adjCkpt.push_back(static_cast<double*>(p));
+        CUDA_TRY(c, cudaMemcpyAsync(p, cons_field(c, q), c->ncells * sizeof(double), cudaMemcpyDeviceToDevice,
+                                    c->stream));
+    }
+    return SIFV_OK;
+}
+
+int load_checkpoint(sifv_ctx* c, size_t idx) {
+    const int nv = nv_of(c);
+    for (int q = 0; q < nv; ++q)
+        CUDA_TRY(c, cudaMemcpyAsync(cons_field(c, q), c->adjCkpt[idx * nv + q], c->ncells * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    return SIFV_OK;
+}
+
+struct HookGuard {
+    sifv_ctx* c;
+    ~HookGuard() {
+        c->stageHook = nullptr;
+        c->forcedDt = -1.0;
+    }
+};
+
+// Forward steps from the current state, either with a given time-step
+// sequence or with the CFL dt and targetDt = tEnd - t; optionally records
+// the sequence and a checkpoint every `every` steps.
+int run_forward(sifv_ctx* c, int step0, double time0, double tEnd, int maxSteps, const double* sched, int nSched,
+                int every, bool record, double& timeOut, int& stepsOut) {
+    double t = time0;
+    int q = 0;
+    for (;;) {
+        if (sched) {
+            if (q >= nSched) break;
+        } else if (!(t < tEnd) || (maxSteps > 0 && q >= maxSteps)) {
+            break;
+        }
+        if (record && q % every == 0) {
+            int st = push_checkpoint(c);
+            if (st != SIFV_OK) return st;
+        }
+        c->forcedDt = sched ? sched[q] : -1.0;
+        CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
+        int status = SIFV_OK;
+        int st = enqueue_step(c, step0 + q, t, sched ? -1.0 : tEnd - t, false, status);
+        c->forcedDt = -1.0;
+        if (st != SIFV_OK) return st;
+        CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        const double dt = c->ctlHost->dt;
+        if (!(dt > 0.0)) return fail(c, SIFV_ERR_NAN, "time step not positive (state blew up)");
+        if (record) c->adjDts.push_back(dt);
+        t += dt;
+        ++q;
+    }
+    timeOut = t;
+    stepsOut = q;
+    return SIFV_OK;
+}
+
+int check_ctx(sifv_ctx* c) {
+    if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
+    cudaSetDevice(c->device);
+    return adjoint_supported(c);
+}
+
+int copy_slot(sifv_ctx* c, double* const* arr, int field, const double* src, double* dst, int onDevice) {
+    const int q = cons_slot(c, field);
+    if (q < 0) return fail(c, SIFV_ERR_BAD_ARG, "field is not a conservative variable of this configuration");
+    const size_t bytes = c->ncells * sizeof(double);
+    if (src)
+        CUDA_TRY(c, cudaMemcpyAsync(arr[q], src, bytes, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    c->stream));
+    else
+        CUDA_TRY(c, cudaMemcpyAsync(dst, arr[q], bytes, onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                    c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SIFV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sifv_adjoint_forward(sifv_ctx_t* c, int step0, double time0, double tEnd, int maxSteps, int checkpointEvery,
+                         const double* dtSchedule, int nSchedule, double* timeOut, int* stepsOut) {
+    int st = check_ctx(c);
+    if (st != SIFV_OK) return st;
+    if (checkpointEvery <= 0) return fail(c, SIFV_ERR_BAD_ARG, "checkpointEvery must be > 0");
+    if (!dtSchedule && !(tEnd < 1e300) && maxSteps <= 0)
+        return fail(c, SIFV_ERR_BAD_ARG, "tEnd must be finite when there is no step limit");
+    free_checkpoints(c);
+    c->adjEvery = checkpointEvery;
+    HookGuard guard{c};
+    double t = 0.0;
+    int n = 0;
+    st = run_forward(c, step0, time0, tEnd, maxSteps, dtSchedule, nSchedule, checkpointEvery, true, t, n);
+    if (st != SIFV_OK) {
+        free_checkpoints(c);
+        return st;
+    }
+    st = push_checkpoint(c);   // final state, restored after the reverse sweep
+    if (st != SIFV_OK) {
+        free_checkpoints(c);
+        return st;
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->adjReady = true;
+    if (timeOut) *timeOut = t;
+    if (stepsOut) *stepsOut = n;
+    return SIFV_OK;
+}
+
+int sifv_adjoint_schedule(const sifv_ctx_t* c, double* dts, int cap, int* n) {
+    if (!c || !n) return SIFV_ERR_BAD_ARG;
+    *n = (int)c->adjDts.size();
+    if (dts) std::memcpy(dts, c->adjDts.data(), sizeof(double) * std::min<size_t>(cap > 0 ? cap : 0, c->adjDts.size()));
+    return SIFV_OK;
+}
+
+int sifv_adjoint_set_seed(sifv_ctx_t* c, int field, const double* src, int onDevice) {
+    int st = check_ctx(c);
+    if (st != SIFV_OK) return st;
+    if (!src) return fail(c, SIFV_ERR_BAD_ARG, "null seed");
+    st = ensure_adj_arrays(c, false);
+    if (st != SIFV_OK) return st;
+    return copy_slot(c, c->lam, field, src, nullptr, onDevice);
+}
+
+int sifv_adjoint_get_gradient(sifv_ctx_t* c, int field, double* dst, int onDevice) {
+    int st = check_ctx(c);
+    if (st != SIFV_OK) return st;
+    if (!dst) return fail(c, SIFV_ERR_BAD_ARG, "null output");
+    st = ensure_adj_arrays(c, false);
+    if (st != SIFV_OK) return st;
+    return copy_slot(c, c->lam, field, nullptr, dst, onDevice);
+}
+
+int sifv_adjoint_backward(sifv_ctx_t* c, double* deviceMs) {
+    int st = check_ctx(c);
+    if (st != SIFV_OK) return st;
+    if (!c->adjReady) return fail(c, SIFV_ERR_BAD_ARG, "no recorded forward run: call sifv_adjoint_forward first");
+    st = ensure_adj_arrays(c, false);
+    if (st != SIFV_OK) return st;
+    const int nv = nv_of(c), RK = c->cfg.RKOrder, K = c->adjEvery, dim = c->cfg.dim;
+    const int nSteps = (int)c->adjDts.size();
+    const size_t nc = c->ncells;
+    const size_t need = (size_t)K * RK * nv * nc;
+    if (c->adjStageCap < need) {
+        if (c->adjStage) cudaFree(c->adjStage);
+        c->adjStage = nullptr;
+        c->adjStageCap = 0;
+        void* p = nullptr;
+        if (cudaMalloc(&p, need * sizeof(double)) != cudaSuccess)
+            return fail(c, SIFV_ERR_CUDA, "cudaMalloc for the adjoint stage states failed (lower checkpointEvery)");
+        c->adjStage = static_cast<double*>(p);
+        c->adjStageCap = need;
+    }
+    for (int q = 0; q < nv; ++q) CUDA_TRY(c, cudaMemsetAsync(c->acc0[q], 0, nc * sizeof(double), c->stream));
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+    HookGuard guard{c};
+    const int nSeg = (nSteps + K - 1) / K;
+    for (int seg = nSeg - 1; seg >= 0; --seg) {
+        const int q0 = seg * K, q1 = std::min(q0 + K, nSteps);
+        st = load_checkpoint(c, (size_t)seg);
+        if (st != SIFV_OK) return st;
+        // recompute the segment, keeping every stage input
+        int qLocal = 0;
+        c->stageHook = [&](int s, int phase) -> int {
+            if (phase != 0) return 0;
+            double* dst = c->adjStage + (size_t)(qLocal * RK + s) * nv * nc;
+            for (int v = 0; v < nv; ++v)
+                if (cudaMemcpyAsync(dst + v * nc, cons_field(c, v), nc * sizeof(double), cudaMemcpyDeviceToDevice,
+                                    c->stream) != cudaSuccess)
+                    return -1;
+            return 0;
+        };
+        for (int q = q0; q < q1; ++q) {
+            qLocal = q - q0;
+            c->forcedDt = c->adjDts[q];
+            CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
+            int status = SIFV_OK;
+            st = enqueue_step(c, q, 0.0, -1.0, false, status);
+            if (st != SIFV_OK) return st;
+        }
+        c->stageHook = nullptr;
+        c->forcedDt = -1.0;
+        // reverse through the segment
+        for (int q = q1 - 1; q >= q0; --q) {
+            for (int s = RK - 1; s >= 0; --s) {
+                Fields Fs = c->F;
+                double* src = c->adjStage + (size_t)((q - q0) * RK + s) * nv * nc;
+                Fs.rho = src;
+                Fs.rhoU = src + nc;
+                if (dim >= 2) Fs.rhoV = src + 2 * nc;
+                if (dim >= 3) Fs.rhoW = src + 3 * nc;
+                Fs.rhoE = src + (size_t)(dim + 1) * nc;
+                k_prim_bc<0><<<blocks((long long)nc, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, Fs, nullptr, 0);
+                AdjArgs A = adj_args(c);
+                A.F = Fs;
+                set_stage_coef(A, RK, s);
+                A.dt = c->adjDts[q];
+                A.dtDev = nullptr;
+                A.stage0 = (s == 0) ? 1 : 0;
+                if (adjoint_stage(A, c->stream) != 0) {
+                    LAUNCH_CHECK(c);
+                    return fail(c, SIFV_ERR_CUDA, "adjoint launch failed");
+                }
+            }
+        }
+        LAUNCH_CHECK(c);
+    }
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    // the context's state is the end of the forward run again
+    st = load_checkpoint(c, (size_t)nSeg);
+    if (st != SIFV_OK) return st;
+    launch_prim_bc(c);
+    for (int q = 0; q < nv; ++q)
+        if (zero_ghosts(c->P, c->lam[q], c->stream) != 0) return fail(c, SIFV_ERR_CUDA, "launch failed");
+    LAUNCH_CHECK(c);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (deviceMs) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        *deviceMs = ms;
+    }
+    return SIFV_OK;
+}
+
+int sifv_tangent_set_direction(sifv_ctx_t* c, int field, const double* src, int onDevice) {
+    int st = check_ctx(c);
+    if (st != SIFV_OK) return st;
+    if (!src) return fail(c, SIFV_ERR_BAD_ARG, "null direction");
+    st = ensure_adj_arrays(c, true);
+    if (st != SIFV_OK) return st;
+    return copy_slot(c, c->tan, field, src, nullptr, onDevice);
+}
+
+int sifv_tangent_get(sifv_ctx_t* c, int field, double* dst, int onDevice) {
+    int st = check_ctx(c);
+    if (st != SIFV_OK) return st;
+    if (!dst) return fail(c, SIFV_ERR_BAD_ARG, "null output");
+    st = ensure_adj_arrays(c, true);
+    if (st != SIFV_OK) return st;
+    return copy_slot(c, c->tan, field, nullptr, dst, onDevice);
+}
+
+int sifv_tangent_forward(sifv_ctx_t* c, int step0, double time0, double tEnd, int maxSteps, const double* dtSchedule,
+                         int nSchedule, double* timeOut, int* stepsOut) {
+    int st = check_ctx(c);
+    if (st != SIFV_OK) return st;
+    if (!dtSchedule && !(tEnd < 1e300) && maxSteps <= 0)
+        return fail(c, SIFV_ERR_BAD_ARG, "tEnd must be finite when there is no step limit");
+    st = ensure_adj_arrays(c, true);
+    if (st != SIFV_OK) return st;
+    const int RK = c->cfg.RKOrder;
+    HookGuard guard{c};
+    c->stageHook = [&](int s, int phase) -> int {
+        if (phase == 0) return 0;
+        AdjArgs A = adj_args(c);
+        set_stage_coef(A, RK, s);
+        A.dtDev = &c->ctl->dt;
+        if (phase == 1) return tangent_faces(A, c->stream);
+        return tangent_update(A, (s == 0 && RK > 1) ? 1 : 0, c->stream);
+    };
+    double t = 0.0;
+    int n = 0;
+    st = run_forward(c, step0, time0, tEnd, maxSteps, dtSchedule, nSchedule, 1, false, t, n);
+    if (st != SIFV_OK) return st;
+    for (int q = 0; q < nv_of(c); ++q)
+        if (zero_ghosts(c->P, c->tan[q], c->stream) != 0) return fail(c, SIFV_ERR_CUDA, "launch failed");
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (timeOut) *timeOut = t;
+    if (stepsOut) *stepsOut = n;
+    return SIFV_OK;
+}
+
+}  // extern "C"
+

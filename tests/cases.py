@@ -131,6 +131,32 @@ def acoustic3d(n=16, semi=True, igr=True, rk=1, recon=abi.WENO5, riemann=abi.HLL
     return cfg, abi.MeshSpec(x, x, x, bc=[BC_PERIODIC] * 6), fields
 
 
+def vortex2d(n=512, beta=5.0, L=10.0, cfl=0.6, recon=abi.WENO5, riemann=abi.HLLC, rk=3):
+    """Isentropic vortex (Shu; examples/2D_isentropic_vortex/2D_isentropic_vortex.cpp:65-94)
+    on the periodic square [-L/2, L/2]^2 centred at the origin, free stream
+    (rho, u, v, p) = (1, 1, 1, 1), R = 1 (T_inf = 1), gamma 1.4."""
+    g = 1.4
+    cfg = abi.config_defaults(dim=2, nGhost=3, RKOrder=rk, reconOrder=recon, riemannSolver=riemann, cfl=cfl,
+                              maxDt=1.0)
+    x = abi.linspace_nodes(n, -0.5 * L, 0.5 * L)
+    c = _centroids(x)
+    X, Y = np.meshgrid(c, c, indexing="xy")
+    dx = X - L * np.round(X / L)
+    dy = Y - L * np.round(Y / L)
+    r2 = dx * dx + dy * dy
+    f = np.exp(0.5 * (1.0 - r2))
+    f2 = np.exp(1.0 - r2)
+    du = -beta / (2.0 * np.pi) * dy * f
+    dv = beta / (2.0 * np.pi) * dx * f
+    dT = -(g - 1.0) * beta * beta / (8.0 * g * np.pi * np.pi) * f2
+    T = 1.0 + dT
+    rho = T ** (1.0 / (g - 1.0))
+    p = T ** (g / (g - 1.0))
+    shape = _ext_shape(cfg, n, n, 1)
+    fields = _single_phase_fields(cfg, shape, rho[None], (1.0 + du)[None], (1.0 + dv)[None], None, p[None], g)
+    return cfg, abi.MeshSpec(x, x, bc=[BC_PERIODIC] * 6), fields
+
+
 def water_air(n=256, x_interface=0.5, p_left=5e8, rho_air=1.0, cfl=0.5, recon=abi.WENO5, riemann=abi.HLLC,
               ng=3, alpha_min=1e-8, rk=3):
     """1D two-phase water-air shock tube (examples/1D_liquid_gas_shocktube/
