@@ -57,6 +57,13 @@ E2E_FIELDS_2D = ("F_RHO", "F_RHOU", "F_RHOV", "F_RHOE", "F_VELU", "F_VELV", "F_P
 # Batched ensemble of two-phase water-air tubes: count, cell range, end time.
 ENS_COUNT, ENS_NMIN, ENS_NMAX, ENS_TEND, ENS_SEED = 2048, 256, 16384, 1e-4, 0
 ENS_BYTES_PER_CELL_UPDATE = 384   # state alphaRho0, alphaRho1, rhoU, rhoE, alpha0, alpha1: 64 B x 6
+# Semi-implicit 3D acoustic pulse with IGR, 256^3 periodic, RK1: 20 timed steps.
+# Algorithmic bytes per cell-update: 272 + 32 per IGR sweep + 40 per Jacobi iteration.
+SI_N, SI_STEPS, SI_WARM = 256, 20, 3
+# Discrete adjoint: isentropic vortex 512^2 to t = 2, checkpoint every 32 steps.
+# Algorithmic bytes per adjoint cell-update: forward recompute 256 + store and
+# read the three stage states 2 x 96 + adjoint state read/write per stage 3 x 64.
+ADJ_N, ADJ_TEND, ADJ_EVERY, ADJ_BYTES_PER_CELL_UPDATE = 512, 2.0, 32, 640
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -180,6 +187,23 @@ def ensemble_cpu_rate(kind, procs, budget_cells=1500):
         out = pool.map(_ens_cpu_worker, [(kind, sh) for sh in shares])
     rate = sum(cu / sec for cu, sec in out if sec > 0)
     return rate, f"{procs} concurrent single-thread processes x {per} seeded tubes of <= {budget_cells} cells each"
+
+
+def semi_cpu_rate(kind, n=64, steps=2):
+    """Reference (or oracle) semi-implicit 3D step on one core: an n^3
+    instance of the same problem, `steps` steps after step 0 (the IGR warm
+    start).  Fewer Jacobi iterations than at 256^3 (they grow with n), so
+    this overstates the CPU rate per cell at the full size."""
+    import backends
+    import cases
+    be = backends.reference(release=True) if kind == "reference" else backends.oracle()
+    ctx = backends.make(be, cases.acoustic3d(n))
+    t = ctx.step(0, 0.0, -1.0)
+    t0 = time.perf_counter()
+    for s in range(steps):
+        t += ctx.step(1 + s, t, -1.0)
+    sec = time.perf_counter() - t0
+    return n ** 3 * steps / sec, f"{n}^3 instance, {steps} steps after the warm-start step, 1 thread"
 
 
 def _dist():
@@ -385,6 +409,66 @@ def run_cuda(args):
             ens2.close()
         return out
 
+    def measure_semi_implicit():
+        """Semi-implicit step with IGR and the Jacobi pressure solve."""
+        case = cases.acoustic3d(SI_N)
+        ctx = backends.cuda().create(case[0], case[1], local)
+        ctx.set_state(case[2])
+        t_sim = 0.0
+        for q in range(SI_WARM):                   # step 0 runs the 50-sweep IGR warm start
+            t_sim += ctx.step(q, t_sim, -1.0)
+        iters = []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for q in range(SI_STEPS):
+            t_sim += ctx.step(SI_WARM + q, t_sim, -1.0)
+            iters.append(ctx.last_pressure_iterations())
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        fam = ctx.profile_step(SI_WARM + SI_STEPS, t_sim, -1.0)
+        ctx.close()
+        cells = SI_N ** 3
+        val = cells * SI_STEPS / sec
+        kj = float(np.mean(iters))
+        nigr = case[0].IGRIters
+        bpc = 272 + 32 * nigr + 40 * kj
+        return {"workload": f"3D acoustic pulse {SI_N}^3 periodic, semi-implicit RK1 + IGR ({nigr} sweeps), "
+                            f"WENO5+HLLC, advective CFL 0.8 (dt = maxDt 1e-2), Jacobi tol 1e-6",
+                "metric": "cell-updates/s", "value": val, "steps": SI_STEPS, "ms_per_step": sec / SI_STEPS * 1e3,
+                "precision": "fp64", "jacobi_iterations": iters,
+                "family_ms_per_step": {k: v[0] for k, v in fam.items()},
+                "roofline": {"bound": "hbm", "bytes_per_cell_update": bpc, "achieved": bpc * val / 1e9,
+                             "unit": "GB/s"}}
+
+    def measure_adjoint():
+        """Forward (recording) and reverse sweep of the vortex adjoint."""
+        case = cases.vortex2d(ADJ_N)
+        ctx = backends.cuda().create(case[0], case[1], local)
+        ctx.set_state(case[2])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, steps = ctx.adjoint_forward(0, 0.0, ADJ_TEND, 0, ADJ_EVERY)
+        fwd_s = time.perf_counter() - t0
+        fids = [abi.F_RHO, abi.F_RHOU, abi.F_RHOV, abi.F_RHOE]
+        seed = np.zeros(ctx.shape)
+        ctx.interior(seed)[...] = 1.0
+        for f in fids:
+            ctx.adjoint_set_seed(f, seed)
+        ctx.adjoint_backward()                       # warm-up (allocates the stage store)
+        for f in fids:
+            ctx.adjoint_set_seed(f, seed)
+        bwd_ms = ctx.adjoint_backward()
+        cells = ADJ_N * ADJ_N
+        ctx.close()
+        val = cells * steps / (bwd_ms / 1e3)
+        return {"workload": f"isentropic vortex {ADJ_N}x{ADJ_N} periodic, WENO5+HLLC SSP-RK3 CFL0.6 to t={ADJ_TEND}, "
+                            f"gradient of U(t_end) w.r.t. U(0), checkpoint every {ADJ_EVERY} steps",
+                "metric": "adjoint cell-updates/s", "value": val, "steps": steps,
+                "backward_seconds": bwd_ms / 1e3, "forward_seconds_recording": fwd_s,
+                "forward_value": cells * steps / fwd_s, "precision": "fp64",
+                "roofline": {"bound": "hbm", "bytes_per_cell_update": ADJ_BYTES_PER_CELL_UPDATE,
+                             "achieved": ADJ_BYTES_PER_CELL_UPDATE * val / 1e9, "unit": "GB/s"}}
+
     if args.kernels_only:
         r = measure(args.precision)
         if rank == 0:
@@ -399,6 +483,12 @@ def run_cuda(args):
     for p in (0, 1, 2):
         if p != args.precision and not args.quick:
             extra[PREC_NAMES[p]] = measure(p)
+    adj = None
+    if ws == 1 and not args.quick and not args.no_adjoint:
+        adj = measure_adjoint()
+    semi = None
+    if ws == 1 and not args.quick and not args.no_semi:
+        semi = measure_semi_implicit()
     ens = None
     if ws == 1 and not args.quick and not args.no_ensemble:
         emx = measure_ensemble(abi.PREC_MIXED, with_clocks=True, with_e2e=True)
@@ -462,6 +552,16 @@ def run_cuda(args):
                                      "roofline_frac": BYTES_PER_CELL_UPDATE * v["value"] / 1e9 / peak}
                                  for k, v in extra.items()},
         }
+        if semi is not None:
+            semi["roofline"]["peak"] = peak
+            semi["roofline"]["frac"] = semi["roofline"]["achieved"] / peak
+            srate, ssample = semi_cpu_rate(kind)
+            semi["cpu_baseline"] = {"value": srate, "unit": UNIT, "cores": 1, "kind": kind, "sample": ssample}
+            result["semi_implicit"] = semi
+        if adj is not None:
+            adj["roofline"]["peak"] = peak
+            adj["roofline"]["frac"] = adj["roofline"]["achieved"] / peak
+            result["adjoint"] = adj
         if ens is not None:
             mx, f64 = ens["mixed"], ens["fp64"]
             ens_cpu, ens_sample = ensemble_cpu_rate(kind, os.cpu_count() or 1)
@@ -500,6 +600,8 @@ def main():
                     help="0 reference-ordered FP64, 1 mixed (FP32 bulk), 2 fast FP64 (default)")
     ap.add_argument("--quick", action="store_true", help="skip the other precisions and the ensemble")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble workload")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint workload")
+    ap.add_argument("--no-semi", action="store_true", help="skip the semi-implicit 3D workload")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the device-timed step loop (no clocks, e2e, CPU baseline): a small case to profile")
     args = ap.parse_args()

@@ -106,10 +106,8 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjArgs A) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long tot = (long long)fnx * fny * fnz;
     if (t >= tot) return;
-    int i = (int)(t % fnx);
-    long long r = t / fnx;
-    int j = (int)(r % fny);
-    int k = (int)(r / fny);
+    int i, j, k;
+    split3(t, fnx, fny, i, j, k);
     const size_t base = cidx(P, i, j, k);   // right cell of the face
     const long st = (DIR == 0) ? 1L : (DIR == 1) ? (long)P.nxT : (long)P.nxT * P.nyT;
     const int pos = (DIR == 0) ? i : (DIR == 1) ? j : k;
@@ -367,10 +365,8 @@ __global__ void __launch_bounds__(128) k_tan_face(AdjArgs A) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long tot = (long long)fnx * fny * fnz;
     if (t >= tot) return;
-    int i = (int)(t % fnx);
-    long long r = t / fnx;
-    int j = (int)(r % fny);
-    int k = (int)(r / fny);
+    int i, j, k;
+    split3(t, fnx, fny, i, j, k);
     const size_t base = cidx(P, i, j, k);
     const long st = (DIR == 0) ? 1L : (DIR == 1) ? (long)P.nxT : (long)P.nxT * P.nyT;
     const bool weno = (P.reconOrder == SIFV_WENO5);

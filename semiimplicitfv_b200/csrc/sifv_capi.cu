@@ -67,6 +67,8 @@ struct sifv_ctx {
     double* adjStage = nullptr;               // stage inputs of one segment
     size_t adjStageCap = 0;
     bool adjReady = false;
+    bool igrTileReady = false;
+    double* jacCoef = nullptr;                // per-cell Jacobi coefficients (2 dim + 2 arrays)                // dynamic shared memory limit of the IGR tile kernel set
     double* lam[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* acc0[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* share[3] = {nullptr, nullptr, nullptr};
@@ -269,15 +271,31 @@ int igr_solve(sifv_ctx* c, int step) {
     k_igr_setup<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(P, c->F, c->alphaIGR);
     c->launches++;
     int iters = (step == 0) ? c->cfg.IGRWarmStartIters : c->cfg.IGRIters;
-    int nplanes = P.nx + P.ny + P.nz - 2;
-    long long lanes = (P.dim == 2) ? P.ny : (long long)P.ny * P.nz;
+    // tiled wavefront: 16^3 tiles in 3D, 32 x 64 tiles in 2D
+    constexpr int T3 = 16, T2X = 32, T2Y = 64;
+    const bool d3 = P.dim == 3;
+    const int tx = d3 ? T3 : T2X, ty = d3 ? T3 : T2Y, tz = d3 ? T3 : 1;
+    const int ntx = (P.nx + tx - 1) / tx, nty = (P.ny + ty - 1) / ty, ntz = (P.nz + tz - 1) / tz;
+    const int nplanes = ntx + nty + ntz - 2;
+    const size_t smem = d3 ? igr_tile_smem<T3, T3, T3>() : igr_tile_smem<T2X, T2Y, 1>();
+    if (P.dim >= 2 && !c->igrTileReady) {
+        cudaError_t e = d3 ? cudaFuncSetAttribute(k_igr_tile<T3, T3, T3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)smem)
+                           : cudaFuncSetAttribute(k_igr_tile<T2X, T2Y, 1>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return fail(c, SIFV_ERR_CUDA, std::string("IGR tile smem: ") + cudaGetErrorString(e));
+        c->igrTileReady = true;
+    }
     for (int it = 0; it < iters; ++it) {
         if (P.dim == 1) {
             k_igr_sweep_1d<<<1, 32, 0, c->stream>>>(P, c->F);
             c->launches++;
         } else {
             for (int pl = 0; pl < nplanes; ++pl) {
-                k_igr_plane<<<blocks(lanes, kCellThreads), kCellThreads, 0, c->stream>>>(P, c->F, pl);
+                if (d3)
+                    k_igr_tile<T3, T3, T3><<<(unsigned)(nty * ntz), T3 * T3, smem, c->stream>>>(P, c->F, pl, ntx, nty);
+                else
+                    k_igr_tile<T2X, T2Y, 1><<<(unsigned)nty, T2Y, smem, c->stream>>>(P, c->F, pl, ntx, nty);
             }
             c->launches += nplanes;
         }
@@ -298,6 +316,12 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
     CUDA_TRY(c, cudaMemsetAsync(&c->ctl->jacobiDone, 0, sizeof(int), c->stream));
     CUDA_TRY(c, cudaMemsetAsync(c->ctl->res, 0, sizeof(unsigned long long) * (size_t)maxIter, c->stream));
     unsigned g = blocks((long long)c->nint, kCellThreads);
+    if (!c->jacCoef) {
+        int sa = SIFV_OK;
+        c->jacCoef = dalloc(c, c->ncells * (size_t)(2 * c->P.dim + 2), sa);
+        if (sa != SIFV_OK) return sa;
+    }
+    k_jacobi_coef<<<g, kCellThreads, 0, c->stream>>>(c->P, rho, rhoc2, c->F, c->ctl, c->jacCoef, c->ncells);
     int it = 0, batch = 4;
     int done = 0;
     while (it < maxIter) {
@@ -305,7 +329,8 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
         for (int q = 0; q < nb; ++q, ++it) {
             const double* pin = (it & 1) ? c->F.pB : c->F.pA;
             double* pout = (it & 1) ? c->F.pA : c->F.pB;
-            k_jacobi<<<g, kCellThreads, 0, c->stream>>>(c->P, rho, rhoc2, rhs, pin, pout, c->F, c->ctl, it, tol);
+            k_jacobi_pre<<<g, kCellThreads, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhs, pin, pout, c->ctl, it,
+                                                            tol);
         }
         c->launches += nb;
         LAUNCH_CHECK(c);

@@ -11,15 +11,32 @@ namespace sifv {
 __device__ __forceinline__ double bits2d(unsigned long long b) { return __longlong_as_double((long long)b); }
 __device__ __forceinline__ unsigned long long d2bits(double d) { return (unsigned long long)__double_as_longlong(d); }
 
+// Split a linear id t = a + n0 (b + n1 c) into (a, b, c); 32-bit unsigned
+// division when t fits (every grid up to 2^32 cells), 64-bit otherwise.
+__device__ __forceinline__ void split3(long long t, int n0, int n1, int& a, int& b, int& c) {
+    if (t < 0x100000000LL) {
+        const unsigned u = (unsigned)t, m0 = (unsigned)n0, m1 = (unsigned)n1;
+        const unsigned r = u / m0;
+        a = (int)(u - r * m0);
+        const unsigned q = r / m1;
+        b = (int)(r - q * m1);
+        c = (int)q;
+    } else {
+        const long long r = t / n0;
+        a = (int)(t - r * n0);
+        const long long q = r / n1;
+        b = (int)(r - q * n1);
+        c = (int)q;
+    }
+}
+
 // Decode a linear id over the extended grid into (i, j, k) with ghosts
 // (i in [-ngx, nx+ngx), ...).  Returns false past the end.
 __device__ __forceinline__ bool ext_coords(const Params& P, long long t, int& i, int& j, int& k) {
     long long tot = (long long)P.nxT * P.nyT * P.nzT;
     if (t >= tot) return false;
-    int ii = (int)(t % P.nxT);
-    long long r = t / P.nxT;
-    int jj = (int)(r % P.nyT);
-    int kk = (int)(r / P.nyT);
+    int ii, jj, kk;
+    split3(t, P.nxT, P.nyT, ii, jj, kk);
     i = ii - P.ngx;
     j = jj - P.ngy;
     k = kk - P.ngz;
@@ -29,10 +46,7 @@ __device__ __forceinline__ bool ext_coords(const Params& P, long long t, int& i,
 __device__ __forceinline__ bool int_coords(const Params& P, long long t, int& i, int& j, int& k) {
     long long tot = (long long)P.nx * P.ny * P.nz;
     if (t >= tot) return false;
-    i = (int)(t % P.nx);
-    long long r = t / P.nx;
-    j = (int)(r % P.ny);
-    k = (int)(r / P.ny);
+    split3(t, P.nx, P.ny, i, j, k);
     return true;
 }
 

@@ -131,6 +131,39 @@ def acoustic3d(n=16, semi=True, igr=True, rk=1, recon=abi.WENO5, riemann=abi.HLL
     return cfg, abi.MeshSpec(x, x, x, bc=[BC_PERIODIC] * 6), fields
 
 
+def acoustic_box(nx, ny, nz=1, semi=True, igr=True, rk=1, bc=BC_PERIODIC, stretch=0.0, max_iter=300, tol=1e-8):
+    """Low-Mach acoustic pulse on a box of nx x ny (x nz) cells, [0,1] per
+    axis, optionally with geometrically stretched x nodes (ratio 1 + stretch
+    per cell); dim = 3 when nz > 1 else 2.  Same state as acoustic3d."""
+    dim = 3 if nz > 1 else 2
+    cfg = abi.config_defaults(dim=dim, nGhost=3, RKOrder=rk, reconOrder=abi.WENO5, riemannSolver=abi.HLLC,
+                              semiImplicit=int(semi), useIGR=int(igr), siCfl=0.8, pressureTol=tol,
+                              maxPressureIters=max_iter, alphaCoeff=10.0, IGRIters=5, IGRWarmStartIters=20)
+    if stretch > 0:
+        w = (1.0 + stretch) ** np.arange(nx)
+        x = np.concatenate([[0.0], np.cumsum(w) / np.sum(w)])
+    else:
+        x = abi.linspace_nodes(nx, 0.0, 1.0)
+    y = abi.linspace_nodes(ny, 0.0, 1.0)
+    z = abi.linspace_nodes(nz, 0.0, 1.0) if dim == 3 else None
+    cx, cy = _centroids(x), _centroids(y)
+    if dim == 3:
+        Z, Y, X = np.meshgrid(_centroids(z), cy, cx, indexing="ij")
+        r2 = (X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2
+    else:
+        Y, X = np.meshgrid(cy, cx, indexing="ij")
+        r2 = ((X - 0.5) ** 2 + (Y - 0.5) ** 2)[None]
+    p = 1.0 + 1e-3 * np.exp(-r2 / 0.01)
+    rho = np.ones_like(p)
+    u = np.full_like(p, 0.1)
+    v = np.full_like(p, 0.05)
+    w = np.zeros_like(p)
+    shape = _ext_shape(cfg, nx, ny, nz)
+    fields = _single_phase_fields(cfg, shape, rho, u, v, w if dim == 3 else None, p, 1.4)
+    mesh = abi.MeshSpec(x, y, z, bc=[bc] * 6) if dim == 3 else abi.MeshSpec(x, y, bc=[bc] * 6)
+    return cfg, mesh, fields
+
+
 def vortex2d(n=512, beta=5.0, L=10.0, cfl=0.6, recon=abi.WENO5, riemann=abi.HLLC, rk=3):
     """Isentropic vortex (Shu; examples/2D_isentropic_vortex/2D_isentropic_vortex.cpp:65-94)
     on the periodic square [-L/2, L/2]^2 centred at the origin, free stream

@@ -94,6 +94,18 @@ def test_acoustic3d_semi_implicit(rk, igr):
     check(cases.acoustic3d(16, rk=rk, igr=igr), 3)
 
 
+@pytest.mark.parametrize("bc,stretch", [(abi.BC_PERIODIC, 0.0), (abi.BC_SLIPWALL, 0.02)])
+def test_igr_tiled_wavefront_3d_ragged(bc, stretch):
+    """Several 16^3 IGR tiles with ragged edges (40 x 36 x 20 cells)."""
+    check(cases.acoustic_box(40, 36, 20, bc=bc, stretch=stretch), 2)
+
+
+@pytest.mark.parametrize("bc", [abi.BC_PERIODIC, abi.BC_OUTFLOW])
+def test_igr_tiled_wavefront_2d_ragged(bc):
+    """Several 32 x 64 IGR tiles with ragged edges (100 x 140 cells)."""
+    check(cases.acoustic_box(100, 140, bc=bc, stretch=0.01), 2)
+
+
 def test_explicit_3d_igr_lf():
     case = cases.acoustic3d(12, semi=False, igr=True, rk=3, riemann=abi.LF)
     case[0].cfl = 0.5
