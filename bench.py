@@ -370,9 +370,13 @@ def run_cuda(args):
         return out
 
     def measure_ensemble(precision, with_clocks=False, with_e2e=False):
-        """The batched-ensemble workload in one launch; returns timing and the
+        """The batched-ensemble workload in one launch per rank (ranks take
+        cost-balanced shares of the tubes); returns this rank's timing and
         per-tube densities (for the mixed-vs-FP64 error)."""
+        from semiimplicitfv_b200.shard import rank_share
         inst = ensemble_instances()
+        costs = [float(len(c[1].x) - 1) ** 2 for c in inst]
+        inst = [inst[k] for k in rank_share(costs, rank, ws)]
         ns = [len(c[1].x) - 1 for c in inst]
         cfg = inst[0][0]
         cfg.precision = precision
@@ -405,7 +409,7 @@ def run_cuda(args):
             ens2.run(ENS_TEND, block_size=bs)
             for f in fids:
                 assert ens2.be.fn["ensemble_get_field"](ens2.h, f, ctypes.c_void_p(packed[f].data_ptr()), 0) == 0
-            out["e2e"] = cu / (time.perf_counter() - t0)
+            out["e2e_s"] = time.perf_counter() - t0
             ens2.close()
         return out
 
@@ -469,6 +473,45 @@ def run_cuda(args):
                 "roofline": {"bound": "hbm", "bytes_per_cell_update": ADJ_BYTES_PER_CELL_UPDATE,
                              "achieved": ADJ_BYTES_PER_CELL_UPDATE * val / 1e9, "unit": "GB/s"}}
 
+    if args.profile_case:
+        # a small instance of one of the other workloads (for ncu captures)
+        t0 = time.perf_counter()
+        if args.profile_case == "semi":
+            case = cases.acoustic3d(args.n)
+            ctx = backends.cuda().create(case[0], case[1], local)
+            ctx.set_state(case[2])
+            t_sim = 0.0
+            for q in range(args.steps):
+                t_sim += ctx.step(q, t_sim, -1.0)
+            ctx.close()
+        elif args.profile_case == "adjoint":
+            case = cases.vortex2d(args.n)
+            ctx = backends.cuda().create(case[0], case[1], local)
+            ctx.set_state(case[2])
+            ctx.adjoint_forward(0, 0.0, 10.0, args.steps, ADJ_EVERY)
+            seed = np.zeros(ctx.shape)
+            ctx.interior(seed)[...] = 1.0
+            for f in (abi.F_RHO, abi.F_RHOU, abi.F_RHOV, abi.F_RHOE):
+                ctx.adjoint_set_seed(f, seed)
+            ctx.adjoint_backward()
+            ctx.close()
+        else:
+            inst = ensemble_instances(count=args.n, nmin=256, nmax=2048)
+            ns = [len(c[1].x) - 1 for c in inst]
+            cfg = inst[0][0]
+            cfg.precision = args.precision if args.precision in (0, 1) else abi.PREC_MIXED
+            ens = backends.cuda().create_ensemble(cfg, ns, [0.0] * len(ns), [1.0] * len(ns), device=local)
+            for f in inst[0][2]:
+                if f != abi.F_SIGMA:
+                    ens.set_field(f, ens.pack([c[2][f] for c in inst]))
+            ens.run(ENS_TEND, max_steps=args.steps, block_size=512)
+            ens.close()
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile_case": args.profile_case, "n": args.n, "steps": args.steps,
+                              "seconds": time.perf_counter() - t0}), flush=True)
+        return
+
     if args.kernels_only:
         r = measure(args.precision)
         if rank == 0:
@@ -490,13 +533,25 @@ def run_cuda(args):
     if ws == 1 and not args.quick and not args.no_semi:
         semi = measure_semi_implicit()
     ens = None
-    if ws == 1 and not args.quick and not args.no_ensemble:
-        emx = measure_ensemble(abi.PREC_MIXED, with_clocks=True, with_e2e=True)
+    if not args.quick and not args.no_ensemble:
+        from semiimplicitfv_b200.shard import max_over_ranks as mor, sum_over_ranks as sor
+        barrier()
+        emx = measure_ensemble(abi.PREC_MIXED, with_clocks=(rank == 0), with_e2e=True)
+        barrier()
         e64 = measure_ensemble(abi.PREC_FP64)
         rel = [np.abs(a - b).mean() / np.abs(b).mean() for a, b in zip(emx["rho"], e64["rho"])]
         linf = [np.abs(a - b).max() / np.abs(b).max() for a, b in zip(emx["rho"], e64["rho"])]
-        ens = {"mixed": emx, "fp64": e64, "l1_rel_max": float(max(rel)), "l1_rel_mean": float(np.mean(rel)),
-               "linf_rel_max": float(max(linf))}
+        dev = "cuda" if ws > 1 else None
+        for e in (emx, e64):     # whole job: all tubes over the slowest rank's time
+            e["ms"] = mor(e["ms"], dev)
+            e["cell_updates"] = sor(e["cell_updates"], dev)
+            e["ncells"] = int(sor(e["ncells"], dev))
+            e["value"] = e["cell_updates"] / (e["ms"] / 1e3)
+            e["steps_min"] = -int(mor(-e["steps_min"], dev))
+            e["steps_max"] = int(mor(e["steps_max"], dev))
+        emx["e2e"] = emx["cell_updates"] / mor(emx["e2e_s"], dev)
+        ens = {"mixed": emx, "fp64": e64, "l1_rel_max": mor(float(max(rel)), dev),
+               "l1_rel_mean": float(np.mean(rel)), "linf_rel_max": mor(float(max(linf)), dev)}
     ms = main["ms"]
     value = main["value"]
     launches = main["launches"]
@@ -568,7 +623,8 @@ def run_cuda(args):
             result["ensemble"] = {
                 "workload": f"{ENS_COUNT} two-phase water-air tubes, cells log-uniform [{ENS_NMIN},{ENS_NMAX}] "
                             f"(seed {ENS_SEED}, {mx['ncells']} cells), WENO5 + mixture HLLC, SSP-RK3 CFL0.5, "
-                            f"t_end={ENS_TEND}, one launch",
+                            f"t_end={ENS_TEND}, one launch per GPU",
+                "scaling": "strong (the tubes are divided across GPUs by cost, cells^2)",
                 "metric": "cell-updates/s", "value": mx["value"], "precision": "mixed-fp32-bulk",
                 "seconds": mx["ms"] / 1e3, "cell_updates": mx["cell_updates"],
                 "steps_min_max": [mx["steps_min"], mx["steps_max"]], "threads_per_tube": mx["block_size"],
@@ -602,6 +658,8 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble workload")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint workload")
     ap.add_argument("--no-semi", action="store_true", help="skip the semi-implicit 3D workload")
+    ap.add_argument("--profile-case", choices=["semi", "adjoint", "ensemble"], default=None,
+                    help="run a small instance of another workload (--n: cells per axis, or tubes) and exit")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the device-timed step loop (no clocks, e2e, CPU baseline): a small case to profile")
     args = ap.parse_args()
