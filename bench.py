@@ -45,8 +45,12 @@ BYTES_PER_CELL_UPDATE = 256   # algorithmic: 64 B x 4 conserved variables per RK
 #            pres and U, writes U0 + pres0); writes 4 U     avg 20.67 x 8 = 165.3
 #   dt       reads rho, velU, velV, pres                         4 x 8 = 32
 #   finish_prim reads 4 U, writes velU, velV, pres              7 x 8 = 56
+#   tile2d   one fused kernel per stage: reads U (4) and, in stages 2-3, U0
+#            (4); writes U' (4); the last stage also writes u, v, p (3)
+#                                             (32 + 21.33 + 32 + 8) = 93.33
 KERNEL_BYTES_PER_CELL_2D = {"sweep_x": 96.0, "sweep_y": 165.33, "dt": 32.0, "finish_prim": 56.0,
-                            "face_x": 64.0, "face_y": 64.0, "assemble": 229.3, "prim_bc": 56.0}
+                            "face_x": 64.0, "face_y": 64.0, "assemble": 229.3, "prim_bc": 56.0,
+                            "tile2d": 93.33}
 # DRAM bytes per cell of one launch, measured by ncu on the 2048^2 case of the
 # same workload (dram__bytes_read.sum + dram__bytes_write.sum over 2048^2 cells)
 # and scaled by the cell count for the benchmark size.

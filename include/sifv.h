@@ -235,6 +235,13 @@ int sifv_profile_step(sifv_ctx_t* ctx, int step, double time, double targetDt, c
  * call, and the number of kernel launches it made. */
 int sifv_last_step_stats(const sifv_ctx_t* ctx, double* deviceMs, int* launches);
 
+/* ---- diagnostics ----------------------------------------------------------- */
+/* Maximum relative error of the fast paths' reciprocal and square root
+ * against IEEE 1/x and sqrt(x) over n arguments spread across [2^-60, 2^60)
+ * (SIFV_PREC_FP64_FAST / SIFV_PREC_MIXED use them; SIFV_PREC_FP64 does not).
+ * Returns 0 or SIFV_ERR_CUDA. */
+int sifv_fastmath_selftest(long long n, double* maxRelRcp, double* maxRelSqrt);
+
 /* ---- discrete adjoint and tangent of the explicit step ------------------ */
 /* Reverse- and forward-mode derivatives of the map U(t0) -> U(tEnd) that
  * sifv_step iterates (ExplicitSolver::step, src/ExplicitSolver.cpp:68-203:

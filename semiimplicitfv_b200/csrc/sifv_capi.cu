@@ -68,7 +68,9 @@ struct sifv_ctx {
     size_t adjStageCap = 0;
     bool adjReady = false;
     bool igrTileReady = false;
-    double* jacCoef = nullptr;                // per-cell Jacobi coefficients (2 dim + 2 arrays)                // dynamic shared memory limit of the IGR tile kernel set
+    double* jacCoef = nullptr;                // per-cell Jacobi coefficients (2 dim + 2 arrays)
+    double* tileB[4] = {nullptr, nullptr, nullptr, nullptr};   // 2D fused-stage scratch states
+    double* tileC[4] = {nullptr, nullptr, nullptr, nullptr};                // dynamic shared memory limit of the IGR tile kernel set
     double* lam[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* acc0[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* share[3] = {nullptr, nullptr, nullptr};
@@ -409,6 +411,58 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
     status = SIFV_OK;
     enqueue_dt(c, targetDt, useEnd);
     unsigned gc = blocks((long long)c->nint, kCellThreads);
+    if (c->sweep && P.dim == 2) {
+        // one fused tile kernel per stage; stage outputs ping-pong through two
+        // scratch states, the last stage writes over the step-start state
+        if (!c->tileB[0]) {
+            int sa = SIFV_OK;
+            for (int q = 0; q < 4; ++q) {
+                c->tileB[q] = dalloc(c, c->ncells, sa);
+                c->tileC[q] = dalloc(c, c->ncells, sa);
+            }
+            if (sa != SIFV_OK) return sa;
+        }
+        double* U[4] = {c->F.rho, c->F.rhoU, c->F.rhoV, c->F.rhoE};
+        const int RK = cfg.RKOrder;
+        for (int s = 0; s < RK; ++s) {
+            StageCoef K{};
+            rk_coef(RK, s, K);
+            TileArgs T{};
+            T.P = c->P;
+            T.C.gamma = c->P.gamma;
+            T.C.pInf = c->P.pInf;
+            T.C.invGm1 = 1.0 / (c->P.gamma - 1.0);
+            T.C.gPinf = c->P.gamma * c->P.pInf;
+            T.eps = cfg.wenoEps;
+            T.ctl = c->ctl;
+            T.a1 = K.c1 / K.c4;
+            T.a2 = K.c2 / K.c4;
+            T.a3 = K.c3 / K.c4;
+            T.inv[0] = c->invW[0];
+            T.inv[1] = c->invW[1];
+            T.last = (s == RK - 1) ? 1 : 0;
+            T.velU = c->F.velU;
+            T.velV = c->F.velV;
+            T.pres = c->F.pres;
+            double* const* in = (s == 0) ? U : (s == 1) ? c->tileB : c->tileC;
+            double* const* out = (RK > 1 && s == RK - 1) ? U : (s == 0) ? c->tileB : c->tileC;
+            for (int q = 0; q < 4; ++q) {
+                T.in[q] = in[q];
+                T.out[q] = out[q];
+                T.u0[q] = (s > 0 && K.c2 != 0.0) ? U[q] : nullptr;
+            }
+            if (tile2d_stage(T, c->stream, cfg.precision == SIFV_PREC_MIXED, c->launches,
+                             c->profiling ? mark_cb : nullptr, c) != 0) {
+                LAUNCH_CHECK(c);
+                return fail(c, SIFV_ERR_CUDA, "tile launch failed");
+            }
+        }
+        if (RK == 1 && tile2d_copy(c->ctl, c->tileB, U, c->ncells, c->stream, c->launches) != 0)
+            return fail(c, SIFV_ERR_CUDA, "copy launch failed");
+        launch_bc_prim(c);
+        LAUNCH_CHECK(c);
+        return SIFV_OK;
+    }
     if (c->sweep) {
         SweepArgs A{};
         A.P = c->P;

@@ -5,8 +5,11 @@
 // equality.
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "sifv_sweep.cuh"
 #include "sifv_sweep_api.h"
+#include "sifv_tile2d.cuh"
 
 namespace sifv {
 
@@ -63,6 +66,70 @@ int sweep_stage(SweepArgs A, cudaStream_t s, bool mixed, int& launches, LaunchMa
     }
 }
 
+namespace {
+
+constexpr int kTileX = 32, kTileY = 16;
+
+template <typename T>
+int tile_launch(const TileArgs& A, cudaStream_t s) {
+    const size_t bytes = sizeof(TileSmem<kTileX, kTileY, T>);
+    if (cudaFuncSetAttribute(k_tile2d<kTileX, kTileY, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bytes) != cudaSuccess)
+        return -1;
+    dim3 g((A.P.nx + kTileX - 1) / kTileX, (A.P.ny + kTileY - 1) / kTileY, 1);
+    k_tile2d<kTileX, kTileY, T><<<g, 256, bytes, s>>>(A);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace
+
+int tile2d_stage(const TileArgs& A, cudaStream_t s, bool mixed, int& launches, LaunchMark mark, void* user) {
+    int st = mixed ? tile_launch<float>(A, s) : tile_launch<double>(A, s);
+    ++launches;
+    if (mark) mark(user, "tile2d");
+    return st;
+}
+
+int tile2d_copy(const Ctl* ctl, const double* const in[4], double* const out[4], size_t n, cudaStream_t s,
+                int& launches) {
+    Copy4 C;
+    for (int q = 0; q < 4; ++q) {
+        C.src[q] = in[q];
+        C.dst[q] = out[q];
+    }
+    k_copy4<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ctl, C, n);
+    ++launches;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+namespace {
+
+// relative errors of frcp / fsqrt_pos against IEEE 1/x and sqrt(x) over
+// x = m 2^e, m uniform in [1, 2) (a fixed 64-bit hash of the index), e in
+// [-60, 60); maxima folded with atomicMax on the bit patterns
+__global__ void k_fastmath_check(long long n, unsigned long long* out) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double eR = 0.0, eS = 0.0;
+    if (t < n) {
+        unsigned long long h = (unsigned long long)t * 0x9E3779B97F4A7C15ull;
+        h ^= h >> 29;
+        h *= 0xBF58476D1CE4E5B9ull;
+        h ^= h >> 32;
+        const double m = 1.0 + (double)(h >> 11) * (1.0 / 9007199254740992.0);
+        const int e = (int)(t % 120) - 60;
+        const double x = ldexp(m, e);
+        const double r0 = 1.0 / x, r1 = frcp(x);
+        const double s0 = sqrt(x), s1 = fsqrt_pos(x);
+        eR = fabs(r1 - r0) / r0;
+        eS = fabs(s1 - s0) / s0;
+        atomicAdd(&out[2], 1ull);
+    }
+    atomicMax(&out[0], (unsigned long long)__double_as_longlong(eR));
+    atomicMax(&out[1], (unsigned long long)__double_as_longlong(eS));
+}
+
+}  // namespace
+
 int sweep_finish_prim(const Params& P, const Fields& F, const Ctl* ctl, cudaStream_t s, int& launches) {
     long long n = (long long)P.nx * P.ny * P.nz;
     k_cons_to_prim_interior<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, F, ctl);
@@ -71,3 +138,19 @@ int sweep_finish_prim(const Params& P, const Fields& F, const Ctl* ctl, cudaStre
 }
 
 }  // namespace sifv
+
+extern "C" int sifv_fastmath_selftest(long long n, double* maxRelRcp, double* maxRelSqrt) {
+    if (n <= 0 || !maxRelRcp || !maxRelSqrt) return -2;
+    unsigned long long* d = nullptr;
+    if (cudaMalloc(&d, 3 * sizeof(unsigned long long)) != cudaSuccess) return -3;
+    cudaMemset(d, 0, 3 * sizeof(unsigned long long));
+    sifv::k_fastmath_check<<<(unsigned)((n + 255) / 256), 256>>>(n, d);
+    cudaError_t e = cudaGetLastError();
+    unsigned long long h[3] = {0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess || h[2] != (unsigned long long)n) return -3;   // every argument checked
+    std::memcpy(maxRelRcp, &h[0], sizeof(double));
+    std::memcpy(maxRelSqrt, &h[1], sizeof(double));
+    return 0;
+}

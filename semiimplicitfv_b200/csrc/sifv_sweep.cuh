@@ -29,6 +29,45 @@
 
 namespace sifv {
 
+// Fast reciprocal and square root of the fast / mixed paths.  FP64: the
+// hardware approximation (rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64)
+// refined by Newton-Raphson iterations, y <- y + y (1 - x y) for 1/x and
+// y <- y + (y / 2)(1 - x y^2) for 1/sqrt(x) (each iteration squares the
+// relative error), and sqrt(x) = x / sqrt(x) with one correction
+// s <- s + (x - s^2) y / 2; within 1 ulp of the IEEE results (checked
+// against them by sifv_fastmath_selftest).  FP32: the single-instruction
+// approximations (about 1 ulp).  The reference-ordered path never uses these.
+__device__ __forceinline__ double frcp(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+__device__ __forceinline__ float frcp(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// sqrt of a positive normal argument
+__device__ __forceinline__ double fsqrt_pos(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x * y, y, 1.0);
+    y = fma(0.5 * y, e, y);
+    e = fma(-x * y, y, 1.0);
+    y = fma(0.5 * y, e, y);
+    double sq = x * y;
+    double r = fma(-sq, sq, x);
+    return fma(r, 0.5 * y, sq);
+}
+__device__ __forceinline__ float fsqrt_pos(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 template <typename T>
 struct Prim5 {
     T rho, u, v, w, p;
@@ -61,8 +100,8 @@ __device__ __forceinline__ void weno5_pair(double v0, double v1, double v2, doub
     double pR2 = (2.0 * v2 + 5.0 * v1 - v0) * (1.0 / 6.0);
     double wL0 = 0.1 * m12, wL1 = 0.6 * m02, wL2 = 0.3 * m01;   // L: d = (.1,.6,.3) on (b0,b1,b2)
     double wR0 = 0.1 * m01, wR1 = 0.6 * m02, wR2 = 0.3 * m12;   // R: d = (.1,.6,.3) on (b2,b1,b0)
-    L = (wL0 * pL0 + wL1 * pL1 + wL2 * pL2) / (wL0 + wL1 + wL2);
-    R = (wR0 * pR0 + wR1 * pR1 + wR2 * pR2) / (wR0 + wR1 + wR2);
+    L = (wL0 * pL0 + wL1 * pL1 + wL2 * pL2) * frcp(wL0 + wL1 + wL2);
+    R = (wR0 * pR0 + wR1 * pR1 + wR2 * pR2) * frcp(wR0 + wR1 + wR2);
 }
 
 // FP32 version: the product form would overflow single precision for
@@ -75,7 +114,7 @@ __device__ __forceinline__ void weno5_pair(float v0, float v1, float v2, float v
     float q0 = eps + ((13.0f / 12.0f) * t0 * t0 + 0.25f * s0 * s0);
     float q1 = eps + ((13.0f / 12.0f) * t1 * t1 + 0.25f * s1 * s1);
     float q2 = eps + ((13.0f / 12.0f) * t2 * t2 + 0.25f * s2 * s2);
-    float r0 = __frcp_rn(q0 * q0), r1 = __frcp_rn(q1 * q1), r2 = __frcp_rn(q2 * q2);
+    float r0 = frcp(q0 * q0), r1 = frcp(q1 * q1), r2 = frcp(q2 * q2);
     float pL0 = (2.0f * v0 - 7.0f * v1 + 11.0f * v2) * (1.0f / 6.0f);
     float pL1 = (-v1 + 5.0f * v2 + 2.0f * v3) * (1.0f / 6.0f);
     float pL2 = (2.0f * v2 + 5.0f * v3 - v4) * (1.0f / 6.0f);
@@ -84,16 +123,16 @@ __device__ __forceinline__ void weno5_pair(float v0, float v1, float v2, float v
     float pR2 = (2.0f * v2 + 5.0f * v1 - v0) * (1.0f / 6.0f);
     float aL0 = 0.1f * r0, aL1 = 0.6f * r1, aL2 = 0.3f * r2;
     float aR0 = 0.1f * r2, aR1 = 0.6f * r1, aR2 = 0.3f * r0;
-    L = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) * __frcp_rn(aL0 + aL1 + aL2);
-    R = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) * __frcp_rn(aR0 + aR1 + aR2);
+    L = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) * frcp(aL0 + aL1 + aL2);
+    R = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) * frcp(aR0 + aR1 + aR2);
 }
 
 template <typename T>
 __device__ __forceinline__ T trcp(T x);
 template <>
-__device__ __forceinline__ double trcp<double>(double x) { return 1.0 / x; }
+__device__ __forceinline__ double trcp<double>(double x) { return frcp(x); }
 template <>
-__device__ __forceinline__ float trcp<float>(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float trcp<float>(float x) { return frcp(x); }
 
 template <typename T>
 struct Flux4 {
@@ -116,12 +155,12 @@ __device__ __forceinline__ void face_flux(int riemann, const FluxConsts& C, cons
     T rhoEL = (L.p + gPinf) * invGm1 + (T)0.5 * L.rho * q2L;
     T rhoER = (R.p + gPinf) * invGm1 + (T)0.5 * R.rho * q2R;
     T irL = trcp(tmax(L.rho, tiny)), irR = trcp(tmax(R.rho, tiny));
-    T cL = sqrt(g * tmax(L.p + pinf, tiny) * irL), cR = sqrt(g * tmax(R.p + pinf, tiny) * irR);
+    T cL = fsqrt_pos(g * tmax(L.p + pinf, tiny) * irL), cR = fsqrt_pos(g * tmax(R.p + pinf, tiny) * irR);
     if (riemann == SIFV_HLLC) {
         T sL = tmin(unL - cL, unR - cR);
         T sR = tmax(unL + cL, unR + cR);
         T aL = L.rho * (sL - unL), aR = R.rho * (sR - unR);
-        T sStar = (R.p - L.p + aL * unL - aR * unR) / (aL - aR);
+        T sStar = (R.p - L.p + aL * unL - aR * unR) * trcp(aL - aR);
         if (sL >= (T)0) {
             F.mass = L.rho * unL;
             F.m0 = F.mass * L.u; F.m1 = F.mass * L.v; F.m2 = F.mass * L.w;
@@ -297,7 +336,7 @@ __global__ void __launch_bounds__(128) k_sweep_x(SweepArgs A) {
         if (!r.valid) return Prim5<double>{0.0, 0.0, 0.0, 0.0, 0.0};
         const int dim = DIM;
         double rho = (r.rho < 1e-14) ? 1e-14 : r.rho;
-        double ir = 1.0 / rho;
+        double ir = frcp(rho);
         double u = r.ru * ir, v = r.rv * ir, w = r.rw * ir;
         double ke = u * u;
         if (dim >= 2) ke += v * v;

@@ -38,6 +38,23 @@ struct SweepArgs {
     const double* inv[3];   // 1 / d per cell (ghosts included)
 };
 
+// One RK stage of the 2D explicit step as one fused tile kernel
+// (sifv_tile2d.cuh): U' = a1 in + a2 u0 + a3 dt R(in), written to `out`
+// (which may be u0, never `in`); `last` also writes the primitives of U'.
+struct TileArgs {
+    Params P;
+    FluxConsts C;
+    double eps;
+    const Ctl* ctl;
+    const double* in[4];    // stage input: rho, rhoU, rhoV, rhoE
+    const double* u0[4];    // step-start state (own cells), null when a2 == 0
+    double* out[4];         // stage output
+    double a1, a2, a3;
+    const double* inv[2];   // 1 / dx, 1 / dy per cell (ghosts included)
+    int last;               // write the primitives of the new state
+    double *velU, *velV, *pres;
+};
+
 // Called after each kernel launch with the kernel family's name (per-kernel
 // timing); may be null.
 typedef void (*LaunchMark)(void* user, const char* family);
@@ -46,6 +63,12 @@ typedef void (*LaunchMark)(void* user, const char* family);
 // (mixed: FP32 reconstruction / Riemann bulk).  Returns 0 on success.
 int sweep_stage(SweepArgs A, cudaStream_t s, bool mixed, int& launches, LaunchMark mark = nullptr,
                 void* user = nullptr);
+
+int tile2d_stage(const TileArgs& A, cudaStream_t s, bool mixed, int& launches, LaunchMark mark = nullptr,
+                 void* user = nullptr);
+// out[q] = in[q] over n values, skipped when the step is (device-side loops).
+int tile2d_copy(const Ctl* ctl, const double* const in[4], double* const out[4], size_t n, cudaStream_t s,
+                int& launches);
 
 // End-of-step conservative -> primitive on interior cells.
 int sweep_finish_prim(const Params& P, const Fields& F, const Ctl* ctl, cudaStream_t s, int& launches);

@@ -155,3 +155,17 @@ def test_mixed_riemann2d_error_within_bound():
     err_mx = np.abs(rmx - rf).mean()
     assert err_mx <= 1.5 * disc, (err_mx, disc)
     assert mixed_vs_fp64 < 0.1 * disc, (mixed_vs_fp64, disc)
+
+
+def test_fast_reciprocal_and_sqrt_within_one_ulp():
+    """The fast paths' Newton-refined reciprocal and square root against
+    IEEE 1/x and sqrt(x) on 2^22 arguments across [2^-60, 2^60)."""
+    import ctypes
+    from semiimplicitfv_b200 import _lib
+    lib = _lib.load()
+    lib.sifv_fastmath_selftest.argtypes = [ctypes.c_longlong, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_double)]
+    r, s = ctypes.c_double(), ctypes.c_double()
+    assert lib.sifv_fastmath_selftest(1 << 22, ctypes.byref(r), ctypes.byref(s)) == 0
+    assert r.value <= 2.23e-16, r.value
+    assert s.value <= 2.23e-16, s.value
