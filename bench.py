@@ -390,7 +390,7 @@ def run_cuda(args):
         packed = {f: torch.from_numpy(ens.pack([c[2][f] for c in inst])).pin_memory() for f in fids}
         for f in fids:
             ens.set_field(f, packed[f].numpy())
-        bs = ens.autotune(10)          # also the warm-up launches
+        bs = ens.autotune(200)         # also the warm-up launches (long enough that the largest tubes weigh in)
         clk = ClockSampler(local) if with_clocks else None
         if clk:
             clk.__enter__()

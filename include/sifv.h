@@ -302,8 +302,10 @@ int sifv_ensemble_get_field(sifv_ensemble_t* e, int field, double* packed, int o
  * returns SIFV_ERR_NAN; tEnd must be finite unless maxSteps > 0. */
 int sifv_ensemble_run(sifv_ensemble_t* e, double tEnd, int maxSteps, int blockSize, double* timesOut,
                       int* stepsOut, double* deviceMs);
-/* Time probeSteps steps of every instance at 128 / 256 / 512 threads per
- * instance, keep the fastest for later runs, restore the state. */
+/* Time a probe at 128 / 256 / 512 (and, mixed, 1024) threads per instance
+ * in which each instance takes steps in proportion to its cell count (as in
+ * a run to a common end time), the largest probeSteps; keep the fastest
+ * block size for later runs and restore the state. */
 int sifv_ensemble_autotune(sifv_ensemble_t* e, int probeSteps, int* blockSizeOut);
 
 /* ---- allocation-free pressure solve ----------------------------------- */

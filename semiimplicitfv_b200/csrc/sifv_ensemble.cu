@@ -26,8 +26,8 @@ struct sifv_ensemble {
     int nphT = 0;
     cudaStream_t stream = nullptr;
     std::vector<void*> allocs;
-    std::vector<long long> off, foff;
-    long long ncells = 0, nfaces = 0;
+    std::vector<long long> off;
+    long long ncells = 0;
     int blockSize = 256;
     std::string err;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -57,32 +57,60 @@ X* ealloc(sifv_ensemble* e, size_t n, int& st) {
 double* efield(sifv_ensemble* e, int f) {
     EnsArgs& A = e->A;
     switch (f) {
-        case SIFV_F_RHO: return A.rho;
-        case SIFV_F_RHOU: return A.rhoU;
-        case SIFV_F_RHOE: return A.rhoE;
+        case SIFV_F_RHO: return A.S[0].rho;
+        case SIFV_F_RHOU: return A.S[0].rhoU;
+        case SIFV_F_RHOE: return A.S[0].rhoE;
         case SIFV_F_VELU: return A.velU;
         case SIFV_F_PRES: return A.pres;
         default: break;
     }
-    if (f >= 16 && f < 16 + e->cfg.nPhases) return A.alphaRho[f - 16];
-    if (f >= 32 && f < 32 + e->cfg.nPhases) return A.alpha[f - 32];
+    if (f >= 16 && f < 16 + e->cfg.nPhases) return A.S[0].alphaRho[f - 16];
+    if (f >= 32 && f < 32 + e->cfg.nPhases) return A.S[0].alpha[f - 32];
     return nullptr;
+}
+
+template <typename T, int NPH>
+int launch_t(const EnsArgs& A, int blockSize, cudaStream_t s) {
+    const size_t bytes = ens_smem_bytes<T, NPH>(blockSize);
+    if (cudaFuncSetAttribute(k_ensemble<T, NPH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+        cudaSuccess)
+        return -1;
+    k_ensemble<T, NPH><<<A.nInst, blockSize, bytes, s>>>(A);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 int launch(sifv_ensemble* e, int blockSize) {
     if (e->cfg.precision == SIFV_PREC_MIXED)
         return ensemble_launch_mixed(e->A, e->nphT, blockSize, e->stream);
-    if (e->nphT == 0) k_ensemble<double, 0><<<e->nInst, blockSize, 0, e->stream>>>(e->A);
-    else if (e->nphT == 2) k_ensemble<double, 2><<<e->nInst, blockSize, 0, e->stream>>>(e->A);
-    else k_ensemble<double, 8><<<e->nInst, blockSize, 0, e->stream>>>(e->A);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    if (e->nphT == 0) return launch_t<double, 0>(e->A, blockSize, e->stream);
+    if (e->nphT == 2) return launch_t<double, 2>(e->A, blockSize, e->stream);
+    return launch_t<double, 8>(e->A, blockSize, e->stream);
+}
+
+// dynamic shared memory of one block, and the largest usable block size
+size_t smem_bytes(const sifv_ensemble* e, int blockSize) {
+    const bool f = e->cfg.precision == SIFV_PREC_MIXED;
+    switch (e->nphT) {
+        case 0: return f ? ens_smem_bytes<float, 0>(blockSize) : ens_smem_bytes<double, 0>(blockSize);
+        case 2: return f ? ens_smem_bytes<float, 2>(blockSize) : ens_smem_bytes<double, 2>(blockSize);
+        default: return f ? ens_smem_bytes<float, 8>(blockSize) : ens_smem_bytes<double, 8>(blockSize);
+    }
+}
+
+int max_block(const sifv_ensemble* e) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    int m = (e->cfg.precision == SIFV_PREC_MIXED) ? 1024 : 512;
+    while (m > 32 && smem_bytes(e, m) + 512 > (size_t)optin) m -= 32;
+    return m;
 }
 
 // all packed state arrays (for the autotuner's save / restore)
 std::vector<double*> state_arrays(sifv_ensemble* e) {
     EnsArgs& A = e->A;
-    std::vector<double*> v = {A.rho, A.rhoU, A.rhoE, A.velU, A.pres};
-    for (int p = 0; p < e->cfg.nPhases; ++p) { v.push_back(A.alphaRho[p]); v.push_back(A.alpha[p]); }
+    std::vector<double*> v = {A.S[0].rho, A.S[0].rhoU, A.S[0].rhoE, A.velU, A.pres};
+    for (int p = 0; p < e->cfg.nPhases; ++p) { v.push_back(A.S[0].alphaRho[p]); v.push_back(A.S[0].alpha[p]); }
     return v;
 }
 
@@ -124,14 +152,11 @@ int sifv_ensemble_create(const sifv_config_t* cfg, int nInst, const int* nCells,
     cudaEventCreate(&e->ev1);
     const int ng = cfg->nGhost;
     e->off.resize(nInst + 1);
-    e->foff.resize(nInst + 1);
-    e->off[0] = e->foff[0] = 0;
+    e->off[0] = 0;
     for (int k = 0; k < nInst; ++k) {
         e->off[k + 1] = e->off[k] + nCells[k] + 2 * ng;
-        e->foff[k + 1] = e->foff[k] + nCells[k] + 1;
     }
     e->ncells = e->off[nInst];
-    e->nfaces = e->foff[nInst];
     // cell widths: Runtime::createUniformMesh nodes a + (b - a) i / n
     // (src/Runtime.cpp:12-17) extended by RectilinearMesh::buildExtendedNodes
     // (src/RectilinearMesh.cpp:91-114)
@@ -159,24 +184,19 @@ int sifv_ensemble_create(const sifv_config_t* cfg, int nInst, const int* nCells,
     int st = SIFV_OK;
     EnsArgs& A = e->A;
     A.nInst = nInst;
-    const size_t M = (size_t)e->ncells, Fn = (size_t)e->nfaces;
-    A.rho = ealloc<double>(e, M, st); A.rhoU = ealloc<double>(e, M, st); A.rhoE = ealloc<double>(e, M, st);
-    A.velU = ealloc<double>(e, M, st); A.pres = ealloc<double>(e, M, st);
-    for (int p = 0; p < cfg->nPhases; ++p) { A.alphaRho[p] = ealloc<double>(e, M, st); A.alpha[p] = ealloc<double>(e, M, st); }
-    if (cfg->RKOrder > 1) {
-        A.rho0 = ealloc<double>(e, M, st); A.rhoU0 = ealloc<double>(e, M, st);
-        A.rhoE0 = ealloc<double>(e, M, st); A.pres0 = ealloc<double>(e, M, st);
-        for (int p = 0; p < cfg->nPhases; ++p) { A.alphaRho0[p] = ealloc<double>(e, M, st); A.alpha0[p] = ealloc<double>(e, M, st); }
+    const size_t M = (size_t)e->ncells;
+    const int nStates = (cfg->RKOrder >= 3) ? 3 : 2;   // the state and the stage outputs
+    for (int k = 0; k < nStates; ++k) {
+        EnsState& S = A.S[k];
+        S.rho = ealloc<double>(e, M, st); S.rhoU = ealloc<double>(e, M, st); S.rhoE = ealloc<double>(e, M, st);
+        for (int p = 0; p < cfg->nPhases; ++p) { S.alphaRho[p] = ealloc<double>(e, M, st); S.alpha[p] = ealloc<double>(e, M, st); }
     }
+    A.velU = ealloc<double>(e, M, st); A.pres = ealloc<double>(e, M, st);
     double* dxd = ealloc<double>(e, M, st);
     A.dx = dxd;
-    A.fMass = ealloc<double>(e, Fn, st); A.fMom = ealloc<double>(e, Fn, st); A.fEnergy = ealloc<double>(e, Fn, st);
-    if (cfg->nPhases > 0) A.fVel = ealloc<double>(e, Fn, st);
-    for (int p = 0; p < cfg->nPhases; ++p) { A.fAlpha[p] = ealloc<double>(e, Fn, st); A.fAR[p] = ealloc<double>(e, Fn, st); }
     int* ord = ealloc<int>(e, nInst, st);
     int* nn = ealloc<int>(e, nInst, st);
     long long* offd = ealloc<long long>(e, nInst + 1, st);
-    long long* foffd = ealloc<long long>(e, nInst + 1, st);
     A.time = ealloc<double>(e, nInst, st);
     A.steps = ealloc<int>(e, nInst, st);
     A.lastDt = ealloc<double>(e, nInst, st);
@@ -186,10 +206,9 @@ int sifv_ensemble_create(const sifv_config_t* cfg, int nInst, const int* nCells,
         cudaMemcpyAsync(ord, order.data(), nInst * sizeof(int), cudaMemcpyHostToDevice, e->stream);
         cudaMemcpyAsync(nn, nCells, nInst * sizeof(int), cudaMemcpyHostToDevice, e->stream);
         cudaMemcpyAsync(offd, e->off.data(), (nInst + 1) * sizeof(long long), cudaMemcpyHostToDevice, e->stream);
-        cudaMemcpyAsync(foffd, e->foff.data(), (nInst + 1) * sizeof(long long), cudaMemcpyHostToDevice, e->stream);
         if (cudaStreamSynchronize(e->stream) != cudaSuccess) st = efail(e, SIFV_ERR_CUDA, "upload failed");
     }
-    A.order = ord; A.n = nn; A.off = offd; A.foff = foffd;
+    A.order = ord; A.n = nn; A.off = offd;
     Params& P = A.P;
     P.dim = 1; P.ny = P.nz = 1; P.ngx = ng; P.ngy = P.ngz = 0; P.nyT = P.nzT = 1;
     P.bc[0] = bc[0]; P.bc[1] = bc[1];
@@ -258,7 +277,9 @@ int sifv_ensemble_run(sifv_ensemble_t* e, double tEnd, int maxSteps, int blockSi
                       int* stepsOut, double* deviceMs) {
     if (!e) return efail(nullptr, SIFV_ERR_BAD_ARG, "null ensemble");
     int bs = blockSize > 0 ? blockSize : e->blockSize;
-    if (bs % 32 != 0 || bs < 32 || bs > 512) return efail(e, SIFV_ERR_BAD_ARG, "blockSize must be a multiple of 32 in [32, 512]");
+    const int maxBs = max_block(e);
+    if (bs % 32 != 0 || bs < 32 || bs > maxBs)
+        return efail(e, SIFV_ERR_BAD_ARG, "blockSize must be a multiple of 32 in [32, " + std::to_string(maxBs) + "]");
     if (!(tEnd < 1e300) && maxSteps <= 0) return efail(e, SIFV_ERR_BAD_ARG, "tEnd must be finite when there is no step limit");
     cudaSetDevice(e->device);
     e->A.tEnd = tEnd;
@@ -281,9 +302,11 @@ int sifv_ensemble_run(sifv_ensemble_t* e, double tEnd, int maxSteps, int blockSi
     return SIFV_OK;
 }
 
-// Pick the block size (128 / 256 / 512 threads per instance) with the
-// shortest time for `probeSteps` steps of every instance; the state is
-// restored afterwards.
+// Pick the block size (128 / 256 / 512 threads per instance, and 1024 with
+// FP32 bulk, as shared memory allows) with the shortest time for a probe in
+// which every instance takes steps in proportion to its cell count (as in a
+// run to a common end time at a fixed CFL), the largest probeSteps steps;
+// the state is restored afterwards.
 int sifv_ensemble_autotune(sifv_ensemble_t* e, int probeSteps, int* blockSizeOut) {
     if (!e) return efail(nullptr, SIFV_ERR_BAD_ARG, "null ensemble");
     cudaSetDevice(e->device);
@@ -306,12 +329,24 @@ int sifv_ensemble_autotune(sifv_ensemble_t* e, int probeSteps, int* blockSizeOut
     cudaStreamSynchronize(e->stream);
     int best = 256;
     float bestMs = 1e30f;
-    const int cands[3] = {128, 256, 512};
+    const int cands[4] = {128, 256, 512, 1024};
+    const int maxBs = max_block(e);
+    std::vector<int> nc(e->nInst), lim(e->nInst);
+    cudaMemcpy(nc.data(), e->A.n, e->nInst * sizeof(int), cudaMemcpyDeviceToHost);
+    const int nMax = *std::max_element(nc.begin(), nc.end());
+    for (int k = 0; k < e->nInst; ++k)
+        lim[k] = s0[k] + std::max(1, (int)((long long)std::max(probeSteps, 1) * nc[k] / std::max(nMax, 1)));
+    int* limD = nullptr;
+    if (cudaMalloc(&limD, e->nInst * sizeof(int)) != cudaSuccess) {
+        for (void* p : saved) cudaFree(p);
+        return efail(e, SIFV_ERR_CUDA, "cudaMalloc failed");
+    }
+    cudaMemcpy(limD, lim.data(), e->nInst * sizeof(int), cudaMemcpyHostToDevice);
+    e->A.stepLimit = limD;
     for (int bs : cands) {
-        // probe: every instance advances up to probeSteps steps past the
-        // furthest step count, without an end-time cap
+        if (bs > maxBs) continue;
         e->A.tEnd = 1e300;
-        e->A.maxSteps = *std::max_element(s0.begin(), s0.end()) + std::max(probeSteps, 1);
+        e->A.maxSteps = 0x7fffffff;
         cudaEventRecord(e->ev0, e->stream);
         if (launch(e, bs) != 0) continue;
         cudaEventRecord(e->ev1, e->stream);
@@ -325,6 +360,8 @@ int sifv_ensemble_autotune(sifv_ensemble_t* e, int probeSteps, int* blockSizeOut
         cudaMemcpyAsync(e->A.steps, s0.data(), e->nInst * sizeof(int), cudaMemcpyHostToDevice, e->stream);
         cudaStreamSynchronize(e->stream);
     }
+    e->A.stepLimit = nullptr;
+    cudaFree(limD);
     for (void* s : saved) cudaFree(s);
     e->blockSize = best;
     if (blockSizeOut) *blockSizeOut = best;

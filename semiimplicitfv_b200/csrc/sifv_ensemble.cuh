@@ -4,15 +4,24 @@
 // One CTA owns one instance and runs that instance's whole time loop
 // (the explicit step of ExplicitSolver::step, src/ExplicitSolver.cpp:68-203,
 // with the targetDt = tEnd - t cap of the reference's time loop,
-// src/RKTimeStepping.cpp:258-266): its own acoustic dt (block-wide minimum),
-// then per SSP-RK stage three phases separated by __syncthreads:
-//   1. conservative -> primitive of the interior and the ghost fill,
-//   2. face reconstruction + Riemann flux (+ upwinded partial-density flux),
-//   3. flux divergence, sources and the stage update.
-// Blocks never wait on each other, so instances of any size (and step
-// count) retire independently; the host orders instances by cost (N^2) so
-// the longest start first.  State arrays are packed per instance with
-// ghosts, x fastest (offsets in EnsArgs).
+// src/RKTimeStepping.cpp:258-266): its own acoustic dt (block-wide minimum
+// over the stored primitives), then per SSP-RK stage the instance is walked
+// in chunks of blockDim cells; per chunk, separated by __syncthreads:
+//   1. the primitives of the chunk and its 3-cell halo (ghosts through the
+//      PRIM ghost map, src/RectilinearMesh.cpp:498-524) are computed from the
+//      stage input into shared memory (FP64 conversion, T copies for the
+//      reconstruction),
+//   2. every face of the chunk: reconstruction + Riemann flux (+ upwinded
+//      partial-density flux), into shared memory,
+//   3. every cell: flux divergence, sources, the stage update and the
+//      multiphase clamps, written to the stage output; the last stage also
+//      writes the primitives of the new state.
+// The stage input and output are different packed states (S[0] the state,
+// S[1], S[2] scratch; the last stage writes S[0], which only the cell itself
+// reads there as U0), so chunks never see each other's updates.  Blocks never
+// wait on each other, so instances of any size (and step count) retire
+// independently; the host orders instances by cost (N^2) so the longest
+// start first.  State arrays are packed per instance with ghosts, x fastest.
 //
 // T is the arithmetic of the reconstruction / Riemann bulk (double: the
 // reference's operation order, bit-identical to the single-instance path;
@@ -21,8 +30,15 @@
 #pragma once
 
 #include "sifv_common.cuh"
+#include "sifv_fastmath.cuh"
 
 namespace sifv {
+
+struct EnsState {             // one packed conservative state
+    double *rho, *rhoU, *rhoE;
+    double* alphaRho[MAXPH];
+    double* alpha[MAXPH];
+};
 
 struct EnsArgs {
     Params P;                 // per-instance values nx / nxT are set per block
@@ -30,19 +46,9 @@ struct EnsArgs {
     const int* order;         // block -> instance (cost-sorted)
     const int* n;             // interior cells per instance
     const long long* off;     // packed cell offset per instance (ghosts included)
-    const long long* foff;    // packed face offset per instance (n + 1 faces)
-    // packed fields (ghosts included)
-    double *rho, *rhoU, *rhoE, *velU, *pres;
-    double* alphaRho[MAXPH];
-    double* alpha[MAXPH];
-    double *rho0, *rhoU0, *rhoE0, *pres0;
-    double* alphaRho0[MAXPH];
-    double* alpha0[MAXPH];
+    EnsState S[3];            // S[0]: the state; S[1], S[2]: stage outputs
+    double *velU, *pres;      // primitives of the state (rho: S[0].rho)
     const double* dx;         // packed cell widths (ghosts included)
-    // packed face scratch
-    double *fMass, *fMom, *fEnergy, *fVel;
-    double* fAlpha[MAXPH];
-    double* fAR[MAXPH];
     // per instance
     double* time;
     int* steps;
@@ -50,6 +56,7 @@ struct EnsArgs {
     int* status;              // 0 ok, 1 the time step was not positive (state blew up)
     double cfl, maxDt, constDt, tEnd;
     int maxSteps;
+    const int* stepLimit;     // per-instance step limit (autotuner probes), may be null
 };
 
 // std::min(dt, x) over a block, NaN ignored; result broadcast to all threads.
@@ -71,13 +78,45 @@ __device__ __forceinline__ double block_min_bcast(double v, double* sm) {
     return sm[32];
 }
 
+// Dynamic shared memory of one block of `threads` threads (chunks of
+// threads - 6 cells): staged primitives (T), FP64 density / partial
+// densities (multiphase), the face values (FP64) and, with FP32 bulk
+// arithmetic, both face values of every staged cell (T).
 template <typename T, int NPH>
-__global__ void __launch_bounds__(512) k_ensemble(EnsArgs A) {
+__host__ __device__ constexpr size_t ens_smem_bytes(int threads) {
+    return ((size_t)(3 + NPH) * threads * sizeof(T) + 7) / 8 * 8 +
+           (NPH > 0 ? (size_t)(1 + NPH) * threads * sizeof(double) : 0) +
+           (size_t)(4 + 2 * NPH) * (threads - 5) * sizeof(double) +
+           (sizeof(T) == 4 ? ((size_t)2 * (3 + NPH) * threads * sizeof(T) + 7) / 8 * 8 : 0);
+}
+
+// Largest block: 1024 threads with FP32 bulk arithmetic (fits the register
+// file at <= 64 registers per thread), 512 with FP64.
+template <typename T>
+struct EnsMaxThreads {
+    static constexpr int value = (sizeof(T) == 4) ? 1024 : 512;
+};
+
+template <typename T, int NPH>
+__global__ void __launch_bounds__(EnsMaxThreads<T>::value) k_ensemble(EnsArgs A) {
+    extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double red[33];
+    constexpr int NVR = 3 + NPH;       // reconstructed: rho, u, p, alpha[NPH]
+    const int CH = blockDim.x - 6;     // cells per chunk: the chunk and its 3-cell halo fill the block
+    const int W = CH + 6;              // staged positions
+    T* sW = reinterpret_cast<T*>(smraw);
+    double* sD = reinterpret_cast<double*>(smraw + ((size_t)NVR * W * sizeof(T) + 7) / 8 * 8);
+    double* sF = sD + (NPH > 0 ? (1 + NPH) * W : 0);   // face values (4 + 2 NPH rows of CH + 1):
+                                                         // mass, mom, energy, fvel, alpha[NPH], AR[NPH]
+    // FP32 bulk: per staged cell its high-face (sHi) and low-face (sLo) values
+    // from one set of WENO5 smoothness indicators (mixed precision only)
+    T* sHi = reinterpret_cast<T*>(sF + (4 + 2 * NPH) * (CH + 1));
+    T* sLo = sHi + NVR * W;
+    constexpr bool kPair = sizeof(T) == 4;
+
     const int inst = A.order[blockIdx.x];
     const int n = A.n[inst];
     const long long base = A.off[inst];
-    const long long fb = A.foff[inst];
     Params P = A.P;
     const int ng = P.ngx;
     P.nx = n;
@@ -88,11 +127,12 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs A) {
     double t = A.time[inst];
     int steps = A.steps[inst];
     double dtLast = 0.0;
-    // cell q (may be a ghost) -> packed index
     auto at = [&](int q) -> long long { return base + ng + q; };
+    const EnsState& S0 = A.S[0];
 
-    while (t < A.tEnd && steps < A.maxSteps) {
-        // ---- dt: computeAcousticTimeStep (src/RKTimeStepping.cpp:43-123) ----
+    const int limit = A.stepLimit ? min(A.maxSteps, A.stepLimit[inst]) : A.maxSteps;
+    while (t < A.tEnd && steps < limit) {
+        // ---- dt: computeAcousticTimeStep (src/RKTimeStepping.cpp:43-123) on the stored primitives ----
         double dt;
         if (A.constDt > 0) {
             dt = A.constDt;
@@ -105,12 +145,12 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs A) {
                     double a[NPH > 0 ? NPH : 1], ar[NPH > 0 ? NPH : 1];
 #pragma unroll
                     for (int ph = 0; ph < NPH; ++ph) {
-                        a[ph] = (ph < P.nPh) ? A.alpha[ph][c] : 0.0;
-                        ar[ph] = (ph < P.nPh) ? A.alphaRho[ph][c] : 0.0;
+                        a[ph] = (ph < P.nPh) ? S0.alpha[ph][c] : 0.0;
+                        ar[ph] = (ph < P.nPh) ? S0.alphaRho[ph][c] : 0.0;
                     }
-                    cs = mixture_sound_speed<NPH>(P, A.rho[c], A.pres[c], a, ar);
+                    cs = mixture_sound_speed<NPH>(P, S0.rho[c], A.pres[c], a, ar);
                 } else {
-                    cs = single_sound_speed(P, A.rho[c], A.pres[c]);
+                    cs = single_sound_speed(P, S0.rho[c], A.pres[c]);
                 }
                 v = smin(v, A.cfl * (A.dx[c] / (fabs(A.velU[c]) + cs)));
             }
@@ -135,223 +175,297 @@ __global__ void __launch_bounds__(512) k_ensemble(EnsArgs A) {
                 else if (s == 1) { c1 = 1.0; c2 = 3.0; c3 = 1.0; c4 = 4.0; }
                 else { c1 = 2.0; c2 = 1.0; c3 = 2.0; c4 = 3.0; }
             }
-            // ---- phase 1: cons -> prim (interior), then PRIM ghost fill ----
-            for (int q = threadIdx.x; q < n; q += blockDim.x) {
-                long long c = at(q);
-                if (NPH > 0) {
-                    double rho = 0.0;
+            // stage input / output: S0 -> S1 (-> S2) -> S0; RK1 writes S1 and copies it back
+            const EnsState& In = A.S[s];
+            const bool lastStage = (s == RK - 1);
+            const EnsState& Out = (lastStage && RK > 1) ? A.S[0] : A.S[s + 1];
+            const bool writePrim = lastStage && RK > 1;
+
+            for (int c0 = 0; c0 < n; c0 += CH) {
+                // ---- 1. primitives of positions c0-3 .. c0+CH+2 ----
+                for (int k = threadIdx.x; k < W; k += blockDim.x) {
+                    const int q = c0 - 3 + k;
+                    if (q >= n + 3) {
 #pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph)
-                        if (ph < P.nPh) rho += A.alphaRho[ph][c];
-                    double rs = smax(rho, 1e-14);
-                    A.rho[c] = rs;
-                    double u = A.rhoU[c] / rs;
-                    A.velU[c] = u;
-                    double ke = 0.5 * rs * u * u;
+                        for (int v = 0; v < NVR; ++v) sW[v * W + k] = T(0.0);
+                        continue;
+                    }
+                    double sn, sa;
+                    const int sq = prim_src(q, n, P.bc[0], P.bc[1], sn, sa);
+                    const long long c = at(sq);
+                    double rhoP, u, p;
                     double a[NPH > 0 ? NPH : 1];
+                    if (NPH > 0) {
+                        double rho = 0.0;
 #pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph) a[ph] = (ph < P.nPh) ? A.alpha[ph][c] : 0.0;
-                    A.pres[c] = mixture_pressure<NPH>(P, A.rhoE[c] - ke, a);
-                } else {
-                    double rho = smax(A.rho[c], 1e-14);
-                    double u = A.rhoU[c] / rho;
-                    double ke = 0.0 + u * u;
-                    ke *= 0.5 * rho;
-                    double e = A.rhoE[c] - ke;
-                    A.velU[c] = u;
-                    A.pres[c] = P.eosStiffened ? (P.gamma - 1.0) * e - P.gamma * P.pInf
-                                               : smax((P.gamma - 1.0) * e, 1e-14);
-                }
-            }
-            __syncthreads();
-            for (int g = threadIdx.x; g < 2 * ng; g += blockDim.x) {
-                int q = (g < ng) ? -1 - g : n + (g - ng);
-                double sn, sa;
-                int sq = prim_src(q, n, P.bc[0], P.bc[1], sn, sa);
-                long long d = at(q), sc = at(sq);
-                A.rho[d] = A.rho[sc];
-                A.velU[d] = (sn * sa) * A.velU[sc];
-                A.pres[d] = A.pres[sc];
+                        for (int ph = 0; ph < NPH; ++ph)
+                            if (ph < P.nPh) rho += In.alphaRho[ph][c];
+                        const double rs = smax(rho, 1e-14);
+                        rhoP = rs;
+                        u = In.rhoU[c] / rs;
+                        const double ke = 0.5 * rs * u * u;
 #pragma unroll
-                for (int ph = 0; ph < NPH; ++ph)
-                    if (ph < P.nPh) { A.alphaRho[ph][d] = A.alphaRho[ph][sc]; A.alpha[ph][d] = A.alpha[ph][sc]; }
-            }
-            __syncthreads();
-            // ---- phase 2: faces f in [0, n]: left cell f-1, right cell f ----
-            for (int f = threadIdx.x; f <= n; f += blockDim.x) {
-                FaceState<NPH, T> L, R;
-                L.u[1] = L.u[2] = R.u[1] = R.u[2] = T(0.0);
-                L.sigma = R.sigma = T(0.0);
-                long long c = at(f);
-                auto rec = [&](const double* fld, T& l, T& r) {
-                    T v0 = T(fld[c - 3]), v1 = T(fld[c - 2]), v2 = T(fld[c - 1]), v3 = T(fld[c]),
-                      v4 = T(fld[c + 1]), v5 = T(fld[c + 2]);
-                    if (weno) { l = weno5L<T>(v0, v1, v2, v3, v4, T(eps)); r = weno5R<T>(v1, v2, v3, v4, v5, T(eps)); }
-                    else { l = upwind5L<T>(v0, v1, v2, v3, v4); r = upwind5R<T>(v1, v2, v3, v4, v5); }
-                };
-                rec(A.rho, L.rho, R.rho);
-                rec(A.velU, L.u[0], R.u[0]);
-                rec(A.pres, L.p, R.p);
+                        for (int ph = 0; ph < NPH; ++ph) a[ph] = (ph < P.nPh) ? In.alpha[ph][c] : 0.0;
+                        p = mixture_pressure<NPH>(P, In.rhoE[c] - ke, a);
+                        sD[k] = rs;
 #pragma unroll
-                for (int ph = 0; ph < NPH; ++ph) {
-                    L.alpha[ph] = R.alpha[ph] = T(0.0);
-                    if (ph < P.nPh) rec(A.alpha[ph], L.alpha[ph], R.alpha[ph]);
+                        for (int ph = 0; ph < NPH; ++ph) sD[(1 + ph) * W + k] = (ph < P.nPh) ? In.alphaRho[ph][c] : 0.0;
+                    } else {
+                        const double rc = In.rho[c];
+                        const double rho = smax(rc, 1e-14);
+                        u = In.rhoU[c] / rho;
+                        double ke = 0.0 + u * u;
+                        ke *= 0.5 * rho;
+                        const double e = In.rhoE[c] - ke;
+                        p = P.eosStiffened ? (P.gamma - 1.0) * e - P.gamma * P.pInf : smax((P.gamma - 1.0) * e, 1e-14);
+                        rhoP = rc;
+                    }
+                    sW[k] = T(rhoP);
+                    sW[W + k] = T((sn * sa) * u);
+                    sW[2 * W + k] = T(p);
+#pragma unroll
+                    for (int ph = 0; ph < NPH; ++ph) sW[(3 + ph) * W + k] = T(a[ph]);
                 }
-                if (NPH > 0) {
-                    eff_gamma_piinf<NPH, T>(P, L.alpha, L.gEff, L.piEff);
-                    eff_gamma_piinf<NPH, T>(P, R.alpha, R.gEff, R.piEff);
-                } else {
-                    L.gEff = R.gEff = T(P.gamma);
-                    L.piEff = R.piEff = T(P.pInf);
+                __syncthreads();
+                if (kPair && weno) {   // staged cells 2 .. CH+3 (left cells and right cells of the faces)
+                    for (int k = threadIdx.x + 2; k <= CH + 3; k += blockDim.x) {
+#pragma unroll
+                        for (int v = 0; v < NVR; ++v) {
+                            if (v >= 3 && v - 3 >= P.nPh) continue;
+                            const T* w = sW + v * W + k - 2;
+                            weno5_pair(w[0], w[1], w[2], w[3], w[4], T(eps), sHi[v * W + k], sLo[v * W + k]);
+                        }
+                    }
+                    __syncthreads();
                 }
-                FaceFlux<NPH, T> Fx;
-                switch (P.riemann) {
-                    case SIFV_HLLC: hllc_flux<0, NPH, T>(P, L, R, Fx); break;
-                    case SIFV_RUSANOV: rusanov_flux<0, NPH, T>(P, L, R, Fx); break;
-                    default: lf_flux<0, NPH, T>(P, L, R, Fx); break;
-                }
-                const long long fi = fb + f;
-                A.fMass[fi] = (double)Fx.mass;
-                A.fMom[fi] = (double)Fx.mom[0];
-                A.fEnergy[fi] = (double)Fx.energy;
-                if (NPH > 0) {
-                    A.fVel[fi] = (double)Fx.fvel;
-                    long long upw = ((double)Fx.mass >= 0) ? c - 1 : c;
-                    double rhoUpw = smax(A.rho[upw], 1e-14);
+                // ---- 2. faces f = c0 .. c0+CH (left cell f-1, right cell f) ----
+                for (int k = threadIdx.x; k <= CH; k += blockDim.x) {
+                    const int f = c0 + k;
+                    if (f > n) continue;
+                    FaceState<NPH, T> L, R;
+                    L.u[1] = L.u[2] = R.u[1] = R.u[2] = T(0.0);
+                    L.sigma = R.sigma = T(0.0);
+                    auto rec = [&](int v, T& l, T& r) {
+                        const T* w = sW + v * W + k;   // cells f-3 .. f+2
+                        if (kPair && weno) { l = sHi[v * W + k + 2]; r = sLo[v * W + k + 3]; }
+                        else if (weno) { l = weno5L<T>(w[0], w[1], w[2], w[3], w[4], T(eps)); r = weno5R<T>(w[1], w[2], w[3], w[4], w[5], T(eps)); }
+                        else { l = upwind5L<T>(w[0], w[1], w[2], w[3], w[4]); r = upwind5R<T>(w[1], w[2], w[3], w[4], w[5]); }
+                    };
+                    rec(0, L.rho, R.rho);
+                    rec(1, L.u[0], R.u[0]);
+                    rec(2, L.p, R.p);
 #pragma unroll
                     for (int ph = 0; ph < NPH; ++ph) {
-                        if (ph < P.nPh) {
-                            A.fAlpha[ph][fi] = (double)Fx.alpha[ph];
-                            A.fAR[ph][fi] = (A.alphaRho[ph][upw] / rhoUpw) * (double)Fx.mass;
+                        L.alpha[ph] = R.alpha[ph] = T(0.0);
+                        if (ph < P.nPh) rec(3 + ph, L.alpha[ph], R.alpha[ph]);
+                    }
+                    if (NPH > 0) {
+                        eff_gamma_piinf<NPH, T>(P, L.alpha, L.gEff, L.piEff);
+                        eff_gamma_piinf<NPH, T>(P, R.alpha, R.gEff, R.piEff);
+                    } else {
+                        L.gEff = R.gEff = T(P.gamma);
+                        L.piEff = R.piEff = T(P.pInf);
+                    }
+                    FaceFlux<NPH, T> Fx;
+                    switch (P.riemann) {
+                        case SIFV_HLLC: hllc_flux<0, NPH, T>(P, L, R, Fx); break;
+                        case SIFV_RUSANOV: rusanov_flux<0, NPH, T>(P, L, R, Fx); break;
+                        default: lf_flux<0, NPH, T>(P, L, R, Fx); break;
+                    }
+                    const int ldF = CH + 1;
+                    sF[k] = (double)Fx.mass;
+                    sF[ldF + k] = (double)Fx.mom[0];
+                    sF[2 * ldF + k] = (double)Fx.energy;
+                    if (NPH > 0) {
+                        sF[3 * ldF + k] = (double)Fx.fvel;
+                        const int upw = ((double)Fx.mass >= 0) ? k + 2 : k + 3;   // staged index of cell f-1 or f
+                        const double rhoUpw = smax(sD[upw], 1e-14);
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph) {
+                            if (ph < P.nPh) {
+                                sF[(4 + ph) * ldF + k] = (double)Fx.alpha[ph];
+                                sF[(4 + NPH + ph) * ldF + k] = (sD[(1 + ph) * W + upw] / rhoUpw) * (double)Fx.mass;
+                            }
                         }
                     }
                 }
-            }
-            __syncthreads();
-            // ---- phase 3: divergence (src/ExplicitSolver.cpp:294-496) + update (127-188) ----
-            for (int q = threadIdx.x; q < n; q += blockDim.x) {
-                long long c = at(q);
-                const long long fl = fb + q, fh = fb + q + 1;
-                double coeff = (1.0 * 1.0) / ((A.dx[c] * 1.0) * 1.0);
-                double rR = 0.0, rU = 0.0, rE = 0.0;
-                rR += coeff * A.fMass[fl]; rR -= coeff * A.fMass[fh];
-                rU += coeff * A.fMom[fl]; rU -= coeff * A.fMom[fh];
-                rE += coeff * A.fEnergy[fl]; rE -= coeff * A.fEnergy[fh];
-                double rAR[NPH > 0 ? NPH : 1], rA[NPH > 0 ? NPH : 1];
-                if (NPH > 0) {
-                    double divU = 0.0;
-                    divU -= coeff * A.fVel[fl];
-                    divU += coeff * A.fVel[fh];
+                __syncthreads();
+                // ---- 3. cells: divergence (src/ExplicitSolver.cpp:294-496) + update (127-188) ----
+                for (int k = threadIdx.x; k < CH; k += blockDim.x) {
+                    const int q = c0 + k;
+                    if (q >= n) continue;
+                    const long long c = at(q);
+                    const int ldF = CH + 1;
+                    const int fl = k, fh = k + 1;
+                    double coeff = (1.0 * 1.0) / ((A.dx[c] * 1.0) * 1.0);
+                    double rR = 0.0, rU = 0.0, rE = 0.0;
+                    rR += coeff * sF[fl]; rR -= coeff * sF[fh];
+                    rU += coeff * sF[ldF + fl]; rU -= coeff * sF[ldF + fh];
+                    rE += coeff * sF[2 * ldF + fl]; rE -= coeff * sF[2 * ldF + fh];
+                    double rAR[NPH > 0 ? NPH : 1], rA[NPH > 0 ? NPH : 1];
+                    if (NPH > 0) {
+                        double divU = 0.0;
+                        divU -= coeff * sF[3 * ldF + fl];
+                        divU += coeff * sF[3 * ldF + fh];
 #pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph) {
-                        if (ph < P.nPh) {
-                            double r1 = 0.0, r2 = 0.0;
-                            r1 += coeff * A.fAR[ph][fl]; r1 -= coeff * A.fAR[ph][fh];
-                            r2 += coeff * A.fAlpha[ph][fl]; r2 -= coeff * A.fAlpha[ph][fh];
-                            r2 += A.alpha[ph][c] * divU;
-                            rAR[ph] = r1;
-                            rA[ph] = r2;
+                        for (int ph = 0; ph < NPH; ++ph) {
+                            if (ph < P.nPh) {
+                                double r1 = 0.0, r2 = 0.0;
+                                r1 += coeff * sF[(4 + NPH + ph) * ldF + fl]; r1 -= coeff * sF[(4 + NPH + ph) * ldF + fh];
+                                r2 += coeff * sF[(4 + ph) * ldF + fl]; r2 -= coeff * sF[(4 + ph) * ldF + fh];
+                                r2 += In.alpha[ph][c] * divU;
+                                rAR[ph] = r1;
+                                rA[ph] = r2;
+                            }
+                        }
+                    }
+                    // the stage input's density: the primitive (mixture: max(sum alphaRho, 1e-14))
+                    const double rhoIn = (NPH > 0) ? sD[k + 3] : In.rho[c];
+                    double nRho, nU, nE, nAR[NPH > 0 ? NPH : 1], nA[NPH > 0 ? NPH : 1];
+                    if (RK == 1) {
+                        nRho = rhoIn + dt * rR;
+                        nU = In.rhoU[c] + dt * rU;
+                        nE = In.rhoE[c] + dt * rE;
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph)
+                            if (ph < P.nPh) nAR[ph] = In.alphaRho[ph][c] + dt * rAR[ph];
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph)
+                            if (ph < P.nPh) nA[ph] = In.alpha[ph][c] + dt * rA[ph];
+                    } else {
+                        // U0 = the step-start state S0 (its density the step-start primitive)
+                        const double rho0 = (s == 0) ? rhoIn : S0.rho[c];
+                        nRho = (c1 * rhoIn + c2 * rho0 + c3 * dt * rR) / c4;
+                        nU = (c1 * In.rhoU[c] + c2 * S0.rhoU[c] + c3 * dt * rU) / c4;
+                        nE = (c1 * In.rhoE[c] + c2 * S0.rhoE[c] + c3 * dt * rE) / c4;
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph)
+                            if (ph < P.nPh)
+                                nAR[ph] = (c1 * In.alphaRho[ph][c] + c2 * S0.alphaRho[ph][c] + c3 * dt * rAR[ph]) / c4;
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph)
+                            if (ph < P.nPh) nA[ph] = (c1 * In.alpha[ph][c] + c2 * S0.alpha[ph][c] + c3 * dt * rA[ph]) / c4;
+                    }
+                    if (NPH > 0) {   // src/ExplicitSolver.cpp:169-185
+                        double rhoSum = 0.0;
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph) {
+                            if (ph < P.nPh) {
+                                double v = smax(nAR[ph], 1e-14);
+                                nAR[ph] = v;
+                                rhoSum += v;
+                            }
+                        }
+                        nRho = rhoSum;
+                        double a[NPH > 0 ? NPH : 1];
+                        double aSum = 0.0;
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph)
+                            if (ph < P.nPh) a[ph] = smax(nA[ph], P.alphaMin);
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph)
+                            if (ph < P.nPh) aSum += a[ph];
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph)
+                            if (ph < P.nPh) nA[ph] = a[ph] / aSum;
+                    }
+                    Out.rho[c] = nRho;
+                    Out.rhoU[c] = nU;
+                    Out.rhoE[c] = nE;
+#pragma unroll
+                    for (int ph = 0; ph < NPH; ++ph)
+                        if (ph < P.nPh) { Out.alphaRho[ph][c] = nAR[ph]; Out.alpha[ph][c] = nA[ph]; }
+                    if (writePrim) {   // final cons -> prim (src/ExplicitSolver.cpp:192-200)
+                        if (NPH > 0) {
+                            double rho = 0.0;
+#pragma unroll
+                            for (int ph = 0; ph < NPH; ++ph)
+                                if (ph < P.nPh) rho += nAR[ph];
+                            const double rs = smax(rho, 1e-14);
+                            Out.rho[c] = rs;
+                            const double u = nU / rs;
+                            A.velU[c] = u;
+                            const double ke = 0.5 * rs * u * u;
+                            double a[NPH > 0 ? NPH : 1];
+#pragma unroll
+                            for (int ph = 0; ph < NPH; ++ph) a[ph] = (ph < P.nPh) ? nA[ph] : 0.0;
+                            A.pres[c] = mixture_pressure<NPH>(P, nE - ke, a);
+                        } else {
+                            const double rho = smax(nRho, 1e-14);
+                            const double u = nU / rho;
+                            double ke = 0.0 + u * u;
+                            ke *= 0.5 * rho;
+                            const double e = nE - ke;
+                            A.velU[c] = u;
+                            A.pres[c] = P.eosStiffened ? (P.gamma - 1.0) * e - P.gamma * P.pInf
+                                                       : smax((P.gamma - 1.0) * e, 1e-14);
                         }
                     }
                 }
-                if (s == 0 && RK > 1) {
-                    A.rho0[c] = A.rho[c]; A.rhoU0[c] = A.rhoU[c]; A.rhoE0[c] = A.rhoE[c]; A.pres0[c] = A.pres[c];
+                __syncthreads();
+            }
+            if (lastStage && RK == 1) {   // S1 -> S0 and the primitives of the new state
+                const EnsState& S1 = A.S[1];
+                for (int q = threadIdx.x; q < n; q += blockDim.x) {
+                    const long long c = at(q);
+                    double nAR[NPH > 0 ? NPH : 1], nA[NPH > 0 ? NPH : 1];
+                    const double nU = S1.rhoU[c], nE = S1.rhoE[c];
+                    S0.rhoU[c] = nU;
+                    S0.rhoE[c] = nE;
 #pragma unroll
                     for (int ph = 0; ph < NPH; ++ph)
-                        if (ph < P.nPh) { A.alphaRho0[ph][c] = A.alphaRho[ph][c]; A.alpha0[ph][c] = A.alpha[ph][c]; }
-                }
-                if (RK == 1) {
-                    A.rho[c] += dt * rR;
-                    A.rhoU[c] += dt * rU;
-                    A.rhoE[c] += dt * rE;
-#pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph)
-                        if (ph < P.nPh) A.alphaRho[ph][c] += dt * rAR[ph];
-#pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph)
-                        if (ph < P.nPh) A.alpha[ph][c] += dt * rA[ph];
-                } else {
-                    A.rho[c] = (c1 * A.rho[c] + c2 * A.rho0[c] + c3 * dt * rR) / c4;
-                    A.rhoU[c] = (c1 * A.rhoU[c] + c2 * A.rhoU0[c] + c3 * dt * rU) / c4;
-                    A.rhoE[c] = (c1 * A.rhoE[c] + c2 * A.rhoE0[c] + c3 * dt * rE) / c4;
-#pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph)
-                        if (ph < P.nPh)
-                            A.alphaRho[ph][c] = (c1 * A.alphaRho[ph][c] + c2 * A.alphaRho0[ph][c] + c3 * dt * rAR[ph]) / c4;
-#pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph)
-                        if (ph < P.nPh) A.alpha[ph][c] = (c1 * A.alpha[ph][c] + c2 * A.alpha0[ph][c] + c3 * dt * rA[ph]) / c4;
-                }
-                if (NPH > 0) {   // src/ExplicitSolver.cpp:169-185
-                    double rhoSum = 0.0;
-#pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph) {
                         if (ph < P.nPh) {
-                            double v = smax(A.alphaRho[ph][c], 1e-14);
-                            A.alphaRho[ph][c] = v;
-                            rhoSum += v;
+                            nAR[ph] = S1.alphaRho[ph][c];
+                            nA[ph] = S1.alpha[ph][c];
+                            S0.alphaRho[ph][c] = nAR[ph];
+                            S0.alpha[ph][c] = nA[ph];
                         }
+                    if (NPH > 0) {
+                        double rho = 0.0;
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph)
+                            if (ph < P.nPh) rho += nAR[ph];
+                        const double rs = smax(rho, 1e-14);
+                        S0.rho[c] = rs;
+                        const double u = nU / rs;
+                        A.velU[c] = u;
+                        const double ke = 0.5 * rs * u * u;
+                        double a[NPH > 0 ? NPH : 1];
+#pragma unroll
+                        for (int ph = 0; ph < NPH; ++ph) a[ph] = (ph < P.nPh) ? nA[ph] : 0.0;
+                        A.pres[c] = mixture_pressure<NPH>(P, nE - ke, a);
+                    } else {
+                        const double nRho = S1.rho[c];
+                        S0.rho[c] = nRho;
+                        const double rho = smax(nRho, 1e-14);
+                        const double u = nU / rho;
+                        double ke = 0.0 + u * u;
+                        ke *= 0.5 * rho;
+                        const double e = nE - ke;
+                        A.velU[c] = u;
+                        A.pres[c] = P.eosStiffened ? (P.gamma - 1.0) * e - P.gamma * P.pInf
+                                                   : smax((P.gamma - 1.0) * e, 1e-14);
                     }
-                    A.rho[c] = rhoSum;
-                    double a[NPH > 0 ? NPH : 1];
-                    double aSum = 0.0;
-#pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph)
-                        if (ph < P.nPh) a[ph] = smax(A.alpha[ph][c], P.alphaMin);
-#pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph)
-                        if (ph < P.nPh) aSum += a[ph];
-#pragma unroll
-                    for (int ph = 0; ph < NPH; ++ph)
-                        if (ph < P.nPh) A.alpha[ph][c] = a[ph] / aSum;
                 }
-            }
-            __syncthreads();
-        }
-        // ---- final cons -> prim + ghosts (src/ExplicitSolver.cpp:192-200) ----
-        for (int q = threadIdx.x; q < n; q += blockDim.x) {
-            long long c = at(q);
-            if (NPH > 0) {
-                double rho = 0.0;
-#pragma unroll
-                for (int ph = 0; ph < NPH; ++ph)
-                    if (ph < P.nPh) rho += A.alphaRho[ph][c];
-                double rs = smax(rho, 1e-14);
-                A.rho[c] = rs;
-                double u = A.rhoU[c] / rs;
-                A.velU[c] = u;
-                double ke = 0.5 * rs * u * u;
-                double a[NPH > 0 ? NPH : 1];
-#pragma unroll
-                for (int ph = 0; ph < NPH; ++ph) a[ph] = (ph < P.nPh) ? A.alpha[ph][c] : 0.0;
-                A.pres[c] = mixture_pressure<NPH>(P, A.rhoE[c] - ke, a);
-            } else {
-                double rho = smax(A.rho[c], 1e-14);
-                double u = A.rhoU[c] / rho;
-                double ke = 0.0 + u * u;
-                ke *= 0.5 * rho;
-                double e = A.rhoE[c] - ke;
-                A.velU[c] = u;
-                A.pres[c] = P.eosStiffened ? (P.gamma - 1.0) * e - P.gamma * P.pInf : smax((P.gamma - 1.0) * e, 1e-14);
+                __syncthreads();
             }
         }
-        __syncthreads();
-        for (int g = threadIdx.x; g < 2 * ng; g += blockDim.x) {
-            int q = (g < ng) ? -1 - g : n + (g - ng);
-            double sn, sa;
-            int sq = prim_src(q, n, P.bc[0], P.bc[1], sn, sa);
-            long long d = at(q), sc = at(sq);
-            A.rho[d] = A.rho[sc];
-            A.velU[d] = (sn * sa) * A.velU[sc];
-            A.pres[d] = A.pres[sc];
-#pragma unroll
-            for (int ph = 0; ph < NPH; ++ph)
-                if (ph < P.nPh) { A.alphaRho[ph][d] = A.alphaRho[ph][sc]; A.alpha[ph][d] = A.alpha[ph][sc]; }
-        }
-        __syncthreads();
         t += dt;
         ++steps;
         dtLast = dt;
+    }
+    // PRIM ghost fill of the state (src/RectilinearMesh.cpp:498-524), for the caller
+    for (int g = threadIdx.x; g < 2 * ng; g += blockDim.x) {
+        int q = (g < ng) ? -1 - g : n + (g - ng);
+        double sn, sa;
+        int sq = prim_src(q, n, P.bc[0], P.bc[1], sn, sa);
+        long long d = at(q), sc = at(sq);
+        S0.rho[d] = S0.rho[sc];
+        A.velU[d] = (sn * sa) * A.velU[sc];
+        A.pres[d] = A.pres[sc];
+#pragma unroll
+        for (int ph = 0; ph < NPH; ++ph)
+            if (ph < P.nPh) { S0.alphaRho[ph][d] = S0.alphaRho[ph][sc]; S0.alpha[ph][d] = S0.alpha[ph][sc]; }
     }
     if (threadIdx.x == 0) {
         A.time[inst] = t;
