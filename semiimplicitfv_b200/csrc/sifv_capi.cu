@@ -68,7 +68,8 @@ struct sifv_ctx {
     size_t adjStageCap = 0;
     bool adjReady = false;
     bool igrTileReady = false;
-    double* jacCoef = nullptr;                // per-cell Jacobi coefficients (2 dim + 2 arrays)
+    double* jacCoef = nullptr;                // Jacobi coefficients: per face (dim arrays) or per cell (2 dim + 2)
+    bool uniformAxes = false;                 // interior cell widths bitwise equal along every active axis
     double* tileB[4] = {nullptr, nullptr, nullptr, nullptr};   // 2D fused-stage scratch states
     double* tileC[4] = {nullptr, nullptr, nullptr, nullptr};                // dynamic shared memory limit of the IGR tile kernel set
     double* lam[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -318,12 +319,16 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
     CUDA_TRY(c, cudaMemsetAsync(&c->ctl->jacobiDone, 0, sizeof(int), c->stream));
     CUDA_TRY(c, cudaMemsetAsync(c->ctl->res, 0, sizeof(unsigned long long) * (size_t)maxIter, c->stream));
     unsigned g = blocks((long long)c->nint, kCellThreads);
+    const bool faceCoef = c->uniformAxes;
     if (!c->jacCoef) {
         int sa = SIFV_OK;
-        c->jacCoef = dalloc(c, c->ncells * (size_t)(2 * c->P.dim + 2), sa);
+        c->jacCoef = dalloc(c, c->ncells * (size_t)(faceCoef ? c->P.dim : 2 * c->P.dim + 2), sa);
         if (sa != SIFV_OK) return sa;
     }
-    k_jacobi_coef<<<g, kCellThreads, 0, c->stream>>>(c->P, rho, rhoc2, c->F, c->ctl, c->jacCoef, c->ncells);
+    if (faceCoef)
+        k_jacobi_fcoef<<<g, kCellThreads, 0, c->stream>>>(c->P, rho, c->F, c->jacCoef, c->ncells);
+    else
+        k_jacobi_coef<<<g, kCellThreads, 0, c->stream>>>(c->P, rho, rhoc2, c->F, c->ctl, c->jacCoef, c->ncells);
     int it = 0, batch = 4;
     int done = 0;
     while (it < maxIter) {
@@ -331,8 +336,12 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
         for (int q = 0; q < nb; ++q, ++it) {
             const double* pin = (it & 1) ? c->F.pB : c->F.pA;
             double* pout = (it & 1) ? c->F.pA : c->F.pB;
-            k_jacobi_pre<<<g, kCellThreads, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhs, pin, pout, c->ctl, it,
-                                                            tol);
+            if (faceCoef)
+                k_jacobi_face<<<g, kCellThreads, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhoc2, rhs, pin, pout,
+                                                                 c->ctl, it, tol);
+            else
+                k_jacobi_pre<<<g, kCellThreads, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhs, pin, pout, c->ctl,
+                                                                it, tol);
         }
         c->launches += nb;
         LAUNCH_CHECK(c);
@@ -695,6 +704,13 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
         return w;
     };
     std::vector<double> dxv = widths(xe), dyv = widths(ye), dzv = widths(ze);
+    auto uniform = [](const std::vector<double>& w, int ng, int n) {
+        for (int i = 1; i < n; ++i)
+            if (!(w[ng + i] == w[ng])) return false;
+        return true;
+    };
+    c->uniformAxes = uniform(dxv, P.ngx, nx) && (dim < 2 || uniform(dyv, P.ngy, ny)) &&
+                     (dim < 3 || uniform(dzv, P.ngz, nz));
     double dx0 = dxv[P.ngx];
     c->alphaIGR = cfg->alphaCoeff * dx0 * dx0;   // src/IGR.cpp:108
     auto a2 = [&](const std::vector<double>& w) {
