@@ -235,6 +235,15 @@ int sifv_profile_step(sifv_ctx_t* ctx, int step, double time, double targetDt, c
  * call, and the number of kernel launches it made. */
 int sifv_last_step_stats(const sifv_ctx_t* ctx, double* deviceMs, int* launches);
 
+/* ---- pressure solver selection ----------------------------------------- */
+/* The PressureSolver plugin the semi-implicit step and sifv_pressure_solve
+ * use: JacobiPressureSolver (src/JacobiPressureSolver.cpp:57-108, default)
+ * or GaussSeidelPressureSolver (src/GaussSeidelPressureSolver.cpp:10-49,
+ * lexicographic in-place sweeps run as a tiled wavefront, bit-identical). */
+#define SIFV_PRESSURE_JACOBI 0
+#define SIFV_PRESSURE_GAUSS_SEIDEL 1
+int sifv_set_pressure_solver(sifv_ctx_t* ctx, int kind);
+
 /* ---- diagnostics ----------------------------------------------------------- */
 /* Maximum relative error of the fast paths' reciprocal and square root
  * against IEEE 1/x and sqrt(x) over n arguments spread across [2^-60, 2^60)

@@ -70,6 +70,8 @@ struct sifv_ctx {
     bool igrTileReady = false;
     double* jacCoef = nullptr;                // Jacobi coefficients: per face (dim arrays) or per cell (2 dim + 2)
     bool uniformAxes = false;                 // interior cell widths bitwise equal along every active axis
+    int pressureKind = 0;                     // 0 Jacobi (default), 1 Gauss-Seidel
+    double* gsCoef = nullptr;                 // per-cell Gauss-Seidel coefficients (2 dim + 2 arrays)
     double* tileB[4] = {nullptr, nullptr, nullptr, nullptr};   // 2D fused-stage scratch states
     double* tileC[4] = {nullptr, nullptr, nullptr, nullptr};                // dynamic shared memory limit of the IGR tile kernel set
     double* lam[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -367,6 +369,88 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
     return SIFV_OK;
 }
 
+// GaussSeidelPressureSolver::solve on the device: in place on F.pA (the
+// initial guess), coefficients once per solve, per iteration a scalar ghost
+// fill and one tiled-wavefront sweep; convergence as jacobi_run.
+int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rhs, double tol, int maxIter,
+           int& iters, const double*& result) {
+    int st = ensure_res(c, maxIter);
+    if (st != SIFV_OK) return st;
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->jacobiDone, 0, sizeof(int), c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->ctl->res, 0, sizeof(unsigned long long) * (size_t)maxIter, c->stream));
+    const Params& P = c->P;
+    unsigned g = blocks((long long)c->nint, kCellThreads);
+    if (!c->gsCoef) {
+        int sa = SIFV_OK;
+        c->gsCoef = dalloc(c, c->ncells * (size_t)(2 * P.dim + 2), sa);
+        if (sa != SIFV_OK) return sa;
+    }
+    k_jacobi_coef<<<g, kCellThreads, 0, c->stream>>>(P, rho, rhoc2, c->F, c->ctl, c->gsCoef, c->ncells);
+    constexpr int T3 = 16, T2X = 32, T2Y = 64;
+    const bool d3 = P.dim == 3;
+    const int tx = d3 ? T3 : T2X, ty = d3 ? T3 : T2Y, tz = d3 ? T3 : 1;
+    const int ntx = (P.nx + tx - 1) / tx, nty = (P.ny + ty - 1) / ty, ntz = (P.nz + tz - 1) / tz;
+    const int nplanes = ntx + nty + ntz - 2;
+    const size_t smem = d3 ? gs_tile_smem<T3, T3, T3>() : gs_tile_smem<T2X, T2Y, 1>();
+    if (P.dim >= 2) {
+        cudaError_t e = d3 ? cudaFuncSetAttribute(k_gs_tile<T3, T3, T3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)smem)
+                           : cudaFuncSetAttribute(k_gs_tile<T2X, T2Y, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)smem);
+        if (e != cudaSuccess) return fail(c, SIFV_ERR_CUDA, std::string("GS tile smem: ") + cudaGetErrorString(e));
+    }
+    double* pp = c->F.pA;
+    int it = 0, batch = 2, done = 0;
+    while (it < maxIter) {
+        int nb = std::min(batch, maxIter - it);
+        for (int q = 0; q < nb; ++q, ++it) {
+            k_gs_ghosts<<<blocks((long long)c->ncells, kCellThreads), kCellThreads, 0, c->stream>>>(P, pp, c->ctl, it,
+                                                                                                     tol);
+            if (P.dim == 1) {
+                k_gs_sweep_1d<<<1, 32, 0, c->stream>>>(P, c->gsCoef, c->ncells, rhs, pp, c->ctl, it, tol);
+                c->launches += 2;
+            } else {
+                for (int pl = 0; pl < nplanes; ++pl) {
+                    if (d3)
+                        k_gs_tile<T3, T3, T3><<<(unsigned)(nty * ntz), T3 * T3, smem, c->stream>>>(
+                            P, c->gsCoef, c->ncells, rhs, pp, c->ctl, it, tol, pl, ntx, nty);
+                    else
+                        k_gs_tile<T2X, T2Y, 1><<<(unsigned)nty, T2Y, smem, c->stream>>>(P, c->gsCoef, c->ncells, rhs,
+                                                                                      pp, c->ctl, it, tol, pl, ntx,
+                                                                                      nty);
+                }
+                c->launches += 1 + nplanes;
+            }
+        }
+        LAUNCH_CHECK(c);
+        CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl) + sizeof(unsigned long long) * (size_t)it,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        if (c->ctlHost->jacobiDone) {
+            done = c->ctlHost->jacobiDone;
+            break;
+        }
+        double last;
+        unsigned long long b = c->ctlHost->res[it - 1];
+        std::memcpy(&last, &b, sizeof(double));
+        if (last < tol) {
+            done = it;
+            break;
+        }
+        batch = std::min(batch * 2, 16);
+    }
+    iters = done ? done : maxIter;
+    result = pp;
+    mark(c, "gauss_seidel");
+    return SIFV_OK;
+}
+
+int pressure_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rhs, double tol, int maxIter,
+                 int& iters, const double*& result) {
+    if (c->pressureKind == 1) return gs_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
+    return jacobi_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
+}
+
 void rk_coef(int order, int s, StageCoef& K) {
     // src/ExplicitSolver.cpp:92-103
     static const double t1[1][4] = {{1.0, 0.0, 1.0, 1.0}};
@@ -535,8 +619,8 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
             LAUNCH_CHECK(c);
             int iters = 0;
             const double* pres = nullptr;
-            int st = jacobi_run(c, c->F.rho, c->F.rhoc2, c->F.pRhs, cfg.pressureTol, cfg.maxPressureIters, iters,
-                                pres);
+            int st = pressure_run(c, c->F.rho, c->F.rhoc2, c->F.pRhs, cfg.pressureTol, cfg.maxPressureIters, iters,
+                                  pres);
             if (st != SIFV_OK) return st;
             c->lastIters = iters;
             if (iters >= cfg.maxPressureIters) {
@@ -952,10 +1036,13 @@ int sifv_pressure_solve(sifv_ctx_t* c, const double* rho, const double* rhoc2, c
     CUDA_TRY(c, cudaMemcpyAsync(&c->ctl->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
     int n = 0;
     const double* res = nullptr;
-    int st = jacobi_run(c, dRho, dRhoc2, dRhs, tol, maxIter, n, res);
+    int st = pressure_run(c, dRho, dRhoc2, dRhs, tol, maxIter, n, res);
     if (st != SIFV_OK) return st;
-    k_jacobi_finish<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, c->F.pA, c->F.pB,
-                                                                                             dP, c->ctl, maxIter);
+    if (c->pressureKind == 1)   // in place on pA; the ghosts keep their last fill, as the reference's array
+        CUDA_TRY(c, cudaMemcpyAsync(dP, c->F.pA, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    else
+        k_jacobi_finish<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(
+            c->P, c->F.pA, c->F.pB, dP, c->ctl, maxIter);
     LAUNCH_CHECK(c);
     if (!onDevice) CUDA_TRY(c, cudaMemcpyAsync(pressure, dP, bytes, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -1002,6 +1089,14 @@ int sifv_advective_dt(sifv_ctx_t* c, double cfl, double maxDt, double* dt) {
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     unsigned long long b = c->ctlHost->dtBits;
     std::memcpy(dt, &b, sizeof(double));
+    return SIFV_OK;
+}
+
+int sifv_set_pressure_solver(sifv_ctx_t* c, int kind) {
+    if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
+    if (kind != SIFV_PRESSURE_JACOBI && kind != SIFV_PRESSURE_GAUSS_SEIDEL)
+        return fail(c, SIFV_ERR_BAD_ARG, "unknown pressure solver");
+    c->pressureKind = kind;
     return SIFV_OK;
 }
 

@@ -1017,6 +1017,117 @@ __global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, int pl
     }
 }
 
+// ---------------------------------------------------------------------------
+// Gauss-Seidel pressure solve (GaussSeidelPressureSolver::solve,
+// src/GaussSeidelPressureSolver.cpp:10-49): per iteration the scalar ghosts of
+// p are filled from the current iterate, then one lexicographic in-place sweep
+// p <- (rhs + rho c^2 dt^2 offDiag) / (1 + rho c^2 dt^2 diagL) with the
+// PressureLaplacian coefficients (src/PressureLaplacian.cpp:6-60, evaluated
+// once per solve by k_jacobi_coef), max |p_new - p_old| as the residual.  The
+// sweep runs as the same tiled wavefront as the IGR sweep (bit-identical to
+// the lexicographic order).  Every kernel of iteration `it` is a no-op once
+// iteration it-1 converged (device-side check, as k_jacobi).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool gs_converged(Ctl* ctl, int it, double tol) {
+    if (ctl->jacobiDone) return true;
+    if (it > 0 && bits2d(ctl->res[it - 1]) < tol) {
+        if (threadIdx.x == 0) ctl->jacobiDone = it;
+        return true;
+    }
+    return false;
+}
+
+__global__ void k_gs_ghosts(Params P, double* __restrict__ f, Ctl* ctl, int it, double tol) {
+    if (gs_converged(ctl, it, tol)) return;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!ext_coords(P, t, i, j, k)) return;
+    if (is_interior(P, i, j, k)) return;
+    f[cidx(P, i, j, k)] = f[scalar_idx(P, i, j, k)];
+}
+
+// one cell: coefficients in k_jacobi_coef's layout (x-, x+, y-, y+, z-, z+,
+// coeff, denom) at cf[q * nc]; neighbours pm / pp per axis
+__device__ __forceinline__ double gs_cell(int dim, const double* cf, size_t nc, double rhsC, const double* pn) {
+    double od = 0.0;
+    od += cf[0] * pn[0] + cf[nc] * pn[1];
+    if (dim >= 2) od += cf[2 * nc] * pn[2] + cf[3 * nc] * pn[3];
+    if (dim >= 3) od += cf[4 * nc] * pn[4] + cf[5 * nc] * pn[5];
+    const double coeff = cf[(size_t)(2 * dim) * nc], denom = cf[(size_t)(2 * dim + 1) * nc];
+    return (rhsC + coeff * od) / denom;
+}
+
+__global__ void k_gs_sweep_1d(Params P, const double* __restrict__ coef, size_t nc, const double* __restrict__ rhs,
+                              double* __restrict__ p, Ctl* ctl, int it, double tol) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (gs_converged(ctl, it, tol)) return;
+    double maxRes = 0.0;
+    for (int i = 0; i < P.nx; ++i) {
+        const size_t c = cidx(P, i, 0, 0);
+        const double nb[2] = {p[c - 1], p[c + 1]};
+        const double pOld = p[c];
+        const double pn = gs_cell(1, coef + c, nc, rhs[c], nb);
+        p[c] = pn;
+        maxRes = smax(maxRes, fabs(pn - pOld));
+    }
+    atomicMax(&ctl->res[it], d2bits(maxRes));
+}
+
+template <int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TY * TZ) k_gs_tile(Params P, const double* __restrict__ coef, size_t nc,
+                                                     const double* __restrict__ rhs, double* __restrict__ p, Ctl* ctl,
+                                                     int it, double tol, int plane, int ntx, int nty) {
+    extern __shared__ double smem[];
+    constexpr int D3 = (TZ > 1) ? 1 : 0;
+    constexpr int HX = TX + 2, HY = TY + 2;
+    if (gs_converged(ctl, it, tol)) return;
+    const int J = (int)(blockIdx.x % (unsigned)nty), K = (int)(blockIdx.x / (unsigned)nty);
+    const int I = plane - J - K;
+    if (I < 0 || I >= ntx) return;
+    const int i0 = I * TX, j0 = J * TY, k0 = K * TZ;
+    const int ex = min(TX, P.nx - i0), ey = min(TY, P.ny - j0), ez = D3 ? min(TZ, P.nz - k0) : 1;
+    const int hx = ex + 2, hy = ey + 2, hz = D3 ? ez + 2 : 1;
+    const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5, nwarp = (int)blockDim.x >> 5;
+    for (int line = warp; line < hy * hz; line += nwarp) {
+        const int b = line % hy, c = line / hy;
+        for (int a = lane; a < hx; a += 32)
+            cp_async8(&smem[(c * HY + b) * HX + a], &p[cidx(P, i0 + a - 1, j0 + b - 1, D3 ? k0 + c - 1 : k0)]);
+    }
+    cp_async_wait_all();
+    const int tb = (int)threadIdx.x % TY, tc = (int)threadIdx.x / TY;
+    const bool act = tb < ey && tc < ez;
+    const int hLine = ((tc + D3) * HY + (tb + 1)) * HX + 1;
+    const int dim = P.dim;
+    double maxRes = 0.0;
+    __syncthreads();
+    const int nq = ex + ey + ez - 2;
+    for (int q = 0; q < nq; ++q) {
+        const int a = q - tb - tc;
+        if (act && a >= 0 && a < ex) {
+            const int h = hLine + a;
+            const size_t c = cidx(P, i0 + a, j0 + tb, k0 + tc);
+            const double nb[6] = {smem[h - 1], smem[h + 1], smem[h - HX], smem[h + HX],
+                                  D3 ? smem[h - HX * HY] : 0.0, D3 ? smem[h + HX * HY] : 0.0};
+            const double pOld = smem[h];
+            const double pn = gs_cell(dim, coef + c, nc, rhs[c], nb);
+            smem[h] = pn;
+            maxRes = smax(maxRes, fabs(pn - pOld));
+        }
+        __syncthreads();
+    }
+    for (int line = warp; line < ey * ez; line += nwarp) {
+        const int b = line % ey, c = line / ey;
+        for (int a = lane; a < ex; a += 32)
+            p[cidx(P, i0 + a, j0 + b, k0 + c)] = smem[((c + D3) * HY + (b + 1)) * HX + (a + 1)];
+    }
+    block_max_to(maxRes, &ctl->res[it]);
+}
+
+template <int TX, int TY, int TZ>
+constexpr size_t gs_tile_smem() {
+    return sizeof(double) * (size_t)(TX + 2) * (TY + 2) * (TZ > 1 ? TZ + 2 : 1);
+}
+
 template <int TX, int TY, int TZ>
 constexpr size_t igr_tile_smem() {
     return sizeof(double) * (2 * (size_t)(TX + 2) * (TY + 2) * (TZ > 1 ? TZ + 2 : 1) + 2 * (size_t)TX * TY * TZ);
