@@ -19,6 +19,7 @@
 #include "IGR.hpp"
 #include "IdealGasEOS.hpp"
 #include "JacobiPressureSolver.hpp"
+#include "GaussSeidelPressureSolver.hpp"
 #include "MPIContext.hpp"
 #include "RectilinearMesh.hpp"
 #include "SemiImplicitSolver.hpp"
@@ -148,11 +149,11 @@ double sifv_adapter_selftest_explicit(int n, int nsteps, int precision, int bcCo
     }
 }
 
-// Semi-implicit + IGR: reference SemiImplicitSolver(Jacobi) vs
-// CudaSemiImplicitSolver on the periodic 3D pulse (n^3, RK1).  `plugin`
-// != 0 instead plugs CudaJacobiPressureSolver into the REFERENCE solver
-// (the PressureSolver plugin interface).  *itersOut: last pressure
-// iterations of the CUDA side.
+// Semi-implicit + IGR: reference SemiImplicitSolver vs CudaSemiImplicitSolver
+// on the periodic 3D pulse (n^3, RK1).  `plugin` bit 0 instead plugs the
+// CUDA PressureSolver into the REFERENCE solver (the PressureSolver plugin
+// interface); bit 1 selects Gauss-Seidel instead of Jacobi on both sides.
+// *itersOut: last pressure iterations of the CUDA side.
 double sifv_adapter_selftest_semi(int n, int nsteps, int plugin, int* itersOut) {
     try {
         SimulationConfig cfg;
@@ -172,19 +173,24 @@ double sifv_adapter_selftest_semi(int n, int nsteps, int plugin, int* itersOut) 
         sb.allocate(b.mesh->totalCells(), cfg);
         pulseIC(*a.mesh, sa, *eos);
         pulseIC(*b.mesh, sb, *eos);
-        SemiImplicitSolver ref(*a.mesh, riemann, std::make_shared<JacobiPressureSolver>(), eos, igr, cfg);
+        const bool gs = (plugin & 2) != 0;
+        plugin &= 1;
+        auto refSolver = [gs]() -> std::shared_ptr<PressureSolver> {
+            if (gs) return std::make_shared<GaussSeidelPressureSolver>();
+            return std::make_shared<JacobiPressureSolver>();
+        };
+        SemiImplicitSolver ref(*a.mesh, riemann, refSolver(), eos, igr, cfg);
         ref.setHaloExchange(a.halo.get());
         std::unique_ptr<SemiImplicitSolver> refPlug;
         std::unique_ptr<b200::CudaSemiImplicitSolver> gpu;
         if (plugin) {
-            refPlug = std::make_unique<SemiImplicitSolver>(*b.mesh, riemann,
-                                                           std::make_shared<b200::CudaJacobiPressureSolver>(), eos,
-                                                           igr, cfg);
+            std::shared_ptr<PressureSolver> cudaPS;
+            if (gs) cudaPS = std::make_shared<b200::CudaGaussSeidelPressureSolver>();
+            else cudaPS = std::make_shared<b200::CudaJacobiPressureSolver>();
+            refPlug = std::make_unique<SemiImplicitSolver>(*b.mesh, riemann, cudaPS, eos, igr, cfg);
             refPlug->setHaloExchange(b.halo.get());
         } else {
-            gpu = std::make_unique<b200::CudaSemiImplicitSolver>(*b.mesh, riemann,
-                                                                 std::make_shared<JacobiPressureSolver>(), eos, igr,
-                                                                 cfg);
+            gpu = std::make_unique<b200::CudaSemiImplicitSolver>(*b.mesh, riemann, refSolver(), eos, igr, cfg);
             gpu->setHaloExchange(b.halo.get());
         }
         SimulationConfig ca = cfg, cb = cfg;

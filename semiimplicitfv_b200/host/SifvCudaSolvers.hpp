@@ -8,7 +8,8 @@
 //
 //   ExplicitSolver      (include/ExplicitSolver.hpp:21-36)      -> CudaExplicitSolver
 //   SemiImplicitSolver  (include/SemiImplicitSolver.hpp:22-46)  -> CudaSemiImplicitSolver
-//   PressureSolver      (include/PressureSolver.hpp:13-41)      -> CudaJacobiPressureSolver
+//   PressureSolver      (include/PressureSolver.hpp:13-41)      -> CudaJacobiPressureSolver,
+//                                                                  CudaGaussSeidelPressureSolver
 //
 // Errors of the C ABI are rethrown as the reference's exception types
 // (std::invalid_argument for configuration errors, std::runtime_error
@@ -186,6 +187,7 @@ protected:
             sifv_config_t c = toSifvConfig(config, *eos_, *riemann_, precision_);
             MeshNodes nodes(mesh, halo_);
             throwStatus(sifv_create(&c, &nodes.m, device_, &ctx_), "sifv_create");
+            throwStatus(sifv_set_pressure_solver(ctx_, pressureKind_), ctx_, "sifv_set_pressure_solver");
             dim_ = config.dim;
             nPhases_ = config.multiPhaseParams.nPhases;
             uploadState(ctx_, state, dim_, nPhases_);
@@ -204,6 +206,7 @@ protected:
     HaloExchange* halo_ = nullptr;
     sifv_ctx_t* ctx_ = nullptr;
     int device_, precision_;
+    int pressureKind_ = SIFV_PRESSURE_JACOBI;
     SyncPolicy sync_;
     int dim_ = 0, nPhases_ = 0;
 };
@@ -226,7 +229,8 @@ public:
 };
 
 // Drop-in for SemiImplicitSolver (include/SemiImplicitSolver.hpp:22-46) with
-// the Jacobi pressure solve on the GPU.
+// the pressure solve on the GPU: Jacobi or Gauss-Seidel, whichever
+// PressureSolver the constructor receives (by its name()).
 class CudaSemiImplicitSolver : public CudaStepperBase {
 public:
     CudaSemiImplicitSolver(const RectilinearMesh& /*mesh*/, std::shared_ptr<RiemannSolver> riemannSolver,
@@ -236,8 +240,9 @@ public:
         : CudaStepperBase(std::move(riemannSolver), std::move(eos), config, device, SIFV_PREC_FP64, sync),
           pressure_(std::move(pressureSolver)) {
         if (!config.semiImplicit) throw std::invalid_argument("CudaSemiImplicitSolver needs semiImplicit == true");
-        if (pressure_ && pressure_->name() != "Jacobi")
-            throw std::invalid_argument("the CUDA semi-implicit step solves the pressure with Jacobi");
+        if (pressure_ && pressure_->name() == "GaussSeidel") pressureKind_ = SIFV_PRESSURE_GAUSS_SEIDEL;
+        else if (pressure_ && pressure_->name() != "Jacobi")
+            throw std::invalid_argument("the CUDA semi-implicit step solves the pressure with Jacobi or GaussSeidel");
     }
 
     double step(const SimulationConfig& config, const RectilinearMesh& mesh, SolutionState& state,
@@ -255,13 +260,16 @@ private:
     int lastIters_ = 0;
 };
 
-// Drop-in PressureSolver (include/PressureSolver.hpp:13-41): the Jacobi
-// iteration of src/JacobiPressureSolver.cpp on the GPU.  Host arrays in,
-// host arrays out; the device context is cached per mesh.
-class CudaJacobiPressureSolver : public PressureSolver {
+// Drop-in PressureSolver (include/PressureSolver.hpp:13-41) on the GPU: the
+// Jacobi iteration of src/JacobiPressureSolver.cpp or the Gauss-Seidel sweeps
+// of src/GaussSeidelPressureSolver.cpp.  Host arrays in, host arrays out; the
+// device context is cached per mesh.
+class CudaPressureSolverPlugin : public PressureSolver {
 public:
-    explicit CudaJacobiPressureSolver(int device = 0) : device_(device) {}
-    ~CudaJacobiPressureSolver() override { if (ctx_) sifv_destroy(ctx_); }
+    CudaPressureSolverPlugin(int kind, int device) : kind_(kind), device_(device) {}
+    ~CudaPressureSolverPlugin() override { if (ctx_) sifv_destroy(ctx_); }
+    CudaPressureSolverPlugin(const CudaPressureSolverPlugin&) = delete;
+    CudaPressureSolverPlugin& operator=(const CudaPressureSolverPlugin&) = delete;
 
     int solve(const RectilinearMesh& mesh, const std::vector<double>& rho, const std::vector<double>& rhoc2,
               const std::vector<double>& rhs, std::vector<double>& pressure, double dt, double tolerance,
@@ -275,7 +283,7 @@ public:
         return run(mesh, &halo, rho, rhoc2, rhs, pressure, dt, tolerance, maxIter);
     }
 
-    std::string name() const override { return "Jacobi"; }
+    std::string name() const override { return kind_ == SIFV_PRESSURE_GAUSS_SEIDEL ? "GaussSeidel" : "Jacobi"; }
 
 private:
     int run(const RectilinearMesh& mesh, const HaloExchange* halo, const std::vector<double>& rho,
@@ -294,6 +302,7 @@ private:
             c.maxPressureIters = maxIter;
             MeshNodes nodes(mesh, halo);
             throwStatus(sifv_create(&c, &nodes.m, device_, &ctx_), "sifv_create");
+            throwStatus(sifv_set_pressure_solver(ctx_, kind_), ctx_, "sifv_set_pressure_solver");
             for (int q = 0; q < 4; ++q) key_[q] = key[q];
         }
         int iters = 0;
@@ -303,9 +312,20 @@ private:
         return iters;
     }
 
-    int device_;
+    int kind_, device_;
     sifv_ctx_t* ctx_ = nullptr;
     int key_[4] = {-1, -1, -1, -1};
+};
+
+class CudaJacobiPressureSolver : public CudaPressureSolverPlugin {
+public:
+    explicit CudaJacobiPressureSolver(int device = 0) : CudaPressureSolverPlugin(SIFV_PRESSURE_JACOBI, device) {}
+};
+
+class CudaGaussSeidelPressureSolver : public CudaPressureSolverPlugin {
+public:
+    explicit CudaGaussSeidelPressureSolver(int device = 0)
+        : CudaPressureSolverPlugin(SIFV_PRESSURE_GAUSS_SEIDEL, device) {}
 };
 
 }  // namespace b200

@@ -54,3 +54,13 @@ def test_pressure_solver_plugin_in_reference_solver(lib):
     it = ctypes.c_int()
     assert lib.sifv_adapter_selftest_semi(12, 3, 1, ctypes.byref(it)) == 0.0
     assert it.value > 0
+
+
+@pytest.mark.parametrize("plugin", [2, 3])
+def test_gauss_seidel_adapters_bit_identical(lib, plugin):
+    """CudaSemiImplicitSolver given a GaussSeidelPressureSolver (2), and
+    CudaGaussSeidelPressureSolver plugged into the reference's own
+    SemiImplicitSolver (3), against the reference with Gauss-Seidel."""
+    it = ctypes.c_int()
+    assert lib.sifv_adapter_selftest_semi(12, 3, plugin, ctypes.byref(it)) == 0.0
+    assert it.value > 0
