@@ -57,6 +57,11 @@ KERNEL_BYTES_PER_CELL_2D = {"sweep_x": 96.0, "sweep_y": 165.33, "dt": 32.0, "fin
 NCU_DRAM_BYTES_PER_CELL = {(2, "sweep_y"): 164.8, (2, "sweep_x"): 84.5, (1, "sweep_y"): 164.7,
                            (1, "sweep_x"): 86.2, (0, "assemble"): 166.2, (2, "tile2d"): 55.3,
                            (1, "tile2d"): 55.3}
+# FP64 / FP32 pipe utilisation of the dominant kernel (ncu, 2048^2 case of the
+# same workload: sm__inst_executed_pipe_fp64 / _fma, percent of the pipe's
+# instruction peak while active) -- the co-bound of the HBM roofline.
+NCU_PIPE_FRAC = {(2, "tile2d"): {"fp64": 0.608, "fma_fp32": 0.042, "issue_active": 0.487},
+                 (1, "tile2d"): {"fp64": 0.067, "fma_fp32": 0.418, "issue_active": 0.746}}
 # Fields a 2D step reads and writes (host-authoritative drop-in round trip).
 E2E_FIELDS_2D = ("F_RHO", "F_RHOU", "F_RHOV", "F_RHOE", "F_VELU", "F_VELV", "F_PRES")
 # Batched ensemble of two-phase water-air tubes: count, cell range, end time.
@@ -597,7 +602,10 @@ def run_cuda(args):
                          "peak_source": peak_kind,
                          "step": {"achieved": step_achieved, "frac": step_achieved / peak,
                                   "bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
-                         "kernel_ms_per_step": {k: v[0] / 2 for k, v in fam.items()}},
+                         "kernel_ms_per_step": {k: v[0] / 2 for k, v in fam.items()},
+                         "compute_co_bound": dict(NCU_PIPE_FRAC.get((args.precision, dom), {}),
+                                                  source="ncu on the 2048^2 case of this workload "
+                                                         "(profiles/tile2d_stage_riemann2d_2048.md)")},
             "cpu_baseline": {"value": cpu, "unit": UNIT, "cores": 1, "kind": kind,
                              "sample": f"{cpu_n}x{cpu_n} instance, {cpu_steps} steps, 1 thread"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": main["e2e_bytes"],
