@@ -7,8 +7,10 @@ the state resident in HBM (sifv_advance); `e2e` times K steps the way the
 drop-in solver with host-authoritative state runs them: per step the state
 fields the step reads are copied from pinned host buffers (sifv_set_field),
 sifv_step runs and returns dt, and the fields it writes are copied back
-(sifv_get_field).  The `ensemble` object times the batched-ensemble
-workload (2048 two-phase water-air tubes, one launch).
+(sifv_get_field).  The same JSON line carries the other workloads as
+objects: `semi_implicit` (3D acoustic pulse 256^3 with IGR and the Jacobi
+pressure solve), `adjoint` (isentropic-vortex discrete adjoint 512^2) and
+`ensemble` (2048 two-phase water-air tubes in one launch).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 

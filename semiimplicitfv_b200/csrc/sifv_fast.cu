@@ -77,7 +77,7 @@ int tile_launch(const TileArgs& A, cudaStream_t s) {
                              (int)bytes) != cudaSuccess)
         return -1;
     dim3 g((A.P.nx + kTileX - 1) / kTileX, (A.P.ny + kTileY - 1) / kTileY, 1);
-    k_tile2d<kTileX, kTileY, T><<<g, 256, bytes, s>>>(A);
+    k_tile2d<kTileX, kTileY, T><<<g, TileThreads<T>::value, bytes, s>>>(A);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -33,8 +33,16 @@ struct TileSmem {
     T fy[4][TY + 1][TX];
 };
 
+// Threads per block: FP64 512 (2 blocks of 96 KB per SM: 32 warps), FP32
+// 256 (4 blocks of 48 KB per SM).
+template <typename T>
+struct TileThreads {
+    static constexpr int value = (sizeof(T) == 8) ? 512 : 256;
+    static constexpr int blocks = (sizeof(T) == 8) ? 2 : 4;
+};
+
 template <int TX, int TY, typename T>
-__global__ void __launch_bounds__(256) k_tile2d(TileArgs A) {
+__global__ void __launch_bounds__(TileThreads<T>::value, TileThreads<T>::blocks) k_tile2d(TileArgs A) {
     using S = TileSmem<TX, TY, T>;
     extern __shared__ __align__(16) unsigned char smemRaw[];
     S& sm = *reinterpret_cast<S*>(smemRaw);
