@@ -129,6 +129,13 @@ typedef struct sifv_config {
     double bfA[3], bfB[3], bfC[3], bfD[3];
     /* SIFV_PREC_* */
     int    precision;
+    /* ViscousParams (include/SimulationConfig.hpp:62-65): dynamic viscosity
+     * mu, or per-phase viscosities phaseMu[0 .. nPhaseMu-1] (nPhaseMu ==
+     * nPhases; 0 = the scalar mu).  Viscous when mu > 0 or nPhaseMu > 0
+     * (SimulationConfig::hasViscosity). */
+    double mu;
+    double phaseMu[SIFV_MAX_PHASES];
+    int    nPhaseMu;
 } sifv_config_t;
 
 /* Mesh: physical node coordinates per axis (n+1 entries; NULL for an

@@ -96,6 +96,8 @@ static SimulationConfig toConfig(const sifv_config_t* c) {
         s.bodyForceParams.c[d] = c->bfC[d];
         s.bodyForceParams.d[d] = c->bfD[d];
     }
+    s.viscousParams.mu = c->mu;
+    s.viscousParams.phaseMu.assign(c->phaseMu, c->phaseMu + c->nPhaseMu);
     return s;
 }
 

@@ -766,6 +766,9 @@ static void scatter_face(ctx_t* m, const Flux* F, int hasL, size_t iL, double co
     }
 }
 
+static int has_viscosity(const sifv_config_t* c);
+static void add_viscous_fluxes(ctx_t* m);
+
 static void compute_rhs(ctx_t* m) {
     const int nPh = m->c.nPhases;
     const int semi = m->c.semiImplicit;
@@ -857,6 +860,175 @@ static void compute_rhs(ctx_t* m) {
                     m->rhsRhoE[idx] += m->rho[idx] * work;
                 }
     }
+    /* viscous stress: src/ExplicitSolver.cpp:523-527, src/SemiImplicitSolver.cpp:509-513 */
+    if (has_viscosity(&m->c)) add_viscous_fluxes(m);
+}
+
+/* ---- viscous stress: addViscousFluxes, src/ViscousFlux.cpp:24-303 ---- */
+static int has_viscosity(const sifv_config_t* c) { return c->mu > 0.0 || c->nPhaseMu > 0; }
+
+/* computeFaceMu (src/ViscousFlux.cpp:8-21): mixture rule per cell, face average */
+static double face_mu(const ctx_t* m, size_t iL, size_t iR) {
+    if (m->c.nPhaseMu == 0) return m->c.mu;
+    double muL = 0.0, muR = 0.0;
+    for (int ph = 0; ph < m->c.nPhases; ++ph) {
+        muL += m->alpha[ph][iL] * m->c.phaseMu[ph];
+        muR += m->alpha[ph][iR] * m->c.phaseMu[ph];
+    }
+    return 0.5 * (muL + muR);
+}
+
+/* accumulate one face's stress into its two cells (L: +, R: -) */
+static void visc_scatter(ctx_t* m, int hasL, size_t iL, double cL, int hasR, size_t iR, double cR, double t0,
+                         double t1, double t2, double work) {
+    const int dim = m->dim;
+    if (hasL) {
+        m->rhsRhoU[iL] += cL * t0;
+        if (dim >= 2) m->rhsRhoV[iL] += cL * t1;
+        if (dim >= 3) m->rhsRhoW[iL] += cL * t2;
+        m->rhsRhoE[iL] += cL * work;
+    }
+    if (hasR) {
+        m->rhsRhoU[iR] -= cR * t0;
+        if (dim >= 2) m->rhsRhoV[iR] -= cR * t1;
+        if (dim >= 3) m->rhsRhoW[iR] -= cR * t2;
+        m->rhsRhoE[iR] -= cR * work;
+    }
+}
+
+static void add_viscous_fluxes(ctx_t* m) {
+    const int dim = m->dim;
+    const double* U = m->velU;
+    const double* V = m->velV;
+    const double* W = m->velW;
+    for (int k = 0; k < m->nz; ++k)
+        for (int j = 0; j < m->ny; ++j)
+            for (int i = 0; i <= m->nx; ++i) {
+                size_t iL = IDX(m, i - 1, j, k), iR = IDX(m, i, j, k);
+                double dxi = 0.5 * (DX(m, i - 1) + DX(m, i));
+                double dudx = (U[iR] - U[iL]) / dxi, dvdx = 0.0, dwdx = 0.0;
+                if (dim >= 2) dvdx = (V[iR] - V[iL]) / dxi;
+                if (dim >= 3) dwdx = (W[iR] - W[iL]) / dxi;
+                double dudy = 0.0, dvdy = 0.0;
+                if (dim >= 2) {
+                    double dyj = DY(m, j);
+                    size_t Ljm = IDX(m, i - 1, j - 1, k), Ljp = IDX(m, i - 1, j + 1, k);
+                    size_t Rjm = IDX(m, i, j - 1, k), Rjp = IDX(m, i, j + 1, k);
+                    double dudyL = (U[Ljp] - U[Ljm]) / (2.0 * dyj), dudyR = (U[Rjp] - U[Rjm]) / (2.0 * dyj);
+                    dudy = 0.5 * (dudyL + dudyR);
+                    double dvdyL = (V[Ljp] - V[Ljm]) / (2.0 * dyj), dvdyR = (V[Rjp] - V[Rjm]) / (2.0 * dyj);
+                    dvdy = 0.5 * (dvdyL + dvdyR);
+                }
+                double dudz = 0.0, dwdz = 0.0;
+                if (dim >= 3) {
+                    double dzk = DZ(m, k);
+                    size_t Lkm = IDX(m, i - 1, j, k - 1), Lkp = IDX(m, i - 1, j, k + 1);
+                    size_t Rkm = IDX(m, i, j, k - 1), Rkp = IDX(m, i, j, k + 1);
+                    double dudzL = (U[Lkp] - U[Lkm]) / (2.0 * dzk), dudzR = (U[Rkp] - U[Rkm]) / (2.0 * dzk);
+                    dudz = 0.5 * (dudzL + dudzR);
+                    double dwdzL = (W[Lkp] - W[Lkm]) / (2.0 * dzk), dwdzR = (W[Rkp] - W[Rkm]) / (2.0 * dzk);
+                    dwdz = 0.5 * (dwdzL + dwdzR);
+                }
+                double divU = dudx + dvdy + dwdz;
+                double muF = face_mu(m, iL, iR);
+                double txx = muF * (2.0 * dudx - (2.0 / 3.0) * divU);
+                double txy = muF * (dvdx + dudy);
+                double txz = muF * (dwdx + dudz);
+                double uF = 0.5 * (U[iL] + U[iR]), vF = 0.0, wF = 0.0;
+                if (dim >= 2) vF = 0.5 * (V[iL] + V[iR]);
+                if (dim >= 3) wF = 0.5 * (W[iL] + W[iR]);
+                double work = txx * uF + txy * vF + txz * wF;
+                double area = DY(m, j) * DZ(m, k);
+                visc_scatter(m, i >= 1, iL, (i >= 1) ? area / VOL(m, i - 1, j, k) : 0.0, i < m->nx, iR,
+                             (i < m->nx) ? area / VOL(m, i, j, k) : 0.0, txx, txy, txz, work);
+            }
+    if (dim >= 2)
+        for (int k = 0; k < m->nz; ++k)
+            for (int j = 0; j <= m->ny; ++j)
+                for (int i = 0; i < m->nx; ++i) {
+                    size_t iL = IDX(m, i, j - 1, k), iR = IDX(m, i, j, k);
+                    double dyj = 0.5 * (DY(m, j - 1) + DY(m, j));
+                    double dudy = (U[iR] - U[iL]) / dyj, dvdy = (V[iR] - V[iL]) / dyj, dwdy = 0.0;
+                    if (dim >= 3) dwdy = (W[iR] - W[iL]) / dyj;
+                    double dxi = DX(m, i);
+                    size_t Lim = IDX(m, i - 1, j - 1, k), Lip = IDX(m, i + 1, j - 1, k);
+                    size_t Rim = IDX(m, i - 1, j, k), Rip = IDX(m, i + 1, j, k);
+                    double dudxL = (U[Lip] - U[Lim]) / (2.0 * dxi), dudxR = (U[Rip] - U[Rim]) / (2.0 * dxi);
+                    double dudx = 0.5 * (dudxL + dudxR);
+                    double dvdxL = (V[Lip] - V[Lim]) / (2.0 * dxi), dvdxR = (V[Rip] - V[Rim]) / (2.0 * dxi);
+                    double dvdx = 0.5 * (dvdxL + dvdxR);
+                    double dvdz = 0.0, dwdz = 0.0;
+                    if (dim >= 3) {
+                        double dzk = DZ(m, k);
+                        size_t Lkm = IDX(m, i, j - 1, k - 1), Lkp = IDX(m, i, j - 1, k + 1);
+                        size_t Rkm = IDX(m, i, j, k - 1), Rkp = IDX(m, i, j, k + 1);
+                        double dvdzL = (V[Lkp] - V[Lkm]) / (2.0 * dzk), dvdzR = (V[Rkp] - V[Rkm]) / (2.0 * dzk);
+                        dvdz = 0.5 * (dvdzL + dvdzR);
+                        double dwdzL = (W[Lkp] - W[Lkm]) / (2.0 * dzk), dwdzR = (W[Rkp] - W[Rkm]) / (2.0 * dzk);
+                        dwdz = 0.5 * (dwdzL + dwdzR);
+                    }
+                    double divU = dudx + dvdy + dwdz;
+                    double muF = face_mu(m, iL, iR);
+                    double tyx = muF * (dudy + dvdx);
+                    double tyy = muF * (2.0 * dvdy - (2.0 / 3.0) * divU);
+                    double tyz = muF * (dwdy + dvdz);
+                    double uF = 0.5 * (U[iL] + U[iR]), vF = 0.5 * (V[iL] + V[iR]), wF = 0.0;
+                    if (dim >= 3) wF = 0.5 * (W[iL] + W[iR]);
+                    double work = tyx * uF + tyy * vF + tyz * wF;
+                    double area = DX(m, i) * DZ(m, k);
+                    visc_scatter(m, j >= 1, iL, (j >= 1) ? area / VOL(m, i, j - 1, k) : 0.0, j < m->ny, iR,
+                                 (j < m->ny) ? area / VOL(m, i, j, k) : 0.0, tyx, tyy, tyz, work);
+                }
+    if (dim >= 3)
+        for (int k = 0; k <= m->nz; ++k)
+            for (int j = 0; j < m->ny; ++j)
+                for (int i = 0; i < m->nx; ++i) {
+                    size_t iL = IDX(m, i, j, k - 1), iR = IDX(m, i, j, k);
+                    double dzk = 0.5 * (DZ(m, k - 1) + DZ(m, k));
+                    double dudz = (U[iR] - U[iL]) / dzk, dvdz = (V[iR] - V[iL]) / dzk, dwdz = (W[iR] - W[iL]) / dzk;
+                    double dxi = DX(m, i);
+                    size_t Lim = IDX(m, i - 1, j, k - 1), Lip = IDX(m, i + 1, j, k - 1);
+                    size_t Rim = IDX(m, i - 1, j, k), Rip = IDX(m, i + 1, j, k);
+                    double dudxL = (U[Lip] - U[Lim]) / (2.0 * dxi), dudxR = (U[Rip] - U[Rim]) / (2.0 * dxi);
+                    double dudx = 0.5 * (dudxL + dudxR);
+                    double dwdxL = (W[Lip] - W[Lim]) / (2.0 * dxi), dwdxR = (W[Rip] - W[Rim]) / (2.0 * dxi);
+                    double dwdx = 0.5 * (dwdxL + dwdxR);
+                    double dyj = DY(m, j);
+                    size_t Ljm = IDX(m, i, j - 1, k - 1), Ljp = IDX(m, i, j + 1, k - 1);
+                    size_t Rjm = IDX(m, i, j - 1, k), Rjp = IDX(m, i, j + 1, k);
+                    double dvdyL = (V[Ljp] - V[Ljm]) / (2.0 * dyj), dvdyR = (V[Rjp] - V[Rjm]) / (2.0 * dyj);
+                    double dvdy = 0.5 * (dvdyL + dvdyR);
+                    double dwdyL = (W[Ljp] - W[Ljm]) / (2.0 * dyj), dwdyR = (W[Rjp] - W[Rjm]) / (2.0 * dyj);
+                    double dwdy = 0.5 * (dwdyL + dwdyR);
+                    double divU = dudx + dvdy + dwdz;
+                    double muF = face_mu(m, iL, iR);
+                    double tzx = muF * (dudz + dwdx);
+                    double tzy = muF * (dvdz + dwdy);
+                    double tzz = muF * (2.0 * dwdz - (2.0 / 3.0) * divU);
+                    double uF = 0.5 * (U[iL] + U[iR]), vF = 0.5 * (V[iL] + V[iR]), wF = 0.5 * (W[iL] + W[iR]);
+                    double work = tzx * uF + tzy * vF + tzz * wF;
+                    double area = DX(m, i) * DY(m, j);
+                    visc_scatter(m, k >= 1, iL, (k >= 1) ? area / VOL(m, i, j, k - 1) : 0.0, k < m->nz, iR,
+                                 (k < m->nz) ? area / VOL(m, i, j, k) : 0.0, tzx, tzy, tzz, work);
+                }
+}
+
+/* computeViscousDt, src/RKTimeStepping.cpp:161-188 */
+static double viscous_dt(const ctx_t* m, double mu, double cfl, double maxDt) {
+    double dt = maxDt;
+    const int dim = m->dim;
+    for (int k = 0; k < m->nz; ++k)
+        for (int j = 0; j < m->ny; ++j)
+            for (int i = 0; i < m->nx; ++i) {
+                size_t idx = IDX(m, i, j, k);
+                double dxMin = DX(m, i);
+                if (dim >= 2) dxMin = smin(dxMin, DY(m, j));
+                if (dim >= 3) dxMin = smin(dxMin, DZ(m, k));
+                double nu = mu / smax(m->rho[idx], 1e-14);
+                double dtCell = dxMin * dxMin / (2.0 * dim * nu);
+                dt = smin(dt, cfl * dtCell);
+            }
+    return dt;
 }
 
 /* ---- IGR ---- */
@@ -1104,7 +1276,13 @@ static void mp_post(ctx_t* m, size_t idx) {
 /* ExplicitSolver::step, src/ExplicitSolver.cpp:68-203 */
 static double explicit_step(ctx_t* m, int step, double targetDt) {
     const sifv_config_t* c = &m->c;
-    double dt = (c->constDt > 0) ? c->constDt : acoustic_dt(m, c->cfl, c->maxDt);
+    double dt;
+    if (c->constDt > 0) {
+        dt = c->constDt;
+    } else {
+        dt = acoustic_dt(m, c->cfl, c->maxDt);
+        if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->cfl, c->maxDt));
+    }
     if (targetDt > 0) dt = smin(dt, targetDt);
     double rk[3][4];
     rk_coefs(c->RKOrder, rk);
@@ -1280,6 +1458,7 @@ static void correction_step(ctx_t* m, double dt) {
 static double semi_step(ctx_t* m, int step, double targetDt) {
     const sifv_config_t* c = &m->c;
     double dt = advective_dt(m, c->siCfl, c->siMaxDt);
+    if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->siCfl, c->siMaxDt));
     if (targetDt > 0) dt = smin(dt, targetDt);
     dt = sclamp(dt, c->siMinDt, c->siMaxDt);
     double rk[3][4];
@@ -1379,6 +1558,13 @@ static int validate(const sifv_config_t* c, char* err) {
         if (c->phasePInf[p] < 0.0) FAIL("multiPhaseParams.phases[].pInf must be >= 0");
     }
     if (c->nPhases > 0 && c->alphaMin <= 0.0) FAIL("multiPhaseParams.alphaMin must be > 0");
+    if (c->mu < 0.0) FAIL("viscousParams.mu must be >= 0");
+    if (c->nPhaseMu > 0) {
+        if (c->nPhases <= 0) FAIL("viscousParams.phaseMu requires multi-phase (nPhases >= 2)");
+        if (c->nPhaseMu != c->nPhases) FAIL("viscousParams.phaseMu.size() must equal nPhases");
+        for (int p = 0; p < c->nPhaseMu; ++p)
+            if (c->phaseMu[p] < 0.0) FAIL("viscousParams.phaseMu[] must be >= 0");
+    }
     return SIFV_OK;
 #undef FAIL
 }

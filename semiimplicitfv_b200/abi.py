@@ -59,6 +59,7 @@ class Config(C.Structure):
         ("alphaMin", C.c_double),
         ("bfA", C.c_double * 3), ("bfB", C.c_double * 3), ("bfC", C.c_double * 3), ("bfD", C.c_double * 3),
         ("precision", C.c_int),
+        ("mu", C.c_double), ("phaseMu", C.c_double * MAX_PHASES), ("nPhaseMu", C.c_int),
     ]
 
 
@@ -84,6 +85,7 @@ def config_defaults(**overrides) -> Config:
     c.alphaCoeff, c.IGRIters, c.IGRWarmStartIters = 1.0, 5, 50
     c.nPhases, c.alphaMin = 0, 1e-8
     c.precision = PREC_FP64
+    c.mu, c.nPhaseMu = 0.0, 0
     for k, v in overrides.items():
         if k in ("phaseGamma", "phasePInf"):
             arr = getattr(c, k)

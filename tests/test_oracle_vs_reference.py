@@ -4,6 +4,8 @@ sources compiled in place (oracle/_ref/libsifv_ref.so, -ffp-contract=off).
 Every field (ghosts included) must be bit-identical after several steps,
 over reconstruction orders, Riemann solvers, boundary conditions, EOS
 kinds, multi-phase, IGR, and the semi-implicit Jacobi path."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -121,3 +123,34 @@ def test_standalone_pressure_solve_and_dt():
     assert np.array_equal(co.interior(po), cr.interior(pr))
     assert co.acoustic_dt(0.6, 1.0) == cr.acoustic_dt(0.6, 1.0)
     assert co.advective_dt(0.8, 1.0) == cr.advective_dt(0.8, 1.0)
+
+
+def _viscous_cases():
+    c2 = cases.riemann2d(32, bc=abi.BC_NOSLIPWALL)
+    c2[0].mu = 0.01
+    wa = cases.water_air(64, p_left=2e5)
+    wa[0].nPhaseMu = 2
+    wa[0].phaseMu[0], wa[0].phaseMu[1] = 1.0e-3, 1.8e-5
+    a3 = cases.acoustic3d(10, igr=False)
+    a3[0].mu = 0.05
+    v2 = cases.vortex2d(32)
+    v2[0].mu = 0.02
+    return {"riemann2d_noslip": (c2, 6), "water_air_phase_mu": (wa, 6), "acoustic3d_semi": (a3, 3),
+            "vortex_periodic": (v2, 4)}
+
+
+@pytest.mark.parametrize("name", ["riemann2d_noslip", "water_air_phase_mu", "acoustic3d_semi", "vortex_periodic"])
+def test_viscous_stress(name):
+    """addViscousFluxes (src/ViscousFlux.cpp) and computeViscousDt
+    (src/RKTimeStepping.cpp:161-188) in the explicit and semi-implicit steps."""
+    case, n = _viscous_cases()[name]
+    _compare(case, n)
+
+
+def test_viscous_config_validation():
+    lib = backends.oracle()
+    bad = abi.config_defaults(dim=1, nGhost=3, reconOrder=abi.WENO5)
+    bad.mu = -1.0
+    assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.ERR_BAD_CONFIG
+    bad.mu, bad.nPhaseMu = 0.0, 2
+    assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.ERR_BAD_CONFIG
