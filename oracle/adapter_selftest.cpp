@@ -102,18 +102,12 @@ void pulseIC(const RectilinearMesh& mesh, SolutionState& st, const IdealGasEOS& 
             }
 }
 
-}  // namespace
-
-extern "C" {
-
-// Explicit: reference ExplicitSolver vs CudaExplicitSolver on the 2D Riemann
-// problem, n x n, nsteps steps.  Returns the worst relative L-inf over
-// rho, rhoU, rhoV, rhoE (negative on an exception).
-double sifv_adapter_selftest_explicit(int n, int nsteps, int precision, int bcCode) {
+double explicitCase(int n, int nsteps, int precision, int bcCode, double mu) {
     try {
         SimulationConfig cfg;
         cfg.dim = 2; cfg.nGhost = 3; cfg.RKOrder = 3; cfg.reconOrder = ReconstructionOrder::WENO5;
         cfg.explicitParams.cfl = 0.6;
+        cfg.viscousParams.mu = mu;
         cfg.validate();
         BoundaryCondition bc = static_cast<BoundaryCondition>(bcCode);
         std::array<int, 3> periods = {0, 0, 0};
@@ -147,6 +141,22 @@ double sifv_adapter_selftest_explicit(int n, int nsteps, int precision, int bcCo
     } catch (...) {
         return -1.0;
     }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Explicit: reference ExplicitSolver vs CudaExplicitSolver on the 2D Riemann
+// problem, n x n, nsteps steps.  Returns the worst relative L-inf over
+// rho, rhoU, rhoV, rhoE (negative on an exception).
+double sifv_adapter_selftest_explicit(int n, int nsteps, int precision, int bcCode) {
+    return explicitCase(n, nsteps, precision, bcCode, 0.0);
+}
+
+// The same with viscousParams.mu = mu (viscous stress + viscous dt limit).
+double sifv_adapter_selftest_explicit_viscous(int n, int nsteps, int bcCode, double mu) {
+    return explicitCase(n, nsteps, SIFV_PREC_FP64, bcCode, mu);
 }
 
 // Semi-implicit + IGR: reference SemiImplicitSolver vs CudaSemiImplicitSolver

@@ -166,6 +166,14 @@ int validate(const sifv_config_t* c, std::string& msg) {
     }
     if (c->nPhases > 0 && c->alphaMin <= 0.0) return bad("multiPhaseParams.alphaMin must be > 0");
     if (c->riemannSolver < SIFV_LF || c->riemannSolver > SIFV_HLLC) return bad("unknown riemannSolver");
+    if (c->mu < 0.0) return bad("viscousParams.mu must be >= 0");
+    if (c->nPhaseMu < 0 || c->nPhaseMu > SIFV_MAX_PHASES) return bad("viscousParams.phaseMu has too many entries");
+    if (c->nPhaseMu > 0) {
+        if (c->nPhases <= 0) return bad("viscousParams.phaseMu requires multi-phase (nPhases >= 2)");
+        if (c->nPhaseMu != c->nPhases) return bad("viscousParams.phaseMu.size() must equal nPhases");
+        for (int p = 0; p < c->nPhaseMu; ++p)
+            if (c->phaseMu[p] < 0.0) return bad("viscousParams.phaseMu[] must be >= 0");
+    }
     if (c->precision != SIFV_PREC_FP64 && c->precision != SIFV_PREC_MIXED && c->precision != SIFV_PREC_FP64_FAST)
         return bad("unknown precision");
     return SIFV_OK;
@@ -479,6 +487,10 @@ void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
     if (cfg.semiImplicit) {
         k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, cfg.siMaxDt);
         k_dt_advective<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.siCfl);
+        if (c->P.visc) {
+            k_dt_viscous<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.siCfl);
+            c->launches++;
+        }
         k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, -1.0, targetDt, 1, cfg.siMinDt, cfg.siMaxDt, useEnd ? 1 : 0);
         c->launches += 3;
     } else if (c->forcedDt > 0) {
@@ -488,6 +500,10 @@ void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
         if (cfg.constDt <= 0) {
             k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, cfg.maxDt);
             NPH_DISPATCH(c, (k_dt_acoustic<NPHV><<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.cfl)));
+            if (c->P.visc) {
+                k_dt_viscous<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.cfl);
+                c->launches++;
+            }
             c->launches += 2;
         }
         k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, cfg.constDt, targetDt, 0, 0.0, 0.0, useEnd ? 1 : 0);
@@ -601,6 +617,17 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
             if (st != SIFV_OK) return st;
         }
         for (int d = 0; d < P.dim; ++d) launch_face(c, d);
+        if (P.visc) {
+            for (int d = 0; d < P.dim; ++d) {
+                long long nf = (long long)(P.nx + (d == 0)) * (P.ny + (d == 1)) * (P.nz + (d == 2));
+                unsigned gf = blocks(nf, kCellThreads);
+                if (d == 0) k_visc_face<0><<<gf, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl);
+                else if (d == 1) k_visc_face<1><<<gf, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl);
+                else k_visc_face<2><<<gf, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl);
+                c->launches++;
+            }
+            mark(c, "viscous");
+        }
         if (!cfg.semiImplicit) {
             if (c->stageHook && c->stageHook(s, 1) != 0) return SIFV_ERR_CUDA;
             NPH_DISPATCH(c, (k_assemble<NPHV, 0><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, K)));
@@ -678,10 +705,11 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     if (cfg->precision != SIFV_PREC_FP64) {
         bool bf = false;
         for (int d = 0; d < 3; ++d) bf = bf || cfg->bfA[d] != 0.0 || cfg->bfB[d] != 0.0;
-        if (cfg->semiImplicit || cfg->nPhases > 0 || cfg->useIGR || cfg->reconOrder != SIFV_WENO5 || bf)
+        const bool visc = cfg->mu > 0.0 || cfg->nPhaseMu > 0;
+        if (cfg->semiImplicit || cfg->nPhases > 0 || cfg->useIGR || cfg->reconOrder != SIFV_WENO5 || bf || visc)
             return fail(nullptr, SIFV_ERR_UNSUPPORTED,
                         "SIFV_PREC_MIXED / SIFV_PREC_FP64_FAST run the explicit single-phase WENO5 step without "
-                        "IGR or body force; use SIFV_PREC_FP64 for this configuration");
+                        "IGR, body force or viscosity; use SIFV_PREC_FP64 for this configuration");
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -734,6 +762,10 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
         P.phasePInf[p] = cfg->phasePInf[p];
     }
     P.alphaMin = cfg->alphaMin;
+    P.visc = (cfg->mu > 0.0 || cfg->nPhaseMu > 0) ? 1 : 0;
+    P.perPhaseMu = cfg->nPhaseMu > 0 ? 1 : 0;
+    P.mu = cfg->mu;
+    for (int p = 0; p < SIFV_MAX_PHASES; ++p) P.phaseMu[p] = (p < cfg->nPhaseMu) ? cfg->phaseMu[p] : 0.0;
     c->nphT = (cfg->nPhases == 0) ? 0 : (cfg->nPhases <= 2) ? 2 : 8;
     c->W = (cfg->reconOrder == SIFV_WENO1 || cfg->reconOrder == SIFV_UPWIND1) ? 1
          : (cfg->reconOrder == SIFV_WENO3 || cfg->reconOrder == SIFV_UPWIND3) ? 3 : 5;
@@ -776,6 +808,8 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
             F.flux[d][FS_ALPHA + p] = dalloc(c, nf, st);
             F.flux[d][FS_AR + p] = dalloc(c, nf, st);
         }
+        if (P.visc)
+            for (int q = 0; q < 4; ++q) F.flux[d][FS_VISC + q] = (q == 0 || q == 3 || q < dim) ? dalloc(c, nf, st) : nullptr;
     }
     // geometry: per-cell widths incl. ghosts, and IGR alpha/d^2
     static const double unit[2] = {0.0, 1.0};
@@ -1150,10 +1184,10 @@ int cons_slot(const sifv_ctx* c, int field) {
 int adjoint_supported(sifv_ctx* c) {
     const sifv_config_t& g = c->cfg;
     if (g.semiImplicit || g.useIGR || g.nPhases > 0 || has_body_force(g) || g.precision != SIFV_PREC_FP64 ||
-        (g.reconOrder != SIFV_WENO5 && g.reconOrder != SIFV_UPWIND5) || g.nGhost > 7)
+        (g.reconOrder != SIFV_WENO5 && g.reconOrder != SIFV_UPWIND5) || g.nGhost > 7 || c->P.visc)
         return fail(c, SIFV_ERR_UNSUPPORTED,
                     "the adjoint / tangent covers the explicit single-phase WENO5 / UPWIND5 step in SIFV_PREC_FP64 "
-                    "without IGR or body force (nGhost <= 7)");
+                    "without IGR, body force or viscosity (nGhost <= 7)");
     return SIFV_OK;
 }
 

@@ -37,7 +37,8 @@ enum FluxSlot : int {
     FS_FVEL = 6,    // faceVelocity (semi-implicit, multi-phase)
     FS_ALPHA = 7,   // alphaFlux[ph]         7 .. 7+MAXPH-1
     FS_AR = 7 + MAXPH,  // upwinded alphaRho flux[ph]
-    FS_COUNT = 7 + 2 * MAXPH
+    FS_VISC = 7 + 2 * MAXPH,   // viscous stress on the face: tau.x, tau.y, tau.z, work (4 slots)
+    FS_COUNT = 11 + 2 * MAXPH
 };
 
 struct Params {
@@ -58,6 +59,10 @@ struct Params {
     double gamma, pInf;
     double phaseGamma[MAXPH], phasePInf[MAXPH];
     double alphaMin;
+    int visc;                // viscous stress on (SimulationConfig::hasViscosity)
+    int perPhaseMu;          // per-phase viscosities (else the scalar mu)
+    double mu;
+    double phaseMu[MAXPH];
 };
 
 struct Fields {

@@ -271,6 +271,22 @@ __global__ void __launch_bounds__(256) k_assemble(Params P, Fields F, const Ctl*
         rE += rho * work;
     }
 
+    if (P.visc) {   // addViscousFluxes (src/ViscousFlux.cpp:24-303): per direction low face (-), high face (+)
+        DIMLOOP(d) {
+            const double co = cf.coeff[d];
+            const long long lo = cf.lo[d], hi = cf.lo[d] + cf.hiOff[d];
+            double* const* fv = F.flux[d] + FS_VISC;
+            rU -= co * fv[0][lo];
+            if (dim >= 2) rV -= co * fv[1][lo];
+            if (dim >= 3) rW -= co * fv[2][lo];
+            rE -= co * fv[3][lo];
+            rU += co * fv[0][hi];
+            if (dim >= 2) rV += co * fv[1][hi];
+            if (dim >= 3) rW += co * fv[2][hi];
+            rE += co * fv[3][hi];
+        }
+    }
+
     const double dt = ctl->dt;
     const double c1 = K.c1, c2 = K.c2, c3 = K.c3, c4 = K.c4;
     const int RK = P.RKOrder;
@@ -411,6 +427,144 @@ __global__ void __launch_bounds__(256) k_dt_advective(Params P, Fields F, Ctl* c
         v = cfl * dtCell;
     }
     block_min_to(v, &ctl->dtBits);
+}
+
+// computeViscousDt (src/RKTimeStepping.cpp:161-188), folded into the same
+// minimum as the acoustic / advective step (std::min of the two).
+__global__ void __launch_bounds__(256) k_dt_viscous(Params P, Fields F, Ctl* ctl, double cfl) {
+    if (ctl->skip) return;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    double v = __longlong_as_double(0x7ff0000000000000LL);
+    if (int_coords(P, t, i, j, k)) {
+        const int dim = P.dim;
+        size_t c = cidx(P, i, j, k);
+        double dxMin = F.dx[i + P.ngx];
+        if (dim >= 2) dxMin = smin(dxMin, F.dy[j + P.ngy]);
+        if (dim >= 3) dxMin = smin(dxMin, F.dz[k + P.ngz]);
+        double nu = P.mu / smax(F.rho[c], 1e-14);
+        double dtCell = dxMin * dxMin / (2.0 * dim * nu);
+        v = cfl * dtCell;
+    }
+    block_min_to(v, &ctl->dtBits);
+}
+
+// Viscous stress on the faces of direction DIR (src/ViscousFlux.cpp:24-303):
+// central normal gradients, transverse gradients averaged over the two
+// cells, face viscosity (computeFaceMu, 8-21), face-averaged velocity for the
+// work term; stored per face as tau.x, tau.y, tau.z, work.
+template <int DIR>
+__global__ void __launch_bounds__(256) k_visc_face(Params P, Fields F, const Ctl* __restrict__ ctl) {
+    if (ctl && ctl->skip) return;
+    const int dim = P.dim;
+    const int fnx = P.nx + (DIR == 0), fny = P.ny + (DIR == 1), fnz = P.nz + (DIR == 2);
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long tot = (long long)fnx * fny * fnz;
+    if (t >= tot) return;
+    int i, j, k;
+    split3(t, fnx, fny, i, j, k);
+    const double* U = F.velU;
+    const double* V = F.velV;
+    const double* W = F.velW;
+    auto at = [&](int a, int b, int c) { return cidx(P, a, b, c); };
+    const int li = i - (DIR == 0), lj = j - (DIR == 1), lk = k - (DIR == 2);
+    const size_t iL = at(li, lj, lk), iR = at(i, j, k);
+    double muF;
+    if (!P.perPhaseMu) {
+        muF = P.mu;
+    } else {
+        double muL = 0.0, muR = 0.0;
+        for (int ph = 0; ph < P.nPh; ++ph) {
+            muL += F.alpha[ph][iL] * P.phaseMu[ph];
+            muR += F.alpha[ph][iR] * P.phaseMu[ph];
+        }
+        muF = 0.5 * (muL + muR);
+    }
+    double t0, t1, t2, work;
+    if (DIR == 0) {
+        double dxi = 0.5 * (F.dx[i - 1 + P.ngx] + F.dx[i + P.ngx]);
+        double dudx = (U[iR] - U[iL]) / dxi, dvdx = 0.0, dwdx = 0.0;
+        if (dim >= 2) dvdx = (V[iR] - V[iL]) / dxi;
+        if (dim >= 3) dwdx = (W[iR] - W[iL]) / dxi;
+        double dudy = 0.0, dvdy = 0.0;
+        if (dim >= 2) {
+            double dyj = F.dy[j + P.ngy];
+            size_t Ljm = at(i - 1, j - 1, k), Ljp = at(i - 1, j + 1, k), Rjm = at(i, j - 1, k), Rjp = at(i, j + 1, k);
+            double dudyL = (U[Ljp] - U[Ljm]) / (2.0 * dyj), dudyR = (U[Rjp] - U[Rjm]) / (2.0 * dyj);
+            dudy = 0.5 * (dudyL + dudyR);
+            double dvdyL = (V[Ljp] - V[Ljm]) / (2.0 * dyj), dvdyR = (V[Rjp] - V[Rjm]) / (2.0 * dyj);
+            dvdy = 0.5 * (dvdyL + dvdyR);
+        }
+        double dudz = 0.0, dwdz = 0.0;
+        if (dim >= 3) {
+            double dzk = F.dz[k + P.ngz];
+            size_t Lkm = at(i - 1, j, k - 1), Lkp = at(i - 1, j, k + 1), Rkm = at(i, j, k - 1), Rkp = at(i, j, k + 1);
+            double dudzL = (U[Lkp] - U[Lkm]) / (2.0 * dzk), dudzR = (U[Rkp] - U[Rkm]) / (2.0 * dzk);
+            dudz = 0.5 * (dudzL + dudzR);
+            double dwdzL = (W[Lkp] - W[Lkm]) / (2.0 * dzk), dwdzR = (W[Rkp] - W[Rkm]) / (2.0 * dzk);
+            dwdz = 0.5 * (dwdzL + dwdzR);
+        }
+        double divU = dudx + dvdy + dwdz;
+        t0 = muF * (2.0 * dudx - (2.0 / 3.0) * divU);
+        t1 = muF * (dvdx + dudy);
+        t2 = muF * (dwdx + dudz);
+        double uF = 0.5 * (U[iL] + U[iR]), vF = 0.0, wF = 0.0;
+        if (dim >= 2) vF = 0.5 * (V[iL] + V[iR]);
+        if (dim >= 3) wF = 0.5 * (W[iL] + W[iR]);
+        work = t0 * uF + t1 * vF + t2 * wF;
+    } else if (DIR == 1) {
+        double dyj = 0.5 * (F.dy[j - 1 + P.ngy] + F.dy[j + P.ngy]);
+        double dudy = (U[iR] - U[iL]) / dyj, dvdy = (V[iR] - V[iL]) / dyj, dwdy = 0.0;
+        if (dim >= 3) dwdy = (W[iR] - W[iL]) / dyj;
+        double dxi = F.dx[i + P.ngx];
+        size_t Lim = at(i - 1, j - 1, k), Lip = at(i + 1, j - 1, k), Rim = at(i - 1, j, k), Rip = at(i + 1, j, k);
+        double dudxL = (U[Lip] - U[Lim]) / (2.0 * dxi), dudxR = (U[Rip] - U[Rim]) / (2.0 * dxi);
+        double dudx = 0.5 * (dudxL + dudxR);
+        double dvdxL = (V[Lip] - V[Lim]) / (2.0 * dxi), dvdxR = (V[Rip] - V[Rim]) / (2.0 * dxi);
+        double dvdx = 0.5 * (dvdxL + dvdxR);
+        double dvdz = 0.0, dwdz = 0.0;
+        if (dim >= 3) {
+            double dzk = F.dz[k + P.ngz];
+            size_t Lkm = at(i, j - 1, k - 1), Lkp = at(i, j - 1, k + 1), Rkm = at(i, j, k - 1), Rkp = at(i, j, k + 1);
+            double dvdzL = (V[Lkp] - V[Lkm]) / (2.0 * dzk), dvdzR = (V[Rkp] - V[Rkm]) / (2.0 * dzk);
+            dvdz = 0.5 * (dvdzL + dvdzR);
+            double dwdzL = (W[Lkp] - W[Lkm]) / (2.0 * dzk), dwdzR = (W[Rkp] - W[Rkm]) / (2.0 * dzk);
+            dwdz = 0.5 * (dwdzL + dwdzR);
+        }
+        double divU = dudx + dvdy + dwdz;
+        t0 = muF * (dudy + dvdx);
+        t1 = muF * (2.0 * dvdy - (2.0 / 3.0) * divU);
+        t2 = muF * (dwdy + dvdz);
+        double uF = 0.5 * (U[iL] + U[iR]), vF = 0.5 * (V[iL] + V[iR]), wF = 0.0;
+        if (dim >= 3) wF = 0.5 * (W[iL] + W[iR]);
+        work = t0 * uF + t1 * vF + t2 * wF;
+    } else {
+        double dzk = 0.5 * (F.dz[k - 1 + P.ngz] + F.dz[k + P.ngz]);
+        double dudz = (U[iR] - U[iL]) / dzk, dvdz = (V[iR] - V[iL]) / dzk, dwdz = (W[iR] - W[iL]) / dzk;
+        double dxi = F.dx[i + P.ngx];
+        size_t Lim = at(i - 1, j, k - 1), Lip = at(i + 1, j, k - 1), Rim = at(i - 1, j, k), Rip = at(i + 1, j, k);
+        double dudxL = (U[Lip] - U[Lim]) / (2.0 * dxi), dudxR = (U[Rip] - U[Rim]) / (2.0 * dxi);
+        double dudx = 0.5 * (dudxL + dudxR);
+        double dwdxL = (W[Lip] - W[Lim]) / (2.0 * dxi), dwdxR = (W[Rip] - W[Rim]) / (2.0 * dxi);
+        double dwdx = 0.5 * (dwdxL + dwdxR);
+        double dyj = F.dy[j + P.ngy];
+        size_t Ljm = at(i, j - 1, k - 1), Ljp = at(i, j + 1, k - 1), Rjm = at(i, j - 1, k), Rjp = at(i, j + 1, k);
+        double dvdyL = (V[Ljp] - V[Ljm]) / (2.0 * dyj), dvdyR = (V[Rjp] - V[Rjm]) / (2.0 * dyj);
+        double dvdy = 0.5 * (dvdyL + dvdyR);
+        double dwdyL = (W[Ljp] - W[Ljm]) / (2.0 * dyj), dwdyR = (W[Rjp] - W[Rjm]) / (2.0 * dyj);
+        double dwdy = 0.5 * (dwdyL + dwdyR);
+        double divU = dudx + dvdy + dwdz;
+        t0 = muF * (dudz + dwdx);
+        t1 = muF * (dvdz + dwdy);
+        t2 = muF * (2.0 * dwdz - (2.0 / 3.0) * divU);
+        double uF = 0.5 * (U[iL] + U[iR]), vF = 0.5 * (V[iL] + V[iR]), wF = 0.5 * (W[iL] + W[iR]);
+        work = t0 * uF + t1 * vF + t2 * wF;
+    }
+    double* const* out = F.flux[DIR] + FS_VISC;
+    out[0][t] = t0;
+    if (dim >= 2) out[1][t] = t1;
+    if (dim >= 3) out[2][t] = t2;
+    out[3][t] = work;
 }
 
 // Reset the dt accumulator to maxDt (dt starts at maxDt in the reference).

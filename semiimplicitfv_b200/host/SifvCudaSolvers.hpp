@@ -102,8 +102,12 @@ inline sifv_config_t toSifvConfig(const SimulationConfig& c, const EquationOfSta
         s.bfD[d] = c.bodyForceParams.d[d];
     }
     s.precision = precision;
-    if (c.hasViscosity() || c.hasSurfaceTension())
-        throw std::invalid_argument("the CUDA step has no viscous or surface-tension terms");
+    s.mu = c.viscousParams.mu;
+    if (c.viscousParams.phaseMu.size() > (size_t)SIFV_MAX_PHASES)
+        throw std::invalid_argument("viscousParams.phaseMu has more than SIFV_MAX_PHASES entries");
+    s.nPhaseMu = (int)c.viscousParams.phaseMu.size();
+    for (int p = 0; p < s.nPhaseMu; ++p) s.phaseMu[p] = c.viscousParams.phaseMu[p];
+    if (c.hasSurfaceTension()) throw std::invalid_argument("the CUDA step has no surface-tension term");
     return s;
 }
 

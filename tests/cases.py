@@ -244,6 +244,34 @@ def advection1d(n=128, semi=False, riemann=abi.LF, cfl=0.8, rk=3):
     return cfg, abi.MeshSpec(x, bc=[BC_PERIODIC] * 6), fields
 
 
+VISCOUS_CASES = ["riemann2d_noslip", "water_air_phase_mu", "acoustic3d_semi", "vortex_periodic"]
+
+
+def viscous(name):
+    """Viscous variants (viscousParams, include/SimulationConfig.hpp:62-65):
+    scalar mu on the no-slip 2D Riemann box, per-phase mu on water-air,
+    scalar mu on the semi-implicit 3D pulse and on the periodic vortex.
+    Returns (case, steps)."""
+    if name == "riemann2d_noslip":
+        c = riemann2d(32, bc=abi.BC_NOSLIPWALL)
+        c[0].mu = 0.01
+        return c, 6
+    if name == "water_air_phase_mu":
+        c = water_air(64, p_left=2e5)
+        c[0].nPhaseMu = 2
+        c[0].phaseMu[0], c[0].phaseMu[1] = 1.0e-3, 1.8e-5
+        return c, 6
+    if name == "acoustic3d_semi":
+        c = acoustic3d(10, igr=False)
+        c[0].mu = 0.05
+        return c, 3
+    if name == "vortex_periodic":
+        c = vortex2d(32)
+        c[0].mu = 0.02
+        return c, 4
+    raise KeyError(name)
+
+
 def run_steps(ctx, nsteps, t_end=None, step0=0, time0=0.0):
     """Drive ctx.step like the reference drivers: targetDt = t_end - t when
     given.  Returns (time, steps, dts)."""

@@ -64,3 +64,11 @@ def test_gauss_seidel_adapters_bit_identical(lib, plugin):
     it = ctypes.c_int()
     assert lib.sifv_adapter_selftest_semi(12, 3, plugin, ctypes.byref(it)) == 0.0
     assert it.value > 0
+
+
+@pytest.mark.parametrize("bc", [abi.BC_NOSLIPWALL, abi.BC_PERIODIC])
+def test_explicit_adapter_viscous_bit_identical(lib, bc):
+    """viscousParams.mu carried through the adapter into the CUDA step."""
+    lib.sifv_adapter_selftest_explicit_viscous.restype = ctypes.c_double
+    lib.sifv_adapter_selftest_explicit_viscous.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+    assert lib.sifv_adapter_selftest_explicit_viscous(40, 8, bc, 0.01) == 0.0

@@ -151,6 +151,11 @@ def test_adjoint_rejects_unsupported():
     with pytest.raises(abi.AbiError) as e:
         ctx.adjoint_forward(0, 0.0, 1e-5, 0, 4)
     assert e.value.status == abi.ERR_UNSUPPORTED
+    cv, _ = cases.viscous("vortex_periodic")
+    ctxv = backends.make(backends.cuda(), cv)
+    with pytest.raises(abi.AbiError) as e:
+        ctxv.adjoint_forward(0, 0.0, 1e-3, 0, 4)
+    assert e.value.status == abi.ERR_UNSUPPORTED
     ctx2 = backends.make(backends.cuda(), cases.sod(32))
     with pytest.raises(abi.AbiError) as e:
         ctx2.adjoint_backward()

@@ -200,6 +200,10 @@ def test_ensemble_rejects_unsupported():
     with pytest.raises(abi.AbiError) as e:
         be.create_ensemble(cfgf, [32], [0.0], [1.0])
     assert e.value.status == abi.ERR_UNSUPPORTED
+    cfgv = abi.config_defaults(dim=1, nGhost=3, reconOrder=abi.WENO5, mu=1e-3)
+    with pytest.raises(abi.AbiError) as e:
+        be.create_ensemble(cfgv, [32], [0.0], [1.0])
+    assert e.value.status == abi.ERR_UNSUPPORTED
     cfg = abi.config_defaults(dim=1, nGhost=3, reconOrder=abi.WENO5)
     with pytest.raises(abi.AbiError) as e:
         be.create_ensemble(cfg, [2], [0.0], [1.0])

@@ -227,3 +227,47 @@ def test_gauss_seidel_standalone_solve():
     po, io, _ = co.pressure_solve(rho, rhoc2, rhs, p0, 1e-2, 1e-12, 60)
     assert ig == io
     assert np.array_equal(cg.interior(pg), co.interior(po))
+
+
+@pytest.mark.parametrize("name", cases.VISCOUS_CASES)
+def test_viscous_stress(name):
+    """addViscousFluxes (src/ViscousFlux.cpp:24-303) on every face and the
+    viscous step limit (computeViscousDt, src/RKTimeStepping.cpp:161-188),
+    explicit and semi-implicit, scalar and per-phase viscosity:
+    bit-identical to the oracle."""
+    case, n = cases.viscous(name)
+    check(case, n)
+
+
+def test_viscous_3d_explicit_walls():
+    """All three face directions with transverse gradients through the
+    corner ghosts (no-slip walls on every side), RK2, LF."""
+    case = cases.acoustic3d(9, semi=False, igr=False, rk=2, riemann=abi.LF)
+    case[0].mu = 0.03
+    case[1].bc = [abi.BC_NOSLIPWALL, abi.BC_SLIPWALL, abi.BC_NOSLIPWALL, abi.BC_OUTFLOW,
+                  abi.BC_SYMMETRY, abi.BC_NOSLIPWALL]
+    check(case, 4)
+
+
+def test_viscous_advance_matches_step():
+    case, _ = cases.viscous("riemann2d_noslip")
+    c1 = backends.make(backends.cuda(), case)
+    c2 = backends.make(backends.cuda(), case)
+    t1, s1, _ = cases.run_steps(c1, 5, t_end=0.05)
+    t2, s2 = c2.advance(0, 0.0, 0.05, 5)
+    assert s1 == s2 and t1 == t2
+    for fid in (abi.F_RHO, abi.F_RHOU, abi.F_RHOV, abi.F_RHOE):
+        assert np.array_equal(c1.get_field(fid), c2.get_field(fid))
+
+
+def test_viscous_rejected_outside_reference_precision():
+    case, _ = cases.viscous("vortex_periodic")
+    case[0].precision = abi.PREC_FP64_FAST
+    with pytest.raises(abi.AbiError) as e:
+        backends.cuda().create(case[0], case[1])
+    assert e.value.status == abi.ERR_UNSUPPORTED
+    case[0].precision = abi.PREC_FP64
+    case[0].mu = -1.0
+    with pytest.raises(abi.AbiError) as e:
+        backends.cuda().create(case[0], case[1])
+    assert e.value.status == abi.ERR_BAD_CONFIG

@@ -125,25 +125,11 @@ def test_standalone_pressure_solve_and_dt():
     assert co.advective_dt(0.8, 1.0) == cr.advective_dt(0.8, 1.0)
 
 
-def _viscous_cases():
-    c2 = cases.riemann2d(32, bc=abi.BC_NOSLIPWALL)
-    c2[0].mu = 0.01
-    wa = cases.water_air(64, p_left=2e5)
-    wa[0].nPhaseMu = 2
-    wa[0].phaseMu[0], wa[0].phaseMu[1] = 1.0e-3, 1.8e-5
-    a3 = cases.acoustic3d(10, igr=False)
-    a3[0].mu = 0.05
-    v2 = cases.vortex2d(32)
-    v2[0].mu = 0.02
-    return {"riemann2d_noslip": (c2, 6), "water_air_phase_mu": (wa, 6), "acoustic3d_semi": (a3, 3),
-            "vortex_periodic": (v2, 4)}
-
-
-@pytest.mark.parametrize("name", ["riemann2d_noslip", "water_air_phase_mu", "acoustic3d_semi", "vortex_periodic"])
+@pytest.mark.parametrize("name", cases.VISCOUS_CASES)
 def test_viscous_stress(name):
     """addViscousFluxes (src/ViscousFlux.cpp) and computeViscousDt
     (src/RKTimeStepping.cpp:161-188) in the explicit and semi-implicit steps."""
-    case, n = _viscous_cases()[name]
+    case, n = cases.viscous(name)
     _compare(case, n)
 
 
@@ -154,3 +140,13 @@ def test_viscous_config_validation():
     assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.ERR_BAD_CONFIG
     bad.mu, bad.nPhaseMu = 0.0, 2
     assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.ERR_BAD_CONFIG
+
+
+def test_viscous_3d_explicit_walls():
+    """All three face directions, transverse gradients through corner ghosts
+    of mixed wall kinds, RK2 + LF."""
+    case = cases.acoustic3d(9, semi=False, igr=False, rk=2, riemann=abi.LF)
+    case[0].mu = 0.03
+    case[1].bc = [abi.BC_NOSLIPWALL, abi.BC_SLIPWALL, abi.BC_NOSLIPWALL, abi.BC_OUTFLOW,
+                  abi.BC_SYMMETRY, abi.BC_NOSLIPWALL]
+    _compare(case, 4)
