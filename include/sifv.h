@@ -136,6 +136,11 @@ typedef struct sifv_config {
     double mu;
     double phaseMu[SIFV_MAX_PHASES];
     int    nPhaseMu;
+    /* SurfaceTensionParams (include/SimulationConfig.hpp:67-70): capillary
+     * coefficient sigma (0 = off; needs nPhases >= 2, the interface is
+     * phase 0's volume fraction) and the |grad alpha| regularisation. */
+    double stSigma;
+    double stEpsGradAlpha;
 } sifv_config_t;
 
 /* Mesh: physical node coordinates per axis (n+1 entries; NULL for an

@@ -98,6 +98,8 @@ static SimulationConfig toConfig(const sifv_config_t* c) {
     }
     s.viscousParams.mu = c->mu;
     s.viscousParams.phaseMu.assign(c->phaseMu, c->phaseMu + c->nPhaseMu);
+    s.surfaceTensionParams.sigma = c->stSigma;
+    s.surfaceTensionParams.epsGradAlpha = c->stEpsGradAlpha;
     return s;
 }
 

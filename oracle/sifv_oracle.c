@@ -768,6 +768,7 @@ static void scatter_face(ctx_t* m, const Flux* F, int hasL, size_t iL, double co
 
 static int has_viscosity(const sifv_config_t* c);
 static void add_viscous_fluxes(ctx_t* m);
+static void add_surface_tension_fluxes(ctx_t* m);
 
 static void compute_rhs(ctx_t* m) {
     const int nPh = m->c.nPhases;
@@ -862,6 +863,8 @@ static void compute_rhs(ctx_t* m) {
     }
     /* viscous stress: src/ExplicitSolver.cpp:523-527, src/SemiImplicitSolver.cpp:509-513 */
     if (has_viscosity(&m->c)) add_viscous_fluxes(m);
+    /* capillary stress: src/ExplicitSolver.cpp:529-534, src/SemiImplicitSolver.cpp:515-520 */
+    if (m->c.stSigma > 0.0) add_surface_tension_fluxes(m);
 }
 
 /* ---- viscous stress: addViscousFluxes, src/ViscousFlux.cpp:24-303 ---- */
@@ -1026,6 +1029,123 @@ static double viscous_dt(const ctx_t* m, double mu, double cfl, double maxDt) {
                 if (dim >= 3) dxMin = smin(dxMin, DZ(m, k));
                 double nu = mu / smax(m->rho[idx], 1e-14);
                 double dtCell = dxMin * dxMin / (2.0 * dim * nu);
+                dt = smin(dt, cfl * dtCell);
+            }
+    return dt;
+}
+
+/* ---- capillary stress: addSurfaceTensionFluxes, src/SurfaceTension.cpp:8-254 ---- */
+/* T = sigma (|g| I - g g^T / |g|) of g = grad alpha_0 at the face (normal:
+ * two-cell difference; transverse: central differences averaged over the
+ * two cells), |g| regularised by epsGradAlpha; work T.u_face.  Same
+ * accumulation as the viscous stress. */
+static void add_surface_tension_fluxes(ctx_t* m) {
+    const int dim = m->dim;
+    const double sigma = m->c.stSigma, eps = m->c.stEpsGradAlpha;
+    const double* a = m->alpha[0];
+    const double* U = m->velU;
+    const double* V = m->velV;
+    const double* W = m->velW;
+    for (int k = 0; k < m->nz; ++k)
+        for (int j = 0; j < m->ny; ++j)
+            for (int i = 0; i <= m->nx; ++i) {
+                size_t iL = IDX(m, i - 1, j, k), iR = IDX(m, i, j, k);
+                double dxi = 0.5 * (DX(m, i - 1) + DX(m, i));
+                double gx = (a[iR] - a[iL]) / dxi, gy = 0.0, gz = 0.0;
+                if (dim >= 2) {
+                    double dyj = DY(m, j);
+                    double gL = (a[IDX(m, i - 1, j + 1, k)] - a[IDX(m, i - 1, j - 1, k)]) / (2.0 * dyj);
+                    double gR = (a[IDX(m, i, j + 1, k)] - a[IDX(m, i, j - 1, k)]) / (2.0 * dyj);
+                    gy = 0.5 * (gL + gR);
+                }
+                if (dim >= 3) {
+                    double dzk = DZ(m, k);
+                    double gL = (a[IDX(m, i - 1, j, k + 1)] - a[IDX(m, i - 1, j, k - 1)]) / (2.0 * dzk);
+                    double gR = (a[IDX(m, i, j, k + 1)] - a[IDX(m, i, j, k - 1)]) / (2.0 * dzk);
+                    gz = 0.5 * (gL + gR);
+                }
+                double ng = sqrt(gx * gx + gy * gy + gz * gz);
+                double reg = smax(ng, eps);
+                double txx = sigma * (gy * gy + gz * gz) / reg;
+                double txy = -sigma * gx * gy / reg;
+                double txz = -sigma * gx * gz / reg;
+                double uF = 0.5 * (U[iL] + U[iR]), vF = 0.0, wF = 0.0;
+                if (dim >= 2) vF = 0.5 * (V[iL] + V[iR]);
+                if (dim >= 3) wF = 0.5 * (W[iL] + W[iR]);
+                double work = txx * uF + txy * vF + txz * wF;
+                double area = DY(m, j) * DZ(m, k);
+                visc_scatter(m, i >= 1, iL, (i >= 1) ? area / VOL(m, i - 1, j, k) : 0.0, i < m->nx, iR,
+                             (i < m->nx) ? area / VOL(m, i, j, k) : 0.0, txx, txy, txz, work);
+            }
+    if (dim >= 2)
+        for (int k = 0; k < m->nz; ++k)
+            for (int j = 0; j <= m->ny; ++j)
+                for (int i = 0; i < m->nx; ++i) {
+                    size_t iL = IDX(m, i, j - 1, k), iR = IDX(m, i, j, k);
+                    double dyj = 0.5 * (DY(m, j - 1) + DY(m, j));
+                    double gy = (a[iR] - a[iL]) / dyj, gz = 0.0;
+                    double dxi = DX(m, i);
+                    double gxL = (a[IDX(m, i + 1, j - 1, k)] - a[IDX(m, i - 1, j - 1, k)]) / (2.0 * dxi);
+                    double gxR = (a[IDX(m, i + 1, j, k)] - a[IDX(m, i - 1, j, k)]) / (2.0 * dxi);
+                    double gx = 0.5 * (gxL + gxR);
+                    if (dim >= 3) {
+                        double dzk = DZ(m, k);
+                        double gL = (a[IDX(m, i, j - 1, k + 1)] - a[IDX(m, i, j - 1, k - 1)]) / (2.0 * dzk);
+                        double gR = (a[IDX(m, i, j, k + 1)] - a[IDX(m, i, j, k - 1)]) / (2.0 * dzk);
+                        gz = 0.5 * (gL + gR);
+                    }
+                    double ng = sqrt(gx * gx + gy * gy + gz * gz);
+                    double reg = smax(ng, eps);
+                    double tyx = -sigma * gy * gx / reg;
+                    double tyy = sigma * (gx * gx + gz * gz) / reg;
+                    double tyz = -sigma * gy * gz / reg;
+                    double uF = 0.5 * (U[iL] + U[iR]), vF = 0.5 * (V[iL] + V[iR]), wF = 0.0;
+                    if (dim >= 3) wF = 0.5 * (W[iL] + W[iR]);
+                    double work = tyx * uF + tyy * vF + tyz * wF;
+                    double area = DX(m, i) * DZ(m, k);
+                    visc_scatter(m, j >= 1, iL, (j >= 1) ? area / VOL(m, i, j - 1, k) : 0.0, j < m->ny, iR,
+                                 (j < m->ny) ? area / VOL(m, i, j, k) : 0.0, tyx, tyy, tyz, work);
+                }
+    if (dim >= 3)
+        for (int k = 0; k <= m->nz; ++k)
+            for (int j = 0; j < m->ny; ++j)
+                for (int i = 0; i < m->nx; ++i) {
+                    size_t iL = IDX(m, i, j, k - 1), iR = IDX(m, i, j, k);
+                    double dzk = 0.5 * (DZ(m, k - 1) + DZ(m, k));
+                    double gz = (a[iR] - a[iL]) / dzk;
+                    double dxi = DX(m, i);
+                    double gxL = (a[IDX(m, i + 1, j, k - 1)] - a[IDX(m, i - 1, j, k - 1)]) / (2.0 * dxi);
+                    double gxR = (a[IDX(m, i + 1, j, k)] - a[IDX(m, i - 1, j, k)]) / (2.0 * dxi);
+                    double gx = 0.5 * (gxL + gxR);
+                    double dyj = DY(m, j);
+                    double gyL = (a[IDX(m, i, j + 1, k - 1)] - a[IDX(m, i, j - 1, k - 1)]) / (2.0 * dyj);
+                    double gyR = (a[IDX(m, i, j + 1, k)] - a[IDX(m, i, j - 1, k)]) / (2.0 * dyj);
+                    double gy = 0.5 * (gyL + gyR);
+                    double ng = sqrt(gx * gx + gy * gy + gz * gz);
+                    double reg = smax(ng, eps);
+                    double tzx = -sigma * gz * gx / reg;
+                    double tzy = -sigma * gz * gy / reg;
+                    double tzz = sigma * (gx * gx + gy * gy) / reg;
+                    double uF = 0.5 * (U[iL] + U[iR]), vF = 0.5 * (V[iL] + V[iR]), wF = 0.5 * (W[iL] + W[iR]);
+                    double work = tzx * uF + tzy * vF + tzz * wF;
+                    double area = DX(m, i) * DY(m, j);
+                    visc_scatter(m, k >= 1, iL, (k >= 1) ? area / VOL(m, i, j, k - 1) : 0.0, k < m->nz, iR,
+                                 (k < m->nz) ? area / VOL(m, i, j, k) : 0.0, tzx, tzy, tzz, work);
+                }
+}
+
+/* computeCapillaryDt, src/RKTimeStepping.cpp:201-228 */
+static double capillary_dt(const ctx_t* m, double sigma, double cfl, double maxDt) {
+    double dt = maxDt;
+    const int dim = m->dim;
+    for (int k = 0; k < m->nz; ++k)
+        for (int j = 0; j < m->ny; ++j)
+            for (int i = 0; i < m->nx; ++i) {
+                size_t idx = IDX(m, i, j, k);
+                double dxMin = DX(m, i);
+                if (dim >= 2) dxMin = smin(dxMin, DY(m, j));
+                if (dim >= 3) dxMin = smin(dxMin, DZ(m, k));
+                double dtCell = sqrt(smax(m->rho[idx], 1e-14) * dxMin * dxMin * dxMin / sigma);
                 dt = smin(dt, cfl * dtCell);
             }
     return dt;
@@ -1282,6 +1402,7 @@ static double explicit_step(ctx_t* m, int step, double targetDt) {
     } else {
         dt = acoustic_dt(m, c->cfl, c->maxDt);
         if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->cfl, c->maxDt));
+        if (c->stSigma > 0.0) dt = smin(dt, capillary_dt(m, c->stSigma, c->cfl, c->maxDt));
     }
     if (targetDt > 0) dt = smin(dt, targetDt);
     double rk[3][4];
@@ -1459,6 +1580,7 @@ static double semi_step(ctx_t* m, int step, double targetDt) {
     const sifv_config_t* c = &m->c;
     double dt = advective_dt(m, c->siCfl, c->siMaxDt);
     if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->siCfl, c->siMaxDt));
+    if (c->stSigma > 0.0) dt = smin(dt, capillary_dt(m, c->stSigma, c->siCfl, c->siMaxDt));
     if (targetDt > 0) dt = smin(dt, targetDt);
     dt = sclamp(dt, c->siMinDt, c->siMaxDt);
     double rk[3][4];
@@ -1565,6 +1687,9 @@ static int validate(const sifv_config_t* c, char* err) {
         for (int p = 0; p < c->nPhaseMu; ++p)
             if (c->phaseMu[p] < 0.0) FAIL("viscousParams.phaseMu[] must be >= 0");
     }
+    if (c->stSigma < 0.0) FAIL("surfaceTensionParams.sigma must be >= 0");
+    if (c->stEpsGradAlpha <= 0.0) FAIL("surfaceTensionParams.epsGradAlpha must be > 0");
+    if (c->stSigma > 0.0 && c->nPhases <= 0) FAIL("surfaceTensionParams.sigma requires multi-phase (nPhases >= 2)");
     return SIFV_OK;
 #undef FAIL
 }

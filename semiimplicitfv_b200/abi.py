@@ -60,6 +60,7 @@ class Config(C.Structure):
         ("bfA", C.c_double * 3), ("bfB", C.c_double * 3), ("bfC", C.c_double * 3), ("bfD", C.c_double * 3),
         ("precision", C.c_int),
         ("mu", C.c_double), ("phaseMu", C.c_double * MAX_PHASES), ("nPhaseMu", C.c_int),
+        ("stSigma", C.c_double), ("stEpsGradAlpha", C.c_double),
     ]
 
 
@@ -86,6 +87,7 @@ def config_defaults(**overrides) -> Config:
     c.nPhases, c.alphaMin = 0, 1e-8
     c.precision = PREC_FP64
     c.mu, c.nPhaseMu = 0.0, 0
+    c.stSigma, c.stEpsGradAlpha = 0.0, 1e-8
     for k, v in overrides.items():
         if k in ("phaseGamma", "phasePInf"):
             arr = getattr(c, k)

@@ -174,6 +174,10 @@ int validate(const sifv_config_t* c, std::string& msg) {
         for (int p = 0; p < c->nPhaseMu; ++p)
             if (c->phaseMu[p] < 0.0) return bad("viscousParams.phaseMu[] must be >= 0");
     }
+    if (c->stSigma < 0.0) return bad("surfaceTensionParams.sigma must be >= 0");
+    if (c->stEpsGradAlpha <= 0.0) return bad("surfaceTensionParams.epsGradAlpha must be > 0");
+    if (c->stSigma > 0.0 && c->nPhases <= 0)
+        return bad("surfaceTensionParams.sigma requires multi-phase (nPhases >= 2)");
     if (c->precision != SIFV_PREC_FP64 && c->precision != SIFV_PREC_MIXED && c->precision != SIFV_PREC_FP64_FAST)
         return bad("unknown precision");
     return SIFV_OK;
@@ -491,6 +495,10 @@ void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
             k_dt_viscous<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.siCfl);
             c->launches++;
         }
+        if (c->P.cap) {
+            k_dt_capillary<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.siCfl);
+            c->launches++;
+        }
         k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, -1.0, targetDt, 1, cfg.siMinDt, cfg.siMaxDt, useEnd ? 1 : 0);
         c->launches += 3;
     } else if (c->forcedDt > 0) {
@@ -502,6 +510,10 @@ void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
             NPH_DISPATCH(c, (k_dt_acoustic<NPHV><<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.cfl)));
             if (c->P.visc) {
                 k_dt_viscous<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.cfl);
+                c->launches++;
+            }
+            if (c->P.cap) {
+                k_dt_capillary<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.cfl);
                 c->launches++;
             }
             c->launches += 2;
@@ -628,6 +640,17 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEn
             }
             mark(c, "viscous");
         }
+        if (P.cap) {
+            for (int d = 0; d < P.dim; ++d) {
+                long long nf = (long long)(P.nx + (d == 0)) * (P.ny + (d == 1)) * (P.nz + (d == 2));
+                unsigned gf = blocks(nf, kCellThreads);
+                if (d == 0) k_cap_face<0><<<gf, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl);
+                else if (d == 1) k_cap_face<1><<<gf, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl);
+                else k_cap_face<2><<<gf, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl);
+                c->launches++;
+            }
+            mark(c, "capillary");
+        }
         if (!cfg.semiImplicit) {
             if (c->stageHook && c->stageHook(s, 1) != 0) return SIFV_ERR_CUDA;
             NPH_DISPATCH(c, (k_assemble<NPHV, 0><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, K)));
@@ -685,6 +708,7 @@ void sifv_config_defaults(sifv_config_t* c) {
     c->alphaCoeff = 1.0; c->IGRIters = 5; c->IGRWarmStartIters = 50;
     c->nPhases = 0; c->alphaMin = 1e-8;
     c->precision = SIFV_PREC_FP64;
+    c->stSigma = 0.0; c->stEpsGradAlpha = 1e-8;
 }
 
 int sifv_config_validate(const sifv_config_t* cfg) {
@@ -705,11 +729,11 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     if (cfg->precision != SIFV_PREC_FP64) {
         bool bf = false;
         for (int d = 0; d < 3; ++d) bf = bf || cfg->bfA[d] != 0.0 || cfg->bfB[d] != 0.0;
-        const bool visc = cfg->mu > 0.0 || cfg->nPhaseMu > 0;
+        const bool visc = cfg->mu > 0.0 || cfg->nPhaseMu > 0 || cfg->stSigma > 0.0;
         if (cfg->semiImplicit || cfg->nPhases > 0 || cfg->useIGR || cfg->reconOrder != SIFV_WENO5 || bf || visc)
             return fail(nullptr, SIFV_ERR_UNSUPPORTED,
                         "SIFV_PREC_MIXED / SIFV_PREC_FP64_FAST run the explicit single-phase WENO5 step without "
-                        "IGR, body force or viscosity; use SIFV_PREC_FP64 for this configuration");
+                        "IGR, body force, viscosity or surface tension; use SIFV_PREC_FP64 for this configuration");
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -766,6 +790,9 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     P.perPhaseMu = cfg->nPhaseMu > 0 ? 1 : 0;
     P.mu = cfg->mu;
     for (int p = 0; p < SIFV_MAX_PHASES; ++p) P.phaseMu[p] = (p < cfg->nPhaseMu) ? cfg->phaseMu[p] : 0.0;
+    P.cap = cfg->stSigma > 0.0 ? 1 : 0;
+    P.stSigma = cfg->stSigma;
+    P.stEps = cfg->stEpsGradAlpha;
     c->nphT = (cfg->nPhases == 0) ? 0 : (cfg->nPhases <= 2) ? 2 : 8;
     c->W = (cfg->reconOrder == SIFV_WENO1 || cfg->reconOrder == SIFV_UPWIND1) ? 1
          : (cfg->reconOrder == SIFV_WENO3 || cfg->reconOrder == SIFV_UPWIND3) ? 3 : 5;
@@ -810,6 +837,8 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
         }
         if (P.visc)
             for (int q = 0; q < 4; ++q) F.flux[d][FS_VISC + q] = (q == 0 || q == 3 || q < dim) ? dalloc(c, nf, st) : nullptr;
+        if (P.cap)
+            for (int q = 0; q < 4; ++q) F.flux[d][FS_CAP + q] = (q == 0 || q == 3 || q < dim) ? dalloc(c, nf, st) : nullptr;
     }
     // geometry: per-cell widths incl. ghosts, and IGR alpha/d^2
     static const double unit[2] = {0.0, 1.0};
@@ -1184,10 +1213,10 @@ int cons_slot(const sifv_ctx* c, int field) {
 int adjoint_supported(sifv_ctx* c) {
     const sifv_config_t& g = c->cfg;
     if (g.semiImplicit || g.useIGR || g.nPhases > 0 || has_body_force(g) || g.precision != SIFV_PREC_FP64 ||
-        (g.reconOrder != SIFV_WENO5 && g.reconOrder != SIFV_UPWIND5) || g.nGhost > 7 || c->P.visc)
+        (g.reconOrder != SIFV_WENO5 && g.reconOrder != SIFV_UPWIND5) || g.nGhost > 7 || c->P.visc || c->P.cap)
         return fail(c, SIFV_ERR_UNSUPPORTED,
                     "the adjoint / tangent covers the explicit single-phase WENO5 / UPWIND5 step in SIFV_PREC_FP64 "
-                    "without IGR, body force or viscosity (nGhost <= 7)");
+                    "without IGR, body force, viscosity or surface tension (nGhost <= 7)");
     return SIFV_OK;
 }
 

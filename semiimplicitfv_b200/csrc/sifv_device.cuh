@@ -38,7 +38,8 @@ enum FluxSlot : int {
     FS_ALPHA = 7,   // alphaFlux[ph]         7 .. 7+MAXPH-1
     FS_AR = 7 + MAXPH,  // upwinded alphaRho flux[ph]
     FS_VISC = 7 + 2 * MAXPH,   // viscous stress on the face: tau.x, tau.y, tau.z, work (4 slots)
-    FS_COUNT = 11 + 2 * MAXPH
+    FS_CAP = 11 + 2 * MAXPH,   // capillary stress on the face, same layout (4 slots)
+    FS_COUNT = 15 + 2 * MAXPH
 };
 
 struct Params {
@@ -63,6 +64,8 @@ struct Params {
     int perPhaseMu;          // per-phase viscosities (else the scalar mu)
     double mu;
     double phaseMu[MAXPH];
+    int cap;                 // capillary stress on (SimulationConfig::hasSurfaceTension)
+    double stSigma, stEps;
 };
 
 struct Fields {

@@ -128,11 +128,11 @@ int sifv_ensemble_create(const sifv_config_t* cfg, int nInst, const int* nCells,
     if (sifv_config_validate(cfg) != SIFV_OK) return efail(nullptr, SIFV_ERR_BAD_CONFIG, sifv_last_error(nullptr));
     bool bf = false;
     for (int d = 0; d < 3; ++d) bf = bf || cfg->bfA[d] != 0.0 || cfg->bfB[d] != 0.0;
-    if (cfg->dim != 1 || cfg->semiImplicit || cfg->useIGR || bf || cfg->mu > 0.0 || cfg->nPhaseMu > 0 ||
+    if (cfg->dim != 1 || cfg->semiImplicit || cfg->useIGR || bf || cfg->mu > 0.0 || cfg->nPhaseMu > 0 || cfg->stSigma > 0.0 ||
         (cfg->reconOrder != SIFV_WENO5 && cfg->reconOrder != SIFV_UPWIND5) ||
         (cfg->precision != SIFV_PREC_FP64 && cfg->precision != SIFV_PREC_MIXED))
         return efail(nullptr, SIFV_ERR_UNSUPPORTED,
-                     "ensembles run the explicit 1D WENO5/UPWIND5 step (no IGR, body force or viscosity) in "
+                     "ensembles run the explicit 1D WENO5/UPWIND5 step (no IGR, body force, viscosity or surface tension) in "
                      "SIFV_PREC_FP64 or SIFV_PREC_MIXED");
     for (int k = 0; k < nInst; ++k)
         if (nCells[k] < cfg->nGhost || !(xHi[k] > xLo[k]))

@@ -231,6 +231,26 @@ __device__ __forceinline__ void mp_post(const Params& P, const Fields& F, size_t
 
 // MODE 0: explicit SSP-RK update (src/ExplicitSolver.cpp:127-188).
 // MODE 1: semi-implicit star update (src/SemiImplicitSolver.cpp:159-223).
+// A face stress (viscous or capillary, four face arrays from `slot`: the
+// momentum components and the work) added to one cell's rhs: per direction
+// the low face (-) then the high face (+), the reference's face-loop order.
+__device__ __forceinline__ void add_face_stress(int dim, const Fields& F, const CellFaces& cf, int slot,
+                                                double& rU, double& rV, double& rW, double& rE) {
+    DIMLOOP(d) {
+        const double co = cf.coeff[d];
+        const long long lo = cf.lo[d], hi = cf.lo[d] + cf.hiOff[d];
+        double* const* fv = F.flux[d] + slot;
+        rU -= co * fv[0][lo];
+        if (dim >= 2) rV -= co * fv[1][lo];
+        if (dim >= 3) rW -= co * fv[2][lo];
+        rE -= co * fv[3][lo];
+        rU += co * fv[0][hi];
+        if (dim >= 2) rV += co * fv[1][hi];
+        if (dim >= 3) rW += co * fv[2][hi];
+        rE += co * fv[3][hi];
+    }
+}
+
 template <int NPH, int MODE>
 __global__ void __launch_bounds__(256) k_assemble(Params P, Fields F, const Ctl* __restrict__ ctl, StageCoef K) {
     if (ctl->skip) return;
@@ -271,21 +291,10 @@ __global__ void __launch_bounds__(256) k_assemble(Params P, Fields F, const Ctl*
         rE += rho * work;
     }
 
-    if (P.visc) {   // addViscousFluxes (src/ViscousFlux.cpp:24-303): per direction low face (-), high face (+)
-        DIMLOOP(d) {
-            const double co = cf.coeff[d];
-            const long long lo = cf.lo[d], hi = cf.lo[d] + cf.hiOff[d];
-            double* const* fv = F.flux[d] + FS_VISC;
-            rU -= co * fv[0][lo];
-            if (dim >= 2) rV -= co * fv[1][lo];
-            if (dim >= 3) rW -= co * fv[2][lo];
-            rE -= co * fv[3][lo];
-            rU += co * fv[0][hi];
-            if (dim >= 2) rV += co * fv[1][hi];
-            if (dim >= 3) rW += co * fv[2][hi];
-            rE += co * fv[3][hi];
-        }
-    }
+    // addViscousFluxes (src/ViscousFlux.cpp:24-303), then addSurfaceTensionFluxes
+    // (src/SurfaceTension.cpp:8-254)
+    if (P.visc) add_face_stress(dim, F, cf, FS_VISC, rU, rV, rW, rE);
+    if (P.cap) add_face_stress(dim, F, cf, FS_CAP, rU, rV, rW, rE);
 
     const double dt = ctl->dt;
     const double c1 = K.c1, c2 = K.c2, c3 = K.c3, c4 = K.c4;
@@ -564,6 +573,88 @@ __global__ void __launch_bounds__(256) k_visc_face(Params P, Fields F, const Ctl
     out[0][t] = t0;
     if (dim >= 2) out[1][t] = t1;
     if (dim >= 3) out[2][t] = t2;
+    out[3][t] = work;
+}
+
+// computeCapillaryDt (src/RKTimeStepping.cpp:201-228), folded into the same
+// minimum as the other limits.
+__global__ void __launch_bounds__(256) k_dt_capillary(Params P, Fields F, Ctl* ctl, double cfl) {
+    if (ctl->skip) return;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    double v = __longlong_as_double(0x7ff0000000000000LL);
+    if (int_coords(P, t, i, j, k)) {
+        const int dim = P.dim;
+        size_t c = cidx(P, i, j, k);
+        double dxMin = F.dx[i + P.ngx];
+        if (dim >= 2) dxMin = smin(dxMin, F.dy[j + P.ngy]);
+        if (dim >= 3) dxMin = smin(dxMin, F.dz[k + P.ngz]);
+        double dtCell = sqrt(smax(F.rho[c], 1e-14) * dxMin * dxMin * dxMin / P.stSigma);
+        v = cfl * dtCell;
+    }
+    block_min_to(v, &ctl->dtBits);
+}
+
+// Capillary stress T = sigma (|g| I - g g^T / |g|) on the faces of direction
+// DIR, g = grad alpha_0 (normal: two-cell difference; transverse: central
+// differences averaged over the two cells), |g| floored at epsGradAlpha;
+// work T.u with the face-averaged velocity (src/SurfaceTension.cpp:8-254).
+// Stored per face as T.x, T.y, T.z, work.
+template <int DIR>
+__global__ void __launch_bounds__(256) k_cap_face(Params P, Fields F, const Ctl* __restrict__ ctl) {
+    if (ctl && ctl->skip) return;
+    const int dim = P.dim;
+    const int fnx = P.nx + (DIR == 0), fny = P.ny + (DIR == 1), fnz = P.nz + (DIR == 2);
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long tot = (long long)fnx * fny * fnz;
+    if (t >= tot) return;
+    int i, j, k;
+    split3(t, fnx, fny, i, j, k);
+    const double* a = F.alpha[0];
+    auto at = [&](int x, int y, int z) { return a[cidx(P, x, y, z)]; };
+    const int li = i - (DIR == 0), lj = j - (DIR == 1), lk = k - (DIR == 2);
+    const size_t iL = cidx(P, li, lj, lk), iR = cidx(P, i, j, k);
+    const double sigma = P.stSigma;
+    double g[3] = {0.0, 0.0, 0.0};
+    {   // normal component
+        const double* w = (DIR == 0) ? F.dx : (DIR == 1) ? F.dy : F.dz;
+        const int q = (DIR == 0) ? i + P.ngx : (DIR == 1) ? j + P.ngy : k + P.ngz;
+        g[DIR] = (a[iR] - a[iL]) / (0.5 * (w[q - 1] + w[q]));
+    }
+    if (DIR != 0) {   // x transverse (dim >= 2 whenever DIR != 0)
+        const double d = F.dx[i + P.ngx];
+        const double gL = (at(li + 1, lj, lk) - at(li - 1, lj, lk)) / (2.0 * d);
+        const double gR = (at(i + 1, j, k) - at(i - 1, j, k)) / (2.0 * d);
+        g[0] = 0.5 * (gL + gR);
+    }
+    if (DIR != 1 && dim >= 2) {
+        const double d = F.dy[j + P.ngy];
+        const double gL = (at(li, lj + 1, lk) - at(li, lj - 1, lk)) / (2.0 * d);
+        const double gR = (at(i, j + 1, k) - at(i, j - 1, k)) / (2.0 * d);
+        g[1] = 0.5 * (gL + gR);
+    }
+    if (DIR != 2 && dim >= 3) {
+        const double d = F.dz[k + P.ngz];
+        const double gL = (at(li, lj, lk + 1) - at(li, lj, lk - 1)) / (2.0 * d);
+        const double gR = (at(i, j, k + 1) - at(i, j, k - 1)) / (2.0 * d);
+        g[2] = 0.5 * (gL + gR);
+    }
+    const double ng = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+    const double reg = smax(ng, P.stEps);
+    // tangential-plane part on the diagonal, -sigma g_n g_t / |g| off it
+    constexpr int T1 = (DIR == 0) ? 1 : 0, T2 = (DIR == 2) ? 1 : 2;
+    double T[3];
+    T[DIR] = sigma * (g[T1] * g[T1] + g[T2] * g[T2]) / reg;
+    T[T1] = -sigma * g[DIR] * g[T1] / reg;
+    T[T2] = -sigma * g[DIR] * g[T2] / reg;
+    double uF = 0.5 * (F.velU[iL] + F.velU[iR]), vF = 0.0, wF = 0.0;
+    if (dim >= 2) vF = 0.5 * (F.velV[iL] + F.velV[iR]);
+    if (dim >= 3) wF = 0.5 * (F.velW[iL] + F.velW[iR]);
+    const double work = T[0] * uF + T[1] * vF + T[2] * wF;
+    double* const* out = F.flux[DIR] + FS_CAP;
+    out[0][t] = T[0];
+    if (dim >= 2) out[1][t] = T[1];
+    if (dim >= 3) out[2][t] = T[2];
     out[3][t] = work;
 }
 

@@ -107,7 +107,8 @@ inline sifv_config_t toSifvConfig(const SimulationConfig& c, const EquationOfSta
         throw std::invalid_argument("viscousParams.phaseMu has more than SIFV_MAX_PHASES entries");
     s.nPhaseMu = (int)c.viscousParams.phaseMu.size();
     for (int p = 0; p < s.nPhaseMu; ++p) s.phaseMu[p] = c.viscousParams.phaseMu[p];
-    if (c.hasSurfaceTension()) throw std::invalid_argument("the CUDA step has no surface-tension term");
+    s.stSigma = c.surfaceTensionParams.sigma;
+    s.stEpsGradAlpha = c.surfaceTensionParams.epsGradAlpha;
     return s;
 }
 

@@ -244,6 +244,77 @@ def advection1d(n=128, semi=False, riemann=abi.LF, cfl=0.8, rk=3):
     return cfg, abi.MeshSpec(x, bc=[BC_PERIODIC] * 6), fields
 
 
+def droplet(n=48, dim=2, semi=False, sigma=0.0728, rk=3, bc=BC_OUTFLOW):
+    """Water droplet in air with surface tension (examples/2D_laplace_pressure_jump/
+    2D_laplace_pressure_jump.cpp:39-83): radius 1 mm in [0, 6 mm]^dim, water
+    gamma 4.4 / pInf 6e8 / rho 1000, air gamma 1.4 / rho 1.225, interface
+    alpha_w = (1 - tanh((r - R0) / 3 dx)) / 2 clipped to [alphaMin, 1 - alphaMin],
+    energy from p = pAtm + (sigma / R0) alpha-profile, stored pressure pAtm,
+    fluid at rest.  dim = 3 puts a sphere in the cube."""
+    L, R0, p_atm, rw, ra, amin = 6.0e-3, 1.0e-3, 1.0e5, 1000.0, 1.225, 1e-8
+    cfg = abi.config_defaults(dim=dim, nGhost=3, RKOrder=rk, reconOrder=abi.WENO5, riemannSolver=abi.HLLC,
+                              cfl=0.5, semiImplicit=int(semi), siCfl=0.5, pressureTol=1e-3, maxPressureIters=200,
+                              nPhases=2, phaseGamma=[4.4, 1.4], phasePInf=[6.0e8, 0.0], alphaMin=amin,
+                              stSigma=sigma)
+    x = abi.linspace_nodes(n, 0.0, L)
+    c = _centroids(x)
+    if dim == 3:
+        Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+        r = np.sqrt((X - 0.5 * L) ** 2 + (Y - 0.5 * L) ** 2 + (Z - 0.5 * L) ** 2)
+    else:
+        Y, X = np.meshgrid(c, c, indexing="ij")
+        r = np.sqrt((X - 0.5 * L) ** 2 + (Y - 0.5 * L) ** 2)[None]
+    eps = 3.0 * (x[1] - x[0])
+    prof = 0.5 * (1.0 - np.tanh((r - R0) / eps))
+    aw = np.maximum(amin, np.minimum(1.0 - amin, prof))
+    aa = 1.0 - aw
+    p = p_atm + (0.0728 / R0) * prof   # Laplace jump sigma / R0 of water-air
+    shape = _ext_shape(cfg, n, n if dim >= 2 else 1, n if dim >= 3 else 1)
+    sl = _interior_slices(cfg)
+    fids = [F_RHO, F_RHOU, F_RHOV, F_RHOE, F_VELU, F_VELV, F_PRES, F_SIGMA,
+            F_ALPHARHO(0), F_ALPHARHO(1), F_ALPHA(0), F_ALPHA(1)]
+    if dim >= 3:
+        fids += [F_RHOW, F_VELW]
+    f = {fid: np.zeros(shape) for fid in fids}
+    f[F_ALPHARHO(0)][sl] = aw * rw
+    f[F_ALPHARHO(1)][sl] = aa * ra
+    f[F_ALPHA(0)][sl] = aw
+    f[F_ALPHA(1)][sl] = aa
+    f[F_RHO][sl] = aw * rw + aa * ra
+    f[F_PRES][sl] = p_atm
+    # mixtureTotalEnergy(rho, p, alphas, ke=0) (src/MixtureEOS.cpp:65-76)
+    e = 0.0 + aw * (p + 4.4 * 6.0e8) / (4.4 - 1.0)
+    e = e + aa * (p + 1.4 * 0.0) / (1.4 - 1.0)
+    f[F_RHOE][sl] = e
+    mesh = abi.MeshSpec(x, x, x, bc=[bc] * 6) if dim == 3 else abi.MeshSpec(x, x, bc=[bc] * 6)
+    return cfg, mesh, f
+
+
+CAPILLARY_CASES = ["droplet2d", "droplet2d_semi", "droplet3d_walls", "droplet2d_viscous"]
+
+
+def capillary(name):
+    """Surface-tension variants (surfaceTensionParams, include/SimulationConfig.hpp:67-70).
+    Returns (case, steps)."""
+    if name == "droplet2d":
+        return droplet(40), 5
+    if name == "droplet2d_semi":
+        return droplet(32, semi=True, rk=2), 3
+    if name == "droplet3d_walls":
+        c = droplet(14, dim=3, rk=2)
+        c[1].bc = [abi.BC_NOSLIPWALL, abi.BC_SLIPWALL, abi.BC_OUTFLOW, abi.BC_SYMMETRY,
+                   abi.BC_NOSLIPWALL, abi.BC_OUTFLOW]
+        return c, 3
+    if name == "droplet2d_viscous":
+        c = droplet(32, bc=abi.BC_PERIODIC)
+        c[0].nPhaseMu = 2
+        c[0].phaseMu[0], c[0].phaseMu[1] = 1.0e-3, 1.8e-5
+        c[0].mu = 1.0e-4
+        c[0].stEpsGradAlpha = 1e-3
+        return c, 4
+    raise KeyError(name)
+
+
 VISCOUS_CASES = ["riemann2d_noslip", "water_air_phase_mu", "acoustic3d_semi", "vortex_periodic"]
 
 

@@ -271,3 +271,22 @@ def test_viscous_rejected_outside_reference_precision():
     with pytest.raises(abi.AbiError) as e:
         backends.cuda().create(case[0], case[1])
     assert e.value.status == abi.ERR_BAD_CONFIG
+
+
+@pytest.mark.parametrize("name", cases.CAPILLARY_CASES)
+def test_surface_tension(name):
+    """addSurfaceTensionFluxes (src/SurfaceTension.cpp:8-254) on every face
+    and the capillary step limit (computeCapillaryDt,
+    src/RKTimeStepping.cpp:201-228), explicit and semi-implicit, 2D and 3D,
+    alone and after the viscous stress: bit-identical to the oracle."""
+    case, n = cases.capillary(name)
+    check(case, n)
+
+
+def test_surface_tension_rejected_without_phases():
+    case, _ = cases.viscous("vortex_periodic")
+    case[0].mu = 0.0
+    case[0].stSigma = 0.07
+    with pytest.raises(abi.AbiError) as e:
+        backends.cuda().create(case[0], case[1])
+    assert e.value.status == abi.ERR_BAD_CONFIG

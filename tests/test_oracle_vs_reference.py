@@ -150,3 +150,26 @@ def test_viscous_3d_explicit_walls():
     case[1].bc = [abi.BC_NOSLIPWALL, abi.BC_SLIPWALL, abi.BC_NOSLIPWALL, abi.BC_OUTFLOW,
                   abi.BC_SYMMETRY, abi.BC_NOSLIPWALL]
     _compare(case, 4)
+
+
+@pytest.mark.parametrize("name", cases.CAPILLARY_CASES)
+def test_surface_tension(name):
+    """addSurfaceTensionFluxes (src/SurfaceTension.cpp) and computeCapillaryDt
+    (src/RKTimeStepping.cpp:201-228), explicit and semi-implicit, 2D and 3D,
+    alone and after the viscous stress."""
+    case, n = cases.capillary(name)
+    _compare(case, n)
+
+
+def test_surface_tension_config_validation():
+    lib = backends.oracle()
+    bad = abi.config_defaults(dim=2, nGhost=3, reconOrder=abi.WENO5, nPhases=2, phaseGamma=[4.4, 1.4],
+                              phasePInf=[6e8, 0.0])
+    bad.stSigma = -1.0
+    assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.ERR_BAD_CONFIG
+    bad.stSigma, bad.stEpsGradAlpha = 0.07, 0.0
+    assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.ERR_BAD_CONFIG
+    bad.stEpsGradAlpha = 1e-8
+    assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.OK
+    bad.nPhases = 0
+    assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.ERR_BAD_CONFIG
