@@ -256,6 +256,84 @@ int sifv_last_step_stats(const sifv_ctx_t* ctx, double* deviceMs, int* launches)
 #define SIFV_PRESSURE_GAUSS_SEIDEL 1
 int sifv_set_pressure_solver(sifv_ctx_t* ctx, int kind);
 
+/* ---- output path: NaN check, VTK, time loop ------------------------------- */
+/* runTimeLoop's NaN check (src/RKTimeStepping.cpp:280-311) on the device:
+ * the first interior cell in (k, j, i) order holding a NaN in rho, rhoU,
+ * rhoE, pres, rhoV (dim >= 2) or rhoW (dim >= 3), tested in that order.
+ * *field = the SIFV_F_* id of that field, or -1 when there is none;
+ * *cell = its interior index i + nx (j + ny k) (-1 when none). */
+int sifv_check_nan(sifv_ctx_t* ctx, int* field, long long* cell);
+
+/* VTK XML output with the files and bytes of VTKSession / VTKWriter
+ * (src/VTKSession.cpp, src/VTKWriter.cpp) for one rank:
+ *   <dir>/<base>.pvd                                 time series
+ *   <dir>/snapshot_<n>/<base>_<n>_r0.vtr             the piece (RectilinearGrid, ASCII)
+ *   <dir>/snapshot_<n>/<base>_<n>.pvtr               its parallel meta-file
+ * The session is host-side: sifv_vtk_open writes the .pvd header.
+ * nThreads <= 0: one formatting thread per hardware thread. */
+typedef struct sifv_vtk sifv_vtk_t;
+int sifv_vtk_open(const char* dir, const char* baseName, const sifv_config_t* cfg, const sifv_mesh_t* mesh,
+                  int nThreads, sifv_vtk_t** out);
+/* Host fields in the context layout (totalCells doubles, ghosts included):
+ * every pointer the written arrays need (pres, sigma when useIGR, rhoE,
+ * vel and mom of the active dims, rho single-phase or alphaRho[] / alpha[]
+ * of each phase). */
+typedef struct sifv_vtk_fields {
+    const double* pres;
+    const double* sigma;
+    const double* rhoE;
+    const double* vel[3];
+    const double* mom[3];
+    const double* rho;
+    const double* alphaRho[SIFV_MAX_PHASES];
+    const double* alpha[SIFV_MAX_PHASES];
+} sifv_vtk_fields_t;
+/* VTKSession::write(state, time) from host arrays; synchronous. */
+int sifv_vtk_write_host(sifv_vtk_t* vtk, double time, const sifv_vtk_fields_t* fields);
+/* VTKSession::write from a context's device state: the fields are copied
+ * to a device staging slot on the context's stream (the next step may run
+ * at once), brought to pinned host memory on a copy stream and written by
+ * the session's writer thread while the context keeps stepping.  Two
+ * staging slots; a third write waits for the oldest. */
+int sifv_vtk_write(sifv_vtk_t* vtk, sifv_ctx_t* ctx, double time);
+/* Wait for every queued write; returns the first write error. */
+int sifv_vtk_flush(sifv_vtk_t* vtk);
+/* Flush, then release the session (VTKSession::finalize). */
+int sifv_vtk_close(sifv_vtk_t* vtk);
+const char* sifv_vtk_last_error(const sifv_vtk_t* vtk);
+
+/* runTimeLoop (src/RKTimeStepping.cpp:241-356, TimeLoopParams
+ * include/RKTimeStepping.hpp:91-99) on a context: output at t = 0 and
+ * whenever t >= nextOutput - 1e-12 outputInterval, dt capped to hit every
+ * output time and endTime, NaN check at each output.  Explicit steps
+ * without body force run device-resident (dt, time and the output
+ * condition live on the device; the host looks in every `batch` steps);
+ * semi-implicit and body-force steps run one step per host round trip.
+ * progress (may be NULL) is called for step 1 and every printInterval-th
+ * step with the step's dt.  vtk may be NULL (no files).  Returns SIFV_OK,
+ * or SIFV_ERR_NAN with *result naming the field and cell (the snapshot of
+ * that output is still written, as in the reference). */
+typedef struct sifv_time_loop {
+    double endTime;
+    double outputInterval;
+    int printInterval;
+    int checkNaN;
+    int step0;        /* SimulationConfig::step at entry */
+    int batch;        /* device-resident steps between host checks (<= 0: 64) */
+} sifv_time_loop_t;
+typedef struct sifv_loop_result {
+    double time;
+    int steps;        /* SimulationConfig::step at exit */
+    int outputs;      /* outputs reached, t = 0 included */
+    int nanField;     /* SIFV_F_* of the NaN, -1 = none */
+    long long nanCell;
+    double nanTime;
+    int nanStep;
+} sifv_loop_result_t;
+typedef void (*sifv_progress_fn)(void* user, int step, double time, double dt);
+int sifv_run_time_loop(sifv_ctx_t* ctx, const sifv_time_loop_t* params, sifv_vtk_t* vtk,
+                       sifv_progress_fn progress, void* user, sifv_loop_result_t* result);
+
 /* ---- diagnostics ----------------------------------------------------------- */
 /* Maximum relative error of the fast paths' reciprocal and square root
  * against IEEE 1/x and sqrt(x) over n arguments spread across [2^-60, 2^60)

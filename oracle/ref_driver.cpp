@@ -30,6 +30,8 @@
 #include "SimulationConfig.hpp"
 #include "SolutionState.hpp"
 #include "StiffenedGasEOS.hpp"
+#include "Runtime.hpp"
+#include "VTKSession.hpp"
 
 #include "sifv.h"
 
@@ -318,6 +320,42 @@ int sifvr_igr_solve(sifvr_ctx* ctx, int step) {
     cfg.step = step;
     ctx->igr->solveEntropicPressure(cfg, mesh, ctx->state, gradU, *ctx->halo);
     return SIFV_OK;
+}
+
+// The reference's own runTimeLoop (src/RKTimeStepping.cpp:241-356) with its
+// VTKSession (src/VTKSession.cpp) over this context's solver, starting at
+// t = 0, step 0.  The Runtime only provides the MPI context VTKSession
+// reads (global sizes, this rank's extent); the mesh written is the
+// context's own.  *stepsOut = SimulationConfig::step at exit.
+int sifvr_reference_time_loop(sifvr_ctx* ctx, const char* dir, const char* base, double endTime, double outputInterval,
+                        int printInterval, int* stepsOut) {
+    try {
+        int argc = 0;
+        char** argv = nullptr;
+        Runtime rt(argc, argv);
+        const RectilinearMesh& m = *ctx->mesh;
+        if (ctx->config.dim == 1) rt.createUniformMesh(ctx->config, m.nx(), 0.0, 1.0);
+        else if (ctx->config.dim == 2) rt.createUniformMesh(ctx->config, m.nx(), 0.0, 1.0, m.ny(), 0.0, 1.0);
+        else rt.createUniformMesh(ctx->config, m.nx(), 0.0, 1.0, m.ny(), 0.0, 1.0, m.nz(), 0.0, 1.0);
+        VTKSession vtk(rt, base, m, ctx->config, dir);
+        TimeLoopParams p;
+        p.endTime = endTime;
+        p.outputInterval = outputInterval;
+        p.printInterval = printInterval;
+        p.checkNaN = true;
+        ctx->config.step = 0;
+        ctx->config.time = 0.0;
+        auto stepFn = [ctx](double targetDt) {
+            if (ctx->semi) return ctx->semi->step(ctx->config, *ctx->mesh, ctx->state, targetDt);
+            return ctx->expl->step(ctx->config, *ctx->mesh, ctx->state, targetDt);
+        };
+        runTimeLoop(rt, ctx->config, m, ctx->state, vtk, stepFn, p);
+        if (stepsOut) *stepsOut = ctx->config.step;
+        return SIFV_OK;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return SIFV_ERR_BAD_ARG;
+    }
 }
 
 }  // extern "C"

@@ -1851,3 +1851,29 @@ int sifvo_apply_bc(ctx_t* m) {
     apply_bc_prim(m);
     return SIFV_OK;
 }
+
+/* runTimeLoop's NaN check (src/RKTimeStepping.cpp:280-292): the first
+ * interior cell in (k, j, i) order with a NaN in rho, rhoU, rhoE, pres,
+ * rhoV (dim >= 2), rhoW (dim >= 3), tested in that order. */
+int sifvo_check_nan(ctx_t* m, int* field, long long* cell) {
+    *field = -1;
+    *cell = -1;
+    for (int k = 0; k < m->nz; ++k)
+        for (int j = 0; j < m->ny; ++j)
+            for (int i = 0; i < m->nx; ++i) {
+                size_t idx = IDX(m, i, j, k);
+                int f = -1;
+                if (isnan(m->rho[idx])) f = SIFV_F_RHO;
+                else if (isnan(m->rhoU[idx])) f = SIFV_F_RHOU;
+                else if (isnan(m->rhoE[idx])) f = SIFV_F_RHOE;
+                else if (isnan(m->pres[idx])) f = SIFV_F_PRES;
+                else if (m->dim >= 2 && isnan(m->rhoV[idx])) f = SIFV_F_RHOV;
+                else if (m->dim >= 3 && isnan(m->rhoW[idx])) f = SIFV_F_RHOW;
+                if (f >= 0) {
+                    *field = f;
+                    *cell = (long long)i + (long long)m->nx * ((long long)j + (long long)m->ny * k);
+                    return SIFV_OK;
+                }
+            }
+    return SIFV_OK;
+}

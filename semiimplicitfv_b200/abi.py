@@ -136,6 +136,25 @@ class MeshSpec:
         return m
 
 
+class VtkFields(C.Structure):
+    _fields_ = [("pres", C.c_void_p), ("sigma", C.c_void_p), ("rhoE", C.c_void_p), ("vel", C.c_void_p * 3),
+                ("mom", C.c_void_p * 3), ("rho", C.c_void_p), ("alphaRho", C.c_void_p * MAX_PHASES),
+                ("alpha", C.c_void_p * MAX_PHASES)]
+
+
+class TimeLoop(C.Structure):
+    _fields_ = [("endTime", C.c_double), ("outputInterval", C.c_double), ("printInterval", C.c_int),
+                ("checkNaN", C.c_int), ("step0", C.c_int), ("batch", C.c_int)]
+
+
+class LoopResult(C.Structure):
+    _fields_ = [("time", C.c_double), ("steps", C.c_int), ("outputs", C.c_int), ("nanField", C.c_int),
+                ("nanCell", C.c_longlong), ("nanTime", C.c_double), ("nanStep", C.c_int)]
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_double, C.c_double)
+
+
 class AbiError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"status {status}: {msg}")
@@ -192,6 +211,18 @@ _OPTIONAL_SIGS = {
     "ensemble_run": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_double),
                                C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "ensemble_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "check_nan": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+    "vtk_open": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(Config), C.POINTER(Mesh), C.c_int,
+                           C.POINTER(C.c_void_p)]),
+    "vtk_write_host": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(VtkFields)]),
+    "vtk_write": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
+    "vtk_flush": (C.c_int, [C.c_void_p]),
+    "vtk_close": (C.c_int, [C.c_void_p]),
+    "vtk_last_error": (C.c_char_p, [C.c_void_p]),
+    "run_time_loop": (C.c_int, [C.c_void_p, C.POINTER(TimeLoop), C.c_void_p, PROGRESS_FN, C.c_void_p,
+                                C.POINTER(LoopResult)]),
+    "reference_time_loop": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_int,
+                                      C.POINTER(C.c_int)]),
 }
 
 
@@ -239,6 +270,57 @@ class Backend:
         if st != OK:
             raise AbiError(st, self.fn["ensemble_last_error"](None).decode())
         return Ensemble(self, h, cfg, list(n_cells))
+
+
+class VtkSession:
+    """VTKSession-compatible output (.pvd / .pvtr / .vtr) of one rank."""
+
+    def __init__(self, be: "Backend", directory: str, base: str, cfg: Config, mesh: MeshSpec, threads: int = 0):
+        if "vtk_open" not in be.fn:
+            raise AbiError(ERR_UNSUPPORTED, f"{be.name} has no VTK entry points")
+        self.be = be
+        self.h = C.c_void_p()
+        ms = mesh.cstruct()
+        st = be.fn["vtk_open"](directory.encode(), base.encode(), C.byref(cfg), C.byref(ms), threads, C.byref(self.h))
+        if st != OK:
+            raise AbiError(st, be.fn["vtk_last_error"](None).decode())
+
+    def _check(self, st: int):
+        if st != OK:
+            raise AbiError(st, self.be.fn["vtk_last_error"](self.h).decode())
+
+    def write_host(self, time: float, fields: dict):
+        """fields: SIFV_F_* id -> full (ghosted) float64 array."""
+        keep = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in fields.items()}
+        f = VtkFields()
+        ptr = lambda fid: keep[fid].ctypes.data if fid in keep else None
+        f.pres, f.sigma, f.rhoE, f.rho = ptr(F_PRES), ptr(F_SIGMA), ptr(F_RHOE), ptr(F_RHO)
+        for d, (v, m) in enumerate(((F_VELU, F_RHOU), (F_VELV, F_RHOV), (F_VELW, F_RHOW))):
+            f.vel[d], f.mom[d] = ptr(v), ptr(m)
+        for p in range(MAX_PHASES):
+            f.alphaRho[p], f.alpha[p] = ptr(F_ALPHARHO(p)), ptr(F_ALPHA(p))
+        self._check(self.be.fn["vtk_write_host"](self.h, time, C.byref(f)))
+
+    def write(self, ctx: "Context", time: float):
+        st = self.be.fn["vtk_write"](self.h, ctx.h, time)
+        if st != OK:
+            raise AbiError(st, self.be.error(ctx.h))
+
+    def flush(self):
+        self._check(self.be.fn["vtk_flush"](self.h))
+
+    def close(self):
+        if self.h:
+            h, self.h = self.h, None
+            st = self.be.fn["vtk_close"](h)
+            if st != OK:
+                raise AbiError(st, "VTK write failed")
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Ensemble:
@@ -350,6 +432,33 @@ class Context:
         dt = C.c_double()
         self._check(self.be.fn["step"](self.h, step, time, target_dt, C.byref(dt)))
         return dt.value
+
+    def check_nan(self):
+        """(SIFV_F_* id, interior cell) of the first NaN, or (-1, -1)."""
+        f, c = C.c_int(), C.c_longlong()
+        self._check(self.be.fn["check_nan"](self.h, C.byref(f), C.byref(c)))
+        return f.value, c.value
+
+    def run_time_loop(self, end_time: float, output_interval: float, vtk: Optional[VtkSession] = None,
+                      print_interval: int = 1, check_nan: bool = True, step0: int = 0, batch: int = 0,
+                      progress=None):
+        """runTimeLoop on this context; returns (status, LoopResult).
+        progress(step, time, dt) is called at the printed steps."""
+        p = TimeLoop(end_time, output_interval, print_interval, int(check_nan), step0, batch)
+        r = LoopResult()
+        cb = PROGRESS_FN(lambda _u, s, t, dt: progress(s, t, dt)) if progress else PROGRESS_FN()
+        st = self.be.fn["run_time_loop"](self.h, C.byref(p), vtk.h if vtk else None, cb, None, C.byref(r))
+        if st < 0 and st != ERR_NAN:
+            raise AbiError(st, self.be.error(self.h))
+        return st, r
+
+    def reference_time_loop(self, directory: str, base: str, end_time: float, output_interval: float,
+                            print_interval: int = 1) -> int:
+        """The reference's own runTimeLoop + VTKSession (reference backend only)."""
+        n = C.c_int()
+        self._check(self.be.fn["reference_time_loop"](self.h, directory.encode(), base.encode(), end_time,
+                                                      output_interval, print_interval, C.byref(n)))
+        return n.value
 
     def advance(self, step0: int, time0: float, t_end: float, n_steps: int):
         t, n = C.c_double(), C.c_int()

@@ -18,9 +18,10 @@ LIB = os.path.join(PKG, "libsifv_b200.so")
 # FMA contraction; the fused sweep path (sifv_fast.cu) with it.
 SOURCES = [("sifv_capi.cu", ["--fmad=false"]), ("sifv_noalloc.cu", ["--fmad=false"]),
            ("sifv_fast.cu", ["--fmad=true"]), ("sifv_ensemble.cu", ["--fmad=false"]),
-           ("sifv_ensemble_mixed.cu", ["--fmad=true", "--use_fast_math"]), ("sifv_adjoint.cu", ["--fmad=true"])]
+           ("sifv_ensemble_mixed.cu", ["--fmad=true", "--use_fast_math"]), ("sifv_adjoint.cu", ["--fmad=true"]),
+           ("sifv_vtk.cpp", [])]
 HEADERS = ["sifv_device.cuh", "sifv_common.cuh", "sifv_kernels.cuh", "sifv_sweep.cuh", "sifv_sweep_api.h",
-           "sifv_ensemble.cuh", "sifv_ensemble_api.h", "sifv_adjoint.cuh", "sifv_adjoint_api.h", "sifv_dual.cuh", "sifv_tile2d.cuh", "sifv_fastmath.cuh"]
+           "sifv_ensemble.cuh", "sifv_ensemble_api.h", "sifv_adjoint.cuh", "sifv_adjoint_api.h", "sifv_dual.cuh", "sifv_tile2d.cuh", "sifv_fastmath.cuh", "sifv_vtk_api.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -54,7 +55,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
     cmds, objs = [], []
     for src, extra in SOURCES:
-        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         objs.append(obj)
         cmds.append([_nvcc(), *NVCC_FLAGS, *extra, *inc, "-c", os.path.join(CSRC, src), "-o", obj])
     with cf.ThreadPoolExecutor(len(cmds)) as ex:

@@ -5,9 +5,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -15,6 +18,7 @@
 #include "sifv_adjoint_api.h"
 #include "sifv_kernels.cuh"
 #include "sifv_sweep_api.h"
+#include "sifv_vtk_api.h"
 
 using namespace sifv;
 
@@ -81,6 +85,8 @@ struct sifv_ctx {
     double* tan0[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* tanW[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double* tanF[3][5] = {};
+    double* loopLog = nullptr;                // per-step dt of a device-resident time-loop batch
+    int loopLogCap = 0;
 };
 
 namespace {
@@ -485,7 +491,7 @@ void body_force(const sifv_config_t& c, double time, StageCoef& K) {
 }
 
 // dt reduction + finalisation on the device.
-void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
+void enqueue_dt(sifv_ctx* c, double targetDt, int useEnd) {
     const sifv_config_t& cfg = c->cfg;
     unsigned g = blocks((long long)c->nint, kCellThreads);
     if (cfg.semiImplicit) {
@@ -499,7 +505,7 @@ void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
             k_dt_capillary<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.siCfl);
             c->launches++;
         }
-        k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, -1.0, targetDt, 1, cfg.siMinDt, cfg.siMaxDt, useEnd ? 1 : 0);
+        k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, -1.0, targetDt, 1, cfg.siMinDt, cfg.siMaxDt, useEnd);
         c->launches += 3;
     } else if (c->forcedDt > 0) {
         k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, c->forcedDt, -1.0, 0, 0.0, 0.0, 0);
@@ -518,7 +524,7 @@ void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
             }
             c->launches += 2;
         }
-        k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, cfg.constDt, targetDt, 0, 0.0, 0.0, useEnd ? 1 : 0);
+        k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, cfg.constDt, targetDt, 0, 0.0, 0.0, useEnd);
         c->launches += 1;
     }
     mark(c, "dt");
@@ -526,7 +532,7 @@ void enqueue_dt(sifv_ctx* c, double targetDt, bool useEnd) {
 
 // One step, everything enqueued on the stream; semi-implicit steps
 // synchronise once per Jacobi batch.
-int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, bool useEnd, int& status) {
+int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd, int& status) {
     const sifv_config_t& cfg = c->cfg;
     const Params& P = c->P;
     status = SIFV_OK;
@@ -920,6 +926,7 @@ int sifv_destroy(sifv_ctx_t* c) {
     if (c->ownStream) cudaStreamDestroy(c->ownStream);
     for (double* p : c->adjCkpt) cudaFree(p);
     if (c->adjStage) cudaFree(c->adjStage);
+    if (c->loopLog) cudaFree(c->loopLog);
     delete c;
     return SIFV_OK;
 }
@@ -1563,3 +1570,300 @@ int sifv_tangent_forward(sifv_ctx_t* c, int step0, double time0, double tEnd, in
 
 }  // extern "C"
 
+
+// ===========================================================================
+// Output path: NaN check, VTK snapshots from the device, runTimeLoop
+// ===========================================================================
+namespace {
+
+// Device staging of one VTK session: two slots, each a device copy of the
+// written fields (taken on the context's stream) and its pinned host copy
+// (brought over on the session's copy stream).
+struct VtkStage {
+    int device = -1;
+    size_t n = 0;
+    int nf = 0;
+    double* dev[2] = {nullptr, nullptr};
+    double* host[2] = {nullptr, nullptr};
+    cudaStream_t copy = nullptr;
+    cudaEvent_t staged[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+    bool busy[2] = {false, false};
+    std::mutex mu;
+};
+
+void release_stage(void* p) {
+    auto* s = static_cast<VtkStage*>(p);
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->copy) cudaStreamSynchronize(s->copy);
+    for (int q = 0; q < 2; ++q) {
+        if (s->dev[q]) cudaFree(s->dev[q]);
+        if (s->host[q]) cudaFreeHost(s->host[q]);
+        if (s->staged[q]) cudaEventDestroy(s->staged[q]);
+        if (s->copied[q]) cudaEventDestroy(s->copied[q]);
+    }
+    if (s->copy) cudaStreamDestroy(s->copy);
+    delete s;
+}
+
+// The context's fields a snapshot writes, in a fixed order (pointers into
+// `fields` are filled from the same order by vtk_fields_at).
+std::vector<int> vtk_field_ids(const sifv::VtkLayout& L) {
+    std::vector<int> ids = {SIFV_F_PRES};
+    if (L.useIGR) ids.push_back(SIFV_F_SIGMA);
+    ids.push_back(SIFV_F_RHOE);
+    const int vel[3] = {SIFV_F_VELU, SIFV_F_VELV, SIFV_F_VELW}, mom[3] = {SIFV_F_RHOU, SIFV_F_RHOV, SIFV_F_RHOW};
+    for (int d = 0; d < L.dim; ++d) ids.push_back(vel[d]);
+    for (int d = 0; d < L.dim; ++d) ids.push_back(mom[d]);
+    if (L.nPhases <= 0) ids.push_back(SIFV_F_RHO);
+    for (int p = 0; p < L.nPhases; ++p) ids.push_back(SIFV_F_ALPHARHO(p));
+    for (int p = 0; p < L.nPhases; ++p) ids.push_back(SIFV_F_ALPHA(p));
+    return ids;
+}
+
+sifv_vtk_fields_t vtk_fields_at(const std::vector<int>& ids, const double* base, size_t n) {
+    sifv_vtk_fields_t f{};
+    for (size_t q = 0; q < ids.size(); ++q) {
+        const double* a = base + q * n;
+        const int id = ids[q];
+        if (id == SIFV_F_PRES) f.pres = a;
+        else if (id == SIFV_F_SIGMA) f.sigma = a;
+        else if (id == SIFV_F_RHOE) f.rhoE = a;
+        else if (id >= SIFV_F_VELU && id <= SIFV_F_VELW) f.vel[id - SIFV_F_VELU] = a;
+        else if (id >= SIFV_F_RHOU && id <= SIFV_F_RHOW) f.mom[id - SIFV_F_RHOU] = a;
+        else if (id == SIFV_F_RHO) f.rho = a;
+        else if (id >= 16 && id < 32) f.alphaRho[id - 16] = a;
+        else if (id >= 32) f.alpha[id - 32] = a;
+    }
+    return f;
+}
+
+int nan_scan(sifv_ctx* c, int& field, long long& cell) {
+    field = -1;
+    cell = -1;
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->nanCode, 0xff, sizeof(unsigned long long), c->stream));
+    k_nan_scan<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl);
+    LAUNCH_CHECK(c);
+    unsigned long long code = 0;
+    CUDA_TRY(c, cudaMemcpyAsync(&c->ctlHost->nanCode, &c->ctl->nanCode, sizeof(code), cudaMemcpyDeviceToHost,
+                                c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    code = c->ctlHost->nanCode;
+    if (code == ~0ull) return SIFV_OK;
+    static const int order[6] = {SIFV_F_RHO, SIFV_F_RHOU, SIFV_F_RHOE, SIFV_F_PRES, SIFV_F_RHOV, SIFV_F_RHOW};
+    field = order[code & 7ull];
+    cell = (long long)(code >> 3);
+    return SIFV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sifv_check_nan(sifv_ctx_t* c, int* field, long long* cell) {
+    if (!c || !field || !cell) return fail(c, SIFV_ERR_BAD_ARG, "null argument");
+    cudaSetDevice(c->device);
+    return nan_scan(c, *field, *cell);
+}
+
+int sifv_vtk_write(sifv_vtk_t* v, sifv_ctx_t* c, double time) {
+    if (!v || !c) return fail(c, SIFV_ERR_BAD_ARG, "null argument");
+    const sifv::VtkLayout& L = sifv::vtk_layout(v);
+    const int ny = c->P.dim >= 2 ? c->P.ny : 1, nz = c->P.dim >= 3 ? c->P.nz : 1;
+    if (L.dim != c->P.dim || L.nx != c->P.nx || L.ny != ny || L.nz != nz || L.ngx != c->P.ngx ||
+        L.ngy != c->P.ngy || L.ngz != c->P.ngz || L.nPhases != c->cfg.nPhases || L.useIGR != (c->cfg.useIGR ? 1 : 0))
+        return fail(c, SIFV_ERR_BAD_ARG, "the VTK session was opened for another mesh or configuration");
+    cudaSetDevice(c->device);
+    auto* S = static_cast<VtkStage*>(sifv::vtk_stage(v));
+    const std::vector<int> ids = vtk_field_ids(L);
+    if (!S) {
+        S = new VtkStage();
+        S->device = c->device;
+        S->n = c->ncells;
+        S->nf = (int)ids.size();
+        if (cudaStreamCreateWithFlags(&S->copy, cudaStreamNonBlocking) != cudaSuccess) {
+            delete S;
+            return fail(c, SIFV_ERR_CUDA, "cannot create the VTK copy stream");
+        }
+        sifv::vtk_set_stage(v, S, release_stage);
+    }
+    if (S->device != c->device || S->n != c->ncells)
+        return fail(c, SIFV_ERR_BAD_ARG, "the VTK session stages another context's device");
+    int slot = -1;
+    for (int attempt = 0; attempt < 2 && slot < 0; ++attempt) {
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            for (int q = 0; q < 2 && slot < 0; ++q)
+                if (!S->busy[q]) slot = q;
+            if (slot >= 0) S->busy[slot] = true;
+        }
+        if (slot < 0) sifv_vtk_flush(v);   // both slots in flight: wait for the writer
+    }
+    if (slot < 0) return fail(c, SIFV_ERR_CUDA, "no VTK staging slot");
+    const size_t bytes = S->n * sizeof(double);
+    if (!S->dev[slot]) {
+        if (cudaMalloc(&S->dev[slot], bytes * S->nf) != cudaSuccess ||
+            cudaHostAlloc(&S->host[slot], bytes * S->nf, cudaHostAllocDefault) != cudaSuccess ||
+            cudaEventCreateWithFlags(&S->staged[slot], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&S->copied[slot], cudaEventDisableTiming) != cudaSuccess) {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->busy[slot] = false;
+            return fail(c, SIFV_ERR_CUDA, "cannot allocate the VTK staging slot");
+        }
+    }
+    for (int q = 0; q < S->nf; ++q)
+        CUDA_TRY(c, cudaMemcpyAsync(S->dev[slot] + q * S->n, field_ptr(c, ids[q]), bytes, cudaMemcpyDeviceToDevice,
+                                    c->stream));
+    CUDA_TRY(c, cudaEventRecord(S->staged[slot], c->stream));
+    CUDA_TRY(c, cudaStreamWaitEvent(S->copy, S->staged[slot], 0));
+    CUDA_TRY(c, cudaMemcpyAsync(S->host[slot], S->dev[slot], bytes * S->nf, cudaMemcpyDeviceToHost, S->copy));
+    CUDA_TRY(c, cudaEventRecord(S->copied[slot], S->copy));
+    const int n = sifv::vtk_next_file(v);
+    const size_t cells = S->n;
+    sifv::vtk_enqueue(v, [v, S, slot, n, time, ids, cells](std::string& e) -> int {
+        cudaSetDevice(S->device);
+        int st = SIFV_OK;
+        if (cudaEventSynchronize(S->copied[slot]) != cudaSuccess) {
+            e = "VTK snapshot copy failed";
+            st = SIFV_ERR_CUDA;
+        } else {
+            sifv_vtk_fields_t f = vtk_fields_at(ids, S->host[slot], cells);
+            st = sifv::vtk_write_snapshot(v, n, time, &f, e);
+        }
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->busy[slot] = false;
+        return st;
+    });
+    return SIFV_OK;
+}
+
+int sifv_run_time_loop(sifv_ctx_t* c, const sifv_time_loop_t* prm, sifv_vtk_t* vtk, sifv_progress_fn progress,
+                       void* user, sifv_loop_result_t* res) {
+    if (!c || !prm) return fail(c, SIFV_ERR_BAD_ARG, "null argument");
+    if (!(prm->outputInterval > 0.0)) return fail(c, SIFV_ERR_BAD_ARG, "outputInterval must be > 0");
+    if (!(prm->endTime < INFINITY)) return fail(c, SIFV_ERR_BAD_ARG, "endTime must be finite");
+    sifv_loop_result_t r{};
+    r.nanField = -1;
+    r.nanCell = -1;
+    const double endTime = prm->endTime, every = prm->outputInterval;
+    const int printEvery = prm->printInterval > 0 ? prm->printInterval : 1;
+    cudaSetDevice(c->device);
+    c->launches = 0;
+    int st = SIFV_OK;
+    double time = 0.0;
+    int step = prm->step0;
+    double nextOutput = every;
+    // one output: the snapshot, then the NaN check (src/RKTimeStepping.cpp:275-311)
+    auto output = [&](double t) -> int {
+        r.outputs++;
+        if (vtk) {
+            int s = sifv_vtk_write(vtk, c, t);
+            if (s != SIFV_OK) return s;
+        }
+        if (prm->checkNaN) {
+            int f;
+            long long cell;
+            int s = nan_scan(c, f, cell);
+            if (s != SIFV_OK) return s;
+            if (f >= 0) {
+                r.nanField = f;
+                r.nanCell = cell;
+                r.nanTime = t;
+                r.nanStep = step;
+                return fail(c, SIFV_ERR_NAN, "NaN detected at an output step");
+            }
+        }
+        return SIFV_OK;
+    };
+    auto finish = [&](int s) -> int {
+        r.time = time;
+        r.steps = step;
+        if (res) *res = r;
+        if (vtk) {
+            int f = sifv_vtk_flush(vtk);
+            if (s == SIFV_OK && f != SIFV_OK) s = fail(c, f, sifv_vtk_last_error(vtk));
+        }
+        return s;
+    };
+    if (vtk) {
+        st = sifv_vtk_write(vtk, c, 0.0);
+        if (st != SIFV_OK) return finish(st);
+    }
+    r.outputs = 1;
+    const bool resident = !c->cfg.semiImplicit && !c->cfg.useIGR && !has_body_force(c->cfg);
+    if (!resident) {
+        while (time < endTime) {
+            double targetDt = endTime - time;
+            if (nextOutput < endTime) targetDt = std::min(targetDt, nextOutput - time);
+            double dt = 0.0;
+            st = sifv_step(c, step, time, targetDt, &dt);
+            if (st < 0) return finish(st);
+            time += dt;
+            step++;
+            if (time >= nextOutput - 1e-12 * every) {
+                nextOutput += every;
+                st = output(time);
+                if (st != SIFV_OK) return finish(st);
+            }
+            if (progress && (step % printEvery == 0 || step == 1)) progress(user, step, time, dt);
+        }
+        return finish(SIFV_OK);
+    }
+    const int batchMax = prm->batch > 0 ? prm->batch : 64;
+    if (c->loopLogCap < batchMax) {
+        if (c->loopLog) cudaFree(c->loopLog);
+        c->loopLog = nullptr;
+        c->loopLogCap = 0;
+        CUDA_TRY(c, cudaMalloc(&c->loopLog, sizeof(double) * batchMax));
+        c->loopLogCap = batchMax;
+    }
+    std::vector<double> log(batchMax);
+    Ctl h{};
+    h.time = 0.0;
+    h.tEnd = endTime;
+    h.nextOutput = nextOutput;
+    h.outInterval = every;
+    CUDA_TRY(c, cudaMemcpyAsync(c->ctl, &h, offsetof(Ctl, res), cudaMemcpyHostToDevice, c->stream));
+    int perOutput = 0, sinceOutput = 0;   // steps of the last full output interval / of the current one
+    while (time < endTime) {
+        int B = batchMax;
+        if (perOutput > 0) B = std::max(1, std::min(batchMax, perOutput - sinceOutput + 1));
+        int status = SIFV_OK;
+        for (int q = 0; q < B; ++q) {
+            st = enqueue_step(c, step + q, 0.0, -1.0, 2, status);
+            if (st != SIFV_OK) return finish(st);
+            k_time_advance<<<1, 1, 0, c->stream>>>(c->ctl, c->loopLog, q);
+            c->launches++;
+        }
+        LAUNCH_CHECK(c);
+        CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, offsetof(Ctl, res), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaMemcpyAsync(log.data(), c->loopLog, sizeof(double) * B, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        const bool due = c->ctlHost->outputDue != 0;
+        int ran = 0;
+        while (ran < B && log[ran] >= 0.0) ++ran;
+        for (int q = 0; q < ran; ++q) {   // the host's copy of the device's time arithmetic
+            time += log[q];
+            step++;
+            sinceOutput++;
+            if (due && q == ran - 1) {
+                nextOutput += every;
+                perOutput = sinceOutput;
+                sinceOutput = 0;
+                st = output(time);
+                if (st != SIFV_OK) return finish(st);
+            }
+            if (progress && (step % printEvery == 0 || step == 1)) progress(user, step, time, log[q]);
+        }
+        if (time != c->ctlHost->time) return finish(fail(c, SIFV_ERR_CUDA, "device and host time disagree"));
+        if (due) {
+            k_loop_resume<<<1, 1, 0, c->stream>>>(c->ctl);
+            c->launches++;
+        }
+        if (ran == 0 && !due) break;   // nothing left to run (t >= endTime on the device)
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return finish(SIFV_OK);
+}
+
+}  // extern "C"

@@ -94,6 +94,13 @@ struct Ctl {
     int jacobiDone;              // iterations taken when converged, else 0
     int stepsTaken;
     int errFlag;
+    // device-resident time loop (runTimeLoop): next output time, interval,
+    // and the flag set by the step that reaches an output
+    double nextOutput;
+    double outInterval;
+    int outputDue;
+    int pad0;
+    unsigned long long nanCode;  // NaN scan: min over (interior cell * 8 + field order)
     unsigned long long res[1];   // per-iteration max residual bits (sized at allocation)
 };
 

@@ -666,17 +666,20 @@ __global__ void k_dt_init(Ctl* ctl, double maxDt) {
 
 // dt = min(maxDt, reduction); constDt; min with targetDt; semi-implicit
 // clamp (src/ExplicitSolver.cpp:72-90, src/SemiImplicitSolver.cpp:110-123).
-// useEnd: device-resident loop, targetDt = tEnd - time and steps past tEnd
-// are skipped.
+// useEnd 1: device-resident loop, targetDt = tEnd - time and steps past tEnd
+// are skipped.  useEnd 2: runTimeLoop (src/RKTimeStepping.cpp:259-266):
+// targetDt also capped at the next output time, and steps after the one
+// that reached an output are skipped until the host has handled it.
 __global__ void k_dt_finalize(Ctl* ctl, double constDt, double targetDt, int clampSemi, double minDt, double maxDt,
                               int useEnd) {
     if (useEnd) {
-        if (!(ctl->time < ctl->tEnd)) {
+        if (ctl->outputDue || !(ctl->time < ctl->tEnd)) {
             ctl->skip = 1;
             return;
         }
         ctl->skip = 0;
         targetDt = ctl->tEnd - ctl->time;
+        if (useEnd == 2 && ctl->nextOutput < ctl->tEnd) targetDt = smin(targetDt, ctl->nextOutput - ctl->time);
     }
     double dt = (constDt > 0) ? constDt : bits2d(ctl->dtBits);
     if (targetDt > 0) dt = smin(dt, targetDt);
@@ -684,10 +687,48 @@ __global__ void k_dt_finalize(Ctl* ctl, double constDt, double targetDt, int cla
     ctl->dt = dt;
 }
 
-__global__ void k_time_advance(Ctl* ctl) {
-    if (ctl->skip) return;
+// time += dt (src/RKTimeStepping.cpp:272-273); with an output interval, the
+// output test of runTimeLoop (275-277).  dtLog[slot]: the step's dt, or -1
+// for a skipped step.
+__global__ void k_time_advance(Ctl* ctl, double* dtLog = nullptr, int slot = 0) {
+    if (ctl->skip) {
+        if (dtLog) dtLog[slot] = -1.0;
+        return;
+    }
     ctl->time += ctl->dt;
     ctl->stepsTaken += 1;
+    if (dtLog) dtLog[slot] = ctl->dt;
+    if (ctl->outInterval > 0.0 && ctl->time >= ctl->nextOutput - 1e-12 * ctl->outInterval) {
+        ctl->outputDue = 1;
+        ctl->nextOutput += ctl->outInterval;
+    }
+}
+
+// The host has written the output: steps run again.
+__global__ void k_loop_resume(Ctl* ctl) {
+    ctl->outputDue = 0;
+    ctl->skip = 0;
+}
+
+// runTimeLoop's NaN check (src/RKTimeStepping.cpp:280-292): the first
+// interior cell in (k, j, i) order with a NaN in rho, rhoU, rhoE, pres, rhoV,
+// rhoW (that order within the cell), as min(cell * 8 + field order).
+__global__ void __launch_bounds__(256) k_nan_scan(Params P, Fields F, Ctl* ctl) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(P, t, i, j, k)) return;
+    const size_t c = cidx(P, i, j, k);
+    int f = -1;
+    if (isnan(F.rho[c])) f = 0;
+    else if (isnan(F.rhoU[c])) f = 1;
+    else if (isnan(F.rhoE[c])) f = 2;
+    else if (isnan(F.pres[c])) f = 3;
+    else if (P.dim >= 2 && isnan(F.rhoV[c])) f = 4;
+    else if (P.dim >= 3 && isnan(F.rhoW[c])) f = 5;
+    if (f < 0) return;
+    const unsigned long long lin =
+        (unsigned long long)i + (unsigned long long)P.nx * ((unsigned long long)j + (unsigned long long)P.ny * k);
+    atomicMin(&ctl->nanCode, lin * 8ull + (unsigned long long)f);
 }
 
 // ---------------------------------------------------------------------------

@@ -356,9 +356,14 @@ def run_steps(ctx, nsteps, t_end=None, step0=0, time0=0.0):
     return t, s, dts
 
 
-def run_time_loop(ctx, t_end, output_interval):
-    """runTimeLoop's dt sequence (src/RKTimeStepping.cpp:241-275): targetDt is
-    clamped to the next output time; config.step increments per step."""
+def run_time_loop(ctx, t_end, output_interval, on_output=None, print_interval=None, on_print=None):
+    """runTimeLoop (src/RKTimeStepping.cpp:241-356): output at t = 0 and when
+    t >= nextOutput - 1e-12 outputInterval, targetDt clamped to the next
+    output time, config.step incremented per step; on_output(time, step)
+    at each output, on_print(step, time, dt) at step 1 and every
+    print_interval-th step."""
+    if on_output:
+        on_output(0.0, 0)
     time, step = 0.0, 0
     next_out = output_interval
     while time < t_end:
@@ -369,5 +374,25 @@ def run_time_loop(ctx, t_end, output_interval):
         time += dt
         step += 1
         if time >= next_out - 1e-12 * output_interval:
+            if on_output:
+                on_output(time, step)
             next_out += output_interval
+        if on_print and (step % print_interval == 0 or step == 1):
+            on_print(step, time, dt)
     return time, step
+
+
+def output_fields(ctx, cfg):
+    """The fields a VTK snapshot of ``ctx`` reads, as SIFV_F_* -> array."""
+    ids = [abi.F_PRES, abi.F_RHOE, abi.F_VELU, abi.F_RHOU]
+    if cfg.useIGR:
+        ids.append(abi.F_SIGMA)
+    if cfg.dim >= 2:
+        ids += [abi.F_VELV, abi.F_RHOV]
+    if cfg.dim >= 3:
+        ids += [abi.F_VELW, abi.F_RHOW]
+    if cfg.nPhases == 0:
+        ids.append(abi.F_RHO)
+    for p in range(cfg.nPhases):
+        ids += [abi.F_ALPHARHO(p), abi.F_ALPHA(p)]
+    return {fid: ctx.get_field(fid) for fid in ids}
