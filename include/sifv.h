@@ -256,6 +256,50 @@ int sifv_last_step_stats(const sifv_ctx_t* ctx, double* deviceMs, int* launches)
 #define SIFV_PRESSURE_GAUSS_SEIDEL 1
 int sifv_set_pressure_solver(sifv_ctx_t* ctx, int kind);
 
+/* ---- immersed boundaries ---------------------------------------------------- */
+/* ImmersedBoundaryMethod (include/ImmersedBoundary.hpp, src/ImmersedBoundary.cpp)
+ * on the explicit step: classifyCells at set-up (cells inside a body are
+ * dead, dead cells with a fluid face neighbour are ghost cells; each ghost
+ * cell gets the mirror image point of its centroid through the body surface
+ * and a bi/trilinear stencil of fluid cells), then per stage and after the
+ * step applyGhostCells (interpolated state, velocity reflected: reversed for
+ * no-slip, normal component mirrored for slip), solid cells skipped in the
+ * update, the dt limits and the IGR sweeps (with the scalar ghost fill of
+ * sigma after each sweep).  Explicit SIFV_PREC_FP64 steps only, as in the
+ * reference (the semi-implicit solver has no immersed boundary). */
+#define SIFV_IB_CIRCLE     0   /* IBCircle(p = cx, cy, r) */
+#define SIFV_IB_RECTANGLE  1   /* IBRectangle(p = cx, cy, hw, hh) */
+#define SIFV_IB_CYLINDER   2   /* IBCylinder(p = c0, c1, r; axis) */
+#define SIFV_IB_PRISM      3   /* IBRectangularPrism(p = cx, cy, cz, hw, hh, hd) */
+#define SIFV_IB_NOSLIP     0   /* IBBody::WallType::NoSlip (the default) */
+#define SIFV_IB_SLIP       1
+#define SIFV_CELL_FLUID    0   /* CellType */
+#define SIFV_CELL_GHOST    1
+#define SIFV_CELL_DEAD     2
+typedef struct sifv_ib_body {
+    int shape;        /* SIFV_IB_CIRCLE .. SIFV_IB_PRISM */
+    int wall;         /* SIFV_IB_NOSLIP / SIFV_IB_SLIP */
+    int axis;         /* cylinder axis (0 x, 1 y, 2 z) */
+    double p[6];
+} sifv_ib_body_t;
+/* Bodies of any shape, through the three queries of IBBody (signed
+ * distance, negative inside; closest surface point; outward normal there),
+ * called on the host during set-up only. */
+typedef struct sifv_ib_shapes {
+    void* user;
+    double (*signedDistance)(void* user, int body, double x, double y, double z);
+    void (*closestPoint)(void* user, int body, double x, double y, double z, double out[3]);
+    void (*outwardNormal)(void* user, int body, double x, double y, double z, double out[3]);
+} sifv_ib_shapes_t;
+/* addBody for each body + classifyCells; nBodies = 0 removes the boundary. */
+int sifv_set_immersed_bodies(sifv_ctx_t* ctx, const sifv_ib_body_t* bodies, int nBodies);
+int sifv_set_immersed_shapes(sifv_ctx_t* ctx, int nBodies, const int* wall, const sifv_ib_shapes_t* shapes);
+/* CellType of every cell (totalCells bytes, SIFV_CELL_*; cells outside the
+ * interior are fluid). */
+int sifv_ib_cell_types(sifv_ctx_t* ctx, unsigned char* types);
+/* applyGhostCells on the context's current primitive state. */
+int sifv_apply_ib_ghost_cells(sifv_ctx_t* ctx);
+
 /* ---- output path: NaN check, VTK, time loop ------------------------------- */
 /* runTimeLoop's NaN check (src/RKTimeStepping.cpp:280-311) on the device:
  * the first interior cell in (k, j, i) order holding a NaN in rho, rhoU,

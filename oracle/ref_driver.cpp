@@ -30,6 +30,7 @@
 #include "SimulationConfig.hpp"
 #include "SolutionState.hpp"
 #include "StiffenedGasEOS.hpp"
+#include "ImmersedBoundary.hpp"
 #include "Runtime.hpp"
 #include "VTKSession.hpp"
 
@@ -57,6 +58,7 @@ struct sifvr_ctx {
     std::unique_ptr<SemiImplicitSolver> semi;
     std::string err;
     int lastIters = 0;
+    std::unique_ptr<ImmersedBoundaryMethod> ibm;
 };
 
 static thread_local std::string g_err;
@@ -356,6 +358,49 @@ int sifvr_reference_time_loop(sifvr_ctx* ctx, const char* dir, const char* base,
         ctx->err = e.what();
         return SIFV_ERR_BAD_ARG;
     }
+}
+
+// ImmersedBoundaryMethod with the reference's own body classes, attached to
+// the explicit solver as Runtime::attachIBM does (src/Runtime.cpp:143-146).
+int sifvr_set_immersed_bodies(sifvr_ctx* ctx, const sifv_ib_body_t* b, int n) {
+    try {
+        if (n > 0 && !ctx->expl) {
+            ctx->err = "the semi-implicit step has no immersed boundary";
+            return SIFV_ERR_UNSUPPORTED;
+        }
+        if (ctx->expl) ctx->expl->setIBM(nullptr);
+        ctx->ibm.reset();
+        if (n == 0) return SIFV_OK;
+        ctx->ibm = std::make_unique<ImmersedBoundaryMethod>();
+        for (int q = 0; q < n; ++q) {
+            const double* p = b[q].p;
+            std::shared_ptr<IBBody> body;
+            if (b[q].shape == SIFV_IB_CIRCLE) body = std::make_shared<IBCircle>(p[0], p[1], p[2]);
+            else if (b[q].shape == SIFV_IB_RECTANGLE) body = std::make_shared<IBRectangle>(p[0], p[1], p[2], p[3]);
+            else if (b[q].shape == SIFV_IB_CYLINDER) body = std::make_shared<IBCylinder>(p[0], p[1], p[2], b[q].axis);
+            else body = std::make_shared<IBRectangularPrism>(p[0], p[1], p[2], p[3], p[4], p[5]);
+            body->setWallType(b[q].wall == SIFV_IB_SLIP ? IBBody::WallType::Slip : IBBody::WallType::NoSlip);
+            ctx->ibm->addBody(body);
+        }
+        ctx->ibm->classifyCells(*ctx->mesh);
+        ctx->expl->setIBM(ctx->ibm.get());
+        return SIFV_OK;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return SIFV_ERR_BAD_ARG;
+    }
+}
+
+int sifvr_ib_cell_types(sifvr_ctx* ctx, unsigned char* types) {
+    const std::size_t n = ctx->mesh->totalCells();
+    for (std::size_t q = 0; q < n; ++q)
+        types[q] = ctx->ibm ? static_cast<unsigned char>(ctx->ibm->cellType(q)) : 0;
+    return SIFV_OK;
+}
+
+int sifvr_apply_ib_ghost_cells(sifvr_ctx* ctx) {
+    if (ctx->ibm) ctx->ibm->applyGhostCells(*ctx->mesh, ctx->state, ctx->config.dim);
+    return SIFV_OK;
 }
 
 }  // extern "C"

@@ -65,8 +65,26 @@ typedef struct sifvo_ctx {
     int lastIters;
     int pressureSolverKind; /* 0 Jacobi, 1 Gauss-Seidel */
     double time;            /* SimulationConfig::time of the current step */
+    /* ImmersedBoundaryMethod (include/ImmersedBoundary.hpp:107-135) */
+    unsigned char* cellType; /* NULL: no immersed boundary */
+    struct IbGhost* ibGhost;
+    int ibCount;
+    sifv_ib_body_t* ibBodies;
+    int ibNBodies;
     char err[256];
 } ctx_t;
+
+/* GhostCellInfo (include/ImmersedBoundary.hpp:96-103) */
+typedef struct IbGhost {
+    size_t cell;
+    int body;
+    double normal[3];
+    int n;
+    size_t interp[8];
+    double w[8];
+} IbGhost;
+
+#define SOLID(m, idx) ((m)->cellType && (m)->cellType[idx] != SIFV_CELL_FLUID)
 
 static char g_err[256];
 
@@ -303,13 +321,14 @@ static void cons_to_prim(ctx_t* m) {
 
 /* ---- time steps ---- */
 /* computeAcousticTimeStep, src/RKTimeStepping.cpp:43-123 */
-static double acoustic_dt(const ctx_t* m, double cfl, double maxDt) {
+static double acoustic_dt(const ctx_t* m, double cfl, double maxDt, int skipSolid) {
     double dt = maxDt;
     double alphas[MAXPH], alphaRhos[MAXPH];
     for (int k = 0; k < m->nz; ++k)
         for (int j = 0; j < m->ny; ++j)
             for (int i = 0; i < m->nx; ++i) {
                 size_t idx = IDX(m, i, j, k);
+                if (skipSolid && SOLID(m, idx)) continue;
                 double c;
                 if (m->c.nPhases > 0) {
                     for (int ph = 0; ph < m->c.nPhases; ++ph) alphas[ph] = m->alpha[ph][idx];
@@ -768,6 +787,8 @@ static void scatter_face(ctx_t* m, const Flux* F, int hasL, size_t iL, double co
 
 static int has_viscosity(const sifv_config_t* c);
 static void add_viscous_fluxes(ctx_t* m);
+static void ib_apply_ghosts(ctx_t* m);
+static void ib_apply_scalar(ctx_t* m, double* f);
 static void add_surface_tension_fluxes(ctx_t* m);
 
 static void compute_rhs(ctx_t* m) {
@@ -1017,13 +1038,14 @@ static void add_viscous_fluxes(ctx_t* m) {
 }
 
 /* computeViscousDt, src/RKTimeStepping.cpp:161-188 */
-static double viscous_dt(const ctx_t* m, double mu, double cfl, double maxDt) {
+static double viscous_dt(const ctx_t* m, double mu, double cfl, double maxDt, int skipSolid) {
     double dt = maxDt;
     const int dim = m->dim;
     for (int k = 0; k < m->nz; ++k)
         for (int j = 0; j < m->ny; ++j)
             for (int i = 0; i < m->nx; ++i) {
                 size_t idx = IDX(m, i, j, k);
+                if (skipSolid && SOLID(m, idx)) continue;
                 double dxMin = DX(m, i);
                 if (dim >= 2) dxMin = smin(dxMin, DY(m, j));
                 if (dim >= 3) dxMin = smin(dxMin, DZ(m, k));
@@ -1135,13 +1157,14 @@ static void add_surface_tension_fluxes(ctx_t* m) {
 }
 
 /* computeCapillaryDt, src/RKTimeStepping.cpp:201-228 */
-static double capillary_dt(const ctx_t* m, double sigma, double cfl, double maxDt) {
+static double capillary_dt(const ctx_t* m, double sigma, double cfl, double maxDt, int skipSolid) {
     double dt = maxDt;
     const int dim = m->dim;
     for (int k = 0; k < m->nz; ++k)
         for (int j = 0; j < m->ny; ++j)
             for (int i = 0; i < m->nx; ++i) {
                 size_t idx = IDX(m, i, j, k);
+                if (skipSolid && SOLID(m, idx)) continue;
                 double dxMin = DX(m, i);
                 if (dim >= 2) dxMin = smin(dxMin, DY(m, j));
                 if (dim >= 3) dxMin = smin(dxMin, DZ(m, k));
@@ -1225,6 +1248,7 @@ static void igr_solve(ctx_t* m, int step) {
             for (int j = 0; j < m->ny; ++j)
                 for (int i = 0; i < m->nx; ++i) {
                     size_t idx = IDX(m, i, j, k);
+                    if (SOLID(m, idx)) continue;
                     double rhs = igr_rhs(m, m->gradU + 9 * idx, alpha);
                     double diag = 1.0 / m->rho[idx];
                     double offdiag = 0.0;
@@ -1254,6 +1278,7 @@ static void igr_solve(ctx_t* m, int step) {
                     m->sigma[idx] = (rhs + offdiag) / diag;
                 }
         fill_scalar_ghosts(m, m->sigma);
+        if (m->cellType) ib_apply_scalar(m, m->sigma);
     }
 }
 
@@ -1400,9 +1425,9 @@ static double explicit_step(ctx_t* m, int step, double targetDt) {
     if (c->constDt > 0) {
         dt = c->constDt;
     } else {
-        dt = acoustic_dt(m, c->cfl, c->maxDt);
-        if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->cfl, c->maxDt));
-        if (c->stSigma > 0.0) dt = smin(dt, capillary_dt(m, c->stSigma, c->cfl, c->maxDt));
+        dt = acoustic_dt(m, c->cfl, c->maxDt, 1);
+        if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->cfl, c->maxDt, 1));
+        if (c->stSigma > 0.0) dt = smin(dt, capillary_dt(m, c->stSigma, c->cfl, c->maxDt, 1));
     }
     if (targetDt > 0) dt = smin(dt, targetDt);
     double rk[3][4];
@@ -1411,6 +1436,7 @@ static double explicit_step(ctx_t* m, int step, double targetDt) {
     for (int s = 0; s < c->RKOrder; ++s) {
         cons_to_prim(m);
         apply_bc_prim(m);
+        if (m->cellType) ib_apply_ghosts(m);
         if (c->useIGR) {
             velocity_gradients(m);
             igr_solve(m, step);
@@ -1421,6 +1447,7 @@ static double explicit_step(ctx_t* m, int step, double targetDt) {
             for (int j = 0; j < m->ny; ++j)
                 for (int i = 0; i < m->nx; ++i) {
                     size_t idx = IDX(m, i, j, k);
+                    if (SOLID(m, idx)) continue;
                     if (s == 0 && c->RKOrder > 1) save_cell(m, idx);
                     if (c->RKOrder == 1) {
                         m->rho[idx] += dt * m->rhsRho[idx];
@@ -1450,6 +1477,7 @@ static double explicit_step(ctx_t* m, int step, double targetDt) {
     }
     cons_to_prim(m);
     apply_bc_prim(m);
+    if (m->cellType) ib_apply_ghosts(m);
     return dt;
 }
 
@@ -1579,8 +1607,8 @@ static void correction_step(ctx_t* m, double dt) {
 static double semi_step(ctx_t* m, int step, double targetDt) {
     const sifv_config_t* c = &m->c;
     double dt = advective_dt(m, c->siCfl, c->siMaxDt);
-    if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->siCfl, c->siMaxDt));
-    if (c->stSigma > 0.0) dt = smin(dt, capillary_dt(m, c->stSigma, c->siCfl, c->siMaxDt));
+    if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->siCfl, c->siMaxDt, 0));
+    if (c->stSigma > 0.0) dt = smin(dt, capillary_dt(m, c->stSigma, c->siCfl, c->siMaxDt, 0));
     if (targetDt > 0) dt = smin(dt, targetDt);
     dt = sclamp(dt, c->siMinDt, c->siMaxDt);
     double rk[3][4];
@@ -1756,6 +1784,7 @@ int sifvo_destroy(ctx_t* m) {
         free(m->alpha0[p]); free(m->rhsAlphaRho[p]); free(m->rhsAlpha[p]);
     }
     free(m->xL); free(m->xR); free(m->yL); free(m->yR); free(m->zL); free(m->zR);
+    free(m->cellType); free(m->ibGhost); free(m->ibBodies);
     free(m);
     return SIFV_OK;
 }
@@ -1833,7 +1862,7 @@ int sifvo_igr_solve(ctx_t* m, int step) {
 }
 
 int sifvo_acoustic_dt(ctx_t* m, double cfl, double maxDt, double* dt) {
-    *dt = acoustic_dt(m, cfl, maxDt);
+    *dt = acoustic_dt(m, cfl, maxDt, 0);
     return SIFV_OK;
 }
 
@@ -1875,5 +1904,358 @@ int sifvo_check_nan(ctx_t* m, int* field, long long* cell) {
                     return SIFV_OK;
                 }
             }
+    return SIFV_OK;
+}
+
+/* ---- immersed boundaries: src/ImmersedBoundary.cpp ---- */
+static inline double CX(const ctx_t* m, int i) { return 0.5 * (m->xExt[i + m->ngx] + m->xExt[i + m->ngx + 1]); }
+static inline double CY(const ctx_t* m, int j) { return 0.5 * (m->yExt[j + m->ngy] + m->yExt[j + m->ngy + 1]); }
+static inline double CZ(const ctx_t* m, int k) { return 0.5 * (m->zExt[k + m->ngz] + m->zExt[k + m->ngz + 1]); }
+static inline double sgn1(double v) { return (v >= 0) ? 1.0 : -1.0; }
+
+/* cross-section coordinates of a cylinder (src/ImmersedBoundary.cpp:84-96) */
+static void cyl_plane(const sifv_ib_body_t* b, double x, double y, double z, double* p0, double* p1) {
+    if (b->axis == 0) { *p0 = y; *p1 = z; }
+    else if (b->axis == 1) { *p0 = x; *p1 = z; }
+    else { *p0 = x; *p1 = y; }
+}
+
+/* IBCircle / IBRectangle / IBCylinder / IBRectangularPrism::signedDistance
+ * (src/ImmersedBoundary.cpp:11-16, 42-52, 84-96, 127-140) */
+static double ib_sdf(const sifv_ib_body_t* b, double x, double y, double z) {
+    const double* p = b->p;
+    switch (b->shape) {
+        case SIFV_IB_CIRCLE: {
+            double dx = x - p[0], dy = y - p[1];
+            return sqrt(dx * dx + dy * dy) - p[2];
+        }
+        case SIFV_IB_RECTANGLE: {
+            double qx = fabs(x - p[0]) - p[2], qy = fabs(y - p[1]) - p[3];
+            double out = sqrt(smax(qx, 0.0) * smax(qx, 0.0) + smax(qy, 0.0) * smax(qy, 0.0));
+            return out + smin(smax(qx, qy), 0.0);
+        }
+        case SIFV_IB_CYLINDER: {
+            double p0, p1;
+            cyl_plane(b, x, y, z, &p0, &p1);
+            double d0 = p0 - p[0], d1 = p1 - p[1];
+            return sqrt(d0 * d0 + d1 * d1) - p[2];
+        }
+        default: {
+            double qx = fabs(x - p[0]) - p[3], qy = fabs(y - p[1]) - p[4], qz = fabs(z - p[2]) - p[5];
+            double out = sqrt(smax(qx, 0.0) * smax(qx, 0.0) + smax(qy, 0.0) * smax(qy, 0.0) +
+                              smax(qz, 0.0) * smax(qz, 0.0));
+            return out + smin(smax(smax(qx, qy), qz), 0.0);
+        }
+    }
+}
+
+/* closestPoint (src/ImmersedBoundary.cpp:18-28, 54-70, 98-119, 142-165) */
+static void ib_closest(const sifv_ib_body_t* b, double x, double y, double z, double o[3]) {
+    const double* p = b->p;
+    switch (b->shape) {
+        case SIFV_IB_CIRCLE: {
+            double dx = x - p[0], dy = y - p[1];
+            double dist = sqrt(dx * dx + dy * dy);
+            if (dist < 1e-14) { o[0] = p[0] + p[2]; o[1] = p[1]; o[2] = 0.0; return; }
+            double s = p[2] / dist;
+            o[0] = p[0] + dx * s; o[1] = p[1] + dy * s; o[2] = 0.0;
+            return;
+        }
+        case SIFV_IB_RECTANGLE: {
+            double dx = x - p[0], dy = y - p[1];
+            double cxl = sclamp(dx, -p[2], p[2]), cyl = sclamp(dy, -p[3], p[3]);
+            if (fabs(dx) <= p[2] && fabs(dy) <= p[3]) {
+                double tx = p[2] - fabs(dx), ty = p[3] - fabs(dy);
+                if (tx < ty) cxl = (dx >= 0) ? p[2] : -p[2];
+                else cyl = (dy >= 0) ? p[3] : -p[3];
+            }
+            o[0] = p[0] + cxl; o[1] = p[1] + cyl; o[2] = 0.0;
+            return;
+        }
+        case SIFV_IB_CYLINDER: {
+            double p0, p1;
+            cyl_plane(b, x, y, z, &p0, &p1);
+            double d0 = p0 - p[0], d1 = p1 - p[1];
+            double dist = sqrt(d0 * d0 + d1 * d1);
+            double q0, q1;
+            if (dist < 1e-14) { q0 = p[0] + p[2]; q1 = p[1]; }
+            else { double s = p[2] / dist; q0 = p[0] + d0 * s; q1 = p[1] + d1 * s; }
+            if (b->axis == 0) { o[0] = x; o[1] = q0; o[2] = q1; }
+            else if (b->axis == 1) { o[0] = q0; o[1] = y; o[2] = q1; }
+            else { o[0] = q0; o[1] = q1; o[2] = z; }
+            return;
+        }
+        default: {
+            double dx = x - p[0], dy = y - p[1], dz = z - p[2];
+            double cxl = sclamp(dx, -p[3], p[3]), cyl = sclamp(dy, -p[4], p[4]), czl = sclamp(dz, -p[5], p[5]);
+            if (fabs(dx) <= p[3] && fabs(dy) <= p[4] && fabs(dz) <= p[5]) {
+                double tx = p[3] - fabs(dx), ty = p[4] - fabs(dy), tz = p[5] - fabs(dz);
+                if (tx <= ty && tx <= tz) cxl = (dx >= 0) ? p[3] : -p[3];
+                else if (ty <= tx && ty <= tz) cyl = (dy >= 0) ? p[4] : -p[4];
+                else czl = (dz >= 0) ? p[5] : -p[5];
+            }
+            o[0] = p[0] + cxl; o[1] = p[1] + cyl; o[2] = p[2] + czl;
+            return;
+        }
+    }
+}
+
+/* outwardNormal (src/ImmersedBoundary.cpp:30-40, 72-82, 121-140, 167-180) */
+static void ib_normal(const sifv_ib_body_t* b, double x, double y, double z, double o[3]) {
+    const double* p = b->p;
+    switch (b->shape) {
+        case SIFV_IB_CIRCLE: {
+            double dx = x - p[0], dy = y - p[1];
+            double dist = sqrt(dx * dx + dy * dy);
+            if (dist < 1e-14) { o[0] = 1.0; o[1] = 0.0; o[2] = 0.0; return; }
+            o[0] = dx / dist; o[1] = dy / dist; o[2] = 0.0;
+            return;
+        }
+        case SIFV_IB_RECTANGLE: {
+            double cp[3];
+            ib_closest(b, x, y, z, cp);
+            double dx = cp[0] - p[0], dy = cp[1] - p[1];
+            int onX = fabs(fabs(dx) - p[2]) < 1e-12, onY = fabs(fabs(dy) - p[3]) < 1e-12;
+            if (onX && !onY) { o[0] = sgn1(dx); o[1] = 0.0; o[2] = 0.0; }
+            else if (onY && !onX) { o[0] = 0.0; o[1] = sgn1(dy); o[2] = 0.0; }
+            else { double len = sqrt(2.0); o[0] = sgn1(dx) / len; o[1] = sgn1(dy) / len; o[2] = 0.0; }
+            return;
+        }
+        case SIFV_IB_CYLINDER: {
+            double p0, p1;
+            cyl_plane(b, x, y, z, &p0, &p1);
+            double d0 = p0 - p[0], d1 = p1 - p[1];
+            double dist = sqrt(d0 * d0 + d1 * d1);
+            double n0 = 1.0, n1 = 0.0;
+            if (!(dist < 1e-14)) { n0 = d0 / dist; n1 = d1 / dist; }
+            if (b->axis == 0) { o[0] = 0.0; o[1] = n0; o[2] = n1; }
+            else if (b->axis == 1) { o[0] = n0; o[1] = 0.0; o[2] = n1; }
+            else { o[0] = n0; o[1] = n1; o[2] = 0.0; }
+            return;
+        }
+        default: {
+            double cp[3];
+            ib_closest(b, x, y, z, cp);
+            double dx = cp[0] - p[0], dy = cp[1] - p[1], dz = cp[2] - p[2];
+            double nx = 0.0, ny = 0.0, nz = 0.0;
+            if (fabs(fabs(dx) - p[3]) < 1e-12) nx = sgn1(dx);
+            if (fabs(fabs(dy) - p[4]) < 1e-12) ny = sgn1(dy);
+            if (fabs(fabs(dz) - p[5]) < 1e-12) nz = sgn1(dz);
+            double len = sqrt(nx * nx + ny * ny + nz * nz);
+            if (len < 1e-14) { o[0] = 1.0; o[1] = 0.0; o[2] = 0.0; return; }
+            o[0] = nx / len; o[1] = ny / len; o[2] = nz / len;
+            return;
+        }
+    }
+}
+
+/* ImmersedBoundaryMethod::findCell (src/ImmersedBoundary.cpp:190-214) */
+static int ib_find_cell(const ctx_t* m, double coord, int dir) {
+    int n = (dir == 0) ? m->nx : (dir == 1) ? m->ny : m->nz;
+    if (n <= 1) return 0;
+    double (*cen)(const ctx_t*, int) = (dir == 0) ? CX : (dir == 1) ? CY : CZ;
+    if (coord <= cen(m, 0)) return 0;
+    if (coord >= cen(m, n - 1)) return (n - 2 > 0) ? n - 2 : 0;
+    for (int i = 0; i < n - 1; ++i)
+        if (coord >= cen(m, i) && coord < cen(m, i + 1)) return i;
+    return (n - 2 > 0) ? n - 2 : 0;
+}
+
+static double ib_t(double v, double c0, double c1) {
+    double d = c1 - c0;
+    return (d > 1e-14) ? sclamp((v - c0) / d, 0.0, 1.0) : 0.0;
+}
+
+/* ImmersedBoundaryMethod::buildInterpStencil (src/ImmersedBoundary.cpp:216-300) */
+static void ib_stencil(const ctx_t* m, double x, double y, double z, IbGhost* g) {
+    const int dim = m->dim;
+    int i0 = ib_find_cell(m, x, 0);
+    int j0 = (dim >= 2) ? ib_find_cell(m, y, 1) : 0;
+    int k0 = (dim >= 3) ? ib_find_cell(m, z, 2) : 0;
+    int i1 = (i0 + 1 < m->nx - 1) ? i0 + 1 : m->nx - 1;
+    double tx = ib_t(x, CX(m, i0), CX(m, i1));
+    if (dim == 1) {
+        g->n = 2;
+        g->interp[0] = IDX(m, i0, 0, 0); g->interp[1] = IDX(m, i1, 0, 0);
+        g->w[0] = 1.0 - tx; g->w[1] = tx;
+    } else {
+        int j1 = (j0 + 1 < m->ny - 1) ? j0 + 1 : m->ny - 1;
+        double ty = ib_t(y, CY(m, j0), CY(m, j1));
+        if (dim == 2) {
+            g->n = 4;
+            g->interp[0] = IDX(m, i0, j0, 0); g->interp[1] = IDX(m, i1, j0, 0);
+            g->interp[2] = IDX(m, i0, j1, 0); g->interp[3] = IDX(m, i1, j1, 0);
+            g->w[0] = (1.0 - tx) * (1.0 - ty); g->w[1] = tx * (1.0 - ty);
+            g->w[2] = (1.0 - tx) * ty; g->w[3] = tx * ty;
+        } else {
+            int k1 = (k0 + 1 < m->nz - 1) ? k0 + 1 : m->nz - 1;
+            double tz = ib_t(z, CZ(m, k0), CZ(m, k1));
+            g->n = 8;
+            g->interp[0] = IDX(m, i0, j0, k0); g->interp[1] = IDX(m, i1, j0, k0);
+            g->interp[2] = IDX(m, i0, j1, k0); g->interp[3] = IDX(m, i1, j1, k0);
+            g->interp[4] = IDX(m, i0, j0, k1); g->interp[5] = IDX(m, i1, j0, k1);
+            g->interp[6] = IDX(m, i0, j1, k1); g->interp[7] = IDX(m, i1, j1, k1);
+            g->w[0] = (1.0 - tx) * (1.0 - ty) * (1.0 - tz); g->w[1] = tx * (1.0 - ty) * (1.0 - tz);
+            g->w[2] = (1.0 - tx) * ty * (1.0 - tz); g->w[3] = tx * ty * (1.0 - tz);
+            g->w[4] = (1.0 - tx) * (1.0 - ty) * tz; g->w[5] = tx * (1.0 - ty) * tz;
+            g->w[6] = (1.0 - tx) * ty * tz; g->w[7] = tx * ty * tz;
+        }
+    }
+    int allFluid = 1;
+    for (int s = 0; s < g->n; ++s)
+        if (m->cellType[g->interp[s]] != SIFV_CELL_FLUID) { allFluid = 0; break; }
+    if (!allFluid) {
+        size_t f = g->interp[0];
+        for (int s = 0; s < g->n; ++s)
+            if (m->cellType[g->interp[s]] == SIFV_CELL_FLUID) { f = g->interp[s]; break; }
+        g->n = 1;
+        g->interp[0] = f;
+        g->w[0] = 1.0;
+    }
+}
+
+/* ImmersedBoundaryMethod::classifyCells (src/ImmersedBoundary.cpp:302-392) */
+static void ib_classify(ctx_t* m) {
+    const int dim = m->dim;
+    free(m->cellType); free(m->ibGhost);
+    m->cellType = (unsigned char*)calloc(m->n, 1);
+    int* owner = (int*)malloc(m->n * sizeof(int));
+    for (size_t q = 0; q < m->n; ++q) owner[q] = -1;
+    for (int k = 0; k < m->nz; ++k)
+        for (int j = 0; j < m->ny; ++j)
+            for (int i = 0; i < m->nx; ++i) {
+                size_t idx = IDX(m, i, j, k);
+                for (int b = 0; b < m->ibNBodies; ++b)
+                    if (ib_sdf(&m->ibBodies[b], CX(m, i), CY(m, j), CZ(m, k)) < 0) {
+                        m->cellType[idx] = SIFV_CELL_DEAD;
+                        owner[idx] = b;
+                        break;
+                    }
+            }
+    for (int k = 0; k < m->nz; ++k)
+        for (int j = 0; j < m->ny; ++j)
+            for (int i = 0; i < m->nx; ++i) {
+                size_t idx = IDX(m, i, j, k);
+                if (m->cellType[idx] != SIFV_CELL_DEAD) continue;
+                int fl = 0;
+                if (i > 0 && m->cellType[IDX(m, i - 1, j, k)] == SIFV_CELL_FLUID) fl = 1;
+                if (i < m->nx - 1 && m->cellType[IDX(m, i + 1, j, k)] == SIFV_CELL_FLUID) fl = 1;
+                if (dim >= 2) {
+                    if (j > 0 && m->cellType[IDX(m, i, j - 1, k)] == SIFV_CELL_FLUID) fl = 1;
+                    if (j < m->ny - 1 && m->cellType[IDX(m, i, j + 1, k)] == SIFV_CELL_FLUID) fl = 1;
+                }
+                if (dim >= 3) {
+                    if (k > 0 && m->cellType[IDX(m, i, j, k - 1)] == SIFV_CELL_FLUID) fl = 1;
+                    if (k < m->nz - 1 && m->cellType[IDX(m, i, j, k + 1)] == SIFV_CELL_FLUID) fl = 1;
+                }
+                if (fl) m->cellType[idx] = SIFV_CELL_GHOST;
+            }
+    int cap = 0;
+    for (size_t q = 0; q < m->n; ++q) cap += m->cellType[q] == SIFV_CELL_GHOST;
+    m->ibGhost = (IbGhost*)calloc(cap > 0 ? (size_t)cap : 1, sizeof(IbGhost));
+    m->ibCount = 0;
+    for (int k = 0; k < m->nz; ++k)
+        for (int j = 0; j < m->ny; ++j)
+            for (int i = 0; i < m->nx; ++i) {
+                size_t idx = IDX(m, i, j, k);
+                if (m->cellType[idx] != SIFV_CELL_GHOST) continue;
+                IbGhost* g = &m->ibGhost[m->ibCount++];
+                const sifv_ib_body_t* b = &m->ibBodies[owner[idx]];
+                double xG = CX(m, i), yG = CY(m, j), zG = CZ(m, k), cp[3];
+                ib_closest(b, xG, yG, zG, cp);
+                ib_normal(b, xG, yG, zG, g->normal);
+                g->cell = idx;
+                g->body = owner[idx];
+                ib_stencil(m, 2.0 * cp[0] - xG, 2.0 * cp[1] - yG, 2.0 * cp[2] - zG, g);
+            }
+    free(owner);
+}
+
+/* ImmersedBoundaryMethod::applyGhostCells (src/ImmersedBoundary.cpp:394-470) */
+static void ib_apply_ghosts(ctx_t* m) {
+    const int dim = m->dim, nPh = m->c.nPhases;
+    for (int q = 0; q < m->ibCount; ++q) {
+        const IbGhost* g = &m->ibGhost[q];
+        double r = 0.0, u = 0.0, v = 0.0, w = 0.0, p = 0.0, sg = 0.0, e = 0.0;
+        for (int s = 0; s < g->n; ++s) {
+            size_t c = g->interp[s];
+            double ws = g->w[s];
+            r += ws * m->rho[c];
+            u += ws * m->velU[c];
+            if (dim >= 2) v += ws * m->velV[c];
+            if (dim >= 3) w += ws * m->velW[c];
+            p += ws * m->pres[c];
+            sg += ws * m->sigma[c];
+            e += ws * m->rhoE[c];
+        }
+        size_t idx = g->cell;
+        m->rho[idx] = r;
+        m->pres[idx] = p;
+        m->sigma[idx] = sg;
+        m->rhoE[idx] = e;
+        double gu, gv, gw;
+        if (m->ibBodies[g->body].wall == SIFV_IB_NOSLIP) {
+            gu = -u; gv = -v; gw = -w;
+        } else {
+            double dot = u * g->normal[0];
+            if (dim >= 2) dot += v * g->normal[1];
+            if (dim >= 3) dot += w * g->normal[2];
+            gu = u - 2.0 * dot * g->normal[0];
+            gv = v - 2.0 * dot * g->normal[1];
+            gw = w - 2.0 * dot * g->normal[2];
+        }
+        m->velU[idx] = gu;
+        if (dim >= 2) m->velV[idx] = gv;
+        if (dim >= 3) m->velW[idx] = gw;
+        m->rhoU[idx] = r * gu;
+        if (dim >= 2) m->rhoV[idx] = r * gv;
+        if (dim >= 3) m->rhoW[idx] = r * gw;
+        for (int ph = 0; ph < nPh; ++ph) {
+            double val = 0.0;
+            for (int s = 0; s < g->n; ++s) val += g->w[s] * m->alphaRho[ph][g->interp[s]];
+            m->alphaRho[ph][idx] = val;
+        }
+        for (int ph = 0; ph < nPh; ++ph) {
+            double val = 0.0;
+            for (int s = 0; s < g->n; ++s) val += g->w[s] * m->alpha[ph][g->interp[s]];
+            m->alpha[ph][idx] = val;
+        }
+    }
+}
+
+/* ImmersedBoundaryMethod::applyScalarGhostCells (src/ImmersedBoundary.cpp:472-482) */
+static void ib_apply_scalar(ctx_t* m, double* f) {
+    for (int q = 0; q < m->ibCount; ++q) {
+        const IbGhost* g = &m->ibGhost[q];
+        double val = 0.0;
+        for (int s = 0; s < g->n; ++s) val += g->w[s] * f[g->interp[s]];
+        f[g->cell] = val;
+    }
+}
+
+int sifvo_set_immersed_bodies(ctx_t* m, const sifv_ib_body_t* bodies, int nBodies) {
+    if (!m || nBodies < 0 || (nBodies > 0 && !bodies)) return SIFV_ERR_BAD_ARG;
+    if (nBodies > 0 && m->c.semiImplicit) {
+        snprintf(m->err, sizeof(m->err), "the semi-implicit step has no immersed boundary");
+        return SIFV_ERR_UNSUPPORTED;
+    }
+    free(m->ibBodies); free(m->cellType); free(m->ibGhost);
+    m->ibBodies = NULL; m->cellType = NULL; m->ibGhost = NULL;
+    m->ibCount = 0;
+    m->ibNBodies = nBodies;
+    if (nBodies == 0) return SIFV_OK;
+    m->ibBodies = (sifv_ib_body_t*)malloc((size_t)nBodies * sizeof(sifv_ib_body_t));
+    memcpy(m->ibBodies, bodies, (size_t)nBodies * sizeof(sifv_ib_body_t));
+    ib_classify(m);
+    return SIFV_OK;
+}
+
+int sifvo_ib_cell_types(ctx_t* m, unsigned char* types) {
+    for (size_t q = 0; q < m->n; ++q) types[q] = m->cellType ? m->cellType[q] : SIFV_CELL_FLUID;
+    return SIFV_OK;
+}
+
+int sifvo_apply_ib_ghost_cells(ctx_t* m) {
+    if (m->cellType) ib_apply_ghosts(m);
     return SIFV_OK;
 }

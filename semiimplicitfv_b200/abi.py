@@ -136,6 +136,23 @@ class MeshSpec:
         return m
 
 
+IB_CIRCLE, IB_RECTANGLE, IB_CYLINDER, IB_PRISM = 0, 1, 2, 3
+IB_NOSLIP, IB_SLIP = 0, 1
+CELL_FLUID, CELL_GHOST, CELL_DEAD = 0, 1, 2
+
+
+class IbBody(C.Structure):
+    _fields_ = [("shape", C.c_int), ("wall", C.c_int), ("axis", C.c_int), ("p", C.c_double * 6)]
+
+
+def ib_body(shape: int, params, wall: int = IB_NOSLIP, axis: int = 2) -> IbBody:
+    b = IbBody()
+    b.shape, b.wall, b.axis = shape, wall, axis
+    for i, v in enumerate(params):
+        b.p[i] = v
+    return b
+
+
 class VtkFields(C.Structure):
     _fields_ = [("pres", C.c_void_p), ("sigma", C.c_void_p), ("rhoE", C.c_void_p), ("vel", C.c_void_p * 3),
                 ("mom", C.c_void_p * 3), ("rho", C.c_void_p), ("alphaRho", C.c_void_p * MAX_PHASES),
@@ -212,6 +229,9 @@ _OPTIONAL_SIGS = {
                                C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "ensemble_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "check_nan": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+    "set_immersed_bodies": (C.c_int, [C.c_void_p, C.POINTER(IbBody), C.c_int]),
+    "ib_cell_types": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "apply_ib_ghost_cells": (C.c_int, [C.c_void_p]),
     "vtk_open": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(Config), C.POINTER(Mesh), C.c_int,
                            C.POINTER(C.c_void_p)]),
     "vtk_write_host": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(VtkFields)]),
@@ -432,6 +452,19 @@ class Context:
         dt = C.c_double()
         self._check(self.be.fn["step"](self.h, step, time, target_dt, C.byref(dt)))
         return dt.value
+
+    def set_immersed_bodies(self, bodies):
+        """ImmersedBoundaryMethod::addBody for each body + classifyCells."""
+        arr = (IbBody * max(len(bodies), 1))(*bodies)
+        self._check(self.be.fn["set_immersed_bodies"](self.h, arr, len(bodies)))
+
+    def ib_cell_types(self) -> np.ndarray:
+        out = np.empty(self.ncells, dtype=np.uint8)
+        self._check(self.be.fn["ib_cell_types"](self.h, out.ctypes.data_as(C.c_void_p)))
+        return out.reshape(self.shape)
+
+    def apply_ib_ghost_cells(self):
+        self._check(self.be.fn["apply_ib_ghost_cells"](self.h))
 
     def check_nan(self):
         """(SIFV_F_* id, interior cell) of the first NaN, or (-1, -1)."""

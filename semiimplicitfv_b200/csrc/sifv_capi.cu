@@ -18,6 +18,7 @@
 #include "sifv_adjoint_api.h"
 #include "sifv_kernels.cuh"
 #include "sifv_sweep_api.h"
+#include "sifv_ib_api.h"
 #include "sifv_vtk_api.h"
 
 using namespace sifv;
@@ -87,6 +88,11 @@ struct sifv_ctx {
     double* tanF[3][5] = {};
     double* loopLog = nullptr;                // per-step dt of a device-resident time-loop batch
     int loopLogCap = 0;
+    // immersed boundary (sifv_set_immersed_*)
+    std::vector<double> cenX, cenY, cenZ;     // interior cell centroids
+    std::vector<unsigned char> ibTypes;       // CellType per cell (host copy), empty when off
+    IbDev ib{};
+    std::vector<void*> ibAllocs;
 };
 
 namespace {
@@ -289,6 +295,22 @@ void launch_scalar_ghosts(sifv_ctx* c, double* f) {
     c->launches++;
 }
 
+// applyGhostCells / applyScalarGhostCells of the immersed boundary, when set.
+void launch_ib_ghost(sifv_ctx* c) {
+    if (!c->ib.count) return;
+    const unsigned g = c->ib.sequential ? 1u : blocks(c->ib.count, kCellThreads);
+    NPH_DISPATCH(c, (k_ib_ghost<NPHV><<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ib, c->ctl)));
+    c->launches++;
+    mark(c, "ib_ghost");
+}
+
+void launch_ib_scalar(sifv_ctx* c, double* f) {
+    if (!c->ib.count) return;
+    const unsigned g = c->ib.sequential ? 1u : blocks(c->ib.count, kCellThreads);
+    k_ib_scalar<<<g, kCellThreads, 0, c->stream>>>(c->ib, f, c->ctl);
+    c->launches++;
+}
+
 int igr_solve(sifv_ctx* c, int step) {
     const Params& P = c->P;
     k_igr_setup<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(P, c->F, c->alphaIGR);
@@ -323,6 +345,7 @@ int igr_solve(sifv_ctx* c, int step) {
             c->launches += nplanes;
         }
         launch_scalar_ghosts(c, c->F.sigma);
+        launch_ib_scalar(c, c->F.sigma);   // src/IGR.cpp:156
     }
     mark(c, "igr");
     LAUNCH_CHECK(c);
@@ -630,6 +653,7 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
         body_force(cfg, time, K);
         if (c->stageHook && c->stageHook(s, 0) != 0) return SIFV_ERR_CUDA;
         launch_prim_bc(c);
+        launch_ib_ghost(c);   // src/ExplicitSolver.cpp:116
         if (cfg.useIGR) {
             int st = igr_solve(c, step);
             if (st != SIFV_OK) return st;
@@ -692,7 +716,10 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
             LAUNCH_CHECK(c);
         }
     }
-    if (!cfg.semiImplicit) launch_prim_bc(c);   // finalize: src/ExplicitSolver.cpp:192-200
+    if (!cfg.semiImplicit) {   // finalize: src/ExplicitSolver.cpp:192-200
+        launch_prim_bc(c);
+        launch_ib_ghost(c);
+    }
     LAUNCH_CHECK(c);
     return SIFV_OK;
 }
@@ -851,6 +878,14 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     std::vector<double> xe = build_ext(mesh->xNodes, nx, P.ngx);
     std::vector<double> ye = build_ext((dim >= 2) ? mesh->yNodes : unit, ny, P.ngy);
     std::vector<double> ze = build_ext((dim >= 3) ? mesh->zNodes : unit, nz, P.ngz);
+    auto centroids = [](const std::vector<double>& e, int ng, int n) {   // RectilinearMesh::cellCentroidX
+        std::vector<double> cen(n);
+        for (int i = 0; i < n; ++i) cen[i] = 0.5 * (e[i + ng] + e[i + ng + 1]);
+        return cen;
+    };
+    c->cenX = centroids(xe, P.ngx, nx);
+    c->cenY = centroids(ye, P.ngy, ny);
+    c->cenZ = centroids(ze, P.ngz, nz);
     auto widths = [](const std::vector<double>& e) {
         std::vector<double> w(e.size() - 1);
         for (size_t i = 0; i + 1 < e.size(); ++i) w[i] = e[i + 1] - e[i];
@@ -927,6 +962,7 @@ int sifv_destroy(sifv_ctx_t* c) {
     for (double* p : c->adjCkpt) cudaFree(p);
     if (c->adjStage) cudaFree(c->adjStage);
     if (c->loopLog) cudaFree(c->loopLog);
+    for (void* p : c->ibAllocs) cudaFree(p);
     delete c;
     return SIFV_OK;
 }
@@ -1139,8 +1175,10 @@ int sifv_acoustic_dt(sifv_ctx_t* c, double cfl, double maxDt, double* dt) {
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
     k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, maxDt);
+    Fields Fa = c->F;
+    Fa.solid = nullptr;   // the standalone reduction takes every interior cell
     NPH_DISPATCH(c, (k_dt_acoustic<NPHV><<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(
-                         c->P, c->F, c->ctl, cfl)));
+                         c->P, Fa, c->ctl, cfl)));
     LAUNCH_CHECK(c);
     CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -1220,10 +1258,11 @@ int cons_slot(const sifv_ctx* c, int field) {
 int adjoint_supported(sifv_ctx* c) {
     const sifv_config_t& g = c->cfg;
     if (g.semiImplicit || g.useIGR || g.nPhases > 0 || has_body_force(g) || g.precision != SIFV_PREC_FP64 ||
-        (g.reconOrder != SIFV_WENO5 && g.reconOrder != SIFV_UPWIND5) || g.nGhost > 7 || c->P.visc || c->P.cap)
+        (g.reconOrder != SIFV_WENO5 && g.reconOrder != SIFV_UPWIND5) || g.nGhost > 7 || c->P.visc || c->P.cap ||
+        c->ib.count > 0)
         return fail(c, SIFV_ERR_UNSUPPORTED,
                     "the adjoint / tangent covers the explicit single-phase WENO5 / UPWIND5 step in SIFV_PREC_FP64 "
-                    "without IGR, body force, viscosity or surface tension (nGhost <= 7)");
+                    "without IGR, body force, viscosity, surface tension or immersed bodies (nGhost <= 7)");
     return SIFV_OK;
 }
 
@@ -1864,6 +1903,116 @@ int sifv_run_time_loop(sifv_ctx_t* c, const sifv_time_loop_t* prm, sifv_vtk_t* v
     }
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return finish(SIFV_OK);
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Immersed boundaries
+// ===========================================================================
+namespace {
+
+int set_ib(sifv_ctx* c, int nBodies, const int* wall, const sifv_ib_shapes_t* shapes) {
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (void* p : c->ibAllocs) cudaFree(p);
+    c->ibAllocs.clear();
+    c->ib = IbDev{};
+    c->F.solid = nullptr;
+    c->ibTypes.clear();
+    if (nBodies == 0) return SIFV_OK;
+    if (c->cfg.semiImplicit) return fail(c, SIFV_ERR_UNSUPPORTED, "the semi-implicit step has no immersed boundary");
+    if (c->sweep)
+        return fail(c, SIFV_ERR_UNSUPPORTED, "immersed boundaries run in the SIFV_PREC_FP64 explicit step");
+    for (int b = 0; b < nBodies; ++b)
+        if (wall[b] != SIFV_IB_NOSLIP && wall[b] != SIFV_IB_SLIP) return fail(c, SIFV_ERR_BAD_ARG, "unknown wall type");
+    sifv::IbGeometry g;
+    g.dim = c->P.dim;
+    g.nx = c->P.nx;
+    g.ny = c->P.ny;
+    g.nz = c->P.nz;
+    g.ngx = c->P.ngx;
+    g.ngy = c->P.ngy;
+    g.ngz = c->P.ngz;
+    g.nxT = c->P.nxT;
+    g.nyT = c->P.nyT;
+    g.ncells = c->ncells;
+    g.cx = c->cenX;
+    g.cy = c->cenY;
+    g.cz = c->cenZ;
+    sifv::IbTable t;
+    sifv::ib_classify(g, nBodies, wall, *shapes, t);
+    c->ibTypes = t.type;
+    auto up = [&](const void* src, size_t bytes) -> void* {
+        void* p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(bytes, 1)) != cudaSuccess) return nullptr;
+        c->ibAllocs.push_back(p);
+        if (bytes && cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+        return p;
+    };
+    const size_t m = t.cell.size();
+    auto* solid = static_cast<const unsigned char*>(up(t.type.data(), t.type.size()));
+    IbDev d{};
+    d.count = (int)m;
+    d.sequential = t.sequential;
+    d.cell = static_cast<const long long*>(up(t.cell.data(), m * sizeof(long long)));
+    d.wall = static_cast<const int*>(up(t.wall.data(), m * sizeof(int)));
+    d.normal = static_cast<const double*>(up(t.normal.data(), m * 3 * sizeof(double)));
+    d.n = static_cast<const int*>(up(t.n.data(), m * sizeof(int)));
+    d.interp = static_cast<const long long*>(up(t.interp.data(), m * 8 * sizeof(long long)));
+    d.w = static_cast<const double*>(up(t.w.data(), m * 8 * sizeof(double)));
+    if (!solid || !d.cell || !d.wall || !d.normal || !d.n || !d.interp || !d.w) {
+        for (void* p : c->ibAllocs) cudaFree(p);
+        c->ibAllocs.clear();
+        c->ibTypes.clear();
+        return fail(c, SIFV_ERR_CUDA, "cannot upload the immersed-boundary tables");
+    }
+    c->ib = d;
+    c->F.solid = solid;
+    return SIFV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sifv_set_immersed_bodies(sifv_ctx_t* c, const sifv_ib_body_t* bodies, int nBodies) {
+    if (!c || nBodies < 0 || (nBodies > 0 && !bodies)) return fail(c, SIFV_ERR_BAD_ARG, "bad immersed-body list");
+    std::vector<int> wall(nBodies);
+    for (int b = 0; b < nBodies; ++b) {
+        const sifv_ib_body_t& q = bodies[b];
+        if (q.shape < SIFV_IB_CIRCLE || q.shape > SIFV_IB_PRISM) return fail(c, SIFV_ERR_BAD_ARG, "unknown body shape");
+        if (q.shape == SIFV_IB_CYLINDER && (q.axis < 0 || q.axis > 2))
+            return fail(c, SIFV_ERR_BAD_ARG, "cylinder axis must be 0, 1 or 2");
+        wall[b] = q.wall;
+    }
+    sifv_ib_shapes_t s{};
+    sifv::ib_builtin_shapes(bodies, s);
+    return set_ib(c, nBodies, wall.data(), &s);
+}
+
+int sifv_set_immersed_shapes(sifv_ctx_t* c, int nBodies, const int* wall, const sifv_ib_shapes_t* shapes) {
+    if (!c || nBodies < 0 || (nBodies > 0 && (!wall || !shapes || !shapes->signedDistance || !shapes->closestPoint ||
+                                              !shapes->outwardNormal)))
+        return fail(c, SIFV_ERR_BAD_ARG, "bad immersed-shape queries");
+    return set_ib(c, nBodies, wall, shapes);
+}
+
+int sifv_ib_cell_types(sifv_ctx_t* c, unsigned char* types) {
+    if (!c || !types) return fail(c, SIFV_ERR_BAD_ARG, "null argument");
+    if (c->ibTypes.empty()) std::memset(types, SIFV_CELL_FLUID, c->ncells);
+    else std::memcpy(types, c->ibTypes.data(), c->ncells);
+    return SIFV_OK;
+}
+
+int sifv_apply_ib_ghost_cells(sifv_ctx_t* c) {
+    if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
+    launch_ib_ghost(c);
+    LAUNCH_CHECK(c);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return SIFV_OK;
 }
 
 }  // extern "C"

@@ -82,6 +82,22 @@ struct Fields {
     double *igrRhs, *igrDiag;
     const double *dx, *dy, *dz;     // per cell incl. ghosts (dx(i) at [i + ngx])
     const double *adx2, *ady2, *adz2;  // alpha / (d*d) per cell (IGR)
+    const unsigned char* solid;        // immersed-boundary CellType per cell (nonzero: solid), or nullptr
+};
+
+// Immersed-boundary ghost cells on the device (GhostCellInfo,
+// include/ImmersedBoundary.hpp:96-103), entry q: cell[q], wall[q] (0
+// no-slip, 1 slip), normal[3q..3q+2], n[q] stencil cells interp[8q..],
+// weights w[8q..].  sequential: some stencil reads another ghost cell, so
+// the entries run one after another in list order.
+struct IbDev {
+    int count, sequential;
+    const long long* cell;
+    const int* wall;
+    const double* normal;
+    const int* n;
+    const long long* interp;
+    const double* w;
 };
 
 // Step control block in device memory.

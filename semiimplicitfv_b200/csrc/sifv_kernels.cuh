@@ -259,6 +259,7 @@ __global__ void __launch_bounds__(256) k_assemble(Params P, Fields F, const Ctl*
     if (!int_coords(P, t, i, j, k)) return;
     const int dim = P.dim;
     const size_t c = cidx(P, i, j, k);
+    if (F.solid && F.solid[c]) return;   // immersed-boundary solid cells are not updated
     CellFaces cf;
     cell_faces(P, F, i, j, k, cf);
 
@@ -399,7 +400,7 @@ __global__ void __launch_bounds__(256) k_dt_acoustic(Params P, Fields F, Ctl* ct
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
     double v = __longlong_as_double(0x7ff0000000000000LL);
-    if (int_coords(P, t, i, j, k)) {
+    if (int_coords(P, t, i, j, k) && !(F.solid && F.solid[cidx(P, i, j, k)])) {   // ibm: solid cells skipped
         const int dim = P.dim;
         size_t c = cidx(P, i, j, k);
         double cs;
@@ -445,7 +446,7 @@ __global__ void __launch_bounds__(256) k_dt_viscous(Params P, Fields F, Ctl* ctl
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
     double v = __longlong_as_double(0x7ff0000000000000LL);
-    if (int_coords(P, t, i, j, k)) {
+    if (int_coords(P, t, i, j, k) && !(F.solid && F.solid[cidx(P, i, j, k)])) {   // ibm: solid cells skipped
         const int dim = P.dim;
         size_t c = cidx(P, i, j, k);
         double dxMin = F.dx[i + P.ngx];
@@ -583,7 +584,7 @@ __global__ void __launch_bounds__(256) k_dt_capillary(Params P, Fields F, Ctl* c
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
     double v = __longlong_as_double(0x7ff0000000000000LL);
-    if (int_coords(P, t, i, j, k)) {
+    if (int_coords(P, t, i, j, k) && !(F.solid && F.solid[cidx(P, i, j, k)])) {   // ibm: solid cells skipped
         const int dim = P.dim;
         size_t c = cidx(P, i, j, k);
         double dxMin = F.dx[i + P.ngx];
@@ -656,6 +657,104 @@ __global__ void __launch_bounds__(256) k_cap_face(Params P, Fields F, const Ctl*
     if (dim >= 2) out[1][t] = T[1];
     if (dim >= 3) out[2][t] = T[2];
     out[3][t] = work;
+}
+
+// ImmersedBoundaryMethod::applyGhostCells (src/ImmersedBoundary.cpp:394-470)
+// for entry q: stencil-weighted state at the image point, velocity reversed
+// (no-slip) or its normal component mirrored (slip), momentum from the
+// interpolated density.
+template <int NPH>
+__device__ void ib_ghost_entry(const Params& P, const Fields& F, const IbDev& G, int q) {
+    const int dim = P.dim;
+    const int n = G.n[q];
+    const long long* cs = G.interp + 8 * (size_t)q;
+    const double* ws = G.w + 8 * (size_t)q;
+    double r = 0.0, u = 0.0, v = 0.0, w = 0.0, p = 0.0, sg = 0.0, e = 0.0;
+    for (int s = 0; s < n; ++s) {
+        const size_t c = (size_t)cs[s];
+        const double wt = ws[s];
+        r += wt * F.rho[c];
+        u += wt * F.velU[c];
+        if (dim >= 2) v += wt * F.velV[c];
+        if (dim >= 3) w += wt * F.velW[c];
+        p += wt * F.pres[c];
+        sg += wt * F.sigma[c];
+        e += wt * F.rhoE[c];
+    }
+    const size_t idx = (size_t)G.cell[q];
+    F.rho[idx] = r;
+    F.pres[idx] = p;
+    F.sigma[idx] = sg;
+    F.rhoE[idx] = e;
+    double gu, gv, gw;
+    if (G.wall[q] == 0) {
+        gu = -u;
+        gv = -v;
+        gw = -w;
+    } else {
+        const double* nr = G.normal + 3 * (size_t)q;
+        double dot = u * nr[0];
+        if (dim >= 2) dot += v * nr[1];
+        if (dim >= 3) dot += w * nr[2];
+        gu = u - 2.0 * dot * nr[0];
+        gv = v - 2.0 * dot * nr[1];
+        gw = w - 2.0 * dot * nr[2];
+    }
+    F.velU[idx] = gu;
+    if (dim >= 2) F.velV[idx] = gv;
+    if (dim >= 3) F.velW[idx] = gw;
+    F.rhoU[idx] = r * gu;
+    if (dim >= 2) F.rhoV[idx] = r * gv;
+    if (dim >= 3) F.rhoW[idx] = r * gw;
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            double val = 0.0;
+            for (int s = 0; s < n; ++s) val += ws[s] * F.alphaRho[ph][cs[s]];
+            F.alphaRho[ph][idx] = val;
+        }
+    }
+#pragma unroll
+    for (int ph = 0; ph < NPH; ++ph) {
+        if (ph < P.nPh) {
+            double val = 0.0;
+            for (int s = 0; s < n; ++s) val += ws[s] * F.alpha[ph][cs[s]];
+            F.alpha[ph][idx] = val;
+        }
+    }
+}
+
+// One thread per ghost entry; one thread for the whole list, in order, when
+// a stencil reads another ghost cell (the reference's sequential loop).
+template <int NPH>
+__global__ void __launch_bounds__(256) k_ib_ghost(Params P, Fields F, IbDev G, const Ctl* __restrict__ ctl) {
+    if (ctl && ctl->skip) return;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (G.sequential) {
+        if (t == 0)
+            for (int q = 0; q < G.count; ++q) ib_ghost_entry<NPH>(P, F, G, q);
+        return;
+    }
+    if (t < G.count) ib_ghost_entry<NPH>(P, F, G, (int)t);
+}
+
+// applyScalarGhostCells (src/ImmersedBoundary.cpp:472-482).
+__global__ void __launch_bounds__(256) k_ib_scalar(IbDev G, double* __restrict__ f, const Ctl* __restrict__ ctl) {
+    if (ctl && ctl->skip) return;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    auto one = [&](int q) {
+        const long long* cs = G.interp + 8 * (size_t)q;
+        const double* ws = G.w + 8 * (size_t)q;
+        double val = 0.0;
+        for (int s = 0; s < G.n[q]; ++s) val += ws[s] * f[cs[s]];
+        f[G.cell[q]] = val;
+    };
+    if (G.sequential) {
+        if (t == 0)
+            for (int q = 0; q < G.count; ++q) one(q);
+        return;
+    }
+    if (t < G.count) one((int)t);
 }
 
 // Reset the dt accumulator to maxDt (dt starts at maxDt in the reference).
@@ -1181,6 +1280,7 @@ __global__ void __launch_bounds__(256) k_igr_setup(Params P, Fields F, double al
 __device__ __forceinline__ void igr_cell(const Params& P, const Fields& F, int i, int j, int k) {
     const int dim = P.dim;
     size_t c = cidx(P, i, j, k);
+    if (F.solid && F.solid[c]) return;   // solid cells keep sigma (src/IGR.cpp:51)
     const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
     double* S = F.sigma;
     double rho_i = F.rho[c];
@@ -1275,7 +1375,7 @@ __global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, int pl
     const int nq = ex + ey + ez - 2;
     for (int q = 0; q < nq; ++q) {
         const int a = q - tb - tc;
-        if (act && a >= 0 && a < ex) {
+        if (act && a >= 0 && a < ex && !(F.solid && F.solid[cidx(P, i0 + a, j0 + tb, k0 + tc)])) {
             const int h = hLine + a;
             const int l = lLine + a;
             const double rho_i = sR[h];

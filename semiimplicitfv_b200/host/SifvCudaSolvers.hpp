@@ -28,6 +28,7 @@
 #include "EquationOfState.hpp"
 #include "HaloExchange.hpp"
 #include "IGR.hpp"
+#include "ImmersedBoundary.hpp"
 #include "PressureSolver.hpp"
 #include "RectilinearMesh.hpp"
 #include "RiemannSolver.hpp"
@@ -171,7 +172,7 @@ public:
         : riemann_(std::move(riemann)), eos_(std::move(eos)), device_(device), precision_(precision), sync_(sync) {
         config.validate();
     }
-    ~CudaStepperBase() { if (ctx_) sifv_destroy(ctx_); }
+    virtual ~CudaStepperBase() { if (ctx_) sifv_destroy(ctx_); }
     CudaStepperBase(const CudaStepperBase&) = delete;
     CudaStepperBase& operator=(const CudaStepperBase&) = delete;
 
@@ -193,6 +194,7 @@ protected:
             MeshNodes nodes(mesh, halo_);
             throwStatus(sifv_create(&c, &nodes.m, device_, &ctx_), "sifv_create");
             throwStatus(sifv_set_pressure_solver(ctx_, pressureKind_), ctx_, "sifv_set_pressure_solver");
+            afterCreate();
             dim_ = config.dim;
             nPhases_ = config.multiPhaseParams.nPhases;
             uploadState(ctx_, state, dim_, nPhases_);
@@ -206,6 +208,9 @@ protected:
         return dt;
     }
 
+    // set-up that needs the context (called once, right after it exists)
+    virtual void afterCreate() {}
+
     std::shared_ptr<RiemannSolver> riemann_;
     std::shared_ptr<EquationOfState> eos_;
     HaloExchange* halo_ = nullptr;
@@ -214,6 +219,23 @@ protected:
     int pressureKind_ = SIFV_PRESSURE_JACOBI;
     SyncPolicy sync_;
     int dim_ = 0, nPhases_ = 0;
+};
+
+// Drop-in for ImmersedBoundaryMethod (include/ImmersedBoundary.hpp:107-135)
+// that also keeps its bodies: CudaExplicitSolver::setIBM classifies the same
+// cells on the GPU side through the bodies' own IBBody queries, so bodies of
+// any shape carry over.  Use it where the driver declares its
+// ImmersedBoundaryMethod; addBody / classifyCells / cellType work unchanged.
+class CudaImmersedBoundary : public ImmersedBoundaryMethod {
+public:
+    void addBody(std::shared_ptr<IBBody> body) {
+        ImmersedBoundaryMethod::addBody(body);
+        cudaBodies_.push_back(std::move(body));
+    }
+    const std::vector<std::shared_ptr<IBBody>>& bodies() const { return cudaBodies_; }
+
+private:
+    std::vector<std::shared_ptr<IBBody>> cudaBodies_;
 };
 
 // Drop-in for ExplicitSolver (include/ExplicitSolver.hpp:21-36).
@@ -231,6 +253,46 @@ public:
                 double targetDt = -1.0) {
         return stepImpl(config, mesh, state, targetDt);
     }
+
+    // ExplicitSolver::setIBM (include/ExplicitSolver.hpp:39-42); nullptr detaches.
+    void setIBM(CudaImmersedBoundary* ibm) {
+        ibm_ = ibm;
+        if (ctx_) attachIBM();
+    }
+
+protected:
+    void afterCreate() override {
+        if (ibm_) attachIBM();
+    }
+
+private:
+    void attachIBM() {
+        if (!ibm_) {
+            throwStatus(sifv_set_immersed_shapes(ctx_, 0, nullptr, nullptr), ctx_, "sifv_set_immersed_shapes");
+            return;
+        }
+        const auto& bodies = ibm_->bodies();
+        std::vector<int> wall;
+        for (const auto& b : bodies)
+            wall.push_back(b->wallType() == IBBody::WallType::Slip ? SIFV_IB_SLIP : SIFV_IB_NOSLIP);
+        sifv_ib_shapes_t s{};
+        s.user = ibm_;
+        s.signedDistance = [](void* u, int b, double x, double y, double z) {
+            return static_cast<CudaImmersedBoundary*>(u)->bodies()[b]->signedDistance(x, y, z);
+        };
+        s.closestPoint = [](void* u, int b, double x, double y, double z, double o[3]) {
+            auto p = static_cast<CudaImmersedBoundary*>(u)->bodies()[b]->closestPoint(x, y, z);
+            o[0] = p[0]; o[1] = p[1]; o[2] = p[2];
+        };
+        s.outwardNormal = [](void* u, int b, double x, double y, double z, double o[3]) {
+            auto p = static_cast<CudaImmersedBoundary*>(u)->bodies()[b]->outwardNormal(x, y, z);
+            o[0] = p[0]; o[1] = p[1]; o[2] = p[2];
+        };
+        throwStatus(sifv_set_immersed_shapes(ctx_, (int)bodies.size(), wall.data(), &s), ctx_,
+                    "sifv_set_immersed_shapes");
+    }
+
+    CudaImmersedBoundary* ibm_ = nullptr;
 };
 
 // Drop-in for SemiImplicitSolver (include/SemiImplicitSolver.hpp:22-46) with

@@ -315,6 +315,61 @@ def capillary(name):
     raise KeyError(name)
 
 
+def flow_over_circle(nx=40, ny=20, slip=False, igr=False):
+    """Uniform Mach 0.2 stream past a circle (examples/2D_flow_over_circle/
+    2D_flow_over_circle.cpp:19-170): [0, 4] x [0, 2], circle (1, 1) r 0.2,
+    rho 1, u 1, p = 1 / (1.4 M^2); x outflow, y slip walls; cfl 0.5,
+    maxDt 1; IGR alphaCoeff 1.  Returns (case, bodies)."""
+    cfg = abi.config_defaults(dim=2, nGhost=3, RKOrder=3, reconOrder=abi.WENO5, riemannSolver=abi.HLLC,
+                              cfl=0.5, maxDt=1.0, useIGR=int(igr), alphaCoeff=1.0, IGRIters=5,
+                              IGRWarmStartIters=50)
+    x = abi.linspace_nodes(nx, 0.0, 4.0)
+    y = abi.linspace_nodes(ny, 0.0, 2.0)
+    p_inf = 1.0 / (1.4 * 0.2 * 0.2)
+    shape = _ext_shape(cfg, nx, ny, 1)
+    one = np.ones((1, ny, nx))
+    fields = _single_phase_fields(cfg, shape, one, one, 0.0 * one, None, p_inf * one, 1.4)
+    mesh = abi.MeshSpec(x, y, bc=[BC_OUTFLOW, BC_OUTFLOW, abi.BC_SLIPWALL, abi.BC_SLIPWALL, 0, 0])
+    body = abi.ib_body(abi.IB_CIRCLE, [1.0, 1.0, 0.2], abi.IB_SLIP if slip else abi.IB_NOSLIP)
+    return (cfg, mesh, fields), [body]
+
+
+IB_CASES = ["circle_noslip", "circle_slip_igr", "rectangle_riemann", "prism_cylinder_3d", "droplet_rectangle",
+            "two_circles_1d", "slit_sequential"]
+
+
+def immersed(name):
+    """Immersed-boundary cases: (case, bodies, steps)."""
+    if name == "circle_noslip":
+        case, bodies = flow_over_circle(48, 24)
+        return case, bodies, 6
+    if name == "circle_slip_igr":
+        case, bodies = flow_over_circle(40, 20, slip=True, igr=True)
+        return case, bodies, 3
+    if name == "rectangle_riemann":
+        case = riemann2d(36, bc=abi.BC_SLIPWALL)
+        return case, [abi.ib_body(abi.IB_RECTANGLE, [0.45, 0.55, 0.12, 0.08], abi.IB_SLIP),
+                      abi.ib_body(abi.IB_CIRCLE, [0.7, 0.3, 0.09])], 6
+    if name == "prism_cylinder_3d":
+        case = acoustic3d(14, semi=False, igr=False, rk=2)
+        case[1].bc = [abi.BC_OUTFLOW, abi.BC_SLIPWALL, abi.BC_NOSLIPWALL, abi.BC_OUTFLOW,
+                      abi.BC_SYMMETRY, abi.BC_OUTFLOW]
+        return case, [abi.ib_body(abi.IB_PRISM, [0.3, 0.35, 0.5, 0.12, 0.1, 0.2], abi.IB_SLIP),
+                      abi.ib_body(abi.IB_CYLINDER, [0.7, 0.6, 0.13], abi.IB_NOSLIP, axis=1)], 4
+    if name == "droplet_rectangle":
+        case = droplet(24)
+        return case, [abi.ib_body(abi.IB_RECTANGLE, [1.2e-3, 3.0e-3, 4e-4, 1.5e-3], abi.IB_NOSLIP)], 4
+    if name == "two_circles_1d":
+        case = water_air(64, p_left=2e5)
+        return case, [abi.ib_body(abi.IB_CIRCLE, [0.25, 0.5, 0.06]),
+                      abi.ib_body(abi.IB_CIRCLE, [0.8, 0.5, 0.05], abi.IB_SLIP)], 6
+    if name == "slit_sequential":   # a sub-cell slit: some stencils see only ghost cells
+        case = riemann2d(40, bc=abi.BC_SLIPWALL)
+        return case, [abi.ib_body(abi.IB_RECTANGLE, [0.3, 0.5, 0.1, 0.2]),
+                      abi.ib_body(abi.IB_RECTANGLE, [0.51, 0.5, 0.1, 0.2], abi.IB_SLIP)], 5
+    raise KeyError(name)
+
+
 VISCOUS_CASES = ["riemann2d_noslip", "water_air_phase_mu", "acoustic3d_semi", "vortex_periodic"]
 
 

@@ -72,3 +72,12 @@ def test_explicit_adapter_viscous_bit_identical(lib, bc):
     lib.sifv_adapter_selftest_explicit_viscous.restype = ctypes.c_double
     lib.sifv_adapter_selftest_explicit_viscous.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
     assert lib.sifv_adapter_selftest_explicit_viscous(40, 8, bc, 0.01) == 0.0
+
+
+@pytest.mark.parametrize("slip,igr", [(0, 0), (1, 0), (0, 1)])
+def test_explicit_adapter_immersed_boundary_bit_identical(lib, slip, igr):
+    """CudaExplicitSolver + CudaImmersedBoundary against ExplicitSolver +
+    ImmersedBoundaryMethod with the same IBCircle."""
+    lib.sifv_adapter_selftest_ibm.restype = ctypes.c_double
+    lib.sifv_adapter_selftest_ibm.argtypes = [ctypes.c_int] * 4
+    assert lib.sifv_adapter_selftest_ibm(48, 6, slip, igr) == 0.0

@@ -290,3 +290,65 @@ def test_surface_tension_rejected_without_phases():
     with pytest.raises(abi.AbiError) as e:
         backends.cuda().create(case[0], case[1])
     assert e.value.status == abi.ERR_BAD_CONFIG
+
+
+@pytest.mark.parametrize("name", cases.IB_CASES)
+def test_immersed_boundary(name):
+    """ImmersedBoundaryMethod on the GPU: cell classification, the ghost-cell
+    fill per stage (parallel, or in list order when a stencil reads another
+    ghost cell), solid cells out of the update, the dt limit and the IGR
+    sweeps; bit-identical to the oracle."""
+    case, bodies, n = cases.immersed(name)
+    cg = backends.make(backends.cuda(), case)
+    co = backends.make(backends.oracle(), case)
+    cg.set_immersed_bodies(bodies)
+    co.set_immersed_bodies(bodies)
+    assert np.array_equal(cg.ib_cell_types(), co.ib_cell_types())
+    check_pair = run_pair_contexts(cg, co, n)
+    assert check_pair
+
+
+def run_pair_contexts(cg, co, n):
+    _, _, dtg = cases.run_steps(cg, n)
+    _, _, dto = cases.run_steps(co, n)
+    assert dtg == dto
+    for fid in _fields(cg.cfg):
+        assert np.array_equal(cg.get_field(fid), co.get_field(fid)), fid
+    return True
+
+
+def test_immersed_boundary_time_loop_and_removal():
+    """The device-resident time loop runs the ghost-cell fill too, and an
+    empty body list restores the plain step."""
+    case, bodies, _ = cases.immersed("circle_noslip")
+    cg = backends.make(backends.cuda(), case)
+    co = backends.make(backends.oracle(), case)
+    cg.set_immersed_bodies(bodies)
+    co.set_immersed_bodies(bodies)
+    st, r = cg.run_time_loop(0.05, 0.02, batch=4)
+    t, n = cases.run_time_loop(co, 0.05, 0.02)
+    assert st == abi.OK and r.steps == n and r.time == t
+    for fid in _fields(case[0]):
+        assert np.array_equal(cg.get_field(fid), co.get_field(fid)), fid
+    cg.set_immersed_bodies([])
+    co.set_immersed_bodies([])
+    assert not cg.ib_cell_types().any()
+    _, _, dtg = cases.run_steps(cg, 3, step0=n, time0=t)
+    _, _, dto = cases.run_steps(co, 3, step0=n, time0=t)
+    assert dtg == dto
+    for fid in _fields(case[0]):
+        assert np.array_equal(cg.get_field(fid), co.get_field(fid)), fid
+
+
+def test_immersed_boundary_rejected_where_unsupported():
+    case, bodies, _ = cases.immersed("circle_noslip")
+    semi = cases.acoustic3d(8)
+    cs = backends.make(backends.cuda(), semi)
+    with pytest.raises(abi.AbiError) as e:
+        cs.set_immersed_bodies([abi.ib_body(abi.IB_PRISM, [0.5, 0.5, 0.5, 0.1, 0.1, 0.1])])
+    assert e.value.status == abi.ERR_UNSUPPORTED
+    case[0].precision = abi.PREC_FP64_FAST
+    cf = backends.make(backends.cuda(), case)
+    with pytest.raises(abi.AbiError) as e:
+        cf.set_immersed_bodies(bodies)
+    assert e.value.status == abi.ERR_UNSUPPORTED

@@ -173,3 +173,24 @@ def test_surface_tension_config_validation():
     assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.OK
     bad.nPhases = 0
     assert lib.fn["config_validate"](ctypes.byref(bad)) == abi.ERR_BAD_CONFIG
+
+
+@pytest.mark.parametrize("name", cases.IB_CASES)
+def test_immersed_boundary(name):
+    """ImmersedBoundaryMethod (src/ImmersedBoundary.cpp): classifyCells with
+    the four body shapes, applyGhostCells per stage, solid cells out of the
+    update, the dt limit and the IGR sweeps."""
+    case, bodies, n = cases.immersed(name)
+    ref = backends.reference()
+    cr = backends.make(ref, case)
+    co = backends.make(backends.oracle(), case)
+    cr.set_immersed_bodies(bodies)
+    co.set_immersed_bodies(bodies)
+    types = co.ib_cell_types()
+    assert np.array_equal(types, cr.ib_cell_types())
+    assert (types == abi.CELL_GHOST).sum() > 0 and (types == abi.CELL_DEAD).sum() > 0
+    _, _, dr = cases.run_steps(cr, n)
+    _, _, do = cases.run_steps(co, n)
+    assert dr == do
+    for fid in cases.output_fields(co, case[0]):
+        assert np.array_equal(co.get_field(fid), cr.get_field(fid)), fid
