@@ -254,6 +254,14 @@ int sifv_last_step_stats(const sifv_ctx_t* ctx, double* deviceMs, int* launches)
  * lexicographic in-place sweeps run as a tiled wavefront, bit-identical). */
 #define SIFV_PRESSURE_JACOBI 0
 #define SIFV_PRESSURE_GAUSS_SEIDEL 1
+/* HyprePressureSolver (src/HyprePressureSolver.cpp, built with Hypre only):
+ * conjugate gradients preconditioned by one multigrid V-cycle (weighted
+ * Jacobi relaxation, Galerkin coarse levels), stopping when the residual's
+ * two-norm falls to tol times the right-hand side's; Neumann faces on
+ * physical boundaries.  The same linear system and stopping rule as the
+ * reference's Hypre PCG+PFMG, not its bits: the multigrid hierarchy is this
+ * library's own.  Iteration counts stay nearly flat as the mesh grows. */
+#define SIFV_PRESSURE_PCG_MG 2
 int sifv_set_pressure_solver(sifv_ctx_t* ctx, int kind);
 
 /* ---- immersed boundaries ---------------------------------------------------- */

@@ -136,6 +136,7 @@ class MeshSpec:
         return m
 
 
+PRESSURE_JACOBI, PRESSURE_GAUSS_SEIDEL, PRESSURE_PCG_MG = 0, 1, 2
 IB_CIRCLE, IB_RECTANGLE, IB_CYLINDER, IB_PRISM = 0, 1, 2, 3
 IB_NOSLIP, IB_SLIP = 0, 1
 CELL_FLUID, CELL_GHOST, CELL_DEAD = 0, 1, 2
@@ -607,12 +608,15 @@ class Context:
         fams = names.value.decode().split("\n") if n.value else []
         return {f: (ms[k], cnt[k]) for k, f in enumerate(fams)}
 
-    def interior(self, arr: np.ndarray) -> np.ndarray:
-        """Slice the physical cells out of a (k, j, i) field."""
+    def interior_slices(self):
+        """(k, j, i) slices of the physical cells."""
         d = self.cfg.dim
         g = self.ng
-        gi = g
         gj = g if d >= 2 else 0
         gk = g if d >= 3 else 0
         nz, ny, nx = self.shape
-        return arr[gk:nz - gk, gj:ny - gj, gi:nx - gi]
+        return slice(gk, nz - gk), slice(gj, ny - gj), slice(g, nx - g)
+
+    def interior(self, arr: np.ndarray) -> np.ndarray:
+        """Slice the physical cells out of a (k, j, i) field."""
+        return arr[self.interior_slices()]

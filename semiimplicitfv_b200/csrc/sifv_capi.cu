@@ -17,6 +17,7 @@
 #include "sifv.h"
 #include "sifv_adjoint_api.h"
 #include "sifv_kernels.cuh"
+#include "sifv_mg.cuh"
 #include "sifv_sweep_api.h"
 #include "sifv_ib_api.h"
 #include "sifv_vtk_api.h"
@@ -93,6 +94,11 @@ struct sifv_ctx {
     std::vector<unsigned char> ibTypes;       // CellType per cell (host copy), empty when off
     IbDev ib{};
     std::vector<void*> ibAllocs;
+    // PCG + multigrid pressure solver (SIFV_PRESSURE_PCG_MG)
+    std::vector<MgLevel> mg;
+    double* cg[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // x r z p q 1/m
+    double* cgScal = nullptr;    // 8 device scalars
+    double* cgPartial = nullptr; // block partial sums of the fine level
 };
 
 namespace {
@@ -227,16 +233,24 @@ double* field_ptr(sifv_ctx* c, int f) {
     return nullptr;
 }
 
+// Grow the control block's residual history to n entries; the control
+// fields (dt, time, flags) carry over to the new block.
 int ensure_res(sifv_ctx* c, int n) {
     if (n <= c->resCap) return SIFV_OK;
-    if (c->ctl) cudaFree(c->ctl);
-    if (c->ctlHost) cudaFreeHost(c->ctlHost);
-    c->ctl = nullptr;
-    c->ctlHost = nullptr;
+    Ctl* old = c->ctl;
+    Ctl* oldHost = c->ctlHost;
+    Ctl* fresh = nullptr;
+    Ctl* freshHost = nullptr;
     size_t bytes = sizeof(Ctl) + sizeof(unsigned long long) * (size_t)(n + 1);
-    CUDA_TRY(c, cudaMalloc(&c->ctl, bytes));
-    CUDA_TRY(c, cudaMallocHost(&c->ctlHost, bytes));
-    CUDA_TRY(c, cudaMemsetAsync(c->ctl, 0, bytes, c->stream));
+    CUDA_TRY(c, cudaMalloc(&fresh, bytes));
+    CUDA_TRY(c, cudaMallocHost(&freshHost, bytes));
+    CUDA_TRY(c, cudaMemsetAsync(fresh, 0, bytes, c->stream));
+    if (old) CUDA_TRY(c, cudaMemcpyAsync(fresh, old, offsetof(Ctl, res), cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (old) cudaFree(old);
+    if (oldHost) cudaFreeHost(oldHost);
+    c->ctl = fresh;
+    c->ctlHost = freshHost;
     c->resCap = n;
     return SIFV_OK;
 }
@@ -486,8 +500,153 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
     return SIFV_OK;
 }
 
+// Multigrid hierarchy for the fine mesh: every axis longer than 1 halves
+// (ceil) until a level holds at most 256 cells.
+int mg_alloc(sifv_ctx* c) {
+    if (!c->mg.empty()) return SIFV_OK;
+    int st = SIFV_OK;
+    int nx = c->P.nx, ny = c->P.ny, nz = c->P.nz;
+    for (int l = 0;; ++l) {
+        MgLevel L{};
+        L.nx = nx; L.ny = ny; L.nz = nz;
+        L.n = (long long)nx * ny * nz;
+        L.m = dalloc(c, L.n, st);
+        L.tx = dalloc(c, L.n, st);
+        L.ty = dalloc(c, L.n, st);
+        L.tz = dalloc(c, L.n, st);
+        L.diag = dalloc(c, L.n, st);
+        L.r = dalloc(c, L.n, st);
+        L.t = dalloc(c, L.n, st);
+        if (l > 0) {
+            L.x = dalloc(c, L.n, st);
+            L.b = dalloc(c, L.n, st);
+        }
+        if (st != SIFV_OK) return st;
+        c->mg.push_back(L);
+        if (L.n <= 256 || (nx <= 2 && ny <= 2 && nz <= 2)) break;
+        nx = (nx > 1) ? (nx + 1) / 2 : 1;
+        ny = (ny > 1) ? (ny + 1) / 2 : 1;
+        nz = (nz > 1) ? (nz + 1) / 2 : 1;
+    }
+    const long long n0 = c->mg[0].n;
+    for (int q = 0; q < 6; ++q) c->cg[q] = dalloc(c, n0, st);
+    c->cgScal = dalloc(c, 8, st);
+    c->cgPartial = dalloc(c, blocks(n0, kCellThreads) + 1, st);
+    return st;
+}
+
+constexpr double kMgOmega = 0.8;       // weighted-Jacobi relaxation
+constexpr int kMgCoarsestSweeps = 60;  // relaxation sweeps on the coarsest level
+
+// z = V(r): one V(1,1)-cycle from z = 0 (level 0 reads b = r, writes x = z).
+void mg_vcycle(sifv_ctx* c, int l, const double* r0, double* z0) {
+    const int dim = c->P.dim;
+    MgLevel L = c->mg[l];
+    if (l == 0) {
+        L.b = const_cast<double*>(r0);
+        L.x = z0;
+    }
+    const unsigned g = blocks(L.n, kCellThreads);
+    if (l + 1 == (int)c->mg.size()) {
+        k_mg_coarsest<<<1, 1024, 0, c->stream>>>(L, dim, kMgOmega, kMgCoarsestSweeps);
+        c->launches++;
+        return;
+    }
+    MgLevel C = c->mg[l + 1];
+    k_mg_smooth0<<<g, kCellThreads, 0, c->stream>>>(L, kMgOmega);
+    k_mg_residual<<<g, kCellThreads, 0, c->stream>>>(L, dim);
+    k_mg_restrict<<<blocks(C.n, kCellThreads), kCellThreads, 0, c->stream>>>(L, C);
+    c->launches += 3;
+    mg_vcycle(c, l + 1, nullptr, nullptr);
+    k_mg_prolong<<<g, kCellThreads, 0, c->stream>>>(L, C);
+    k_mg_smooth<<<g, kCellThreads, 0, c->stream>>>(L, dim, L.x, L.t, kMgOmega);
+    cudaMemcpyAsync(L.x, L.t, sizeof(double) * L.n, cudaMemcpyDeviceToDevice, c->stream);
+    c->launches += 2;
+}
+
+// HyprePressureSolver::solve (src/HyprePressureSolver.cpp:333-399): PCG on
+// the symmetric scaled system with a multigrid V-cycle as preconditioner,
+// stopping when |r|_2 <= tol |rhs|_2 on the unscaled system.  Initial guess
+// and result in F.pA (interior; ghosts untouched).
+int mg_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rhs, double tol, int maxIter,
+           int& iters, const double*& result) {
+    int st = mg_alloc(c);
+    if (st != SIFV_OK) return st;
+    st = ensure_res(c, maxIter);
+    if (st != SIFV_OK) return st;
+    const int dim = c->P.dim;
+    MgLevel L0 = c->mg[0];
+    const long long n0 = L0.n;
+    const unsigned g0 = blocks(n0, kCellThreads);
+    double *x = c->cg[0], *r = c->cg[1], *z = c->cg[2], *p = c->cg[3], *q = c->cg[4], *wInv = c->cg[5];
+    double* s = c->cgScal;
+    double* part = c->cgPartial;
+    MgLevel Lf = L0;
+    Lf.x = x;
+    Lf.b = r;   // the scaled right-hand side lands in r, then r = b - M x in place
+    k_mg_fine<<<g0, kCellThreads, 0, c->stream>>>(c->P, c->F, rho, rhoc2, rhs, c->F.pA, c->ctl, Lf, wInv);
+    for (size_t l = 0; l + 1 < c->mg.size(); ++l)
+        k_mg_coarsen<<<blocks(c->mg[l + 1].n, kCellThreads), kCellThreads, 0, c->stream>>>(c->mg[l], c->mg[l + 1], dim);
+    for (const MgLevel& L : c->mg) k_mg_diag<<<blocks(L.n, kCellThreads), kCellThreads, 0, c->stream>>>(L, dim);
+    // |rhs|^2 into s[4], then r = b - M x and |r/m|^2 into s[2]
+    k_mg_bnorm<<<g0, kCellThreads, 0, c->stream>>>(n0, r, wInv, part);
+    k_mg_sum<<<1, 1024, 0, c->stream>>>(part, (int)g0, s, 4);
+    Lf.b = r;
+    k_mg_residual0<<<g0, kCellThreads, 0, c->stream>>>(Lf, dim, wInv, r, part);
+    k_mg_sum<<<1, 1024, 0, c->stream>>>(part, (int)g0, s, 2);
+    c->launches += 6 + 2 * (int)c->mg.size();
+    LAUNCH_CHECK(c);
+    double hs[5];
+    CUDA_TRY(c, cudaMemcpyAsync(hs, s, sizeof(hs), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    const double bb = hs[4], eps = tol * tol;
+    double rr = hs[2];
+    int it = 0;
+    if (bb == 0.0) {   // Hypre: zero right-hand side -> zero solution
+        CUDA_TRY(c, cudaMemsetAsync(x, 0, sizeof(double) * n0, c->stream));
+        rr = 0.0;
+    } else if (!(rr <= eps * bb)) {
+        mg_vcycle(c, 0, r, z);
+        k_mg_dot<<<g0, kCellThreads, 0, c->stream>>>(n0, r, z, part);
+        k_mg_sum<<<1, 1024, 0, c->stream>>>(part, (int)g0, s, 0);
+        k_cg_direction<<<g0, kCellThreads, 0, c->stream>>>(n0, s, z, p, 1);
+        c->launches += 3;
+        while (it < maxIter) {
+            ++it;
+            k_mg_matvec_dot<<<g0, kCellThreads, 0, c->stream>>>(L0, dim, p, q, part);
+            k_mg_sum<<<1, 1024, 0, c->stream>>>(part, (int)g0, s, 1);
+            k_cg_update<<<g0, kCellThreads, 0, c->stream>>>(n0, s, x, r, p, q, wInv, part);
+            k_mg_sum<<<1, 1024, 0, c->stream>>>(part, (int)g0, s, 2);
+            c->launches += 4;
+            LAUNCH_CHECK(c);
+            CUDA_TRY(c, cudaMemcpyAsync(&hs[2], s + 2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+            rr = hs[2];
+            if (rr <= eps * bb || !(rr == rr)) break;
+            mg_vcycle(c, 0, r, z);
+            k_mg_dot<<<g0, kCellThreads, 0, c->stream>>>(n0, r, z, part);
+            k_mg_sum<<<1, 1024, 0, c->stream>>>(part, (int)g0, s, 3);
+            k_cg_direction<<<g0, kCellThreads, 0, c->stream>>>(n0, s, z, p, 0);
+            k_cg_shift<<<1, 1, 0, c->stream>>>(s);
+            c->launches += 4;
+        }
+    }
+    k_mg_scatter<<<g0, kCellThreads, 0, c->stream>>>(c->P, Lf, c->F.pA);
+    c->launches++;
+    LAUNCH_CHECK(c);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    // relative residual of the last iteration where the semi-implicit step looks for it
+    const double rel = (bb > 0.0) ? std::sqrt(rr / bb) : 0.0;
+    iters = it;
+    if (it > 0) std::memcpy(&c->ctlHost->res[it - 1], &rel, sizeof(double));
+    result = c->F.pA;
+    mark(c, "pcg_mg");
+    return SIFV_OK;
+}
+
 int pressure_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rhs, double tol, int maxIter,
                  int& iters, const double*& result) {
+    if (c->pressureKind == 2) return mg_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
     if (c->pressureKind == 1) return gs_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
     return jacobi_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
 }
@@ -1144,7 +1303,7 @@ int sifv_pressure_solve(sifv_ctx_t* c, const double* rho, const double* rhoc2, c
     const double* res = nullptr;
     int st = pressure_run(c, dRho, dRhoc2, dRhs, tol, maxIter, n, res);
     if (st != SIFV_OK) return st;
-    if (c->pressureKind == 1)   // in place on pA; the ghosts keep their last fill, as the reference's array
+    if (c->pressureKind >= 1)   // in place on pA; the ghosts keep their last fill, as the reference's array
         CUDA_TRY(c, cudaMemcpyAsync(dP, c->F.pA, bytes, cudaMemcpyDeviceToDevice, c->stream));
     else
         k_jacobi_finish<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(
@@ -1202,7 +1361,7 @@ int sifv_advective_dt(sifv_ctx_t* c, double cfl, double maxDt, double* dt) {
 
 int sifv_set_pressure_solver(sifv_ctx_t* c, int kind) {
     if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
-    if (kind != SIFV_PRESSURE_JACOBI && kind != SIFV_PRESSURE_GAUSS_SEIDEL)
+    if (kind != SIFV_PRESSURE_JACOBI && kind != SIFV_PRESSURE_GAUSS_SEIDEL && kind != SIFV_PRESSURE_PCG_MG)
         return fail(c, SIFV_ERR_BAD_ARG, "unknown pressure solver");
     c->pressureKind = kind;
     return SIFV_OK;

@@ -307,9 +307,12 @@ public:
         : CudaStepperBase(std::move(riemannSolver), std::move(eos), config, device, SIFV_PREC_FP64, sync),
           pressure_(std::move(pressureSolver)) {
         if (!config.semiImplicit) throw std::invalid_argument("CudaSemiImplicitSolver needs semiImplicit == true");
-        if (pressure_ && pressure_->name() == "GaussSeidel") pressureKind_ = SIFV_PRESSURE_GAUSS_SEIDEL;
-        else if (pressure_ && pressure_->name() != "Jacobi")
-            throw std::invalid_argument("the CUDA semi-implicit step solves the pressure with Jacobi or GaussSeidel");
+        const std::string kind = pressure_ ? pressure_->name() : std::string("Jacobi");
+        if (kind == "GaussSeidel") pressureKind_ = SIFV_PRESSURE_GAUSS_SEIDEL;
+        else if (kind == "PCG+MG" || kind == "HyprePCG+PFMG") pressureKind_ = SIFV_PRESSURE_PCG_MG;
+        else if (kind != "Jacobi")
+            throw std::invalid_argument(
+                "the CUDA semi-implicit step solves the pressure with Jacobi, GaussSeidel or PCG+MG");
     }
 
     double step(const SimulationConfig& config, const RectilinearMesh& mesh, SolutionState& state,
@@ -328,8 +331,9 @@ private:
 };
 
 // Drop-in PressureSolver (include/PressureSolver.hpp:13-41) on the GPU: the
-// Jacobi iteration of src/JacobiPressureSolver.cpp or the Gauss-Seidel sweeps
-// of src/GaussSeidelPressureSolver.cpp.  Host arrays in, host arrays out; the
+// Jacobi iteration of src/JacobiPressureSolver.cpp, the Gauss-Seidel sweeps
+// of src/GaussSeidelPressureSolver.cpp, or conjugate gradients with a
+// multigrid V-cycle in place of HyprePressureSolver (PCG+PFMG).  Host arrays in, host arrays out; the
 // device context is cached per mesh.
 class CudaPressureSolverPlugin : public PressureSolver {
 public:
@@ -350,7 +354,9 @@ public:
         return run(mesh, &halo, rho, rhoc2, rhs, pressure, dt, tolerance, maxIter);
     }
 
-    std::string name() const override { return kind_ == SIFV_PRESSURE_GAUSS_SEIDEL ? "GaussSeidel" : "Jacobi"; }
+    std::string name() const override {
+        return kind_ == SIFV_PRESSURE_GAUSS_SEIDEL ? "GaussSeidel" : kind_ == SIFV_PRESSURE_PCG_MG ? "PCG+MG" : "Jacobi";
+    }
 
 private:
     int run(const RectilinearMesh& mesh, const HaloExchange* halo, const std::vector<double>& rho,
@@ -393,6 +399,14 @@ class CudaGaussSeidelPressureSolver : public CudaPressureSolverPlugin {
 public:
     explicit CudaGaussSeidelPressureSolver(int device = 0)
         : CudaPressureSolverPlugin(SIFV_PRESSURE_GAUSS_SEIDEL, device) {}
+};
+
+// In place of HyprePressureSolver (include/HyprePressureSolver.hpp), which
+// needs Hypre: the same system, Neumann faces on physical boundaries, the
+// same two-norm relative-residual stopping rule; returns the CG iterations.
+class CudaPcgMgPressureSolver : public CudaPressureSolverPlugin {
+public:
+    explicit CudaPcgMgPressureSolver(int device = 0) : CudaPressureSolverPlugin(SIFV_PRESSURE_PCG_MG, device) {}
 };
 
 }  // namespace b200

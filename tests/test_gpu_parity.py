@@ -352,3 +352,22 @@ def test_immersed_boundary_rejected_where_unsupported():
     with pytest.raises(abi.AbiError) as e:
         cf.set_immersed_bodies(bodies)
     assert e.value.status == abi.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("kind", [abi.PRESSURE_JACOBI, abi.PRESSURE_GAUSS_SEIDEL])
+def test_standalone_solve_with_more_iterations_than_the_config(kind):
+    """A standalone solve allowed more iterations than maxPressureIters grows
+    the residual history and keeps dt."""
+    case = cases.acoustic3d(10)
+    case[0].maxPressureIters = 20
+    cg = backends.make(backends.cuda(), case)
+    co = backends.make(backends.oracle(), case)
+    cg.set_pressure_solver(kind)
+    co.set_pressure_solver(kind)
+    rng = np.random.default_rng(5)
+    n = cg.ncells
+    args = (1.0 + 0.1 * rng.random(n), 1.4 + 0.2 * rng.random(n), rng.random(n), rng.random(n))
+    pg, ig, _ = cg.pressure_solve(*args, 0.1, 1e-12, 500)
+    po, io, _ = co.pressure_solve(*args, 0.1, 1e-12, 500)
+    assert ig == io and ig > 20
+    assert np.array_equal(cg.interior(pg), co.interior(po))
