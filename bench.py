@@ -426,35 +426,55 @@ def run_cuda(args):
         return out
 
     def measure_semi_implicit():
-        """Semi-implicit step with IGR and the Jacobi pressure solve."""
-        case = cases.acoustic3d(SI_N)
-        ctx = backends.cuda().create(case[0], case[1], local)
-        ctx.set_state(case[2])
-        t_sim = 0.0
-        for q in range(SI_WARM):                   # step 0 runs the 50-sweep IGR warm start
-            t_sim += ctx.step(q, t_sim, -1.0)
-        iters = []
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for q in range(SI_STEPS):
-            t_sim += ctx.step(SI_WARM + q, t_sim, -1.0)
-            iters.append(ctx.last_pressure_iterations())
-        torch.cuda.synchronize()
-        sec = time.perf_counter() - t0
-        fam = ctx.profile_step(SI_WARM + SI_STEPS, t_sim, -1.0)
-        ctx.close()
+        """Semi-implicit step with IGR and the Jacobi pressure solve: FP64 (the
+        reference order, bit-identical to the oracle) and mixed (FP32 inner
+        Jacobi sweeps inside FP64 refinement), with the mixed state's L1 / Linf
+        error against the FP64 one after the same steps."""
+        def run(precision):
+            case = cases.acoustic3d(SI_N)
+            case[0].precision = precision
+            ctx = backends.cuda().create(case[0], case[1], local)
+            ctx.set_state(case[2])
+            t_sim = 0.0
+            for q in range(SI_WARM):                   # step 0 runs the 50-sweep IGR warm start
+                t_sim += ctx.step(q, t_sim, -1.0)
+            iters = []
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for q in range(SI_STEPS):
+                t_sim += ctx.step(SI_WARM + q, t_sim, -1.0)
+                iters.append(ctx.last_pressure_iterations())
+            torch.cuda.synchronize()
+            sec = time.perf_counter() - t0
+            fields = {f: ctx.interior(ctx.get_field(f)).copy() for f in (abi.F_RHO, abi.F_RHOU, abi.F_RHOE, abi.F_PRES)}
+            fam = ctx.profile_step(SI_WARM + SI_STEPS, t_sim, -1.0)
+            ctx.close()
+            return case, sec, iters, fields, fam
+
+        case, sec, iters, f64, fam = run(abi.PREC_FP64)
+        _, sec_m, iters_m, fmx, fam_m = run(abi.PREC_MIXED)
         cells = SI_N ** 3
         val = cells * SI_STEPS / sec
+        val_m = cells * SI_STEPS / sec_m
         kj = float(np.mean(iters))
         nigr = case[0].IGRIters
         bpc = 272 + 32 * nigr + 40 * kj
+        err = {}
+        for f, name in ((abi.F_RHO, "rho"), (abi.F_RHOU, "rhoU"), (abi.F_RHOE, "rhoE"), (abi.F_PRES, "pres")):
+            d = np.abs(fmx[f] - f64[f])
+            err[name] = {"l1_rel": float(d.mean() / np.abs(f64[f]).mean()),
+                         "linf_rel": float(d.max() / np.abs(f64[f]).max())}
         return {"workload": f"3D acoustic pulse {SI_N}^3 periodic, semi-implicit RK1 + IGR ({nigr} sweeps), "
                             f"WENO5+HLLC, advective CFL 0.8 (dt = maxDt 1e-2), Jacobi tol 1e-6",
                 "metric": "cell-updates/s", "value": val, "steps": SI_STEPS, "ms_per_step": sec / SI_STEPS * 1e3,
                 "precision": "fp64", "jacobi_iterations": iters,
                 "family_ms_per_step": {k: v[0] for k, v in fam.items()},
                 "roofline": {"bound": "hbm", "bytes_per_cell_update": bpc, "achieved": bpc * val / 1e9,
-                             "unit": "GB/s"}}
+                             "unit": "GB/s"},
+                "mixed": {"precision": "FP32 inner Jacobi sweeps + FP64 refinement, rest FP64",
+                          "value": val_m, "ms_per_step": sec_m / SI_STEPS * 1e3, "jacobi_iterations": iters_m,
+                          "family_ms_per_step": {k: v[0] for k, v in fam_m.items()},
+                          "error_vs_fp64": err}}
 
     def measure_adjoint():
         """Forward (recording) and reverse sweep of the vortex adjoint."""

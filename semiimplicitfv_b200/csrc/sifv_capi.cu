@@ -99,6 +99,12 @@ struct sifv_ctx {
     double* cg[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // x r z p q 1/m
     double* cgScal = nullptr;    // 8 device scalars
     double* cgPartial = nullptr; // block partial sums of the fine level
+    // mixed-precision Jacobi (semi-implicit SIFV_PREC_MIXED)
+    double* mxCoef = nullptr;    // k_jacobi_coef layout, FP64
+    float* mxW = nullptr;        // 2 dim FP32 weights per cell
+    float* mxD = nullptr;        // FP32 delta
+    float* mxE[2] = {nullptr, nullptr};
+    int lastInPlace = 0;         // the last pressure solve left its result in F.pA
 };
 
 namespace {
@@ -644,8 +650,79 @@ int mg_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
     return SIFV_OK;
 }
 
+// JacobiPressureSolver::solve with FP32 inner sweeps and FP64 refinement
+// (SIFV_PREC_MIXED semi-implicit step): batches of FP32 sweeps between FP64
+// Jacobi changes; result in place in F.pA.
+int jacobi_mixed_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rhs, double tol, int maxIter,
+                     int& iters, const double*& result) {
+    int st = ensure_res(c, maxIter);
+    if (st != SIFV_OK) return st;
+    const Params& P = c->P;
+    const long long n = (long long)c->nint;
+    if (!c->mxCoef) {
+        int sa = SIFV_OK;
+        c->mxCoef = dalloc(c, c->ncells * (size_t)(2 * P.dim + 2), sa);
+        if (sa != SIFV_OK) return sa;
+        void* p = nullptr;
+        const size_t fl = sizeof(float) * (size_t)n;
+        CUDA_TRY(c, cudaMalloc(&p, fl * (size_t)(2 * P.dim + 3)));
+        c->allocs.push_back(p);
+        c->mxW = static_cast<float*>(p);
+        c->mxD = c->mxW + (size_t)(2 * P.dim) * n;
+        c->mxE[0] = c->mxD + n;
+        c->mxE[1] = c->mxE[0] + n;
+    }
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->jacobiDone, 0, sizeof(int), c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->ctl->res, 0, sizeof(unsigned long long) * (size_t)maxIter, c->stream));
+    const unsigned g = blocks(n, kCellThreads);
+    k_jacobi_coef<<<g, kCellThreads, 0, c->stream>>>(P, rho, rhoc2, c->F, c->ctl, c->mxCoef, c->ncells);
+    k_mx_weights<<<g, kCellThreads, 0, c->stream>>>(P, c->mxCoef, c->ncells, c->mxW, n);
+    c->launches += 2;
+    constexpr int kInner = 8;   // FP32 sweeps per FP64 refinement
+    int it = 0, done = 0;
+    while (it < maxIter && !done) {
+        // iteration `it` in FP64: the change at p, also e_1
+        k_mx_delta<<<g, kCellThreads, 0, c->stream>>>(P, c->mxCoef, c->ncells, rhs, c->F.pA, c->mxD, c->mxE[0],
+                                                       c->ctl, it);
+        int cur = 0;
+        const int first = it;
+        ++it;
+        for (int q = 1; q < kInner && it < maxIter; ++q, ++it) {
+            k_mx_sweep<<<g, kCellThreads, 0, c->stream>>>(P, c->mxW, c->mxD, c->mxE[cur], c->mxE[cur ^ 1], c->ctl, it,
+                                                          tol);
+            cur ^= 1;
+        }
+        c->launches += it - first;
+        LAUNCH_CHECK(c);
+        CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl) + sizeof(unsigned long long) * (size_t)it,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        int last = it;   // iterations whose update is in e
+        if (c->ctlHost->jacobiDone) {
+            done = last = c->ctlHost->jacobiDone;
+        } else {
+            double lr;
+            unsigned long long b = c->ctlHost->res[it - 1];
+            std::memcpy(&lr, &b, sizeof(double));
+            if (lr < tol) done = it;
+        }
+        // the buffer written by the last sweep that ran: sweep q (1-based in the batch) writes mxE[q & 1]
+        const int ran = last - first;   // 1 .. kInner
+        k_mx_apply<<<g, kCellThreads, 0, c->stream>>>(P, c->mxE[(ran - 1) & 1], c->F.pA);
+        c->launches++;
+    }
+    iters = done ? done : maxIter;
+    result = c->F.pA;
+    c->lastInPlace = 1;
+    mark(c, "jacobi_mixed");
+    return SIFV_OK;
+}
+
 int pressure_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rhs, double tol, int maxIter,
                  int& iters, const double*& result) {
+    c->lastInPlace = (c->pressureKind != 0) ? 1 : 0;
+    if (c->pressureKind == 0 && c->cfg.precision == SIFV_PREC_MIXED)
+        return jacobi_mixed_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
     if (c->pressureKind == 2) return mg_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
     if (c->pressureKind == 1) return gs_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
     return jacobi_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
@@ -918,14 +995,16 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     std::string m;
     int st = validate(cfg, m);
     if (st != SIFV_OK) return fail(nullptr, st, m);
-    if (cfg->precision != SIFV_PREC_FP64) {
+    const bool semiMixed = cfg->semiImplicit && cfg->precision == SIFV_PREC_MIXED;
+    if (cfg->precision != SIFV_PREC_FP64 && !semiMixed) {
         bool bf = false;
         for (int d = 0; d < 3; ++d) bf = bf || cfg->bfA[d] != 0.0 || cfg->bfB[d] != 0.0;
         const bool visc = cfg->mu > 0.0 || cfg->nPhaseMu > 0 || cfg->stSigma > 0.0;
         if (cfg->semiImplicit || cfg->nPhases > 0 || cfg->useIGR || cfg->reconOrder != SIFV_WENO5 || bf || visc)
             return fail(nullptr, SIFV_ERR_UNSUPPORTED,
                         "SIFV_PREC_MIXED / SIFV_PREC_FP64_FAST run the explicit single-phase WENO5 step without "
-                        "IGR, body force, viscosity or surface tension; use SIFV_PREC_FP64 for this configuration");
+                        "IGR, body force, viscosity or surface tension (the semi-implicit step takes SIFV_PREC_MIXED: "
+                        "FP32 inner Jacobi sweeps); use SIFV_PREC_FP64 for this configuration");
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -1074,7 +1153,7 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
             cudaMemcpyAsync(g[q], src[q]->data(), src[q]->size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     }
     F.dx = g[0]; F.dy = g[1]; F.dz = g[2]; F.adx2 = g[3]; F.ady2 = g[4]; F.adz2 = g[5];
-    if (cfg->precision != SIFV_PREC_FP64) {
+    if (cfg->precision != SIFV_PREC_FP64 && !cfg->semiImplicit) {
         c->sweep = true;
         c->rhoP = dalloc(c, n, st);
         c->rhsBuf[0] = dalloc(c, n, st);
@@ -1303,7 +1382,7 @@ int sifv_pressure_solve(sifv_ctx_t* c, const double* rho, const double* rhoc2, c
     const double* res = nullptr;
     int st = pressure_run(c, dRho, dRhoc2, dRhs, tol, maxIter, n, res);
     if (st != SIFV_OK) return st;
-    if (c->pressureKind >= 1)   // in place on pA; the ghosts keep their last fill, as the reference's array
+    if (c->lastInPlace)   // in place on pA; the ghosts keep their last fill, as the reference's array
         CUDA_TRY(c, cudaMemcpyAsync(dP, c->F.pA, bytes, cudaMemcpyDeviceToDevice, c->stream));
     else
         k_jacobi_finish<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(

@@ -1158,6 +1158,104 @@ __global__ void k_jacobi_finish(Params P, const double* __restrict__ pA, const d
     dst[c] = src[c];
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-precision Jacobi (SIFV_PREC_MIXED, semi-implicit): FP32 inner sweeps
+// inside FP64 iterative refinement.  m Jacobi iterations from p are
+// p + e_m with e_0 = 0, e_{k+1} = delta + J e_k, delta = D^-1 (b - A p) the
+// FP64 Jacobi change at p and J = D^-1 (off-diagonal part); the e sweeps run
+// in FP32 on FP32 weights, then p += e in FP64 and delta is re-evaluated in
+// FP64, which removes the FP32 error each batch.  The change |e_{k+1} - e_k|
+// of a sweep is the Jacobi change of that iteration, so the stopping rule
+// (max change < tol) and the iteration count are the reference's
+// (src/JacobiPressureSolver.cpp:57-108) up to FP32 rounding of the change.
+// Compact arrays (interior cells, x fastest); weights w[q * n + t] for the
+// faces x-, x+, y-, y+, z-, z+.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mx_weights(Params P, const double* __restrict__ coef, size_t nc,
+                                                    float* __restrict__ w, long long n) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(P, t, i, j, k)) return;
+    const size_t c = cidx(P, i, j, k);
+    const int nq = 2 * P.dim;
+    const double coeff = coef[(size_t)nq * nc + c], denom = coef[(size_t)(nq + 1) * nc + c];
+    for (int q = 0; q < nq; ++q) w[q * n + t] = (float)(coeff * coef[q * nc + c] / denom);
+}
+
+// FP64 Jacobi change at p (k_jacobi_pre's expressions): delta = p_new - p;
+// e = delta (the first sweep of the batch), max |delta| -> res[it].
+__global__ void __launch_bounds__(256) k_mx_delta(Params P, const double* __restrict__ coef, size_t nc,
+                                                  const double* __restrict__ rhs, const double* __restrict__ pin,
+                                                  float* __restrict__ d32, float* __restrict__ e, Ctl* ctl, int it) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    double res = 0.0;
+    if (int_coords(P, t, i, j, k)) {
+        const int dim = P.dim;
+        const size_t c = cidx(P, i, j, k);
+        const size_t xm = scalar_idx(P, i - 1, j, k), xp = scalar_idx(P, i + 1, j, k);
+        const double* cf = coef + c;
+        double od = 0.0;
+        od += cf[0] * pin[xm] + cf[nc] * pin[xp];
+        if (dim >= 2) od += cf[2 * nc] * pin[scalar_idx(P, i, j - 1, k)] + cf[3 * nc] * pin[scalar_idx(P, i, j + 1, k)];
+        if (dim >= 3) od += cf[4 * nc] * pin[scalar_idx(P, i, j, k - 1)] + cf[5 * nc] * pin[scalar_idx(P, i, j, k + 1)];
+        const double coeff = cf[(size_t)(2 * dim) * nc];
+        const double denom = cf[(size_t)(2 * dim + 1) * nc];
+        const double dl = (rhs[c] + coeff * od) / denom - pin[c];
+        d32[t] = (float)dl;
+        e[t] = (float)dl;
+        res = fabs(dl);
+    }
+    block_max_to(res, &ctl->res[it]);
+}
+
+// compact neighbour of interior cell (i, j, k) along an axis under the scalar
+// ghost map (periodic wrap, else the boundary cell itself)
+__device__ __forceinline__ long long mx_nb(const Params& P, int i, int j, int k, int axis, int side) {
+    int q[3] = {i, j, k};
+    const int n[3] = {P.nx, P.ny, P.nz};
+    int v = q[axis] + side;
+    if (v < 0) v = (P.bc[2 * axis] == SIFV_BC_PERIODIC) ? n[axis] - 1 : 0;
+    else if (v >= n[axis]) v = (P.bc[2 * axis + 1] == SIFV_BC_PERIODIC) ? 0 : n[axis] - 1;
+    q[axis] = v;
+    return q[0] + (long long)P.nx * (q[1] + (long long)P.ny * q[2]);
+}
+
+// One FP32 sweep e_out = delta + J e_in, iteration `it` of the count; a no-op
+// once an earlier iteration's change fell below tol (as k_jacobi_pre).
+__global__ void __launch_bounds__(256) k_mx_sweep(Params P, const float* __restrict__ w, const float* __restrict__ d32,
+                                                  const float* __restrict__ ein, float* __restrict__ eout, Ctl* ctl,
+                                                  int it, double tol) {
+    if (ctl->jacobiDone) return;
+    if (it > 0 && bits2d(ctl->res[it - 1]) < tol) {
+        if (threadIdx.x == 0) ctl->jacobiDone = it;
+        return;
+    }
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    double res = 0.0;
+    if (int_coords(P, t, i, j, k)) {
+        const long long n = (long long)P.nx * P.ny * P.nz;
+        float od = w[t] * ein[mx_nb(P, i, j, k, 0, -1)] + w[n + t] * ein[mx_nb(P, i, j, k, 0, 1)];
+        if (P.dim >= 2)
+            od += w[2 * n + t] * ein[mx_nb(P, i, j, k, 1, -1)] + w[3 * n + t] * ein[mx_nb(P, i, j, k, 1, 1)];
+        if (P.dim >= 3)
+            od += w[4 * n + t] * ein[mx_nb(P, i, j, k, 2, -1)] + w[5 * n + t] * ein[mx_nb(P, i, j, k, 2, 1)];
+        const float en = d32[t] + od;
+        eout[t] = en;
+        res = (double)fabsf(en - ein[t]);
+    }
+    block_max_to(res, &ctl->res[it]);
+}
+
+// p += e (interior cells of the ghosted FP64 array)
+__global__ void __launch_bounds__(256) k_mx_apply(Params P, const float* __restrict__ e, double* __restrict__ p) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!int_coords(P, t, i, j, k)) return;
+    p[cidx(P, i, j, k)] += (double)e[t];
+}
+
 // SemiImplicitSolver::correctionStep (src/SemiImplicitSolver.cpp:590-678),
 // all per-cell parts fused: momentum from the face-averaged gradient of
 // p + sigma (scalar-ghost-filled), velocities, pres = p, and total energy
