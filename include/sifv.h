@@ -422,6 +422,11 @@ int sifv_tangent_set_direction(sifv_ctx_t* ctx, int field, const double* dir, in
 int sifv_tangent_forward(sifv_ctx_t* ctx, int step0, double time0, double tEnd, int maxSteps,
                          const double* dtSchedule, int nSchedule, double* timeOut, int* stepsOut);
 int sifv_tangent_get(sifv_ctx_t* ctx, int field, double* out, int onDevice);
+/* Arithmetic of the reverse sweep's local Jacobians (the flux and
+ * reconstruction derivatives of every face): SIFV_PREC_FP64 (default) or
+ * SIFV_PREC_MIXED (FP32; the forward trajectory, the adjoint state and the
+ * accumulation of the face shares stay FP64). */
+int sifv_adjoint_set_precision(sifv_ctx_t* ctx, int precision);
 
 /* ---- batched ensembles -------------------------------------------------- */
 /* Many independent 1D problems of different sizes (same configuration and

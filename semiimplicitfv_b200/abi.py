@@ -219,6 +219,7 @@ _OPTIONAL_SIGS = {
     "tangent_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
                                   C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "tangent_get": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "adjoint_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "ensemble_create": (C.c_int, [C.POINTER(Config), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                   C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_void_p)]),
     "ensemble_destroy": (C.c_int, [C.c_void_p]),
@@ -515,6 +516,10 @@ class Context:
         self._check(self.be.fn["adjoint_forward"](self.h, step0, time0, t_end, max_steps, every, p, n,
                                                   C.byref(t), C.byref(k)))
         return t.value, k.value
+
+    def adjoint_set_precision(self, precision: int):
+        """PREC_FP64 or PREC_MIXED (FP32 local Jacobians in the reverse sweep)."""
+        self._check(self.be.fn["adjoint_set_precision"](self.h, precision))
 
     def adjoint_schedule(self) -> np.ndarray:
         n = C.c_int()

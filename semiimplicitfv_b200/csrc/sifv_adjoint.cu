@@ -11,11 +11,17 @@ long long nfaces(const Params& P, int d) {
     return (long long)(P.nx + (d == 0)) * (P.ny + (d == 1)) * (P.nz + (d == 2));
 }
 
+template <int DIM, typename S>
+void adj_faces(const AdjArgs& A, cudaStream_t s) {
+    k_adj_face<0, DIM, S><<<nblocks(nfaces(A.P, 0), 128), 128, 0, s>>>(A);
+    if (DIM >= 2) k_adj_face<(DIM >= 2 ? 1 : 0), DIM, S><<<nblocks(nfaces(A.P, 1), 128), 128, 0, s>>>(A);
+    if (DIM >= 3) k_adj_face<(DIM >= 3 ? 2 : 0), DIM, S><<<nblocks(nfaces(A.P, 2), 128), 128, 0, s>>>(A);
+}
+
 template <int DIM>
 void adj_stage(const AdjArgs& A, cudaStream_t s) {
-    k_adj_face<0, DIM><<<nblocks(nfaces(A.P, 0), 128), 128, 0, s>>>(A);
-    if (DIM >= 2) k_adj_face<(DIM >= 2 ? 1 : 0), DIM><<<nblocks(nfaces(A.P, 1), 128), 128, 0, s>>>(A);
-    if (DIM >= 3) k_adj_face<(DIM >= 3 ? 2 : 0), DIM><<<nblocks(nfaces(A.P, 2), 128), 128, 0, s>>>(A);
+    if (A.fp32) adj_faces<DIM, float>(A, s);
+    else adj_faces<DIM, double>(A, s);
     const long long n = (long long)A.P.nx * A.P.ny * A.P.nz;
     k_adj_cell<DIM><<<nblocks(n, 128), 128, 0, s>>>(A);
 }

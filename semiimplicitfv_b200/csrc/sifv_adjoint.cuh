@@ -96,7 +96,9 @@ __device__ __forceinline__ const T& flux_comp(const FaceFlux<0, T>& Fx, int q, i
 //   side 0: left state, stencil cells f-3..f+1 (k = 0..4)
 //   side 1: right state, stencil cells f-2..f+2
 // ---------------------------------------------------------------------------
-template <int DIR, int DIM>
+// S: the arithmetic of the local Jacobians (double; float for the FP32
+// reverse sweep, whose shares are still stored and gathered in FP64).
+template <int DIR, int DIM, typename S>
 __global__ void __launch_bounds__(128) k_adj_face(AdjArgs A) {
     constexpr int NVN = NV<DIM>::n;
     constexpr int ND = 2 * NVN;
@@ -115,7 +117,7 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjArgs A) {
     const int dim = DIM;
 
     // mu = dJ/dF (cons order)
-    double mu[NVN];
+    S mu[NVN];
     {
         const bool rIn = pos < nd, lIn = pos >= 1;
         const int li = (DIR == 0) ? i - 1 : i, lj = (DIR == 1) ? j - 1 : j, lk = (DIR == 2) ? k - 1 : k;
@@ -125,27 +127,28 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjArgs A) {
         for (int q = 0; q < NVN; ++q) {
             double lr = rIn ? A.lam[q][base] : 0.0;
             double ll = lIn ? A.lam[q][base - st] : 0.0;
-            mu[q] = cR * lr - cL * ll;
+            mu[q] = (S)(cR * lr - cL * ll);
         }
     }
     const bool weno = (P.reconOrder == SIFV_WENO5);
     // reconstruction values and stencil gradients
-    double WL[NVN], WR[NVN], dL[NVN][5], dR[NVN][5];
+    S WL[NVN], WR[NVN], dL[NVN][5], dR[NVN][5];
 #pragma unroll
     for (int v = 0; v < NVN; ++v) {
         const double* f = prim_ptr(F, v, dim);
-        double s[6];
+        S s[6];
 #pragma unroll
-        for (int q = 0; q < 6; ++q) s[q] = f[base + (q - 3) * st];
+        for (int q = 0; q < 6; ++q) s[q] = (S)f[base + (q - 3) * st];
         // left state: stencil cells 0..4, right state: cells 1..5 (each seeded 0..4)
-        Dual<5> x[5], l, rr;
-        const Dual<5> e5(P.wenoEps);
+        using D5 = Dual<5, S>;
+        D5 x[5], l, rr;
+        const D5 e5(P.wenoEps);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) x[q] = Dual<5>::seed(s[q], q);
-        l = weno ? weno5L<Dual<5>>(x[0], x[1], x[2], x[3], x[4], e5) : upwind5L<Dual<5>>(x[0], x[1], x[2], x[3], x[4]);
+        for (int q = 0; q < 5; ++q) x[q] = D5::seed(s[q], q);
+        l = weno ? weno5L<D5>(x[0], x[1], x[2], x[3], x[4], e5) : upwind5L<D5>(x[0], x[1], x[2], x[3], x[4]);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) x[q] = Dual<5>::seed(s[q + 1], q);
-        rr = weno ? weno5R<Dual<5>>(x[0], x[1], x[2], x[3], x[4], e5) : upwind5R<Dual<5>>(x[0], x[1], x[2], x[3], x[4]);
+        for (int q = 0; q < 5; ++q) x[q] = D5::seed(s[q + 1], q);
+        rr = weno ? weno5R<D5>(x[0], x[1], x[2], x[3], x[4], e5) : upwind5R<D5>(x[0], x[1], x[2], x[3], x[4]);
         WL[v] = l.v;
         WR[v] = rr.v;
 #pragma unroll
@@ -155,27 +158,27 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjArgs A) {
         }
     }
     // flux Jacobian w.r.t. (WL, WR)
-    FaceState<0, Dual<ND>> L, R;
-    L.rho = Dual<ND>::seed(WL[0], 0);
-    R.rho = Dual<ND>::seed(WR[0], NVN);
+    FaceState<0, Dual<ND, S>> L, R;
+    L.rho = Dual<ND, S>::seed(WL[0], 0);
+    R.rho = Dual<ND, S>::seed(WR[0], NVN);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        L.u[d] = (d < DIM) ? Dual<ND>::seed(WL[1 + d], 1 + d) : Dual<ND>(0.0);
-        R.u[d] = (d < DIM) ? Dual<ND>::seed(WR[1 + d], NVN + 1 + d) : Dual<ND>(0.0);
+        L.u[d] = (d < DIM) ? Dual<ND, S>::seed(WL[1 + d], 1 + d) : Dual<ND, S>(0.0);
+        R.u[d] = (d < DIM) ? Dual<ND, S>::seed(WR[1 + d], NVN + 1 + d) : Dual<ND, S>(0.0);
     }
-    L.p = Dual<ND>::seed(WL[DIM + 1], DIM + 1);
-    R.p = Dual<ND>::seed(WR[DIM + 1], NVN + DIM + 1);
-    L.sigma = R.sigma = Dual<ND>(0.0);
-    L.gEff = R.gEff = Dual<ND>(P.gamma);
-    L.piEff = R.piEff = Dual<ND>(P.pInf);
-    FaceFlux<0, Dual<ND>> Fx;
-    riemann_T<DIR, Dual<ND>>(P, L, R, Fx);
-    double gW[ND];
+    L.p = Dual<ND, S>::seed(WL[DIM + 1], DIM + 1);
+    R.p = Dual<ND, S>::seed(WR[DIM + 1], NVN + DIM + 1);
+    L.sigma = R.sigma = Dual<ND, S>(0.0);
+    L.gEff = R.gEff = Dual<ND, S>(P.gamma);
+    L.piEff = R.piEff = Dual<ND, S>(P.pInf);
+    FaceFlux<0, Dual<ND, S>> Fx;
+    riemann_T<DIR, Dual<ND, S>>(P, L, R, Fx);
+    S gW[ND];
 #pragma unroll
-    for (int a = 0; a < ND; ++a) gW[a] = 0.0;
+    for (int a = 0; a < ND; ++a) gW[a] = S(0);
 #pragma unroll
     for (int q = 0; q < NVN; ++q) {
-        const Dual<ND>& fq = flux_comp(Fx, q, dim);
+        const Dual<ND, S>& fq = flux_comp(Fx, q, dim);
 #pragma unroll
         for (int a = 0; a < ND; ++a) gW[a] += mu[q] * fq.d[a];
     }
@@ -184,8 +187,8 @@ __global__ void __launch_bounds__(128) k_adj_face(AdjArgs A) {
     for (int v = 0; v < NVN; ++v) {
 #pragma unroll
         for (int q = 0; q < 5; ++q) {
-            sh[(size_t)((0 * 5 + q) * NVN + v) * tot + t] = gW[v] * dL[v][q];
-            sh[(size_t)((1 * 5 + q) * NVN + v) * tot + t] = gW[NVN + v] * dR[v][q];
+            sh[(size_t)((0 * 5 + q) * NVN + v) * tot + t] = (double)(gW[v] * dL[v][q]);
+            sh[(size_t)((1 * 5 + q) * NVN + v) * tot + t] = (double)(gW[NVN + v] * dR[v][q]);
         }
     }
 }

@@ -17,6 +17,7 @@ struct AdjArgs {
     double dt, a1, a2, a3;   // dt and c1/c4, c2/c4, c3/c4 of the stage
     const double* dtDev;     // non-null: dt is read from device memory (the step's CFL dt)
     int stage0;          // stage 0 of a step: lam += acc0, acc0 = 0
+    int fp32;            // local Jacobians of the reverse sweep in FP32
     double* tan[5];      // tangent dU (interior cells)
     double* tan0[5];     // tangent of the step-start state
     double* tanW[5];     // tangent of the primitives (all cells)

@@ -105,6 +105,7 @@ struct sifv_ctx {
     float* mxD = nullptr;        // FP32 delta
     float* mxE[2] = {nullptr, nullptr};
     int lastInPlace = 0;         // the last pressure solve left its result in F.pA
+    int adjFp32 = 0;             // FP32 local Jacobians in the reverse sweep
 };
 
 namespace {
@@ -1545,6 +1546,7 @@ AdjArgs adj_args(sifv_ctx* c) {
         A.share[d] = c->share[d];
         for (int q = 0; q < 5; ++q) A.tanF[d][q] = c->tanF[d][q];
     }
+    A.fp32 = c->adjFp32;
     return A;
 }
 
@@ -1685,6 +1687,14 @@ int sifv_adjoint_schedule(const sifv_ctx_t* c, double* dts, int cap, int* n) {
     if (!c || !n) return SIFV_ERR_BAD_ARG;
     *n = (int)c->adjDts.size();
     if (dts) std::memcpy(dts, c->adjDts.data(), sizeof(double) * std::min<size_t>(cap > 0 ? cap : 0, c->adjDts.size()));
+    return SIFV_OK;
+}
+
+int sifv_adjoint_set_precision(sifv_ctx_t* c, int precision) {
+    if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
+    if (precision != SIFV_PREC_FP64 && precision != SIFV_PREC_MIXED)
+        return fail(c, SIFV_ERR_BAD_ARG, "the reverse sweep runs in SIFV_PREC_FP64 or SIFV_PREC_MIXED");
+    c->adjFp32 = (precision == SIFV_PREC_MIXED) ? 1 : 0;
     return SIFV_OK;
 }
 

@@ -1,7 +1,8 @@
 // sifv_dual.cuh -- forward-mode dual numbers for the local Jacobians of the
 // discrete adjoint and the tangent of the explicit step.
 //
-// Dual<N> carries a value and N partial derivatives.  Instantiating the
+// Dual<N, S> carries a value and N partial derivatives in scalar type S
+// (double, or float for the FP32 reverse sweep).  Instantiating the
 // reconstruction and Riemann templates of sifv_device.cuh with T = Dual<N>
 // differentiates exactly the arithmetic the forward step executes: every
 // comparison (wave-speed estimates, HLLC branch selection, smax/smin
@@ -13,18 +14,18 @@
 
 namespace sifv {
 
-template <int N>
+template <int N, typename S = double>
 struct Dual {
-    double v;
-    double d[N];
+    S v;
+    S d[N];
     __device__ __forceinline__ Dual() {}
-    __device__ __forceinline__ Dual(double x) : v(x) {
+    __device__ __forceinline__ Dual(double x) : v((S)x) {
 #pragma unroll
-        for (int q = 0; q < N; ++q) d[q] = 0.0;
+        for (int q = 0; q < N; ++q) d[q] = S(0);
     }
     __device__ __forceinline__ static Dual seed(double x, int q) {
         Dual r(x);
-        r.d[q] = 1.0;
+        r.d[q] = S(1);
         return r;
     }
     __device__ __forceinline__ Dual& operator+=(const Dual& b) {
@@ -46,8 +47,8 @@ struct Dual {
         return *this;
     }
     __device__ __forceinline__ Dual& operator/=(const Dual& b) {
-        const double inv = 1.0 / b.v;
-        const double r = v * inv;
+        const S inv = S(1) / b.v;
+        const S r = v * inv;
 #pragma unroll
         for (int q = 0; q < N; ++q) d[q] = (d[q] - r * b.d[q]) * inv;
         v = r;
@@ -55,79 +56,81 @@ struct Dual {
     }
 };
 
-template <int N>
-__device__ __forceinline__ Dual<N> operator-(const Dual<N>& a) {
-    Dual<N> r;
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator-(const Dual<N, S>& a) {
+    Dual<N, S> r;
     r.v = -a.v;
 #pragma unroll
     for (int q = 0; q < N; ++q) r.d[q] = -a.d[q];
     return r;
 }
-template <int N>
-__device__ __forceinline__ Dual<N> operator+(Dual<N> a, const Dual<N>& b) { return a += b; }
-template <int N>
-__device__ __forceinline__ Dual<N> operator-(Dual<N> a, const Dual<N>& b) { return a -= b; }
-template <int N>
-__device__ __forceinline__ Dual<N> operator*(Dual<N> a, const Dual<N>& b) { return a *= b; }
-template <int N>
-__device__ __forceinline__ Dual<N> operator/(Dual<N> a, const Dual<N>& b) { return a /= b; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator+(Dual<N, S> a, const Dual<N, S>& b) { return a += b; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator-(Dual<N, S> a, const Dual<N, S>& b) { return a -= b; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator*(Dual<N, S> a, const Dual<N, S>& b) { return a *= b; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator/(Dual<N, S> a, const Dual<N, S>& b) { return a /= b; }
 
 // mixed with plain doubles
-template <int N>
-__device__ __forceinline__ Dual<N> operator+(Dual<N> a, double b) { a.v += b; return a; }
-template <int N>
-__device__ __forceinline__ Dual<N> operator+(double b, Dual<N> a) { a.v += b; return a; }
-template <int N>
-__device__ __forceinline__ Dual<N> operator-(Dual<N> a, double b) { a.v -= b; return a; }
-template <int N>
-__device__ __forceinline__ Dual<N> operator-(double b, const Dual<N>& a) { Dual<N> r = -a; r.v += b; return r; }
-template <int N>
-__device__ __forceinline__ Dual<N> operator*(Dual<N> a, double b) {
-    a.v *= b;
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator+(Dual<N, S> a, double b) { a.v += b; return a; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator+(double b, Dual<N, S> a) { a.v += b; return a; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator-(Dual<N, S> a, double b) { a.v -= b; return a; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator-(double b, const Dual<N, S>& a) { Dual<N, S> r = -a; r.v += b; return r; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator*(Dual<N, S> a, double b) {
+    const S sb = (S)b;
+    a.v *= sb;
 #pragma unroll
-    for (int q = 0; q < N; ++q) a.d[q] *= b;
+    for (int q = 0; q < N; ++q) a.d[q] *= sb;
     return a;
 }
-template <int N>
-__device__ __forceinline__ Dual<N> operator*(double b, Dual<N> a) { return a * b; }
-template <int N>
-__device__ __forceinline__ Dual<N> operator/(Dual<N> a, double b) {
-    const double inv = 1.0 / b;
-    a.v /= b;
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator*(double b, Dual<N, S> a) { return a * b; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator/(Dual<N, S> a, double b) {
+    const S sb = (S)b;
+    const S inv = S(1) / sb;
+    a.v /= sb;
 #pragma unroll
     for (int q = 0; q < N; ++q) a.d[q] *= inv;
     return a;
 }
-template <int N>
-__device__ __forceinline__ Dual<N> operator/(double b, const Dual<N>& a) { return Dual<N>(b) / a; }
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> operator/(double b, const Dual<N, S>& a) { return Dual<N, S>(b) / a; }
 
 // comparisons act on values
-template <int N> __device__ __forceinline__ bool operator<(const Dual<N>& a, const Dual<N>& b) { return a.v < b.v; }
-template <int N> __device__ __forceinline__ bool operator>(const Dual<N>& a, const Dual<N>& b) { return a.v > b.v; }
-template <int N> __device__ __forceinline__ bool operator<=(const Dual<N>& a, const Dual<N>& b) { return a.v <= b.v; }
-template <int N> __device__ __forceinline__ bool operator>=(const Dual<N>& a, const Dual<N>& b) { return a.v >= b.v; }
-template <int N> __device__ __forceinline__ bool operator<(const Dual<N>& a, double b) { return a.v < b; }
-template <int N> __device__ __forceinline__ bool operator>(const Dual<N>& a, double b) { return a.v > b; }
-template <int N> __device__ __forceinline__ bool operator<=(const Dual<N>& a, double b) { return a.v <= b; }
-template <int N> __device__ __forceinline__ bool operator>=(const Dual<N>& a, double b) { return a.v >= b; }
-template <int N> __device__ __forceinline__ bool operator<(double a, const Dual<N>& b) { return a < b.v; }
-template <int N> __device__ __forceinline__ bool operator>(double a, const Dual<N>& b) { return a > b.v; }
+template <int N, typename S> __device__ __forceinline__ bool operator<(const Dual<N, S>& a, const Dual<N, S>& b) { return a.v < b.v; }
+template <int N, typename S> __device__ __forceinline__ bool operator>(const Dual<N, S>& a, const Dual<N, S>& b) { return a.v > b.v; }
+template <int N, typename S> __device__ __forceinline__ bool operator<=(const Dual<N, S>& a, const Dual<N, S>& b) { return a.v <= b.v; }
+template <int N, typename S> __device__ __forceinline__ bool operator>=(const Dual<N, S>& a, const Dual<N, S>& b) { return a.v >= b.v; }
+template <int N, typename S> __device__ __forceinline__ bool operator<(const Dual<N, S>& a, double b) { return a.v < b; }
+template <int N, typename S> __device__ __forceinline__ bool operator>(const Dual<N, S>& a, double b) { return a.v > b; }
+template <int N, typename S> __device__ __forceinline__ bool operator<=(const Dual<N, S>& a, double b) { return a.v <= b; }
+template <int N, typename S> __device__ __forceinline__ bool operator>=(const Dual<N, S>& a, double b) { return a.v >= b; }
+template <int N, typename S> __device__ __forceinline__ bool operator<(double a, const Dual<N, S>& b) { return a < b.v; }
+template <int N, typename S> __device__ __forceinline__ bool operator>(double a, const Dual<N, S>& b) { return a > b.v; }
 
-template <int N>
-__device__ __forceinline__ Dual<N> sqrt(const Dual<N>& a) {
-    Dual<N> r;
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> sqrt(const Dual<N, S>& a) {
+    Dual<N, S> r;
     r.v = ::sqrt(a.v);
-    const double h = (r.v > 0.0) ? 0.5 / r.v : 0.0;
+    const S h = (r.v > S(0)) ? S(0.5) / r.v : S(0);
 #pragma unroll
     for (int q = 0; q < N; ++q) r.d[q] = h * a.d[q];
     return r;
 }
 
-template <int N>
-__device__ __forceinline__ Dual<N> fabs(const Dual<N>& a) {
-    if (a.v > 0.0) return a;
-    if (a.v < 0.0) return -a;
-    return Dual<N>(0.0);
+template <int N, typename S>
+__device__ __forceinline__ Dual<N, S> fabs(const Dual<N, S>& a) {
+    if (a.v > S(0)) return a;
+    if (a.v < S(0)) return -a;
+    return Dual<N, S>(0.0);
 }
 
 }  // namespace sifv

@@ -218,3 +218,45 @@ def test_vortex512_gradient_64_directions():
     info = (max(td_rel), float(np.median(fd6)), max(fd6), max(fd_best))
     assert max(td_rel) <= 1e-10, info
     assert max(fd_best) <= 1e-6, info
+
+
+def _gradient(case, t_end, lam, every, precision):
+    ctx = backends.make(backends.cuda(), case)
+    ctx.adjoint_set_precision(precision)
+    ctx.adjoint_forward(0, 0.0, t_end, 0, every)
+    for f, a in lam.items():
+        ctx.adjoint_set_seed(f, a)
+    ctx.adjoint_backward()
+    return {f: ctx.adjoint_get_gradient(f) for f in lam}, ctx
+
+
+@pytest.mark.parametrize("name", ["vortex", "riemann2d_walls", "sod"])
+def test_fp32_reverse_sweep_close_to_fp64(name):
+    """FP32 local Jacobians in the reverse sweep (the forward trajectory and
+    the adjoint accumulation stay FP64): for random seeds the gradient
+    agrees with the FP64 one to 1e-3 relative (L-infinity over the field's
+    maximum; single-precision round-off accumulated over every stage)."""
+    if name == "vortex":
+        case, t_end = cases.vortex2d(64), 0.5
+    elif name == "riemann2d_walls":
+        case, t_end = cases.riemann2d(48, bc=abi.BC_SLIPWALL), 0.05
+    else:
+        case, t_end = cases.sod(200), 0.05
+    probe = backends.make(backends.cuda(), case)
+    rng = np.random.default_rng(11)
+    mask = _interior_mask(probe)
+    fids = cons_fids(case[0].dim)
+    lam = {f: np.where(mask, rng.standard_normal(probe.shape), 0.0) for f in fids}
+    g64, _ = _gradient(case, t_end, lam, 8, abi.PREC_FP64)
+    g32, _ = _gradient(case, t_end, lam, 8, abi.PREC_MIXED)
+    for f in fids:
+        scale = np.abs(g64[f]).max()
+        assert np.abs(g32[f] - g64[f]).max() <= 1e-3 * scale, f
+        assert np.all(g32[f][~mask] == 0.0)
+
+
+def test_fp32_reverse_sweep_rejects_other_precisions():
+    ctx = backends.make(backends.cuda(), cases.sod(32))
+    with pytest.raises(abi.AbiError) as e:
+        ctx.adjoint_set_precision(abi.PREC_FP64_FAST)
+    assert e.value.status == abi.ERR_BAD_ARG
