@@ -68,10 +68,19 @@ int sweep_stage(SweepArgs A, cudaStream_t s, bool mixed, int& launches, LaunchMa
 
 namespace {
 
-constexpr int kTileX = 32, kTileY = 16;
+// 32 x 14 cells: with 512 threads every reconstruction / flux phase of the
+// FP64 stage has at most one item per thread ((32+2)*14 = 476, 32*(14+2) =
+// 512, 33*14, 32*15), and with 256 threads (FP32 bulk) at most two, where
+// 32 x 16 needed two and three.
+template <typename T>
+struct TileDims {
+    static constexpr int x = 32;
+    static constexpr int y = 14;
+};
 
 template <typename T>
 int tile_launch(const TileArgs& A, cudaStream_t s) {
+    constexpr int kTileX = TileDims<T>::x, kTileY = TileDims<T>::y;
     const size_t bytes = sizeof(TileSmem<kTileX, kTileY, T>);
     if (cudaFuncSetAttribute(k_tile2d<kTileX, kTileY, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)bytes) != cudaSuccess)
