@@ -57,13 +57,13 @@ KERNEL_BYTES_PER_CELL_2D = {"sweep_x": 96.0, "sweep_y": 165.33, "dt": 32.0, "fin
 # same workload (dram__bytes_read.sum + dram__bytes_write.sum over 2048^2 cells)
 # and scaled by the cell count for the benchmark size.
 NCU_DRAM_BYTES_PER_CELL = {(2, "sweep_y"): 164.8, (2, "sweep_x"): 84.5, (1, "sweep_y"): 164.7,
-                           (1, "sweep_x"): 86.2, (0, "assemble"): 166.2, (2, "tile2d"): 55.3,
-                           (1, "tile2d"): 55.3}
+                           (1, "sweep_x"): 86.2, (0, "assemble"): 166.2, (2, "tile2d"): 55.69,
+                           (1, "tile2d"): 54.83}
 # FP64 / FP32 pipe utilisation of the dominant kernel (ncu, 2048^2 case of the
 # same workload: sm__inst_executed_pipe_fp64 / _fma, percent of the pipe's
 # instruction peak while active) -- the co-bound of the HBM roofline.
-NCU_PIPE_FRAC = {(2, "tile2d"): {"fp64": 0.608, "fma_fp32": 0.042, "issue_active": 0.487},
-                 (1, "tile2d"): {"fp64": 0.067, "fma_fp32": 0.418, "issue_active": 0.746}}
+NCU_PIPE_FRAC = {(2, "tile2d"): {"fp64": 0.688, "fma_fp32": 0.053, "issue_active": 0.579},
+                 (1, "tile2d"): {"fp64": 0.072, "fma_fp32": 0.460, "issue_active": 0.807}}
 # Fields a 2D step reads and writes (host-authoritative drop-in round trip).
 E2E_FIELDS_2D = ("F_RHO", "F_RHOU", "F_RHOV", "F_RHOE", "F_VELU", "F_VELV", "F_PRES")
 # Batched ensemble of two-phase water-air tubes: count, cell range, end time.

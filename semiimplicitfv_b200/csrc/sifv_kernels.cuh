@@ -1433,6 +1433,7 @@ __global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, int pl
     double* sR = smem + HN;
     double* sRhs = smem + 2 * HN;
     double* sDiag = sRhs + TN;
+    double* sAx = sDiag + TN;   // alpha / dx^2 of the tile's columns (no global load inside the wavefront)
     const int J = (int)(blockIdx.x % (unsigned)nty), K = (int)(blockIdx.x / (unsigned)nty);
     const int I = plane - J - K;
     if (I < 0 || I >= ntx) return;
@@ -1460,6 +1461,7 @@ __global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, int pl
             cp_async8(&sDiag[l], &F.igrDiag[g]);
         }
     }
+    for (int a = threadIdx.x; a < ex; a += blockDim.x) cp_async8(&sAx[a], &F.adx2[i0 + a + P.ngx]);
     cp_async_wait_all();
     // thread (tb, tc) owns the x-line (., tb, tc) of the tile and updates
     // its cell a = q - tb - tc at cell plane q
@@ -1480,7 +1482,7 @@ __global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, int pl
             double off = 0.0;
             {
                 double rfl = 0.5 * (rho_i + sR[h - 1]), rfr = 0.5 * (rho_i + sR[h + 1]);
-                off += F.adx2[i0 + a + P.ngx] * (sS[h - 1] / rfl + sS[h + 1] / rfr);
+                off += sAx[a] * (sS[h - 1] / rfl + sS[h + 1] / rfr);
             }
             {
                 double rfl = 0.5 * (rho_i + sR[h - HX]), rfr = 0.5 * (rho_i + sR[h + HX]);
@@ -1614,7 +1616,7 @@ constexpr size_t gs_tile_smem() {
 
 template <int TX, int TY, int TZ>
 constexpr size_t igr_tile_smem() {
-    return sizeof(double) * (2 * (size_t)(TX + 2) * (TY + 2) * (TZ > 1 ? TZ + 2 : 1) + 2 * (size_t)TX * TY * TZ);
+    return sizeof(double) * (2 * (size_t)(TX + 2) * (TY + 2) * (TZ > 1 ? TZ + 2 : 1) + 2 * (size_t)TX * TY * TZ + TX);
 }
 
 }  // namespace sifv
