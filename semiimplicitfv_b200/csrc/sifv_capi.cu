@@ -74,6 +74,7 @@ struct sifv_ctx {
     size_t adjStageCap = 0;
     bool adjReady = false;
     bool igrTileReady = false;
+    double* igrRec = nullptr;                 // IGR sweep records (k_igr_records), then one int flag
     double* jacCoef = nullptr;                // Jacobi coefficients: per face (dim arrays) or per cell (2 dim + 2)
     bool uniformAxes = false;                 // interior cell widths bitwise equal along every active axis
     int pressureKind = 0;                     // 0 Jacobi (default), 1 Gauss-Seidel
@@ -352,13 +353,39 @@ int igr_solve(sifv_ctx* c, int step) {
         if (e != cudaSuccess) return fail(c, SIFV_ERR_CUDA, std::string("IGR tile smem: ") + cudaGetErrorString(e));
         c->igrTileReady = true;
     }
+    // 3D: the record sweep (k_igr_tile_rec) when its 16-byte halo copies are
+    // aligned (even row length, 16-byte aligned sigma and rho)
+    const bool rec = d3 && T3 == kIgrTile && P.nxT % 2 == 0 && ((uintptr_t)c->F.sigma % 16) == 0 &&
+                     ((uintptr_t)c->F.rho % 16) == 0;
+    int* slowRecs = nullptr;
+    if (rec) {
+        const int ntiles = ntx * nty * ntz;
+        const size_t nrec = igr_record_doubles(ntiles);
+        if (!c->igrRec) {
+            int sa = SIFV_OK;
+            c->igrRec = dalloc(c, nrec + 2, sa);
+            if (sa != SIFV_OK) return sa;
+            cudaError_t e = cudaFuncSetAttribute(k_igr_tile_rec, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)igr_tile_rec_smem());
+            if (e != cudaSuccess)
+                return fail(c, SIFV_ERR_CUDA, std::string("IGR record tile smem: ") + cudaGetErrorString(e));
+        }
+        slowRecs = reinterpret_cast<int*>(c->igrRec + nrec);
+        CUDA_TRY(c, cudaMemsetAsync(slowRecs, 0, sizeof(int), c->stream));
+        const long long total = (long long)ntiles * kIgrTile * kIgrTile * kIgrRecsPerLine;
+        k_igr_records<<<blocks(total, 256), 256, 0, c->stream>>>(P, c->F, c->igrRec, ntx, nty, total, slowRecs);
+        c->launches++;
+    }
     for (int it = 0; it < iters; ++it) {
         if (P.dim == 1) {
             k_igr_sweep_1d<<<1, 32, 0, c->stream>>>(P, c->F);
             c->launches++;
         } else {
             for (int pl = 0; pl < nplanes; ++pl) {
-                if (d3)
+                if (rec)
+                    k_igr_tile_rec<<<(unsigned)(nty * ntz), kIgrTile * kIgrTile, igr_tile_rec_smem(), c->stream>>>(
+                        P, c->F, c->igrRec, slowRecs, pl, ntx, nty);
+                else if (d3)
                     k_igr_tile<T3, T3, T3><<<(unsigned)(nty * ntz), T3 * T3, smem, c->stream>>>(P, c->F, pl, ntx, nty);
                 else
                     k_igr_tile<T2X, T2Y, 1><<<(unsigned)nty, T2Y, smem, c->stream>>>(P, c->F, pl, ntx, nty);

@@ -1504,6 +1504,235 @@ __global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, int pl
 }
 
 // ---------------------------------------------------------------------------
+// IGR sweep with precomputed reciprocals (3D, 16^3 tiles).
+//
+// The face densities 0.5 (rho_i + rho_nb) and the diagonal are fixed for all
+// sweeps of one IGR solve, so their reciprocals are computed once per solve
+// (k_igr_records, correctly rounded IEEE divisions) and each division of the
+// sweep becomes div_markstein: the same correctly rounded quotient from a
+// multiply and four fused multiply-adds instead of a full division on the
+// serial path of the wavefront.
+// ---------------------------------------------------------------------------
+
+// Correctly rounded a / b given y = RN(1 / b).  q0 = a y is within 1.5 ulp of
+// a / b; one residual correction q1 = RN(q0 + RN(a - b q0) y) is faithful
+// (within 1 ulp); Markstein's theorem (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990: for y = RN(1 / b) and a faithful q, r = a - b q is exact
+// and RN(q + r y) = RN(a / b)) makes the second correction the correctly
+// rounded quotient.  Valid when |y| lies in [2^-450, 2^450] and a is +0 or
+// |a| lies in [2^-450, 2^450] (quotient and residual then stay clear of
+// overflow and gradual underflow; a = +0 gives +0 or -0 as a / b does).
+// Callers check both with igr_fast_operand / igr_fast_recip and take the
+// plain division otherwise.
+__device__ __forceinline__ double div_markstein(double a, double b, double y) {
+    const double q0 = a * y;
+    const double q1 = fma(fma(-q0, b, a), y, q0);
+    return fma(fma(-q1, b, a), y, q1);
+}
+// |x| in [2^-450, 2^450] (biased exponent 573..1473)
+__device__ __forceinline__ bool igr_fast_recip(double x) {
+    return ((unsigned)__double2hiint(x) & 0x7ff00000u) - 0x23d00000u <= 0x38400000u;
+}
+// the same, or x = +0
+__device__ __forceinline__ bool igr_fast_operand(double x) {
+    return igr_fast_recip(x) || (((unsigned)__double2hiint(x) | (unsigned)__double2loint(x)) == 0u);
+}
+// igr_cell's update from staged values with plain divisions; kept out of
+// line so that the compiler does not if-convert it into the common path.
+__device__ __noinline__ double igr_cell_plain(double sxm, double sxp, double sym, double syp, double szm, double szp,
+                                              double rflx, double rfrx, double rfly, double rfry, double rflz,
+                                              double rfrz, double ax, double ay, double az, double rhs, double diag) {
+    double off = 0.0;
+    off += ax * (sxm / rflx + sxp / rfrx);
+    off += ay * (sym / rfly + syp / rfry);
+    off += az * (szm / rflz + szp / rfrz);
+    return (rhs + off) / diag;
+}
+__device__ __noinline__ double div_rn_plain(double a, double b) { return a / b; }
+
+// Records of the tile sweep.  The x-line (., tb, tc) of a tile has records
+// n = 0..16 (n = 16 only carries the left x-face of the cell past the tile,
+// i.e. the right x-face of n = 15); a record is 8 doubles in four 16-byte
+// chunks: 1 / rho_f of the x-, y-, y+, z-, z+ faces, the rhs, the diagonal
+// and 1 / diagonal.  Chunk ch of record n of line (tb, tc) of tile t sits at
+// double2 index (((t * 16 + tc) * 17 + (tb + n) % 17) * 4 + ch) * 16 + tb:
+// the 16 lines of one tc fetch records with equal tb + n at the same cell
+// plane, so each chunk of their fetch is one contiguous 256-byte run.
+constexpr int kIgrTile = 16;
+constexpr int kIgrRecsPerLine = kIgrTile + 1;
+constexpr int kIgrRecDoubles = 8;
+constexpr int kIgrPrefetch = 2;                  // records in flight ahead of the cell being updated
+constexpr int kIgrRing = kIgrPrefetch + 2;       // ring slots per thread
+
+__host__ __device__ __forceinline__ size_t igr_rec_index(long long tile, int tb, int tc, int n) {
+    return ((((size_t)tile * kIgrTile + tc) * kIgrRecsPerLine + (tb + n) % kIgrRecsPerLine) * 4) * kIgrTile + tb;
+}
+inline size_t igr_record_doubles(int ntiles) {
+    return (size_t)ntiles * (kIgrTile * kIgrTile) * kIgrRecsPerLine * kIgrRecDoubles;
+}
+inline size_t igr_tile_rec_smem() {
+    return sizeof(double) * (2 * 20 * 18 * 18 + kIgrRing * kIgrRecDoubles * kIgrTile * kIgrTile + kIgrTile);
+}
+
+// One thread per record, in storage order (tile, tc, (tb + n) % 17, tb) so
+// that a warp's stores are contiguous.  The face densities use the sweep's expressions
+// (0.5 (rho_i + rho_nb) with the cell's own density first) and so the
+// reciprocal belongs to exactly the divisor that the sweep forms.  A
+// reciprocal outside div_markstein's range sets *slowRecs (cleared before
+// the launch): the sweeps of this solve then divide plainly.
+__global__ void __launch_bounds__(256) k_igr_records(Params P, Fields F, double* __restrict__ rec, int ntx, int nty,
+                                                     long long total, int* __restrict__ slowRecs) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    constexpr int T = kIgrTile;
+    const int tb = (int)(idx % T);
+    const int sk = (int)((idx / T) % kIgrRecsPerLine);   // (tb + n) % 17
+    const int tc = (int)((idx / ((long long)T * kIgrRecsPerLine)) % T);
+    const long long tile = idx / ((long long)kIgrRecsPerLine * T * T);
+    const int n = (sk - tb + kIgrRecsPerLine) % kIgrRecsPerLine;
+    const int I = (int)(tile % ntx), J = (int)((tile / ntx) % nty), K = (int)(tile / ((long long)ntx * nty));
+    const int i0 = I * T, j0 = J * T, k0 = K * T;
+    const int ex = min(T, P.nx - i0), ey = min(T, P.ny - j0), ez = min(T, P.nz - k0);
+    if (tb >= ey || tc >= ez || n > ex) return;
+    const size_t c = cidx(P, i0 + n, j0 + tb, k0 + tc);
+    const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+    const double rho_i = F.rho[c];
+    double2* o = reinterpret_cast<double2*>(rec) + igr_rec_index(tile, tb, tc, n);
+    const double rxl = 1.0 / (0.5 * (rho_i + F.rho[c - 1]));
+    if (n == ex) {
+        o[0] = make_double2(rxl, 0.0);
+        if (!igr_fast_recip(rxl)) atomicOr(slowRecs, 1);
+        return;
+    }
+    const double diag = F.igrDiag[c];
+    const double ryl = 1.0 / (0.5 * (rho_i + F.rho[c - sy])), ryr = 1.0 / (0.5 * (rho_i + F.rho[c + sy]));
+    const double rzl = 1.0 / (0.5 * (rho_i + F.rho[c - sz])), rzr = 1.0 / (0.5 * (rho_i + F.rho[c + sz]));
+    const double rd = 1.0 / diag;
+    o[0] = make_double2(rxl, ryl);
+    o[kIgrTile] = make_double2(ryr, rzl);
+    o[2 * kIgrTile] = make_double2(rzr, F.igrRhs[c]);
+    o[3 * kIgrTile] = make_double2(diag, rd);
+    if (!(igr_fast_recip(rxl) && igr_fast_recip(ryl) && igr_fast_recip(ryr) && igr_fast_recip(rzl) &&
+          igr_fast_recip(rzr) && igr_fast_recip(rd)))
+        atomicOr(slowRecs, 1);
+}
+
+__device__ __forceinline__ void cp_async16(void* smemDst, const void* gmemSrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smemDst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmemSrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// The tiled wavefront of k_igr_tile<16, 16, 16> (same tile planes, same cell
+// planes inside a tile, igr_cell's arithmetic in igr_cell's order) with
+//  - the sigma and rho halos staged in 16-byte copies: each halo row holds
+//    20 doubles from the even ghosted column at or below the tile's first
+//    halo column (requires an even row length nxT and 16-byte aligned
+//    fields), the tile's columns start at offset xoff in {0, 1};
+//  - each thread streaming the records of its x-line through a ring of
+//    kIgrRing slots, kIgrPrefetch records ahead of the cell it updates;
+//  - the divisions done by div_markstein (one operand check per cell);
+//  - each updated cell stored to global memory as soon as it is computed.
+// Thread (tb, tc) owns the x-line (., tb, tc) of the tile and updates its
+// cell a = q - tb - tc at cell plane q.
+__global__ void __launch_bounds__(256, 1)
+    k_igr_tile_rec(Params P, Fields F, const double* __restrict__ rec, const int* __restrict__ slowRecs, int plane,
+                   int ntx, int nty) {
+    constexpr int T = kIgrTile, HXP = 20, HY = T + 2, HZ = T + 2, HN = HXP * HY * HZ;
+    constexpr int NT = T * T, D = kIgrPrefetch, R = kIgrRing;
+    extern __shared__ __align__(16) double smem[];
+    double* sS = smem;
+    double* sR = smem + HN;
+    double2* ring = reinterpret_cast<double2*>(smem + 2 * HN);   // [R][4 chunks][NT threads]
+    double* sAx = smem + 2 * HN + R * kIgrRecDoubles * NT;
+    const int J = (int)(blockIdx.x % (unsigned)nty), K = (int)(blockIdx.x / (unsigned)nty);
+    const int I = plane - J - K;
+    if (I < 0 || I >= ntx) return;
+    const int tid = (int)threadIdx.x;
+    const int i0 = I * T, j0 = J * T, k0 = K * T;
+    const int ex = min(T, P.nx - i0), ey = min(T, P.ny - j0), ez = min(T, P.nz - k0);
+    const int hy = ey + 2, hz = ez + 2;
+    const int xg = i0 - 1 + P.ngx;   // ghosted column of the first halo column
+    const int xs = xg & ~1;
+    const int xoff = xg - xs;
+    for (int w = tid; w < hy * hz * (HXP / 2); w += NT) {
+        const int m = w % (HXP / 2), row = w / (HXP / 2);
+        const int b = row % hy, c = row / hy;
+        const int x = xs + 2 * m;
+        if (x + 1 < P.nxT) {
+            const size_t g = (size_t)x + (size_t)P.nxT * ((size_t)(j0 + b - 1 + P.ngy) +
+                                                          (size_t)P.nyT * (size_t)(k0 + c - 1 + P.ngz));
+            const int h = (c * HY + b) * HXP + 2 * m;
+            cp_async16(&sS[h], &F.sigma[g]);
+            cp_async16(&sR[h], &F.rho[g]);
+        }
+    }
+    for (int a = tid; a < ex; a += NT) cp_async8(&sAx[a], &F.adx2[i0 + a + P.ngx]);
+    cp_async_commit();
+    const int tb = tid % T, tc = tid / T;
+    const bool act = tb < ey && tc < ez;
+    const long long tile = (long long)I + (long long)ntx * (J + (long long)nty * K);
+    const double2* lineRec = reinterpret_cast<const double2*>(rec) + igr_rec_index(tile, 0, tc, 0);   // (tile, tc) block
+    // record n of this thread's line goes to ring slot n % R; one commit
+    // group per (pre-)step, so that at cell plane q the group of record
+    // a + 1 is the (D+1)-th most recent one
+    auto issue = [&](int n) {
+        if (act && n >= 0 && n <= ex) {
+            double2* dst = ring + (size_t)(n % R) * 4 * NT + tid;
+            const double2* src = lineRec + (size_t)((tb + n) % kIgrRecsPerLine) * 4 * T + tb;
+#pragma unroll
+            for (int ch = 0; ch < 4; ++ch) cp_async16(dst + ch * NT, src + ch * T);
+        }
+        cp_async_commit();
+    };
+    for (int q = -(D + 1); q < 0; ++q) issue(q - tb - tc + D + 1);
+    cp_async_wait_group<D + 1>();   // the staging group (older than the D + 1 record groups)
+    const double ady = act ? F.ady2[j0 + tb + P.ngy] : 0.0;
+    const double adz = act ? F.adz2[k0 + tc + P.ngz] : 0.0;
+    const int hLine = ((tc + 1) * HY + (tb + 1)) * HXP + 1 + xoff;
+    const size_t gLine = cidx(P, i0, j0 + tb, k0 + tc);
+    const bool fastRecs = *slowRecs == 0;
+    __syncthreads();
+    const int nq = ex + ey + ez - 2;
+    for (int q = 0; q < nq; ++q) {
+        const int a = q - tb - tc;
+        issue(a + D + 1);
+        cp_async_wait_group<D>();   // records a and a + 1 of this thread have landed
+        if (act && a >= 0 && a < ex && !(F.solid && F.solid[gLine + a])) {
+            const double2* ra = ring + (size_t)(a % R) * 4 * NT + tid;
+            const double2 c0 = ra[0], c1 = ra[NT], c2 = ra[2 * NT], c3 = ra[3 * NT];
+            const double rxr = ring[(size_t)((a + 1) % R) * 4 * NT + tid].x;
+            const int h = hLine + a;
+            const double rho_i = sR[h];
+            const double sxm = sS[h - 1], sxp = sS[h + 1], sym = sS[h - HXP], syp = sS[h + HXP];
+            const double szm = sS[h - HXP * HY], szp = sS[h + HXP * HY];
+            const double rflx = 0.5 * (rho_i + sR[h - 1]), rfrx = 0.5 * (rho_i + sR[h + 1]);
+            const double rfly = 0.5 * (rho_i + sR[h - HXP]), rfry = 0.5 * (rho_i + sR[h + HXP]);
+            const double rflz = 0.5 * (rho_i + sR[h - HXP * HY]), rfrz = 0.5 * (rho_i + sR[h + HXP * HY]);
+            double v;
+            if (fastRecs && igr_fast_operand(sxm) && igr_fast_operand(sxp) && igr_fast_operand(sym) &&
+                igr_fast_operand(syp) && igr_fast_operand(szm) && igr_fast_operand(szp)) {
+                double off = 0.0;
+                off += sAx[a] * (div_markstein(sxm, rflx, c0.x) + div_markstein(sxp, rfrx, rxr));
+                off += ady * (div_markstein(sym, rfly, c0.y) + div_markstein(syp, rfry, c1.x));
+                off += adz * (div_markstein(szm, rflz, c1.y) + div_markstein(szp, rfrz, c2.x));
+                const double num = c2.y + off;
+                v = igr_fast_operand(num) ? div_markstein(num, c3.x, c3.y) : div_rn_plain(num, c3.x);
+            } else {
+                v = igr_cell_plain(sxm, sxp, sym, syp, szm, szp, rflx, rfrx, rfly, rfry, rflz, rfrz, sAx[a], ady, adz,
+                                   c2.y, c3.x);
+            }
+            sS[h] = v;
+            F.sigma[gLine + a] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Gauss-Seidel pressure solve (GaussSeidelPressureSolver::solve,
 // src/GaussSeidelPressureSolver.cpp:10-49): per iteration the scalar ghosts of
 // p are filled from the current iterate, then one lexicographic in-place sweep

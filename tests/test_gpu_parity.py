@@ -100,6 +100,14 @@ def test_igr_tiled_wavefront_3d_ragged(bc, stretch):
     check(cases.acoustic_box(40, 36, 20, bc=bc, stretch=stretch), 2)
 
 
+@pytest.mark.parametrize("nx,ny,nz", [(48, 34, 40), (35, 40, 33)])
+def test_igr_record_sweep_3d(nx, ny, nz):
+    """3D IGR sweeps with precomputed reciprocals (even row length: 48 + 6
+    ghosts, tiles ragged in y and z) and the plain tile sweep they fall back to
+    (odd row length: 35 + 6 ghosts), both bit-identical to the oracle."""
+    check(cases.acoustic_box(nx, ny, nz, bc=abi.BC_SLIPWALL, stretch=0.01), 2)
+
+
 @pytest.mark.parametrize("bc", [abi.BC_PERIODIC, abi.BC_OUTFLOW])
 def test_igr_tiled_wavefront_2d_ragged(bc):
     """Several 32 x 64 IGR tiles with ragged edges (100 x 140 cells)."""
