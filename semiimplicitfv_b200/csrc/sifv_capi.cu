@@ -106,6 +106,9 @@ struct sifv_ctx {
     float* mxD = nullptr;        // FP32 delta
     float* mxE[2] = {nullptr, nullptr};
     int lastInPlace = 0;         // the last pressure solve left its result in F.pA
+    int jacPrevIters = 0;        // iterations of the previous Jacobi solve (first batch size)
+    unsigned jacGrid = 0;        // resident-grid size of the grid-stride Jacobi kernels
+    unsigned mxGrid = 0;         // the same for k_mx_sweep
     int adjFp32 = 0;             // FP32 local Jacobians in the reverse sweep
 };
 
@@ -382,10 +385,21 @@ int igr_solve(sifv_ctx* c, int step) {
             c->launches++;
         } else {
             for (int pl = 0; pl < nplanes; ++pl) {
-                if (rec)
-                    k_igr_tile_rec<<<(unsigned)(nty * ntz), kIgrTile * kIgrTile, igr_tile_rec_smem(), c->stream>>>(
-                        P, c->F, c->igrRec, slowRecs, pl, ntx, nty);
-                else if (d3)
+                if (rec) {
+                    // planes after the first overlap their prologue with the previous plane
+                    cudaLaunchAttribute at[1];
+                    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                    at[0].val.programmaticStreamSerializationAllowed = 1;
+                    cudaLaunchConfig_t lc = {};
+                    lc.gridDim = dim3((unsigned)(nty * ntz));
+                    lc.blockDim = dim3(kIgrTile * kIgrTile);
+                    lc.dynamicSmemBytes = igr_tile_rec_smem();
+                    lc.stream = c->stream;
+                    lc.attrs = at;
+                    lc.numAttrs = pl > 0 ? 1 : 0;
+                    CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_igr_tile_rec, P, c->F, (const double*)c->igrRec,
+                                                   (const int*)slowRecs, pl, ntx, nty));
+                } else if (d3)
                     k_igr_tile<T3, T3, T3><<<(unsigned)(nty * ntz), T3 * T3, smem, c->stream>>>(P, c->F, pl, ntx, nty);
                 else
                     k_igr_tile<T2X, T2Y, 1><<<(unsigned)nty, T2Y, smem, c->stream>>>(P, c->F, pl, ntx, nty);
@@ -420,18 +434,40 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
         k_jacobi_fcoef<<<g, kCellThreads, 0, c->stream>>>(c->P, rho, c->F, c->jacCoef, c->ncells);
     else
         k_jacobi_coef<<<g, kCellThreads, 0, c->stream>>>(c->P, rho, rhoc2, c->F, c->ctl, c->jacCoef, c->ncells);
-    int it = 0, batch = 4;
+    // Batches between host convergence checks: 4, 8, 16, 32; a solve after an
+    // earlier one starts with 3/4 of its iteration count in one batch (the
+    // counts change slowly from step to step), which spares most of the
+    // launches that only find the solve converged.
+    if (!c->jacGrid) {
+        int sm = 0, nb1 = 0, nb2 = 0;
+        CUDA_TRY(c, cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, c->device));
+        CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb1, k_jacobi_face, kCellThreads, 0));
+        CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_jacobi_pre, kCellThreads, 0));
+        c->jacGrid = (unsigned)std::max(1, sm * std::max(1, std::min(nb1, nb2)));
+    }
+    const unsigned gj = std::min(g, c->jacGrid);
+    int it = 0, batch = c->jacPrevIters > 5 ? (3 * c->jacPrevIters) / 4 : 4;
+    bool first = true;
     int done = 0;
     while (it < maxIter) {
         int nb = std::min(batch, maxIter - it);
         for (int q = 0; q < nb; ++q, ++it) {
             const double* pin = (it & 1) ? c->F.pB : c->F.pA;
             double* pout = (it & 1) ? c->F.pA : c->F.pB;
-            if (faceCoef)
-                k_jacobi_face<<<g, kCellThreads, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhoc2, rhs, pin, pout,
+            if (c->P.dim == 3) {
+                const dim3 g3((unsigned)((c->P.nx + 31) / 32), (unsigned)((c->P.ny + 7) / 8),
+                              (unsigned)((c->P.nz + kJacZ - 1) / kJacZ));
+                if (faceCoef)
+                    k_jacobi3<true><<<g3, 256, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhoc2, rhs, pin, pout,
+                                                               c->ctl, it, tol);
+                else
+                    k_jacobi3<false><<<g3, 256, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhoc2, rhs, pin, pout,
+                                                                c->ctl, it, tol);
+            } else if (faceCoef)
+                k_jacobi_face<<<gj, kCellThreads, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhoc2, rhs, pin, pout,
                                                                  c->ctl, it, tol);
             else
-                k_jacobi_pre<<<g, kCellThreads, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhs, pin, pout, c->ctl,
+                k_jacobi_pre<<<gj, kCellThreads, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhs, pin, pout, c->ctl,
                                                                 it, tol);
         }
         c->launches += nb;
@@ -450,9 +486,11 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
             done = it;
             break;
         }
-        batch = std::min(batch * 2, 32);
+        batch = first && batch > 4 ? 4 : std::min(batch * 2, 32);
+        first = false;
     }
     iters = done ? done : maxIter;
+    c->jacPrevIters = iters;
     result = (iters & 1) ? c->F.pB : c->F.pA;
     mark(c, "jacobi");
     return SIFV_OK;
@@ -706,6 +744,13 @@ int jacobi_mixed_run(sifv_ctx* c, const double* rho, const double* rhoc2, const 
     k_jacobi_coef<<<g, kCellThreads, 0, c->stream>>>(P, rho, rhoc2, c->F, c->ctl, c->mxCoef, c->ncells);
     k_mx_weights<<<g, kCellThreads, 0, c->stream>>>(P, c->mxCoef, c->ncells, c->mxW, n);
     c->launches += 2;
+    if (!c->mxGrid) {
+        int sm = 0, nb = 0;
+        CUDA_TRY(c, cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, c->device));
+        CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_mx_sweep, kCellThreads, 0));
+        c->mxGrid = (unsigned)std::max(1, sm * std::max(1, nb));
+    }
+    const unsigned gs = std::min(g, c->mxGrid);   // grid-stride FP32 sweeps
     constexpr int kInner = 8;   // FP32 sweeps per FP64 refinement
     int it = 0, done = 0;
     while (it < maxIter && !done) {
@@ -716,7 +761,7 @@ int jacobi_mixed_run(sifv_ctx* c, const double* rho, const double* rhoc2, const 
         const int first = it;
         ++it;
         for (int q = 1; q < kInner && it < maxIter; ++q, ++it) {
-            k_mx_sweep<<<g, kCellThreads, 0, c->stream>>>(P, c->mxW, c->mxD, c->mxE[cur], c->mxE[cur ^ 1], c->ctl, it,
+            k_mx_sweep<<<gs, kCellThreads, 0, c->stream>>>(P, c->mxW, c->mxD, c->mxE[cur], c->mxE[cur ^ 1], c->ctl, it,
                                                           tol);
             cur ^= 1;
         }

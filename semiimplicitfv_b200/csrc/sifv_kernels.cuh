@@ -1002,6 +1002,60 @@ __global__ void __launch_bounds__(256) k_jacobi_coef(Params P, const double* __r
     coef[(size_t)(2 * dim + 1) * nc + c] = 1.0 + coeff * diag;
 }
 
+// Neighbour indices of interior cell (i, j, k) for the Jacobi stencil:
+// plain strides inside, the scalar ghost map (periodic wrap / zero gradient,
+// scalar_src) across the boundary, one axis at a time.
+struct JacNb {
+    size_t c, xm, xp, ym, yp, zm, zp;
+};
+__device__ __forceinline__ JacNb jacobi_nb(const Params& P, int i, int j, int k) {
+    JacNb n;
+    const long long sy = P.nxT, sz = (long long)P.nxT * P.nyT;
+    n.c = cidx(P, i, j, k);
+    n.xm = n.c + (long long)(scalar_src(i - 1, P.nx, P.bc[0], P.bc[1]) - i);
+    n.xp = n.c + (long long)(scalar_src(i + 1, P.nx, P.bc[0], P.bc[1]) - i);
+    n.ym = n.yp = n.zm = n.zp = n.c;
+    if (P.dim >= 2) {
+        n.ym = n.c + (long long)(scalar_src(j - 1, P.ny, P.bc[2], P.bc[3]) - j) * sy;
+        n.yp = n.c + (long long)(scalar_src(j + 1, P.ny, P.bc[2], P.bc[3]) - j) * sy;
+    }
+    if (P.dim >= 3) {
+        n.zm = n.c + (long long)(scalar_src(k - 1, P.nz, P.bc[4], P.bc[5]) - k) * sz;
+        n.zp = n.c + (long long)(scalar_src(k + 1, P.nz, P.bc[4], P.bc[5]) - k) * sz;
+    }
+    return n;
+}
+
+// One Jacobi update of one interior cell from the per-cell coefficients;
+// returns |p_new - p_old|.
+__device__ __forceinline__ double jacobi_pre_update(const Params& P, const double* __restrict__ coef, size_t nc,
+                                                    const double* __restrict__ rhs, const double* __restrict__ pin,
+                                                    double* __restrict__ pout, const JacNb& n) {
+    const int dim = P.dim;
+    const size_t c = n.c;
+    const double* cf = coef + c;
+    double od = 0.0;
+    od += cf[0] * pin[n.xm] + cf[nc] * pin[n.xp];
+    if (dim >= 2) od += cf[2 * nc] * pin[n.ym] + cf[3 * nc] * pin[n.yp];
+    if (dim >= 3) od += cf[4 * nc] * pin[n.zm] + cf[5 * nc] * pin[n.zp];
+    const double coeff = cf[(size_t)(2 * dim) * nc];
+    const double denom = cf[(size_t)(2 * dim + 1) * nc];
+    double pn = (rhs[c] + coeff * od) / denom;
+    pout[c] = pn;
+    return fabs(pn - pin[c]);
+}
+__device__ __forceinline__ double jacobi_pre_cell(const Params& P, const double* __restrict__ coef, size_t nc,
+                                                  const double* __restrict__ rhs, const double* __restrict__ pin,
+                                                  double* __restrict__ pout, long long t) {
+    int i, j, k;
+    split3(t, P.nx, P.ny, i, j, k);
+    return jacobi_pre_update(P, coef, nc, rhs, pin, pout, jacobi_nb(P, i, j, k));
+}
+
+// Grid-stride Jacobi iteration (a grid of a few blocks per SM, two cells in
+// flight per thread): the convergence check, the block reduction and the
+// residual atomic run once per block instead of once per 256 cells.  A NaN
+// residual counts as 0, as in block_max_to.
 __global__ void __launch_bounds__(256) k_jacobi_pre(Params P, const double* __restrict__ coef, size_t nc,
                                                     const double* __restrict__ rhs, const double* __restrict__ pin,
                                                     double* __restrict__ pout, Ctl* ctl, int it, double tol) {
@@ -1010,34 +1064,14 @@ __global__ void __launch_bounds__(256) k_jacobi_pre(Params P, const double* __re
         if (threadIdx.x == 0) ctl->jacobiDone = it;
         return;
     }
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int i, j, k;
+    const long long tot = (long long)P.nx * P.ny * P.nz;
+    const long long stride = (long long)gridDim.x * blockDim.x;
     double res = 0.0;
-    if (int_coords(P, t, i, j, k)) {
-        const int dim = P.dim;
-        const size_t c = cidx(P, i, j, k);
-        const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
-        // neighbours: plain strides away from the boundary, the scalar ghost
-        // map (periodic wrap / zero gradient) on the boundary layer
-        const bool inner = i > 0 && i < P.nx - 1 && (dim < 2 || (j > 0 && j < P.ny - 1)) &&
-                           (dim < 3 || (k > 0 && k < P.nz - 1));
-        size_t xm = c - 1, xp = c + 1, ym = c - sy, yp = c + sy, zm = c - sz, zp = c + sz;
-        if (!inner) {
-            xm = scalar_idx(P, i - 1, j, k);
-            xp = scalar_idx(P, i + 1, j, k);
-            if (dim >= 2) { ym = scalar_idx(P, i, j - 1, k); yp = scalar_idx(P, i, j + 1, k); }
-            if (dim >= 3) { zm = scalar_idx(P, i, j, k - 1); zp = scalar_idx(P, i, j, k + 1); }
-        }
-        const double* cf = coef + c;
-        double od = 0.0;
-        od += cf[0] * pin[xm] + cf[nc] * pin[xp];
-        if (dim >= 2) od += cf[2 * nc] * pin[ym] + cf[3 * nc] * pin[yp];
-        if (dim >= 3) od += cf[4 * nc] * pin[zm] + cf[5 * nc] * pin[zp];
-        const double coeff = cf[(size_t)(2 * dim) * nc];
-        const double denom = cf[(size_t)(2 * dim + 1) * nc];
-        double pn = (rhs[c] + coeff * od) / denom;
-        pout[c] = pn;
-        res = fabs(pn - pin[c]);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += 2 * stride) {
+        const double r0 = jacobi_pre_cell(P, coef, nc, rhs, pin, pout, t);
+        const double r1 = (t + stride < tot) ? jacobi_pre_cell(P, coef, nc, rhs, pin, pout, t + stride) : 0.0;
+        res = smax(res, r0);
+        res = smax(res, r1);
     }
     block_max_to(res, &ctl->res[it]);
 }
@@ -1094,6 +1128,45 @@ __global__ void __launch_bounds__(256) k_jacobi_fcoef(Params P, const double* __
     }
 }
 
+__device__ __forceinline__ double jacobi_face_update(const Params& P, const double* __restrict__ fc, size_t nc,
+                                                     const double* __restrict__ rhoc2, const double* __restrict__ rhs,
+                                                     const double* __restrict__ pin, double* __restrict__ pout,
+                                                     double dt2, const JacNb& n) {
+    const int dim = P.dim;
+    const size_t c = n.c;
+    const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+    double coeff = rhoc2[c] * dt2;
+    double od = 0.0, diag = 0.0;
+    {
+        const double cL = fc[c], cR = fc[c + 1];
+        od += cL * pin[n.xm] + cR * pin[n.xp];
+        diag += cL + cR;
+    }
+    if (dim >= 2) {
+        const double cL = fc[nc + c], cR = fc[nc + c + sy];
+        od += cL * pin[n.ym] + cR * pin[n.yp];
+        diag += cL + cR;
+    }
+    if (dim >= 3) {
+        const double cL = fc[2 * nc + c], cR = fc[2 * nc + c + sz];
+        od += cL * pin[n.zm] + cR * pin[n.zp];
+        diag += cL + cR;
+    }
+    double denom = 1.0 + coeff * diag;
+    double pn = (rhs[c] + coeff * od) / denom;
+    pout[c] = pn;
+    return fabs(pn - pin[c]);
+}
+__device__ __forceinline__ double jacobi_face_cell(const Params& P, const double* __restrict__ fc, size_t nc,
+                                                   const double* __restrict__ rhoc2, const double* __restrict__ rhs,
+                                                   const double* __restrict__ pin, double* __restrict__ pout,
+                                                   double dt2, long long t) {
+    int i, j, k;
+    split3(t, P.nx, P.ny, i, j, k);
+    return jacobi_face_update(P, fc, nc, rhoc2, rhs, pin, pout, dt2, jacobi_nb(P, i, j, k));
+}
+
+// Grid-stride form as k_jacobi_pre.
 __global__ void __launch_bounds__(256) k_jacobi_face(Params P, const double* __restrict__ fc, size_t nc,
                                                      const double* __restrict__ rhoc2,
                                                      const double* __restrict__ rhs, const double* __restrict__ pin,
@@ -1103,45 +1176,52 @@ __global__ void __launch_bounds__(256) k_jacobi_face(Params P, const double* __r
         if (threadIdx.x == 0) ctl->jacobiDone = it;
         return;
     }
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int i, j, k;
+    const double dt = ctl->dt;
+    const double dt2 = dt * dt;
+    const long long tot = (long long)P.nx * P.ny * P.nz;
+    const long long stride = (long long)gridDim.x * blockDim.x;
     double res = 0.0;
-    if (int_coords(P, t, i, j, k)) {
-        const int dim = P.dim;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += 2 * stride) {
+        const double r0 = jacobi_face_cell(P, fc, nc, rhoc2, rhs, pin, pout, dt2, t);
+        const double r1 = (t + stride < tot) ? jacobi_face_cell(P, fc, nc, rhoc2, rhs, pin, pout, dt2, t + stride)
+                                             : 0.0;
+        res = smax(res, r0);
+        res = smax(res, r1);
+    }
+    block_max_to(res, &ctl->res[it]);
+}
+
+// 3D Jacobi iteration: 32 x 8 blocks of (x, y) columns, each thread walking
+// kJacZ cells along z (no index division; the ghost remap per axis only
+// where a neighbour leaves the domain).  FACE selects the per-face
+// (k_jacobi_face) or per-cell (k_jacobi_pre) coefficients; the update of each
+// cell is the same function as theirs.
+constexpr int kJacZ = 16;
+template <bool FACE>
+__global__ void __launch_bounds__(256) k_jacobi3(Params P, const double* __restrict__ coef, size_t nc,
+                                                 const double* __restrict__ rhoc2, const double* __restrict__ rhs,
+                                                 const double* __restrict__ pin, double* __restrict__ pout, Ctl* ctl,
+                                                 int it, double tol) {
+    if (ctl->jacobiDone) return;
+    if (it > 0 && bits2d(ctl->res[it - 1]) < tol) {
+        if (threadIdx.x == 0) ctl->jacobiDone = it;
+        return;
+    }
+    const int i = (int)blockIdx.x * 32 + (int)(threadIdx.x & 31);
+    const int j = (int)blockIdx.y * 8 + (int)(threadIdx.x >> 5);
+    const int k0 = (int)blockIdx.z * kJacZ;
+    double res = 0.0;
+    if (i < P.nx && j < P.ny) {
         const double dt = ctl->dt;
         const double dt2 = dt * dt;
-        const size_t c = cidx(P, i, j, k);
-        const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
-        const bool inner = i > 0 && i < P.nx - 1 && (dim < 2 || (j > 0 && j < P.ny - 1)) &&
-                           (dim < 3 || (k > 0 && k < P.nz - 1));
-        size_t xm = c - 1, xp = c + 1, ym = c - sy, yp = c + sy, zm = c - sz, zp = c + sz;
-        if (!inner) {
-            xm = scalar_idx(P, i - 1, j, k);
-            xp = scalar_idx(P, i + 1, j, k);
-            if (dim >= 2) { ym = scalar_idx(P, i, j - 1, k); yp = scalar_idx(P, i, j + 1, k); }
-            if (dim >= 3) { zm = scalar_idx(P, i, j, k - 1); zp = scalar_idx(P, i, j, k + 1); }
+        const int k1 = min(k0 + kJacZ, P.nz);
+#pragma unroll 4
+        for (int k = k0; k < k1; ++k) {
+            const JacNb n = jacobi_nb(P, i, j, k);
+            const double r = FACE ? jacobi_face_update(P, coef, nc, rhoc2, rhs, pin, pout, dt2, n)
+                                  : jacobi_pre_update(P, coef, nc, rhs, pin, pout, n);
+            res = smax(res, r);
         }
-        double coeff = rhoc2[c] * dt2;
-        double od = 0.0, diag = 0.0;
-        {
-            const double cL = fc[c], cR = fc[c + 1];
-            od += cL * pin[xm] + cR * pin[xp];
-            diag += cL + cR;
-        }
-        if (dim >= 2) {
-            const double cL = fc[nc + c], cR = fc[nc + c + sy];
-            od += cL * pin[ym] + cR * pin[yp];
-            diag += cL + cR;
-        }
-        if (dim >= 3) {
-            const double cL = fc[2 * nc + c], cR = fc[2 * nc + c + sz];
-            od += cL * pin[zm] + cR * pin[zp];
-            diag += cL + cR;
-        }
-        double denom = 1.0 + coeff * diag;
-        double pn = (rhs[c] + coeff * od) / denom;
-        pout[c] = pn;
-        res = fabs(pn - pin[c]);
     }
     block_max_to(res, &ctl->res[it]);
 }
@@ -1222,7 +1302,22 @@ __device__ __forceinline__ long long mx_nb(const Params& P, int i, int j, int k,
 }
 
 // One FP32 sweep e_out = delta + J e_in, iteration `it` of the count; a no-op
-// once an earlier iteration's change fell below tol (as k_jacobi_pre).
+// once an earlier iteration's change fell below tol (as k_jacobi_pre), and
+// grid-stride with two cells in flight per thread as k_jacobi_pre.
+__device__ __forceinline__ double mx_sweep_cell(const Params& P, const float* __restrict__ w,
+                                                const float* __restrict__ d32, const float* __restrict__ ein,
+                                                float* __restrict__ eout, long long n, long long t) {
+    int i, j, k;
+    split3(t, P.nx, P.ny, i, j, k);
+    float od = w[t] * ein[mx_nb(P, i, j, k, 0, -1)] + w[n + t] * ein[mx_nb(P, i, j, k, 0, 1)];
+    if (P.dim >= 2)
+        od += w[2 * n + t] * ein[mx_nb(P, i, j, k, 1, -1)] + w[3 * n + t] * ein[mx_nb(P, i, j, k, 1, 1)];
+    if (P.dim >= 3)
+        od += w[4 * n + t] * ein[mx_nb(P, i, j, k, 2, -1)] + w[5 * n + t] * ein[mx_nb(P, i, j, k, 2, 1)];
+    const float en = d32[t] + od;
+    eout[t] = en;
+    return (double)fabsf(en - ein[t]);
+}
 __global__ void __launch_bounds__(256) k_mx_sweep(Params P, const float* __restrict__ w, const float* __restrict__ d32,
                                                   const float* __restrict__ ein, float* __restrict__ eout, Ctl* ctl,
                                                   int it, double tol) {
@@ -1231,19 +1326,14 @@ __global__ void __launch_bounds__(256) k_mx_sweep(Params P, const float* __restr
         if (threadIdx.x == 0) ctl->jacobiDone = it;
         return;
     }
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int i, j, k;
+    const long long n = (long long)P.nx * P.ny * P.nz;
+    const long long stride = (long long)gridDim.x * blockDim.x;
     double res = 0.0;
-    if (int_coords(P, t, i, j, k)) {
-        const long long n = (long long)P.nx * P.ny * P.nz;
-        float od = w[t] * ein[mx_nb(P, i, j, k, 0, -1)] + w[n + t] * ein[mx_nb(P, i, j, k, 0, 1)];
-        if (P.dim >= 2)
-            od += w[2 * n + t] * ein[mx_nb(P, i, j, k, 1, -1)] + w[3 * n + t] * ein[mx_nb(P, i, j, k, 1, 1)];
-        if (P.dim >= 3)
-            od += w[4 * n + t] * ein[mx_nb(P, i, j, k, 2, -1)] + w[5 * n + t] * ein[mx_nb(P, i, j, k, 2, 1)];
-        const float en = d32[t] + od;
-        eout[t] = en;
-        res = (double)fabsf(en - ein[t]);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += 2 * stride) {
+        const double r0 = mx_sweep_cell(P, w, d32, ein, eout, n, t);
+        const double r1 = (t + stride < n) ? mx_sweep_cell(P, w, d32, ein, eout, n, t + stride) : 0.0;
+        res = smax(res, r0);
+        res = smax(res, r1);
     }
     block_max_to(res, &ctl->res[it]);
 }
@@ -1635,7 +1725,11 @@ __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.w
 //  - each thread streaming the records of its x-line through a ring of
 //    kIgrRing slots, kIgrPrefetch records ahead of the cell it updates;
 //  - the divisions done by div_markstein (one operand check per cell);
-//  - each updated cell stored to global memory as soon as it is computed.
+//  - each updated cell stored to global memory as soon as it is computed;
+//  - the tile planes after the first of a sweep launched with programmatic
+//    stream serialization (griddepcontrol): a plane's blocks stage the rho
+//    halo and their first records while the previous plane still runs, and
+//    read sigma only after it has completed.
 // Thread (tb, tc) owns the x-line (., tb, tc) of the tile and updates its
 // cell a = q - tb - tc at cell plane q.
 __global__ void __launch_bounds__(256, 1)
@@ -1658,18 +1752,24 @@ __global__ void __launch_bounds__(256, 1)
     const int xg = i0 - 1 + P.ngx;   // ghosted column of the first halo column
     const int xs = xg & ~1;
     const int xoff = xg - xs;
-    for (int w = tid; w < hy * hz * (HXP / 2); w += NT) {
-        const int m = w % (HXP / 2), row = w / (HXP / 2);
-        const int b = row % hy, c = row / hy;
-        const int x = xs + 2 * m;
-        if (x + 1 < P.nxT) {
-            const size_t g = (size_t)x + (size_t)P.nxT * ((size_t)(j0 + b - 1 + P.ngy) +
-                                                          (size_t)P.nyT * (size_t)(k0 + c - 1 + P.ngz));
-            const int h = (c * HY + b) * HXP + 2 * m;
-            cp_async16(&sS[h], &F.sigma[g]);
-            cp_async16(&sR[h], &F.rho[g]);
+    // Launched with programmatic stream serialization after the previous
+    // tile plane: let the next plane's blocks start, and stage everything
+    // that no tile plane writes (rho halo, alpha / dx^2, the first records)
+    // before waiting for the previous plane to complete.
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+    auto stageHalo = [&](double* dst, const double* src) {
+        for (int w = tid; w < hy * hz * (HXP / 2); w += NT) {
+            const int m = w % (HXP / 2), row = w / (HXP / 2);
+            const int b = row % hy, c = row / hy;
+            const int x = xs + 2 * m;
+            if (x + 1 < P.nxT) {
+                const size_t g = (size_t)x + (size_t)P.nxT * ((size_t)(j0 + b - 1 + P.ngy) +
+                                                              (size_t)P.nyT * (size_t)(k0 + c - 1 + P.ngz));
+                cp_async16(&dst[(c * HY + b) * HXP + 2 * m], &src[g]);
+            }
         }
-    }
+    };
+    stageHalo(sR, F.rho);
     for (int a = tid; a < ex; a += NT) cp_async8(&sAx[a], &F.adx2[i0 + a + P.ngx]);
     cp_async_commit();
     const int tb = tid % T, tc = tid / T;
@@ -1677,8 +1777,8 @@ __global__ void __launch_bounds__(256, 1)
     const long long tile = (long long)I + (long long)ntx * (J + (long long)nty * K);
     const double2* lineRec = reinterpret_cast<const double2*>(rec) + igr_rec_index(tile, 0, tc, 0);   // (tile, tc) block
     // record n of this thread's line goes to ring slot n % R; one commit
-    // group per (pre-)step, so that at cell plane q the group of record
-    // a + 1 is the (D+1)-th most recent one
+    // group per (pre-)step: at cell plane q >= D the group of record a + 1
+    // is the (D+1)-th most recent one (earlier ones complete before the loop)
     auto issue = [&](int n) {
         if (act && n >= 0 && n <= ex) {
             double2* dst = ring + (size_t)(n % R) * 4 * NT + tid;
@@ -1689,12 +1789,15 @@ __global__ void __launch_bounds__(256, 1)
         cp_async_commit();
     };
     for (int q = -(D + 1); q < 0; ++q) issue(q - tb - tc + D + 1);
-    cp_async_wait_group<D + 1>();   // the staging group (older than the D + 1 record groups)
     const double ady = act ? F.ady2[j0 + tb + P.ngy] : 0.0;
     const double adz = act ? F.adz2[k0 + tc + P.ngz] : 0.0;
     const int hLine = ((tc + 1) * HY + (tb + 1)) * HXP + 1 + xoff;
     const size_t gLine = cidx(P, i0, j0 + tb, k0 + tc);
     const bool fastRecs = *slowRecs == 0;
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");   // sigma of the previous tile planes
+    stageHalo(sS, F.sigma);
+    cp_async_commit();
+    cp_async_wait_group<0>();
     __syncthreads();
     const int nq = ex + ey + ez - 2;
     for (int q = 0; q < nq; ++q) {
