@@ -1194,11 +1194,73 @@ __global__ void __launch_bounds__(256) k_jacobi_face(Params P, const double* __r
 // 3D Jacobi iteration: 32 x 8 blocks of (x, y) columns, each thread walking
 // kJacZ cells along z (no index division; the ghost remap per axis only
 // where a neighbour leaves the domain).  FACE selects the per-face
-// (k_jacobi_face) or per-cell (k_jacobi_pre) coefficients; the update of each
-// cell is the same function as theirs.
+// (k_jacobi_face) or per-cell (k_jacobi_pre) coefficients, with their update
+// expressions in their order.  The inputs of the next cell of the column are
+// loaded before the current cell is computed, so that their memory latency
+// overlaps the division.
 constexpr int kJacZ = 16;
+struct JacIn {
+    double rc, rh, dn, pc, pxm, pxp, pym, pyp, pzm, pzp, c0, c1, c2, c3, c4, c5;
+};
 template <bool FACE>
-__global__ void __launch_bounds__(256) k_jacobi3(Params P, const double* __restrict__ coef, size_t nc,
+__device__ __forceinline__ JacIn jacobi3_load(const Params& P, const double* __restrict__ coef, size_t nc,
+                                              const double* __restrict__ rhoc2, const double* __restrict__ rhs,
+                                              const double* __restrict__ pin, const JacNb& n) {
+    JacIn v;
+    const size_t c = n.c;
+    const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+    v.rh = rhs[c];
+    v.pc = pin[c];
+    v.pxm = pin[n.xm];
+    v.pxp = pin[n.xp];
+    v.pym = pin[n.ym];
+    v.pyp = pin[n.yp];
+    v.pzm = pin[n.zm];
+    v.pzp = pin[n.zp];
+    if (FACE) {
+        v.rc = rhoc2[c];
+        v.dn = 0.0;
+        v.c0 = coef[c];
+        v.c1 = coef[c + 1];
+        v.c2 = coef[nc + c];
+        v.c3 = coef[nc + c + sy];
+        v.c4 = coef[2 * nc + c];
+        v.c5 = coef[2 * nc + c + sz];
+    } else {
+        const double* cf = coef + c;
+        v.c0 = cf[0];
+        v.c1 = cf[nc];
+        v.c2 = cf[2 * nc];
+        v.c3 = cf[3 * nc];
+        v.c4 = cf[4 * nc];
+        v.c5 = cf[5 * nc];
+        v.rc = cf[6 * nc];
+        v.dn = cf[7 * nc];
+    }
+    return v;
+}
+template <bool FACE>
+__device__ __forceinline__ double jacobi3_new(const JacIn& v, double dt2) {
+    if (FACE) {   // jacobi_face_update, dim 3
+        double coeff = v.rc * dt2;
+        double od = 0.0, diag = 0.0;
+        od += v.c0 * v.pxm + v.c1 * v.pxp;
+        diag += v.c0 + v.c1;
+        od += v.c2 * v.pym + v.c3 * v.pyp;
+        diag += v.c2 + v.c3;
+        od += v.c4 * v.pzm + v.c5 * v.pzp;
+        diag += v.c4 + v.c5;
+        double denom = 1.0 + coeff * diag;
+        return (v.rh + coeff * od) / denom;
+    }
+    double od = 0.0;   // jacobi_pre_update, dim 3
+    od += v.c0 * v.pxm + v.c1 * v.pxp;
+    od += v.c2 * v.pym + v.c3 * v.pyp;
+    od += v.c4 * v.pzm + v.c5 * v.pzp;
+    return (v.rh + v.rc * od) / v.dn;
+}
+template <bool FACE>
+__global__ void __launch_bounds__(256, 3) k_jacobi3(Params P, const double* __restrict__ coef, size_t nc,
                                                  const double* __restrict__ rhoc2, const double* __restrict__ rhs,
                                                  const double* __restrict__ pin, double* __restrict__ pout, Ctl* ctl,
                                                  int it, double tol) {
@@ -1215,12 +1277,18 @@ __global__ void __launch_bounds__(256) k_jacobi3(Params P, const double* __restr
         const double dt = ctl->dt;
         const double dt2 = dt * dt;
         const int k1 = min(k0 + kJacZ, P.nz);
-#pragma unroll 4
+        JacNb n = jacobi_nb(P, i, j, k0);
+        JacIn v = jacobi3_load<FACE>(P, coef, nc, rhoc2, rhs, pin, n);
         for (int k = k0; k < k1; ++k) {
-            const JacNb n = jacobi_nb(P, i, j, k);
-            const double r = FACE ? jacobi_face_update(P, coef, nc, rhoc2, rhs, pin, pout, dt2, n)
-                                  : jacobi_pre_update(P, coef, nc, rhs, pin, pout, n);
-            res = smax(res, r);
+            const size_t c = n.c;
+            const JacIn cur = v;
+            if (k + 1 < k1) {
+                n = jacobi_nb(P, i, j, k + 1);
+                v = jacobi3_load<FACE>(P, coef, nc, rhoc2, rhs, pin, n);
+            }
+            const double pn = jacobi3_new<FACE>(cur, dt2);
+            pout[c] = pn;
+            res = smax(res, fabs(pn - cur.pc));
         }
     }
     block_max_to(res, &ctl->res[it]);
@@ -1304,19 +1372,26 @@ __device__ __forceinline__ long long mx_nb(const Params& P, int i, int j, int k,
 // One FP32 sweep e_out = delta + J e_in, iteration `it` of the count; a no-op
 // once an earlier iteration's change fell below tol (as k_jacobi_pre), and
 // grid-stride with two cells in flight per thread as k_jacobi_pre.
+__device__ __forceinline__ double mx_sweep_update(const Params& P, const float* __restrict__ w,
+                                                  const float* __restrict__ d32, const float* __restrict__ ein,
+                                                  float* __restrict__ eout, long long n, long long t, long long xm,
+                                                  long long xp, long long ym, long long yp, long long zm,
+                                                  long long zp) {
+    float od = w[t] * ein[xm] + w[n + t] * ein[xp];
+    if (P.dim >= 2) od += w[2 * n + t] * ein[ym] + w[3 * n + t] * ein[yp];
+    if (P.dim >= 3) od += w[4 * n + t] * ein[zm] + w[5 * n + t] * ein[zp];
+    const float en = d32[t] + od;
+    eout[t] = en;
+    return (double)fabsf(en - ein[t]);
+}
 __device__ __forceinline__ double mx_sweep_cell(const Params& P, const float* __restrict__ w,
                                                 const float* __restrict__ d32, const float* __restrict__ ein,
                                                 float* __restrict__ eout, long long n, long long t) {
     int i, j, k;
     split3(t, P.nx, P.ny, i, j, k);
-    float od = w[t] * ein[mx_nb(P, i, j, k, 0, -1)] + w[n + t] * ein[mx_nb(P, i, j, k, 0, 1)];
-    if (P.dim >= 2)
-        od += w[2 * n + t] * ein[mx_nb(P, i, j, k, 1, -1)] + w[3 * n + t] * ein[mx_nb(P, i, j, k, 1, 1)];
-    if (P.dim >= 3)
-        od += w[4 * n + t] * ein[mx_nb(P, i, j, k, 2, -1)] + w[5 * n + t] * ein[mx_nb(P, i, j, k, 2, 1)];
-    const float en = d32[t] + od;
-    eout[t] = en;
-    return (double)fabsf(en - ein[t]);
+    return mx_sweep_update(P, w, d32, ein, eout, n, t, mx_nb(P, i, j, k, 0, -1), mx_nb(P, i, j, k, 0, 1),
+                           P.dim >= 2 ? mx_nb(P, i, j, k, 1, -1) : t, P.dim >= 2 ? mx_nb(P, i, j, k, 1, 1) : t,
+                           P.dim >= 3 ? mx_nb(P, i, j, k, 2, -1) : t, P.dim >= 3 ? mx_nb(P, i, j, k, 2, 1) : t);
 }
 __global__ void __launch_bounds__(256) k_mx_sweep(Params P, const float* __restrict__ w, const float* __restrict__ d32,
                                                   const float* __restrict__ ein, float* __restrict__ eout, Ctl* ctl,
@@ -1334,6 +1409,58 @@ __global__ void __launch_bounds__(256) k_mx_sweep(Params P, const float* __restr
         const double r1 = (t + stride < n) ? mx_sweep_cell(P, w, d32, ein, eout, n, t + stride) : 0.0;
         res = smax(res, r0);
         res = smax(res, r1);
+    }
+    block_max_to(res, &ctl->res[it]);
+}
+
+// 3D form of k_mx_sweep: the column walk of k_jacobi3 (interior indexing,
+// mx_nb's wrap / clamp per axis only where a neighbour leaves the domain,
+// the next cell's inputs in flight while the current one is computed).
+__global__ void __launch_bounds__(256) k_mx_sweep3(Params P, const float* __restrict__ w,
+                                                   const float* __restrict__ d32, const float* __restrict__ ein,
+                                                   float* __restrict__ eout, Ctl* ctl, int it, double tol) {
+    if (ctl->jacobiDone) return;
+    if (it > 0 && bits2d(ctl->res[it - 1]) < tol) {
+        if (threadIdx.x == 0) ctl->jacobiDone = it;
+        return;
+    }
+    const int i = (int)blockIdx.x * 32 + (int)(threadIdx.x & 31);
+    const int j = (int)blockIdx.y * 8 + (int)(threadIdx.x >> 5);
+    const int k0 = (int)blockIdx.z * kJacZ;
+    double res = 0.0;
+    if (i < P.nx && j < P.ny) {
+        const long long n = (long long)P.nx * P.ny * P.nz;
+        const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+        const long long dxm = scalar_src(i - 1, P.nx, P.bc[0], P.bc[1]) - i;
+        const long long dxp = scalar_src(i + 1, P.nx, P.bc[0], P.bc[1]) - i;
+        const long long dym = (scalar_src(j - 1, P.ny, P.bc[2], P.bc[3]) - j) * sy;
+        const long long dyp = (scalar_src(j + 1, P.ny, P.bc[2], P.bc[3]) - j) * sy;
+        const int k1 = min(k0 + kJacZ, P.nz);
+        // inputs of the next cell loaded before the current one is computed;
+        // the arithmetic is mx_sweep_update's (dim 3)
+        float v[14];
+        auto load = [&](int k) {
+            const long long t = i + sy * j + sz * k;
+            const long long zm = t + (scalar_src(k - 1, P.nz, P.bc[4], P.bc[5]) - k) * sz;
+            const long long zp = t + (scalar_src(k + 1, P.nz, P.bc[4], P.bc[5]) - k) * sz;
+            v[0] = w[t]; v[1] = ein[t + dxm]; v[2] = w[n + t]; v[3] = ein[t + dxp];
+            v[4] = w[2 * n + t]; v[5] = ein[t + dym]; v[6] = w[3 * n + t]; v[7] = ein[t + dyp];
+            v[8] = w[4 * n + t]; v[9] = ein[zm]; v[10] = w[5 * n + t]; v[11] = ein[zp];
+            v[12] = d32[t]; v[13] = ein[t];
+        };
+        load(k0);
+        for (int k = k0; k < k1; ++k) {
+            float u[14];
+#pragma unroll
+            for (int q = 0; q < 14; ++q) u[q] = v[q];
+            if (k + 1 < k1) load(k + 1);
+            float od = u[0] * u[1] + u[2] * u[3];
+            od += u[4] * u[5] + u[6] * u[7];
+            od += u[8] * u[9] + u[10] * u[11];
+            const float en = u[12] + od;
+            eout[i + sy * j + sz * k] = en;
+            res = smax(res, (double)fabsf(en - u[13]));
+        }
     }
     block_max_to(res, &ctl->res[it]);
 }
