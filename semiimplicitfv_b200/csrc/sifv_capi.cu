@@ -751,6 +751,7 @@ int jacobi_mixed_run(sifv_ctx* c, const double* rho, const double* rhoc2, const 
         c->mxGrid = (unsigned)std::max(1, sm * std::max(1, nb));
     }
     const unsigned gs = std::min(g, c->mxGrid);   // grid-stride FP32 sweeps
+    const dim3 g3((unsigned)((P.nx + 31) / 32), (unsigned)((P.ny + 7) / 8), (unsigned)((P.nz + kJacZ - 1) / kJacZ));
     constexpr int kInner = 8;   // FP32 sweeps per FP64 refinement
     int it = 0, done = 0;
     while (it < maxIter && !done) {
@@ -761,8 +762,12 @@ int jacobi_mixed_run(sifv_ctx* c, const double* rho, const double* rhoc2, const 
         const int first = it;
         ++it;
         for (int q = 1; q < kInner && it < maxIter; ++q, ++it) {
-            k_mx_sweep<<<gs, kCellThreads, 0, c->stream>>>(P, c->mxW, c->mxD, c->mxE[cur], c->mxE[cur ^ 1], c->ctl, it,
-                                                          tol);
+            if (P.dim == 3)
+                k_mx_sweep3<<<g3, 256, 0, c->stream>>>(P, c->mxW, c->mxD, c->mxE[cur], c->mxE[cur ^ 1], c->ctl, it,
+                                                       tol);
+            else
+                k_mx_sweep<<<gs, kCellThreads, 0, c->stream>>>(P, c->mxW, c->mxD, c->mxE[cur], c->mxE[cur ^ 1], c->ctl,
+                                                              it, tol);
             cur ^= 1;
         }
         c->launches += it - first;
