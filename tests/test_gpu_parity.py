@@ -160,6 +160,43 @@ def test_standalone_pressure_solve_dt_and_igr():
     assert np.array_equal(cg.get_field(abi.F_SIGMA), co.get_field(abi.F_SIGMA))
 
 
+@pytest.mark.parametrize("plant", ["sigma", "rho"])
+def test_igr_record_sweep_fallbacks(plant):
+    """The record sweep's exact-quotient guards: planted -0, tiny and huge
+    sigma values send those cells to plain divisions; densities of 1e200 put
+    face reciprocals outside the fast range, so the whole solve divides
+    plainly.  Either way sigma stays bit-identical to the oracle's sweeps."""
+    case = cases.acoustic_box(48, 34, 40, bc=abi.BC_PERIODIC)
+    cg = backends.make(backends.cuda(), case)
+    co = backends.make(backends.oracle(), case)
+    for c in (cg, co):
+        c.convert_cons_to_prim()
+        c.apply_bc()
+    if plant == "sigma":
+        sig = cg.get_field(abi.F_SIGMA)
+        flat = sig.reshape(-1)
+        rng = np.random.default_rng(5)
+        flat[:] = 1e-3 * rng.random(flat.size)
+        idx = rng.choice(flat.size, 400, replace=False)
+        flat[idx[0::4]] = -0.0
+        flat[idx[1::4]] = 1e-200
+        flat[idx[2::4]] = -1e200
+        flat[idx[3::4]] = 0.0
+        for c in (cg, co):
+            c.set_field(abi.F_SIGMA, sig)
+    else:
+        rho = cg.get_field(abi.F_RHO)
+        inner = cg.interior(rho)
+        inner[::7, ::5, ::9] = 1e200
+        for c in (cg, co):
+            c.set_field(abi.F_RHO, rho)
+            c.apply_bc()
+    for c in (cg, co):
+        c.igr_solve(1)
+    a, b = cg.get_field(abi.F_SIGMA), co.get_field(abi.F_SIGMA)
+    assert np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
 def test_not_converged_status():
     case = cases.acoustic3d(8)
     cg = backends.make(backends.cuda(), case)
