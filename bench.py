@@ -476,6 +476,31 @@ def run_cuda(args):
                           "family_ms_per_step": {k: v[0] for k, v in fam_m.items()},
                           "error_vs_fp64": err}}
 
+    def measure_pressure_solvers():
+        """Device time of the pressure solve of the first step after the
+        warm-up of the 256^3 semi-implicit workload with each pressure solver
+        (reference-ordered Jacobi and Gauss-Seidel, and PCG with a multigrid
+        V-cycle in place of Hypre's PCG + PFMG), from the per-family CUDA
+        events of sifv_profile_step, with the iteration count."""
+        out = {}
+        for name, kind in (("jacobi", abi.PRESSURE_JACOBI), ("gauss_seidel", abi.PRESSURE_GAUSS_SEIDEL),
+                           ("pcg_mg", abi.PRESSURE_PCG_MG)):
+            try:
+                case = cases.acoustic3d(SI_N)
+                ctx = backends.cuda().create(case[0], case[1], local)
+                ctx.set_state(case[2])
+                ctx.set_pressure_solver(kind)
+                t_sim = 0.0
+                for q in range(SI_WARM):
+                    t_sim += ctx.step(q, t_sim, -1.0)
+                fam = ctx.profile_step(SI_WARM, t_sim, -1.0)
+                out[name] = {"ms": fam[name][0], "iterations": ctx.last_pressure_iterations(),
+                             "step_ms": sum(v[0] for v in fam.values())}
+                ctx.close()
+            except Exception as e:   # a failed extra measurement must not cost the bench line
+                out[name] = {"error": str(e)[:200]}
+        return out
+
     def measure_adjoint():
         """Forward (recording) and reverse sweep of the vortex adjoint."""
         case = cases.vortex2d(ADJ_N)
@@ -682,6 +707,7 @@ def run_cuda(args):
             semi["roofline"]["frac"] = semi["roofline"]["achieved"] / peak
             srate, ssample = semi_cpu_rate(kind)
             semi["cpu_baseline"] = {"value": srate, "unit": UNIT, "cores": 1, "kind": kind, "sample": ssample}
+            semi["pressure_solvers"] = measure_pressure_solvers()
             result["semi_implicit"] = semi
         if adj is not None:
             adj["roofline"]["peak"] = peak
