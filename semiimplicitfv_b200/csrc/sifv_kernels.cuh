@@ -2042,23 +2042,41 @@ __global__ void __launch_bounds__(TY * TZ) k_gs_tile(Params P, const double* __r
     const int tb = (int)threadIdx.x % TY, tc = (int)threadIdx.x / TY;
     const bool act = tb < ey && tc < ez;
     const int hLine = ((tc + D3) * HY + (tb + 1)) * HX + 1;
-    const int dim = P.dim;
+    constexpr int DIM = D3 ? 3 : 2;
+    constexpr int NCO = 2 * DIM + 2;   // k_jacobi_coef's per-cell coefficients
     double maxRes = 0.0;
     __syncthreads();
     const int nq = ex + ey + ez - 2;
-    for (int q = 0; q < nq; ++q) {
+    // The coefficients and rhs of a thread's cells stream from global memory:
+    // those of cell a + 2 are loaded at cell plane q (cell a), into the
+    // register set that cell plane q + 2 computes with, so that their latency
+    // overlaps two cell planes.  The three sets rotate roles every plane
+    // (X computes, Z receives), with no copies between them.
+    double sA[NCO + 1], sB[NCO + 1], sC[NCO + 1];
+    auto step = [&](int q, double (&X)[NCO + 1], double (&Z)[NCO + 1]) {
         const int a = q - tb - tc;
+        if (act && a + 2 >= 0 && a + 2 < ex) {
+            const size_t c = cidx(P, i0 + a + 2, j0 + tb, k0 + tc);
+#pragma unroll
+            for (int k = 0; k < NCO; ++k) Z[k] = coef[c + (size_t)k * nc];
+            Z[NCO] = rhs[c];
+        }
+        if (q < 0 || q >= nq) return;
         if (act && a >= 0 && a < ex) {
             const int h = hLine + a;
-            const size_t c = cidx(P, i0 + a, j0 + tb, k0 + tc);
             const double nb[6] = {smem[h - 1], smem[h + 1], smem[h - HX], smem[h + HX],
                                   D3 ? smem[h - HX * HY] : 0.0, D3 ? smem[h + HX * HY] : 0.0};
             const double pOld = smem[h];
-            const double pn = gs_cell(dim, coef + c, nc, rhs[c], nb);
+            const double pn = gs_cell(DIM, X, 1, X[NCO], nb);
             smem[h] = pn;
             maxRes = smax(maxRes, fabs(pn - pOld));
         }
         __syncthreads();
+    };
+    for (int q = -2; q < nq; q += 3) {
+        step(q, sA, sC);
+        step(q + 1, sB, sA);
+        step(q + 2, sC, sB);
     }
     for (int line = warp; line < ey * ez; line += nwarp) {
         const int b = line % ey, c = line / ey;
