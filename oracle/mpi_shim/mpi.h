@@ -1,16 +1,26 @@
 /*
- * Single-rank MPI shim -- TEST INFRASTRUCTURE ONLY.
+ * MPI shim -- TEST INFRASTRUCTURE ONLY.
  *
  * Lets the SemiImplicitFV reference sources (C++17 + MPI) compile and run
- * as one rank in a container that has no MPI library, so that the
- * reference itself can serve as the parity oracle.  Only the symbols the
- * reference calls are provided.  Semantics for a communicator of size 1:
+ * in a container that has no MPI library, so that the reference itself can
+ * serve as the parity oracle and as the timed CPU baseline.  Only the
+ * symbols the reference calls are provided.
+ *
+ * By default the process is ONE rank:
  *   - MPI_Cart_shift returns rank 0 (self) for periodic directions and
  *     MPI_PROC_NULL otherwise, as a 1x1x1 Cartesian topology would
  *     (src/MPIContext.cpp:138-140 relies on this);
  *   - MPI_Isend / MPI_Irecv to self are matched by tag in MPI_Waitall
  *     (the periodic self-exchange of src/HaloExchange.cpp:387-408);
  *   - reductions and gathers copy the single contribution.
+ *
+ * sifv_mpi_shim_run(nranks, fn, user) runs fn(user, rank) on nranks
+ * threads that form MPI_COMM_WORLD together (the reference keeps no
+ * mutable static state, so its objects of every rank live in one
+ * process): MPI_Dims_create factorises as evenly as possible, Cartesian
+ * ranks are row-major with no reordering, sends are buffered copies,
+ * receives match (source, tag) in order, and reductions combine the
+ * contributions in rank order.  It returns when every rank has returned.
  */
 #ifndef SIFV_MPI_SHIM_H
 #define SIFV_MPI_SHIM_H
@@ -61,6 +71,8 @@ int MPI_Isend(const void* buf, int count, MPI_Datatype type, int dest, int tag,
 int MPI_Irecv(void* buf, int count, MPI_Datatype type, int source, int tag,
               MPI_Comm comm, MPI_Request* req);
 int MPI_Waitall(int count, MPI_Request reqs[], MPI_Status statuses[]);
+
+int sifv_mpi_shim_run(int nranks, void (*fn)(void* user, int rank), void* user);
 
 #ifdef __cplusplus
 }

@@ -36,8 +36,11 @@
 
 #include "sifv.h"
 
+#include <array>
+#include <chrono>
 #include <cstring>
 #include <exception>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <vector>
@@ -403,4 +406,124 @@ int sifvr_apply_ib_ghost_cells(sifvr_ctx* ctx) {
     return SIFV_OK;
 }
 
+// The reference's own solver decomposed over nranks MPI ranks (threads of
+// this process through the MPI shim's sifv_mpi_shim_run), as an MPI launch
+// of the reference's drivers would run it: MPIContext::create splits the
+// global mesh (src/MPIContext.cpp:80-170), HaloExchange moves the ghost
+// layers (src/HaloExchange.cpp:387-465) and dt / residuals are reduced over
+// the ranks.  Every rank copies the interior block of the global initial
+// fields init[f] (ghosts included, x fastest; its own ghosts start at
+// zero, as in the reference's drivers), takes `warmup` steps, then `steps`
+// steps between two barriers, and copies its interior block back into
+// out[f] (global arrays; may be null).  secondsOut = the timed steps' wall
+// time, maximum over the ranks; dtsOut (warmup + steps values, may be
+// null) = the time steps; dimsOut = the process grid.
+struct MpiRunArgs {
+    const sifv_config_t* cfg;
+    const sifv_mesh_t* mesh;
+    int nfields;
+    const int* fieldIds;
+    const double* const* init;
+    double* const* out;
+    int warmup, steps;
+    double seconds;
+    double* dts;
+    int dims[3];
+    int status;
+    std::mutex m;
+    std::string err;
+};
+
+static void mpi_rank_main(void* user, int rank) {
+    MpiRunArgs& A = *static_cast<MpiRunArgs*>(user);
+    sifvr_ctx* ctx = nullptr;
+    int st = sifvr_create(A.cfg, A.mesh, 0, &ctx);
+    if (st != SIFV_OK) {
+        std::lock_guard<std::mutex> lock(A.m);
+        A.status = st;
+        A.err = g_err;
+        return;   // every rank fails the same way (same configuration)
+    }
+    const int dim = ctx->config.dim, ng = ctx->config.nGhost;
+    const std::array<int, 6> ext = ctx->mpi->localExtent();
+    const int gng[3] = {ng, dim >= 2 ? ng : 0, dim >= 3 ? ng : 0};
+    const long long gnx = A.mesh->nx + 2LL * gng[0];
+    const long long gny = (dim >= 2 ? A.mesh->ny : 1) + 2LL * gng[1];
+    const RectilinearMesh& m = *ctx->mesh;
+    auto globalIndex = [&](int i, int j, int k) -> std::size_t {
+        return static_cast<std::size_t>(((long long)(k + ext[4] + gng[2]) * gny + (j + ext[2] + gng[1])) * gnx +
+                                        (i + ext[0] + gng[0]));
+    };
+    for (int f = 0; f < A.nfields; ++f) {
+        std::vector<double>* v = fieldVec(ctx, A.fieldIds[f]);
+        if (!v || v->empty() || !A.init || !A.init[f]) continue;
+        std::fill(v->begin(), v->end(), 0.0);
+        for (int k = 0; k < m.nz(); ++k)
+            for (int j = 0; j < m.ny(); ++j)
+                for (int i = 0; i < m.nx(); ++i) (*v)[m.index(i, j, k)] = A.init[f][globalIndex(i, j, k)];
+    }
+    double t = 0.0;
+    int step = 0;
+    auto one = [&]() {
+        double dt = 0.0;
+        if (sifvr_step(ctx, step, t, -1.0, &dt) != SIFV_OK) {
+            std::lock_guard<std::mutex> lock(A.m);
+            A.status = SIFV_ERR_BAD_ARG;
+            A.err = ctx->err;
+        }
+        if (rank == 0 && A.dts) A.dts[step] = dt;
+        t += dt;
+        ++step;
+    };
+    for (int q = 0; q < A.warmup; ++q) one();
+    double token = 0.0;
+    MPI_Allreduce(MPI_IN_PLACE, &token, 1, MPI_DOUBLE, MPI_MAX, MPI_COMM_WORLD);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int q = 0; q < A.steps; ++q) one();
+    MPI_Allreduce(MPI_IN_PLACE, &token, 1, MPI_DOUBLE, MPI_MAX, MPI_COMM_WORLD);
+    double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    MPI_Allreduce(MPI_IN_PLACE, &sec, 1, MPI_DOUBLE, MPI_MAX, MPI_COMM_WORLD);
+    for (int f = 0; f < A.nfields && A.out; ++f) {
+        std::vector<double>* v = fieldVec(ctx, A.fieldIds[f]);
+        if (!v || v->empty() || !A.out[f]) continue;
+        for (int k = 0; k < m.nz(); ++k)
+            for (int j = 0; j < m.ny(); ++j)
+                for (int i = 0; i < m.nx(); ++i) A.out[f][globalIndex(i, j, k)] = (*v)[m.index(i, j, k)];
+    }
+    if (rank == 0) {
+        A.seconds = sec;
+        for (int d = 0; d < 3; ++d) A.dims[d] = ctx->mpi->dims()[d];
+    }
+    sifvr_destroy(ctx);
+}
+
+int sifvr_mpi_run(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int nranks, int nfields, const int* fieldIds,
+                  const double* const* init, double* const* out, int warmup, int steps, double* secondsOut,
+                  double* dtsOut, int* dimsOut) {
+    if (!cfg || !mesh || nranks < 1 || warmup < 0 || steps < 0) return SIFV_ERR_BAD_ARG;
+    MpiRunArgs A;
+    A.cfg = cfg;
+    A.mesh = mesh;
+    A.nfields = nfields;
+    A.fieldIds = fieldIds;
+    A.init = init;
+    A.out = out;
+    A.warmup = warmup;
+    A.steps = steps;
+    A.seconds = 0.0;
+    A.dts = dtsOut;
+    A.dims[0] = A.dims[1] = A.dims[2] = 0;
+    A.status = SIFV_OK;
+    if (sifv_mpi_shim_run(nranks, mpi_rank_main, &A) != 0) return SIFV_ERR_BAD_ARG;
+    if (A.status != SIFV_OK) {
+        g_err = A.err;
+        return A.status;
+    }
+    if (secondsOut) *secondsOut = A.seconds;
+    if (dimsOut)
+        for (int d = 0; d < 3; ++d) dimsOut[d] = A.dims[d];
+    return SIFV_OK;
+}
+
 }  // extern "C"
+

@@ -36,9 +36,11 @@ def reference(release: bool = False):
     if key not in _cache:
         path = os.path.join(ORACLE_DIR, "_ref", "libsifv_ref_release.so" if release else "libsifv_ref.so")
         if not os.path.exists(path):
-            ref_src = "/root/reference/src/ExplicitSolver.cpp"
-            if os.path.exists(ref_src):
-                subprocess.run(["make", "-s", "-j8", "-C", ORACLE_DIR, "ref"], check=True)
+            # oracle/Makefile builds it where the reference sources are present
+            # (SIFV_REFERENCE_DIR overrides its default location), else skips
+            ref = os.environ.get("SIFV_REFERENCE_DIR")
+            subprocess.run(["make", "-s", "-j8", "-C", ORACLE_DIR, "ref"] + ([f"REF={ref}"] if ref else []),
+                           check=True, stdout=subprocess.DEVNULL)
         if not os.path.exists(path):
             _cache[key] = None
         else:
@@ -59,3 +61,34 @@ def make(backend: abi.Backend, case):
     ctx = backend.create(cfg, mesh)
     ctx.set_state(fields)
     return ctx
+
+
+def mpi_run(backend: abi.Backend, case, nranks: int, warmup: int, steps: int, fids=None, gather: bool = True):
+    """Run the reference's own solver on ``case`` decomposed over ``nranks``
+    MPI ranks (threads of this process through the MPI shim):
+    ``warmup`` steps, then ``steps`` timed steps.  Returns (seconds of the
+    timed steps, max over ranks; the dts of all steps; the process grid;
+    {field id: global array} of the final state when ``gather``)."""
+    import numpy as np
+    f = backend.lib.sifvr_mpi_run
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.POINTER(abi.Config), ctypes.POINTER(abi.Mesh), ctypes.c_int, ctypes.c_int,
+                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                  ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                  ctypes.POINTER(ctypes.c_int)]
+    cfg, mesh, fields = case
+    fids = list(fields) if fids is None else list(fids)
+    init = [np.ascontiguousarray(fields[k], dtype=np.float64) for k in fids]
+    out = [np.zeros_like(a) for a in init] if gather else None
+    ids = (ctypes.c_int * len(fids))(*fids)
+    pin = (ctypes.c_void_p * len(fids))(*[a.ctypes.data for a in init])
+    pout = (ctypes.c_void_p * len(fids))(*[a.ctypes.data for a in out]) if gather else None
+    sec = ctypes.c_double()
+    dts = (ctypes.c_double * max(warmup + steps, 1))()
+    dims = (ctypes.c_int * 3)()
+    ms = mesh.cstruct()
+    st = f(ctypes.byref(cfg), ctypes.byref(ms), nranks, len(fids), ids, pin, pout, warmup, steps,
+           ctypes.byref(sec), dts, dims)
+    if st != abi.OK:
+        raise abi.AbiError(st, backend.error(None))
+    return sec.value, list(dts)[:warmup + steps], tuple(dims), (dict(zip(fids, out)) if gather else None)
