@@ -66,6 +66,7 @@ NCU_PIPE_FRAC = {(2, "tile2d"): {"fp64": 0.688, "fma_fp32": 0.053, "issue_active
                  (1, "tile2d"): {"fp64": 0.072, "fma_fp32": 0.460, "issue_active": 0.807}}
 # Fields a 2D step reads and writes (host-authoritative drop-in round trip).
 E2E_FIELDS_2D = ("F_RHO", "F_RHOU", "F_RHOV", "F_RHOE", "F_VELU", "F_VELV", "F_PRES")
+CONS_NAMES_2D = ("rho", "rhoU", "rhoV", "rhoE")
 # Batched ensemble of two-phase water-air tubes: count, cell range, end time.
 ENS_COUNT, ENS_NMIN, ENS_NMAX, ENS_TEND, ENS_SEED = 2048, 256, 16384, 1e-4, 0
 ENS_BYTES_PER_CELL_UPDATE = 384   # state alphaRho0, alphaRho1, rhoU, rhoE, alpha0, alpha1: 64 B x 6
@@ -241,34 +242,61 @@ def cpu_rate(kind: str, n: int, steps: int) -> float:
     return n * n * steps / dt
 
 
-def _cpu_worker(args):
-    kind, n, steps = args
-    return cpu_rate(kind, n, steps)
+def _host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def workload_config(n: int) -> dict:
+    """The `config` object both arms print (the same workload)."""
+    return {"workload": f"2D four-quadrant Riemann {n}x{n} (+3 ghosts), WENO5+HLLC SSP-RK3 CFL0.6, outflow",
+            "l2": (f"inputs larger than L2 (state 4 x {n * n * 8 / 1e6:.0f} MB)" if 4 * n * n * 8 > 126e6
+                   else f"state 4 x {n * n * 8 / 1e6:.0f} MB fits in L2")}
+
+
+def reference_decomposed_rate(n: int, warmup: int, steps: int, ranks: int):
+    """The reference's own solver on the n x n workload, decomposed over
+    `ranks` MPI ranks (threads through the MPI shim; the reference is
+    single-threaded per rank): `warmup` steps, then `steps` timed steps.
+    Returns (cell-updates/s, seconds, process grid)."""
+    import backends
+    import cases
+    be = backends.reference(release=True)
+    sec, _, dims, _ = backends.mpi_run(be, cases.riemann2d(n), ranks, warmup, steps, gather=False)
+    return n * n * steps / sec, sec, dims
 
 
 def run_reference(args):
+    """--impl reference: the reference's CPU solver on the same 4096^2
+    workload, all host cores (one MPI rank per core through the MPI shim,
+    the reference's own domain decomposition and halo exchange), W warm-up
+    steps then K timed steps of the full grid."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
     import backends
-    kind = "reference" if backends.reference(release=True) is not None else "port"
-    procs = os.cpu_count() or 1
-    n = 512
-    steps = max(args.steps, 1)
-    t0 = time.perf_counter()
-    with mp.get_context("spawn").Pool(procs) as pool:
-        rates = pool.map(_cpu_worker, [(kind, n, steps)] * procs)
-    wall = time.perf_counter() - t0
-    value = float(sum(rates))
+    n = args.n
+    cores = _host_cores()
+    if backends.reference(release=True) is not None:
+        value, sec, dims = reference_decomposed_rate(n, args.warmup, args.steps, cores)
+        kind = "reference"
+        sample = (f"{n}x{n}, {args.warmup} warm-up + {args.steps} timed steps of the full grid, decomposed over "
+                  f"{cores} MPI ranks ({dims[0]}x{dims[1]}; threads of one process through the MPI shim), "
+                  f"reference built with its Release flags; wall {sec:.1f} s for the timed steps")
+    else:   # the reference sources were never built here: the oracle port on one core, bounded sample
+        value = cpu_rate("port", 768, 3)
+        sec = n * n * args.steps / value
+        kind, cores = "port", 1
+        sample = "C restatement on one core, 768x768 instance, 3 steps (reference build absent)"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 4096 * 4096 / value * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "2D four-quadrant Riemann 4096x4096 (sampled as independent 512x512 instances)",
-                   "scheme": "WENO5+HLLC SSP-RK3 CFL0.6"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
-                         "sample": f"{procs} concurrent single-thread processes, each {steps} steps of a "
-                                   f"{n}x{n} instance (reference is single-threaded per rank); wall {wall:.1f}s"},
+        "precision": "fp64 (the reference's CPU solver)",
+        "config": workload_config(n),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -290,6 +318,7 @@ def run_cuda(args):
     import backends
     import cases
     from semiimplicitfv_b200 import abi
+    CONS_2D = (abi.F_RHO, abi.F_RHOU, abi.F_RHOV, abi.F_RHOE)
     n = args.n
     cells = n * n
     stream = torch.cuda.current_stream()
@@ -338,7 +367,9 @@ def run_cuda(args):
         step_idx += args.steps
         _, launches = ctx.last_step_stats()
         out = {"ms": ms, "value": ws * cells * args.steps / (ms / 1e3), "launches": launches,
-               "clocks": clk.summary() if clk else None}
+               "clocks": clk.summary() if clk else None, "t": t_sim,
+               # the conservative state after the warm-up and timed steps (error against FP64)
+               "state": {f: ctx.interior(ctx.get_field(f)).copy() for f in CONS_2D} if rank == 0 else None}
         if with_clocks:
             # per-kernel-family device time of two more steps (CUDA events on the launch stream)
             fam = {}
@@ -380,6 +411,23 @@ def run_cuda(args):
             out["e2e_bytes"] = len(fids) * ctx.ncells * 8
         ctx.close()
         return out
+
+    def measure_fine(t_final):
+        """The same problem on a 2n x 2n grid, reference-ordered FP64, run
+        to t_final, averaged over 2 x 2 blocks onto the n x n cells (exact
+        restriction of finite-volume cell averages): the reference solution
+        of the discretisation error."""
+        case = cases.riemann2d(2 * n)
+        case[0].precision = abi.PREC_FP64
+        ctx = backends.cuda().create(case[0], case[1], local)
+        ctx.set_state(case[2])
+        t, steps = ctx.advance(0, 0.0, t_final, 100000)
+        fine = {}
+        for f in CONS_2D:
+            a = ctx.interior(ctx.get_field(f))[0]
+            fine[f] = 0.25 * (a[0::2, 0::2] + a[1::2, 0::2] + a[0::2, 1::2] + a[1::2, 1::2])[None]
+        ctx.close()
+        return fine, t, steps
 
     def measure_ensemble(precision, with_clocks=False, with_e2e=False):
         """The batched-ensemble workload in one launch per rank (ranks take
@@ -644,6 +692,33 @@ def run_cuda(args):
         emx["e2e"] = emx["cell_updates"] / mor(emx["e2e_s"], dev)
         ens = {"mixed": emx, "fp64": e64, "l1_rel_max": mor(float(max(rel)), dev),
                "l1_rel_mean": float(np.mean(rel)), "linf_rel_max": mor(float(max(linf)), dev)}
+    accuracy = None
+    if rank == 0 and not args.quick and PREC_NAMES[0] in extra:
+        # every result's L1 / L-inf error against the FP64 (reference-ordered)
+        # state after the same steps, and against the 2n x 2n FP64 solution
+        # at the same time (the discretisation error)
+        runs = {PREC_NAMES[args.precision]: main, **extra}
+        ref = runs[PREC_NAMES[0]]
+        fine, t_fine, fine_steps = measure_fine(ref["t"])
+
+        def err(a, b):
+            d = np.abs(a - b)
+            return {"l1": float(d.mean()), "l1_rel": float(d.mean() / np.abs(b).mean()),
+                    "linf_rel": float(d.max() / np.abs(b).max())}
+        accuracy = {"vs_fp64": {}, "vs_fine_grid": {},
+                    "fine_grid": f"{2 * n}x{2 * n} reference-ordered FP64 to the same t = {t_fine:.6e} "
+                                 f"({fine_steps} steps), 2x2-block averages"}
+        for name, r in runs.items():
+            if name != PREC_NAMES[0]:
+                accuracy["vs_fp64"][name] = {v: err(r["state"][f], ref["state"][f]) for f, v in zip(CONS_2D, CONS_NAMES_2D)}
+            accuracy["vs_fine_grid"][name] = {v: err(r["state"][f], fine[f]) for f, v in zip(CONS_2D, CONS_NAMES_2D)}
+        d64 = accuracy["vs_fine_grid"][PREC_NAMES[0]]
+        for name in runs:
+            if name != PREC_NAMES[0]:
+                accuracy["vs_fine_grid"][name]["l1_over_fp64"] = max(
+                    accuracy["vs_fine_grid"][name][v]["l1"] / max(d64[v]["l1"], 1e-300) for v in CONS_NAMES_2D)
+        for r in runs.values():
+            r.pop("state", None)
     ms = main["ms"]
     value = main["value"]
     launches = main["launches"]
@@ -666,17 +741,21 @@ def run_cuda(args):
     result = None
     if rank == 0:
         kind = "reference" if backends.reference(release=True) is not None else "port"
-        cpu_n, cpu_steps = 768, 3
-        cpu = cpu_rate(kind, cpu_n, cpu_steps)
+        if kind == "reference":   # bounded sample: 1 + 2 steps of the same grid on all host cores
+            cpu_cores = _host_cores()
+            cpu, cpu_sec, cpu_dims = reference_decomposed_rate(n, 1, 2, cpu_cores)
+            cpu_sample = (f"{n}x{n}, 1 warm-up + 2 timed steps of the full grid, decomposed over {cpu_cores} MPI "
+                          f"ranks ({cpu_dims[0]}x{cpu_dims[1]}, threads through the MPI shim), Release flags")
+        else:
+            cpu_cores, cpu = 1, cpu_rate(kind, 768, 3)
+            cpu_sample = "C restatement on one core, 768x768 instance, 3 steps"
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision != 1 else "f32-bulk/f64-state",
             "data": "synthetic",
-            "config": {"workload": f"2D four-quadrant Riemann {n}x{n} (+3 ghosts), WENO5+HLLC SSP-RK3 CFL0.6, "
-                                   "outflow, state resident in HBM",
-                       "precision": PREC_NAMES[args.precision],
-                       "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (4 x 134 MB state)"},
+            "precision": PREC_NAMES[args.precision], "parallelism": f"replicas x{ws}",
+            "config": workload_config(n),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "traffic_source": "ncu dram bytes per cell on the 2048^2 case x cells",
@@ -686,10 +765,8 @@ def run_cuda(args):
                                   "bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
                          "kernel_ms_per_step": {k: v[0] / 2 for k, v in fam.items()},
                          "compute_co_bound": dict(NCU_PIPE_FRAC.get((args.precision, dom), {}),
-                                                  source="ncu on the 2048^2 case of this workload "
-                                                         "(profiles/tile2d_stage_riemann2d_2048.md)")},
-            "cpu_baseline": {"value": cpu, "unit": UNIT, "cores": 1, "kind": kind,
-                             "sample": f"{cpu_n}x{cpu_n} instance, {cpu_steps} steps, 1 thread"},
+                                                  source="ncu on the 2048^2 case of this workload")},
+            "cpu_baseline": {"value": cpu, "unit": UNIT, "cores": cpu_cores, "kind": kind, "sample": cpu_sample},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": main["e2e_bytes"],
                     "d2h_bytes_per_step": main["e2e_bytes"] + 8,
                     "api": "per step: sifv_set_field x7 from pinned host buffers, sifv_step (dt to the host), "
@@ -699,8 +776,11 @@ def run_cuda(args):
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "other_precisions": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
-                                     "roofline_frac": BYTES_PER_CELL_UPDATE * v["value"] / 1e9 / peak}
+                                     "roofline_frac": BYTES_PER_CELL_UPDATE * v["value"] / 1e9 / peak,
+                                     "error_vs_fp64": (accuracy or {}).get("vs_fp64", {}).get(k)}
                                  for k, v in extra.items()},
+            "error_vs_fp64": (accuracy or {}).get("vs_fp64", {}).get(PREC_NAMES[args.precision]),
+            "accuracy": accuracy,
         }
         if semi is not None:
             semi["roofline"]["peak"] = peak

@@ -30,6 +30,7 @@ namespace {
 namespace {
 
 using sifv_nal_ctl = sifv::Ctl;
+using CUresult_t = int;   // the driver API's CUresult (0 = success)
 
 // Sizes of the static scratch (SIFV_NOALLOC_* in include/sifv.h).
 constexpr size_t kMaxCells = SIFV_NOALLOC_MAX_CELLS;
@@ -47,7 +48,15 @@ constexpr size_t kTotal = kCtl + 2 * kMaxCells + 3 * (size_t)kMaxAxis;
 static __device__ __align__(256) double g_noalloc_scratch[kTotal];
 
 constexpr int kMaxDevices = 64;
-double* g_scratch_addr[kMaxDevices] = {nullptr};
+// Per device: the id of the CUDA context the address was looked up in, and
+// the address.  A device reset, or another context made current on the same
+// device, loads the module again, possibly at another address, so the
+// address is looked up again whenever the current context's id changes.
+struct ScratchSlot {
+    unsigned long long ctxId;
+    double* addr;
+};
+ScratchSlot g_scratch[kMaxDevices] = {};
 std::mutex g_setup_mutex;
 thread_local std::string g_noalloc_err;
 thread_local double g_width_buf[kMaxAxis];   // host staging of one axis' widths
@@ -57,24 +66,65 @@ int nal_fail(int code, const char* msg) {
     return code;
 }
 
+// Driver entry points cuCtxGetCurrent / cuCtxGetId, reached through the
+// runtime's entry-point table so that the library needs no link against
+// the driver library.
+using CtxGetCurrent = CUresult_t (*)(void**);
+using CtxGetId = CUresult_t (*)(void*, unsigned long long*);
+
+int driver_entry_points(CtxGetCurrent* getCurrent, CtxGetId* getId) {
+    static CtxGetCurrent gc = nullptr;
+    static CtxGetId gi = nullptr;
+    if (!gc || !gi) {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            qa != cudaDriverEntryPointSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+            qb != cudaDriverEntryPointSuccess)
+            return nal_fail(SIFV_ERR_CUDA, "driver entry points cuCtxGetCurrent / cuCtxGetId not found");
+        gc = reinterpret_cast<CtxGetCurrent>(a);
+        gi = reinterpret_cast<CtxGetId>(b);
+    }
+    *getCurrent = gc;
+    *getId = gi;
+    return SIFV_OK;
+}
+
 // Device address of the static array on the current device.  The host-side
 // name g_noalloc_scratch is only a stand-in, so the address is looked up
-// once per device with that device current.
+// (cudaGetSymbolAddress) with the device current, once per device and
+// context, and kept for later calls.  When no context is current yet, the
+// look-up itself initialises the device's primary context.
 int scratch_for_current_device(double** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return nal_fail(SIFV_ERR_CUDA, "cudaGetDevice failed");
     if (dev < 0 || dev >= kMaxDevices) return nal_fail(SIFV_ERR_UNSUPPORTED, "device index above 63");
+    CtxGetCurrent getCurrent = nullptr;
+    CtxGetId getId = nullptr;
+    int st = driver_entry_points(&getCurrent, &getId);
+    if (st != SIFV_OK) return st;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (getCurrent(&ctx) != 0) return nal_fail(SIFV_ERR_CUDA, "cuCtxGetCurrent failed");
+    if (ctx && getId(ctx, &id) != 0) return nal_fail(SIFV_ERR_CUDA, "cuCtxGetId failed");
+    if (!ctx || !g_scratch[dev].addr || g_scratch[dev].ctxId != id) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) {
             g_noalloc_err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
             return SIFV_ERR_CUDA;
         }
-        g_scratch_addr[dev] = static_cast<double*>(p);
+        if (!ctx) {   // the look-up made the primary context current
+            if (getCurrent(&ctx) != 0 || !ctx || getId(ctx, &id) != 0)
+                return nal_fail(SIFV_ERR_CUDA, "no current CUDA context after initialisation");
+        }
+        g_scratch[dev].addr = static_cast<double*>(p);
+        g_scratch[dev].ctxId = id;
     }
-    *out = g_scratch_addr[dev];
+    *out = g_scratch[dev].addr;
     return SIFV_OK;
 }
 
