@@ -71,6 +71,11 @@ extern "C" {
 #define SIFV_BC_PERIODIC   2
 #define SIFV_BC_SLIPWALL   3
 #define SIFV_BC_NOSLIPWALL 4
+/* A face shared with a neighbouring rank of a domain decomposition (the
+ * reference's non-physical MPI faces, src/MPIContext.cpp:80-170): its ghost
+ * layers hold the neighbour's cells, filled by the context's halo exchange
+ * (sifv_set_comm), instead of a boundary condition. */
+#define SIFV_BC_EXCHANGE   16
 /* single-phase EOS: IdealGasEOS (src/IdealGasEOS.cpp) or StiffenedGasEOS (src/StiffenedGasEOS.cpp) */
 #define SIFV_EOS_IDEAL     0
 #define SIFV_EOS_STIFFENED 1
@@ -464,6 +469,37 @@ int sifv_ensemble_run(sifv_ensemble_t* e, double tEnd, int maxSteps, int blockSi
  * block size for later runs and restore the state. */
 int sifv_ensemble_autotune(sifv_ensemble_t* e, int probeSteps, int* blockSizeOut);
 
+/* ---- domain decomposition (one rank per GPU) -------------------------- */
+/* The halo exchange and dt reduction of a context whose mesh has
+ * SIFV_BC_EXCHANGE faces: HaloExchange::exchangeStateDirection
+ * (src/HaloExchange.cpp:387-465) and the MPI_Allreduce of the time step
+ * (src/RKTimeStepping.cpp:148-159), supplied by the caller (NCCL, MPI, or
+ * host copies).  The library calls them while it queues a step on its
+ * stream:
+ *   exchange(user, fields, nfields, stream): fields are nfields arrays of
+ *     the context's extended grid (device arrays; host arrays for a CPU
+ *     backend).  For every SIFV_BC_EXCHANGE face, send the nGhost layers of
+ *     cells next to the face to the neighbour across it and receive the
+ *     neighbour's into this context's nGhost ghost layers of that face,
+ *     ordered after the work already on `stream` and before the work queued
+ *     after the call.  The fields are the conservative state the next
+ *     stage reads (rho, rhoU, [rhoV], [rhoW], rhoE, then alphaRho / alpha of
+ *     each phase).
+ *   allreduce_min(user, value, stream): replace the non-negative double at
+ *     device address `value` by its minimum over all ranks, ordered the same
+ *     way.
+ * Both return 0 on success; a non-zero return ends the step with
+ * SIFV_ERR_CUDA.  The explicit step supports exchange faces (reference
+ * order in 1-3D, the fast / mixed 2D step); the semi-implicit step, IGR,
+ * viscous / capillary terms and immersed boundaries are rejected with
+ * SIFV_ERR_UNSUPPORTED.  A NULL comm clears the hooks. */
+typedef struct sifv_comm {
+    int (*exchange)(void* user, double* const* fields, int nfields, void* stream);
+    int (*allreduce_min)(void* user, double* value, void* stream);
+    void* user;
+} sifv_comm_t;
+int sifv_set_comm(sifv_ctx_t* ctx, const sifv_comm_t* comm);
+
 /* ---- allocation-free pressure solve ----------------------------------- */
 /* Sizes of the static device scratch behind sifv_pressure_solve_noalloc
  * (reserved on every GPU that loads the library, about 32 MB). */
@@ -485,11 +521,17 @@ int sifv_ensemble_autotune(sifv_ensemble_t* e, int probeSteps, int* blockSizeOut
  * initial guess and receives the solution in its interior cells (ghosts
  * untouched).  Work is queued on `stream` (NULL: the legacy default
  * stream).  Meshes or maxIter above the SIFV_NOALLOC_* limits are rejected
- * with SIFV_ERR_BAD_ARG.  The first call on a device looks up the static
- * array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture.  All calls on a device
- * share the one array: calls that overlap on the GPU race and must be
- * serialised by the caller.  Errors: sifv_noalloc_last_error(). */
+ * with SIFV_ERR_BAD_ARG.  The first call on a device (and the first after
+ * a device reset, or under another context on that device) looks up the
+ * static array's device address (cudaGetSymbolAddress) with that device
+ * current and keeps it for later calls; make that first call before any
+ * stream capture.  Each call waits on `stream` (cudaStreamSynchronize)
+ * while it runs: it reads the convergence flag back to the host between
+ * batches of iterations, and it returns once the solution is in `pressure`.
+ * All calls on a device share the one array and find the previous call's
+ * contents there (the call clears what must start at zero): calls that
+ * overlap on the GPU race and must be serialised by the caller.
+ * Errors: sifv_noalloc_last_error(). */
 int sifv_pressure_solve_noalloc(const sifv_mesh_t* mesh, int dim, int nGhost, const double* rho,
                                 const double* rhoc2, const double* rhs, double* pressure, double dt,
                                 double tol, int maxIter, void* stream, int* iters);

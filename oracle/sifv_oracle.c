@@ -71,6 +71,10 @@ typedef struct sifvo_ctx {
     int ibCount;
     sifv_ib_body_t* ibBodies;
     int ibNBodies;
+    /* domain decomposition: faces with SIFV_BC_EXCHANGE, and the caller's
+     * halo exchange / dt reduction (sifv_comm_t) */
+    int exchangeFaces;
+    sifv_comm_t comm;
     char err[256];
 } ctx_t;
 
@@ -143,46 +147,59 @@ static int ghost_src(int bc, int high, int g, int n, double* s_norm, double* s_a
     }
 }
 
-/* RectilinearMesh::applyBoundaryConditions (PRIM), src/RectilinearMesh.cpp:127-418 */
+/* RectilinearMesh::applyBoundaryConditions (PRIM), src/RectilinearMesh.cpp:127-418;
+ * with exchange faces (src/RectilinearMesh.cpp:498-524) the exchanged ghost
+ * layers stay as converted, and the fills of the faster axes also cover
+ * them (the reference's exchanged slabs carry the neighbour's already
+ * filled ghosts of those axes). */
 static void apply_bc_prim(ctx_t* m) {
     double sn, sa;
+    const int EX = SIFV_BC_EXCHANGE;
+    const int jlo = (m->dim >= 2 && m->bc[2] == EX) ? -m->ngy : 0, jhi = m->ny + ((m->dim >= 2 && m->bc[3] == EX) ? m->ngy : 0);
+    const int klo = (m->dim >= 3 && m->bc[4] == EX) ? -m->ngz : 0, khi = m->nz + ((m->dim >= 3 && m->bc[5] == EX) ? m->ngz : 0);
     /* fillGhostX, src/RectilinearMesh.cpp:137-224 */
-    for (int k = 0; k < m->nz; ++k)
-        for (int j = 0; j < m->ny; ++j) {
-            for (int g = 1; g <= m->ngx; ++g) {
-                int si = ghost_src(m->bc[0], 0, g, m->nx, &sn, &sa);
-                copy_cell_p(m, IDX(m, -g, j, k), IDX(m, si, j, k), sn * sa, sa, sa);
-            }
-            for (int g = 1; g <= m->ngx; ++g) {
-                int si = ghost_src(m->bc[1], 1, g, m->nx, &sn, &sa);
-                copy_cell_p(m, IDX(m, m->nx - 1 + g, j, k), IDX(m, si, j, k), sn * sa, sa, sa);
-            }
+    for (int k = klo; k < khi; ++k)
+        for (int j = jlo; j < jhi; ++j) {
+            if (m->bc[0] != EX)
+                for (int g = 1; g <= m->ngx; ++g) {
+                    int si = ghost_src(m->bc[0], 0, g, m->nx, &sn, &sa);
+                    copy_cell_p(m, IDX(m, -g, j, k), IDX(m, si, j, k), sn * sa, sa, sa);
+                }
+            if (m->bc[1] != EX)
+                for (int g = 1; g <= m->ngx; ++g) {
+                    int si = ghost_src(m->bc[1], 1, g, m->nx, &sn, &sa);
+                    copy_cell_p(m, IDX(m, m->nx - 1 + g, j, k), IDX(m, si, j, k), sn * sa, sa, sa);
+                }
         }
     /* fillGhostY, src/RectilinearMesh.cpp:230-320 */
     if (m->dim >= 2)
-        for (int k = 0; k < m->nz; ++k)
+        for (int k = klo; k < khi; ++k)
             for (int i = -m->ngx; i < m->nx + m->ngx; ++i) {
-                for (int g = 1; g <= m->ngy; ++g) {
-                    int sj = ghost_src(m->bc[2], 0, g, m->ny, &sn, &sa);
-                    copy_cell_p(m, IDX(m, i, -g, k), IDX(m, i, sj, k), sa, sn * sa, sa);
-                }
-                for (int g = 1; g <= m->ngy; ++g) {
-                    int sj = ghost_src(m->bc[3], 1, g, m->ny, &sn, &sa);
-                    copy_cell_p(m, IDX(m, i, m->ny - 1 + g, k), IDX(m, i, sj, k), sa, sn * sa, sa);
-                }
+                if (m->bc[2] != EX)
+                    for (int g = 1; g <= m->ngy; ++g) {
+                        int sj = ghost_src(m->bc[2], 0, g, m->ny, &sn, &sa);
+                        copy_cell_p(m, IDX(m, i, -g, k), IDX(m, i, sj, k), sa, sn * sa, sa);
+                    }
+                if (m->bc[3] != EX)
+                    for (int g = 1; g <= m->ngy; ++g) {
+                        int sj = ghost_src(m->bc[3], 1, g, m->ny, &sn, &sa);
+                        copy_cell_p(m, IDX(m, i, m->ny - 1 + g, k), IDX(m, i, sj, k), sa, sn * sa, sa);
+                    }
             }
     /* fillGhostZ, src/RectilinearMesh.cpp:326-418 */
     if (m->dim >= 3)
         for (int j = -m->ngy; j < m->ny + m->ngy; ++j)
             for (int i = -m->ngx; i < m->nx + m->ngx; ++i) {
-                for (int g = 1; g <= m->ngz; ++g) {
-                    int sk = ghost_src(m->bc[4], 0, g, m->nz, &sn, &sa);
-                    copy_cell_p(m, IDX(m, i, j, -g), IDX(m, i, j, sk), sa, sa, sn * sa);
-                }
-                for (int g = 1; g <= m->ngz; ++g) {
-                    int sk = ghost_src(m->bc[5], 1, g, m->nz, &sn, &sa);
-                    copy_cell_p(m, IDX(m, i, j, m->nz - 1 + g), IDX(m, i, j, sk), sa, sa, sn * sa);
-                }
+                if (m->bc[4] != EX)
+                    for (int g = 1; g <= m->ngz; ++g) {
+                        int sk = ghost_src(m->bc[4], 0, g, m->nz, &sn, &sa);
+                        copy_cell_p(m, IDX(m, i, j, -g), IDX(m, i, j, sk), sa, sa, sn * sa);
+                    }
+                if (m->bc[5] != EX)
+                    for (int g = 1; g <= m->ngz; ++g) {
+                        int sk = ghost_src(m->bc[5], 1, g, m->nz, &sn, &sa);
+                        copy_cell_p(m, IDX(m, i, j, m->nz - 1 + g), IDX(m, i, j, sk), sa, sa, sn * sa);
+                    }
             }
 }
 
@@ -267,56 +284,84 @@ static double mixture_total_energy(const ctx_t* m, double p, const double* alpha
 
 /* SolutionState::convertConservativeToPrimitiveVariables, src/SolutionState.cpp:187-205,
  * with IdealGasEOS::toPrimitive (src/IdealGasEOS.cpp:46-64) or
- * StiffenedGasEOS::toPrimitive (src/StiffenedGasEOS.cpp:47-64). */
-static void cons_to_prim_single(ctx_t* m) {
+ * StiffenedGasEOS::toPrimitive (src/StiffenedGasEOS.cpp:47-64): one cell. */
+static void cons_to_prim_single_cell(ctx_t* m, size_t idx) {
     const double g = m->c.gamma, pinf = m->c.pInf;
     const int stiff = (m->c.eosKind == SIFV_EOS_STIFFENED);
-    for (int k = 0; k < m->nz; ++k)
-        for (int j = 0; j < m->ny; ++j)
-            for (int i = 0; i < m->nx; ++i) {
-                size_t idx = IDX(m, i, j, k);
-                double U[3] = {m->rhoU[idx], (m->dim >= 2) ? m->rhoV[idx] : 0.0, (m->dim >= 3) ? m->rhoW[idx] : 0.0};
-                double rho = smax(m->rho[idx], 1e-14);
-                double u[3] = {0.0, 0.0, 0.0};
-                for (int d = 0; d < m->dim; ++d) u[d] = U[d] / rho;
-                double ke = 0.0;
-                for (int d = 0; d < m->dim; ++d) ke += u[d] * u[d];
-                ke *= 0.5 * rho;
-                double e = m->rhoE[idx] - ke;
-                double p = stiff ? (g - 1.0) * e - g * pinf : smax((g - 1.0) * e, 1e-14);
-                m->velU[idx] = u[0];
-                if (m->dim >= 2) m->velV[idx] = u[1];
-                if (m->dim >= 3) m->velW[idx] = u[2];
-                m->pres[idx] = p;
-            }
+    double U[3] = {m->rhoU[idx], (m->dim >= 2) ? m->rhoV[idx] : 0.0, (m->dim >= 3) ? m->rhoW[idx] : 0.0};
+    double rho = smax(m->rho[idx], 1e-14);
+    double u[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < m->dim; ++d) u[d] = U[d] / rho;
+    double ke = 0.0;
+    for (int d = 0; d < m->dim; ++d) ke += u[d] * u[d];
+    ke *= 0.5 * rho;
+    double e = m->rhoE[idx] - ke;
+    double p = stiff ? (g - 1.0) * e - g * pinf : smax((g - 1.0) * e, 1e-14);
+    m->velU[idx] = u[0];
+    if (m->dim >= 2) m->velV[idx] = u[1];
+    if (m->dim >= 3) m->velW[idx] = u[2];
+    m->pres[idx] = p;
 }
 
-/* MixtureEOS::convertConservativeToPrimitive, src/MixtureEOS.cpp:99-143 */
-static void cons_to_prim_mixture(ctx_t* m) {
+/* MixtureEOS::convertConservativeToPrimitive, src/MixtureEOS.cpp:99-143: one cell */
+static void cons_to_prim_mixture_cell(ctx_t* m, size_t idx) {
     double alphas[MAXPH];
-    for (int k = 0; k < m->nz; ++k)
-        for (int j = 0; j < m->ny; ++j)
-            for (int i = 0; i < m->nx; ++i) {
+    double rho = 0.0;
+    for (int ph = 0; ph < m->c.nPhases; ++ph) rho += m->alphaRho[ph][idx];
+    m->rho[idx] = smax(rho, 1e-14);
+    double rs = m->rho[idx];
+    m->velU[idx] = m->rhoU[idx] / rs;
+    if (m->dim >= 2) m->velV[idx] = m->rhoV[idx] / rs;
+    if (m->dim >= 3) m->velW[idx] = m->rhoW[idx] / rs;
+    double ke = 0.5 * rs * m->velU[idx] * m->velU[idx];
+    if (m->dim >= 2) ke += 0.5 * rs * m->velV[idx] * m->velV[idx];
+    if (m->dim >= 3) ke += 0.5 * rs * m->velW[idx] * m->velW[idx];
+    for (int ph = 0; ph < m->c.nPhases; ++ph) alphas[ph] = m->alpha[ph][idx];
+    double rhoE_internal = m->rhoE[idx] - ke;
+    m->pres[idx] = mixture_pressure(m, rhoE_internal, alphas);
+}
+
+static void cons_to_prim_box(ctx_t* m, int i0, int i1, int j0, int j1, int k0, int k1) {
+    for (int k = k0; k < k1; ++k)
+        for (int j = j0; j < j1; ++j)
+            for (int i = i0; i < i1; ++i) {
                 size_t idx = IDX(m, i, j, k);
-                double rho = 0.0;
-                for (int ph = 0; ph < m->c.nPhases; ++ph) rho += m->alphaRho[ph][idx];
-                m->rho[idx] = smax(rho, 1e-14);
-                double rs = m->rho[idx];
-                m->velU[idx] = m->rhoU[idx] / rs;
-                if (m->dim >= 2) m->velV[idx] = m->rhoV[idx] / rs;
-                if (m->dim >= 3) m->velW[idx] = m->rhoW[idx] / rs;
-                double ke = 0.5 * rs * m->velU[idx] * m->velU[idx];
-                if (m->dim >= 2) ke += 0.5 * rs * m->velV[idx] * m->velV[idx];
-                if (m->dim >= 3) ke += 0.5 * rs * m->velW[idx] * m->velW[idx];
-                for (int ph = 0; ph < m->c.nPhases; ++ph) alphas[ph] = m->alpha[ph][idx];
-                double rhoE_internal = m->rhoE[idx] - ke;
-                m->pres[idx] = mixture_pressure(m, rhoE_internal, alphas);
+                if (m->c.nPhases > 0) cons_to_prim_mixture_cell(m, idx);
+                else cons_to_prim_single_cell(m, idx);
             }
 }
 
+/* Interior cells; on a decomposed mesh also the ghost layers of the
+ * exchange faces, which hold the neighbour's conservative cells (the
+ * reference exchanges the neighbour's primitives instead, the same values:
+ * the conversion is per cell). */
 static void cons_to_prim(ctx_t* m) {
-    if (m->c.nPhases > 0) cons_to_prim_mixture(m);
-    else cons_to_prim_single(m);
+    cons_to_prim_box(m, 0, m->nx, 0, m->ny, 0, m->nz);
+    if (!m->exchangeFaces) return;
+    if (m->bc[0] == SIFV_BC_EXCHANGE) cons_to_prim_box(m, -m->ngx, 0, 0, m->ny, 0, m->nz);
+    if (m->bc[1] == SIFV_BC_EXCHANGE) cons_to_prim_box(m, m->nx, m->nx + m->ngx, 0, m->ny, 0, m->nz);
+    if (m->dim >= 2 && m->bc[2] == SIFV_BC_EXCHANGE) cons_to_prim_box(m, 0, m->nx, -m->ngy, 0, 0, m->nz);
+    if (m->dim >= 2 && m->bc[3] == SIFV_BC_EXCHANGE) cons_to_prim_box(m, 0, m->nx, m->ny, m->ny + m->ngy, 0, m->nz);
+    if (m->dim >= 3 && m->bc[4] == SIFV_BC_EXCHANGE) cons_to_prim_box(m, 0, m->nx, 0, m->ny, -m->ngz, 0);
+    if (m->dim >= 3 && m->bc[5] == SIFV_BC_EXCHANGE) cons_to_prim_box(m, 0, m->nx, 0, m->ny, m->nz, m->nz + m->ngz);
+}
+
+/* HaloExchange (src/HaloExchange.cpp:387-465) through the caller's hook:
+ * the conservative cells next to every exchange face to the neighbour, the
+ * neighbour's into the ghost layers. */
+static int exchange_cons(ctx_t* m) {
+    if (!m->exchangeFaces) return SIFV_OK;
+    if (!m->comm.exchange) return SIFV_ERR_BAD_ARG;
+    double* f[5 + 2 * MAXPH];
+    int n = 0;
+    f[n++] = m->rho;
+    f[n++] = m->rhoU;
+    if (m->dim >= 2) f[n++] = m->rhoV;
+    if (m->dim >= 3) f[n++] = m->rhoW;
+    f[n++] = m->rhoE;
+    for (int ph = 0; ph < m->c.nPhases; ++ph) f[n++] = m->alphaRho[ph];
+    for (int ph = 0; ph < m->c.nPhases; ++ph) f[n++] = m->alpha[ph];
+    return m->comm.exchange(m->comm.user, f, n, NULL) == 0 ? SIFV_OK : SIFV_ERR_CUDA;
 }
 
 /* ---- time steps ---- */
@@ -1428,12 +1473,15 @@ static double explicit_step(ctx_t* m, int step, double targetDt) {
         dt = acoustic_dt(m, c->cfl, c->maxDt, 1);
         if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->cfl, c->maxDt, 1));
         if (c->stSigma > 0.0) dt = smin(dt, capillary_dt(m, c->stSigma, c->cfl, c->maxDt, 1));
+        /* decomposed run: MPI_Allreduce(MIN), src/RKTimeStepping.cpp:148-159 */
+        if (m->comm.allreduce_min) m->comm.allreduce_min(m->comm.user, &dt, NULL);
     }
     if (targetDt > 0) dt = smin(dt, targetDt);
     double rk[3][4];
     rk_coefs(c->RKOrder, rk);
     const int nPh = c->nPhases;
     for (int s = 0; s < c->RKOrder; ++s) {
+        if (exchange_cons(m) != SIFV_OK) return -1.0;
         cons_to_prim(m);
         apply_bc_prim(m);
         if (m->cellType) ib_apply_ghosts(m);
@@ -1475,6 +1523,7 @@ static double explicit_step(ctx_t* m, int step, double targetDt) {
                     if (nPh > 0) mp_post(m, idx);
                 }
     }
+    if (exchange_cons(m) != SIFV_OK) return -1.0;
     cons_to_prim(m);
     apply_bc_prim(m);
     if (m->cellType) ib_apply_ghosts(m);
@@ -1748,7 +1797,16 @@ int sifvo_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, 
     m->xExt = build_ext(mesh->xNodes ? mesh->xNodes : unit, m->nx, m->ngx);
     m->yExt = build_ext((cfg->dim >= 2 && mesh->yNodes) ? mesh->yNodes : unit, m->ny, m->ngy);
     m->zExt = build_ext((cfg->dim >= 3 && mesh->zNodes) ? mesh->zNodes : unit, m->nz, m->ngz);
-    for (int f = 0; f < 6; ++f) m->bc[f] = mesh->bc[f];
+    for (int f = 0; f < 6; ++f) {
+        m->bc[f] = mesh->bc[f];
+        if (f < 2 * cfg->dim && mesh->bc[f] == SIFV_BC_EXCHANGE) m->exchangeFaces = 1;
+    }
+    if (m->exchangeFaces && (cfg->semiImplicit || cfg->useIGR || has_viscosity(cfg) || cfg->stSigma > 0.0)) {
+        snprintf(g_err, sizeof(g_err), "SIFV_BC_EXCHANGE faces are supported by the explicit step without IGR, "
+                                       "viscosity or surface tension");
+        free(m->xExt); free(m->yExt); free(m->zExt); free(m);
+        return SIFV_ERR_UNSUPPORTED;
+    }
     size_t n = m->n;
     double** all[] = {&m->rho, &m->rhoU, &m->rhoV, &m->rhoW, &m->rhoE, &m->velU, &m->velV, &m->velW, &m->pres,
                       &m->sigma, &m->rho0, &m->rhoU0, &m->rhoV0, &m->rhoW0, &m->rhoE0, &m->pres0, &m->rhoUStar,
@@ -1768,6 +1826,12 @@ int sifvo_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, 
     m->yL = (Prim*)calloc(nyf, sizeof(Prim)); m->yR = (Prim*)calloc(nyf, sizeof(Prim));
     m->zL = (Prim*)calloc(nzf, sizeof(Prim)); m->zR = (Prim*)calloc(nzf, sizeof(Prim));
     *out = m;
+    return SIFV_OK;
+}
+
+int sifvo_set_comm(ctx_t* m, const sifv_comm_t* comm) {
+    if (comm) m->comm = *comm;
+    else memset(&m->comm, 0, sizeof(m->comm));
     return SIFV_OK;
 }
 
@@ -1835,6 +1899,10 @@ int sifvo_step(ctx_t* m, int step, double time, double targetDt, double* dtOut) 
     m->time = time;
     double dt = m->c.semiImplicit ? semi_step(m, step, targetDt) : explicit_step(m, step, targetDt);
     if (dtOut) *dtOut = dt;
+    if (dt < 0.0) {
+        snprintf(m->err, sizeof(m->err), "halo exchange failed (or not set: sifvo_set_comm)");
+        return SIFV_ERR_CUDA;
+    }
     return SIFV_OK;
 }
 
@@ -2237,6 +2305,10 @@ int sifvo_set_immersed_bodies(ctx_t* m, const sifv_ib_body_t* bodies, int nBodie
     if (!m || nBodies < 0 || (nBodies > 0 && !bodies)) return SIFV_ERR_BAD_ARG;
     if (nBodies > 0 && m->c.semiImplicit) {
         snprintf(m->err, sizeof(m->err), "the semi-implicit step has no immersed boundary");
+        return SIFV_ERR_UNSUPPORTED;
+    }
+    if (nBodies > 0 && m->exchangeFaces) {
+        snprintf(m->err, sizeof(m->err), "immersed boundaries are not supported with SIFV_BC_EXCHANGE faces");
         return SIFV_ERR_UNSUPPORTED;
     }
     free(m->ibBodies); free(m->cellType); free(m->ibGhost);

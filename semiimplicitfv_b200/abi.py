@@ -27,6 +27,7 @@ WENO1, WENO3, WENO5, UPWIND1, UPWIND3, UPWIND5 = range(6)
 LF, RUSANOV, HLLC = range(3)
 # BoundaryCondition (include/RectilinearMesh.hpp:14-20)
 BC_SYMMETRY, BC_OUTFLOW, BC_PERIODIC, BC_SLIPWALL, BC_NOSLIPWALL = range(5)
+BC_EXCHANGE = 16   # a face shared with a neighbouring rank (ghost layers filled by the halo exchange)
 EOS_IDEAL, EOS_STIFFENED = 0, 1
 PREC_FP64, PREC_MIXED, PREC_FP64_FAST = 0, 1, 2
 
@@ -171,6 +172,13 @@ class LoopResult(C.Structure):
 
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_double, C.c_double)
+# sifv_comm_t: halo exchange and dt reduction of a decomposed run
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_void_p)
+ALLREDUCE_MIN_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+
+
+class Comm(C.Structure):
+    _fields_ = [("exchange", EXCHANGE_FN), ("allreduce_min", ALLREDUCE_MIN_FN), ("user", C.c_void_p)]
 
 
 class AbiError(RuntimeError):
@@ -245,6 +253,7 @@ _OPTIONAL_SIGS = {
                                 C.POINTER(LoopResult)]),
     "reference_time_loop": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_int,
                                       C.POINTER(C.c_int)]),
+    "set_comm": (C.c_int, [C.c_void_p, C.POINTER(Comm)]),
 }
 
 
@@ -454,6 +463,32 @@ class Context:
         dt = C.c_double()
         self._check(self.be.fn["step"](self.h, step, time, target_dt, C.byref(dt)))
         return dt.value
+
+    def set_comm(self, exchange, allreduce_min):
+        """Halo exchange and dt reduction of a decomposed run (sifv_set_comm):
+        exchange(pointers, stream) gets the field addresses (ints) the
+        step asks to exchange; allreduce_min(pointer, stream) the address of
+        the device (or host) double to reduce.  Both return None or 0; an
+        exception is reported to the library as a failure."""
+        def ex(user, fields, n, stream):
+            try:
+                r = exchange([fields[q] for q in range(n)], stream)
+                return int(r or 0)
+            except Exception:   # a Python error must not cross the C boundary
+                import traceback
+                traceback.print_exc()
+                return 1
+
+        def mn(user, value, stream):
+            try:
+                return int(allreduce_min(value, stream) or 0)
+            except Exception:
+                import traceback
+                traceback.print_exc()
+                return 1
+        self._comm_cb = (EXCHANGE_FN(ex), ALLREDUCE_MIN_FN(mn))   # kept alive with the context
+        c = Comm(self._comm_cb[0], self._comm_cb[1], None)
+        self._check(self.be.fn["set_comm"](self.h, C.byref(c)))
 
     def set_immersed_bodies(self, bodies):
         """ImmersedBoundaryMethod::addBody for each body + classifyCells."""

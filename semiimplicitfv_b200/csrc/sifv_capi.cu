@@ -67,6 +67,10 @@ struct sifv_ctx {
     // discrete adjoint / tangent (sifv_adjoint_*, sifv_tangent_*)
     double forcedDt = -1.0;                   // > 0: the steps use this dt (no CFL reduction)
     std::function<int(int, int)> stageHook;   // (stage, phase): 0 before the prim fill, 1 before the update, 2 after
+    bool dtReady = false;                     // ctl->dtBits holds the acoustic dt of the current state
+                                              // (folded in by the last fast 2D stage of the previous step)
+    bool exchangeFaces = false;               // the mesh has SIFV_BC_EXCHANGE faces
+    sifv_comm_t comm{};                       // halo exchange / dt reduction of a decomposed run
     int adjEvery = 0;
     std::vector<double> adjDts;               // time-step sequence of the recorded forward run
     std::vector<double*> adjCkpt;             // (dim + 2) arrays per checkpoint, then the final state
@@ -309,7 +313,7 @@ void launch_prim_bc(sifv_ctx* c, bool interiorOnly = false) {
 }
 
 void launch_bc_prim(sifv_ctx* c) {
-    long long n = (long long)c->ncells;
+    long long n = ghost_count(c->P);
     NPH_DISPATCH(c, (k_bc_prim<NPHV><<<blocks(n, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, c->F)));
     c->launches++;
     mark(c, "bc_prim");
@@ -828,7 +832,36 @@ void body_force(const sifv_config_t& c, double time, StageCoef& K) {
 }
 
 // dt reduction + finalisation on the device.
-void enqueue_dt(sifv_ctx* c, double targetDt, int useEnd) {
+// Halo exchange of a decomposed run (sifv_set_comm): the ghost layers of the
+// SIFV_BC_EXCHANGE faces of `fields` from the neighbouring ranks.
+int exchange_fields(sifv_ctx* c, double* const* fields, int n) {
+    if (!c->exchangeFaces) return SIFV_OK;
+    if (!c->comm.exchange)
+        return fail(c, SIFV_ERR_BAD_ARG, "the mesh has SIFV_BC_EXCHANGE faces: set the halo exchange (sifv_set_comm)");
+    if (c->comm.exchange(c->comm.user, fields, n, c->stream) != 0)
+        return fail(c, SIFV_ERR_CUDA, "halo exchange failed");
+    return SIFV_OK;
+}
+
+// ... of the conservative state the next stage converts (src/HaloExchange.cpp:
+// the reference exchanges the primitives after converting; converting the
+// exchanged conservative cells gives the same bits, as the conversion is
+// per cell).
+int exchange_cons(sifv_ctx* c) {
+    if (!c->exchangeFaces) return SIFV_OK;
+    double* f[5 + 2 * SIFV_MAX_PHASES];
+    int n = 0;
+    f[n++] = c->F.rho;
+    f[n++] = c->F.rhoU;
+    if (c->P.dim >= 2) f[n++] = c->F.rhoV;
+    if (c->P.dim >= 3) f[n++] = c->F.rhoW;
+    f[n++] = c->F.rhoE;
+    for (int ph = 0; ph < c->P.nPh; ++ph) f[n++] = c->F.alphaRho[ph];
+    for (int ph = 0; ph < c->P.nPh; ++ph) f[n++] = c->F.alpha[ph];
+    return exchange_fields(c, f, n);
+}
+
+int enqueue_dt(sifv_ctx* c, double targetDt, int useEnd) {
     const sifv_config_t& cfg = c->cfg;
     unsigned g = blocks((long long)c->nint, kCellThreads);
     if (cfg.semiImplicit) {
@@ -848,7 +881,9 @@ void enqueue_dt(sifv_ctx* c, double targetDt, int useEnd) {
         k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, c->forcedDt, -1.0, 0, 0.0, 0.0, 0);
         c->launches += 1;
     } else {
-        if (cfg.constDt <= 0) {
+        if (cfg.constDt <= 0 && c->dtReady) {
+            // the previous step's last stage left min(maxDt, acoustic dt) of this state in ctl->dtBits
+        } else if (cfg.constDt <= 0) {
             k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, cfg.maxDt);
             NPH_DISPATCH(c, (k_dt_acoustic<NPHV><<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.cfl)));
             if (c->P.visc) {
@@ -861,10 +896,16 @@ void enqueue_dt(sifv_ctx* c, double targetDt, int useEnd) {
             }
             c->launches += 2;
         }
+        // decomposed run: the minimum over the ranks (src/RKTimeStepping.cpp:148-159)
+        if (cfg.constDt <= 0 && c->comm.allreduce_min &&
+            c->comm.allreduce_min(c->comm.user, reinterpret_cast<double*>(&c->ctl->dtBits), c->stream) != 0)
+            return fail(c, SIFV_ERR_CUDA, "dt reduction over the ranks failed");
+        c->dtReady = false;
         k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, cfg.constDt, targetDt, 0, 0.0, 0.0, useEnd);
         c->launches += 1;
     }
     mark(c, "dt");
+    return SIFV_OK;
 }
 
 // One step, everything enqueued on the stream; semi-implicit steps
@@ -873,7 +914,10 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
     const sifv_config_t& cfg = c->cfg;
     const Params& P = c->P;
     status = SIFV_OK;
-    enqueue_dt(c, targetDt, useEnd);
+    {
+        int st = enqueue_dt(c, targetDt, useEnd);
+        if (st != SIFV_OK) return st;
+    }
     unsigned gc = blocks((long long)c->nint, kCellThreads);
     if (c->sweep && P.dim == 2) {
         // one fused tile kernel per stage; stage outputs ping-pong through two
@@ -905,6 +949,14 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
             T.inv[0] = c->invW[0];
             T.inv[1] = c->invW[1];
             T.last = (s == RK - 1) ? 1 : 0;
+            T.dtNext = (T.last && cfg.constDt <= 0 && c->forcedDt <= 0) ? 1 : 0;
+            T.cfl = cfg.cfl;
+            T.dx = c->F.dx;
+            T.dy = c->F.dy;
+            if (T.dtNext) {   // accumulator of the next step's dt
+                k_dt_init<<<1, 1, 0, c->stream>>>(c->ctl, cfg.maxDt);
+                c->launches++;
+            }
             T.velU = c->F.velU;
             T.velV = c->F.velV;
             T.pres = c->F.pres;
@@ -914,6 +966,10 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
                 T.in[q] = in[q];
                 T.out[q] = out[q];
                 T.u0[q] = (s > 0 && K.c2 != 0.0) ? U[q] : nullptr;
+            }
+            {
+                int st = exchange_fields(c, const_cast<double* const*>(in), 4);
+                if (st != SIFV_OK) return st;
             }
             if (tile2d_stage(T, c->stream, cfg.precision == SIFV_PREC_MIXED, c->launches,
                              c->profiling ? mark_cb : nullptr, c) != 0) {
@@ -925,6 +981,7 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
             return fail(c, SIFV_ERR_CUDA, "copy launch failed");
         launch_bc_prim(c);
         LAUNCH_CHECK(c);
+        c->dtReady = cfg.constDt <= 0 && c->forcedDt <= 0;
         return SIFV_OK;
     }
     if (c->sweep) {
@@ -966,6 +1023,10 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
         rk_coef(cfg.RKOrder, s, K);
         body_force(cfg, time, K);
         if (c->stageHook && c->stageHook(s, 0) != 0) return SIFV_ERR_CUDA;
+        {
+            int st = exchange_cons(c);
+            if (st != SIFV_OK) return st;
+        }
         launch_prim_bc(c);
         launch_ib_ghost(c);   // src/ExplicitSolver.cpp:116
         if (cfg.useIGR) {
@@ -1031,6 +1092,8 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
         }
     }
     if (!cfg.semiImplicit) {   // finalize: src/ExplicitSolver.cpp:192-200
+        int st = exchange_cons(c);
+        if (st != SIFV_OK) return st;
         launch_prim_bc(c);
         launch_ib_ghost(c);
     }
@@ -1097,13 +1160,30 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
         return fail(nullptr, SIFV_ERR_UNSUPPORTED, "every active axis needs at least nGhost cells");
     if (!mesh->xNodes || (dim >= 2 && !mesh->yNodes) || (dim >= 3 && !mesh->zNodes))
         return fail(nullptr, SIFV_ERR_BAD_ARG, "node arrays of the active axes are required");
-    for (int f = 0; f < 6; ++f)
+    bool exchangeFaces = false;
+    for (int f = 0; f < 6; ++f) {
+        if (mesh->bc[f] == SIFV_BC_EXCHANGE && f < 2 * dim) {
+            exchangeFaces = true;
+            continue;
+        }
         if (mesh->bc[f] < SIFV_BC_SYMMETRY || mesh->bc[f] > SIFV_BC_NOSLIPWALL)
             return fail(nullptr, SIFV_ERR_BAD_ARG, "unknown boundary condition");
+    }
+    if (exchangeFaces) {
+        const bool visc = cfg->mu > 0.0 || cfg->nPhaseMu > 0 || cfg->stSigma > 0.0;
+        if (cfg->semiImplicit || cfg->useIGR || visc)
+            return fail(nullptr, SIFV_ERR_UNSUPPORTED,
+                        "SIFV_BC_EXCHANGE faces (domain decomposition) are supported by the explicit step without "
+                        "IGR, viscosity or surface tension");
+        if (cfg->precision != SIFV_PREC_FP64 && dim != 2)
+            return fail(nullptr, SIFV_ERR_UNSUPPORTED,
+                        "SIFV_BC_EXCHANGE faces on the fast / mixed path are supported in 2D (use SIFV_PREC_FP64)");
+    }
 
     sifv_ctx* c = new sifv_ctx();
     c->cfg = *cfg;
     c->device = device;
+    c->exchangeFaces = exchangeFaces;
     if (cudaSetDevice(device) != cudaSuccess) { delete c; return fail(nullptr, SIFV_ERR_CUDA, "cudaSetDevice failed"); }
     if (cudaStreamCreateWithFlags(&c->ownStream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
@@ -1296,6 +1376,12 @@ int sifv_set_stream(sifv_ctx_t* c, void* stream) {
     return SIFV_OK;
 }
 
+int sifv_set_comm(sifv_ctx_t* c, const sifv_comm_t* comm) {
+    if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
+    c->comm = comm ? *comm : sifv_comm_t{};
+    return SIFV_OK;
+}
+
 int sifv_synchronize(sifv_ctx_t* c) {
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return SIFV_OK;
@@ -1331,6 +1417,7 @@ int sifv_get_field(sifv_ctx_t* c, int field, double* dst, int onDevice) {
 int sifv_step(sifv_ctx_t* c, int step, double time, double targetDt, double* dtOut) {
     if (!c) return fail(nullptr, SIFV_ERR_BAD_ARG, "null context");
     cudaSetDevice(c->device);
+    c->dtReady = false;   // the state may have changed since the last call
     c->launches = 0;
     CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
     CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
@@ -1352,6 +1439,7 @@ int sifv_advance(sifv_ctx_t* c, int step0, double time0, double tEnd, int nSteps
     if (c->cfg.useIGR) return fail(c, SIFV_ERR_UNSUPPORTED, "sifv_advance does not run IGR; use sifv_step");
     if (has_body_force(c->cfg)) return fail(c, SIFV_ERR_UNSUPPORTED, "sifv_advance does not run body forces");
     cudaSetDevice(c->device);
+    c->dtReady = false;   // the state may have changed since the last call
     c->launches = 0;
     Ctl h{};
     h.time = time0;
@@ -1379,6 +1467,7 @@ int sifv_profile_step(sifv_ctx_t* c, int step, double time, double targetDt, cha
                       double* ms, int* counts, int maxFamilies, int* nFamilies) {
     if (!c || !names || !ms || !counts || !nFamilies) return fail(c, SIFV_ERR_BAD_ARG, "null argument");
     cudaSetDevice(c->device);
+    c->dtReady = false;   // the state may have changed since the last call
     c->launches = 0;
     c->marks.clear();
     c->profiling = true;
@@ -2112,6 +2201,7 @@ int sifv_run_time_loop(sifv_ctx_t* c, const sifv_time_loop_t* prm, sifv_vtk_t* v
     const double endTime = prm->endTime, every = prm->outputInterval;
     const int printEvery = prm->printInterval > 0 ? prm->printInterval : 1;
     cudaSetDevice(c->device);
+    c->dtReady = false;   // the state may have changed since the last call
     c->launches = 0;
     int st = SIFV_OK;
     double time = 0.0;
@@ -2238,6 +2328,8 @@ int sifv_run_time_loop(sifv_ctx_t* c, const sifv_time_loop_t* prm, sifv_vtk_t* v
 namespace {
 
 int set_ib(sifv_ctx* c, int nBodies, const int* wall, const sifv_ib_shapes_t* shapes) {
+    if (nBodies > 0 && c->exchangeFaces)
+        return fail(c, SIFV_ERR_UNSUPPORTED, "immersed boundaries are not supported with SIFV_BC_EXCHANGE faces");
     cudaSetDevice(c->device);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     for (void* p : c->ibAllocs) cudaFree(p);

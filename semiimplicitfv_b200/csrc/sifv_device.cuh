@@ -133,14 +133,16 @@ __device__ __forceinline__ size_t cidx(const Params& P, int i, int j, int k) {
 
 // Ghost source along one axis for the PRIM fill (the BoundaryCondition
 // switch of fillGhostX/Y/Z, src/RectilinearMesh.cpp:147-166, 188-207).
-// Returns the interior index; sn multiplies the normal velocity, sa all
-// velocity components.  Requires n >= nGhost.
+// Returns the interior index (the ghost index itself on an exchange face,
+// whose ghost layers hold the neighbouring rank's cells); sn multiplies the
+// normal velocity, sa all velocity components.  Requires n >= nGhost.
 __device__ __forceinline__ int prim_src(int i, int n, int bcLo, int bcHi, double& sn, double& sa) {
     sn = 1.0;
     sa = 1.0;
     if (i < 0) {
         int g = -i;
         switch (bcLo) {
+            case SIFV_BC_EXCHANGE: return i;   // the neighbour's cells, held in the ghost layers
             case SIFV_BC_SYMMETRY: return g - 1;
             case SIFV_BC_PERIODIC: return n - g;
             case SIFV_BC_SLIPWALL: sn = -1.0; return g - 1;
@@ -151,6 +153,7 @@ __device__ __forceinline__ int prim_src(int i, int n, int bcLo, int bcHi, double
     if (i >= n) {
         int g = i - n + 1;
         switch (bcHi) {
+            case SIFV_BC_EXCHANGE: return i;
             case SIFV_BC_SYMMETRY: return n - g;
             case SIFV_BC_PERIODIC: return g - 1;
             case SIFV_BC_SLIPWALL: sn = -1.0; return n - g;
@@ -165,8 +168,8 @@ __device__ __forceinline__ int prim_src(int i, int n, int bcLo, int bcHi, double
 // (RectilinearMesh::fillScalarGhosts, src/RectilinearMesh.cpp:424-492):
 // periodic wrap, otherwise zero gradient.
 __device__ __forceinline__ int scalar_src(int i, int n, int bcLo, int bcHi) {
-    if (i < 0) return (bcLo == SIFV_BC_PERIODIC) ? n + i : 0;
-    if (i >= n) return (bcHi == SIFV_BC_PERIODIC) ? i - n : n - 1;
+    if (i < 0) return (bcLo == SIFV_BC_PERIODIC) ? n + i : (bcLo == SIFV_BC_EXCHANGE) ? i : 0;
+    if (i >= n) return (bcHi == SIFV_BC_PERIODIC) ? i - n : (bcHi == SIFV_BC_EXCHANGE) ? i : n - 1;
     return i;
 }
 
