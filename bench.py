@@ -14,9 +14,9 @@ pressure solve), `adjoint` (isentropic-vortex discrete adjoint 512^2) and
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 
-Multi-GPU: one process per GPU (torchrun), every rank advances its own
-4096^2 instance (weak scaling, replicas: the single-GPU path needs no
-exchange); time = max over ranks.
+Multi-GPU: one process per GPU (torchrun); the 4096^2 grid is cut into
+slabs of rows, one per rank, with the 3-row halo exchange of every RK stage
+and the dt all-reduce over NCCL (strong scaling); time = max over ranks.
 """
 from __future__ import annotations
 
@@ -293,7 +293,7 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "precision": "fp64 (the reference's CPU solver)",
         "config": workload_config(n),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
@@ -317,7 +317,7 @@ def run_cuda(args):
 
     import backends
     import cases
-    from semiimplicitfv_b200 import abi
+    from semiimplicitfv_b200 import abi, slab
     CONS_2D = (abi.F_RHO, abi.F_RHOU, abi.F_RHOV, abi.F_RHOE)
     n = args.n
     cells = n * n
@@ -335,13 +335,22 @@ def run_cuda(args):
         return x
 
     def make_ctx(precision):
+        """This rank's context: the whole grid on one GPU; with N ranks its
+        slab of rows (slab decomposition along y, halo exchange and dt
+        reduction over NCCL through the library's hooks)."""
         case = cases.riemann2d(n)
         case[0].precision = precision
-        ctx = backends.cuda().create(case[0], case[1], local)
-        for fid, arr in case[2].items():   # inputs uploaded from pinned host memory
+        mesh, fields = case[1], case[2]
+        if ws > 1:
+            mesh, start, count = slab.slab_mesh(case[1], 2, rank, ws)
+            fields = slab.slab_fields(case[2], case[0], start, count)
+        ctx = backends.cuda().create(case[0], mesh, local)
+        for fid, arr in fields.items():   # inputs uploaded from pinned host memory
             pinned = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
             ctx.be.fn["set_field"](ctx.h, fid, ctypes.c_void_p(pinned.data_ptr()), 0)
         ctx.be.fn["set_stream"](ctx.h, ctypes.c_void_p(stream.cuda_stream))
+        if ws > 1:
+            slab.DistExchange(ctx, rank, ws, periodic=False, device=True).attach()
         return ctx
 
     def measure(precision, with_clocks=False, with_e2e=False):
@@ -366,10 +375,10 @@ def run_cuda(args):
         ms = max_over_ranks(e0.elapsed_time(e1))
         step_idx += args.steps
         _, launches = ctx.last_step_stats()
-        out = {"ms": ms, "value": ws * cells * args.steps / (ms / 1e3), "launches": launches,
+        out = {"ms": ms, "value": cells * args.steps / (ms / 1e3), "launches": launches,
                "clocks": clk.summary() if clk else None, "t": t_sim,
                # the conservative state after the warm-up and timed steps (error against FP64)
-               "state": {f: ctx.interior(ctx.get_field(f)).copy() for f in CONS_2D} if rank == 0 else None}
+               "state": {f: ctx.interior(ctx.get_field(f)).copy() for f in CONS_2D} if ws == 1 else None}
         if with_clocks:
             # per-kernel-family device time of two more steps (CUDA events on the launch stream)
             fam = {}
@@ -388,7 +397,7 @@ def run_cuda(args):
             for q in range(args.steps):
                 t_sim += ctx.step(step_idx + q, t_sim, -1.0)
             torch.cuda.synchronize()
-            out["e2e_resident"] = ws * cells * args.steps / max_over_ranks(time.perf_counter() - t0)
+            out["e2e_resident"] = cells * args.steps / max_over_ranks(time.perf_counter() - t0)
             step_idx += args.steps
             # (2) host-authoritative drop-in: per step the fields the step reads go up
             # from pinned host buffers, sifv_step runs, the fields it writes come back
@@ -407,7 +416,7 @@ def run_cuda(args):
                 for f in fids:
                     assert get_f(ctx.h, f, ctypes.c_void_p(host[f].data_ptr()), 0) == 0
             torch.cuda.synchronize()
-            out["e2e"] = ws * cells * args.steps / max_over_ranks(time.perf_counter() - t0)
+            out["e2e"] = cells * args.steps / max_over_ranks(time.perf_counter() - t0)
             out["e2e_bytes"] = len(fids) * ctx.ncells * 8
         ctx.close()
         return out
@@ -693,7 +702,7 @@ def run_cuda(args):
         ens = {"mixed": emx, "fp64": e64, "l1_rel_max": mor(float(max(rel)), dev),
                "l1_rel_mean": float(np.mean(rel)), "linf_rel_max": mor(float(max(linf)), dev)}
     accuracy = None
-    if rank == 0 and not args.quick and PREC_NAMES[0] in extra:
+    if ws == 1 and not args.quick and PREC_NAMES[0] in extra:
         # every result's L1 / L-inf error against the FP64 (reference-ordered)
         # state after the same steps, and against the 2n x 2n FP64 solution
         # at the same time (the discretisation error)
@@ -751,10 +760,12 @@ def run_cuda(args):
             cpu_sample = "C restatement on one core, 768x768 instance, 3 steps"
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f64" if args.precision != 1 else "f32-bulk/f64-state",
             "data": "synthetic",
-            "precision": PREC_NAMES[args.precision], "parallelism": f"replicas x{ws}",
+            "precision": PREC_NAMES[args.precision],
+            "parallelism": (f"slab decomposition over {ws} GPUs (rows split along y, 3-row halo exchange per RK "
+                            f"stage and dt all-reduce over NCCL)" if ws > 1 else "1 GPU"),
             "config": workload_config(n),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

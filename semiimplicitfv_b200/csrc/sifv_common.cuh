@@ -43,6 +43,46 @@ __device__ __forceinline__ bool ext_coords(const Params& P, long long t, int& i,
     return true;
 }
 
+// Decode a linear id over the ghost cells only: the two z slabs (full x-y
+// planes), then per interior z the two y slabs (full rows), then per
+// interior (y, z) the two x slabs.  Returns false past the end.
+__host__ __device__ __forceinline__ long long ghost_count(const Params& P) {
+    return 2LL * P.ngz * P.nxT * P.nyT + (long long)P.nz * (2LL * P.ngy * P.nxT) +
+           (long long)P.nz * P.ny * (2LL * P.ngx);
+}
+__device__ __forceinline__ bool ghost_coords(const Params& P, long long t, int& i, int& j, int& k) {
+    const long long zs = 2LL * P.ngz * P.nxT * P.nyT;
+    if (t < zs) {
+        const long long plane = (long long)P.nxT * P.nyT;
+        const int g = (int)(t / plane);
+        const long long r = t - g * plane;
+        j = (int)(r / P.nxT) - P.ngy;
+        i = (int)(r % P.nxT) - P.ngx;
+        k = (g < P.ngz) ? g - P.ngz : P.nz + (g - P.ngz);
+        return true;
+    }
+    t -= zs;
+    const long long ys = (long long)P.nz * (2LL * P.ngy * P.nxT);
+    if (t < ys) {
+        const long long per = 2LL * P.ngy * P.nxT;
+        k = (int)(t / per);
+        const long long r = t - k * per;
+        const int g = (int)(r / P.nxT);
+        i = (int)(r % P.nxT) - P.ngx;
+        j = (g < P.ngy) ? g - P.ngy : P.ny + (g - P.ngy);
+        return true;
+    }
+    t -= ys;
+    const long long per = 2LL * P.ngx;
+    if (t >= (long long)P.nz * P.ny * per) return false;
+    const long long line = t / per;
+    const int g = (int)(t - line * per);
+    j = (int)(line % P.ny);
+    k = (int)(line / P.ny);
+    i = (g < P.ngx) ? g - P.ngx : P.nx + (g - P.ngx);
+    return true;
+}
+
 __device__ __forceinline__ bool int_coords(const Params& P, long long t, int& i, int& j, int& k) {
     long long tot = (long long)P.nx * P.ny * P.nz;
     if (t >= tot) return false;

@@ -9,7 +9,7 @@
 
 #include "sifv_sweep.cuh"
 #include "sifv_sweep_api.h"
-#include "sifv_tile2d.cuh"
+#include "sifv_march2d.cuh"
 
 namespace sifv {
 
@@ -68,34 +68,60 @@ int sweep_stage(SweepArgs A, cudaStream_t s, bool mixed, int& launches, LaunchMa
 
 namespace {
 
-// 32 x 14 cells: with 512 threads every reconstruction / flux phase of the
-// FP64 stage has at most one item per thread ((32+2)*14 = 476, 32*(14+2) =
-// 512, 33*14, 32*15), and with 256 threads (FP32 bulk) at most two, where
-// 32 x 16 needed two and three.
-template <typename T>
-struct TileDims {
-    static constexpr int x = 32;
-    static constexpr int y = 14;
-};
+// Work units of the marching stage kernel: strips of 30 columns, each cut
+// into segments so that every resident warp gets at most one unit (a
+// segment first converts 6 rows and reconstructs 2 before its first update,
+// so segments stay at least 32 rows long).
+template <typename T, int RS>
+int march_launch(TileArgs A, cudaStream_t s) {
+    using S = MarchShape<T>;
+    static int residentWarps[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t bytes = sizeof(MarchWarpSmem<T>) * S::warps;
+    if (dev < 0 || dev >= 64) return -1;
+    if (residentWarps[dev] == 0) {
+        if (cudaFuncSetAttribute(k_march2d<T, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+            cudaSuccess)
+            return -1;
+        int sms = 0, perSm = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_march2d<T, RS>, S::warps * 32, bytes) !=
+                cudaSuccess)
+            return -1;
+        residentWarps[dev] = (perSm > 0 ? perSm : 1) * sms * S::warps;
+    }
+    const int W = residentWarps[dev];
+    A.strips = (A.P.nx + S::cols - 1) / S::cols;
+    int segs = W / A.strips;
+    const int maxSegs = (A.P.ny + 31) / 32;
+    if (segs > maxSegs) segs = maxSegs;
+    if (segs < 1) segs = 1;
+    A.segRows = (A.P.ny + segs - 1) / segs;
+    A.segs = (A.P.ny + A.segRows - 1) / A.segRows;
+    const long long units = (long long)A.strips * A.segs;
+    const long long blocksNeeded = (units + S::warps - 1) / S::warps;
+    const long long maxBlocks = (W + S::warps - 1) / S::warps;
+    const unsigned grid = (unsigned)(blocksNeeded < maxBlocks ? blocksNeeded : maxBlocks);
+    k_march2d<T, RS><<<grid, S::warps * 32, bytes, s>>>(A);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
 
 template <typename T>
-int tile_launch(const TileArgs& A, cudaStream_t s) {
-    constexpr int kTileX = TileDims<T>::x, kTileY = TileDims<T>::y;
-    const size_t bytes = sizeof(TileSmem<kTileX, kTileY, T>);
-    if (cudaFuncSetAttribute(k_tile2d<kTileX, kTileY, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)bytes) != cudaSuccess)
-        return -1;
-    dim3 g((A.P.nx + kTileX - 1) / kTileX, (A.P.ny + kTileY - 1) / kTileY, 1);
-    k_tile2d<kTileX, kTileY, T><<<g, TileThreads<T>::value, bytes, s>>>(A);
-    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+int march_dispatch(const TileArgs& A, cudaStream_t s) {
+    switch (A.P.riemann) {
+        case SIFV_HLLC: return march_launch<T, SIFV_HLLC>(A, s);
+        case SIFV_RUSANOV: return march_launch<T, SIFV_RUSANOV>(A, s);
+        default: return march_launch<T, SIFV_LF>(A, s);
+    }
 }
 
 }  // namespace
 
 int tile2d_stage(const TileArgs& A, cudaStream_t s, bool mixed, int& launches, LaunchMark mark, void* user) {
-    int st = mixed ? tile_launch<float>(A, s) : tile_launch<double>(A, s);
+    int st = mixed ? march_dispatch<float>(A, s) : march_dispatch<double>(A, s);
     ++launches;
-    if (mark) mark(user, "tile2d");
+    if (mark) mark(user, "march2d");
     return st;
 }
 

@@ -47,6 +47,24 @@ __device__ __forceinline__ float fsqrt_pos(float x) {
     return y;
 }
 
+// 1 / sqrt(x) of a positive normal argument: the hardware approximation
+// refined by two Newton-Raphson iterations (FP64; within 1 ulp of IEEE
+// 1 / sqrt(x), checked by sifv_fastmath_selftest), the single-instruction
+// approximation in FP32.
+__device__ __forceinline__ double frsqrt_pos(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x * y, y, 1.0);
+    y = fma(0.5 * y, e, y);
+    e = fma(-x * y, y, 1.0);
+    return fma(0.5 * y, e, y);
+}
+__device__ __forceinline__ float frsqrt_pos(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Both WENO5 face values of the cell whose 5-cell stencil is v0..v4
 // (v2 = the cell): L = value at its right face from the left,
 // R = value at its left face from the right.
@@ -61,16 +79,17 @@ __device__ __forceinline__ void weno5_pair(double v0, double v1, double v2, doub
     q0 *= q0; q1 *= q1; q2 *= q2;
     // a_k = d_k / q_k; multiplying through by q0 q1 q2 leaves one division per side
     double m01 = q0 * q1, m02 = q0 * q2, m12 = q1 * q2;
-    double pL0 = (2.0 * v0 - 7.0 * v1 + 11.0 * v2) * (1.0 / 6.0);
-    double pL1 = (-v1 + 5.0 * v2 + 2.0 * v3) * (1.0 / 6.0);
-    double pL2 = (2.0 * v2 + 5.0 * v3 - v4) * (1.0 / 6.0);
-    double pR0 = (2.0 * v4 - 7.0 * v3 + 11.0 * v2) * (1.0 / 6.0);
-    double pR1 = (-v3 + 5.0 * v2 + 2.0 * v1) * (1.0 / 6.0);
-    double pR2 = (2.0 * v2 + 5.0 * v1 - v0) * (1.0 / 6.0);
+    // candidate polynomials times 6; the 1/6 goes into the normalisation
+    double pL0 = 2.0 * v0 - 7.0 * v1 + 11.0 * v2;
+    double pL1 = -v1 + 5.0 * v2 + 2.0 * v3;
+    double pL2 = 2.0 * v2 + 5.0 * v3 - v4;
+    double pR0 = 2.0 * v4 - 7.0 * v3 + 11.0 * v2;
+    double pR1 = -v3 + 5.0 * v2 + 2.0 * v1;
+    double pR2 = 2.0 * v2 + 5.0 * v1 - v0;
     double wL0 = 0.1 * m12, wL1 = 0.6 * m02, wL2 = 0.3 * m01;   // L: d = (.1,.6,.3) on (b0,b1,b2)
     double wR0 = 0.1 * m01, wR1 = 0.6 * m02, wR2 = 0.3 * m12;   // R: d = (.1,.6,.3) on (b2,b1,b0)
-    L = (wL0 * pL0 + wL1 * pL1 + wL2 * pL2) * frcp(wL0 + wL1 + wL2);
-    R = (wR0 * pR0 + wR1 * pR1 + wR2 * pR2) * frcp(wR0 + wR1 + wR2);
+    L = (wL0 * pL0 + wL1 * pL1 + wL2 * pL2) * frcp(6.0 * (wL0 + wL1 + wL2));
+    R = (wR0 * pR0 + wR1 * pR1 + wR2 * pR2) * frcp(6.0 * (wR0 + wR1 + wR2));
 }
 
 // FP32 version: the product form would overflow single precision for
@@ -95,6 +114,9 @@ __device__ __forceinline__ void weno5_pair(float v0, float v1, float v2, float v
     L = (aL0 * pL0 + aL1 * pL1 + aL2 * pL2) * frcp(aL0 + aL1 + aL2);
     R = (aR0 * pR0 + aR1 * pR1 + aR2 * pR2) * frcp(aR0 + aR1 + aR2);
 }
+
+template <typename T>
+__device__ __forceinline__ T trsqrt(T x) { return frsqrt_pos(x); }
 
 template <typename T>
 __device__ __forceinline__ T trcp(T x);

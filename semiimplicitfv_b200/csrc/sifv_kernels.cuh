@@ -62,12 +62,12 @@ __global__ void k_prim_bc(Params P, Fields F, const Ctl* __restrict__ ctl, int i
 // PRIM ghost fill from the primitive fields as they stand
 // (RectilinearMesh::applyBoundaryConditions(state, PRIM, halo),
 // src/RectilinearMesh.cpp:498-524 with SolutionState::copyCell_P).
+// One thread per ghost cell (ghost_coords).
 template <int NPH>
 __global__ void k_bc_prim(Params P, Fields F) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
-    if (!ext_coords(P, t, i, j, k)) return;
-    if (is_interior(P, i, j, k)) return;
+    if (!ghost_coords(P, t, i, j, k)) return;
     const int dim = P.dim;
     size_t d = cidx(P, i, j, k);
     double sg[3];

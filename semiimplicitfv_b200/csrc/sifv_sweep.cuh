@@ -45,9 +45,13 @@ struct Flux4 {
     T mass, m0, m1, m2, energy;
 };
 
-// Single-phase face flux on the normal axis D: HLLC (src/HLLCSolver.cpp:7-161)
-// with the reciprocals shared, Rusanov (src/RusanovSolver.cpp:7-83) or LF
-// (src/LFSolver.cpp:8-75), with pressure (explicit step).
+// Single-phase face flux on the normal axis D: HLLC (src/HLLCSolver.cpp:7-161),
+// Rusanov (src/RusanovSolver.cpp:7-83) or LF (src/LFSolver.cpp:8-75), with
+// pressure (explicit step).  The HLLC arithmetic is rearranged to need two
+// reciprocals per face: the sound speed sqrt(g p' / rho) is evaluated as
+// g p' / sqrt(g p' rho) (one reciprocal square root, no 1 / rho), and in the
+// star state rho* e = (s - u) rhoE / (s - s*) and rho* p / a = p / (s - s*)
+// (a = rho (s - u)), so neither 1 / rho nor 1 / a is formed.
 template <int D, int DIM, typename T>
 __device__ __forceinline__ void face_flux(int riemann, const FluxConsts& C, const Prim5<T>& L, const Prim5<T>& R,
                                           Flux4<T>& F) {
@@ -60,8 +64,8 @@ __device__ __forceinline__ void face_flux(int riemann, const FluxConsts& C, cons
     if (DIM >= 3) { q2L += L.w * L.w; q2R += R.w * R.w; }
     T rhoEL = (L.p + gPinf) * invGm1 + (T)0.5 * L.rho * q2L;
     T rhoER = (R.p + gPinf) * invGm1 + (T)0.5 * R.rho * q2R;
-    T irL = trcp(tmax(L.rho, tiny)), irR = trcp(tmax(R.rho, tiny));
-    T cL = fsqrt_pos(g * tmax(L.p + pinf, tiny) * irL), cR = fsqrt_pos(g * tmax(R.p + pinf, tiny) * irR);
+    const T gpL = g * tmax(L.p + pinf, tiny), gpR = g * tmax(R.p + pinf, tiny);
+    T cL = gpL * trsqrt(gpL * tmax(L.rho, tiny)), cR = gpR * trsqrt(gpR * tmax(R.rho, tiny));
     if (riemann == SIFV_HLLC) {
         T sL = tmin(unL - cL, unR - cR);
         T sR = tmax(unL + cL, unR + cR);
@@ -81,7 +85,6 @@ __device__ __forceinline__ void face_flux(int riemann, const FluxConsts& C, cons
             const bool left = sStar >= (T)0;
             const Prim5<T>& W = left ? L : R;
             T s = left ? sL : sR, un = left ? unL : unR, rhoE = left ? rhoEL : rhoER, a = left ? aL : aR;
-            T ir = left ? irL : irR;
             T inv = trcp(s - sStar);
             T rhoStar = a * inv;                    // rho (s - u) / (s - s*)
             T fm = W.rho * un;
@@ -94,8 +97,8 @@ __device__ __forceinline__ void face_flux(int riemann, const FluxConsts& C, cons
             F.m1 = fm * w1 + s * (rhoStar * ws[1] - W.rho * w1);
             F.m2 = fm * w2 + s * (rhoStar * ws[2] - W.rho * w2);
             if (D == 0) F.m0 += W.p; else if (D == 1) F.m1 += W.p; else F.m2 += W.p;
-            T e = rhoE * ir;                         // rhoE / rho
-            T EStar = rhoStar * (e + du * (sStar + W.p * trcp(a)));
+            // rho* (e + du (s* + p / a)) with e = rhoE / rho
+            T EStar = (s - un) * inv * rhoE + du * (rhoStar * sStar + W.p * inv);
             F.energy = (rhoE + W.p) * un + s * (EStar - rhoE);
         }
     } else {

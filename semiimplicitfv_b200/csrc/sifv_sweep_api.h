@@ -38,14 +38,14 @@ struct SweepArgs {
     const double* inv[3];   // 1 / d per cell (ghosts included)
 };
 
-// One RK stage of the 2D explicit step as one fused tile kernel
-// (sifv_tile2d.cuh): U' = a1 in + a2 u0 + a3 dt R(in), written to `out`
+// One RK stage of the 2D explicit step as one fused kernel
+// (sifv_march2d.cuh): U' = a1 in + a2 u0 + a3 dt R(in), written to `out`
 // (which may be u0, never `in`); `last` also writes the primitives of U'.
 struct TileArgs {
     Params P;
     FluxConsts C;
     double eps;
-    const Ctl* ctl;
+    Ctl* ctl;
     const double* in[4];    // stage input: rho, rhoU, rhoV, rhoE
     const double* u0[4];    // step-start state (own cells), null when a2 == 0
     double* out[4];         // stage output
@@ -53,6 +53,12 @@ struct TileArgs {
     const double* inv[2];   // 1 / dx, 1 / dy per cell (ghosts included)
     int last;               // write the primitives of the new state
     double *velU, *velV, *pres;
+    int strips, segs, segRows;   // work units: strips of 30 columns x segments of segRows rows (set by the launcher)
+    // last stage: fold the acoustic dt of the new state (k_dt_acoustic's
+    // expressions) into ctl->dtBits for the next step
+    int dtNext;
+    double cfl;
+    const double *dx, *dy;      // cell widths (ghosts included)
 };
 
 // Called after each kernel launch with the kernel family's name (per-kernel
