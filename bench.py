@@ -40,30 +40,34 @@ PREC_NAMES = {0: "fp64-reference-order", 1: "mixed-fp32-bulk", 2: "fp64-fast"}
 UNIT = "cell-updates/s"
 BYTES_PER_CELL_UPDATE = 256   # algorithmic: 64 B x 4 conserved variables per RK3 step
 # Algorithmic bytes per cell of one launch of each kernel family of the 2D
-# fused-sweep step (FP64 arrays, 8 B per value):
-#   sweep_x  reads rho, rhoU, rhoV, rhoE; writes the stage density copy,
-#            velU, velV, pres and the 4-array rhs              12 x 8 = 96
-#   sweep_y  reads rho, velU, velV, pres, 4 rhs, 4 U and 4 U0 (stage 0:
-#            pres and U, writes U0 + pres0); writes 4 U     avg 20.67 x 8 = 165.3
-#   dt       reads rho, velU, velV, pres                         4 x 8 = 32
-#   finish_prim reads 4 U, writes velU, velV, pres              7 x 8 = 56
-#   tile2d   one fused kernel per stage: reads U (4) and, in stages 2-3, U0
+# step (FP64 arrays, 8 B per value):
+#   march2d  one fused kernel per stage: reads U (4) and, in stages 2-3, U0
 #            (4); writes U' (4); the last stage also writes u, v, p (3)
 #                                             (32 + 21.33 + 32 + 8) = 93.33
-KERNEL_BYTES_PER_CELL_2D = {"sweep_x": 96.0, "sweep_y": 165.33, "dt": 32.0, "finish_prim": 56.0,
-                            "face_x": 64.0, "face_y": 64.0, "assemble": 229.3, "prim_bc": 56.0,
-                            "tile2d": 93.33}
-# DRAM bytes per cell of one launch, measured by ncu on the 2048^2 case of the
-# same workload (dram__bytes_read.sum + dram__bytes_write.sum over 2048^2 cells)
-# and scaled by the cell count for the benchmark size.
-NCU_DRAM_BYTES_PER_CELL = {(2, "sweep_y"): 164.8, (2, "sweep_x"): 84.5, (1, "sweep_y"): 164.7,
-                           (1, "sweep_x"): 86.2, (0, "assemble"): 166.2, (2, "tile2d"): 55.69,
-                           (1, "tile2d"): 54.83}
-# FP64 / FP32 pipe utilisation of the dominant kernel (ncu, 2048^2 case of the
-# same workload: sm__inst_executed_pipe_fp64 / _fma, percent of the pipe's
-# instruction peak while active) -- the co-bound of the HBM roofline.
-NCU_PIPE_FRAC = {(2, "tile2d"): {"fp64": 0.688, "fma_fp32": 0.053, "issue_active": 0.579},
-                 (1, "tile2d"): {"fp64": 0.072, "fma_fp32": 0.460, "issue_active": 0.807}}
+#   dt       reads rho, velU, velV, pres                         4 x 8 = 32
+#   bc_prim  ghost cells only (negligible per interior cell)
+KERNEL_BYTES_PER_CELL_2D = {"march2d": 93.33, "dt": 32.0, "bc_prim": 0.0, "face_x": 64.0, "face_y": 64.0,
+                            "assemble": 229.3, "prim_bc": 56.0}
+# Per launch of the dominant kernel, measured by ncu on the 2048^2 case of the
+# same workload (3 launches = one step, averaged): DRAM bytes per cell
+# (dram__bytes_read.sum + dram__bytes_write.sum) and FP64 / FMA-pipe
+# instructions per cell, with the SHA-1 of the kernel sources they were taken
+# on.  When the sources have changed since, the figures are reported as stale
+# (traffic null) instead of being applied to a different kernel.
+NCU_KERNEL_SOURCES = ("semiimplicitfv_b200/csrc/sifv_march2d.cuh", "semiimplicitfv_b200/csrc/sifv_sweep.cuh",
+                      "semiimplicitfv_b200/csrc/sifv_fastmath.cuh")
+NCU_CAPTURE = {}   # (precision, kernel) -> {"sha": ..., "dram_bytes_per_cell": ..., "fp64_inst_per_cell": ...}
+
+
+def _kernel_sources_sha() -> str:
+    import hashlib
+    h = hashlib.sha1()
+    for f in NCU_KERNEL_SOURCES:
+        with open(os.path.join(ROOT, f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
 # Fields a 2D step reads and writes (host-authoritative drop-in round trip).
 E2E_FIELDS_2D = ("F_RHO", "F_RHOU", "F_RHOV", "F_RHOE", "F_VELU", "F_VELV", "F_PRES")
 CONS_NAMES_2D = ("rho", "rhoU", "rhoV", "rhoE")
@@ -745,8 +749,17 @@ def run_cuda(args):
     dom_ms = fam[dom][0] / fam[dom][1]
     dom_bytes = KERNEL_BYTES_PER_CELL_2D.get(dom, float("nan")) * cells
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    tpc = NCU_DRAM_BYTES_PER_CELL.get((args.precision, dom))
-    traffic = tpc * cells if tpc is not None else None
+    cap = NCU_CAPTURE.get((args.precision, dom))
+    sha = _kernel_sources_sha()
+    fresh = cap is not None and cap.get("sha") == sha
+    traffic = cap["dram_bytes_per_cell"] * cells if fresh else None
+    fp64_peak = None
+    try:
+        tf = ctypes.c_double()
+        if backends.cuda().lib.sifv_fp64_peak_probe(5, ctypes.byref(tf)) == 0:
+            fp64_peak = tf.value
+    except Exception:
+        pass
     result = None
     if rank == 0:
         kind = "reference" if backends.reference(release=True) is not None else "port"
@@ -769,14 +782,24 @@ def run_cuda(args):
             "config": workload_config(n),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "traffic_source": "ncu dram bytes per cell on the 2048^2 case x cells",
+                         "traffic_source": (f"ncu dram bytes per cell of one {dom} launch (average over the 3 "
+                                            f"stage launches of a step, 2048^2 case) x {cells} cells" if fresh else
+                                            f"no ncu capture of the current {dom} sources ({sha})"),
                          "kernel": dom, "bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
                          "peak_source": peak_kind,
                          "step": {"achieved": step_achieved, "frac": step_achieved / peak,
                                   "bytes_per_cell_update": BYTES_PER_CELL_UPDATE},
                          "kernel_ms_per_step": {k: v[0] / 2 for k, v in fam.items()},
-                         "compute_co_bound": dict(NCU_PIPE_FRAC.get((args.precision, dom), {}),
-                                                  source="ncu on the 2048^2 case of this workload")},
+                         "compute_co_bound": {
+                             "fp64_peak_tflops": fp64_peak,
+                             "fp64_peak_source": "measured: FP64 FMA throughput probe (sifv_fp64_peak_probe)",
+                             "fp64_inst_per_cell": cap.get("fp64_inst_per_cell") if fresh else None,
+                             "fp64_inst_rate_frac": (cap["fp64_inst_per_cell"] * cells / (dom_ms / 1e3) /
+                                                     (fp64_peak * 1e12 / 2.0)
+                                                     if fresh and fp64_peak and cap.get("fp64_inst_per_cell")
+                                                     else None),
+                             "note": "FP64 instructions per cell from the ncu capture over the probe's FMA "
+                                     "instruction rate"}},
             "cpu_baseline": {"value": cpu, "unit": UNIT, "cores": cpu_cores, "kind": kind, "sample": cpu_sample},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": main["e2e_bytes"],
                     "d2h_bytes_per_step": main["e2e_bytes"] + 8,

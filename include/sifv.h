@@ -500,6 +500,12 @@ typedef struct sifv_comm {
 } sifv_comm_t;
 int sifv_set_comm(sifv_ctx_t* ctx, const sifv_comm_t* comm);
 
+/* Measured FP64 fused multiply-add throughput of the current device (TFLOP/s,
+ * 2 flops per FMA, best of `reps` timed launches of a resident grid): the
+ * FP64 co-bound the benchmark reports beside the HBM roofline of the fused
+ * stage kernels.  No counterpart in the reference. */
+int sifv_fp64_peak_probe(int reps, double* tflops);
+
 /* ---- allocation-free pressure solve ----------------------------------- */
 /* Sizes of the static device scratch behind sifv_pressure_solve_noalloc
  * (reserved on every GPU that loads the library, about 32 MB). */

@@ -72,27 +72,23 @@ namespace {
 // into segments so that every resident warp gets at most one unit (a
 // segment first converts 6 rows and reconstructs 2 before its first update,
 // so segments stay at least 32 rows long).
-template <typename T, int RS>
-int march_launch(TileArgs A, cudaStream_t s) {
-    using S = MarchShape<T>;
-    static int residentWarps[64] = {0};
+template <typename Kernel>
+int march_launch(Kernel kernel, size_t bytes, int* residentWarps, TileArgs A, cudaStream_t s) {
+    constexpr int kWarps = 4, kCols = 30;
     int dev = 0;
     cudaGetDevice(&dev);
-    const size_t bytes = sizeof(MarchWarpSmem<T>) * S::warps;
     if (dev < 0 || dev >= 64) return -1;
     if (residentWarps[dev] == 0) {
-        if (cudaFuncSetAttribute(k_march2d<T, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
-            cudaSuccess)
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
             return -1;
         int sms = 0, perSm = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_march2d<T, RS>, S::warps * 32, bytes) !=
-                cudaSuccess)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kWarps * 32, bytes) != cudaSuccess)
             return -1;
-        residentWarps[dev] = (perSm > 0 ? perSm : 1) * sms * S::warps;
+        residentWarps[dev] = (perSm > 0 ? perSm : 1) * sms * kWarps;
     }
     const int W = residentWarps[dev];
-    A.strips = (A.P.nx + S::cols - 1) / S::cols;
+    A.strips = (A.P.nx + kCols - 1) / kCols;
     int segs = W / A.strips;
     const int maxSegs = (A.P.ny + 31) / 32;
     if (segs > maxSegs) segs = maxSegs;
@@ -100,26 +96,38 @@ int march_launch(TileArgs A, cudaStream_t s) {
     A.segRows = (A.P.ny + segs - 1) / segs;
     A.segs = (A.P.ny + A.segRows - 1) / A.segRows;
     const long long units = (long long)A.strips * A.segs;
-    const long long blocksNeeded = (units + S::warps - 1) / S::warps;
-    const long long maxBlocks = (W + S::warps - 1) / S::warps;
+    const long long blocksNeeded = (units + kWarps - 1) / kWarps;
+    const long long maxBlocks = (W + kWarps - 1) / kWarps;
     const unsigned grid = (unsigned)(blocksNeeded < maxBlocks ? blocksNeeded : maxBlocks);
-    k_march2d<T, RS><<<grid, S::warps * 32, bytes, s>>>(A);
+    kernel<<<grid, kWarps * 32, bytes, s>>>(A);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-template <typename T>
-int march_dispatch(const TileArgs& A, cudaStream_t s) {
+template <int RS>
+int march_fp64(const TileArgs& A, cudaStream_t s) {
+    static int resident[64] = {0};
+    return march_launch(k_march2d<double, RS>, sizeof(MarchWarpSmem<double>) * MarchShape<double>::warps, resident,
+                        A, s);
+}
+
+template <int RS>
+int march_mixed(const TileArgs& A, cudaStream_t s) {
+    static int resident[64] = {0};
+    return march_launch(k_march2d_mixed<RS>, march_mixed_smem(), resident, A, s);
+}
+
+int march_dispatch(const TileArgs& A, cudaStream_t s, bool mixed) {
     switch (A.P.riemann) {
-        case SIFV_HLLC: return march_launch<T, SIFV_HLLC>(A, s);
-        case SIFV_RUSANOV: return march_launch<T, SIFV_RUSANOV>(A, s);
-        default: return march_launch<T, SIFV_LF>(A, s);
+        case SIFV_HLLC: return mixed ? march_mixed<SIFV_HLLC>(A, s) : march_fp64<SIFV_HLLC>(A, s);
+        case SIFV_RUSANOV: return mixed ? march_mixed<SIFV_RUSANOV>(A, s) : march_fp64<SIFV_RUSANOV>(A, s);
+        default: return mixed ? march_mixed<SIFV_LF>(A, s) : march_fp64<SIFV_LF>(A, s);
     }
 }
 
 }  // namespace
 
 int tile2d_stage(const TileArgs& A, cudaStream_t s, bool mixed, int& launches, LaunchMark mark, void* user) {
-    int st = mixed ? march_dispatch<float>(A, s) : march_dispatch<double>(A, s);
+    int st = march_dispatch(A, s, mixed);
     ++launches;
     if (mark) mark(user, "march2d");
     return st;
@@ -173,6 +181,64 @@ int sweep_finish_prim(const Params& P, const Fields& F, const Ctl* ctl, cudaStre
 }
 
 }  // namespace sifv
+
+namespace sifv {
+namespace {
+
+// FP64 fused multiply-add throughput: every thread runs 8 independent
+// chains of `iters` dependent FMAs (x <- x * a + b with |a| < 1, so the
+// values stay finite) and stores their sum (so nothing is optimised away).
+__global__ void __launch_bounds__(256) k_fp64_fma_probe(int iters, double a, double b, double* out) {
+    double x[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) x[q] = (double)(threadIdx.x + q);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) x[q] = fma(x[q], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s += x[q];
+    if (s == 12345.678) out[blockIdx.x] = s;   // practically never: keeps the chains live
+}
+
+}  // namespace
+}  // namespace sifv
+
+// Measured FP64 FMA throughput of the current device (the FP64 co-bound of
+// the fused stage kernels): a resident grid of the probe kernel, best of
+// `reps` launches timed with CUDA events; *tflops = 2 flops per FMA.
+extern "C" int sifv_fp64_peak_probe(int reps, double* tflops) {
+    if (reps <= 0 || !tflops) return -2;
+    int dev = 0, sms = 0, perSm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, sifv::k_fp64_fma_probe, 256, 0))
+        return -3;
+    const int blocks = sms * (perSm > 0 ? perSm : 1), iters = 4096;
+    double* d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * blocks) != cudaSuccess) return -3;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    cudaError_t err = cudaSuccess;
+    for (int r = 0; r <= reps && err == cudaSuccess; ++r) {   // the first launch warms up
+        cudaEventRecord(e0);
+        sifv::k_fp64_fma_probe<<<blocks, 256>>>(iters, 0.999999, 1e-7, d);
+        cudaEventRecord(e1);
+        err = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (r > 0 && ms < best) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    if (err != cudaSuccess) return -3;
+    const double flops = 2.0 * 8.0 * iters * 256.0 * blocks;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return 0;
+}
 
 extern "C" int sifv_fastmath_selftest(long long n, double* maxRelRcp, double* maxRelSqrt) {
     if (n <= 0 || !maxRelRcp || !maxRelSqrt) return -2;
