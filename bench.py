@@ -355,6 +355,11 @@ def run_cuda(args):
         ctx.be.fn["set_stream"](ctx.h, ctypes.c_void_p(stream.cuda_stream))
         if ws > 1:
             slab.DistExchange(ctx, rank, ws, periodic=False, device=True).attach()
+        if args.units_per_warp:
+            ctx.set_work_units(args.units_per_warp)
+            ctx.tuned = args.units_per_warp
+        else:
+            ctx.tuned = ctx.autotune(5)   # work-unit shape of the fused stage kernel (part of the warm-up)
         return ctx
 
     def measure(precision, with_clocks=False, with_e2e=False):
@@ -379,7 +384,7 @@ def run_cuda(args):
         ms = max_over_ranks(e0.elapsed_time(e1))
         step_idx += args.steps
         _, launches = ctx.last_step_stats()
-        out = {"ms": ms, "value": cells * args.steps / (ms / 1e3), "launches": launches,
+        out = {"ms": ms, "value": cells * args.steps / (ms / 1e3), "launches": launches, "tuned": ctx.tuned,
                "clocks": clk.summary() if clk else None, "t": t_sim,
                # the conservative state after the warm-up and timed steps (error against FP64)
                "state": {f: ctx.interior(ctx.get_field(f)).copy() for f in CONS_2D} if ws == 1 else None}
@@ -669,7 +674,8 @@ def run_cuda(args):
         r = measure(args.precision)
         if rank == 0:
             print(json.dumps({"kernels_only": True, "n": n, "precision": PREC_NAMES[args.precision],
-                              "ms_per_step": r["ms"] / args.steps, "value": r["value"]}), flush=True)
+                              "ms_per_step": r["ms"] / args.steps, "value": r["value"],
+                              "units_per_warp": r["tuned"]}), flush=True)
         if ws > 1:
             torch.distributed.destroy_process_group()
         return
@@ -808,6 +814,9 @@ def run_cuda(args):
                     "resident_value": main["e2e_resident"],
                     "resident_api": "sifv_step only, state resident on the GPU (dt to the host each step)"},
             "gpu_launches": launches,
+            "autotune": {"units_per_warp": main["tuned"],
+                         "what": "work units (30-column strip x row segment) per resident warp of the fused "
+                                 "stage kernel, chosen by timing 1-4 (sifv_autotune)"},
             "clocks": clk.summary(),
             "other_precisions": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
                                      "roofline_frac": BYTES_PER_CELL_UPDATE * v["value"] / 1e9 / peak,
@@ -870,6 +879,8 @@ def main():
     ap.add_argument("--no-semi", action="store_true", help="skip the semi-implicit 3D workload")
     ap.add_argument("--profile-case", choices=["semi", "adjoint", "ensemble"], default=None,
                     help="run a small instance of another workload (--n: cells per axis, or tubes) and exit")
+    ap.add_argument("--units-per-warp", type=int, default=0, choices=[0, 1, 2, 3, 4],
+                    help="fix the work units per warp of the 2D fused stage (0: choose by sifv_autotune)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="only the device-timed step loop (no clocks, e2e, CPU baseline): a small case to profile")
     args = ap.parse_args()

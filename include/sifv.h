@@ -469,6 +469,18 @@ int sifv_ensemble_run(sifv_ensemble_t* e, double tEnd, int maxSteps, int blockSi
  * block size for later runs and restore the state. */
 int sifv_ensemble_autotune(sifv_ensemble_t* e, int probeSteps, int* blockSizeOut);
 
+/* Work-unit shape of the 2D fused stage kernel (fast FP64 / mixed):
+ * times `reps` launches of a step's first stage (from the current state into
+ * scratch, so the state is not changed) for 1-4 work units per resident
+ * warp and keeps the fastest for later steps of this context; *choice = the
+ * units per warp chosen (0: the configuration has no fused 2D stage).  No
+ * counterpart in the reference. */
+int sifv_autotune(sifv_ctx_t* ctx, int reps, int* choice);
+/* Set the work units per resident warp of the 2D fused stage kernel (1-4)
+ * without timing; SIFV_ERR_BAD_ARG outside 1-4.  Every choice computes each
+ * cell with the same arithmetic. */
+int sifv_set_work_units(sifv_ctx_t* ctx, int unitsPerWarp);
+
 /* ---- domain decomposition (one rank per GPU) -------------------------- */
 /* The halo exchange and dt reduction of a context whose mesh has
  * SIFV_BC_EXCHANGE faces: HaloExchange::exchangeStateDirection

@@ -254,6 +254,8 @@ _OPTIONAL_SIGS = {
     "reference_time_loop": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_double, C.c_double, C.c_int,
                                       C.POINTER(C.c_int)]),
     "set_comm": (C.c_int, [C.c_void_p, C.POINTER(Comm)]),
+    "autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "set_work_units": (C.c_int, [C.c_void_p, C.c_int]),
 }
 
 
@@ -463,6 +465,17 @@ class Context:
         dt = C.c_double()
         self._check(self.be.fn["step"](self.h, step, time, target_dt, C.byref(dt)))
         return dt.value
+
+    def autotune(self, reps: int = 5) -> int:
+        """sifv_autotune: the work-unit shape of the 2D fused stage; returns
+        the units per warp chosen (0: nothing to tune)."""
+        ch = C.c_int()
+        self._check(self.be.fn["autotune"](self.h, reps, C.byref(ch)))
+        return ch.value
+
+    def set_work_units(self, units_per_warp: int):
+        """sifv_set_work_units: fix the work-unit shape of the 2D fused stage."""
+        self._check(self.be.fn["set_work_units"](self.h, units_per_warp))
 
     def set_comm(self, exchange, allreduce_min):
         """Halo exchange and dt reduction of a decomposed run (sifv_set_comm):

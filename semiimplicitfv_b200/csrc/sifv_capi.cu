@@ -70,6 +70,7 @@ struct sifv_ctx {
     bool dtReady = false;                     // ctl->dtBits holds the acoustic dt of the current state
                                               // (folded in by the last fast 2D stage of the previous step)
     bool exchangeFaces = false;               // the mesh has SIFV_BC_EXCHANGE faces
+    int marchScale = 1;                       // work units per resident warp of the 2D fused stage (sifv_autotune)
     sifv_comm_t comm{};                       // halo exchange / dt reduction of a decomposed run
     int adjEvery = 0;
     std::vector<double> adjDts;               // time-step sequence of the recorded forward run
@@ -79,6 +80,7 @@ struct sifv_ctx {
     bool adjReady = false;
     bool igrTileReady = false;
     double* igrRec = nullptr;                 // IGR sweep records (k_igr_records), then one int flag
+    double* gsRec = nullptr;                  // Gauss-Seidel sweep records (k_gs_records), then one int flag
     double* jacCoef = nullptr;                // Jacobi coefficients: per face (dim arrays) or per cell (2 dim + 2)
     bool uniformAxes = false;                 // interior cell widths bitwise equal along every active axis
     int pressureKind = 0;                     // 0 Jacobi (default), 1 Gauss-Seidel
@@ -531,13 +533,51 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
         if (e != cudaSuccess) return fail(c, SIFV_ERR_CUDA, std::string("GS tile smem: ") + cudaGetErrorString(e));
     }
     double* pp = c->F.pA;
+    // 3D: the record sweep (k_gs_tile_rec) when its 16-byte halo copies are
+    // aligned (even row length, 16-byte aligned iterate)
+    const bool recs = d3 && T3 == kIgrTile && P.nxT % 2 == 0 && ((uintptr_t)pp % 16) == 0;
+    int* slowRecs = nullptr;
+    if (recs) {
+        const long long ntiles = (long long)ntx * nty * ntz;
+        const size_t nrec = gs_record_doubles(ntiles);
+        if (!c->gsRec) {
+            int sa = SIFV_OK;
+            c->gsRec = dalloc(c, nrec + 2, sa);
+            if (sa != SIFV_OK) return sa;
+            CUDA_TRY(c, cudaFuncSetAttribute(k_gs_tile_rec, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)gs_tile_rec_smem()));
+        }
+        slowRecs = reinterpret_cast<int*>(c->gsRec + nrec);
+        CUDA_TRY(c, cudaMemsetAsync(slowRecs, 0, sizeof(int), c->stream));
+        const long long total = ntiles * kIgrTile * kIgrTile * kIgrTile;
+        k_gs_records<<<blocks(total, 256), 256, 0, c->stream>>>(P, c->gsCoef, c->ncells, rhs, c->gsRec, ntx, nty,
+                                                                 total, slowRecs);
+        c->launches++;
+    }
     int it = 0, batch = 2, done = 0;
     while (it < maxIter) {
         int nb = std::min(batch, maxIter - it);
         for (int q = 0; q < nb; ++q, ++it) {
             k_gs_ghosts<<<blocks((long long)c->ncells, kCellThreads), kCellThreads, 0, c->stream>>>(P, pp, c->ctl, it,
                                                                                                      tol);
-            if (P.dim == 1) {
+            if (recs) {
+                for (int pl = 0; pl < nplanes; ++pl) {
+                    // planes after the first overlap their record prologue with the previous plane
+                    cudaLaunchAttribute at[1];
+                    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                    at[0].val.programmaticStreamSerializationAllowed = 1;
+                    cudaLaunchConfig_t lc = {};
+                    lc.gridDim = dim3((unsigned)(nty * ntz));
+                    lc.blockDim = dim3(kIgrTile * kIgrTile);
+                    lc.dynamicSmemBytes = gs_tile_rec_smem();
+                    lc.stream = c->stream;
+                    lc.attrs = at;
+                    lc.numAttrs = pl > 0 ? 1 : 0;
+                    CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_gs_tile_rec, P, (const double*)c->gsRec,
+                                                   (const int*)slowRecs, pp, c->ctl, it, tol, pl, ntx, nty));
+                }
+                c->launches += 1 + nplanes;
+            } else if (P.dim == 1) {
                 k_gs_sweep_1d<<<1, 32, 0, c->stream>>>(P, c->gsCoef, c->ncells, rhs, pp, c->ctl, it, tol);
                 c->launches += 2;
             } else {
@@ -960,6 +1000,7 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
             T.velU = c->F.velU;
             T.velV = c->F.velV;
             T.pres = c->F.pres;
+            T.unitScale = c->marchScale;
             double* const* in = (s == 0) ? U : (s == 1) ? c->tileB : c->tileC;
             double* const* out = (RK > 1 && s == RK - 1) ? U : (s == 0) ? c->tileB : c->tileC;
             for (int q = 0; q < 4; ++q) {
@@ -1373,6 +1414,74 @@ size_t sifv_total_cells(const sifv_ctx_t* c) { return c ? c->ncells : 0; }
 
 int sifv_set_stream(sifv_ctx_t* c, void* stream) {
     c->stream = stream ? static_cast<cudaStream_t>(stream) : c->ownStream;
+    return SIFV_OK;
+}
+
+int sifv_autotune(sifv_ctx_t* c, int reps, int* choice) {
+    if (!c || reps <= 0 || !choice) return fail(c, SIFV_ERR_BAD_ARG, "bad argument");
+    *choice = 0;
+    if (!(c->sweep && c->P.dim == 2)) return SIFV_OK;   // only the 2D fused stage has a shape to tune
+    cudaSetDevice(c->device);
+    if (!c->tileB[0]) {
+        int sa = SIFV_OK;
+        for (int q = 0; q < 4; ++q) {
+            c->tileB[q] = dalloc(c, c->ncells, sa);
+            c->tileC[q] = dalloc(c, c->ncells, sa);
+        }
+        if (sa != SIFV_OK) return sa;
+    }
+    // probe: the first stage of a step from the current state into the scratch
+    // state (the state itself is not written), no primitives, no dt
+    const sifv_config_t& cfg = c->cfg;
+    StageCoef K{};
+    rk_coef(cfg.RKOrder, 0, K);
+    TileArgs T{};
+    T.P = c->P;
+    T.C.gamma = c->P.gamma;
+    T.C.pInf = c->P.pInf;
+    T.C.invGm1 = 1.0 / (c->P.gamma - 1.0);
+    T.C.gPinf = c->P.gamma * c->P.pInf;
+    T.eps = cfg.wenoEps;
+    T.ctl = c->ctl;
+    T.a1 = K.c1 / K.c4;
+    T.a2 = K.c2 / K.c4;
+    T.a3 = K.c3 / K.c4;
+    T.inv[0] = c->invW[0];
+    T.inv[1] = c->invW[1];
+    double* U[4] = {c->F.rho, c->F.rhoU, c->F.rhoV, c->F.rhoE};
+    for (int q = 0; q < 4; ++q) {
+        T.in[q] = U[q];
+        T.out[q] = c->tileB[q];
+        T.u0[q] = nullptr;
+    }
+    CUDA_TRY(c, cudaMemsetAsync(&c->ctl->skip, 0, sizeof(int), c->stream));
+    const bool mixed = cfg.precision == SIFV_PREC_MIXED;
+    int launches = 0, best = 1;
+    float bestMs = 1e30f;
+    for (int scale = 1; scale <= 4; ++scale) {
+        T.unitScale = scale;
+        if (tile2d_stage(T, c->stream, mixed, launches) != 0) return fail(c, SIFV_ERR_CUDA, "autotune launch failed");
+        CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+        for (int r = 0; r < reps; ++r)
+            if (tile2d_stage(T, c->stream, mixed, launches) != 0)
+                return fail(c, SIFV_ERR_CUDA, "autotune launch failed");
+        CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+        CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        if (ms < bestMs) {
+            bestMs = ms;
+            best = scale;
+        }
+    }
+    c->marchScale = best;
+    *choice = best;
+    return SIFV_OK;
+}
+
+int sifv_set_work_units(sifv_ctx_t* c, int unitsPerWarp) {
+    if (!c || unitsPerWarp < 1 || unitsPerWarp > 4) return fail(c, SIFV_ERR_BAD_ARG, "units per warp must be 1-4");
+    c->marchScale = unitsPerWarp;
     return SIFV_OK;
 }
 

@@ -69,9 +69,10 @@ int sweep_stage(SweepArgs A, cudaStream_t s, bool mixed, int& launches, LaunchMa
 namespace {
 
 // Work units of the marching stage kernel: strips of 30 columns, each cut
-// into segments so that every resident warp gets at most one unit (a
-// segment first converts 6 rows and reconstructs 2 before its first update,
-// so segments stay at least 32 rows long).
+// into segments so that every resident warp gets about unitScale units (1
+// by default; sifv_autotune picks it by timing), segments at least 32 rows
+// long (a segment first converts 6 rows and reconstructs 2 before its first
+// update).
 template <typename Kernel>
 int march_launch(Kernel kernel, size_t bytes, int* residentWarps, TileArgs A, cudaStream_t s) {
     constexpr int kWarps = 4, kCols = 30;
@@ -89,7 +90,7 @@ int march_launch(Kernel kernel, size_t bytes, int* residentWarps, TileArgs A, cu
     }
     const int W = residentWarps[dev];
     A.strips = (A.P.nx + kCols - 1) / kCols;
-    int segs = W / A.strips;
+    int segs = (W * (A.unitScale > 1 ? A.unitScale : 1)) / A.strips;
     const int maxSegs = (A.P.ny + 31) / 32;
     if (segs > maxSegs) segs = maxSegs;
     if (segs < 1) segs = 1;

@@ -1779,7 +1779,10 @@ __device__ __noinline__ double div_rn_plain(double a, double b) { return a / b; 
 constexpr int kIgrTile = 16;
 constexpr int kIgrRecsPerLine = kIgrTile + 1;
 constexpr int kIgrRecDoubles = 8;
-constexpr int kIgrPrefetch = 2;                  // records in flight ahead of the cell being updated
+#ifndef SIFV_IGR_PREFETCH
+#define SIFV_IGR_PREFETCH 2
+#endif
+constexpr int kIgrPrefetch = SIFV_IGR_PREFETCH;  // records in flight ahead of the cell being updated
 constexpr int kIgrRing = kIgrPrefetch + 2;       // ring slots per thread
 
 __host__ __device__ __forceinline__ size_t igr_rec_index(long long tile, int tb, int tc, int n) {
@@ -2082,6 +2085,150 @@ __global__ void __launch_bounds__(TY * TZ) k_gs_tile(Params P, const double* __r
         const int b = line % ey, c = line / ey;
         for (int a = lane; a < ex; a += 32)
             p[cidx(P, i0 + a, j0 + b, k0 + c)] = smem[((c + D3) * HY + (b + 1)) * HX + (a + 1)];
+    }
+    block_max_to(maxRes, &ctl->res[it]);
+}
+
+// ---------------------------------------------------------------------------
+// Gauss-Seidel sweep with precomputed records (3D, 16^3 tiles): the tiled
+// wavefront of k_gs_tile<16, 16, 16> with the treatment of the IGR record
+// sweep.  The coefficients, coeff, denominator and rhs of a cell are fixed
+// for the whole solve, so they are laid out once per solve as records that
+// the 16 lines of one tile row fetch as contiguous runs (k_gs_records), with
+// the reciprocal of the denominator: the division (rhs + coeff od) / denom
+// becomes div_markstein's correctly rounded quotient (a plain division where
+// its operand check fails, or for the whole solve when a reciprocal is out
+// of range).  Each thread streams its line's records through a shared-memory
+// ring, each new p is stored as it is computed, and tile planes after the
+// first are launched with programmatic stream serialization (their records
+// arrive while the previous plane runs; p is read after it completes).
+// Record: 10 doubles in five 16-byte chunks (x-, x+, y-, y+, z-, z+
+// coefficients, coeff, denom, 1 / denom, rhs); chunk ch of cell n of line
+// (tb, tc) of tile t at double2 index (((t 16 + tc) 16 + (tb + n) % 16) 5 + ch) 16 + tb.
+// ---------------------------------------------------------------------------
+constexpr int kGsRecChunks = 5;
+
+__host__ __device__ __forceinline__ size_t gs_rec_index(long long tile, int tb, int tc, int n) {
+    return ((((size_t)tile * kIgrTile + tc) * kIgrTile + (tb + n) % kIgrTile) * kGsRecChunks) * kIgrTile + tb;
+}
+inline size_t gs_record_doubles(long long ntiles) {
+    return (size_t)ntiles * kIgrTile * kIgrTile * kIgrTile * 2 * kGsRecChunks;
+}
+inline size_t gs_tile_rec_smem() {
+    return sizeof(double) * (20 * 18 * 18 + kIgrRing * 2 * kGsRecChunks * kIgrTile * kIgrTile);
+}
+
+// Records of the solve from k_jacobi_coef's per-cell coefficients (layout
+// coef[q * nc + c], q = 0..7 in 3D) and the rhs; one thread per record.
+__global__ void __launch_bounds__(256) k_gs_records(Params P, const double* __restrict__ coef, size_t nc,
+                                                    const double* __restrict__ rhs, double* __restrict__ rec,
+                                                    int ntx, int nty, long long total, int* __restrict__ slowRecs) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    constexpr int T = kIgrTile;
+    const int tb = (int)(idx % T);
+    const int sk = (int)((idx / T) % T);
+    const int tc = (int)((idx / ((long long)T * T)) % T);
+    const long long tile = idx / ((long long)T * T * T);
+    const int n = (sk - tb + T) % T;
+    const int I = (int)(tile % ntx), J = (int)((tile / ntx) % nty), K = (int)(tile / ((long long)ntx * nty));
+    const int i0 = I * T, j0 = J * T, k0 = K * T;
+    const int ex = min(T, P.nx - i0), ey = min(T, P.ny - j0), ez = min(T, P.nz - k0);
+    if (tb >= ey || tc >= ez || n >= ex) return;
+    const size_t c = cidx(P, i0 + n, j0 + tb, k0 + tc);
+    double2* o = reinterpret_cast<double2*>(rec) + gs_rec_index(tile, tb, tc, n);
+    const double denom = coef[7 * nc + c];
+    const double rd = 1.0 / denom;
+    o[0] = make_double2(coef[c], coef[nc + c]);
+    o[T] = make_double2(coef[2 * nc + c], coef[3 * nc + c]);
+    o[2 * T] = make_double2(coef[4 * nc + c], coef[5 * nc + c]);
+    o[3 * T] = make_double2(coef[6 * nc + c], denom);
+    o[4 * T] = make_double2(rd, rhs[c]);
+    if (!igr_fast_recip(rd)) atomicOr(slowRecs, 1);
+}
+
+// One tile plane of Gauss-Seidel iteration `it` (a no-op once iteration
+// it-1 converged); the residual max goes to ctl->res[it].  Requires an even
+// row length nxT and a 16-byte aligned iterate.
+__global__ void __launch_bounds__(256, 1) k_gs_tile_rec(Params P, const double* __restrict__ rec,
+                                                        const int* __restrict__ slowRecs, double* __restrict__ p,
+                                                        Ctl* ctl, int it, double tol, int plane, int ntx, int nty) {
+    constexpr int T = kIgrTile, HXP = 20, HY = T + 2, HN = HXP * HY * (T + 2);
+    constexpr int NT = T * T, D = kIgrPrefetch, R = kIgrRing, CH = kGsRecChunks;
+    extern __shared__ __align__(16) double smem[];
+    double* sP = smem;
+    double2* ring = reinterpret_cast<double2*>(smem + HN);   // [R][CH chunks][NT threads]
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+    const int J = (int)(blockIdx.x % (unsigned)nty), K = (int)(blockIdx.x / (unsigned)nty);
+    const int I = plane - J - K;
+    if (I < 0 || I >= ntx) return;
+    const int tid = (int)threadIdx.x;
+    const int i0 = I * T, j0 = J * T, k0 = K * T;
+    const int ex = min(T, P.nx - i0), ey = min(T, P.ny - j0), ez = min(T, P.nz - k0);
+    const int hy = ey + 2, hz = ez + 2;
+    const int xg = i0 - 1 + P.ngx;
+    const int xs = xg & ~1;
+    const int xoff = xg - xs;
+    const int tb = tid % T, tc = tid / T;
+    const bool act = tb < ey && tc < ez;
+    const long long tile = (long long)I + (long long)ntx * (J + (long long)nty * K);
+    const double2* lineRec = reinterpret_cast<const double2*>(rec) + gs_rec_index(tile, 0, tc, 0);
+    auto issue = [&](int n) {
+        if (act && n >= 0 && n < ex) {
+            double2* dst = ring + (size_t)(n % R) * CH * NT + tid;
+            const double2* src = lineRec + (size_t)((tb + n) % T) * CH * T + tb;
+#pragma unroll
+            for (int ch = 0; ch < CH; ++ch) cp_async16(dst + ch * NT, src + ch * T);
+        }
+        cp_async_commit();
+    };
+    // the first records (fixed for the solve) arrive while the previous plane runs
+    for (int q = -D; q < 0; ++q) issue(q - tb - tc + D);
+    const int hLine = ((tc + 1) * HY + (tb + 1)) * HXP + 1 + xoff;
+    const size_t gLine = cidx(P, i0, j0 + tb, k0 + tc);
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");   // p of the previous tile planes
+    if (gs_converged(ctl, it, tol)) {
+        cp_async_wait_group<0>();
+        return;
+    }
+    const bool fastRecs = *slowRecs == 0;
+    for (int w = tid; w < hy * hz * (HXP / 2); w += NT) {
+        const int m = w % (HXP / 2), row = w / (HXP / 2);
+        const int b = row % hy, c = row / hy;
+        const int x = xs + 2 * m;
+        if (x + 1 < P.nxT) {
+            const size_t g = (size_t)x + (size_t)P.nxT * ((size_t)(j0 + b - 1 + P.ngy) +
+                                                          (size_t)P.nyT * (size_t)(k0 + c - 1 + P.ngz));
+            cp_async16(&sP[(c * HY + b) * HXP + 2 * m], &p[g]);
+        }
+    }
+    cp_async_commit();
+    cp_async_wait_group<0>();
+    __syncthreads();
+    double maxRes = 0.0;
+    const int nq = ex + ey + ez - 2;
+    for (int q = 0; q < nq; ++q) {
+        const int a = q - tb - tc;
+        issue(a + D);
+        cp_async_wait_group<D>();   // record a of this thread has landed
+        if (act && a >= 0 && a < ex) {
+            const double2* ra = ring + (size_t)(a % R) * CH * NT + tid;
+            const double2 c0 = ra[0], c1 = ra[NT], c2 = ra[2 * NT], c3 = ra[3 * NT], c4 = ra[4 * NT];
+            const int h = hLine + a;
+            // gs_cell's order: od = cf0 p(x-) + cf1 p(x+), then y, then z
+            double od = 0.0;
+            od += c0.x * sP[h - 1] + c0.y * sP[h + 1];
+            od += c1.x * sP[h - HXP] + c1.y * sP[h + HXP];
+            od += c2.x * sP[h - HXP * HY] + c2.y * sP[h + HXP * HY];
+            const double num = c4.y + c3.x * od;
+            const double pn = (fastRecs && igr_fast_operand(num)) ? div_markstein(num, c3.y, c4.x)
+                                                                  : div_rn_plain(num, c3.y);
+            const double pOld = sP[h];
+            sP[h] = pn;
+            p[gLine + a] = pn;
+            maxRes = smax(maxRes, fabs(pn - pOld));
+        }
+        __syncthreads();
     }
     block_max_to(maxRes, &ctl->res[it]);
 }

@@ -54,6 +54,7 @@ struct TileArgs {
     int last;               // write the primitives of the new state
     double *velU, *velV, *pres;
     int strips, segs, segRows;   // work units: strips of 30 columns x segments of segRows rows (set by the launcher)
+    int unitScale;               // work units per resident warp (autotuned; 0 or 1: one)
     // last stage: fold the acoustic dt of the new state (k_dt_acoustic's
     // expressions) into ctl->dtBits for the next step
     int dtNext;

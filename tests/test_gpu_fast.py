@@ -169,3 +169,32 @@ def test_fast_reciprocal_and_sqrt_within_one_ulp():
     assert lib.sifv_fastmath_selftest(1 << 22, ctypes.byref(r), ctypes.byref(s)) == 0
     assert r.value <= 2.23e-16, r.value
     assert s.value <= 2.23e-16, s.value
+
+
+@pytest.mark.parametrize("prec", [abi.PREC_FP64_FAST, abi.PREC_MIXED])
+def test_autotuned_work_units_leave_results_unchanged(prec):
+    """sifv_autotune picks the work-unit shape of the fused 2D stage by
+    timing; every shape computes each cell with the same arithmetic, so the
+    state after the same steps is bit-identical, and the probe launches do
+    not touch the state."""
+    def run(units):
+        case = cases.riemann2d(300)
+        case[0].precision = prec
+        c = backends.make(backends.cuda(), case)
+        chosen = None
+        if units == "tune":
+            chosen = c.autotune(3)
+        elif units is not None:
+            c.set_work_units(units)
+        cases.run_steps(c, 6)
+        return c, chosen
+    a, _ = run(None)
+    b, chosen = run("tune")
+    assert chosen in (1, 2, 3, 4)
+    runs = [b] + [run(u)[0] for u in (1, 2, 3, 4)]
+    for fid in (abi.F_RHO, abi.F_RHOU, abi.F_RHOV, abi.F_RHOE, abi.F_PRES):
+        x = a.get_field(fid)
+        for r in runs:
+            assert np.array_equal(x.view(np.int64), r.get_field(fid).view(np.int64)), fid
+    with pytest.raises(abi.AbiError):
+        a.set_work_units(5)
