@@ -268,7 +268,7 @@ def reference_decomposed_rate(n: int, warmup: int, steps: int, ranks: int):
     import backends
     import cases
     be = backends.reference(release=True)
-    sec, _, dims, _ = backends.mpi_run(be, cases.riemann2d(n), ranks, warmup, steps, gather=False)
+    sec, _, dims, _, _ = backends.mpi_run(be, cases.riemann2d(n), ranks, warmup, steps, gather=False)
     return n * n * steps / sec, sec, dims
 
 

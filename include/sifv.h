@@ -482,33 +482,46 @@ int sifv_autotune(sifv_ctx_t* ctx, int reps, int* choice);
 int sifv_set_work_units(sifv_ctx_t* ctx, int unitsPerWarp);
 
 /* ---- domain decomposition (one rank per GPU) -------------------------- */
-/* The halo exchange and dt reduction of a context whose mesh has
- * SIFV_BC_EXCHANGE faces: HaloExchange::exchangeStateDirection
- * (src/HaloExchange.cpp:387-465) and the MPI_Allreduce of the time step
- * (src/RKTimeStepping.cpp:148-159), supplied by the caller (NCCL, MPI, or
- * host copies).  The library calls them while it queues a step on its
- * stream:
+/* The halo exchange and reductions of a context whose mesh has
+ * SIFV_BC_EXCHANGE faces: HaloExchange (src/HaloExchange.cpp:387-465), the
+ * MPI_Allreduce of the time step (src/RKTimeStepping.cpp:125-159) and of the
+ * pressure solvers' residual (src/JacobiPressureSolver.cpp:99-100,
+ * src/GaussSeidelPressureSolver.cpp:92-93), supplied by the caller (NCCL,
+ * MPI, or host copies).  The library calls them while it queues a step on
+ * its stream:
  *   exchange(user, fields, nfields, stream): fields are nfields arrays of
  *     the context's extended grid (device arrays; host arrays for a CPU
  *     backend).  For every SIFV_BC_EXCHANGE face, send the nGhost layers of
  *     cells next to the face to the neighbour across it and receive the
  *     neighbour's into this context's nGhost ghost layers of that face,
  *     ordered after the work already on `stream` and before the work queued
- *     after the call.  The fields are the conservative state the next
- *     stage reads (rho, rhoU, [rhoV], [rhoW], rhoE, then alphaRho / alpha of
- *     each phase).
+ *     after the call.  Every rank asks for the same fields in the same order:
+ *     at each stage start the conservative state (rho, rhoU, [rhoV], [rhoW],
+ *     rhoE, alphaRho and alpha of each phase, then sigma with IGR or in the
+ *     semi-implicit step); in the semi-implicit step the primitives after the
+ *     star update and after the correction (rho, velU, [velV], [velW], pres,
+ *     sigma, alphaRho, alpha); one scalar (sigma after every IGR sweep, the
+ *     pressure iterate before every Jacobi / Gauss-Seidel iteration and the
+ *     solution after the solve).
  *   allreduce_min(user, value, stream): replace the non-negative double at
- *     device address `value` by its minimum over all ranks, ordered the same
- *     way.
- * Both return 0 on success; a non-zero return ends the step with
- * SIFV_ERR_CUDA.  The explicit step supports exchange faces (reference
- * order in 1-3D, the fast / mixed 2D step); the semi-implicit step, IGR,
- * viscous / capillary terms and immersed boundaries are rejected with
- * SIFV_ERR_UNSUPPORTED.  A NULL comm clears the hooks. */
+ *     `value` (device address; host for a CPU backend) by its minimum over
+ *     all ranks, ordered the same way (the time step).
+ *   allreduce_max(user, value, stream): the same with the maximum (the
+ *     pressure solvers' residual, once per iteration).
+ * Each returns 0 on success; a non-zero return ends the step with
+ * SIFV_ERR_CUDA.  Supported on a decomposed mesh: the explicit step
+ * (reference order in 1-3D, with or without IGR; the fast / mixed 2D step)
+ * and the reference-ordered semi-implicit step (with or without IGR; Jacobi
+ * or Gauss-Seidel pressure solve, each rank sweeping its own cells in the
+ * reference's order as its MPI ranks do).  Viscous / capillary terms,
+ * immersed boundaries, the mixed-precision semi-implicit step and the PCG
+ * solver are rejected with SIFV_ERR_UNSUPPORTED.  A NULL comm clears the
+ * hooks.  allreduce_max may be NULL for an explicit step. */
 typedef struct sifv_comm {
     int (*exchange)(void* user, double* const* fields, int nfields, void* stream);
     int (*allreduce_min)(void* user, double* value, void* stream);
     void* user;
+    int (*allreduce_max)(void* user, double* value, void* stream);
 } sifv_comm_t;
 int sifv_set_comm(sifv_ctx_t* ctx, const sifv_comm_t* comm);
 

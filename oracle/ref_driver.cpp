@@ -136,7 +136,10 @@ const char* sifvr_last_error(const sifvr_ctx* ctx) {
     return ctx ? ctx->err.c_str() : g_err.c_str();
 }
 
-int sifvr_create(const sifv_config_t* cfg, const sifv_mesh_t* m, int /*device*/, sifvr_ctx** out) {
+// A context on a process grid of procsPerDir ranks per axis (0: MPI_Dims_create
+// chooses), the third argument of MPIContext::create (src/MPIContext.cpp:80-120).
+static int create_on_grid(const sifv_config_t* cfg, const sifv_mesh_t* m, const std::array<int, 3>& procs,
+                          sifvr_ctx** out) {
     *out = nullptr;
     try {
         int mpiInit = 0;
@@ -155,7 +158,7 @@ int sifvr_create(const sifv_config_t* cfg, const sifv_mesh_t* m, int /*device*/,
         for (int d = 0; d < 3; ++d)
             periods[d] = (m->bc[2 * d] == SIFV_BC_PERIODIC && m->bc[2 * d + 1] == SIFV_BC_PERIODIC) ? 1 : 0;
         ctx->mpi = std::make_unique<MPIContext>(
-            MPIContext::create(gnx, gny, gnz, xn, yn, zn, config.dim, periods));
+            MPIContext::create(gnx, gny, gnz, xn, yn, zn, config.dim, periods, procs));
         ctx->mesh = std::make_unique<RectilinearMesh>(config, ctx->mpi->localXNodes(),
                                                       ctx->mpi->localYNodes(), ctx->mpi->localZNodes());
         for (int f = 0; f < 6; ++f)
@@ -188,6 +191,10 @@ int sifvr_create(const sifv_config_t* cfg, const sifv_mesh_t* m, int /*device*/,
         g_err = e.what();
         return SIFV_ERR_BAD_CONFIG;
     }
+}
+
+int sifvr_create(const sifv_config_t* cfg, const sifv_mesh_t* m, int /*device*/, sifvr_ctx** out) {
+    return create_on_grid(cfg, m, {0, 0, 0}, out);
 }
 
 // Swap the pressure solver of a semi-implicit context: 0 Jacobi, 1 Gauss-Seidel.
@@ -411,16 +418,21 @@ int sifvr_apply_ib_ghost_cells(sifvr_ctx* ctx) {
 // of the reference's drivers would run it: MPIContext::create splits the
 // global mesh (src/MPIContext.cpp:80-170), HaloExchange moves the ghost
 // layers (src/HaloExchange.cpp:387-465) and dt / residuals are reduced over
-// the ranks.  Every rank copies the interior block of the global initial
+// the ranks.  procsPerDir (may be null: MPI_Dims_create chooses) fixes the
+// process grid, e.g. {1, 1, n} for slabs along z; pressureKind picks the
+// semi-implicit pressure solver (0 Jacobi, 1 Gauss-Seidel).  Every rank copies the interior block of the global initial
 // fields init[f] (ghosts included, x fastest; its own ghosts start at
 // zero, as in the reference's drivers), takes `warmup` steps, then `steps`
 // steps between two barriers, and copies its interior block back into
 // out[f] (global arrays; may be null).  secondsOut = the timed steps' wall
 // time, maximum over the ranks; dtsOut (warmup + steps values, may be
-// null) = the time steps; dimsOut = the process grid.
+// null) = the time steps; itersOut (the same length, may be null) = the
+// pressure iterations of each step's last stage; dimsOut = the process grid.
 struct MpiRunArgs {
     const sifv_config_t* cfg;
     const sifv_mesh_t* mesh;
+    std::array<int, 3> procs;
+    int pressureKind;
     int nfields;
     const int* fieldIds;
     const double* const* init;
@@ -428,6 +440,7 @@ struct MpiRunArgs {
     int warmup, steps;
     double seconds;
     double* dts;
+    int* iters;
     int dims[3];
     int status;
     std::mutex m;
@@ -437,7 +450,8 @@ struct MpiRunArgs {
 static void mpi_rank_main(void* user, int rank) {
     MpiRunArgs& A = *static_cast<MpiRunArgs*>(user);
     sifvr_ctx* ctx = nullptr;
-    int st = sifvr_create(A.cfg, A.mesh, 0, &ctx);
+    int st = create_on_grid(A.cfg, A.mesh, A.procs, &ctx);
+    if (st == SIFV_OK && A.pressureKind != 0) st = sifvr_set_pressure_solver(ctx, A.pressureKind);
     if (st != SIFV_OK) {
         std::lock_guard<std::mutex> lock(A.m);
         A.status = st;
@@ -472,6 +486,7 @@ static void mpi_rank_main(void* user, int rank) {
             A.err = ctx->err;
         }
         if (rank == 0 && A.dts) A.dts[step] = dt;
+        if (rank == 0 && A.iters) A.iters[step] = ctx->lastIters;
         t += dt;
         ++step;
     };
@@ -497,13 +512,17 @@ static void mpi_rank_main(void* user, int rank) {
     sifvr_destroy(ctx);
 }
 
-int sifvr_mpi_run(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int nranks, int nfields, const int* fieldIds,
-                  const double* const* init, double* const* out, int warmup, int steps, double* secondsOut,
-                  double* dtsOut, int* dimsOut) {
+int sifvr_mpi_run(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int nranks, const int* procsPerDir,
+                  int pressureKind, int nfields, const int* fieldIds, const double* const* init, double* const* out,
+                  int warmup, int steps, double* secondsOut, double* dtsOut, int* itersOut, int* dimsOut) {
     if (!cfg || !mesh || nranks < 1 || warmup < 0 || steps < 0) return SIFV_ERR_BAD_ARG;
     MpiRunArgs A;
     A.cfg = cfg;
     A.mesh = mesh;
+    A.procs = {0, 0, 0};
+    if (procsPerDir)
+        for (int d = 0; d < 3; ++d) A.procs[d] = procsPerDir[d];
+    A.pressureKind = pressureKind;
     A.nfields = nfields;
     A.fieldIds = fieldIds;
     A.init = init;
@@ -512,6 +531,7 @@ int sifvr_mpi_run(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int nranks,
     A.steps = steps;
     A.seconds = 0.0;
     A.dts = dtsOut;
+    A.iters = itersOut;
     A.dims[0] = A.dims[1] = A.dims[2] = 0;
     A.status = SIFV_OK;
     if (sifv_mpi_shim_run(nranks, mpi_rank_main, &A) != 0) return SIFV_ERR_BAD_ARG;

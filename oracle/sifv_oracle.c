@@ -75,6 +75,7 @@ typedef struct sifvo_ctx {
      * halo exchange / dt reduction (sifv_comm_t) */
     int exchangeFaces;
     sifv_comm_t comm;
+    int commFailed; /* a hook failed (or was missing) during the current step */
     char err[256];
 } ctx_t;
 
@@ -203,31 +204,64 @@ static void apply_bc_prim(ctx_t* m) {
             }
 }
 
-/* RectilinearMesh::fillScalarGhosts, src/RectilinearMesh.cpp:424-492 (and
- * the halo variant 526-624): periodic wrap, otherwise zero gradient. */
+/* Halo exchange of n fields through the caller's hook (HaloExchange,
+ * src/HaloExchange.cpp:387-465): the nGhost layers next to every exchange
+ * face to the neighbour, the neighbour's into the ghost layers.  A failure
+ * is kept in commFailed and ends the step. */
+static void exchange_n(ctx_t* m, double* const* f, int n) {
+    if (!m->exchangeFaces) return;
+    if (!m->comm.exchange || m->comm.exchange(m->comm.user, f, n, NULL) != 0) m->commFailed = 1;
+}
+
+/* Maximum over the ranks (the residual MPI_Allreduce of the pressure solvers,
+ * src/JacobiPressureSolver.cpp:99-100, src/GaussSeidelPressureSolver.cpp:92-93). */
+static void allreduce_max(ctx_t* m, double* v) {
+    if (!m->exchangeFaces) return;
+    if (!m->comm.allreduce_max || m->comm.allreduce_max(m->comm.user, v, NULL) != 0) m->commFailed = 1;
+}
+
+/* RectilinearMesh::fillScalarGhosts, src/RectilinearMesh.cpp:424-492, and
+ * the halo variant 526-624: periodic wrap, otherwise zero gradient.  On a
+ * decomposed mesh the exchange comes first and the faces it fills are
+ * skipped; the faster axes' fills then also cover the exchanged ghost layers
+ * of the slower axes, which reproduces the values the reference's
+ * onion-peel order (fill x, exchange y including x ghosts, ...) gives there:
+ * a ghost's source lies in its own line along the filled axis. */
 static void fill_scalar_ghosts(ctx_t* m, double* f) {
-    for (int k = 0; k < m->nz; ++k)
-        for (int j = 0; j < m->ny; ++j)
+    const int EX = SIFV_BC_EXCHANGE;
+    exchange_n(m, &f, 1);
+    const int jlo = (m->dim >= 2 && m->bc[2] == EX) ? -m->ngy : 0, jhi = m->ny + ((m->dim >= 2 && m->bc[3] == EX) ? m->ngy : 0);
+    const int klo = (m->dim >= 3 && m->bc[4] == EX) ? -m->ngz : 0, khi = m->nz + ((m->dim >= 3 && m->bc[5] == EX) ? m->ngz : 0);
+    for (int k = klo; k < khi; ++k)
+        for (int j = jlo; j < jhi; ++j)
             for (int g = 1; g <= m->ngx; ++g) {
-                f[IDX(m, -g, j, k)] = (m->bc[0] == SIFV_BC_PERIODIC) ? f[IDX(m, m->nx - g, j, k)] : f[IDX(m, 0, j, k)];
-                f[IDX(m, m->nx - 1 + g, j, k)] =
-                    (m->bc[1] == SIFV_BC_PERIODIC) ? f[IDX(m, g - 1, j, k)] : f[IDX(m, m->nx - 1, j, k)];
+                if (m->bc[0] != EX)
+                    f[IDX(m, -g, j, k)] = (m->bc[0] == SIFV_BC_PERIODIC) ? f[IDX(m, m->nx - g, j, k)] : f[IDX(m, 0, j, k)];
+                if (m->bc[1] != EX)
+                    f[IDX(m, m->nx - 1 + g, j, k)] =
+                        (m->bc[1] == SIFV_BC_PERIODIC) ? f[IDX(m, g - 1, j, k)] : f[IDX(m, m->nx - 1, j, k)];
             }
     if (m->dim >= 2)
-        for (int k = 0; k < m->nz; ++k)
+        for (int k = klo; k < khi; ++k)
             for (int i = -m->ngx; i < m->nx + m->ngx; ++i)
                 for (int g = 1; g <= m->ngy; ++g) {
-                    f[IDX(m, i, -g, k)] = (m->bc[2] == SIFV_BC_PERIODIC) ? f[IDX(m, i, m->ny - g, k)] : f[IDX(m, i, 0, k)];
-                    f[IDX(m, i, m->ny - 1 + g, k)] =
-                        (m->bc[3] == SIFV_BC_PERIODIC) ? f[IDX(m, i, g - 1, k)] : f[IDX(m, i, m->ny - 1, k)];
+                    if (m->bc[2] != EX)
+                        f[IDX(m, i, -g, k)] =
+                            (m->bc[2] == SIFV_BC_PERIODIC) ? f[IDX(m, i, m->ny - g, k)] : f[IDX(m, i, 0, k)];
+                    if (m->bc[3] != EX)
+                        f[IDX(m, i, m->ny - 1 + g, k)] =
+                            (m->bc[3] == SIFV_BC_PERIODIC) ? f[IDX(m, i, g - 1, k)] : f[IDX(m, i, m->ny - 1, k)];
                 }
     if (m->dim >= 3)
         for (int j = -m->ngy; j < m->ny + m->ngy; ++j)
             for (int i = -m->ngx; i < m->nx + m->ngx; ++i)
                 for (int g = 1; g <= m->ngz; ++g) {
-                    f[IDX(m, i, j, -g)] = (m->bc[4] == SIFV_BC_PERIODIC) ? f[IDX(m, i, j, m->nz - g)] : f[IDX(m, i, j, 0)];
-                    f[IDX(m, i, j, m->nz - 1 + g)] =
-                        (m->bc[5] == SIFV_BC_PERIODIC) ? f[IDX(m, i, j, g - 1)] : f[IDX(m, i, j, m->nz - 1)];
+                    if (m->bc[4] != EX)
+                        f[IDX(m, i, j, -g)] =
+                            (m->bc[4] == SIFV_BC_PERIODIC) ? f[IDX(m, i, j, m->nz - g)] : f[IDX(m, i, j, 0)];
+                    if (m->bc[5] != EX)
+                        f[IDX(m, i, j, m->nz - 1 + g)] =
+                            (m->bc[5] == SIFV_BC_PERIODIC) ? f[IDX(m, i, j, g - 1)] : f[IDX(m, i, j, m->nz - 1)];
                 }
 }
 
@@ -352,7 +386,7 @@ static void cons_to_prim(ctx_t* m) {
 static int exchange_cons(ctx_t* m) {
     if (!m->exchangeFaces) return SIFV_OK;
     if (!m->comm.exchange) return SIFV_ERR_BAD_ARG;
-    double* f[5 + 2 * MAXPH];
+    double* f[6 + 2 * MAXPH];
     int n = 0;
     f[n++] = m->rho;
     f[n++] = m->rhoU;
@@ -361,7 +395,29 @@ static int exchange_cons(ctx_t* m) {
     f[n++] = m->rhoE;
     for (int ph = 0; ph < m->c.nPhases; ++ph) f[n++] = m->alphaRho[ph];
     for (int ph = 0; ph < m->c.nPhases; ++ph) f[n++] = m->alpha[ph];
+    /* sigma travels with the reference's PRIM set; it matters with IGR and in
+     * the semi-implicit correction */
+    if (m->c.useIGR || m->c.semiImplicit) f[n++] = m->sigma;
     return m->comm.exchange(m->comm.user, f, n, NULL) == 0 ? SIFV_OK : SIFV_ERR_CUDA;
+}
+
+/* The reference's PRIM exchange (HaloExchange::packState, VarSet::PRIM,
+ * src/HaloExchange.cpp:204-212) where the primitives are not functions of
+ * the conservative cells: after the semi-implicit star update and after the
+ * correction. */
+static void exchange_prim(ctx_t* m) {
+    if (!m->exchangeFaces) return;
+    double* f[6 + 2 * MAXPH];
+    int n = 0;
+    f[n++] = m->rho;
+    f[n++] = m->velU;
+    if (m->dim >= 2) f[n++] = m->velV;
+    if (m->dim >= 3) f[n++] = m->velW;
+    f[n++] = m->pres;
+    f[n++] = m->sigma;
+    for (int ph = 0; ph < m->c.nPhases; ++ph) f[n++] = m->alphaRho[ph];
+    for (int ph = 0; ph < m->c.nPhases; ++ph) f[n++] = m->alpha[ph];
+    exchange_n(m, f, n);
 }
 
 /* ---- time steps ---- */
@@ -1388,6 +1444,7 @@ static int jacobi_solve(ctx_t* m, const double* rho, const double* rhoc2, const 
         for (int k = 0; k < m->nz; ++k)
             for (int j = 0; j < m->ny; ++j)
                 for (int i = 0; i < m->nx; ++i) p[IDX(m, i, j, k)] = pNew[IDX(m, i, j, k)];
+        allreduce_max(m, &maxRes);
         if (maxRes < tol) return it + 1;
     }
     return maxIter;
@@ -1414,6 +1471,7 @@ static int gs_solve(ctx_t* m, const double* rho, const double* rhoc2, const doub
                     double res = fabs(p[idx] - pOld);
                     maxRes = smax(maxRes, res);
                 }
+        allreduce_max(m, &maxRes);
         if (maxRes < tol) return it + 1;
     }
     return maxIter;
@@ -1480,6 +1538,7 @@ static double explicit_step(ctx_t* m, int step, double targetDt) {
     double rk[3][4];
     rk_coefs(c->RKOrder, rk);
     const int nPh = c->nPhases;
+    m->commFailed = 0;
     for (int s = 0; s < c->RKOrder; ++s) {
         if (exchange_cons(m) != SIFV_OK) return -1.0;
         cons_to_prim(m);
@@ -1523,7 +1582,7 @@ static double explicit_step(ctx_t* m, int step, double targetDt) {
                     if (nPh > 0) mp_post(m, idx);
                 }
     }
-    if (exchange_cons(m) != SIFV_OK) return -1.0;
+    if (exchange_cons(m) != SIFV_OK || m->commFailed) return -1.0;
     cons_to_prim(m);
     apply_bc_prim(m);
     if (m->cellType) ib_apply_ghosts(m);
@@ -1633,6 +1692,7 @@ static void correction_step(ctx_t* m, double dt) {
                 if (m->dim >= 2) m->velV[idx] = m->rhoV[idx] / rs;
                 if (m->dim >= 3) m->velW[idx] = m->rhoW[idx] / rs;
             }
+    exchange_prim(m);
     apply_bc_prim(m);
     double alphas[MAXPH];
     for (int k = 0; k < m->nz; ++k)
@@ -1658,13 +1718,18 @@ static double semi_step(ctx_t* m, int step, double targetDt) {
     double dt = advective_dt(m, c->siCfl, c->siMaxDt);
     if (has_viscosity(c)) dt = smin(dt, viscous_dt(m, c->mu, c->siCfl, c->siMaxDt, 0));
     if (c->stSigma > 0.0) dt = smin(dt, capillary_dt(m, c->stSigma, c->siCfl, c->siMaxDt, 0));
+    /* decomposed run: MPI_Allreduce(MIN) of each local dt, src/RKTimeStepping.cpp:125-133 */
+    if (m->exchangeFaces && m->comm.allreduce_min && m->comm.allreduce_min(m->comm.user, &dt, NULL) != 0)
+        return -1.0;
     if (targetDt > 0) dt = smin(dt, targetDt);
     dt = sclamp(dt, c->siMinDt, c->siMaxDt);
     double rk[3][4];
     rk_coefs(c->RKOrder, rk);
     const int nPh = c->nPhases;
     const int RK = c->RKOrder;
+    m->commFailed = 0;
     for (int s = 0; s < RK; ++s) {
+        if (exchange_cons(m) != SIFV_OK) return -1.0;
         cons_to_prim(m);
         apply_bc_prim(m);
         if (c->useIGR) {
@@ -1714,9 +1779,11 @@ static double semi_step(ctx_t* m, int step, double targetDt) {
                     if (m->dim >= 2) m->velV[idx] = m->rhoVStar[idx] / rs;
                     if (m->dim >= 3) m->velW[idx] = m->rhoWStar[idx] / rs;
                 }
+        exchange_prim(m);   /* density + star velocity, src/SemiImplicitSolver.cpp:228-229 */
         apply_bc_prim(m);
         m->lastIters = solve_pressure(m, dt);
         correction_step(m, dt);
+        if (m->commFailed) return -1.0;
     }
     return dt;
 }
@@ -1801,9 +1868,8 @@ int sifvo_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, 
         m->bc[f] = mesh->bc[f];
         if (f < 2 * cfg->dim && mesh->bc[f] == SIFV_BC_EXCHANGE) m->exchangeFaces = 1;
     }
-    if (m->exchangeFaces && (cfg->semiImplicit || cfg->useIGR || has_viscosity(cfg) || cfg->stSigma > 0.0)) {
-        snprintf(g_err, sizeof(g_err), "SIFV_BC_EXCHANGE faces are supported by the explicit step without IGR, "
-                                       "viscosity or surface tension");
+    if (m->exchangeFaces && (has_viscosity(cfg) || cfg->stSigma > 0.0)) {
+        snprintf(g_err, sizeof(g_err), "SIFV_BC_EXCHANGE faces are not supported with viscosity or surface tension");
         free(m->xExt); free(m->yExt); free(m->zExt); free(m);
         return SIFV_ERR_UNSUPPORTED;
     }

@@ -178,7 +178,8 @@ ALLREDUCE_MIN_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
 
 
 class Comm(C.Structure):
-    _fields_ = [("exchange", EXCHANGE_FN), ("allreduce_min", ALLREDUCE_MIN_FN), ("user", C.c_void_p)]
+    _fields_ = [("exchange", EXCHANGE_FN), ("allreduce_min", ALLREDUCE_MIN_FN), ("user", C.c_void_p),
+                ("allreduce_max", ALLREDUCE_MIN_FN)]
 
 
 class AbiError(RuntimeError):
@@ -477,11 +478,12 @@ class Context:
         """sifv_set_work_units: fix the work-unit shape of the 2D fused stage."""
         self._check(self.be.fn["set_work_units"](self.h, units_per_warp))
 
-    def set_comm(self, exchange, allreduce_min):
-        """Halo exchange and dt reduction of a decomposed run (sifv_set_comm):
+    def set_comm(self, exchange, allreduce_min, allreduce_max=None):
+        """Halo exchange and reductions of a decomposed run (sifv_set_comm):
         exchange(pointers, stream) gets the field addresses (ints) the
-        step asks to exchange; allreduce_min(pointer, stream) the address of
-        the device (or host) double to reduce.  Both return None or 0; an
+        step asks to exchange; allreduce_min / allreduce_max(pointer, stream)
+        the address of the device (or host) double to reduce (the time step;
+        the pressure solvers' residual).  Each returns None or 0; an
         exception is reported to the library as a failure."""
         def ex(user, fields, n, stream):
             try:
@@ -492,15 +494,18 @@ class Context:
                 traceback.print_exc()
                 return 1
 
-        def mn(user, value, stream):
-            try:
-                return int(allreduce_min(value, stream) or 0)
-            except Exception:
-                import traceback
-                traceback.print_exc()
-                return 1
-        self._comm_cb = (EXCHANGE_FN(ex), ALLREDUCE_MIN_FN(mn))   # kept alive with the context
-        c = Comm(self._comm_cb[0], self._comm_cb[1], None)
+        def reducer(fn):
+            def red(user, value, stream):
+                try:
+                    return int(fn(value, stream) or 0)
+                except Exception:
+                    import traceback
+                    traceback.print_exc()
+                    return 1
+            return ALLREDUCE_MIN_FN(red)
+        mx = reducer(allreduce_max) if allreduce_max is not None else ALLREDUCE_MIN_FN()
+        self._comm_cb = (EXCHANGE_FN(ex), reducer(allreduce_min), mx)   # kept alive with the context
+        c = Comm(self._comm_cb[0], self._comm_cb[1], None, self._comm_cb[2])
         self._check(self.be.fn["set_comm"](self.h, C.byref(c)))
 
     def set_immersed_bodies(self, bodies):

@@ -342,6 +342,11 @@ void launch_ib_scalar(sifv_ctx* c, double* f) {
     c->launches++;
 }
 
+// halo exchange / reductions of a decomposed mesh (defined with the step)
+int exchange_fields(sifv_ctx* c, double* const* fields, int n);
+int exchange_scalar(sifv_ctx* c, const double* f);
+int reduce_residual(sifv_ctx* c, unsigned long long* slot);
+
 int igr_solve(sifv_ctx* c, int step) {
     const Params& P = c->P;
     k_igr_setup<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(P, c->F, c->alphaIGR);
@@ -412,6 +417,10 @@ int igr_solve(sifv_ctx* c, int step) {
             }
             c->launches += nplanes;
         }
+        {   // fillScalarGhosts(sigma, halo), src/IGR.cpp:155
+            int st = exchange_scalar(c, c->F.sigma);
+            if (st != SIFV_OK) return st;
+        }
         launch_scalar_ghosts(c, c->F.sigma);
         launch_ib_scalar(c, c->F.sigma);   // src/IGR.cpp:156
     }
@@ -460,6 +469,10 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
         for (int q = 0; q < nb; ++q, ++it) {
             const double* pin = (it & 1) ? c->F.pB : c->F.pA;
             double* pout = (it & 1) ? c->F.pA : c->F.pB;
+            {   // decomposed mesh: the iterate's ghost layers from the neighbours (src/JacobiPressureSolver.cpp:72)
+                int st = exchange_scalar(c, pin);
+                if (st != SIFV_OK) return st;
+            }
             if (c->P.dim == 3) {
                 const dim3 g3((unsigned)((c->P.nx + 31) / 32), (unsigned)((c->P.ny + 7) / 8),
                               (unsigned)((c->P.nz + kJacZ - 1) / kJacZ));
@@ -475,6 +488,10 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
             else
                 k_jacobi_pre<<<gj, kCellThreads, 0, c->stream>>>(c->P, c->jacCoef, c->ncells, rhs, pin, pout, c->ctl,
                                                                 it, tol);
+            {   // the iteration's change, maximum over the ranks, before the next iteration tests it
+                int st = reduce_residual(c, &c->ctl->res[it]);
+                if (st != SIFV_OK) return st;
+            }
         }
         c->launches += nb;
         LAUNCH_CHECK(c);
@@ -558,6 +575,10 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
     while (it < maxIter) {
         int nb = std::min(batch, maxIter - it);
         for (int q = 0; q < nb; ++q, ++it) {
+            {   // decomposed mesh: fillScalarGhosts(pressure, halo), src/GaussSeidelPressureSolver.cpp:69
+                int st = exchange_scalar(c, pp);
+                if (st != SIFV_OK) return st;
+            }
             k_gs_ghosts<<<blocks((long long)c->ncells, kCellThreads), kCellThreads, 0, c->stream>>>(P, pp, c->ctl, it,
                                                                                                      tol);
             if (recs) {
@@ -591,6 +612,10 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
                                                                                       nty);
                 }
                 c->launches += 1 + nplanes;
+            }
+            {   // src/GaussSeidelPressureSolver.cpp:92-93
+                int st = reduce_residual(c, &c->ctl->res[it]);
+                if (st != SIFV_OK) return st;
             }
         }
         LAUNCH_CHECK(c);
@@ -842,6 +867,9 @@ int jacobi_mixed_run(sifv_ctx* c, const double* rho, const double* rhoc2, const 
 
 int pressure_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rhs, double tol, int maxIter,
                  int& iters, const double*& result) {
+    if (c->exchangeFaces && (c->pressureKind == 2 || (c->pressureKind == 0 && c->cfg.precision == SIFV_PREC_MIXED)))
+        return fail(c, SIFV_ERR_UNSUPPORTED,
+                    "decomposed mesh: the pressure solve supports Jacobi (FP64) and Gauss-Seidel");
     c->lastInPlace = (c->pressureKind != 0) ? 1 : 0;
     if (c->pressureKind == 0 && c->cfg.precision == SIFV_PREC_MIXED)
         return jacobi_mixed_run(c, rho, rhoc2, rhs, tol, maxIter, iters, result);
@@ -889,7 +917,7 @@ int exchange_fields(sifv_ctx* c, double* const* fields, int n) {
 // per cell).
 int exchange_cons(sifv_ctx* c) {
     if (!c->exchangeFaces) return SIFV_OK;
-    double* f[5 + 2 * SIFV_MAX_PHASES];
+    double* f[6 + 2 * SIFV_MAX_PHASES];
     int n = 0;
     f[n++] = c->F.rho;
     f[n++] = c->F.rhoU;
@@ -898,7 +926,46 @@ int exchange_cons(sifv_ctx* c) {
     f[n++] = c->F.rhoE;
     for (int ph = 0; ph < c->P.nPh; ++ph) f[n++] = c->F.alphaRho[ph];
     for (int ph = 0; ph < c->P.nPh; ++ph) f[n++] = c->F.alpha[ph];
+    // sigma travels with the reference's PRIM set; it matters with IGR and in
+    // the semi-implicit correction
+    if (c->cfg.useIGR || c->cfg.semiImplicit) f[n++] = c->F.sigma;
     return exchange_fields(c, f, n);
+}
+
+// The reference's PRIM exchange (HaloExchange::packState, VarSet::PRIM,
+// src/HaloExchange.cpp:204-212) where the primitives are not functions of
+// the conservative cells: after the semi-implicit star update and after the
+// correction.
+int exchange_prim(sifv_ctx* c) {
+    if (!c->exchangeFaces) return SIFV_OK;
+    double* f[6 + 2 * SIFV_MAX_PHASES];
+    int n = 0;
+    f[n++] = c->F.rho;
+    f[n++] = c->F.velU;
+    if (c->P.dim >= 2) f[n++] = c->F.velV;
+    if (c->P.dim >= 3) f[n++] = c->F.velW;
+    f[n++] = c->F.pres;
+    f[n++] = c->F.sigma;
+    for (int ph = 0; ph < c->P.nPh; ++ph) f[n++] = c->F.alphaRho[ph];
+    for (int ph = 0; ph < c->P.nPh; ++ph) f[n++] = c->F.alpha[ph];
+    return exchange_fields(c, f, n);
+}
+
+// One scalar field (fillScalarGhosts with a HaloExchange, src/RectilinearMesh.cpp:526-624).
+int exchange_scalar(sifv_ctx* c, const double* f) {
+    double* p = const_cast<double*>(f);
+    return exchange_fields(c, &p, 1);
+}
+
+// Maximum over the ranks of a pressure-solver residual slot (the bits of a
+// non-negative double): the MPI_Allreduce of src/JacobiPressureSolver.cpp:99-100.
+int reduce_residual(sifv_ctx* c, unsigned long long* slot) {
+    if (!c->exchangeFaces) return SIFV_OK;
+    if (!c->comm.allreduce_max)
+        return fail(c, SIFV_ERR_BAD_ARG, "the pressure solve of a decomposed mesh needs allreduce_max (sifv_set_comm)");
+    if (c->comm.allreduce_max(c->comm.user, reinterpret_cast<double*>(slot), c->stream) != 0)
+        return fail(c, SIFV_ERR_CUDA, "residual reduction over the ranks failed");
+    return SIFV_OK;
 }
 
 int enqueue_dt(sifv_ctx* c, double targetDt, int useEnd) {
@@ -915,6 +982,10 @@ int enqueue_dt(sifv_ctx* c, double targetDt, int useEnd) {
             k_dt_capillary<<<g, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, cfg.siCfl);
             c->launches++;
         }
+        // decomposed run: the minimum over the ranks (src/RKTimeStepping.cpp:125-133)
+        if (c->comm.allreduce_min &&
+            c->comm.allreduce_min(c->comm.user, reinterpret_cast<double*>(&c->ctl->dtBits), c->stream) != 0)
+            return fail(c, SIFV_ERR_CUDA, "dt reduction over the ranks failed");
         k_dt_finalize<<<1, 1, 0, c->stream>>>(c->ctl, -1.0, targetDt, 1, cfg.siMinDt, cfg.siMaxDt, useEnd);
         c->launches += 3;
     } else if (c->forcedDt > 0) {
@@ -1108,6 +1179,10 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
             NPH_DISPATCH(c, (k_assemble<NPHV, 1><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl, K)));
             c->launches++;
             mark(c, "assemble");
+            {   // density + star velocity, src/SemiImplicitSolver.cpp:228-229
+                int st = exchange_prim(c);
+                if (st != SIFV_OK) return st;
+            }
             launch_bc_prim(c);
             NPH_DISPATCH(c, (k_pressure_setup<NPHV><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, c->ctl)));
             c->launches++;
@@ -1125,9 +1200,18 @@ int enqueue_step(sifv_ctx* c, int step, double time, double targetDt, int useEnd
                 std::memcpy(&last, &b, sizeof(double));
                 if (!(last < cfg.pressureTol)) status = SIFV_NOT_CONVERGED;
             }
+            if (c->exchangeFaces) {   // fillScalarGhosts(pressure_ / sigma, halo), src/SemiImplicitSolver.cpp:581-582
+                int st = exchange_scalar(c, pres);
+                if (st == SIFV_OK) st = exchange_scalar(c, c->F.sigma);
+                if (st != SIFV_OK) return st;
+            }
             NPH_DISPATCH(c, (k_correction<NPHV><<<gc, kCellThreads, 0, c->stream>>>(c->P, c->F, pres, c->ctl)));
             c->launches++;
             mark(c, "correction");
+            {   // src/SemiImplicitSolver.cpp:642
+                int st = exchange_prim(c);
+                if (st != SIFV_OK) return st;
+            }
             launch_bc_prim(c);
             LAUNCH_CHECK(c);
         }
@@ -1212,13 +1296,18 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     }
     if (exchangeFaces) {
         const bool visc = cfg->mu > 0.0 || cfg->nPhaseMu > 0 || cfg->stSigma > 0.0;
-        if (cfg->semiImplicit || cfg->useIGR || visc)
+        if (visc)
             return fail(nullptr, SIFV_ERR_UNSUPPORTED,
-                        "SIFV_BC_EXCHANGE faces (domain decomposition) are supported by the explicit step without "
-                        "IGR, viscosity or surface tension");
-        if (cfg->precision != SIFV_PREC_FP64 && dim != 2)
+                        "SIFV_BC_EXCHANGE faces (domain decomposition) are not supported with viscosity or surface "
+                        "tension");
+        if (cfg->semiImplicit && cfg->precision == SIFV_PREC_MIXED)
             return fail(nullptr, SIFV_ERR_UNSUPPORTED,
-                        "SIFV_BC_EXCHANGE faces on the fast / mixed path are supported in 2D (use SIFV_PREC_FP64)");
+                        "SIFV_BC_EXCHANGE faces: the mixed-precision semi-implicit step is not supported (use "
+                        "SIFV_PREC_FP64)");
+        if (!cfg->semiImplicit && cfg->precision != SIFV_PREC_FP64 && (dim != 2 || cfg->useIGR))
+            return fail(nullptr, SIFV_ERR_UNSUPPORTED,
+                        "SIFV_BC_EXCHANGE faces on the fast / mixed path are supported in 2D without IGR (use "
+                        "SIFV_PREC_FP64)");
     }
 
     sifv_ctx* c = new sifv_ctx();

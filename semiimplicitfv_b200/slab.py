@@ -175,6 +175,11 @@ class DistExchange:
         dist.all_reduce(_view(ptr, 1, self.device), op=dist.ReduceOp.MIN)
         return 0
 
+    def allreduce_max(self, ptr, stream):
+        import torch.distributed as dist
+        dist.all_reduce(_view(ptr, 1, self.device), op=dist.ReduceOp.MAX)
+        return 0
+
     def attach(self):
-        self.ctx.set_comm(self.exchange, self.allreduce_min)
+        self.ctx.set_comm(self.exchange, self.allreduce_min, self.allreduce_max)
         return self

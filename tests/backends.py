@@ -63,19 +63,24 @@ def make(backend: abi.Backend, case):
     return ctx
 
 
-def mpi_run(backend: abi.Backend, case, nranks: int, warmup: int, steps: int, fids=None, gather: bool = True):
+def mpi_run(backend: abi.Backend, case, nranks: int, warmup: int, steps: int, fids=None, gather: bool = True,
+            procs=None, pressure_kind: int = 0):
     """Run the reference's own solver on ``case`` decomposed over ``nranks``
     MPI ranks (threads of this process through the MPI shim):
-    ``warmup`` steps, then ``steps`` timed steps.  Returns (seconds of the
-    timed steps, max over ranks; the dts of all steps; the process grid;
-    {field id: global array} of the final state when ``gather``)."""
+    ``warmup`` steps, then ``steps`` timed steps; ``procs`` fixes the process
+    grid (ranks per axis; None: MPI_Dims_create), ``pressure_kind`` the
+    semi-implicit pressure solver (0 Jacobi, 1 Gauss-Seidel).  Returns
+    (seconds of the timed steps, max over ranks; the dts of all steps; the
+    process grid; {field id: global array} of the final state when
+    ``gather``; the pressure iterations of every step)."""
     import numpy as np
     f = backend.lib.sifvr_mpi_run
     f.restype = ctypes.c_int
-    f.argtypes = [ctypes.POINTER(abi.Config), ctypes.POINTER(abi.Mesh), ctypes.c_int, ctypes.c_int,
+    f.argtypes = [ctypes.POINTER(abi.Config), ctypes.POINTER(abi.Mesh), ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                  ctypes.c_int, ctypes.c_int,
                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
                   ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
-                  ctypes.POINTER(ctypes.c_int)]
+                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     cfg, mesh, fields = case
     fids = list(fields) if fids is None else list(fids)
     init = [np.ascontiguousarray(fields[k], dtype=np.float64) for k in fids]
@@ -85,10 +90,13 @@ def mpi_run(backend: abi.Backend, case, nranks: int, warmup: int, steps: int, fi
     pout = (ctypes.c_void_p * len(fids))(*[a.ctypes.data for a in out]) if gather else None
     sec = ctypes.c_double()
     dts = (ctypes.c_double * max(warmup + steps, 1))()
+    iters = (ctypes.c_int * max(warmup + steps, 1))()
     dims = (ctypes.c_int * 3)()
+    pr = (ctypes.c_int * 3)(*procs) if procs is not None else None
     ms = mesh.cstruct()
-    st = f(ctypes.byref(cfg), ctypes.byref(ms), nranks, len(fids), ids, pin, pout, warmup, steps,
-           ctypes.byref(sec), dts, dims)
+    st = f(ctypes.byref(cfg), ctypes.byref(ms), nranks, pr, pressure_kind, len(fids), ids, pin, pout, warmup, steps,
+           ctypes.byref(sec), dts, iters, dims)
     if st != abi.OK:
         raise abi.AbiError(st, backend.error(None))
-    return sec.value, list(dts)[:warmup + steps], tuple(dims), (dict(zip(fids, out)) if gather else None)
+    return (sec.value, list(dts)[:warmup + steps], tuple(dims), (dict(zip(fids, out)) if gather else None),
+            list(iters)[:warmup + steps])

@@ -65,16 +65,19 @@ class PairExchange:
             self._sync(r, body)
             return 0
 
-        def allreduce_min(ptr, stream):
-            import torch
-            self.ptrs[r] = ptr
-            self._sync(r, lambda peer: self.tmp[r].copy_(slab._view(self.ptrs[peer], 1, True)))
-            with torch.cuda.stream(self.streams[r]):
-                v = slab._view(ptr, 1, True)
-                torch.minimum(v, self.tmp[r], out=v)
-            self.barrier.wait()   # both minima taken before either rank reuses its pointer slot
-            return 0
-        return exchange, allreduce_min
+        def reducer(op):
+            def reduce(ptr, stream):
+                import torch
+                self.ptrs[r] = ptr
+                self._sync(r, lambda peer: self.tmp[r].copy_(slab._view(self.ptrs[peer], 1, True)))
+                with torch.cuda.stream(self.streams[r]):
+                    v = slab._view(ptr, 1, True)
+                    op(v, self.tmp[r], out=v)
+                self.barrier.wait()   # both results taken before either rank reuses its pointer slot
+                return 0
+            return reduce
+        import torch
+        return exchange, reducer(torch.minimum), reducer(torch.maximum)
 
 
 CASES = {
@@ -146,8 +149,15 @@ def test_exchange_faces_need_the_hooks():
 
 
 def test_exchange_faces_reject_unsupported_configs():
-    cfg, mesh, _ = cases.acoustic3d(12)   # semi-implicit + IGR
+    cfg, mesh, _ = cases.acoustic3d(12)   # semi-implicit + IGR, mixed precision (FP32 Jacobi sweeps)
+    cfg.precision = abi.PREC_MIXED
     lmesh, _, _ = slab.slab_mesh(mesh, 3, 0, 2)
+    with pytest.raises(abi.AbiError) as e:
+        backends.cuda().create(cfg, lmesh)
+    assert e.value.status == abi.ERR_UNSUPPORTED
+    cfg, mesh, _ = cases.riemann2d(32)
+    cfg.mu = 1e-3                          # viscous fluxes
+    lmesh, _, _ = slab.slab_mesh(mesh, 2, 0, 2)
     with pytest.raises(abi.AbiError) as e:
         backends.cuda().create(cfg, lmesh)
     assert e.value.status == abi.ERR_UNSUPPORTED

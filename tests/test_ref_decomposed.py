@@ -38,7 +38,7 @@ def test_decomposed_reference_equals_single_rank(name):
     make, nranks, nsteps = CASES[name]
     single = backends.make(ref, make())
     _, _, dts1 = cases.run_steps(single, nsteps)
-    sec, dts, dims, fields = backends.mpi_run(ref, make(), nranks, 0, nsteps)
+    sec, dts, dims, fields, _ = backends.mpi_run(ref, make(), nranks, 0, nsteps)
     assert dims[0] * dims[1] * dims[2] == nranks
     assert dts == dts1
     for fid, arr in fields.items():
@@ -50,5 +50,5 @@ def test_decomposed_reference_equals_single_rank(name):
 def test_dims_create_is_balanced():
     ref = _ref()
     # 12 ranks on a 2D grid: MPI_Dims_create gives 4 x 3
-    _, _, dims, _ = backends.mpi_run(ref, cases.riemann2d(24), 12, 0, 1, gather=False)
+    _, _, dims, _, _ = backends.mpi_run(ref, cases.riemann2d(24), 12, 0, 1, gather=False)
     assert dims == (4, 3, 1)
