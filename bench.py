@@ -56,7 +56,13 @@ KERNEL_BYTES_PER_CELL_2D = {"march2d": 93.33, "dt": 32.0, "bc_prim": 0.0, "face_
 # (traffic null) instead of being applied to a different kernel.
 NCU_KERNEL_SOURCES = ("semiimplicitfv_b200/csrc/sifv_march2d.cuh", "semiimplicitfv_b200/csrc/sifv_sweep.cuh",
                       "semiimplicitfv_b200/csrc/sifv_fastmath.cuh")
-NCU_CAPTURE = {}   # (precision, kernel) -> {"sha": ..., "dram_bytes_per_cell": ..., "fp64_inst_per_cell": ...}
+# (precision, kernel) -> {"sha": ..., "dram_bytes_per_cell": ..., "fp64_inst_per_cell": ...}; from
+# profiles/march2d_fp64_2048.md and profiles/march2d_mixed_2048.md (FP64 thread operations: DADD + DMUL +
+# DFMA issued, per interior cell)
+NCU_CAPTURE = {
+    (2, "march2d"): {"sha": "d415c62de63d6e5d", "dram_bytes_per_cell": 89.56, "fp64_inst_per_cell": 874.3},
+    (1, "march2d"): {"sha": "d415c62de63d6e5d", "dram_bytes_per_cell": 94.34, "fp64_inst_per_cell": 48.2},
+}
 
 
 def _kernel_sources_sha() -> str:

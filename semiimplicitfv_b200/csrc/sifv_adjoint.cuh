@@ -27,12 +27,6 @@
 #include "sifv_common.cuh"
 #include "sifv_dual.cuh"
 
-// Resident blocks per SM asked of k_adj_face (launch bounds; 3: up to 168
-// registers per thread).
-#ifndef SIFV_ADJ_FACE_BLOCKS
-#define SIFV_ADJ_FACE_BLOCKS 3
-#endif
-
 namespace sifv {
 
 // number of primitive (rho, u.., p) and conservative variables
@@ -105,7 +99,7 @@ __device__ __forceinline__ const T& flux_comp(const FaceFlux<0, T>& Fx, int q, i
 // S: the arithmetic of the local Jacobians (double; float for the FP32
 // reverse sweep, whose shares are still stored and gathered in FP64).
 template <int DIR, int DIM, typename S>
-__global__ void __launch_bounds__(128, SIFV_ADJ_FACE_BLOCKS) k_adj_face(AdjArgs A) {
+__global__ void __launch_bounds__(128) k_adj_face(AdjArgs A) {
     constexpr int NVN = NV<DIM>::n;
     constexpr int ND = 2 * NVN;
     const Params& P = A.P;
@@ -137,57 +131,9 @@ __global__ void __launch_bounds__(128, SIFV_ADJ_FACE_BLOCKS) k_adj_face(AdjArgs 
         }
     }
     const bool weno = (P.reconOrder == SIFV_WENO5);
-    // reconstructed face values (the value part of the dual passes below is
-    // the same arithmetic, so these are the values those passes carry)
-    S WL[NVN], WR[NVN];
+    // reconstruction values and stencil gradients
+    S WL[NVN], WR[NVN], dL[NVN][5], dR[NVN][5];
 #pragma unroll
-    for (int v = 0; v < NVN; ++v) {
-        const double* f = prim_ptr(F, v, dim);
-        S s[6];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) s[q] = (S)f[base + (q - 3) * st];
-        const S e = (S)P.wenoEps;
-        WL[v] = weno ? weno5L<S>(s[0], s[1], s[2], s[3], s[4], e) : upwind5L<S>(s[0], s[1], s[2], s[3], s[4]);
-        WR[v] = weno ? weno5R<S>(s[1], s[2], s[3], s[4], s[5], e) : upwind5R<S>(s[1], s[2], s[3], s[4], s[5]);
-    }
-    // flux Jacobian w.r.t. WL, then w.r.t. WR: two passes with NVN
-    // derivative slots each instead of one with 2 NVN (every derivative
-    // component is computed by the same operations either way, so the
-    // result is the same bit for bit; half the dual width keeps the
-    // Riemann solver's intermediates in registers)
-    S gW[ND];
-#pragma unroll
-    for (int a = 0; a < ND; ++a) gW[a] = S(0);
-#pragma unroll 1
-    for (int side = 0; side < 2; ++side) {
-        using DN = Dual<NVN, S>;
-        FaceState<0, DN> L, R;
-        const bool sl = side == 0;
-        L.rho = sl ? DN::seed(WL[0], 0) : DN(WL[0]);
-        R.rho = sl ? DN(WR[0]) : DN::seed(WR[0], 0);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            L.u[d] = (d < DIM) ? (sl ? DN::seed(WL[1 + d], 1 + d) : DN(WL[1 + d])) : DN(0.0);
-            R.u[d] = (d < DIM) ? (sl ? DN(WR[1 + d]) : DN::seed(WR[1 + d], 1 + d)) : DN(0.0);
-        }
-        L.p = sl ? DN::seed(WL[DIM + 1], DIM + 1) : DN(WL[DIM + 1]);
-        R.p = sl ? DN(WR[DIM + 1]) : DN::seed(WR[DIM + 1], DIM + 1);
-        L.sigma = R.sigma = DN(0.0);
-        L.gEff = R.gEff = DN(P.gamma);
-        L.piEff = R.piEff = DN(P.pInf);
-        FaceFlux<0, DN> Fx;
-        riemann_T<DIR, DN>(P, L, R, Fx);
-#pragma unroll
-        for (int q = 0; q < NVN; ++q) {
-            const DN& fq = flux_comp(Fx, q, dim);
-#pragma unroll
-            for (int a = 0; a < NVN; ++a) gW[side * NVN + a] += mu[q] * fq.d[a];
-        }
-    }
-    // reconstruction gradients w.r.t. the stencil (Dual<5> through the
-    // reconstruction), one variable at a time, and the shares they carry
-    double* const sh = A.share[DIR];
-#pragma unroll 1
     for (int v = 0; v < NVN; ++v) {
         const double* f = prim_ptr(F, v, dim);
         S s[6];
@@ -201,12 +147,49 @@ __global__ void __launch_bounds__(128, SIFV_ADJ_FACE_BLOCKS) k_adj_face(AdjArgs 
         for (int q = 0; q < 5; ++q) x[q] = D5::seed(s[q], q);
         l = weno ? weno5L<D5>(x[0], x[1], x[2], x[3], x[4], e5) : upwind5L<D5>(x[0], x[1], x[2], x[3], x[4]);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) sh[(size_t)((0 * 5 + q) * NVN + v) * tot + t] = (double)(gW[v] * l.d[q]);
-#pragma unroll
         for (int q = 0; q < 5; ++q) x[q] = D5::seed(s[q + 1], q);
         rr = weno ? weno5R<D5>(x[0], x[1], x[2], x[3], x[4], e5) : upwind5R<D5>(x[0], x[1], x[2], x[3], x[4]);
+        WL[v] = l.v;
+        WR[v] = rr.v;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) sh[(size_t)((1 * 5 + q) * NVN + v) * tot + t] = (double)(gW[NVN + v] * rr.d[q]);
+        for (int q = 0; q < 5; ++q) {
+            dL[v][q] = l.d[q];
+            dR[v][q] = rr.d[q];
+        }
+    }
+    // flux Jacobian w.r.t. (WL, WR)
+    FaceState<0, Dual<ND, S>> L, R;
+    L.rho = Dual<ND, S>::seed(WL[0], 0);
+    R.rho = Dual<ND, S>::seed(WR[0], NVN);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        L.u[d] = (d < DIM) ? Dual<ND, S>::seed(WL[1 + d], 1 + d) : Dual<ND, S>(0.0);
+        R.u[d] = (d < DIM) ? Dual<ND, S>::seed(WR[1 + d], NVN + 1 + d) : Dual<ND, S>(0.0);
+    }
+    L.p = Dual<ND, S>::seed(WL[DIM + 1], DIM + 1);
+    R.p = Dual<ND, S>::seed(WR[DIM + 1], NVN + DIM + 1);
+    L.sigma = R.sigma = Dual<ND, S>(0.0);
+    L.gEff = R.gEff = Dual<ND, S>(P.gamma);
+    L.piEff = R.piEff = Dual<ND, S>(P.pInf);
+    FaceFlux<0, Dual<ND, S>> Fx;
+    riemann_T<DIR, Dual<ND, S>>(P, L, R, Fx);
+    S gW[ND];
+#pragma unroll
+    for (int a = 0; a < ND; ++a) gW[a] = S(0);
+#pragma unroll
+    for (int q = 0; q < NVN; ++q) {
+        const Dual<ND, S>& fq = flux_comp(Fx, q, dim);
+#pragma unroll
+        for (int a = 0; a < ND; ++a) gW[a] += mu[q] * fq.d[a];
+    }
+    double* const sh = A.share[DIR];
+#pragma unroll
+    for (int v = 0; v < NVN; ++v) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            sh[(size_t)((0 * 5 + q) * NVN + v) * tot + t] = (double)(gW[v] * dL[v][q]);
+            sh[(size_t)((1 * 5 + q) * NVN + v) * tot + t] = (double)(gW[NVN + v] * dR[v][q]);
+        }
     }
 }
 
