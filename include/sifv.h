@@ -392,11 +392,12 @@ int sifv_run_time_loop(sifv_ctx_t* ctx, const sifv_time_loop_t* params, sifv_vtk
                        sifv_progress_fn progress, void* user, sifv_loop_result_t* result);
 
 /* ---- diagnostics ----------------------------------------------------------- */
-/* Maximum relative error of the fast paths' reciprocal and square root
- * against IEEE 1/x and sqrt(x) over n arguments spread across [2^-60, 2^60)
+/* Maximum relative error of the fast paths' reciprocal, square root and
+ * reciprocal square root against IEEE 1/x, sqrt(x) and 1/sqrt(x) (the last
+ * rounded twice) over n arguments spread across [2^-60, 2^60)
  * (SIFV_PREC_FP64_FAST / SIFV_PREC_MIXED use them; SIFV_PREC_FP64 does not).
- * Returns 0 or SIFV_ERR_CUDA. */
-int sifv_fastmath_selftest(long long n, double* maxRelRcp, double* maxRelSqrt);
+ * maxRelRsqrt may be NULL.  Returns 0 or SIFV_ERR_CUDA. */
+int sifv_fastmath_selftest(long long n, double* maxRelRcp, double* maxRelSqrt, double* maxRelRsqrt);
 
 /* ---- discrete adjoint and tangent of the explicit step ------------------ */
 /* Reverse- and forward-mode derivatives of the map U(t0) -> U(tEnd) that

@@ -390,6 +390,51 @@ int igr_solve(sifv_ctx* c, int step) {
         k_igr_records<<<blocks(total, 256), 256, 0, c->stream>>>(P, c->F, c->igrRec, ntx, nty, total, slowRecs);
         c->launches++;
     }
+    // Record sweeps overlap when nothing runs between them (no halo exchange,
+    // no immersed-boundary fix-up): sweep s + 1 trails sweep s by `lag` tile
+    // planes, at least 2 (no face-adjacent tiles in one launch) and, on a
+    // periodic axis, the tiles along it (the wrap-around ghost images of
+    // sweep s are final before sweep s + 1 reads them).
+    if (rec && iters > 1 && !c->exchangeFaces && !c->ib.count) {
+        int lag = 2;
+        if (P.bc[0] == SIFV_BC_PERIODIC) lag = std::max(lag, ntx);
+        if (P.bc[2] == SIFV_BC_PERIODIC) lag = std::max(lag, nty);
+        if (P.bc[4] == SIFV_BC_PERIODIC) lag = std::max(lag, ntz);
+        lag = std::max(lag, (nplanes + kIgrMaxSlots - 1) / kIgrMaxSlots);
+        const int total = nplanes + (iters - 1) * lag;
+        bool first = true;
+        int launched = 0;
+        for (int pc = 0; pc < total; ++pc) {
+            // active sweeps: s with 0 <= pc - s lag < nplanes, a run s0 .. s0 + n - 1 (none when the
+            // lag exceeds the planes of a sweep and pc falls between two sweeps)
+            const int s0 = pc >= nplanes ? (pc - nplanes) / lag + 1 : 0, s1 = std::min(iters - 1, pc / lag);
+            if (s1 < s0) continue;
+            IgrPlanes PL{};
+            PL.top = pc - s0 * lag;
+            PL.lag = lag;
+            PL.n = s1 - s0 + 1;
+            PL.ghosts = 1;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            at[0].val.programmaticStreamSerializationAllowed = 1;
+            cudaLaunchConfig_t lc = {};
+            lc.gridDim = dim3((unsigned)(PL.n * nty * ntz));
+            lc.blockDim = dim3(kIgrTile * kIgrTile);
+            lc.dynamicSmemBytes = igr_tile_rec_smem();
+            lc.stream = c->stream;
+            lc.attrs = at;
+            lc.numAttrs = first ? 0 : 1;
+            first = false;
+            CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_igr_tile_rec, P, c->F, (const double*)c->igrRec,
+                                           (const int*)slowRecs, PL, ntx, nty, ntz));
+            ++launched;
+        }
+        c->launches += launched;
+        launch_scalar_ghosts(c, c->F.sigma);   // the full fill after the last sweep (src/IGR.cpp:155)
+        mark(c, "igr");
+        LAUNCH_CHECK(c);
+        return SIFV_OK;
+    }
     for (int it = 0; it < iters; ++it) {
         if (P.dim == 1) {
             k_igr_sweep_1d<<<1, 32, 0, c->stream>>>(P, c->F);
@@ -408,8 +453,12 @@ int igr_solve(sifv_ctx* c, int step) {
                     lc.stream = c->stream;
                     lc.attrs = at;
                     lc.numAttrs = pl > 0 ? 1 : 0;
+                    IgrPlanes PL{};
+                    PL.top = pl;
+                    PL.lag = 0;
+                    PL.n = 1;
                     CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_igr_tile_rec, P, c->F, (const double*)c->igrRec,
-                                                   (const int*)slowRecs, pl, ntx, nty));
+                                                   (const int*)slowRecs, PL, ntx, nty, ntz));
                 } else if (d3)
                     k_igr_tile<T3, T3, T3><<<(unsigned)(nty * ntz), T3 * T3, smem, c->stream>>>(P, c->F, pl, ntx, nty);
                 else

@@ -153,7 +153,7 @@ namespace {
 // [-60, 60); maxima folded with atomicMax on the bit patterns
 __global__ void k_fastmath_check(long long n, unsigned long long* out) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double eR = 0.0, eS = 0.0;
+    double eR = 0.0, eS = 0.0, eQ = 0.0;
     if (t < n) {
         unsigned long long h = (unsigned long long)t * 0x9E3779B97F4A7C15ull;
         h ^= h >> 29;
@@ -164,12 +164,15 @@ __global__ void k_fastmath_check(long long n, unsigned long long* out) {
         const double x = ldexp(m, e);
         const double r0 = 1.0 / x, r1 = frcp(x);
         const double s0 = sqrt(x), s1 = fsqrt_pos(x);
+        const double q0 = 1.0 / sqrt(x), q1 = frsqrt_pos(x);   // q0 carries two roundings
         eR = fabs(r1 - r0) / r0;
         eS = fabs(s1 - s0) / s0;
+        eQ = fabs(q1 - q0) / q0;
         atomicAdd(&out[2], 1ull);
     }
     atomicMax(&out[0], (unsigned long long)__double_as_longlong(eR));
     atomicMax(&out[1], (unsigned long long)__double_as_longlong(eS));
+    atomicMax(&out[3], (unsigned long long)__double_as_longlong(eQ));
 }
 
 }  // namespace
@@ -241,18 +244,19 @@ extern "C" int sifv_fp64_peak_probe(int reps, double* tflops) {
     return 0;
 }
 
-extern "C" int sifv_fastmath_selftest(long long n, double* maxRelRcp, double* maxRelSqrt) {
+extern "C" int sifv_fastmath_selftest(long long n, double* maxRelRcp, double* maxRelSqrt, double* maxRelRsqrt) {
     if (n <= 0 || !maxRelRcp || !maxRelSqrt) return -2;
     unsigned long long* d = nullptr;
-    if (cudaMalloc(&d, 3 * sizeof(unsigned long long)) != cudaSuccess) return -3;
-    cudaMemset(d, 0, 3 * sizeof(unsigned long long));
+    if (cudaMalloc(&d, 4 * sizeof(unsigned long long)) != cudaSuccess) return -3;
+    cudaMemset(d, 0, 4 * sizeof(unsigned long long));
     sifv::k_fastmath_check<<<(unsigned)((n + 255) / 256), 256>>>(n, d);
     cudaError_t e = cudaGetLastError();
-    unsigned long long h[3] = {0, 0, 0};
+    unsigned long long h[4] = {0, 0, 0, 0};
     if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
     cudaFree(d);
     if (e != cudaSuccess || h[2] != (unsigned long long)n) return -3;   // every argument checked
     std::memcpy(maxRelRcp, &h[0], sizeof(double));
     std::memcpy(maxRelSqrt, &h[1], sizeof(double));
+    if (maxRelRsqrt) std::memcpy(maxRelRsqrt, &h[3], sizeof(double));
     return 0;
 }

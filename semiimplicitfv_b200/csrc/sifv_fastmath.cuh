@@ -9,20 +9,21 @@
 namespace sifv {
 
 // Fast reciprocal and square root of the fast / mixed paths.  FP64: the
-// hardware approximation (rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64)
-// refined by Newton-Raphson iterations, y <- y + y (1 - x y) for 1/x and
-// y <- y + (y / 2)(1 - x y^2) for 1/sqrt(x) (each iteration squares the
-// relative error), and sqrt(x) = x * (1 / sqrt(x)) with one correction
-// s <- s + (x - s^2) y / 2; within 1 ulp of the IEEE results (checked
-// against them by sifv_fastmath_selftest).  FP32: the single-instruction
-// approximations (about 1 ulp).  The reference-ordered path never uses these.
+// hardware approximation (rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64, about
+// 2^-20 relative error, measured) refined by one third-order step: with
+// e = 1 - x y, 1/x = y / (1 - e) = y (1 + e + e^2) + O(e^3); with
+// e = 1 - x y^2, 1/sqrt(x) = y (1 - e)^(-1/2) = y (1 + e/2 + 3 e^2 / 8) + O(e^3),
+// O(e^3) ~ 2^-60, below half an ulp (one step where two Newton-Raphson steps
+// y <- y + y e took four fused operations); sqrt(x) = x * (1 / sqrt(x))
+// with one correction s <- s + (x - s^2) y / 2.  Within 1 ulp of the IEEE
+// results (checked against them by sifv_fastmath_selftest).  FP32: the
+// single-instruction approximations (about 1 ulp).  The reference-ordered
+// path never uses these.
 __device__ __forceinline__ double frcp(double x) {
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    double e = fma(-x, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-x, y, 1.0);
-    return fma(y, e, y);
+    const double e = fma(-x, y, 1.0);
+    return fma(y, fma(e, e, e), y);
 }
 __device__ __forceinline__ float frcp(float x) {
     float y;
@@ -33,10 +34,8 @@ __device__ __forceinline__ float frcp(float x) {
 __device__ __forceinline__ double fsqrt_pos(double x) {
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    double e = fma(-x * y, y, 1.0);
-    y = fma(0.5 * y, e, y);
-    e = fma(-x * y, y, 1.0);
-    y = fma(0.5 * y, e, y);
+    const double e = fma(-x * y, y, 1.0);
+    y = fma(y, e * fma(e, 0.375, 0.5), y);
     double sq = x * y;
     double r = fma(-sq, sq, x);
     return fma(r, 0.5 * y, sq);
@@ -48,16 +47,14 @@ __device__ __forceinline__ float fsqrt_pos(float x) {
 }
 
 // 1 / sqrt(x) of a positive normal argument: the hardware approximation
-// refined by two Newton-Raphson iterations (FP64; within 1 ulp of IEEE
+// refined by the third-order step above (FP64; within 1 ulp of IEEE
 // 1 / sqrt(x), checked by sifv_fastmath_selftest), the single-instruction
 // approximation in FP32.
 __device__ __forceinline__ double frsqrt_pos(double x) {
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    double e = fma(-x * y, y, 1.0);
-    y = fma(0.5 * y, e, y);
-    e = fma(-x * y, y, 1.0);
-    return fma(0.5 * y, e, y);
+    const double e = fma(-x * y, y, 1.0);
+    return fma(y, e * fma(e, 0.375, 0.5), y);
 }
 __device__ __forceinline__ float frsqrt_pos(float x) {
     float y;

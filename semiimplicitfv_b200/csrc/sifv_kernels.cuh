@@ -1783,6 +1783,7 @@ constexpr int kIgrRecDoubles = 8;
 #define SIFV_IGR_PREFETCH 2
 #endif
 constexpr int kIgrPrefetch = SIFV_IGR_PREFETCH;  // records in flight ahead of the cell being updated
+constexpr int kIgrMaxSlots = 8;                  // sweeps overlapping in one launch of k_igr_tile_rec
 constexpr int kIgrRing = kIgrPrefetch + 2;       // ring slots per thread
 
 __host__ __device__ __forceinline__ size_t igr_rec_index(long long tile, int tb, int tc, int n) {
@@ -1862,9 +1863,80 @@ __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.w
 //    read sigma only after it has completed.
 // Thread (tb, tc) owns the x-line (., tb, tc) of the tile and updates its
 // cell a = q - tb - tc at cell plane q.
+//
+// Consecutive sweeps overlap (IgrPlanes): sweep s + 1 runs its tile plane p
+// in the launch that runs sweep s's plane p + lag.  A tile reads its
+// upstream face neighbours (plane p - 1, same sweep, earlier launches) and
+// its downstream ones (plane p + 1 of the previous sweep: complete, and not
+// yet reached by this sweep), as the lexicographic order asks.  The scalar
+// ghost fill between sweeps is done by the boundary tiles at their end
+// (ghosts = 1): a tile on the low face of a zero-gradient axis copies its
+// first layer into the ghost layer, a tile on the high face its last layer;
+// on a periodic axis the high tile writes both images (its own last layer
+// below the low face, the low tile's first layer above the high face; with
+// lag >= tiles along the axis the low tile holds this sweep's final values
+// and the next sweep has not reached it).  Only the ghost layer next to the
+// face is written (the 7-point stencil reads no other); the full fill runs
+// after the last sweep.
+struct IgrPlanes {
+    int top;      // tile plane of the first active sweep; sweep slot u runs plane top - u lag
+    int lag;      // planes between consecutive sweeps
+    int n;        // active sweeps (blocks: n x nty x ntz)
+    int ghosts;   // boundary tiles refresh the scalar ghosts
+};
+__device__ __forceinline__ void igr_tile_ghosts(const Params& P, double* sigma, int I, int J, int K, int ntx,
+                                                int nty, int ntz, int i0, int j0, int k0, int ex, int ey, int ez) {
+    const int tid = (int)threadIdx.x;
+    const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+    // x faces: one thread per (y, z) of the tile
+    {
+        const int b = tid % kIgrTile, c = tid / kIgrTile;
+        if (b < ey && c < ez) {
+            const size_t row = cidx(P, 0, j0 + b, k0 + c);
+            const bool per = P.bc[0] == SIFV_BC_PERIODIC;
+            if (!per && I == 0 && P.bc[0] != SIFV_BC_EXCHANGE) sigma[row - 1] = sigma[row];
+            if (!per && I == ntx - 1 && P.bc[1] != SIFV_BC_EXCHANGE) sigma[row + P.nx] = sigma[row + P.nx - 1];
+            if (per && I == ntx - 1) {
+                sigma[row - 1] = sigma[row + P.nx - 1];
+                sigma[row + P.nx] = sigma[row];
+            }
+        }
+    }
+    // y faces: one thread per (x, z)
+    {
+        const int a = tid % kIgrTile, c = tid / kIgrTile;
+        if (a < ex && c < ez) {
+            const size_t col = cidx(P, i0 + a, 0, k0 + c);
+            const bool per = P.bc[2] == SIFV_BC_PERIODIC;
+            const size_t hi = (size_t)P.ny * sy;
+            if (!per && J == 0 && P.bc[2] != SIFV_BC_EXCHANGE) sigma[col - sy] = sigma[col];
+            if (!per && J == nty - 1 && P.bc[3] != SIFV_BC_EXCHANGE) sigma[col + hi] = sigma[col + hi - sy];
+            if (per && J == nty - 1) {
+                sigma[col - sy] = sigma[col + hi - sy];
+                sigma[col + hi] = sigma[col];
+            }
+        }
+    }
+    // z faces: one thread per (x, y)
+    {
+        const int a = tid % kIgrTile, b = tid / kIgrTile;
+        if (a < ex && b < ey) {
+            const size_t col = cidx(P, i0 + a, j0 + b, 0);
+            const bool per = P.bc[4] == SIFV_BC_PERIODIC;
+            const size_t hi = (size_t)P.nz * sz;
+            if (!per && K == 0 && P.bc[4] != SIFV_BC_EXCHANGE) sigma[col - sz] = sigma[col];
+            if (!per && K == ntz - 1 && P.bc[5] != SIFV_BC_EXCHANGE) sigma[col + hi] = sigma[col + hi - sz];
+            if (per && K == ntz - 1) {
+                sigma[col - sz] = sigma[col + hi - sz];
+                sigma[col + hi] = sigma[col];
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256, 1)
-    k_igr_tile_rec(Params P, Fields F, const double* __restrict__ rec, const int* __restrict__ slowRecs, int plane,
-                   int ntx, int nty) {
+    k_igr_tile_rec(Params P, Fields F, const double* __restrict__ rec, const int* __restrict__ slowRecs,
+                   IgrPlanes PL, int ntx, int nty, int ntz) {
     constexpr int T = kIgrTile, HXP = 20, HY = T + 2, HZ = T + 2, HN = HXP * HY * HZ;
     constexpr int NT = T * T, D = kIgrPrefetch, R = kIgrRing;
     extern __shared__ __align__(16) double smem[];
@@ -1872,8 +1944,11 @@ __global__ void __launch_bounds__(256, 1)
     double* sR = smem + HN;
     double2* ring = reinterpret_cast<double2*>(smem + 2 * HN);   // [R][4 chunks][NT threads]
     double* sAx = smem + 2 * HN + R * kIgrRecDoubles * NT;
-    const int J = (int)(blockIdx.x % (unsigned)nty), K = (int)(blockIdx.x / (unsigned)nty);
-    const int I = plane - J - K;
+    const unsigned perSlot = (unsigned)(nty * ntz);
+    const int slot = (int)(blockIdx.x / perSlot);
+    const unsigned bt = blockIdx.x % perSlot;
+    const int J = (int)(bt % (unsigned)nty), K = (int)(bt / (unsigned)nty);
+    const int I = PL.top - slot * PL.lag - J - K;
     if (I < 0 || I >= ntx) return;
     const int tid = (int)threadIdx.x;
     const int i0 = I * T, j0 = J * T, k0 = K * T;
@@ -1963,6 +2038,7 @@ __global__ void __launch_bounds__(256, 1)
         }
         __syncthreads();
     }
+    if (PL.ghosts) igr_tile_ghosts(P, F.sigma, I, J, K, ntx, nty, ntz, i0, j0, k0, ex, ey, ez);
 }
 
 // ---------------------------------------------------------------------------

@@ -158,17 +158,19 @@ def test_mixed_riemann2d_error_within_bound():
 
 
 def test_fast_reciprocal_and_sqrt_within_one_ulp():
-    """The fast paths' Newton-refined reciprocal and square root against
-    IEEE 1/x and sqrt(x) on 2^22 arguments across [2^-60, 2^60)."""
+    """The fast paths' refined reciprocal, square root and reciprocal square
+    root against IEEE 1/x, sqrt(x) and 1/sqrt(x) on 2^22 arguments across
+    [2^-60, 2^60): within one ulp (2^-52 relative; the reference 1/sqrt(x)
+    is itself rounded twice, so that bound gets half an ulp more)."""
     import ctypes
     from semiimplicitfv_b200 import _lib
     lib = _lib.load()
-    lib.sifv_fastmath_selftest.argtypes = [ctypes.c_longlong, ctypes.POINTER(ctypes.c_double),
-                                           ctypes.POINTER(ctypes.c_double)]
-    r, s = ctypes.c_double(), ctypes.c_double()
-    assert lib.sifv_fastmath_selftest(1 << 22, ctypes.byref(r), ctypes.byref(s)) == 0
+    lib.sifv_fastmath_selftest.argtypes = [ctypes.c_longlong] + [ctypes.POINTER(ctypes.c_double)] * 3
+    r, s, q = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    assert lib.sifv_fastmath_selftest(1 << 22, ctypes.byref(r), ctypes.byref(s), ctypes.byref(q)) == 0
     assert r.value <= 2.23e-16, r.value
     assert s.value <= 2.23e-16, s.value
+    assert q.value <= 3.34e-16, q.value
 
 
 @pytest.mark.parametrize("prec", [abi.PREC_FP64_FAST, abi.PREC_MIXED])

@@ -108,6 +108,21 @@ def test_igr_record_sweep_3d(nx, ny, nz):
     check(cases.acoustic_box(nx, ny, nz, bc=abi.BC_SLIPWALL, stretch=0.01), 2)
 
 
+@pytest.mark.parametrize("shape,bcs", [((40, 36, 34), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_SLIPWALL)),
+                                        ((34, 20, 50), (abi.BC_OUTFLOW, abi.BC_SYMMETRY, abi.BC_PERIODIC)),
+                                        ((50, 40, 18), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_NOSLIPWALL))])
+def test_igr_overlapped_sweeps_mixed_faces(shape, bcs):
+    """Consecutive record sweeps overlapped in one launch sequence (sweep s + 1
+    trailing sweep s by a fixed number of tile planes, boundary tiles
+    refreshing the ghost layer themselves), per-axis boundary kinds (periodic
+    wrap images and zero-gradient copies), several tiles along the periodic
+    axes, ragged edges, the 20-sweep warm start: bit-identical to the
+    oracle's sweep-by-sweep order."""
+    cfg, mesh, fields = cases.acoustic_box(*shape)
+    mesh.bc = [bcs[0]] * 2 + [bcs[1]] * 2 + [bcs[2]] * 2
+    check((cfg, mesh, fields), 2)
+
+
 @pytest.mark.parametrize("bc", [abi.BC_PERIODIC, abi.BC_OUTFLOW])
 def test_igr_tiled_wavefront_2d_ragged(bc):
     """Several 32 x 64 IGR tiles with ragged edges (100 x 140 cells)."""
