@@ -60,8 +60,8 @@ NCU_KERNEL_SOURCES = ("semiimplicitfv_b200/csrc/sifv_march2d.cuh", "semiimplicit
 # profiles/march2d_fp64_2048.md and profiles/march2d_mixed_2048.md (FP64 thread operations: DADD + DMUL +
 # DFMA issued, per interior cell)
 NCU_CAPTURE = {
-    (2, "march2d"): {"sha": "d415c62de63d6e5d", "dram_bytes_per_cell": 89.56, "fp64_inst_per_cell": 874.3},
-    (1, "march2d"): {"sha": "d415c62de63d6e5d", "dram_bytes_per_cell": 94.34, "fp64_inst_per_cell": 48.2},
+    (2, "march2d"): {"sha": "32a04e8cb0599297", "dram_bytes_per_cell": 89.50, "fp64_inst_per_cell": 838.1},
+    (1, "march2d"): {"sha": "32a04e8cb0599297", "dram_bytes_per_cell": 94.32, "fp64_inst_per_cell": 46.4},
 }
 
 

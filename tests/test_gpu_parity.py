@@ -175,6 +175,28 @@ def test_standalone_pressure_solve_dt_and_igr():
     assert np.array_equal(cg.get_field(abi.F_SIGMA), co.get_field(abi.F_SIGMA))
 
 
+@pytest.mark.parametrize("bc", [abi.BC_PERIODIC, abi.BC_SLIPWALL, abi.BC_OUTFLOW])
+@pytest.mark.parametrize("max_iter,dt,tol", [(7, 2e-3, 1e-14), (8, 2e-3, 1e-14), (200, 2e-3, 1e-8),
+                                             (200, 1e-2, 1e-8), (200, 1e-2, 1e-7)])
+def test_jacobi_3d_uniform_axes(bc, max_iter, dt, tol):
+    """3D Jacobi on axes of equal cell widths (per-face coefficients,
+    k_jacobi3<true>, ragged 32 x 8 column tiles and 16-cell z segments):
+    iteration counts -- odd and even caps, convergence after an odd or an
+    even number of iterations, several host batches -- and the iterate are
+    the oracle's bit for bit."""
+    cfg, mesh, fields = cases.acoustic_box(40, 20, 37, bc=bc)
+    mesh.x, mesh.y, mesh.z = np.arange(41) / 64.0, np.arange(21) / 64.0, np.arange(38) / 64.0   # equal widths
+    cg = backends.make(backends.cuda(), (cfg, mesh, fields))
+    co = backends.make(backends.oracle(), (cfg, mesh, fields))
+    rng = np.random.default_rng(max_iter + bc)
+    n = cg.ncells
+    args = (1.0 + 0.1 * rng.random(n), 1.4 + 0.2 * rng.random(n), rng.random(n), rng.random(n))
+    pg, ig, _ = cg.pressure_solve(*args, dt, tol, max_iter)
+    po, io, _ = co.pressure_solve(*args, dt, tol, max_iter)
+    assert ig == io, (ig, io)
+    assert np.array_equal(cg.interior(pg), co.interior(po))
+
+
 @pytest.mark.parametrize("plant", ["sigma", "rho"])
 def test_igr_record_sweep_fallbacks(plant):
     """The record sweep's exact-quotient guards: planted -0, tiny and huge
