@@ -81,6 +81,8 @@ struct sifv_ctx {
     bool igrTileReady = false;
     double* igrRec = nullptr;                 // IGR sweep records (k_igr_records), then one int flag
     double* gsRec = nullptr;                  // Gauss-Seidel sweep records (k_gs_records), then one int flag
+    double* gsBuf[3] = {nullptr, nullptr, nullptr};   // iterates 2-4 (mod 5) of the overlapped Gauss-Seidel sweeps
+    int gsPrevIters = 0;                      // iterations of the previous Gauss-Seidel solve (first batch size)
     double* jacCoef = nullptr;                // Jacobi coefficients: per face (dim arrays) or per cell (2 dim + 2)
     bool uniformAxes = false;                 // interior cell widths bitwise equal along every active axis
     int pressureKind = 0;                     // 0 Jacobi (default), 1 Gauss-Seidel
@@ -322,7 +324,7 @@ void launch_bc_prim(sifv_ctx* c) {
 }
 
 void launch_scalar_ghosts(sifv_ctx* c, double* f) {
-    k_scalar_ghosts<<<blocks((long long)c->ncells, kCellThreads), kCellThreads, 0, c->stream>>>(c->P, f);
+    k_scalar_ghosts<<<blocks(ghost_count(c->P), kCellThreads), kCellThreads, 0, c->stream>>>(c->P, f);
     c->launches++;
 }
 
@@ -620,6 +622,86 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
                                                                  total, slowRecs);
         c->launches++;
     }
+    if (recs && !c->exchangeFaces && maxIter >= 2) {
+        // overlapped iterations (k_gs_tile_rec_ov): iterate n in buf[n % kGsBufs]
+        if (!c->gsBuf[0]) {
+            int sa = SIFV_OK;
+            for (int q = 0; q < kGsBufs - 2; ++q) c->gsBuf[q] = dalloc(c, c->ncells, sa);
+            if (sa != SIFV_OK) return sa;
+            CUDA_TRY(c, cudaFuncSetAttribute(k_gs_tile_rec_ov, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)gs_tile_rec_smem()));
+        }
+        GsBufs B{};
+        B.b[0] = c->F.pA;
+        B.b[1] = c->F.pB;
+        for (int q = 0; q < kGsBufs - 2; ++q) B.b[q + 2] = c->gsBuf[q];
+        int lag = 2;
+        if (P.bc[0] == SIFV_BC_PERIODIC) lag = std::max(lag, ntx);
+        if (P.bc[2] == SIFV_BC_PERIODIC) lag = std::max(lag, nty);
+        if (P.bc[4] == SIFV_BC_PERIODIC) lag = std::max(lag, ntz);
+        lag = std::max(lag, (nplanes + 2) / 3);   // at most three iterations in flight
+        const int S = (nplanes + lag - 1) / lag;
+        // the ghost layers the first iteration reads: iterate 0's images in buf 0 and buf 1
+        const unsigned gg = blocks(ghost_count(P), kCellThreads);
+        k_scalar_ghosts<<<gg, kCellThreads, 0, c->stream>>>(P, B.b[0]);
+        k_scalar_ghosts_from<<<gg, kCellThreads, 0, c->stream>>>(P, B.b[0], B.b[1]);
+        c->launches += 2;
+        const int total = nplanes + (maxIter - 1) * lag;
+        const int guess = std::max(2, c->gsPrevIters > 4 ? (3 * c->gsPrevIters) / 4 : 4);
+        int pc = 0, chunk = nplanes + (guess - 1) * lag, done = 0;
+        bool first = true;
+        while (pc < total && !done) {
+            const int end = std::min(total, pc + chunk);
+            for (; pc < end; ++pc) {
+                const int s0 = pc >= nplanes ? (pc - nplanes) / lag + 1 : 0, s1 = std::min(maxIter - 1, pc / lag);
+                if (s1 < s0) continue;
+                GsPlanes PL{};
+                PL.top = pc - s0 * lag;
+                PL.lag = lag;
+                PL.n = s1 - s0 + 1;
+                PL.it0 = s0;
+                PL.S = S;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                at[0].val.programmaticStreamSerializationAllowed = 1;
+                cudaLaunchConfig_t lc = {};
+                lc.gridDim = dim3((unsigned)(PL.n * nty * ntz));
+                lc.blockDim = dim3(kIgrTile * kIgrTile);
+                lc.dynamicSmemBytes = gs_tile_rec_smem();
+                lc.stream = c->stream;
+                lc.attrs = at;
+                lc.numAttrs = first ? 0 : 1;
+                first = false;
+                CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_gs_tile_rec_ov, P, (const double*)c->gsRec,
+                                               (const int*)slowRecs, B, c->ctl, tol, PL, ntx, nty, ntz));
+                c->launches++;
+            }
+            LAUNCH_CHECK(c);
+            // iterations complete after launch pc - 1: j lag + nplanes - 1 <= pc - 1
+            const int complete = std::min(maxIter, pc >= nplanes ? (pc - nplanes) / lag + 1 : 0);
+            CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl,
+                                        sizeof(Ctl) + sizeof(unsigned long long) * (size_t)std::max(complete, 1),
+                                        cudaMemcpyDeviceToHost, c->stream));
+            CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+            for (int j = 0; j < complete; ++j) {
+                double r;
+                std::memcpy(&r, &c->ctlHost->res[j], sizeof(double));
+                if (r < tol) {
+                    done = j + 1;
+                    break;
+                }
+            }
+            chunk = std::min(2 * chunk, 16 * lag + nplanes);
+        }
+        iters = done ? done : maxIter;
+        c->gsPrevIters = iters;
+        // the result's ghosts as the reference leaves them: filled from the iterate before the last sweep
+        k_scalar_ghosts_from<<<gg, kCellThreads, 0, c->stream>>>(P, B.b[(iters - 1) % kGsBufs], B.b[iters % kGsBufs]);
+        c->launches++;
+        result = B.b[iters % kGsBufs];
+        mark(c, "gauss_seidel");
+        return SIFV_OK;
+    }
     int it = 0, batch = 2, done = 0;
     while (it < maxIter) {
         int nb = std::min(batch, maxIter - it);
@@ -628,8 +710,7 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
                 int st = exchange_scalar(c, pp);
                 if (st != SIFV_OK) return st;
             }
-            k_gs_ghosts<<<blocks((long long)c->ncells, kCellThreads), kCellThreads, 0, c->stream>>>(P, pp, c->ctl, it,
-                                                                                                     tol);
+            k_gs_ghosts<<<blocks(ghost_count(P), kCellThreads), kCellThreads, 0, c->stream>>>(P, pp, c->ctl, it, tol);
             if (recs) {
                 for (int pl = 0; pl < nplanes; ++pl) {
                     // planes after the first overlap their record prologue with the previous plane
@@ -1796,8 +1877,8 @@ int sifv_pressure_solve(sifv_ctx_t* c, const double* rho, const double* rhoc2, c
     const double* res = nullptr;
     int st = pressure_run(c, dRho, dRhoc2, dRhs, tol, maxIter, n, res);
     if (st != SIFV_OK) return st;
-    if (c->lastInPlace)   // in place on pA; the ghosts keep their last fill, as the reference's array
-        CUDA_TRY(c, cudaMemcpyAsync(dP, c->F.pA, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->lastInPlace)   // the whole array (ghosts as the reference's array leaves them)
+        CUDA_TRY(c, cudaMemcpyAsync(dP, res, bytes, cudaMemcpyDeviceToDevice, c->stream));
     else
         k_jacobi_finish<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(
             c->P, c->F.pA, c->F.pB, dP, c->ctl, maxIter);

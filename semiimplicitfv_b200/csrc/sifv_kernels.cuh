@@ -87,12 +87,12 @@ __global__ void k_bc_prim(Params P, Fields F) {
     }
 }
 
-// Scalar ghost fill (RectilinearMesh::fillScalarGhosts, src/RectilinearMesh.cpp:424-492).
+// Scalar ghost fill (RectilinearMesh::fillScalarGhosts, src/RectilinearMesh.cpp:424-492),
+// one thread per ghost cell (ghost_count threads).
 __global__ void k_scalar_ghosts(Params P, double* __restrict__ f) {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
-    if (!ext_coords(P, t, i, j, k)) return;
-    if (is_interior(P, i, j, k)) return;
+    if (t >= ghost_count(P) || !ghost_coords(P, t, i, j, k)) return;
     f[cidx(P, i, j, k)] = f[scalar_idx(P, i, j, k)];
 }
 
@@ -2063,10 +2063,9 @@ __device__ __forceinline__ bool gs_converged(Ctl* ctl, int it, double tol) {
 
 __global__ void k_gs_ghosts(Params P, double* __restrict__ f, Ctl* ctl, int it, double tol) {
     if (gs_converged(ctl, it, tol)) return;
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // one thread per ghost cell
     int i, j, k;
-    if (!ext_coords(P, t, i, j, k)) return;
-    if (is_interior(P, i, j, k)) return;
+    if (t >= ghost_count(P) || !ghost_coords(P, t, i, j, k)) return;
     f[cidx(P, i, j, k)] = f[scalar_idx(P, i, j, k)];
 }
 
@@ -2307,6 +2306,205 @@ __global__ void __launch_bounds__(256, 1) k_gs_tile_rec(Params P, const double* 
         __syncthreads();
     }
     block_max_to(maxRes, &ctl->res[it]);
+}
+
+// Gauss-Seidel iterations overlapped (3D record sweep, no halo exchange):
+// several iterations in one launch sequence, iteration m + 1 trailing
+// iteration m by `lag` tile planes, as the IGR sweeps (k_igr_tile_rec).  A
+// Gauss-Seidel iteration stops on its residual, so the iterations after
+// the current one run speculatively and must not destroy an iterate that
+// turns out to be the answer: iterate n (n = 0 the initial guess) lives in
+// buf[n % kGsBufs], and the iteration producing iterate n + 1 stages its
+// tile and its downstream face halos (x+, y+, z+) from iterate n and its
+// upstream face halos (x-, y-, z-: upstream tiles of the same iteration,
+// earlier launches) from its own buffer -- in-place Gauss-Seidel's operands
+// bit for bit.  Ghost layers (the reference fills them from iterate n
+// before the sweep): boundary tiles write, at their end, the images of
+// their new values -- the low-side ghost layer into the next iteration's
+// buffer, the high-side one into their own (read as downstream halo by the
+// next iteration); periodic images need lag >= tiles along the axis, as
+// for IGR.  With at most S iterations in flight (S = ceil(planes / lag) <=
+// 3), the residuals of iterations m - S and earlier are complete when
+// iteration m starts; its tiles skip when one of them is below tol, so at
+// most S - 1 iterations run past the converged one and never reach its
+// buffer or its predecessor's (five buffers).
+constexpr int kGsBufs = 5;
+struct GsBufs {
+    double* b[kGsBufs];
+};
+struct GsPlanes {
+    int top;   // tile plane of the first active iteration (slot 0); slot u runs plane top - u lag
+    int lag;
+    int n;     // active iterations in this launch
+    int it0;   // index of the iteration in slot 0
+    int S;     // iterations in flight at most
+};
+__global__ void __launch_bounds__(256, 1) k_gs_tile_rec_ov(Params P, const double* __restrict__ rec,
+                                                           const int* __restrict__ slowRecs, GsBufs B, Ctl* ctl,
+                                                           double tol, GsPlanes PL, int ntx, int nty, int ntz) {
+    constexpr int T = kIgrTile, HXP = 20, HY = T + 2, HN = HXP * HY * (T + 2);
+    constexpr int NT = T * T, D = kIgrPrefetch, R = kIgrRing, CH = kGsRecChunks;
+    extern __shared__ __align__(16) double smem[];
+    double* sP = smem;
+    double2* ring = reinterpret_cast<double2*>(smem + HN);   // [R][CH chunks][NT threads]
+    __shared__ int skip;
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+    const unsigned perSlot = (unsigned)(nty * ntz);
+    const int slot = (int)(blockIdx.x / perSlot);
+    const unsigned bt = blockIdx.x % perSlot;
+    const int J = (int)(bt % (unsigned)nty), K = (int)(bt / (unsigned)nty);
+    const int I = PL.top - slot * PL.lag - J - K;
+    if (I < 0 || I >= ntx) return;
+    const int it = PL.it0 + slot;                    // this tile's iteration: iterate it -> it + 1
+    const double* __restrict__ pOld = B.b[it % kGsBufs];
+    double* __restrict__ pNew = B.b[(it + 1) % kGsBufs];
+    const int tid = (int)threadIdx.x;
+    const int i0 = I * T, j0 = J * T, k0 = K * T;
+    const int ex = min(T, P.nx - i0), ey = min(T, P.ny - j0), ez = min(T, P.nz - k0);
+    const int hy = ey + 2, hz = ez + 2;
+    const int xg = i0 - 1 + P.ngx;
+    const int xs = xg & ~1;
+    const int xoff = xg - xs;
+    const int tb = tid % T, tc = tid / T;
+    const bool act = tb < ey && tc < ez;
+    const long long tile = (long long)I + (long long)ntx * (J + (long long)nty * K);
+    const double2* lineRec = reinterpret_cast<const double2*>(rec) + gs_rec_index(tile, 0, tc, 0);
+    auto issue = [&](int n) {
+        if (act && n >= 0 && n < ex) {
+            double2* dst = ring + (size_t)(n % R) * CH * NT + tid;
+            const double2* src = lineRec + (size_t)((tb + n) % T) * CH * T + tb;
+#pragma unroll
+            for (int ch = 0; ch < CH; ++ch) cp_async16(dst + ch * NT, src + ch * T);
+        }
+        cp_async_commit();
+    };
+    for (int q = -D; q < 0; ++q) issue(q - tb - tc + D);
+    const int hLine = ((tc + 1) * HY + (tb + 1)) * HXP + 1 + xoff;
+    const size_t gLine = cidx(P, i0, j0 + tb, k0 + tc);
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");   // the previous tile planes
+    if (tid == 0) {   // the first converged iteration among those complete before this one started
+        int s = 0;
+        for (int j = 0; j <= it - PL.S; ++j)
+            if (bits2d(ctl->res[j]) < tol) { s = 1; break; }
+        skip = s;
+    }
+    __syncthreads();
+    if (skip) {
+        cp_async_wait_group<0>();
+        return;
+    }
+    const bool fastRecs = *slowRecs == 0;
+    // tile and downstream halos from iterate it (the whole box; the upstream faces are replaced below)
+    for (int w = tid; w < hy * hz * (HXP / 2); w += NT) {
+        const int m = w % (HXP / 2), row = w / (HXP / 2);
+        const int b = row % hy, c = row / hy;
+        const int x = xs + 2 * m;
+        if (x + 1 < P.nxT) {
+            const size_t g = (size_t)x + (size_t)P.nxT * ((size_t)(j0 + b - 1 + P.ngy) +
+                                                          (size_t)P.nyT * (size_t)(k0 + c - 1 + P.ngz));
+            cp_async16(&sP[(c * HY + b) * HXP + 2 * m], &pOld[g]);
+        }
+    }
+    cp_async_commit();
+    cp_async_wait_group<0>();
+    __syncthreads();
+    {   // upstream face halos from iterate it + 1 (this iteration's upstream tiles / ghost images)
+        const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+        if (act) {   // x- face: (i0 - 1, j0 + tb, k0 + tc)
+            sP[((tc + 1) * HY + (tb + 1)) * HXP + xoff] = pNew[gLine - 1];
+        }
+        {   // y- face: (i0 + a, j0 - 1, k0 + c)
+            const int a = tid % T, c = tid / T;
+            if (a < ex && c < ez)
+                sP[((c + 1) * HY + 0) * HXP + 1 + xoff + a] = pNew[cidx(P, i0 + a, j0, k0 + c) - sy];
+        }
+        {   // z- face: (i0 + a, j0 + b, k0 - 1)
+            const int a = tid % T, b = tid / T;
+            if (a < ex && b < ey)
+                sP[(0 * HY + (b + 1)) * HXP + 1 + xoff + a] = pNew[cidx(P, i0 + a, j0 + b, k0) - sz];
+        }
+    }
+    __syncthreads();
+    double maxRes = 0.0;
+    const int nq = ex + ey + ez - 2;
+    for (int q = 0; q < nq; ++q) {
+        const int a = q - tb - tc;
+        issue(a + D);
+        cp_async_wait_group<D>();
+        if (act && a >= 0 && a < ex) {
+            const double2* ra = ring + (size_t)(a % R) * CH * NT + tid;
+            const double2 c0 = ra[0], c1 = ra[NT], c2 = ra[2 * NT], c3 = ra[3 * NT], c4 = ra[4 * NT];
+            const int h = hLine + a;
+            double od = 0.0;
+            od += c0.x * sP[h - 1] + c0.y * sP[h + 1];
+            od += c1.x * sP[h - HXP] + c1.y * sP[h + HXP];
+            od += c2.x * sP[h - HXP * HY] + c2.y * sP[h + HXP * HY];
+            const double num = c4.y + c3.x * od;
+            const double pn = (fastRecs && igr_fast_operand(num)) ? div_markstein(num, c3.y, c4.x)
+                                                                  : div_rn_plain(num, c3.y);
+            const double po = sP[h];
+            sP[h] = pn;
+            pNew[gLine + a] = pn;
+            maxRes = smax(maxRes, fabs(pn - po));
+        }
+        __syncthreads();
+    }
+    // ghost images of the new values: low side into the next iteration's buffer, high side into this one
+    {
+        double* __restrict__ pNext = B.b[(it + 2) % kGsBufs];
+        const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+        {
+            const int b = tid % T, c = tid / T;
+            if (b < ey && c < ez) {
+                const size_t row = cidx(P, 0, j0 + b, k0 + c);
+                const bool per = P.bc[0] == SIFV_BC_PERIODIC;
+                if (!per && I == 0) pNext[row - 1] = pNew[row];
+                if (!per && I == ntx - 1) pNew[row + P.nx] = pNew[row + P.nx - 1];
+                if (per && I == ntx - 1) {
+                    pNext[row - 1] = pNew[row + P.nx - 1];
+                    pNew[row + P.nx] = pNew[row];
+                }
+            }
+        }
+        {
+            const int a = tid % T, c = tid / T;
+            if (a < ex && c < ez) {
+                const size_t col = cidx(P, i0 + a, 0, k0 + c);
+                const size_t hi = (size_t)P.ny * sy;
+                const bool per = P.bc[2] == SIFV_BC_PERIODIC;
+                if (!per && J == 0) pNext[col - sy] = pNew[col];
+                if (!per && J == nty - 1) pNew[col + hi] = pNew[col + hi - sy];
+                if (per && J == nty - 1) {
+                    pNext[col - sy] = pNew[col + hi - sy];
+                    pNew[col + hi] = pNew[col];
+                }
+            }
+        }
+        {
+            const int a = tid % T, b = tid / T;
+            if (a < ex && b < ey) {
+                const size_t col = cidx(P, i0 + a, j0 + b, 0);
+                const size_t hi = (size_t)P.nz * sz;
+                const bool per = P.bc[4] == SIFV_BC_PERIODIC;
+                if (!per && K == 0) pNext[col - sz] = pNew[col];
+                if (!per && K == ntz - 1) pNew[col + hi] = pNew[col + hi - sz];
+                if (per && K == ntz - 1) {
+                    pNext[col - sz] = pNew[col + hi - sz];
+                    pNew[col + hi] = pNew[col];
+                }
+            }
+        }
+    }
+    block_max_to(maxRes, &ctl->res[it]);
+}
+
+// The ghost cells of `dst` from the scalar ghost map applied to `src`
+// (fillScalarGhosts of `src`'s interior into `dst`'s ghost layers).
+__global__ void k_scalar_ghosts_from(Params P, const double* __restrict__ src, double* __restrict__ dst) {
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (t >= ghost_count(P) || !ghost_coords(P, t, i, j, k)) return;
+    dst[cidx(P, i, j, k)] = src[scalar_idx(P, i, j, k)];
 }
 
 template <int TX, int TY, int TZ>
