@@ -556,8 +556,7 @@ int sifv_fp64_peak_probe(int reps, double* tflops);
  * with SIFV_ERR_BAD_ARG.  The first call on a device (and the first after
  * a device reset, or under another context on that device) looks up the
  * static array's device address (cudaGetSymbolAddress) with that device
- * current and keeps it for later calls; make that first call before any
- * stream capture.  Each call waits on `stream` (cudaStreamSynchronize)
+ * current and keeps it for later calls.  Each call waits on `stream` (cudaStreamSynchronize)
  * while it runs: it reads the convergence flag back to the host between
  * batches of iterations, and it returns once the solution is in `pressure`.
  * All calls on a device share the one array and find the previous call's
