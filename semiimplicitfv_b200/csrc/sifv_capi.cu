@@ -392,12 +392,12 @@ int igr_solve(sifv_ctx* c, int step) {
         k_igr_records<<<blocks(total, 256), 256, 0, c->stream>>>(P, c->F, c->igrRec, ntx, nty, total, slowRecs);
         c->launches++;
     }
-    // Record sweeps overlap when nothing runs between them (no halo exchange,
+    // Sweeps (record or plain tiles, 2D and 3D) overlap when nothing runs between them (no halo exchange,
     // no immersed-boundary fix-up): sweep s + 1 trails sweep s by `lag` tile
     // planes, at least 2 (no face-adjacent tiles in one launch) and, on a
     // periodic axis, the tiles along it (the wrap-around ghost images of
     // sweep s are final before sweep s + 1 reads them).
-    if (rec && iters > 1 && !c->exchangeFaces && !c->ib.count) {
+    if (P.dim >= 2 && iters > 1 && !c->exchangeFaces && !c->ib.count) {
         int lag = 2;
         if (P.bc[0] == SIFV_BC_PERIODIC) lag = std::max(lag, ntx);
         if (P.bc[2] == SIFV_BC_PERIODIC) lag = std::max(lag, nty);
@@ -421,14 +421,24 @@ int igr_solve(sifv_ctx* c, int step) {
             at[0].val.programmaticStreamSerializationAllowed = 1;
             cudaLaunchConfig_t lc = {};
             lc.gridDim = dim3((unsigned)(PL.n * nty * ntz));
-            lc.blockDim = dim3(kIgrTile * kIgrTile);
-            lc.dynamicSmemBytes = igr_tile_rec_smem();
             lc.stream = c->stream;
-            lc.attrs = at;
-            lc.numAttrs = first ? 0 : 1;
+            if (rec) {
+                lc.blockDim = dim3(kIgrTile * kIgrTile);
+                lc.dynamicSmemBytes = igr_tile_rec_smem();
+                lc.attrs = at;
+                lc.numAttrs = first ? 0 : 1;   // planes after the first overlap their record prologue
+                CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_igr_tile_rec, P, c->F, (const double*)c->igrRec,
+                                               (const int*)slowRecs, PL, ntx, nty, ntz));
+            } else if (d3) {
+                lc.blockDim = dim3(T3 * T3);
+                lc.dynamicSmemBytes = smem;
+                CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_igr_tile<T3, T3, T3>, P, c->F, PL, ntx, nty, ntz));
+            } else {
+                lc.blockDim = dim3(T2Y);
+                lc.dynamicSmemBytes = smem;
+                CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_igr_tile<T2X, T2Y, 1>, P, c->F, PL, ntx, nty, ntz));
+            }
             first = false;
-            CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_igr_tile_rec, P, c->F, (const double*)c->igrRec,
-                                           (const int*)slowRecs, PL, ntx, nty, ntz));
             ++launched;
         }
         c->launches += launched;
@@ -461,10 +471,16 @@ int igr_solve(sifv_ctx* c, int step) {
                     PL.n = 1;
                     CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_igr_tile_rec, P, c->F, (const double*)c->igrRec,
                                                    (const int*)slowRecs, PL, ntx, nty, ntz));
-                } else if (d3)
-                    k_igr_tile<T3, T3, T3><<<(unsigned)(nty * ntz), T3 * T3, smem, c->stream>>>(P, c->F, pl, ntx, nty);
-                else
-                    k_igr_tile<T2X, T2Y, 1><<<(unsigned)nty, T2Y, smem, c->stream>>>(P, c->F, pl, ntx, nty);
+                } else {
+                    IgrPlanes PL{};
+                    PL.top = pl;
+                    PL.n = 1;
+                    if (d3)
+                        k_igr_tile<T3, T3, T3><<<(unsigned)(nty * ntz), T3 * T3, smem, c->stream>>>(P, c->F, PL, ntx,
+                                                                                                  nty, ntz);
+                    else
+                        k_igr_tile<T2X, T2Y, 1><<<(unsigned)nty, T2Y, smem, c->stream>>>(P, c->F, PL, ntx, nty, ntz);
+                }
             }
             c->launches += nplanes;
         }

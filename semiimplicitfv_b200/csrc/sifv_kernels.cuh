@@ -1629,6 +1629,66 @@ __device__ __forceinline__ void cp_async8(double* smemDst, const double* gmemSrc
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Sweeps of one IGR solve overlapped in one launch sequence (k_igr_tile,
+// k_igr_tile_rec): the tile plane of each active sweep, and whether the
+// boundary tiles refresh the scalar ghost layer themselves.
+struct IgrPlanes {
+    int top;      // tile plane of the first active sweep; sweep slot u runs plane top - u lag
+    int lag;      // planes between consecutive sweeps
+    int n;        // active sweeps (blocks: n x nty x ntz)
+    int ghosts;   // boundary tiles refresh the scalar ghosts
+};
+
+__device__ __forceinline__ void igr_tile_ghosts(const Params& P, double* sigma, int I, int J, int K, int ntx,
+                                                int nty, int ntz, int i0, int j0, int k0, int ex, int ey, int ez) {
+    const int nt = (int)blockDim.x;
+    const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+    // x faces: the tile's (y, z) rows
+    {
+        const bool per = P.bc[0] == SIFV_BC_PERIODIC;
+        for (int w = (int)threadIdx.x; w < ey * ez; w += nt) {
+            const int b = w % ey, c = w / ey;
+            const size_t row = cidx(P, 0, j0 + b, k0 + c);
+            if (!per && I == 0 && P.bc[0] != SIFV_BC_EXCHANGE) sigma[row - 1] = sigma[row];
+            if (!per && I == ntx - 1 && P.bc[1] != SIFV_BC_EXCHANGE) sigma[row + P.nx] = sigma[row + P.nx - 1];
+            if (per && I == ntx - 1) {
+                sigma[row - 1] = sigma[row + P.nx - 1];
+                sigma[row + P.nx] = sigma[row];
+            }
+        }
+    }
+    // y faces: the tile's (x, z) columns
+    if (P.dim >= 2) {
+        const bool per = P.bc[2] == SIFV_BC_PERIODIC;
+        const size_t hi = (size_t)P.ny * sy;
+        for (int w = (int)threadIdx.x; w < ex * ez; w += nt) {
+            const int a = w % ex, c = w / ex;
+            const size_t col = cidx(P, i0 + a, 0, k0 + c);
+            if (!per && J == 0 && P.bc[2] != SIFV_BC_EXCHANGE) sigma[col - sy] = sigma[col];
+            if (!per && J == nty - 1 && P.bc[3] != SIFV_BC_EXCHANGE) sigma[col + hi] = sigma[col + hi - sy];
+            if (per && J == nty - 1) {
+                sigma[col - sy] = sigma[col + hi - sy];
+                sigma[col + hi] = sigma[col];
+            }
+        }
+    }
+    // z faces: the tile's (x, y) columns
+    if (P.dim >= 3) {
+        const bool per = P.bc[4] == SIFV_BC_PERIODIC;
+        const size_t hi = (size_t)P.nz * sz;
+        for (int w = (int)threadIdx.x; w < ex * ey; w += nt) {
+            const int a = w % ex, b = w / ex;
+            const size_t col = cidx(P, i0 + a, j0 + b, 0);
+            if (!per && K == 0 && P.bc[4] != SIFV_BC_EXCHANGE) sigma[col - sz] = sigma[col];
+            if (!per && K == ntz - 1 && P.bc[5] != SIFV_BC_EXCHANGE) sigma[col + hi] = sigma[col + hi - sz];
+            if (per && K == ntz - 1) {
+                sigma[col - sz] = sigma[col + hi - sz];
+                sigma[col + hi] = sigma[col];
+            }
+        }
+    }
+}
+
 // Tiled wavefront of the same lexicographic sweep.  The domain is cut into
 // TX x TY x TZ tiles; tile (I, J, K) only reads cells of tiles (I-1, J, K),
 // (I, J-1, K), (I, J, K-1) (already updated in this sweep) and of
@@ -1640,8 +1700,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // every cell is updated with igr_cell's arithmetic in igr_cell's order, so
 // the result is bit-identical to the lexicographic sweep.
 // Dynamic shared memory: (2 (TX+2)(TY+2)(TZ+2 or 1) + 2 TX TY TZ) doubles.
+// Several sweeps overlap as in k_igr_tile_rec (IgrPlanes; boundary tiles
+// refresh the ghost layer at their end).
 template <int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, int plane, int ntx, int nty) {
+__global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, IgrPlanes PL, int ntx, int nty, int ntz) {
     extern __shared__ double smem[];
     constexpr int D3 = (TZ > 1) ? 1 : 0;
     constexpr int HX = TX + 2, HY = TY + 2, HZ = D3 ? TZ + 2 : 1;
@@ -1651,8 +1713,11 @@ __global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, int pl
     double* sRhs = smem + 2 * HN;
     double* sDiag = sRhs + TN;
     double* sAx = sDiag + TN;   // alpha / dx^2 of the tile's columns (no global load inside the wavefront)
-    const int J = (int)(blockIdx.x % (unsigned)nty), K = (int)(blockIdx.x / (unsigned)nty);
-    const int I = plane - J - K;
+    const unsigned perSlot = (unsigned)(nty * ntz);
+    const int slot = (int)(blockIdx.x / perSlot);
+    const unsigned bt = blockIdx.x % perSlot;
+    const int J = (int)(bt % (unsigned)nty), K = (int)(bt / (unsigned)nty);
+    const int I = PL.top - slot * PL.lag - J - K;
     if (I < 0 || I >= ntx) return;
     const int i0 = I * TX, j0 = J * TY, k0 = K * TZ;
     const int ex = min(TX, P.nx - i0), ey = min(TY, P.ny - j0), ez = D3 ? min(TZ, P.nz - k0) : 1;
@@ -1717,6 +1782,10 @@ __global__ void __launch_bounds__(TY * TZ) k_igr_tile(Params P, Fields F, int pl
         const int b = line % ey, c = line / ey;
         for (int a = lane; a < ex; a += 32)
             F.sigma[cidx(P, i0 + a, j0 + b, k0 + c)] = sS[((c + D3) * HY + (b + 1)) * HX + (a + 1)];
+    }
+    if (PL.ghosts) {
+        __syncthreads();   // the tile's sigma, written by all warps above
+        igr_tile_ghosts(P, F.sigma, I, J, K, ntx, nty, ntz, i0, j0, k0, ex, ey, ez);
     }
 }
 
@@ -1878,62 +1947,6 @@ __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.w
 // and the next sweep has not reached it).  Only the ghost layer next to the
 // face is written (the 7-point stencil reads no other); the full fill runs
 // after the last sweep.
-struct IgrPlanes {
-    int top;      // tile plane of the first active sweep; sweep slot u runs plane top - u lag
-    int lag;      // planes between consecutive sweeps
-    int n;        // active sweeps (blocks: n x nty x ntz)
-    int ghosts;   // boundary tiles refresh the scalar ghosts
-};
-__device__ __forceinline__ void igr_tile_ghosts(const Params& P, double* sigma, int I, int J, int K, int ntx,
-                                                int nty, int ntz, int i0, int j0, int k0, int ex, int ey, int ez) {
-    const int tid = (int)threadIdx.x;
-    const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
-    // x faces: one thread per (y, z) of the tile
-    {
-        const int b = tid % kIgrTile, c = tid / kIgrTile;
-        if (b < ey && c < ez) {
-            const size_t row = cidx(P, 0, j0 + b, k0 + c);
-            const bool per = P.bc[0] == SIFV_BC_PERIODIC;
-            if (!per && I == 0 && P.bc[0] != SIFV_BC_EXCHANGE) sigma[row - 1] = sigma[row];
-            if (!per && I == ntx - 1 && P.bc[1] != SIFV_BC_EXCHANGE) sigma[row + P.nx] = sigma[row + P.nx - 1];
-            if (per && I == ntx - 1) {
-                sigma[row - 1] = sigma[row + P.nx - 1];
-                sigma[row + P.nx] = sigma[row];
-            }
-        }
-    }
-    // y faces: one thread per (x, z)
-    {
-        const int a = tid % kIgrTile, c = tid / kIgrTile;
-        if (a < ex && c < ez) {
-            const size_t col = cidx(P, i0 + a, 0, k0 + c);
-            const bool per = P.bc[2] == SIFV_BC_PERIODIC;
-            const size_t hi = (size_t)P.ny * sy;
-            if (!per && J == 0 && P.bc[2] != SIFV_BC_EXCHANGE) sigma[col - sy] = sigma[col];
-            if (!per && J == nty - 1 && P.bc[3] != SIFV_BC_EXCHANGE) sigma[col + hi] = sigma[col + hi - sy];
-            if (per && J == nty - 1) {
-                sigma[col - sy] = sigma[col + hi - sy];
-                sigma[col + hi] = sigma[col];
-            }
-        }
-    }
-    // z faces: one thread per (x, y)
-    {
-        const int a = tid % kIgrTile, b = tid / kIgrTile;
-        if (a < ex && b < ey) {
-            const size_t col = cidx(P, i0 + a, j0 + b, 0);
-            const bool per = P.bc[4] == SIFV_BC_PERIODIC;
-            const size_t hi = (size_t)P.nz * sz;
-            if (!per && K == 0 && P.bc[4] != SIFV_BC_EXCHANGE) sigma[col - sz] = sigma[col];
-            if (!per && K == ntz - 1 && P.bc[5] != SIFV_BC_EXCHANGE) sigma[col + hi] = sigma[col + hi - sz];
-            if (per && K == ntz - 1) {
-                sigma[col - sz] = sigma[col + hi - sz];
-                sigma[col + hi] = sigma[col];
-            }
-        }
-    }
-}
-
 __global__ void __launch_bounds__(256, 1)
     k_igr_tile_rec(Params P, Fields F, const double* __restrict__ rec, const int* __restrict__ slowRecs,
                    IgrPlanes PL, int ntx, int nty, int ntz) {

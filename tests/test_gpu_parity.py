@@ -110,14 +110,19 @@ def test_igr_record_sweep_3d(nx, ny, nz):
 
 @pytest.mark.parametrize("shape,bcs", [((40, 36, 34), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_SLIPWALL)),
                                         ((34, 20, 50), (abi.BC_OUTFLOW, abi.BC_SYMMETRY, abi.BC_PERIODIC)),
-                                        ((50, 40, 18), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_NOSLIPWALL))])
+                                        ((50, 40, 18), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_NOSLIPWALL)),
+                                        ((35, 40, 33), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_PERIODIC)),
+                                        ((100, 140, 1), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_OUTFLOW)),
+                                        ((130, 70, 1), (abi.BC_SLIPWALL, abi.BC_PERIODIC, abi.BC_OUTFLOW))])
 def test_igr_overlapped_sweeps_mixed_faces(shape, bcs):
-    """Consecutive record sweeps overlapped in one launch sequence (sweep s + 1
+    """Consecutive sweeps overlapped in one launch sequence (sweep s + 1
     trailing sweep s by a fixed number of tile planes, boundary tiles
-    refreshing the ghost layer themselves), per-axis boundary kinds (periodic
-    wrap images and zero-gradient copies), several tiles along the periodic
-    axes, ragged edges, the 20-sweep warm start: bit-identical to the
-    oracle's sweep-by-sweep order."""
+    refreshing the ghost layer themselves) -- the 3D record sweep, the plain
+    3D tile sweep of odd row lengths (35 + 6 ghosts) and the 2D 32 x 64 tile
+    sweep -- with per-axis boundary kinds (periodic wrap images and
+    zero-gradient copies), several tiles along the periodic axes, ragged
+    edges, the 20-sweep warm start: bit-identical to the oracle's
+    sweep-by-sweep order."""
     cfg, mesh, fields = cases.acoustic_box(*shape)
     mesh.bc = [bcs[0]] * 2 + [bcs[1]] * 2 + [bcs[2]] * 2
     check((cfg, mesh, fields), 2)
