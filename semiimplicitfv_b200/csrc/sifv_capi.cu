@@ -638,15 +638,22 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
                                                                  total, slowRecs);
         c->launches++;
     }
-    if (recs && !c->exchangeFaces && maxIter >= 2) {
-        // overlapped iterations (k_gs_tile_rec_ov): iterate n in buf[n % kGsBufs]
+    if (P.dim >= 2 && !c->exchangeFaces && maxIter >= 2) {
+        // overlapped iterations (k_gs_tile_rec_ov, k_gs_tile_ov): iterate n in buf[n % kGsBufs]
         if (!c->gsBuf[0]) {
             int sa = SIFV_OK;
             for (int q = 0; q < kGsBufs - 2; ++q) c->gsBuf[q] = dalloc(c, c->ncells, sa);
             if (sa != SIFV_OK) return sa;
+        }
+        if (recs)
             CUDA_TRY(c, cudaFuncSetAttribute(k_gs_tile_rec_ov, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)gs_tile_rec_smem()));
-        }
+        else if (d3)
+            CUDA_TRY(c, cudaFuncSetAttribute(k_gs_tile_ov<T3, T3, T3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
+        else
+            CUDA_TRY(c, cudaFuncSetAttribute(k_gs_tile_ov<T2X, T2Y, 1>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         GsBufs B{};
         B.b[0] = c->F.pA;
         B.b[1] = c->F.pB;
@@ -682,14 +689,26 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
                 at[0].val.programmaticStreamSerializationAllowed = 1;
                 cudaLaunchConfig_t lc = {};
                 lc.gridDim = dim3((unsigned)(PL.n * nty * ntz));
-                lc.blockDim = dim3(kIgrTile * kIgrTile);
-                lc.dynamicSmemBytes = gs_tile_rec_smem();
                 lc.stream = c->stream;
-                lc.attrs = at;
-                lc.numAttrs = first ? 0 : 1;
+                if (recs) {
+                    lc.blockDim = dim3(kIgrTile * kIgrTile);
+                    lc.dynamicSmemBytes = gs_tile_rec_smem();
+                    lc.attrs = at;
+                    lc.numAttrs = first ? 0 : 1;
+                    CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_gs_tile_rec_ov, P, (const double*)c->gsRec,
+                                                   (const int*)slowRecs, B, c->ctl, tol, PL, ntx, nty, ntz));
+                } else if (d3) {
+                    lc.blockDim = dim3(T3 * T3);
+                    lc.dynamicSmemBytes = smem;
+                    CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_gs_tile_ov<T3, T3, T3>, P, (const double*)c->gsCoef,
+                                                   c->ncells, rhs, B, c->ctl, tol, PL, ntx, nty, ntz));
+                } else {
+                    lc.blockDim = dim3(T2Y);
+                    lc.dynamicSmemBytes = smem;
+                    CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_gs_tile_ov<T2X, T2Y, 1>, P, (const double*)c->gsCoef,
+                                                   c->ncells, rhs, B, c->ctl, tol, PL, ntx, nty, ntz));
+                }
                 first = false;
-                CUDA_TRY(c, cudaLaunchKernelEx(&lc, k_gs_tile_rec_ov, P, (const double*)c->gsRec,
-                                               (const int*)slowRecs, B, c->ctl, tol, PL, ntx, nty, ntz));
                 c->launches++;
             }
             LAUNCH_CHECK(c);

@@ -2109,6 +2109,17 @@ __global__ void k_gs_sweep_1d(Params P, const double* __restrict__ coef, size_t 
     atomicMax(&ctl->res[it], d2bits(maxRes));
 }
 
+constexpr int kGsBufs = 5;
+struct GsBufs {
+    double* b[kGsBufs];
+};
+struct GsPlanes {
+    int top;   // tile plane of the first active iteration (slot 0); slot u runs plane top - u lag
+    int lag;
+    int n;     // active iterations in this launch
+    int it0;   // index of the iteration in slot 0
+    int S;     // iterations in flight at most
+};
 template <int TX, int TY, int TZ>
 __global__ void __launch_bounds__(TY * TZ) k_gs_tile(Params P, const double* __restrict__ coef, size_t nc,
                                                      const double* __restrict__ rhs, double* __restrict__ p, Ctl* ctl,
@@ -2174,6 +2185,156 @@ __global__ void __launch_bounds__(TY * TZ) k_gs_tile(Params P, const double* __r
         for (int a = lane; a < ex; a += 32)
             p[cidx(P, i0 + a, j0 + b, k0 + c)] = smem[((c + D3) * HY + (b + 1)) * HX + (a + 1)];
     }
+    block_max_to(maxRes, &ctl->res[it]);
+}
+
+// Ghost images of a finished tile of an overlapped Gauss-Seidel iteration
+// (any tile shape): the low-side ghost layer into the next iteration's
+// buffer, the high-side one into this iteration's (k_gs_tile_rec_ov).
+__device__ __forceinline__ void gs_tile_ghosts(const Params& P, double* pNew, double* pNext, int I, int J, int K,
+                                               int ntx, int nty, int ntz, int i0, int j0, int k0, int ex, int ey,
+                                               int ez) {
+    const int nt = (int)blockDim.x;
+    const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
+    {
+        const bool per = P.bc[0] == SIFV_BC_PERIODIC;
+        for (int w = (int)threadIdx.x; w < ey * ez; w += nt) {
+            const int b = w % ey, c = w / ey;
+            const size_t row = cidx(P, 0, j0 + b, k0 + c);
+            if (!per && I == 0) pNext[row - 1] = pNew[row];
+            if (!per && I == ntx - 1) pNew[row + P.nx] = pNew[row + P.nx - 1];
+            if (per && I == ntx - 1) {
+                pNext[row - 1] = pNew[row + P.nx - 1];
+                pNew[row + P.nx] = pNew[row];
+            }
+        }
+    }
+    if (P.dim >= 2) {
+        const bool per = P.bc[2] == SIFV_BC_PERIODIC;
+        const size_t hi = (size_t)P.ny * sy;
+        for (int w = (int)threadIdx.x; w < ex * ez; w += nt) {
+            const int a = w % ex, c = w / ex;
+            const size_t col = cidx(P, i0 + a, 0, k0 + c);
+            if (!per && J == 0) pNext[col - sy] = pNew[col];
+            if (!per && J == nty - 1) pNew[col + hi] = pNew[col + hi - sy];
+            if (per && J == nty - 1) {
+                pNext[col - sy] = pNew[col + hi - sy];
+                pNew[col + hi] = pNew[col];
+            }
+        }
+    }
+    if (P.dim >= 3) {
+        const bool per = P.bc[4] == SIFV_BC_PERIODIC;
+        const size_t hi = (size_t)P.nz * sz;
+        for (int w = (int)threadIdx.x; w < ex * ey; w += nt) {
+            const int a = w % ex, b = w / ex;
+            const size_t col = cidx(P, i0 + a, j0 + b, 0);
+            if (!per && K == 0) pNext[col - sz] = pNew[col];
+            if (!per && K == ntz - 1) pNew[col + hi] = pNew[col + hi - sz];
+            if (per && K == ntz - 1) {
+                pNext[col - sz] = pNew[col + hi - sz];
+                pNew[col + hi] = pNew[col];
+            }
+        }
+    }
+}
+
+// Overlapped iterations of the plain tile sweep (2D 32 x 64 tiles, 3D rows
+// of odd length): k_gs_tile's arithmetic and order with the buffers,
+// staging, skip rule and ghost images of k_gs_tile_rec_ov.
+template <int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TY * TZ) k_gs_tile_ov(Params P, const double* __restrict__ coef, size_t nc,
+                                                        const double* __restrict__ rhs, GsBufs B, Ctl* ctl,
+                                                        double tol, GsPlanes PL, int ntx, int nty, int ntz) {
+    extern __shared__ double smem[];
+    constexpr int D3 = (TZ > 1) ? 1 : 0;
+    constexpr int HX = TX + 2, HY = TY + 2;
+    __shared__ int skip;
+    const unsigned perSlot = (unsigned)(nty * ntz);
+    const int slot = (int)(blockIdx.x / perSlot);
+    const unsigned bt = blockIdx.x % perSlot;
+    const int J = (int)(bt % (unsigned)nty), K = (int)(bt / (unsigned)nty);
+    const int I = PL.top - slot * PL.lag - J - K;
+    if (I < 0 || I >= ntx) return;
+    const int it = PL.it0 + slot;
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int j = 0; j <= it - PL.S; ++j)
+            if (bits2d(ctl->res[j]) < tol) { s = 1; break; }
+        skip = s;
+    }
+    __syncthreads();
+    if (skip) return;
+    const double* __restrict__ pOld = B.b[it % kGsBufs];
+    double* __restrict__ pNew = B.b[(it + 1) % kGsBufs];
+    const int i0 = I * TX, j0 = J * TY, k0 = K * TZ;
+    const int ex = min(TX, P.nx - i0), ey = min(TY, P.ny - j0), ez = D3 ? min(TZ, P.nz - k0) : 1;
+    const int hx = ex + 2, hy = ey + 2, hz = D3 ? ez + 2 : 1;
+    const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5, nwarp = (int)blockDim.x >> 5;
+    for (int line = warp; line < hy * hz; line += nwarp) {   // tile + downstream halos: iterate it
+        const int b = line % hy, c = line / hy;
+        for (int a = lane; a < hx; a += 32)
+            cp_async8(&smem[(c * HY + b) * HX + a], &pOld[cidx(P, i0 + a - 1, j0 + b - 1, D3 ? k0 + c - 1 : k0)]);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    {   // upstream face halos: iterate it + 1 (this iteration's upstream tiles / ghost images)
+        const int nt = (int)blockDim.x;
+        for (int w = (int)threadIdx.x; w < ey * ez; w += nt) {
+            const int b = w % ey, c = w / ey;
+            smem[((c + D3) * HY + (b + 1)) * HX] = pNew[cidx(P, i0 - 1, j0 + b, k0 + c)];
+        }
+        for (int w = (int)threadIdx.x; w < ex * ez; w += nt) {
+            const int a = w % ex, c = w / ex;
+            smem[((c + D3) * HY) * HX + a + 1] = pNew[cidx(P, i0 + a, j0 - 1, k0 + c)];
+        }
+        if (D3)
+            for (int w = (int)threadIdx.x; w < ex * ey; w += nt) {
+                const int a = w % ex, b = w / ex;
+                smem[(b + 1) * HX + a + 1] = pNew[cidx(P, i0 + a, j0 + b, k0 - 1)];
+            }
+    }
+    const int tb = (int)threadIdx.x % TY, tc = (int)threadIdx.x / TY;
+    const bool act = tb < ey && tc < ez;
+    const int hLine = ((tc + D3) * HY + (tb + 1)) * HX + 1;
+    constexpr int DIM = D3 ? 3 : 2;
+    constexpr int NCO = 2 * DIM + 2;
+    double maxRes = 0.0;
+    __syncthreads();
+    const int nq = ex + ey + ez - 2;
+    double sA[NCO + 1], sB[NCO + 1], sC[NCO + 1];
+    auto step = [&](int q, double (&X)[NCO + 1], double (&Z)[NCO + 1]) {
+        const int a = q - tb - tc;
+        if (act && a + 2 >= 0 && a + 2 < ex) {
+            const size_t c = cidx(P, i0 + a + 2, j0 + tb, k0 + tc);
+#pragma unroll
+            for (int k = 0; k < NCO; ++k) Z[k] = coef[c + (size_t)k * nc];
+            Z[NCO] = rhs[c];
+        }
+        if (q < 0 || q >= nq) return;
+        if (act && a >= 0 && a < ex) {
+            const int h = hLine + a;
+            const double nb[6] = {smem[h - 1], smem[h + 1], smem[h - HX], smem[h + HX],
+                                  D3 ? smem[h - HX * HY] : 0.0, D3 ? smem[h + HX * HY] : 0.0};
+            const double po = smem[h];
+            const double pn = gs_cell(DIM, X, 1, X[NCO], nb);
+            smem[h] = pn;
+            maxRes = smax(maxRes, fabs(pn - po));
+        }
+        __syncthreads();
+    };
+    for (int q = -2; q < nq; q += 3) {
+        step(q, sA, sC);
+        step(q + 1, sB, sA);
+        step(q + 2, sC, sB);
+    }
+    for (int line = warp; line < ey * ez; line += nwarp) {
+        const int b = line % ey, c = line / ey;
+        for (int a = lane; a < ex; a += 32)
+            pNew[cidx(P, i0 + a, j0 + b, k0 + c)] = smem[((c + D3) * HY + (b + 1)) * HX + (a + 1)];
+    }
+    __syncthreads();   // the tile's new values, written by all warps above
+    gs_tile_ghosts(P, pNew, B.b[(it + 2) % kGsBufs], I, J, K, ntx, nty, ntz, i0, j0, k0, ex, ey, ez);
     block_max_to(maxRes, &ctl->res[it]);
 }
 
@@ -2341,17 +2502,6 @@ __global__ void __launch_bounds__(256, 1) k_gs_tile_rec(Params P, const double* 
 // iteration m starts; its tiles skip when one of them is below tol, so at
 // most S - 1 iterations run past the converged one and never reach its
 // buffer or its predecessor's (five buffers).
-constexpr int kGsBufs = 5;
-struct GsBufs {
-    double* b[kGsBufs];
-};
-struct GsPlanes {
-    int top;   // tile plane of the first active iteration (slot 0); slot u runs plane top - u lag
-    int lag;
-    int n;     // active iterations in this launch
-    int it0;   // index of the iteration in slot 0
-    int S;     // iterations in flight at most
-};
 __global__ void __launch_bounds__(256, 1) k_gs_tile_rec_ov(Params P, const double* __restrict__ rec,
                                                            const int* __restrict__ slowRecs, GsBufs B, Ctl* ctl,
                                                            double tol, GsPlanes PL, int ntx, int nty, int ntz) {

@@ -301,13 +301,17 @@ def test_gauss_seidel_pressure_solver(name):
 @pytest.mark.parametrize("shape,bcs", [((40, 36, 34), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_SLIPWALL)),
                                         ((34, 20, 50), (abi.BC_OUTFLOW, abi.BC_SYMMETRY, abi.BC_PERIODIC)),
                                         ((50, 40, 18), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_NOSLIPWALL)),
-                                        ((64, 32, 32), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_PERIODIC))])
+                                        ((64, 32, 32), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_PERIODIC)),
+                                        ((35, 40, 33), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_PERIODIC)),
+                                        ((100, 140, 1), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_OUTFLOW)),
+                                        ((130, 70, 1), (abi.BC_SLIPWALL, abi.BC_PERIODIC, abi.BC_OUTFLOW))])
 @pytest.mark.parametrize("max_iter,dt,tol", [(1, 1e-2, 1e-14), (2, 1e-2, 1e-14), (3, 1e-2, 1e-14),
                                              (7, 1e-2, 1e-14), (300, 2e-3, 1e-9), (300, 1e-2, 1e-8)])
 def test_gauss_seidel_overlapped_iterations(shape, bcs, max_iter, dt, tol):
-    """Gauss-Seidel iterations overlapped in one launch sequence (record
-    sweep, iterates rotating through five buffers, speculative iterations
-    past the converged one discarded): per-axis periodic / zero-gradient
+    """Gauss-Seidel iterations overlapped in one launch sequence (the 3D
+    record sweep, the plain 3D sweep of odd row lengths and the 2D 32 x 64
+    tile sweep; iterates rotating through five buffers, speculative
+    iterations past the converged one discarded): per-axis periodic / zero-gradient
     faces, several tiles along periodic axes, ragged tiles, iteration caps
     of 1-7 and convergence after a few or many host batches.  The iteration
     count and the whole returned array -- interior and the ghost layers the
