@@ -139,9 +139,20 @@ class DistExchange:
         self.block = g * plane
         self.low_ghost, self.low_int = 0, g * plane
         self.high_int, self.high_ghost = n_int * plane, (n_int + g) * plane
+        # The step asks for the same few field sets (and reduction slots) over
+        # and over: the views and operation lists are built once per address
+        # set and reused, which keeps the host's work per exchange small.
+        self._plans = {}
+        self._scalars = {}
 
-    def exchange(self, ptrs, stream):
+    def _plan(self, ptrs):
         import torch.distributed as dist
+        key = tuple(ptrs)
+        plan = self._plans.get(key)
+        if plan is not None:
+            return plan
+        if len(self._plans) > 64:   # the context re-allocated its arrays: forget old addresses
+            self._plans.clear()
         sends, recvs = [], []
         for p in ptrs:
             f = _view(p, self.n, self.device)
@@ -157,14 +168,31 @@ class DistExchange:
                 recvs.append((f[self.low_ghost:self.low_ghost + b], self.lo, self.TAG_TO_LOW))
             if self.hi is not None:
                 recvs.append((f[self.high_ghost:self.high_ghost + b], self.hi, self.TAG_TO_HIGH))
+        ops = None
         if self.device:
-            ops = [dist.P2POp(dist.isend, t.contiguous(), peer) for t, peer, _ in sends] + \
+            ops = [dist.P2POp(dist.isend, t, peer) for t, peer, _ in sends] + \
                   [dist.P2POp(dist.irecv, t, peer) for t, peer, _ in recvs]
+        plan = (sends, recvs, ops)
+        self._plans[key] = plan
+        return plan
+
+    def _scalar(self, ptr):
+        v = self._scalars.get(ptr)
+        if v is None:
+            if len(self._scalars) > 64:
+                self._scalars.clear()
+            v = self._scalars[ptr] = _view(ptr, 1, self.device)
+        return v
+
+    def exchange(self, ptrs, stream):
+        import torch.distributed as dist
+        sends, recvs, ops = self._plan(ptrs)
+        if self.device:
             if ops:
                 for w in dist.batch_isend_irecv(ops):
                     w.wait()
         else:
-            works = [dist.isend(t.contiguous(), peer, tag=tag) for t, peer, tag in sends]
+            works = [dist.isend(t, peer, tag=tag) for t, peer, tag in sends]
             works += [dist.irecv(t, peer, tag=tag) for t, peer, tag in recvs]
             for w in works:
                 w.wait()
@@ -172,12 +200,12 @@ class DistExchange:
 
     def allreduce_min(self, ptr, stream):
         import torch.distributed as dist
-        dist.all_reduce(_view(ptr, 1, self.device), op=dist.ReduceOp.MIN)
+        dist.all_reduce(self._scalar(ptr), op=dist.ReduceOp.MIN)
         return 0
 
     def allreduce_max(self, ptr, stream):
         import torch.distributed as dist
-        dist.all_reduce(_view(ptr, 1, self.device), op=dist.ReduceOp.MAX)
+        dist.all_reduce(self._scalar(ptr), op=dist.ReduceOp.MAX)
         return 0
 
     def attach(self):
