@@ -21,7 +21,8 @@ SOURCES = [("sifv_capi.cu", ["--fmad=false"]), ("sifv_noalloc.cu", ["--fmad=fals
            ("sifv_ensemble_mixed.cu", ["--fmad=true", "--use_fast_math"]), ("sifv_adjoint.cu", ["--fmad=true"]),
            ("sifv_vtk.cpp", []), ("sifv_ib.cpp", ["-Xcompiler", "-ffp-contract=off"])]
 HEADERS = ["sifv_device.cuh", "sifv_common.cuh", "sifv_kernels.cuh", "sifv_sweep.cuh", "sifv_sweep_api.h",
-           "sifv_ensemble.cuh", "sifv_ensemble_api.h", "sifv_adjoint.cuh", "sifv_adjoint_api.h", "sifv_dual.cuh", "sifv_march2d.cuh", "sifv_fastmath.cuh", "sifv_vtk_api.h", "sifv_ib_api.h"]
+           "sifv_ensemble.cuh", "sifv_ensemble_api.h", "sifv_adjoint.cuh", "sifv_adjoint_api.h", "sifv_dual.cuh", "sifv_march2d.cuh", "sifv_fastmath.cuh", "sifv_vtk_api.h", "sifv_ib_api.h",
+           "sifv_mg.cuh", "sifv_gs_march.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

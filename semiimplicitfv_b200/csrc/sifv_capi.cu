@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -17,6 +18,7 @@
 #include "sifv.h"
 #include "sifv_adjoint_api.h"
 #include "sifv_kernels.cuh"
+#include "sifv_gs_march.cuh"
 #include "sifv_mg.cuh"
 #include "sifv_sweep_api.h"
 #include "sifv_ib_api.h"
@@ -81,7 +83,14 @@ struct sifv_ctx {
     bool igrTileReady = false;
     double* igrRec = nullptr;                 // IGR sweep records (k_igr_records), then one int flag
     double* gsRec = nullptr;                  // Gauss-Seidel sweep records (k_gs_records), then one int flag
-    double* gsBuf[3] = {nullptr, nullptr, nullptr};   // iterates 2-4 (mod 5) of the overlapped Gauss-Seidel sweeps
+    std::vector<double*> gsBuf;               // iterate buffers 2 .. of the overlapped Gauss-Seidel sweeps
+    double2* marchQ[kMarchMaxBufs] = {};     // 2D Gauss-Seidel wavefront: iterates (skewed pair layout)
+    double* marchRec = nullptr;               // its records
+    int* marchInt = nullptr;                  // progress [G], flags [2], slowRecs [1], done [marchIntCap]
+    int marchIntCap = -1;
+    int marchOk = -1;                         // -1 unknown, 0 no cooperative launch, 1 usable
+    long long marchCtas = 0;                  // co-resident CTAs of k_march_gs
+    int marchMode = -1;                       // SIFV_GS_MARCH: -1 (unset) periodic meshes, 0 never, 1 always
     int gsPrevIters = 0;                      // iterations of the previous Gauss-Seidel solve (first batch size)
     double* jacCoef = nullptr;                // Jacobi coefficients: per face (dim arrays) or per cell (2 dim + 2)
     bool uniformAxes = false;                 // interior cell widths bitwise equal along every active axis
@@ -586,6 +595,148 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
     return SIFV_OK;
 }
 
+// The 2D iterations as one persistent wavefront (k_march_gs): records and
+// iterate 0 from the coefficients (c->gsCoef) and F.pA, one cooperative
+// launch for all iterations, the iteration count from the per-sweep
+// residuals, the result back into F.pA.  The warps walk along a periodic
+// axis (free for the wavefront), along the longer one when both are
+// periodic.  Returns 1 (nothing done) when the launch does not fit the
+// device or the progress counters would overflow.
+int gs_march(sifv_ctx* c, const double* rhs, double tol, int maxIter, int& iters, const double*& result) {
+    const Params& P = c->P;
+    const bool px = P.bc[0] == SIFV_BC_PERIODIC || P.bc[1] == SIFV_BC_PERIODIC;
+    const bool py = P.bc[2] == SIFV_BC_PERIODIC || P.bc[3] == SIFV_BC_PERIODIC;
+    const bool tr = (py && !px) || (px && py && P.ny > P.nx);   // walk along y
+    const int Nm = tr ? P.ny : P.nx, Nn = tr ? P.nx : P.ny;     // march and row extents
+    const int bm0 = tr ? P.bc[2] : P.bc[0], bm1 = tr ? P.bc[3] : P.bc[1];
+    const int bn0 = tr ? P.bc[0] : P.bc[2], bn1 = tr ? P.bc[1] : P.bc[3];
+    const int NH = (Nm + 1) / 2, SW = NH + 32, NS = NH + 31;
+    const int G = Nn / 32 + 1, GA = (Nn + 1) / 32 + 1;
+    const int ctas = (G + kMarchWarps - 1) / kMarchWarps;
+    if ((long long)(maxIter + 2) * NS >= (1LL << 30)) return 1;
+    // the four instances: batch length 8 or 4 (periodic row axis), walking along x or y
+    using MarchFn = void (*)(Params, GsMarch, Ctl*);
+    const MarchFn fns[4] = {k_march_gs<kMarchWarps, 8, false>, k_march_gs<kMarchWarps, 8, true>,
+                            k_march_gs<kMarchWarps, 4, false>, k_march_gs<kMarchWarps, 4, true>};
+    // D = 4 when a periodic row axis makes the groups' lags (about 32 + 2 D + 10 steps each) longer than
+    // a sweep; otherwise D = 8
+    const bool rowPeriodic = bn0 == SIFV_BC_PERIODIC || bn1 == SIFV_BC_PERIODIC;
+    const bool short8 = rowPeriodic && (long long)G * (32 + 2 * 8 + 10) > NS;
+    const int D = short8 ? 4 : 8;
+    const MarchFn fn = fns[(short8 ? 2 : 0) + (tr ? 1 : 0)];
+    const size_t smem = march_smem(D);
+    if (c->marchOk < 0) {
+        c->marchOk = 0;
+        int coop = 0, sms = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        long long fit = -1;
+        for (int q = 0; q < 4 && coop; ++q) {
+            const size_t sq = march_smem(q < 2 ? 8 : 4);
+            int perSm = 0;
+            if (cudaFuncSetAttribute(fns[q], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sq) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fns[q], 32 * (kMarchWarps + 1), sq) !=
+                    cudaSuccess) {
+                fit = -1;
+                break;
+            }
+            fit = (fit < 0) ? (long long)perSm * sms : std::min(fit, (long long)perSm * sms);
+        }
+        if (fit > 0) {
+            c->marchOk = 1;
+            c->marchCtas = fit;
+        }
+        cudaGetLastError();
+    }
+    if (!c->marchOk || ctas > c->marchCtas) return 1;
+    const size_t qn = (size_t)GA * SW * 32;   // pairs per iterate
+    // buffers: the groups spread over about G (32 + 2 D + 40) / NS sweeps, plus the converged iterate,
+    // its predecessor and one sweep of slack; at most 1 GiB
+    int nb = std::min(kMarchMaxBufs, 4 + (G * (32 + 2 * D + 40) + NS - 1) / NS);
+    nb = std::max(3, std::min<int>(nb, (int)((size_t(1) << 30) / (qn * sizeof(double2)))));
+    int sa = SIFV_OK;
+    if (!c->marchRec) {
+        c->marchRec = dalloc(c, qn * 16, sa);   // 8 double2 per pair
+        if (sa != SIFV_OK) return sa;
+    }
+    for (int q = 0; q < nb; ++q)
+        if (!c->marchQ[q]) {
+            c->marchQ[q] = reinterpret_cast<double2*>(dalloc(c, qn * 2, sa));
+            if (sa != SIFV_OK) return sa;
+        }
+    if (c->marchIntCap < maxIter) {   // ints in double units
+        const int cap = std::max(maxIter, 64);
+        c->marchInt = reinterpret_cast<int*>(dalloc(c, ((size_t)G + 3 + cap + 1) / 2 + 1, sa));
+        if (sa != SIFV_OK) return sa;
+        c->marchIntCap = cap;
+    }
+    int* prog = c->marchInt;
+    int* flags = prog + G;
+    int* slowRecs = flags + 2;
+    int* done = slowRecs + 1;
+    CUDA_TRY(c, cudaMemsetAsync(c->marchInt, 0, sizeof(int) * ((size_t)G + 3 + maxIter), c->stream));
+    const long long total = (long long)qn;
+    k_march_gs_setup<<<blocks(total, 256), 256, 0, c->stream>>>(P, c->gsCoef, c->ncells, rhs, c->F.pA,
+                                                               reinterpret_cast<double2*>(c->marchRec), c->marchQ[0],
+                                                               SW, total, slowRecs, tr ? 1 : 0);
+    GsMarch M{};
+    M.rec = reinterpret_cast<const double2*>(c->marchRec);
+    for (int q = 0; q < nb; ++q) M.q[q] = c->marchQ[q];
+    M.prog = prog;
+    M.done = done;
+    M.flags = flags;
+    M.slowRecs = slowRecs;
+    M.nb = nb;
+    M.G = G;
+    M.GA = GA;
+    M.SW = SW;
+    M.NS = NS;
+    M.NH = NH;
+    M.maxIter = maxIter;
+    M.nx = Nm;
+    M.ny = Nn;
+    M.xsLo = (bm0 == SIFV_BC_PERIODIC) ? Nm - 1 : 0;
+    M.xsHi = (bm1 == SIFV_BC_PERIODIC) ? 0 : Nm - 1;
+    M.perLoY = bn0 == SIFV_BC_PERIODIC;
+    M.perHiY = bn1 == SIFV_BC_PERIODIC;
+    M.tol = tol;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3((unsigned)ctas);
+    lc.blockDim = dim3(32 * (kMarchWarps + 1));
+    lc.dynamicSmemBytes = smem;
+    lc.stream = c->stream;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    CUDA_TRY(c, cudaLaunchKernelEx(&lc, fn, P, M, c->ctl));
+    c->launches += 2;
+    LAUNCH_CHECK(c);
+    int hostFlags[2] = {0, 0};
+    CUDA_TRY(c, cudaMemcpyAsync(hostFlags, flags, sizeof(hostFlags), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl) + sizeof(unsigned long long) * (size_t)maxIter,
+                                cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (hostFlags[1]) return fail(c, SIFV_ERR_CUDA, "Gauss-Seidel wavefront: a wait timed out");
+    iters = maxIter;
+    for (int j = 0; j < maxIter; ++j) {
+        double r;
+        std::memcpy(&r, &c->ctlHost->res[j], sizeof(double));
+        if (r < tol) {
+            iters = j + 1;
+            break;
+        }
+    }
+    k_march_gs_out<<<blocks((long long)P.nxT * P.nyT, kCellThreads), kCellThreads, 0, c->stream>>>(
+        P, c->marchQ[iters % nb], c->marchQ[(iters - 1) % nb], c->F.pA, SW, tr ? 1 : 0);
+    c->launches++;
+    c->gsPrevIters = iters;
+    result = c->F.pA;
+    mark(c, "gauss_seidel");
+    return SIFV_OK;
+}
+
 // GaussSeidelPressureSolver::solve on the device: in place on F.pA (the
 // initial guess), coefficients once per solve, per iteration a scalar ghost
 // fill and one tiled-wavefront sweep; convergence as jacobi_run.
@@ -638,12 +789,33 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
                                                                  total, slowRecs);
         c->launches++;
     }
+    const bool periodic2d = P.bc[0] == SIFV_BC_PERIODIC || P.bc[1] == SIFV_BC_PERIODIC ||
+                            P.bc[2] == SIFV_BC_PERIODIC || P.bc[3] == SIFV_BC_PERIODIC;
+    if (P.dim == 2 && !c->exchangeFaces && maxIter >= 2 && c->marchMode != 0 && (c->marchMode == 1 || periodic2d)) {
+        // the persistent wavefront; the tiled sweeps below overlap many iterations on a mesh without a
+        // periodic face (their iterations lag by 2 tile planes instead of a full row of tiles)
+        const int ms = gs_march(c, rhs, tol, maxIter, iters, result);
+        if (ms != 1) return ms;
+    }
     if (P.dim >= 2 && !c->exchangeFaces && maxIter >= 2) {
-        // overlapped iterations (k_gs_tile_rec_ov, k_gs_tile_ov): iterate n in buf[n % kGsBufs]
-        if (!c->gsBuf[0]) {
+        // overlapped iterations (k_gs_tile_rec_ov, k_gs_tile_ov): iterate n in buf[n % nb], nb = S + 2
+        // for S iterations in flight.  The lag is at least 2 planes and, on a periodic axis, the tiles
+        // along it; in 3D at most three iterations are in flight (a tile plane already fills the GPU),
+        // in 2D as many as the planes allow, within 30 and 1 GiB of extra iterates.
+        int lag = 2;
+        if (P.bc[0] == SIFV_BC_PERIODIC) lag = std::max(lag, ntx);
+        if (P.bc[2] == SIFV_BC_PERIODIC) lag = std::max(lag, nty);
+        if (P.bc[4] == SIFV_BC_PERIODIC) lag = std::max(lag, ntz);
+        const size_t bufBytes = c->ncells * sizeof(double);
+        const int sMax = d3 ? 3 : (int)std::max<size_t>(1, std::min<size_t>(30, (size_t(1) << 30) / bufBytes));
+        lag = std::max(lag, (nplanes + sMax - 1) / sMax);
+        const int S = (nplanes + lag - 1) / lag;
+        const int nb = S + 2;
+        while ((int)c->gsBuf.size() < nb - 2) {
             int sa = SIFV_OK;
-            for (int q = 0; q < kGsBufs - 2; ++q) c->gsBuf[q] = dalloc(c, c->ncells, sa);
+            double* p = dalloc(c, c->ncells, sa);
             if (sa != SIFV_OK) return sa;
+            c->gsBuf.push_back(p);
         }
         if (recs)
             CUDA_TRY(c, cudaFuncSetAttribute(k_gs_tile_rec_ov, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -655,15 +827,10 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
             CUDA_TRY(c, cudaFuncSetAttribute(k_gs_tile_ov<T2X, T2Y, 1>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         GsBufs B{};
+        B.nb = nb;
         B.b[0] = c->F.pA;
         B.b[1] = c->F.pB;
-        for (int q = 0; q < kGsBufs - 2; ++q) B.b[q + 2] = c->gsBuf[q];
-        int lag = 2;
-        if (P.bc[0] == SIFV_BC_PERIODIC) lag = std::max(lag, ntx);
-        if (P.bc[2] == SIFV_BC_PERIODIC) lag = std::max(lag, nty);
-        if (P.bc[4] == SIFV_BC_PERIODIC) lag = std::max(lag, ntz);
-        lag = std::max(lag, (nplanes + 2) / 3);   // at most three iterations in flight
-        const int S = (nplanes + lag - 1) / lag;
+        for (int q = 0; q < nb - 2; ++q) B.b[q + 2] = c->gsBuf[q];
         // the ghost layers the first iteration reads: iterate 0's images in buf 0 and buf 1
         const unsigned gg = blocks(ghost_count(P), kCellThreads);
         k_scalar_ghosts<<<gg, kCellThreads, 0, c->stream>>>(P, B.b[0]);
@@ -683,7 +850,7 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
                 PL.lag = lag;
                 PL.n = s1 - s0 + 1;
                 PL.it0 = s0;
-                PL.S = S;
+                PL.np = nplanes;
                 cudaLaunchAttribute at[1];
                 at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
                 at[0].val.programmaticStreamSerializationAllowed = 1;
@@ -731,9 +898,9 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
         iters = done ? done : maxIter;
         c->gsPrevIters = iters;
         // the result's ghosts as the reference leaves them: filled from the iterate before the last sweep
-        k_scalar_ghosts_from<<<gg, kCellThreads, 0, c->stream>>>(P, B.b[(iters - 1) % kGsBufs], B.b[iters % kGsBufs]);
+        k_scalar_ghosts_from<<<gg, kCellThreads, 0, c->stream>>>(P, B.b[(iters - 1) % nb], B.b[iters % nb]);
         c->launches++;
-        result = B.b[iters % kGsBufs];
+        result = B.b[iters % nb];
         mark(c, "gauss_seidel");
         return SIFV_OK;
     }
@@ -1479,6 +1646,10 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     c->cfg = *cfg;
     c->device = device;
     c->exchangeFaces = exchangeFaces;
+    {
+        const char* e = std::getenv("SIFV_GS_MARCH");
+        c->marchMode = (e && e[0] == '0') ? 0 : (e && e[0] == '1') ? 1 : -1;
+    }
     if (cudaSetDevice(device) != cudaSuccess) { delete c; return fail(nullptr, SIFV_ERR_CUDA, "cudaSetDevice failed"); }
     if (cudaStreamCreateWithFlags(&c->ownStream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;

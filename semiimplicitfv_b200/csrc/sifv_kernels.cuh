@@ -1852,7 +1852,7 @@ constexpr int kIgrRecDoubles = 8;
 #define SIFV_IGR_PREFETCH 2
 #endif
 constexpr int kIgrPrefetch = SIFV_IGR_PREFETCH;  // records in flight ahead of the cell being updated
-constexpr int kIgrMaxSlots = 8;                  // sweeps overlapping in one launch of k_igr_tile_rec
+constexpr int kIgrMaxSlots = 32;                 // sweeps overlapping in one launch of k_igr_tile(_rec)
 constexpr int kIgrRing = kIgrPrefetch + 2;       // ring slots per thread
 
 __host__ __device__ __forceinline__ size_t igr_rec_index(long long tile, int tb, int tc, int n) {
@@ -2109,17 +2109,24 @@ __global__ void k_gs_sweep_1d(Params P, const double* __restrict__ coef, size_t 
     atomicMax(&ctl->res[it], d2bits(maxRes));
 }
 
-constexpr int kGsBufs = 5;
+constexpr int kGsMaxBufs = 34;   // S + 2 buffers for S iterations in flight
 struct GsBufs {
-    double* b[kGsBufs];
+    double* b[kGsMaxBufs];
+    int nb;   // buffers in use
 };
 struct GsPlanes {
     int top;   // tile plane of the first active iteration (slot 0); slot u runs plane top - u lag
     int lag;
     int n;     // active iterations in this launch
     int it0;   // index of the iteration in slot 0
-    int S;     // iterations in flight at most
+    int np;    // tile planes of one iteration
 };
+// The last iteration whose residual is complete when the tile on plane p of
+// iteration it starts: iteration j ends with launch j lag + np - 1, before
+// this tile's launch it lag + p.
+__device__ __forceinline__ int gs_complete_before(const GsPlanes& PL, int it, int p) {
+    return it - (PL.np - p + PL.lag - 1) / PL.lag;
+}
 template <int TX, int TY, int TZ>
 __global__ void __launch_bounds__(TY * TZ) k_gs_tile(Params P, const double* __restrict__ coef, size_t nc,
                                                      const double* __restrict__ rhs, double* __restrict__ p, Ctl* ctl,
@@ -2259,14 +2266,15 @@ __global__ void __launch_bounds__(TY * TZ) k_gs_tile_ov(Params P, const double* 
     const int it = PL.it0 + slot;
     if (threadIdx.x == 0) {
         int s = 0;
-        for (int j = 0; j <= it - PL.S; ++j)
+        const int last = gs_complete_before(PL, it, PL.top - slot * PL.lag);
+        for (int j = 0; j <= last; ++j)
             if (bits2d(ctl->res[j]) < tol) { s = 1; break; }
         skip = s;
     }
     __syncthreads();
     if (skip) return;
-    const double* __restrict__ pOld = B.b[it % kGsBufs];
-    double* __restrict__ pNew = B.b[(it + 1) % kGsBufs];
+    const double* __restrict__ pOld = B.b[it % B.nb];
+    double* __restrict__ pNew = B.b[(it + 1) % B.nb];
     const int i0 = I * TX, j0 = J * TY, k0 = K * TZ;
     const int ex = min(TX, P.nx - i0), ey = min(TY, P.ny - j0), ez = D3 ? min(TZ, P.nz - k0) : 1;
     const int hx = ex + 2, hy = ey + 2, hz = D3 ? ez + 2 : 1;
@@ -2334,7 +2342,7 @@ __global__ void __launch_bounds__(TY * TZ) k_gs_tile_ov(Params P, const double* 
             pNew[cidx(P, i0 + a, j0 + b, k0 + c)] = smem[((c + D3) * HY + (b + 1)) * HX + (a + 1)];
     }
     __syncthreads();   // the tile's new values, written by all warps above
-    gs_tile_ghosts(P, pNew, B.b[(it + 2) % kGsBufs], I, J, K, ntx, nty, ntz, i0, j0, k0, ex, ey, ez);
+    gs_tile_ghosts(P, pNew, B.b[(it + 2) % B.nb], I, J, K, ntx, nty, ntz, i0, j0, k0, ex, ey, ez);
     block_max_to(maxRes, &ctl->res[it]);
 }
 
@@ -2488,7 +2496,7 @@ __global__ void __launch_bounds__(256, 1) k_gs_tile_rec(Params P, const double* 
 // Gauss-Seidel iteration stops on its residual, so the iterations after
 // the current one run speculatively and must not destroy an iterate that
 // turns out to be the answer: iterate n (n = 0 the initial guess) lives in
-// buf[n % kGsBufs], and the iteration producing iterate n + 1 stages its
+// buf[n % B.nb], and the iteration producing iterate n + 1 stages its
 // tile and its downstream face halos (x+, y+, z+) from iterate n and its
 // upstream face halos (x-, y-, z-: upstream tiles of the same iteration,
 // earlier launches) from its own buffer -- in-place Gauss-Seidel's operands
@@ -2497,11 +2505,12 @@ __global__ void __launch_bounds__(256, 1) k_gs_tile_rec(Params P, const double* 
 // their new values -- the low-side ghost layer into the next iteration's
 // buffer, the high-side one into their own (read as downstream halo by the
 // next iteration); periodic images need lag >= tiles along the axis, as
-// for IGR.  With at most S iterations in flight (S = ceil(planes / lag) <=
-// 3), the residuals of iterations m - S and earlier are complete when
-// iteration m starts; its tiles skip when one of them is below tol, so at
-// most S - 1 iterations run past the converged one and never reach its
-// buffer or its predecessor's (five buffers).
+// for IGR.  With at most S iterations in flight (S = ceil(planes / lag)),
+// the residuals of iterations m - S and earlier are complete when iteration
+// m starts, and more of them by its later planes; a tile skips when one of
+// the complete residuals is below tol, so at most S - 1 iterations run past
+// the converged one and never reach its buffer or its predecessor's
+// (S + 2 buffers).
 __global__ void __launch_bounds__(256, 1) k_gs_tile_rec_ov(Params P, const double* __restrict__ rec,
                                                            const int* __restrict__ slowRecs, GsBufs B, Ctl* ctl,
                                                            double tol, GsPlanes PL, int ntx, int nty, int ntz) {
@@ -2519,8 +2528,8 @@ __global__ void __launch_bounds__(256, 1) k_gs_tile_rec_ov(Params P, const doubl
     const int I = PL.top - slot * PL.lag - J - K;
     if (I < 0 || I >= ntx) return;
     const int it = PL.it0 + slot;                    // this tile's iteration: iterate it -> it + 1
-    const double* __restrict__ pOld = B.b[it % kGsBufs];
-    double* __restrict__ pNew = B.b[(it + 1) % kGsBufs];
+    const double* __restrict__ pOld = B.b[it % B.nb];
+    double* __restrict__ pNew = B.b[(it + 1) % B.nb];
     const int tid = (int)threadIdx.x;
     const int i0 = I * T, j0 = J * T, k0 = K * T;
     const int ex = min(T, P.nx - i0), ey = min(T, P.ny - j0), ez = min(T, P.nz - k0);
@@ -2545,9 +2554,10 @@ __global__ void __launch_bounds__(256, 1) k_gs_tile_rec_ov(Params P, const doubl
     const int hLine = ((tc + 1) * HY + (tb + 1)) * HXP + 1 + xoff;
     const size_t gLine = cidx(P, i0, j0 + tb, k0 + tc);
     asm volatile("griddepcontrol.wait;\n" ::: "memory");   // the previous tile planes
-    if (tid == 0) {   // the first converged iteration among those complete before this one started
+    if (tid == 0) {   // a converged iteration among those complete before this tile started
         int s = 0;
-        for (int j = 0; j <= it - PL.S; ++j)
+        const int last = gs_complete_before(PL, it, PL.top - slot * PL.lag);
+        for (int j = 0; j <= last; ++j)
             if (bits2d(ctl->res[j]) < tol) { s = 1; break; }
         skip = s;
     }
@@ -2614,7 +2624,7 @@ __global__ void __launch_bounds__(256, 1) k_gs_tile_rec_ov(Params P, const doubl
     }
     // ghost images of the new values: low side into the next iteration's buffer, high side into this one
     {
-        double* __restrict__ pNext = B.b[(it + 2) % kGsBufs];
+        double* __restrict__ pNext = B.b[(it + 2) % B.nb];
         const size_t sy = (size_t)P.nxT, sz = (size_t)P.nxT * P.nyT;
         {
             const int b = tid % T, c = tid / T;

@@ -113,7 +113,9 @@ def test_igr_record_sweep_3d(nx, ny, nz):
                                         ((50, 40, 18), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_NOSLIPWALL)),
                                         ((35, 40, 33), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_PERIODIC)),
                                         ((100, 140, 1), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_OUTFLOW)),
-                                        ((130, 70, 1), (abi.BC_SLIPWALL, abi.BC_PERIODIC, abi.BC_OUTFLOW))])
+                                        ((130, 70, 1), (abi.BC_SLIPWALL, abi.BC_PERIODIC, abi.BC_OUTFLOW)),
+                                        ((208, 64, 48), (abi.BC_SLIPWALL, abi.BC_OUTFLOW, abi.BC_OUTFLOW)),
+                                        ((600, 520, 1), (abi.BC_OUTFLOW, abi.BC_SLIPWALL, abi.BC_OUTFLOW))])
 def test_igr_overlapped_sweeps_mixed_faces(shape, bcs):
     """Consecutive sweeps overlapped in one launch sequence (sweep s + 1
     trailing sweep s by a fixed number of tile planes, boundary tiles
@@ -121,7 +123,8 @@ def test_igr_overlapped_sweeps_mixed_faces(shape, bcs):
     3D tile sweep of odd row lengths (35 + 6 ghosts) and the 2D 32 x 64 tile
     sweep -- with per-axis boundary kinds (periodic wrap images and
     zero-gradient copies), several tiles along the periodic axes, ragged
-    edges, the 20-sweep warm start: bit-identical to the oracle's
+    edges, more than eight sweeps in one launch (18 and 27 tile planes at a
+    lag of 2), the 20-sweep warm start: bit-identical to the oracle's
     sweep-by-sweep order."""
     cfg, mesh, fields = cases.acoustic_box(*shape)
     mesh.bc = [bcs[0]] * 2 + [bcs[1]] * 2 + [bcs[2]] * 2
@@ -304,18 +307,30 @@ def test_gauss_seidel_pressure_solver(name):
                                         ((64, 32, 32), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_PERIODIC)),
                                         ((35, 40, 33), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_PERIODIC)),
                                         ((100, 140, 1), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_OUTFLOW)),
-                                        ((130, 70, 1), (abi.BC_SLIPWALL, abi.BC_PERIODIC, abi.BC_OUTFLOW))])
+                                        ((130, 70, 1), (abi.BC_SLIPWALL, abi.BC_PERIODIC, abi.BC_OUTFLOW)),
+                                        ((600, 520, 1), (abi.BC_OUTFLOW, abi.BC_SLIPWALL, abi.BC_OUTFLOW)),
+                                        ((330, 200, 1), (abi.BC_OUTFLOW, abi.BC_PERIODIC, abi.BC_OUTFLOW)),
+                                        ((90, 159, 1), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_OUTFLOW))])
 @pytest.mark.parametrize("max_iter,dt,tol", [(1, 1e-2, 1e-14), (2, 1e-2, 1e-14), (3, 1e-2, 1e-14),
                                              (7, 1e-2, 1e-14), (300, 2e-3, 1e-9), (300, 1e-2, 1e-8)])
-def test_gauss_seidel_overlapped_iterations(shape, bcs, max_iter, dt, tol):
+@pytest.mark.parametrize("march", [True, False])
+def test_gauss_seidel_overlapped_iterations(shape, bcs, max_iter, dt, tol, march, monkeypatch):
     """Gauss-Seidel iterations overlapped in one launch sequence (the 3D
     record sweep, the plain 3D sweep of odd row lengths and the 2D 32 x 64
-    tile sweep; iterates rotating through five buffers, speculative
-    iterations past the converged one discarded): per-axis periodic / zero-gradient
-    faces, several tiles along periodic axes, ragged tiles, iteration caps
-    of 1-7 and convergence after a few or many host batches.  The iteration
-    count and the whole returned array -- interior and the ghost layers the
-    reference's last fill leaves -- are the oracle's bit for bit."""
+    tile sweep; iterates rotating through S + 2 buffers for S iterations in
+    flight, 3 in 3D and up to 14 in 2D, speculative iterations past the
+    converged one discarded): per-axis periodic / zero-gradient faces,
+    several tiles along periodic axes, ragged tiles, iteration caps of 1-7
+    and convergence after a few or many host batches.  2D meshes run both
+    2D paths: the persistent wavefront of 32-row warps (k_march_gs, walking
+    along x, or along y when only y is periodic or both are and y is
+    longer; forced with SIFV_GS_MARCH=1) and the tiled sweeps
+    (SIFV_GS_MARCH=0).  The iteration count and the whole returned array --
+    interior and the ghost layers the reference's last fill leaves -- are
+    the oracle's bit for bit."""
+    if shape[2] > 1 and not march:
+        pytest.skip("3D meshes have one path")
+    monkeypatch.setenv("SIFV_GS_MARCH", "1" if march else "0")
     cfg, mesh, fields = cases.acoustic_box(*shape)
     mesh.bc = [bcs[0]] * 2 + [bcs[1]] * 2 + [bcs[2]] * 2
     cg = backends.make(backends.cuda(), (cfg, mesh, fields))
