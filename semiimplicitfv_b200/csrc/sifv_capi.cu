@@ -85,7 +85,8 @@ struct sifv_ctx {
     double* gsRec = nullptr;                  // Gauss-Seidel sweep records (k_gs_records), then one int flag
     std::vector<double*> gsBuf;               // iterate buffers 2 .. of the overlapped Gauss-Seidel sweeps
     double2* marchQ[kMarchMaxBufs] = {};     // 2D Gauss-Seidel wavefront: iterates (skewed pair layout)
-    double* marchRec = nullptr;               // its records
+    double* marchRec = nullptr;               // its records (Gauss-Seidel)
+    double* marchRecIgr = nullptr;            // its records (IGR)
     int* marchInt = nullptr;                  // progress [G], flags [2], slowRecs [1], done [marchIntCap]
     int marchIntCap = -1;
     int marchOk = -1;                         // -1 unknown, 0 no cooperative launch, 1 usable
@@ -358,6 +359,9 @@ int exchange_fields(sifv_ctx* c, double* const* fields, int n);
 int exchange_scalar(sifv_ctx* c, const double* f);
 int reduce_residual(sifv_ctx* c, unsigned long long* slot);
 
+int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter, int& iters,
+              const double*& result);
+
 int igr_solve(sifv_ctx* c, int step) {
     const Params& P = c->P;
     k_igr_setup<<<blocks((long long)c->nint, kCellThreads), kCellThreads, 0, c->stream>>>(P, c->F, c->alphaIGR);
@@ -406,6 +410,21 @@ int igr_solve(sifv_ctx* c, int step) {
     // planes, at least 2 (no face-adjacent tiles in one launch) and, on a
     // periodic axis, the tiles along it (the wrap-around ghost images of
     // sweep s are final before sweep s + 1 reads them).
+    const bool periodic2d = P.bc[0] == SIFV_BC_PERIODIC || P.bc[1] == SIFV_BC_PERIODIC ||
+                            P.bc[2] == SIFV_BC_PERIODIC || P.bc[3] == SIFV_BC_PERIODIC;
+    if (P.dim == 2 && iters > 1 && !c->exchangeFaces && !c->ib.count && !c->F.solid && c->marchMode != 0 &&
+        (c->marchMode == 1 || periodic2d)) {
+        // the persistent wavefront (all sweeps in one launch); the tiled sweeps below overlap well only
+        // without a periodic face
+        int done = 0;
+        const double* res = nullptr;
+        const int ms = march_run(c, 1, nullptr, 0.0, iters, done, res);
+        if (ms == SIFV_OK) {
+            mark(c, "igr");
+            return SIFV_OK;
+        }
+        if (ms != 1) return ms;
+    }
     if (P.dim >= 2 && iters > 1 && !c->exchangeFaces && !c->ib.count) {
         int lag = 2;
         if (P.bc[0] == SIFV_BC_PERIODIC) lag = std::max(lag, ntx);
@@ -595,14 +614,18 @@ int jacobi_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double
     return SIFV_OK;
 }
 
-// The 2D iterations as one persistent wavefront (k_march_gs): records and
-// iterate 0 from the coefficients (c->gsCoef) and F.pA, one cooperative
-// launch for all iterations, the iteration count from the per-sweep
-// residuals, the result back into F.pA.  The warps walk along a periodic
-// axis (free for the wavefront), along the longer one when both are
+// 2D sweeps as one persistent wavefront (k_march_gs): records and iterate 0,
+// one cooperative launch for all sweeps, the result back in the mesh layout.
+// kind 0: Gauss-Seidel pressure iterations from c->gsCoef, rhs and F.pA
+// (result in F.pA, the iteration count from the per-sweep residuals; the
+// ghost layers from the iterate before the last sweep, as the reference's
+// last fill leaves them).  kind 1: `maxIter` IGR sweeps on F.sigma (ghost
+// layers filled from the result, src/IGR.cpp:155).  The warps walk along a
+// periodic axis (free for the wavefront), along the longer one when both are
 // periodic.  Returns 1 (nothing done) when the launch does not fit the
 // device or the progress counters would overflow.
-int gs_march(sifv_ctx* c, const double* rhs, double tol, int maxIter, int& iters, const double*& result) {
+int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter, int& iters,
+              const double*& result) {
     const Params& P = c->P;
     const bool px = P.bc[0] == SIFV_BC_PERIODIC || P.bc[1] == SIFV_BC_PERIODIC;
     const bool py = P.bc[2] == SIFV_BC_PERIODIC || P.bc[3] == SIFV_BC_PERIODIC;
@@ -614,25 +637,29 @@ int gs_march(sifv_ctx* c, const double* rhs, double tol, int maxIter, int& iters
     const int G = Nn / 32 + 1, GA = (Nn + 1) / 32 + 1;
     const int ctas = (G + kMarchWarps - 1) / kMarchWarps;
     if ((long long)(maxIter + 2) * NS >= (1LL << 30)) return 1;
-    // the four instances: batch length 8 or 4 (periodic row axis), walking along x or y
+    // instances: Gauss-Seidel with batch length 8 or 4, IGR with 4 (its records fill the shared memory),
+    // each walking along x or y
     using MarchFn = void (*)(Params, GsMarch, Ctl*);
-    const MarchFn fns[4] = {k_march_gs<kMarchWarps, 8, false>, k_march_gs<kMarchWarps, 8, true>,
-                            k_march_gs<kMarchWarps, 4, false>, k_march_gs<kMarchWarps, 4, true>};
-    // D = 4 when a periodic row axis makes the groups' lags (about 32 + 2 D + 10 steps each) longer than
-    // a sweep; otherwise D = 8
+    const MarchFn fns[6] = {k_march_gs<kMarchWarps, 8, false, 0>, k_march_gs<kMarchWarps, 8, true, 0>,
+                            k_march_gs<kMarchWarps, 4, false, 0>, k_march_gs<kMarchWarps, 4, true, 0>,
+                            k_march_gs<kMarchWarps, 4, false, 1>, k_march_gs<kMarchWarps, 4, true, 1>};
+    const int fnD[6] = {8, 8, 4, 4, 4, 4}, fnKind[6] = {0, 0, 0, 0, 1, 1};
+    // Gauss-Seidel: D = 4 when a periodic row axis makes the groups' lags (about 32 + 2 D + 10 steps
+    // each) longer than a sweep; otherwise D = 8
     const bool rowPeriodic = bn0 == SIFV_BC_PERIODIC || bn1 == SIFV_BC_PERIODIC;
     const bool short8 = rowPeriodic && (long long)G * (32 + 2 * 8 + 10) > NS;
-    const int D = short8 ? 4 : 8;
-    const MarchFn fn = fns[(short8 ? 2 : 0) + (tr ? 1 : 0)];
-    const size_t smem = march_smem(D);
+    const int fi = (kind ? 4 : short8 ? 2 : 0) + (tr ? 1 : 0);
+    const int D = fnD[fi];
+    const MarchFn fn = fns[fi];
+    const size_t smem = march_smem(D, kind);
     if (c->marchOk < 0) {
         c->marchOk = 0;
         int coop = 0, sms = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
         long long fit = -1;
-        for (int q = 0; q < 4 && coop; ++q) {
-            const size_t sq = march_smem(q < 2 ? 8 : 4);
+        for (int q = 0; q < 6 && coop; ++q) {
+            const size_t sq = march_smem(fnD[q], fnKind[q]);
             int perSm = 0;
             if (cudaFuncSetAttribute(fns[q], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sq) != cudaSuccess ||
                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fns[q], 32 * (kMarchWarps + 1), sq) !=
@@ -655,8 +682,9 @@ int gs_march(sifv_ctx* c, const double* rhs, double tol, int maxIter, int& iters
     int nb = std::min(kMarchMaxBufs, 4 + (G * (32 + 2 * D + 40) + NS - 1) / NS);
     nb = std::max(3, std::min<int>(nb, (int)((size_t(1) << 30) / (qn * sizeof(double2)))));
     int sa = SIFV_OK;
-    if (!c->marchRec) {
-        c->marchRec = dalloc(c, qn * 16, sa);   // 8 double2 per pair
+    double*& recBuf = kind ? c->marchRecIgr : c->marchRec;
+    if (!recBuf) {
+        recBuf = dalloc(c, qn * 4 * march_chunks(kind), sa);   // 2 cells x chunks double2 per pair
         if (sa != SIFV_OK) return sa;
     }
     for (int q = 0; q < nb; ++q)
@@ -676,11 +704,15 @@ int gs_march(sifv_ctx* c, const double* rhs, double tol, int maxIter, int& iters
     int* done = slowRecs + 1;
     CUDA_TRY(c, cudaMemsetAsync(c->marchInt, 0, sizeof(int) * ((size_t)G + 3 + maxIter), c->stream));
     const long long total = (long long)qn;
-    k_march_gs_setup<<<blocks(total, 256), 256, 0, c->stream>>>(P, c->gsCoef, c->ncells, rhs, c->F.pA,
-                                                               reinterpret_cast<double2*>(c->marchRec), c->marchQ[0],
-                                                               SW, total, slowRecs, tr ? 1 : 0);
+    if (kind)
+        k_march_igr_setup<<<blocks(total, 256), 256, 0, c->stream>>>(P, c->F, reinterpret_cast<double2*>(recBuf),
+                                                                    c->marchQ[0], SW, total, slowRecs, tr ? 1 : 0);
+    else
+        k_march_gs_setup<<<blocks(total, 256), 256, 0, c->stream>>>(P, c->gsCoef, c->ncells, rhs, c->F.pA,
+                                                                   reinterpret_cast<double2*>(recBuf), c->marchQ[0],
+                                                                   SW, total, slowRecs, tr ? 1 : 0);
     GsMarch M{};
-    M.rec = reinterpret_cast<const double2*>(c->marchRec);
+    M.rec = reinterpret_cast<const double2*>(recBuf);
     for (int q = 0; q < nb; ++q) M.q[q] = c->marchQ[q];
     M.prog = prog;
     M.done = done;
@@ -700,6 +732,7 @@ int gs_march(sifv_ctx* c, const double* rhs, double tol, int maxIter, int& iters
     M.perLoY = bn0 == SIFV_BC_PERIODIC;
     M.perHiY = bn1 == SIFV_BC_PERIODIC;
     M.tol = tol;
+    M.ghost0 = c->F.sigma;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeCooperative;
     at[0].val.cooperative = 1;
@@ -715,12 +748,13 @@ int gs_march(sifv_ctx* c, const double* rhs, double tol, int maxIter, int& iters
     LAUNCH_CHECK(c);
     int hostFlags[2] = {0, 0};
     CUDA_TRY(c, cudaMemcpyAsync(hostFlags, flags, sizeof(hostFlags), cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl) + sizeof(unsigned long long) * (size_t)maxIter,
-                                cudaMemcpyDeviceToHost, c->stream));
+    if (!kind)
+        CUDA_TRY(c, cudaMemcpyAsync(c->ctlHost, c->ctl, sizeof(Ctl) + sizeof(unsigned long long) * (size_t)maxIter,
+                                    cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    if (hostFlags[1]) return fail(c, SIFV_ERR_CUDA, "Gauss-Seidel wavefront: a wait timed out");
+    if (hostFlags[1]) return fail(c, SIFV_ERR_CUDA, "2D sweep wavefront: a wait timed out");
     iters = maxIter;
-    for (int j = 0; j < maxIter; ++j) {
+    for (int j = 0; !kind && j < maxIter; ++j) {
         double r;
         std::memcpy(&r, &c->ctlHost->res[j], sizeof(double));
         if (r < tol) {
@@ -728,12 +762,11 @@ int gs_march(sifv_ctx* c, const double* rhs, double tol, int maxIter, int& iters
             break;
         }
     }
+    double* out = kind ? c->F.sigma : c->F.pA;
     k_march_gs_out<<<blocks((long long)P.nxT * P.nyT, kCellThreads), kCellThreads, 0, c->stream>>>(
-        P, c->marchQ[iters % nb], c->marchQ[(iters - 1) % nb], c->F.pA, SW, tr ? 1 : 0);
+        P, c->marchQ[iters % nb], c->marchQ[(kind ? iters : iters - 1) % nb], out, SW, tr ? 1 : 0);
     c->launches++;
-    c->gsPrevIters = iters;
-    result = c->F.pA;
-    mark(c, "gauss_seidel");
+    result = out;
     return SIFV_OK;
 }
 
@@ -794,7 +827,11 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
     if (P.dim == 2 && !c->exchangeFaces && maxIter >= 2 && c->marchMode != 0 && (c->marchMode == 1 || periodic2d)) {
         // the persistent wavefront; the tiled sweeps below overlap many iterations on a mesh without a
         // periodic face (their iterations lag by 2 tile planes instead of a full row of tiles)
-        const int ms = gs_march(c, rhs, tol, maxIter, iters, result);
+        const int ms = march_run(c, 0, rhs, tol, maxIter, iters, result);
+        if (ms == SIFV_OK) {
+            c->gsPrevIters = iters;
+            mark(c, "gauss_seidel");
+        }
         if (ms != 1) return ms;
     }
     if (P.dim >= 2 && !c->exchangeFaces && maxIter >= 2) {

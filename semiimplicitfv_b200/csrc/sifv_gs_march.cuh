@@ -81,13 +81,17 @@ struct GsMarch {
     int xsLo, xsHi;              // source cells of the ghosts along the march axis
     int perLoY, perHiY;          // the ghost rows across the row axis wrap around
     double tol;
+    const double* ghost0;        // IGR: the stored field, whose ghost cells sweep 0 reads
 };
 
 __host__ __device__ __forceinline__ size_t march_q(int SW, int g, int s, int b) {
     return ((size_t)g * SW + s) * 32 + b;
 }
-inline size_t march_smem(int D) {
-    return ((size_t)kMarchWarps * 2 * D * 8 * 32 + (size_t)kMarchWarps * kMarchRE) * sizeof(double2);
+// record chunks (16 bytes) per cell: Gauss-Seidel 4, IGR 7
+__host__ __device__ constexpr int march_chunks(int kind) { return kind ? 7 : 4; }
+inline size_t march_smem(int D, int kind) {
+    return ((size_t)kMarchWarps * 2 * D * 2 * march_chunks(kind) * 32 + (size_t)kMarchWarps * kMarchRE) *
+           sizeof(double2);
 }
 
 __device__ __forceinline__ unsigned long long march_now() {
@@ -137,6 +141,79 @@ __device__ __forceinline__ double march_cell(bool act, bool fastRecs, double2 c0
     return (fastRecs && igr_fast_operand(num)) ? div_markstein(num, dv, rdv) : div_rn_plain(num, dv);
 }
 
+// The IGR update of one cell (igr_cell, src/IGR.cpp:110-156, 2D) from its
+// record r (face densities and their reciprocals per face, the metric
+// weights, rhs, diagonal and its reciprocal) and the four sigma neighbours:
+// div_markstein's correctly rounded quotients when every operand and
+// reciprocal is in range, plain divisions otherwise.  Inactive cells take
+// the fast path on whatever they hold (their result is discarded).
+__device__ __noinline__ double igr_cell_plain2(double sxm, double sxp, double sym, double syp, double rflx, double rfrx,
+                                               double rfly, double rfry, double ax, double ay, double rhs,
+                                               double diag) {
+    double off = 0.0;
+    off += ax * (sxm / rflx + sxp / rfrx);
+    off += ay * (sym / rfly + syp / rfry);
+    return (rhs + off) / diag;
+}
+template <bool TR>
+__device__ __forceinline__ double igr_march_cell(bool act, bool fastRecs, const double2* r, double pL, double pR,
+                                                 double pD, double pU) {
+    const double sxm = TR ? pD : pL, sxp = TR ? pU : pR, sym = TR ? pL : pD, syp = TR ? pR : pU;
+    if (!act || (fastRecs && igr_fast_operand(sxm) && igr_fast_operand(sxp) && igr_fast_operand(sym) &&
+                 igr_fast_operand(syp))) {
+        double off = 0.0;
+        off += r[4].x * (div_markstein(sxm, r[0].x, r[0].y) + div_markstein(sxp, r[1].x, r[1].y));
+        off += r[4].y * (div_markstein(sym, r[2].x, r[2].y) + div_markstein(syp, r[3].x, r[3].y));
+        const double num = r[5].x + off;
+        return (!act || igr_fast_operand(num)) ? div_markstein(num, r[5].y, r[6].x) : div_rn_plain(num, r[5].y);
+    }
+    return igr_cell_plain2(sxm, sxp, sym, syp, r[0].x, r[1].x, r[2].x, r[3].x, r[4].x, r[4].y, r[5].x, r[5].y);
+}
+
+// IGR records and iterate 0 (interior pairs, and the stored first ghost
+// layer in the ghost rows' slots, which sweep 0 reads).  Record of a cell:
+// (rho_f, 1 / rho_f) of the x-, x+, y-, y+ faces with the sweep's
+// expressions 0.5 (rho_i + rho_nb), (ax, ay), (rhs, diag), (1 / diag, 0).
+__global__ void k_march_igr_setup(Params P, Fields F, double2* __restrict__ rec, double2* __restrict__ q0, int SW,
+                                  long long total, int* __restrict__ slowRecs, int tr) {
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= total) return;
+    const int b = (int)(id & 31);
+    const long long gs = id >> 5;
+    const int s = (int)(gs % SW), g = (int)(gs / SW);
+    const int h = s - b, n = 32 * g + b - 1;
+    const int Nm = tr ? P.ny : P.nx, Nn = tr ? P.nx : P.ny;
+    double v[2] = {0.0, 0.0};
+    if (n >= -1 && n <= Nn && h >= 0 && 2 * h < Nm) {
+        const size_t sy = (size_t)P.nxT;
+        for (int e = 0; e < 2; ++e) {
+            const int m = 2 * h + e;
+            if (m >= Nm) break;
+            const int i = tr ? n : m, j = tr ? m : n;
+            const size_t c = cidx(P, i, j, 0);
+            v[e] = F.sigma[c];
+            if (n < 0 || n >= Nn) continue;   // a ghost row: its stored value only
+            const double rho_i = F.rho[c];
+            const double rflx = 0.5 * (rho_i + F.rho[c - 1]), rfrx = 0.5 * (rho_i + F.rho[c + 1]);
+            const double rfly = 0.5 * (rho_i + F.rho[c - sy]), rfry = 0.5 * (rho_i + F.rho[c + sy]);
+            const double rxl = 1.0 / rflx, rxr = 1.0 / rfrx, ryl = 1.0 / rfly, ryr = 1.0 / rfry;
+            const double diag = F.igrDiag[c], rd = 1.0 / diag;
+            double2* o = rec + ((size_t)gs * 14 + 7 * e) * 32 + b;
+            o[0] = make_double2(rflx, rxl);
+            o[32] = make_double2(rfrx, rxr);
+            o[64] = make_double2(rfly, ryl);
+            o[96] = make_double2(rfry, ryr);
+            o[128] = make_double2(F.adx2[i + P.ngx], F.ady2[j + P.ngy]);
+            o[160] = make_double2(F.igrRhs[c], diag);
+            o[192] = make_double2(rd, 0.0);
+            if (!(igr_fast_recip(rxl) && igr_fast_recip(rxr) && igr_fast_recip(ryl) && igr_fast_recip(ryr) &&
+                  igr_fast_recip(rd)))
+                atomicOr(slowRecs, 1);
+        }
+    }
+    q0[id] = make_double2(v[0], v[1]);
+}
+
 // Records and iterate 0 (interior pairs; ghost cells are read from their sources).
 __global__ void k_march_gs_setup(Params P, const double* __restrict__ coef, size_t nc, const double* __restrict__ rhs,
                                  const double* __restrict__ p0, double2* __restrict__ rec, double2* __restrict__ q0,
@@ -183,12 +260,15 @@ __global__ void k_march_gs_out(Params P, const double2* __restrict__ qFin, const
     out[cidx(P, i, j, 0)] = (m & 1) ? v.y : v.x;
 }
 
-template <int W, int D, bool TR>
+// KIND 0: Gauss-Seidel pressure iterations (residual, convergence);
+// KIND 1: IGR sweeps (a fixed count; sweep 0 reads the stored ghost cells).
+template <int W, int D, bool TR, int KIND>
 __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch M, Ctl* ctl) {
     constexpr int R = 2 * D, RE = kMarchRE;
+    constexpr int CH = march_chunks(KIND), PC = 2 * CH;   // record chunks per cell and per pair
     extern __shared__ __align__(16) unsigned char marchSmem[];
-    double2* ringAll = reinterpret_cast<double2*>(marchSmem);   // [W][R][8][32]
-    double2* eRing = ringAll + (size_t)W * R * 8 * 32;          // [W][RE]
+    double2* ringAll = reinterpret_cast<double2*>(marchSmem);   // [W][R][PC][32]
+    double2* eRing = ringAll + (size_t)W * R * PC * 32;         // [W][RE]
     __shared__ volatile int sp[W];    // compute progress (this CTA)
     __shared__ volatile int pub[W];   // the same, once visible device-wide
     __shared__ volatile int ext[3];   // device-wide progress of the group below the CTA, above it, top row's group
@@ -253,7 +333,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
 
     const int g = c * W + warp;
     if (g >= M.G) return;
-    double2* ring = ringAll + (size_t)warp * R * 8 * 32 + lane;   // slot q, chunk ch at ring[(8 q + ch) 32]
+    double2* ring = ringAll + (size_t)warp * R * PC * 32 + lane;   // slot q, chunk ch at ring[(PC q + ch) 32]
     double2* eMine = eRing + (size_t)warp * RE;
     const double2* eBelow = eRing + (size_t)(warp > 0 ? warp - 1 : 0) * RE;
     const int r = 32 * g + lane;
@@ -313,7 +393,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
                 }
             }
             if (go) __threadfence();
-            while (go && chk < k) {
+            while (KIND == 0 && go && chk < k) {
                 if (*(volatile int*)&M.done[chk] < M.G) break;
                 __threadfence();
                 if (bits2d(*(volatile unsigned long long*)&ctl->res[chk]) < M.tol) {
@@ -331,21 +411,40 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
         double2* __restrict__ Qn = M.q[(k + 1) % M.nb];
         const double2* rowK = Qk + march_q(SW, g, 0, lane);   // slot s at rowK[32 s]
         double2* outP = Qn + march_q(SW, g, 0, lane);         // step t's pair at outP[32 t]
-        const double2* recP = M.rec + march_q(SW, g, 0, 0) * 8 + lane;   // step t, chunk ch at recP[(8 t + ch) 32]
+        const double2* recP = M.rec + march_q(SW, g, 0, 0) * PC + lane;   // step t, chunk ch at recP[(PC t + ch) 32]
+        // IGR sweep 0 reads the ghost cells as stored (the ghost rows' own slots, the stored ghost columns);
+        // every other sweep reads them from their source cells in iterate k
+        const bool stored0 = KIND == 1 && k == 0;
         // own pair of step t at pP[32 t]
         const double2* pP = rowK;
-        if (lowGhostLane && !M.perLoY) pP = Qk + march_q(SW, 0, 1, 1);   // row 0's pair h = t
-        if (topGhostLane)
-            pP = M.perHiY ? Qk + march_q(SW, 0, 1, 1) - 32 * (ptrdiff_t)bT   // row 0's pair h = t + 1 - bT
-                          : Qk + march_q(SW, gT, 0, bT - 1) - 32;           // row ny - 1's pair h = t + 1 - bT
+        int pLoK = pLo;
+        if (!stored0) {
+            if (lowGhostLane && !M.perLoY) pP = Qk + march_q(SW, 0, 1, 1);   // row 0's pair h = t
+            if (topGhostLane)
+                pP = M.perHiY ? Qk + march_q(SW, 0, 1, 1) - 32 * (ptrdiff_t)bT   // row 0's pair h = t + 1 - bT
+                              : Qk + march_q(SW, gT, 0, bT - 1) - 32;           // row ny - 1's pair h = t + 1 - bT
+        } else {
+            pLoK = 0;
+        }
         const double2* eP = (eKind == 1)   ? Qn + march_q(SW, g - 1, 31, 31)
                             : (eKind == 2) ? Qk + march_q(SW, topG, topB, topB)
                             : (eKind == 3) ? Qk + march_q(SW, g + 1, 0, 0) - 32 * 31
-                            : (eKind == 4) ? (M.perHiY ? Qk + march_q(SW, 0, 1, 1) - 32 * 31 : rowK)
+                            : (eKind == 4) ? (stored0 ? Qk + march_q(SW, g + 1, 0, 0) - 32 * 31
+                                              : M.perHiY ? Qk + march_q(SW, 0, 1, 1) - 32 * 31 : rowK)
                                            : rowK;
+        const bool lowFromEdge = M.perLoY && !stored0;   // the low ghost pair from row ny - 1
         // the ghost columns of this row in iterate k: sources xsLo, xsHi
-        const double2 gLp = __ldcg(rowK + 32 * ((M.xsLo >> 1) + lane)), gRp = __ldcg(rowK + 32 * ((M.xsHi >> 1) + lane));
-        const double gL = (M.xsLo & 1) ? gLp.y : gLp.x, gR = (M.xsHi & 1) ? gRp.y : gRp.x;
+        double gL, gR;
+        if (stored0) {
+            const int n = r - 1, nn = rowIn ? n : 0, Nm = M.nx;
+            gL = M.ghost0[TR ? cidx(P, nn, -1, 0) : cidx(P, -1, nn, 0)];
+            gR = M.ghost0[TR ? cidx(P, nn, Nm, 0) : cidx(P, Nm, nn, 0)];
+        } else {
+            const double2 gLp = __ldcg(rowK + 32 * ((M.xsLo >> 1) + lane));
+            const double2 gRp = __ldcg(rowK + 32 * ((M.xsHi >> 1) + lane));
+            gL = (M.xsLo & 1) ? gLp.y : gLp.x;
+            gR = (M.xsHi & 1) ? gRp.y : gRp.x;
+        }
         const int eOff = base & (RE - 1);
 
         // lane 0 waits before using steps up to tu and prefetching edges up to tp
@@ -354,7 +453,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
             if (lane == 0) {
                 const int n0 = (warp > 0) ? base + min(tu + 32, NS) : -1;
                 const int n1 = (warp == 0 && g > 0) ? base + min(tp + 32, NS) : -1;
-                const int n2 = (g == 0 && M.perLoY && topG != 0) ? prevBase + min(tp + topB + 1, NS) : -1;
+                const int n2 = (g == 0 && lowFromEdge && topG != 0) ? prevBase + min(tp + topB + 1, NS) : -1;
                 const int n3 = (hasAbove && tp - 30 > 0) ? prevBase + min(tp - 30, NS) : -1;
                 const int n4 = (warp < W - 1 && hasAbove) ? base + tu - 30 - RE : -1;
                 auto met = [&]() {
@@ -382,13 +481,13 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
         };
         // the records of the batch of steps t0 .. t0 + D - 1 into ring slots (t0 mod 2 D) .. + D - 1, one group
         auto issue_records = [&](int t0) {
-            double2* dst = ring + (size_t)(t0 & (R - 1)) * 8 * 32;
-            const double2* src = recP + (size_t)t0 * 8 * 32;
+            double2* dst = ring + (size_t)(t0 & (R - 1)) * PC * 32;
+            const double2* src = recP + (size_t)t0 * PC * 32;
 #pragma unroll
             for (int u = 0; u < D; ++u)
                 if (t0 + u < NS) {
 #pragma unroll
-                    for (int ch = 0; ch < 8; ++ch) cp_async16(dst + (8 * u + ch) * 32, src + (8 * u + ch) * 32);
+                    for (int ch = 0; ch < PC; ++ch) cp_async16(dst + (PC * u + ch) * 32, src + (PC * u + ch) * 32);
                 }
             cp_async_commit();
         };
@@ -401,7 +500,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
         for (int u = 0; u < D; ++u) {
             pr[u] = make_double2(0.0, 0.0);
             er[u] = make_double2(0.0, 0.0);
-            march_ld(pr[u], pP + 32 * u, u >= pLo);
+            march_ld(pr[u], pP + 32 * u, u >= pLoK);
             march_ld(er[u], eP + 32 * u, (unsigned)(u - eLo) < (unsigned)(eHi - eLo));
         }
         double2 newPair = make_double2(0.0, 0.0);
@@ -410,7 +509,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
             if (!batch_wait(t0 + D - 1, t0 + 2 * D - 1)) { ok = false; break; }
             issue_records(t0 + D);        // the next batch (slots of the batch before this one)
             cp_async_wait_group<1>();     // this batch's records landed
-            const double2* rb = ring + (size_t)(t0 & (R - 1)) * 8 * 32;
+            const double2* rb = ring + (size_t)(t0 & (R - 1)) * PC * 32;
             const double2* pPb = pP + 32 * (size_t)(t0 + D);
             const double2* ePb = eP + 32 * (size_t)(t0 + D);
             double2* outB = outP + 32 * (size_t)t0;
@@ -422,34 +521,42 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
                     const double2 Pn = pr[(u + 1) % D];       // old pair h + 1
                     const double2 eg = er[u];
                     const int tn = t + D;
-                    march_ld(pr[u], pPb + 32 * u, tn < NS && tn >= pLo);
+                    march_ld(pr[u], pPb + 32 * u, tn < NS && tn >= pLoK);
                     march_ld(er[u], ePb + 32 * u, tn < NS && (unsigned)(tn - eLo) < (unsigned)(eHi - eLo));
                     const double2 up = march_shfl_up(newPair);
                     const double2 down = march_shfl_down(Pn);
                     const double2 eb = eBelow[(eOff + t) & (RE - 1)];
                     const double2 pD = (lane == 0) ? (eBelowLane ? eb : eg) : up;
                     const double2 pU = (lane == 31) ? eg : down;
-                    const double2 a0 = rb[(8 * u) * 32], a1 = rb[(8 * u + 1) * 32], a2 = rb[(8 * u + 2) * 32],
-                                  a3 = rb[(8 * u + 3) * 32];
-                    const double2 b0 = rb[(8 * u + 4) * 32], b1 = rb[(8 * u + 5) * 32], b2 = rb[(8 * u + 6) * 32],
-                                  b3 = rb[(8 * u + 7) * 32];
+                    double2 ra[CH], rc[CH];   // records of the pair's two cells
+#pragma unroll
+                    for (int ch = 0; ch < CH; ++ch) {
+                        ra[ch] = rb[(PC * u + ch) * 32];
+                        rc[ch] = rb[(PC * u + CH + ch) * 32];
+                    }
                     const bool act0 = t >= tAct0 && t < tAct1;
                     const bool act1 = act0 && !(t == tLast && !lastOdd);   // the pair's second cell exists
                     // cell 2h: left is the previous pair's second cell (ghost at h = 0), right the pair's second
                     // cell (ghost past the last cell)
                     const double pL0 = (t == lane) ? gL : newPair.y;
                     const double pR0 = (t == tLast && !lastOdd) ? gR : Pt.y;
-                    const double pn0 = march_cell<TR>(act0, fastRecs, a0, a1, a2, a3, pL0, pR0, pD.x, pU.x);
+                    const double pn0 = KIND == 0 ? march_cell<TR>(act0, fastRecs, ra[0], ra[1], ra[2], ra[3], pL0, pR0,
+                                                                  pD.x, pU.x)
+                                                 : igr_march_cell<TR>(act0, fastRecs, ra, pL0, pR0, pD.x, pU.x);
                     // cell 2h + 1: left is cell 2h's new value, right the next pair's first cell
                     const double pR1 = (t == tLast) ? gR : Pn.x;
-                    const double pn1 = march_cell<TR>(act1, fastRecs, b0, b1, b2, b3, pn0, pR1, pD.y, pU.y);
+                    const double pn1 = KIND == 0 ? march_cell<TR>(act1, fastRecs, rc[0], rc[1], rc[2], rc[3], pn0, pR1,
+                                                                  pD.y, pU.y)
+                                                 : igr_march_cell<TR>(act1, fastRecs, rc, pn0, pR1, pD.y, pU.y);
                     const double2 pn = make_double2(pn0, pn1);
-                    maxRes = act0 ? smax(maxRes, fabs(pn0 - Pt.x)) : maxRes;
-                    maxRes = act1 ? smax(maxRes, fabs(pn1 - Pt.y)) : maxRes;
+                    if (KIND == 0) {
+                        maxRes = act0 ? smax(maxRes, fabs(pn0 - Pt.x)) : maxRes;
+                        maxRes = act1 ? smax(maxRes, fabs(pn1 - Pt.y)) : maxRes;
+                    }
                     march_st(outB + 32 * u, pn, act0);
                     march_sts(eMine + ((eOff + t - 31) & (RE - 1)), pn, act0 && eWriter);
                     // the low ghost lane hands lane 1 the ghost pair h = t
-                    newPair = act0 ? pn : (lowGhostLane ? (M.perLoY ? eg : Pt) : newPair);
+                    newPair = act0 ? pn : (lowGhostLane ? (lowFromEdge ? eg : Pt) : newPair);
                 }
             }
             asm volatile("" ::: "memory");
@@ -468,7 +575,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
         for (int o = 16; o > 0; o >>= 1) v = smax(v, __shfl_xor_sync(0xffffffffu, v, o));
         __syncwarp();
         if (lane == 0) {
-            atomicMax(&ctl->res[k], d2bits(v));
+            if (KIND == 0) atomicMax(&ctl->res[k], d2bits(v));
             __threadfence();
             atomicAdd(&M.done[k], 1);
         }
