@@ -115,8 +115,10 @@ def test_igr_record_sweep_3d(nx, ny, nz):
                                         ((100, 140, 1), (abi.BC_PERIODIC, abi.BC_OUTFLOW, abi.BC_OUTFLOW)),
                                         ((130, 70, 1), (abi.BC_SLIPWALL, abi.BC_PERIODIC, abi.BC_OUTFLOW)),
                                         ((208, 64, 48), (abi.BC_SLIPWALL, abi.BC_OUTFLOW, abi.BC_OUTFLOW)),
-                                        ((600, 520, 1), (abi.BC_OUTFLOW, abi.BC_SLIPWALL, abi.BC_OUTFLOW))])
-def test_igr_overlapped_sweeps_mixed_faces(shape, bcs):
+                                        ((600, 520, 1), (abi.BC_OUTFLOW, abi.BC_SLIPWALL, abi.BC_OUTFLOW)),
+                                        ((90, 159, 1), (abi.BC_PERIODIC, abi.BC_PERIODIC, abi.BC_OUTFLOW))])
+@pytest.mark.parametrize("march", [True, False])
+def test_igr_overlapped_sweeps_mixed_faces(shape, bcs, march, monkeypatch):
     """Consecutive sweeps overlapped in one launch sequence (sweep s + 1
     trailing sweep s by a fixed number of tile planes, boundary tiles
     refreshing the ghost layer themselves) -- the 3D record sweep, the plain
@@ -125,7 +127,11 @@ def test_igr_overlapped_sweeps_mixed_faces(shape, bcs):
     zero-gradient copies), several tiles along the periodic axes, ragged
     edges, more than eight sweeps in one launch (18 and 27 tile planes at a
     lag of 2), the 20-sweep warm start: bit-identical to the oracle's
-    sweep-by-sweep order."""
+    sweep-by-sweep order.  2D meshes run both 2D paths: the persistent
+    wavefront (SIFV_GS_MARCH=1) and the tiled sweeps (SIFV_GS_MARCH=0)."""
+    if shape[2] > 1 and not march:
+        pytest.skip("3D meshes have one path")
+    monkeypatch.setenv("SIFV_GS_MARCH", "1" if march else "0")
     cfg, mesh, fields = cases.acoustic_box(*shape)
     mesh.bc = [bcs[0]] * 2 + [bcs[1]] * 2 + [bcs[2]] * 2
     check((cfg, mesh, fields), 2)
