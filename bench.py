@@ -9,7 +9,9 @@ fields the step reads are copied from pinned host buffers (sifv_set_field),
 sifv_step runs and returns dt, and the fields it writes are copied back
 (sifv_get_field).  The same JSON line carries the other workloads as
 objects: `semi_implicit` (3D acoustic pulse 256^3 with IGR and the Jacobi
-pressure solve), `adjoint` (isentropic-vortex discrete adjoint 512^2) and
+pressure solve), `semi_implicit_2d_periodic` (2D 2048^2 periodic with IGR
+and the Gauss-Seidel pressure solve, the 2D wavefront kernels against the
+tiled sweeps), `adjoint` (isentropic-vortex discrete adjoint 512^2) and
 `ensemble` (2048 two-phase water-air tubes in one launch).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
@@ -83,6 +85,7 @@ ENS_BYTES_PER_CELL_UPDATE = 384   # state alphaRho0, alphaRho1, rhoU, rhoE, alph
 # Semi-implicit 3D acoustic pulse with IGR, 256^3 periodic, RK1: 20 timed steps.
 # Algorithmic bytes per cell-update: 272 + 32 per IGR sweep + 40 per Jacobi iteration.
 SI_N, SI_STEPS, SI_WARM = 256, 20, 3
+SI2_N, SI2_STEPS = 2048, 3          # the 2D periodic semi-implicit steps (wavefront vs tiles)
 # Discrete adjoint: isentropic vortex 512^2 to t = 2, checkpoint every 32 steps.
 # Algorithmic bytes per adjoint cell-update: forward recompute 256 + store and
 # read the three stage states 2 x 96 + adjoint state read/write per stage 3 x 64.
@@ -548,6 +551,56 @@ def run_cuda(args):
                           "family_ms_per_step": {k: v[0] for k, v in fam_m.items()},
                           "error_vs_fp64": err}}
 
+    def measure_semi_2d_periodic():
+        """Semi-implicit steps on a periodic 2D mesh with IGR and the
+        Gauss-Seidel pressure solve (the reference's 2D semi-implicit examples
+        use GaussSeidelPressureSolver): both run as the persistent 2D
+        wavefront (k_march_gs); the same steps with the tiled sweeps
+        (SIFV_GS_MARCH=0) beside them.  Device time per step from CUDA events
+        around whole steps after the warm-start step; results are bit-identical
+        between the two."""
+        out = {}
+        prev = os.environ.get("SIFV_GS_MARCH")
+        try:
+            for name, mode in (("wavefront", None), ("tiles", "0")):
+                if mode is None:
+                    os.environ.pop("SIFV_GS_MARCH", None)
+                else:
+                    os.environ["SIFV_GS_MARCH"] = mode
+                case = cases.acoustic_box(SI2_N, SI2_N)
+                ctx = backends.cuda().create(case[0], case[1], local)
+                ctx.set_state(case[2])
+                ctx.set_pressure_solver(abi.PRESSURE_GAUSS_SEIDEL)
+                t_sim = 0.0
+                for q in range(2):                     # step 0: the 20-sweep IGR warm start
+                    t_sim += ctx.step(q, t_sim, -1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                iters = []
+                torch.cuda.synchronize()
+                e0.record()
+                for q in range(SI2_STEPS):
+                    t_sim += ctx.step(2 + q, t_sim, -1.0)
+                    iters.append(ctx.last_pressure_iterations())
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / SI2_STEPS
+                fam = ctx.profile_step(2 + SI2_STEPS, t_sim, -1.0)
+                out[name] = {"ms_per_step": ms, "value": SI2_N * SI2_N / (ms * 1e-3),
+                             "gauss_seidel_iterations": iters,
+                             "family_ms_per_step": {k: v[0] for k, v in fam.items()}}
+                ctx.close()
+        except Exception as e:   # a failed extra measurement must not cost the bench line
+            out["error"] = str(e)[:200]
+        finally:
+            if prev is None:
+                os.environ.pop("SIFV_GS_MARCH", None)
+            else:
+                os.environ["SIFV_GS_MARCH"] = prev
+        out["workload"] = (f"2D acoustic pulse {SI2_N}^2, all faces periodic, semi-implicit RK1 + IGR (5 sweeps), "
+                           f"Gauss-Seidel pressure solve (tol 1e-8, at most 300 iterations), WENO5+HLLC")
+        out["metric"] = "cell-updates/s"
+        return out
+
     def measure_pressure_solvers():
         """Device time of the pressure solve of the first step after the
         warm-up of the 256^3 semi-implicit workload with each pressure solver
@@ -838,6 +891,7 @@ def run_cuda(args):
             semi["cpu_baseline"] = {"value": srate, "unit": UNIT, "cores": 1, "kind": kind, "sample": ssample}
             semi["pressure_solvers"] = measure_pressure_solvers()
             result["semi_implicit"] = semi
+            result["semi_implicit_2d_periodic"] = measure_semi_2d_periodic()
         if adj is not None:
             adj["roofline"]["peak"] = peak
             adj["roofline"]["frac"] = adj["roofline"]["achieved"] / peak

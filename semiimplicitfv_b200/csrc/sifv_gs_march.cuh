@@ -43,9 +43,9 @@
 // Synchronization: each compute warp publishes its progress (steps done,
 // counted across sweeps) in shared memory after each batch of D
 // steps; warp kMarchWarps of the CTA (the helper) turns those into
-// device-wide progress counters after a fence and mirrors the counters of
-// the neighbouring CTAs into shared memory, so no compute warp waits on a
-// device-wide fence.  A sweep starts once every group finished the sweep
+// device-wide progress counters after a fence, so no compute warp waits on a
+// device-wide fence.  A compute warp reads the counters of groups in other
+// CTAs itself, one batch ahead of their use.  A sweep starts once every group finished the sweep
 // that last used its output buffer, and no group starts a sweep after one
 // that is complete and converged.  All CTAs are co-resident (cooperative
 // launch), every wait is bounded (kMarchTimeoutNs) and a wait that gives up
@@ -271,7 +271,6 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
     double2* eRing = ringAll + (size_t)W * R * PC * 32;         // [W][RE]
     __shared__ volatile int sp[W];    // compute progress (this CTA)
     __shared__ volatile int pub[W];   // the same, once visible device-wide
-    __shared__ volatile int ext[3];   // device-wide progress of the group below the CTA, above it, top row's group
     __shared__ volatile int stopS;
     const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
     const int c = (int)blockIdx.x;
@@ -279,15 +278,10 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
         sp[threadIdx.x] = (c * W + (int)threadIdx.x < M.G) ? 0 : kMarchFin;
         pub[threadIdx.x] = sp[threadIdx.x];
     }
-    if (threadIdx.x < 3) ext[threadIdx.x] = 0;
     if (threadIdx.x == 0) stopS = 0;
     __syncthreads();
     const int NS = M.NS, SW = M.SW;
-    // groups outside this CTA whose progress the compute warps need
-    const int gLo = (c > 0) ? c * W - 1 : -1;
-    const int gHi = ((c + 1) * W < M.G) ? (c + 1) * W : -1;
     const int topR = M.ny;   // r of row ny - 1 (source of the periodic low ghost row)
-    const int gsX = (M.perLoY && c == 0 && (topR >> 5) >= W) ? (topR >> 5) : -1;
 
     if (warp == W) {   // helper
         if (lane != 0) return;
@@ -295,7 +289,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
 #pragma unroll
         for (int w = 0; w < W; ++w) last[w] = -1;
         unsigned long long tLast = march_now();
-        for (;;) {
+        for (unsigned it = 0;; ++it) {
             int cur[W];
             bool fin = true, changed = false;
 #pragma unroll
@@ -316,10 +310,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
                 }
                 tLast = march_now();
             }
-            if (gLo >= 0) ext[0] = *(volatile int*)&M.prog[gLo];
-            if (gHi >= 0) ext[1] = *(volatile int*)&M.prog[gHi];
-            if (gsX >= 0) ext[2] = *(volatile int*)&M.prog[gsX];
-            if (*(volatile int*)&M.flags[0]) stopS = 1;
+            if ((it & 63) == 0 && *(volatile int*)&M.flags[0]) stopS = 1;
             if (fin) break;
             if (march_now() - tLast > 2 * kMarchTimeoutNs) {   // compute warps stuck past their own limits
                 atomicOr(&M.flags[1], 1);
@@ -365,11 +356,24 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
     bool ok = true;
     int chk = 0;
 
+    // device-wide progress of the groups in other CTAs this warp waits on -- the group below (lane 0's
+    // edge), the group above (lane 31's edge) and the top row's group (periodic low ghost row) -- as last
+    // read (extV) and as read one batch ahead of its use (extN); lane 0 only
+    const bool inCta0 = g - 1 >= c * W, inCta1 = g + 1 < c * W + W, inCta2 = topG >= c * W && topG < c * W + W;
+    const int extG[3] = {(g > 0 && !inCta0) ? g - 1 : -1, (hasAbove && !inCta1) ? g + 1 : -1,
+                         (g == 0 && M.perLoY && topG != 0 && !inCta2) ? topG : -1};
+    int extV[3] = {0, 0, 0}, extN[3] = {0, 0, 0};
+    auto ext_issue = [&]() {
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            if (extG[q] >= 0) extN[q] = *(volatile int*)&M.prog[extG[q]];
+    };
     auto progress_of = [&](int hgrp) -> int {
         if (hgrp >= c * W && hgrp < c * W + W) return pub[hgrp - c * W];
-        if (hgrp == gLo) return ext[0];
-        if (hgrp == gHi) return ext[1];
-        return ext[2];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            if (extG[q] == hgrp) return extV[q];
+        return -1;   // not reached: every external group a wait names is in extG (a wait on it would time out)
     };
 
     for (int k = 0; k < M.maxIter && ok; ++k) {
@@ -451,6 +455,8 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
         auto batch_wait = [&](int tu, int tp) -> bool {
             bool good = true;
             if (lane == 0) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) extV[q] = extN[q];   // read one batch ago
                 const int n0 = (warp > 0) ? base + min(tu + 32, NS) : -1;
                 const int n1 = (warp == 0 && g > 0) ? base + min(tp + 32, NS) : -1;
                 const int n2 = (g == 0 && lowFromEdge && topG != 0) ? prevBase + min(tp + topB + 1, NS) : -1;
@@ -463,7 +469,11 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
                 };
                 if (!met()) {
                     const unsigned long long tw = march_now();
-                    while (!met()) {
+                    for (;;) {
+                        ext_issue();
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) extV[q] = extN[q];
+                        if (met()) break;
                         if (stopS) { good = false; break; }
                         if (march_now() - tw > kMarchTimeoutNs) {
                             atomicOr(&M.flags[1], 1);
@@ -474,6 +484,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
                         }
                     }
                 }
+                ext_issue();   // for the next batch
             }
             const bool res = __shfl_sync(0xffffffffu, good ? 1 : 0, 0) != 0;
             asm volatile("" ::: "memory");   // no load of the batch moves above the wait

@@ -290,6 +290,22 @@ def _check_with_solver(case, nsteps, kind):
     return cg.last_pressure_iterations()
 
 
+@pytest.mark.parametrize("bcs", [(abi.BC_PERIODIC, abi.BC_PERIODIC), (abi.BC_PERIODIC, abi.BC_SLIPWALL),
+                                 (abi.BC_OUTFLOW, abi.BC_PERIODIC)])
+def test_semi_implicit_2d_periodic_wavefront_steps(bcs):
+    """Three semi-implicit steps on 2D meshes with a periodic face (IGR warm
+    start and 5-sweep solves, Gauss-Seidel pressure solves to tol 1e-8): both
+    run as the persistent wavefront, walking along x (periodic x), along y
+    (periodic y only) or along the longer axis (both periodic, 200 x 300);
+    several CTAs of 32-row groups.  Every field, dt and the iteration counts
+    are the oracle's bit for bit."""
+    nx, ny = (200, 300) if bcs == (abi.BC_PERIODIC, abi.BC_PERIODIC) else (300, 200)
+    cfg, mesh, fields = cases.acoustic_box(nx, ny)
+    mesh.bc = [bcs[0]] * 2 + [bcs[1]] * 2 + [abi.BC_OUTFLOW] * 2
+    iters = _check_with_solver((cfg, mesh, fields), 3, 1)
+    assert iters > 1
+
+
 @pytest.mark.parametrize("name", ["advection1d", "acoustic3d", "box3d_ragged", "box2d_ragged"])
 def test_gauss_seidel_pressure_solver(name):
     """GaussSeidelPressureSolver as the semi-implicit step's plugin: tiled
