@@ -640,10 +640,11 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
     // instances: Gauss-Seidel with batch length 8 or 4, IGR with 4 (its records fill the shared memory),
     // each walking along x or y
     using MarchFn = void (*)(Params, GsMarch, Ctl*);
-    const MarchFn fns[6] = {k_march_gs<kMarchWarps, 8, false, 0>, k_march_gs<kMarchWarps, 8, true, 0>,
-                            k_march_gs<kMarchWarps, 4, false, 0>, k_march_gs<kMarchWarps, 4, true, 0>,
-                            k_march_gs<kMarchWarps, 4, false, 1>, k_march_gs<kMarchWarps, 4, true, 1>};
-    const int fnD[6] = {8, 8, 4, 4, 4, 4}, fnKind[6] = {0, 0, 0, 0, 1, 1};
+    constexpr int DS = kMarchShortD;
+    const MarchFn fns[6] = {k_march_gs<kMarchWarps, 8, false, 0>,  k_march_gs<kMarchWarps, 8, true, 0>,
+                            k_march_gs<kMarchWarps, DS, false, 0>, k_march_gs<kMarchWarps, DS, true, 0>,
+                            k_march_gs<kMarchWarps, 4, false, 1>,  k_march_gs<kMarchWarps, 4, true, 1>};
+    const int fnD[6] = {8, 8, DS, DS, 4, 4}, fnKind[6] = {0, 0, 0, 0, 1, 1};
     // Gauss-Seidel: D = 4 when a periodic row axis makes the groups' lags (about 32 + 2 D + 10 steps
     // each) longer than a sweep; otherwise D = 8
     const bool rowPeriodic = bn0 == SIFV_BC_PERIODIC || bn1 == SIFV_BC_PERIODIC;

@@ -63,6 +63,10 @@ constexpr int kMarchWarps = SIFV_MARCH_WARPS;  // compute warps per CTA
 // than a sweep (each group trails the one below by about 32 + 2 D steps,
 // and a periodic row axis makes the sweep period the sum of those lags).
 // The record ring holds two batches.
+#ifndef SIFV_MARCH_SHORT_D
+#define SIFV_MARCH_SHORT_D 4
+#endif
+constexpr int kMarchShortD = SIFV_MARCH_SHORT_D;
 constexpr int kMarchRE = 256;                  // lane-31 pairs kept for the warp above (power of 2)
 constexpr int kMarchMaxBufs = 16;
 constexpr int kMarchFin = 0x7fffffff;          // progress of a finished group
