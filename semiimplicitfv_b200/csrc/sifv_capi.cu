@@ -641,15 +641,16 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
     // each walking along x or y
     using MarchFn = void (*)(Params, GsMarch, Ctl*);
     constexpr int DS = kMarchShortD;
-    const MarchFn fns[6] = {k_march_gs<kMarchWarps, 8, false, 0>,  k_march_gs<kMarchWarps, 8, true, 0>,
+    const MarchFn fns[8] = {k_march_gs<kMarchWarps, 8, false, 0>,  k_march_gs<kMarchWarps, 8, true, 0>,
                             k_march_gs<kMarchWarps, DS, false, 0>, k_march_gs<kMarchWarps, DS, true, 0>,
-                            k_march_gs<kMarchWarps, 4, false, 1>,  k_march_gs<kMarchWarps, 4, true, 1>};
-    const int fnD[6] = {8, 8, DS, DS, 4, 4}, fnKind[6] = {0, 0, 0, 0, 1, 1};
-    // Gauss-Seidel: D = 4 when a periodic row axis makes the groups' lags (about 32 + 2 D + 10 steps
+                            k_march_gs<kMarchWarps, 8, false, 1>,  k_march_gs<kMarchWarps, 8, true, 1>,
+                            k_march_gs<kMarchWarps, DS, false, 1>, k_march_gs<kMarchWarps, DS, true, 1>};
+    const int fnD[8] = {8, 8, DS, DS, 8, 8, DS, DS}, fnKind[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+    // D = the short batch when a periodic row axis makes the groups' lags (about 32 + 2 D + 10 steps
     // each) longer than a sweep; otherwise D = 8
     const bool rowPeriodic = bn0 == SIFV_BC_PERIODIC || bn1 == SIFV_BC_PERIODIC;
     const bool short8 = rowPeriodic && (long long)G * (32 + 2 * 8 + 10) > NS;
-    const int fi = (kind ? 4 : short8 ? 2 : 0) + (tr ? 1 : 0);
+    const int fi = (kind ? 4 : 0) + (short8 ? 2 : 0) + (tr ? 1 : 0);
     const int D = fnD[fi];
     const MarchFn fn = fns[fi];
     const size_t smem = march_smem(D, kind);
@@ -659,7 +660,7 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
         long long fit = -1;
-        for (int q = 0; q < 6 && coop; ++q) {
+        for (int q = 0; q < 8 && coop; ++q) {
             const size_t sq = march_smem(fnD[q], fnKind[q]);
             int perSm = 0;
             if (cudaFuncSetAttribute(fns[q], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sq) != cudaSuccess ||
@@ -734,6 +735,8 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
     M.perHiY = bn1 == SIFV_BC_PERIODIC;
     M.tol = tol;
     M.ghost0 = c->F.sigma;
+    M.wRow = tr ? c->F.adx2 : c->F.ady2;
+    M.wRowOff = tr ? P.ngx : P.ngy;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeCooperative;
     at[0].val.cooperative = 1;

@@ -86,13 +86,15 @@ struct GsMarch {
     int perLoY, perHiY;          // the ghost rows across the row axis wrap around
     double tol;
     const double* ghost0;        // IGR: the stored field, whose ghost cells sweep 0 reads
+    const double* wRow;          // IGR: the metric weight along the row axis (ady2, or adx2 when TR), per row
+    int wRowOff;                 // its ghost offset
 };
 
 __host__ __device__ __forceinline__ size_t march_q(int SW, int g, int s, int b) {
     return ((size_t)g * SW + s) * 32 + b;
 }
-// record chunks (16 bytes) per cell: Gauss-Seidel 4, IGR 7
-__host__ __device__ constexpr int march_chunks(int kind) { return kind ? 7 : 4; }
+// record chunks (16 bytes) per cell: Gauss-Seidel 4, IGR 6
+__host__ __device__ constexpr int march_chunks(int kind) { return kind ? 6 : 4; }
 inline size_t march_smem(int D, int kind) {
     return ((size_t)kMarchWarps * 2 * D * 2 * march_chunks(kind) * 32 + (size_t)kMarchWarps * kMarchRE) *
            sizeof(double2);
@@ -159,25 +161,29 @@ __device__ __noinline__ double igr_cell_plain2(double sxm, double sxp, double sy
     off += ay * (sym / rfly + syp / rfry);
     return (rhs + off) / diag;
 }
+// The record holds the march axis' metric weight; the row axis' one (wn) is
+// constant along the row.
 template <bool TR>
-__device__ __forceinline__ double igr_march_cell(bool act, bool fastRecs, const double2* r, double pL, double pR,
-                                                 double pD, double pU) {
+__device__ __forceinline__ double igr_march_cell(bool act, bool fastRecs, const double2* r, double wn, double pL,
+                                                 double pR, double pD, double pU) {
     const double sxm = TR ? pD : pL, sxp = TR ? pU : pR, sym = TR ? pL : pD, syp = TR ? pR : pU;
+    const double ax = TR ? wn : r[4].x, ay = TR ? r[4].x : wn;
     if (!act || (fastRecs && igr_fast_operand(sxm) && igr_fast_operand(sxp) && igr_fast_operand(sym) &&
                  igr_fast_operand(syp))) {
         double off = 0.0;
-        off += r[4].x * (div_markstein(sxm, r[0].x, r[0].y) + div_markstein(sxp, r[1].x, r[1].y));
-        off += r[4].y * (div_markstein(sym, r[2].x, r[2].y) + div_markstein(syp, r[3].x, r[3].y));
-        const double num = r[5].x + off;
-        return (!act || igr_fast_operand(num)) ? div_markstein(num, r[5].y, r[6].x) : div_rn_plain(num, r[5].y);
+        off += ax * (div_markstein(sxm, r[0].x, r[0].y) + div_markstein(sxp, r[1].x, r[1].y));
+        off += ay * (div_markstein(sym, r[2].x, r[2].y) + div_markstein(syp, r[3].x, r[3].y));
+        const double num = r[4].y + off;
+        return (!act || igr_fast_operand(num)) ? div_markstein(num, r[5].x, r[5].y) : div_rn_plain(num, r[5].x);
     }
-    return igr_cell_plain2(sxm, sxp, sym, syp, r[0].x, r[1].x, r[2].x, r[3].x, r[4].x, r[4].y, r[5].x, r[5].y);
+    return igr_cell_plain2(sxm, sxp, sym, syp, r[0].x, r[1].x, r[2].x, r[3].x, ax, ay, r[4].y, r[5].x);
 }
 
 // IGR records and iterate 0 (interior pairs, and the stored first ghost
 // layer in the ghost rows' slots, which sweep 0 reads).  Record of a cell:
 // (rho_f, 1 / rho_f) of the x-, x+, y-, y+ faces with the sweep's
-// expressions 0.5 (rho_i + rho_nb), (ax, ay), (rhs, diag), (1 / diag, 0).
+// expressions 0.5 (rho_i + rho_nb), (the march axis' metric weight, rhs),
+// (diag, 1 / diag).
 __global__ void k_march_igr_setup(Params P, Fields F, double2* __restrict__ rec, double2* __restrict__ q0, int SW,
                                   long long total, int* __restrict__ slowRecs, int tr) {
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -202,14 +208,13 @@ __global__ void k_march_igr_setup(Params P, Fields F, double2* __restrict__ rec,
             const double rfly = 0.5 * (rho_i + F.rho[c - sy]), rfry = 0.5 * (rho_i + F.rho[c + sy]);
             const double rxl = 1.0 / rflx, rxr = 1.0 / rfrx, ryl = 1.0 / rfly, ryr = 1.0 / rfry;
             const double diag = F.igrDiag[c], rd = 1.0 / diag;
-            double2* o = rec + ((size_t)gs * 14 + 7 * e) * 32 + b;
+            double2* o = rec + ((size_t)gs * 12 + 6 * e) * 32 + b;
             o[0] = make_double2(rflx, rxl);
             o[32] = make_double2(rfrx, rxr);
             o[64] = make_double2(rfly, ryl);
             o[96] = make_double2(rfry, ryr);
-            o[128] = make_double2(F.adx2[i + P.ngx], F.ady2[j + P.ngy]);
-            o[160] = make_double2(F.igrRhs[c], diag);
-            o[192] = make_double2(rd, 0.0);
+            o[128] = make_double2(tr ? F.ady2[j + P.ngy] : F.adx2[i + P.ngx], F.igrRhs[c]);
+            o[160] = make_double2(diag, rd);
             if (!(igr_fast_recip(rxl) && igr_fast_recip(rxr) && igr_fast_recip(ryl) && igr_fast_recip(ryr) &&
                   igr_fast_recip(rd)))
                 atomicOr(slowRecs, 1);
@@ -333,6 +338,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
     const double2* eBelow = eRing + (size_t)(warp > 0 ? warp - 1 : 0) * RE;
     const int r = 32 * g + lane;
     const bool rowIn = r >= 1 && r <= M.ny;
+    const double wn = (KIND == 1 && rowIn) ? M.wRow[r - 1 + M.wRowOff] : 0.0;   // IGR: row axis' metric weight
     const int nx = M.nx, NH = M.NH;
     const bool fastRecs = *M.slowRecs == 0;
     const int gT = (M.ny + 1) >> 5, bT = (M.ny + 1) & 31;   // the high ghost row r = ny + 1
@@ -557,12 +563,12 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
                     const double pR0 = (t == tLast && !lastOdd) ? gR : Pt.y;
                     const double pn0 = KIND == 0 ? march_cell<TR>(act0, fastRecs, ra[0], ra[1], ra[2], ra[3], pL0, pR0,
                                                                   pD.x, pU.x)
-                                                 : igr_march_cell<TR>(act0, fastRecs, ra, pL0, pR0, pD.x, pU.x);
+                                                 : igr_march_cell<TR>(act0, fastRecs, ra, wn, pL0, pR0, pD.x, pU.x);
                     // cell 2h + 1: left is cell 2h's new value, right the next pair's first cell
                     const double pR1 = (t == tLast) ? gR : Pn.x;
                     const double pn1 = KIND == 0 ? march_cell<TR>(act1, fastRecs, rc[0], rc[1], rc[2], rc[3], pn0, pR1,
                                                                   pD.y, pU.y)
-                                                 : igr_march_cell<TR>(act1, fastRecs, rc, pn0, pR1, pD.y, pU.y);
+                                                 : igr_march_cell<TR>(act1, fastRecs, rc, wn, pn0, pR1, pD.y, pU.y);
                     const double2 pn = make_double2(pn0, pn1);
                     if (KIND == 0) {
                         maxRes = act0 ? smax(maxRes, fabs(pn0 - Pt.x)) : maxRes;
