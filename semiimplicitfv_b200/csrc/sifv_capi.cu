@@ -637,8 +637,7 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
     const int G = Nn / 32 + 1, GA = (Nn + 1) / 32 + 1;
     const int ctas = (G + kMarchWarps - 1) / kMarchWarps;
     if ((long long)(maxIter + 2) * NS >= (1LL << 30)) return 1;
-    // instances: Gauss-Seidel with batch length 8 or 4, IGR with 4 (its records fill the shared memory),
-    // each walking along x or y
+    // instances: Gauss-Seidel and IGR cells, batch length 8 or the short one, each walking along x or y
     using MarchFn = void (*)(Params, GsMarch, Ctl*);
     constexpr int DS = kMarchShortD;
     const MarchFn fns[8] = {k_march_gs<kMarchWarps, 8, false, 0>,  k_march_gs<kMarchWarps, 8, true, 0>,
