@@ -92,6 +92,7 @@ struct sifv_ctx {
     int marchOk = -1;                         // -1 unknown, 0 no cooperative launch, 1 usable
     long long marchCtas = 0;                  // co-resident CTAs of k_march_gs
     int marchMode = -1;                       // SIFV_GS_MARCH: -1 (unset) periodic meshes, 0 never, 1 always
+    int marchSegs = 0;                        // SIFV_GS_MARCH_SEGMENTS: segments along the march axis (0: chosen)
     int gsPrevIters = 0;                      // iterations of the previous Gauss-Seidel solve (first batch size)
     double* jacCoef = nullptr;                // Jacobi coefficients: per face (dim arrays) or per cell (2 dim + 2)
     bool uniformAxes = false;                 // interior cell widths bitwise equal along every active axis
@@ -413,9 +414,10 @@ int igr_solve(sifv_ctx* c, int step) {
     const bool periodic2d = P.bc[0] == SIFV_BC_PERIODIC || P.bc[1] == SIFV_BC_PERIODIC ||
                             P.bc[2] == SIFV_BC_PERIODIC || P.bc[3] == SIFV_BC_PERIODIC;
     if (P.dim == 2 && iters > 1 && !c->exchangeFaces && !c->ib.count && !c->F.solid && c->marchMode != 0 &&
-        (c->marchMode == 1 || periodic2d)) {
-        // the persistent wavefront (all sweeps in one launch); the tiled sweeps below overlap well only
-        // without a periodic face
+        (c->marchMode == 1 || periodic2d || std::max(P.nx, P.ny) >= 1024)) {
+        // the persistent wavefront (all sweeps in one launch): on a mesh with a periodic face, and without
+        // one from 1024 cells along the longer axis (rows cut into segments); the tiled sweeps below
+        // otherwise
         int done = 0;
         const double* res = nullptr;
         const int ms = march_run(c, 1, nullptr, 0.0, iters, done, res);
@@ -629,13 +631,14 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
     const Params& P = c->P;
     const bool px = P.bc[0] == SIFV_BC_PERIODIC || P.bc[1] == SIFV_BC_PERIODIC;
     const bool py = P.bc[2] == SIFV_BC_PERIODIC || P.bc[3] == SIFV_BC_PERIODIC;
-    const bool tr = (py && !px) || (px && py && P.ny > P.nx);   // walk along y
+    // walk along y when only y is periodic, or both or neither are and y is longer
+    const bool tr = (py && !px) || (px == py && P.ny > P.nx);
     const int Nm = tr ? P.ny : P.nx, Nn = tr ? P.nx : P.ny;     // march and row extents
     const int bm0 = tr ? P.bc[2] : P.bc[0], bm1 = tr ? P.bc[3] : P.bc[1];
     const int bn0 = tr ? P.bc[0] : P.bc[2], bn1 = tr ? P.bc[1] : P.bc[3];
     const int NH = (Nm + 1) / 2, SW = NH + 32, NS = NH + 31;
     const int G = Nn / 32 + 1, GA = (Nn + 1) / 32 + 1;
-    const int ctas = (G + kMarchWarps - 1) / kMarchWarps;
+    const int ctasPerSeg = (G + kMarchWarps - 1) / kMarchWarps;
     if ((long long)(maxIter + 2) * NS >= (1LL << 30)) return 1;
     // instances: Gauss-Seidel and IGR cells, batch length 8 or the short one, each walking along x or y
     using MarchFn = void (*)(Params, GsMarch, Ctl*);
@@ -676,11 +679,23 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
         }
         cudaGetLastError();
     }
-    if (!c->marchOk || ctas > c->marchCtas) return 1;
+    if (!c->marchOk || ctasPerSeg > c->marchCtas) return 1;
+    // Without a periodic face the rows are cut into S segments along the march axis (about 192 pairs each,
+    // as many as the co-resident CTAs allow): a segment's sweep k follows the left segment's sweep k and
+    // the right one's sweep k - 1, so the segments work on consecutive sweeps at once.
+    int S = 1;
+    if (!px && !py) {
+        const long long fit = c->marchCtas / ctasPerSeg;
+        S = (int)std::max<long long>(1, std::min<long long>(fit, (NH + 191) / 192));
+        if (c->marchSegs > 0) S = (int)std::min<long long>(fit, c->marchSegs);
+    }
+    const int L = (NH + S - 1) / S;
+    S = (NH + L - 1) / L;
+    const int ctas = ctasPerSeg * S, NSs = L + 31;
     const size_t qn = (size_t)GA * SW * 32;   // pairs per iterate
-    // buffers: the groups spread over about G (32 + 2 D + 40) / NS sweeps, plus the converged iterate,
-    // its predecessor and one sweep of slack; at most 1 GiB
-    int nb = std::min(kMarchMaxBufs, 4 + (G * (32 + 2 * D + 40) + NS - 1) / NS);
+    // buffers: the warps spread over about (G (32 + 2 D + 40) + S NSs) / NSs sweeps, plus the converged
+    // iterate, its predecessor and one sweep of slack; at most 1 GiB
+    int nb = std::min(kMarchMaxBufs, 4 + (G * (32 + 2 * D + 40) + S * NSs + NSs - 1) / NSs);
     nb = std::max(3, std::min<int>(nb, (int)((size_t(1) << 30) / (qn * sizeof(double2)))));
     int sa = SIFV_OK;
     double*& recBuf = kind ? c->marchRecIgr : c->marchRec;
@@ -695,15 +710,15 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
         }
     if (c->marchIntCap < maxIter) {   // ints in double units
         const int cap = std::max(maxIter, 64);
-        c->marchInt = reinterpret_cast<int*>(dalloc(c, ((size_t)G + 3 + cap + 1) / 2 + 1, sa));
+        c->marchInt = reinterpret_cast<int*>(dalloc(c, ((size_t)G * S + 3 + cap + 1) / 2 + 1, sa));
         if (sa != SIFV_OK) return sa;
         c->marchIntCap = cap;
     }
-    int* prog = c->marchInt;
-    int* flags = prog + G;
+    int* prog = c->marchInt;   // [S][G]
+    int* flags = prog + (size_t)G * S;
     int* slowRecs = flags + 2;
     int* done = slowRecs + 1;
-    CUDA_TRY(c, cudaMemsetAsync(c->marchInt, 0, sizeof(int) * ((size_t)G + 3 + maxIter), c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->marchInt, 0, sizeof(int) * ((size_t)G * S + 3 + maxIter), c->stream));
     const long long total = (long long)qn;
     if (kind)
         k_march_igr_setup<<<blocks(total, 256), 256, 0, c->stream>>>(P, c->F, reinterpret_cast<double2*>(recBuf),
@@ -724,6 +739,9 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
     M.GA = GA;
     M.SW = SW;
     M.NS = NS;
+    M.S = S;
+    M.L = L;
+    M.ctasPerSeg = ctasPerSeg;
     M.NH = NH;
     M.maxIter = maxIter;
     M.nx = Nm;
@@ -827,9 +845,11 @@ int gs_run(sifv_ctx* c, const double* rho, const double* rhoc2, const double* rh
     }
     const bool periodic2d = P.bc[0] == SIFV_BC_PERIODIC || P.bc[1] == SIFV_BC_PERIODIC ||
                             P.bc[2] == SIFV_BC_PERIODIC || P.bc[3] == SIFV_BC_PERIODIC;
-    if (P.dim == 2 && !c->exchangeFaces && maxIter >= 2 && c->marchMode != 0 && (c->marchMode == 1 || periodic2d)) {
-        // the persistent wavefront; the tiled sweeps below overlap many iterations on a mesh without a
-        // periodic face (their iterations lag by 2 tile planes instead of a full row of tiles)
+    if (P.dim == 2 && !c->exchangeFaces && maxIter >= 2 && c->marchMode != 0 &&
+        (c->marchMode == 1 || periodic2d || std::max(P.nx, P.ny) >= 2048)) {
+        // the persistent wavefront: on a mesh with a periodic face, and without one from 2048 cells along
+        // the longer axis (rows cut into segments); below that the tiled sweeps, which overlap many
+        // iterations there (their iterations lag by 2 tile planes), are as fast
         const int ms = march_run(c, 0, rhs, tol, maxIter, iters, result);
         if (ms == SIFV_OK) {
             c->gsPrevIters = iters;
@@ -1689,6 +1709,8 @@ int sifv_create(const sifv_config_t* cfg, const sifv_mesh_t* mesh, int device, s
     {
         const char* e = std::getenv("SIFV_GS_MARCH");
         c->marchMode = (e && e[0] == '0') ? 0 : (e && e[0] == '1') ? 1 : -1;
+        const char* es = std::getenv("SIFV_GS_MARCH_SEGMENTS");
+        c->marchSegs = es ? std::atoi(es) : 0;
     }
     if (cudaSetDevice(device) != cudaSuccess) { delete c; return fail(nullptr, SIFV_ERR_CUDA, "cudaSetDevice failed"); }
     if (cudaStreamCreateWithFlags(&c->ownStream, cudaStreamNonBlocking) != cudaSuccess) {

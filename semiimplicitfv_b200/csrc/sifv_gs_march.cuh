@@ -68,7 +68,7 @@ constexpr int kMarchWarps = SIFV_MARCH_WARPS;  // compute warps per CTA
 #endif
 constexpr int kMarchShortD = SIFV_MARCH_SHORT_D;
 constexpr int kMarchRE = 256;                  // lane-31 pairs kept for the warp above (power of 2)
-constexpr int kMarchMaxBufs = 16;
+constexpr int kMarchMaxBufs = 32;
 constexpr int kMarchFin = 0x7fffffff;          // progress of a finished group
 constexpr unsigned long long kMarchTimeoutNs = 2000000000ull;
 
@@ -88,6 +88,8 @@ struct GsMarch {
     const double* ghost0;        // IGR: the stored field, whose ghost cells sweep 0 reads
     const double* wRow;          // IGR: the metric weight along the row axis (ady2, or adx2 when TR), per row
     int wRowOff;                 // its ghost offset
+    int S, L;                    // segments along the march axis and their length in pairs (S = 1: whole rows)
+    int ctasPerSeg;              // CTAs of one segment (its row groups)
 };
 
 __host__ __device__ __forceinline__ size_t march_q(int SW, int g, int s, int b) {
@@ -282,14 +284,21 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
     __shared__ volatile int pub[W];   // the same, once visible device-wide
     __shared__ volatile int stopS;
     const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
-    const int c = (int)blockIdx.x;
+    // CTA -> segment `seg` of the march axis and its row groups g0 .. g0 + W - 1; a warp's progress counter
+    // is prog[seg G + g]
+    const int seg = (int)blockIdx.x / M.ctasPerSeg, g0 = ((int)blockIdx.x % M.ctasPerSeg) * W;
+    const int pbase = seg * M.G;
+    const int NH = M.NH;
+    const int hs0 = seg * M.L, hs1 = min(NH, hs0 + M.L);   // this segment's pairs
+    auto seg_steps = [&](int s) { return min(NH, (s + 1) * M.L) - s * M.L + 31; };
+    const int NS = hs1 - hs0 + 31, SW = M.SW;              // steps per sweep of this segment
+    const int nWarps = M.G * M.S;                           // warps that count a sweep done
     if (threadIdx.x < W) {
-        sp[threadIdx.x] = (c * W + (int)threadIdx.x < M.G) ? 0 : kMarchFin;
+        sp[threadIdx.x] = (g0 + (int)threadIdx.x < M.G) ? 0 : kMarchFin;
         pub[threadIdx.x] = sp[threadIdx.x];
     }
     if (threadIdx.x == 0) stopS = 0;
     __syncthreads();
-    const int NS = M.NS, SW = M.SW;
     const int topR = M.ny;   // r of row ny - 1 (source of the periodic low ghost row)
 
     if (warp == W) {   // helper
@@ -312,7 +321,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
 #pragma unroll
                 for (int w = 0; w < W; ++w) {
                     if (cur[w] != last[w]) {
-                        if (c * W + w < M.G) *(volatile int*)&M.prog[c * W + w] = cur[w];
+                        if (g0 + w < M.G) *(volatile int*)&M.prog[pbase + g0 + w] = cur[w];
                         pub[w] = cur[w];
                         last[w] = cur[w];
                     }
@@ -331,7 +340,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
         return;
     }
 
-    const int g = c * W + warp;
+    const int g = g0 + warp;
     if (g >= M.G) return;
     double2* ring = ringAll + (size_t)warp * R * PC * 32 + lane;   // slot q, chunk ch at ring[(PC q + ch) 32]
     double2* eMine = eRing + (size_t)warp * RE;
@@ -339,25 +348,30 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
     const int r = 32 * g + lane;
     const bool rowIn = r >= 1 && r <= M.ny;
     const double wn = (KIND == 1 && rowIn) ? M.wRow[r - 1 + M.wRowOff] : 0.0;   // IGR: row axis' metric weight
-    const int nx = M.nx, NH = M.NH;
+    const int nx = M.nx;
     const bool fastRecs = *M.slowRecs == 0;
     const int gT = (M.ny + 1) >> 5, bT = (M.ny + 1) & 31;   // the high ghost row r = ny + 1
     const bool hasAbove = g + 1 < M.G;                        // group above with interior rows
     const int topG = topR >> 5, topB = topR & 31;
     const bool lowGhostLane = (g == 0 && lane == 0);
     const bool topGhostLane = (g == gT && lane == bT && bT >= 1);
-    // per-lane step windows: step t updates pair h = t - lane
-    const int tAct0 = rowIn ? lane : NS, tAct1 = rowIn ? lane + NH : NS;
-    const int tLast = lane + ((nx - 1) >> 1);   // the step of the pair holding x = nx - 1
+    // per-lane step windows: step t updates pair h = hs0 + t - lane
+    const int nP = hs1 - hs0;
+    // own pairs are loaded through step NS - 1, or NS before another segment (lane 31's last pair then
+    // reads that segment's first pair)
+    const int tPEnd = NS + (hs1 < NH ? 1 : 0);
+    const int tAct0 = rowIn ? lane : NS, tAct1 = rowIn ? lane + nP : NS;
+    const int hLastX = (nx - 1) >> 1;   // the pair holding x = nx - 1, and its step (last segment only)
+    const int tLast = (hLastX >= hs0 && hLastX < hs1) ? lane + hLastX - hs0 : -1;
     const bool lastOdd = ((nx - 1) & 1) != 0;   // x = nx - 1 is the second cell of its pair
     // the edge pair of step t at eP[32 t] for t in [eLo, eHi): lane 0 the new pair of the row below
     // (group below in another CTA) or of row ny - 1 (periodic low ghost row), lane 31 the old pair of the
     // row above (or of its own row / row 0 when the row above is the high ghost row)
     int eKind = 0, eLo = 0, eHi = 0;
-    if (lane == 0 && warp == 0 && g > 0) { eKind = 1; eHi = NH; }
-    else if (lowGhostLane && M.perLoY) { eKind = 2; eHi = NH; }
-    else if (lane == 31 && hasAbove) { eKind = 3; eLo = 31; eHi = NH + 31; }
-    else if (lane == 31 && g + 1 == gT && bT == 0) { eKind = 4; eLo = 31; eHi = NH + 31; }
+    if (lane == 0 && warp == 0 && g > 0) { eKind = 1; eHi = nP; }
+    else if (lowGhostLane && M.perLoY) { eKind = 2; eHi = nP; }
+    else if (lane == 31 && hasAbove) { eKind = 3; eLo = 31; eHi = nP + 31; }
+    else if (lane == 31 && g + 1 == gT && bT == 0) { eKind = 4; eLo = 31; eHi = nP + 31; }
     const bool eBelowLane = lane == 0 && warp > 0;
     const bool eWriter = lane == 31 && warp < W - 1 && rowIn;
     // the lane's own pair loads: its row, or the source row of the ghost row it stands for, from step pLo
@@ -369,17 +383,17 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
     // device-wide progress of the groups in other CTAs this warp waits on -- the group below (lane 0's
     // edge), the group above (lane 31's edge) and the top row's group (periodic low ghost row) -- as last
     // read (extV) and as read one batch ahead of its use (extN); lane 0 only
-    const bool inCta0 = g - 1 >= c * W, inCta1 = g + 1 < c * W + W, inCta2 = topG >= c * W && topG < c * W + W;
+    const bool inCta0 = g - 1 >= g0, inCta1 = g + 1 < g0 + W, inCta2 = topG >= g0 && topG < g0 + W;
     const int extG[3] = {(g > 0 && !inCta0) ? g - 1 : -1, (hasAbove && !inCta1) ? g + 1 : -1,
                          (g == 0 && M.perLoY && topG != 0 && !inCta2) ? topG : -1};
     int extV[3] = {0, 0, 0}, extN[3] = {0, 0, 0};
     auto ext_issue = [&]() {
 #pragma unroll
         for (int q = 0; q < 3; ++q)
-            if (extG[q] >= 0) extN[q] = *(volatile int*)&M.prog[extG[q]];
+            if (extG[q] >= 0) extN[q] = *(volatile int*)&M.prog[pbase + extG[q]];
     };
     auto progress_of = [&](int hgrp) -> int {
-        if (hgrp >= c * W && hgrp < c * W + W) return pub[hgrp - c * W];
+        if (hgrp >= g0 && hgrp < g0 + W) return pub[hgrp - g0];
 #pragma unroll
         for (int q = 0; q < 3; ++q)
             if (extG[q] == hgrp) return extV[q];
@@ -396,9 +410,15 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
             const int kw = k + 1 - M.nb;
             const unsigned long long tw = march_now();
             while (go) {
-                const bool a = kw < 0 || *(volatile int*)&M.done[kw] >= M.G;
-                const bool b = !(M.perHiY && g == M.G - 1 && g != 0) || *(volatile int*)&M.prog[0] >= base;
-                if (a && b) break;
+                const bool a = kw < 0 || *(volatile int*)&M.done[kw] >= nWarps;
+                const bool b = !(M.perHiY && g == M.G - 1 && g != 0) || *(volatile int*)&M.prog[pbase] >= base;
+                // the segment to the left through sweep k (this row's first pair reads its new last cell),
+                // the one to the right through the first pairs of sweep k - 1 (every lane's first pair is
+                // done after 32 steps; this row's last pair reads its old first cell)
+                const bool sl = seg == 0 || *(volatile int*)&M.prog[pbase - M.G + g] >= (k + 1) * seg_steps(seg - 1);
+                const bool sr = seg == M.S - 1 || k == 0 ||
+                                *(volatile int*)&M.prog[pbase + M.G + g] >= (k - 1) * seg_steps(seg + 1) + 32;
+                if (a && b && sl && sr) break;
                 if (stopS || *(volatile int*)&M.flags[0]) go = false;
                 else if (march_now() - tw > kMarchTimeoutNs) {
                     atomicOr(&M.flags[1], 1);
@@ -408,7 +428,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
             }
             if (go) __threadfence();
             while (KIND == 0 && go && chk < k) {
-                if (*(volatile int*)&M.done[chk] < M.G) break;
+                if (*(volatile int*)&M.done[chk] < nWarps) break;
                 __threadfence();
                 if (bits2d(*(volatile unsigned long long*)&ctl->res[chk]) < M.tol) {
                     *(volatile int*)&M.flags[0] = 1;
@@ -424,32 +444,43 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
         const double2* __restrict__ Qk = M.q[k % M.nb];
         double2* __restrict__ Qn = M.q[(k + 1) % M.nb];
         const double2* rowK = Qk + march_q(SW, g, 0, lane);   // slot s at rowK[32 s]
-        double2* outP = Qn + march_q(SW, g, 0, lane);         // step t's pair at outP[32 t]
-        const double2* recP = M.rec + march_q(SW, g, 0, 0) * PC + lane;   // step t, chunk ch at recP[(PC t + ch) 32]
+        const double2* rowKs = rowK + 32 * hs0;                // step t's slot at rowKs[32 t]
+        double2* outP = Qn + march_q(SW, g, hs0, lane);        // step t's pair at outP[32 t]
+        // step t, chunk ch at recP[(PC t + ch) 32]
+        const double2* recP = M.rec + march_q(SW, g, hs0, 0) * PC + lane;
         // IGR sweep 0 reads the ghost cells as stored (the ghost rows' own slots, the stored ghost columns);
         // every other sweep reads them from their source cells in iterate k
         const bool stored0 = KIND == 1 && k == 0;
         // own pair of step t at pP[32 t]
-        const double2* pP = rowK;
+        const double2* pP = rowKs;
         int pLoK = pLo;
         if (!stored0) {
-            if (lowGhostLane && !M.perLoY) pP = Qk + march_q(SW, 0, 1, 1);   // row 0's pair h = t
-            if (topGhostLane)
-                pP = M.perHiY ? Qk + march_q(SW, 0, 1, 1) - 32 * (ptrdiff_t)bT   // row 0's pair h = t + 1 - bT
-                              : Qk + march_q(SW, gT, 0, bT - 1) - 32;           // row ny - 1's pair h = t + 1 - bT
+            if (lowGhostLane && !M.perLoY) pP = Qk + march_q(SW, 0, hs0 + 1, 1);   // row 0's pair h = hs0 + t
+            if (topGhostLane)   // row 0's / row ny - 1's pair h = hs0 + t + 1 - bT
+                pP = M.perHiY ? Qk + march_q(SW, 0, hs0 + 1, 1) - 32 * (ptrdiff_t)bT
+                              : Qk + march_q(SW, gT, hs0, bT - 1) - 32;
         } else {
             pLoK = 0;
         }
-        const double2* eP = (eKind == 1)   ? Qn + march_q(SW, g - 1, 31, 31)
-                            : (eKind == 2) ? Qk + march_q(SW, topG, topB, topB)
-                            : (eKind == 3) ? Qk + march_q(SW, g + 1, 0, 0) - 32 * 31
-                            : (eKind == 4) ? (stored0 ? Qk + march_q(SW, g + 1, 0, 0) - 32 * 31
-                                              : M.perHiY ? Qk + march_q(SW, 0, 1, 1) - 32 * 31 : rowK)
-                                           : rowK;
+        const double2* eP = (eKind == 1)   ? Qn + march_q(SW, g - 1, hs0 + 31, 31)
+                            : (eKind == 2) ? Qk + march_q(SW, topG, hs0 + topB, topB)
+                            : (eKind == 3) ? Qk + march_q(SW, g + 1, hs0, 0) - 32 * 31
+                            : (eKind == 4) ? (stored0 ? Qk + march_q(SW, g + 1, hs0, 0) - 32 * 31
+                                              : M.perHiY ? Qk + march_q(SW, 0, hs0 + 1, 1) - 32 * 31 : rowKs)
+                                           : rowKs;
         const bool lowFromEdge = M.perLoY && !stored0;   // the low ghost pair from row ny - 1
-        // the ghost columns of this row in iterate k: sources xsLo, xsHi
+        // the ghost columns of this row in iterate k: sources xsLo, xsHi; a segment after the first starts
+        // from the new value of the left segment's last cell instead
         double gL, gR;
-        if (stored0) {
+        if (hs0 > 0) {
+            gL = __ldcg(Qn + march_q(SW, g, hs0 - 1 + lane, lane)).y;
+            gR = 0.0;   // x = nx - 1 lies in the last segment only
+            if (tLast >= 0) {
+                const double2 gRp = __ldcg(rowK + 32 * ((M.xsHi >> 1) + lane));
+                gR = (M.xsHi & 1) ? gRp.y : gRp.x;
+            }
+            if (stored0) gR = M.ghost0[TR ? cidx(P, rowIn ? r - 1 : 0, M.nx, 0) : cidx(P, M.nx, rowIn ? r - 1 : 0, 0)];
+        } else if (stored0) {
             const int n = r - 1, nn = rowIn ? n : 0, Nm = M.nx;
             gL = M.ghost0[TR ? cidx(P, nn, -1, 0) : cidx(P, -1, nn, 0)];
             gR = M.ghost0[TR ? cidx(P, nn, Nm, 0) : cidx(P, Nm, nn, 0)];
@@ -542,7 +573,7 @@ __global__ void __launch_bounds__(32 * (W + 1), 1) k_march_gs(Params P, GsMarch 
                     const double2 Pn = pr[(u + 1) % D];       // old pair h + 1
                     const double2 eg = er[u];
                     const int tn = t + D;
-                    march_ld(pr[u], pPb + 32 * u, tn < NS && tn >= pLoK);
+                    march_ld(pr[u], pPb + 32 * u, tn < tPEnd && tn >= pLoK);
                     march_ld(er[u], ePb + 32 * u, tn < NS && (unsigned)(tn - eLo) < (unsigned)(eHi - eLo));
                     const double2 up = march_shfl_up(newPair);
                     const double2 down = march_shfl_down(Pn);

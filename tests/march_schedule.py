@@ -73,8 +73,9 @@ def ref_gs(nx, ny, bc, cf, p0, tol, maxIter):
     return p, prev, it_done
 
 
-def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, KIND=0):
-    """Run the schedule; returns (the result with one ghost layer, the iteration count)."""
+def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, KIND=0, S=1):
+    """Run the schedule (S segments along the march axis); returns (the
+    result with one ghost layer, the iteration count)."""
     rng = random.Random(seed)
     # march space: m along the walk, n across the lanes
     nx, ny = (pny, pnx) if tr else (pnx, pny)
@@ -82,8 +83,13 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
     def phys(m, n):   # (x, y) of march cell (m, n)
         return (n, m) if tr else (m, n)
     NH = (nx + 1) // 2
-    SW, NS = NH + 32, NH + 31
+    SW = NH + 32
     G, GA = ny // 32 + 1, (ny + 1) // 32 + 1
+    Lseg = (NH + S - 1) // S
+    S = (NH + Lseg - 1) // Lseg
+
+    def seg_steps(s):
+        return min(NH, (s + 1) * Lseg) - s * Lseg + 31
     ctas = (G + W - 1) // W
     qn = GA * SW * 32
 
@@ -136,8 +142,9 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
     done = [0] * maxIter
     res = [0.0] * maxIter
     flags = [0, 0]
-    sp = {g: (0 if g < G else FIN) for g in range(ctas * W)}
-    eRing = {w: [(NAN, NAN)] * RE for w in range(ctas * W)}
+    sp = {(s, g): (0 if g < G else FIN) for s in range(S) for g in range(ctas * W)}
+    eRing = {(s, w): [(NAN, NAN)] * RE for s in range(S) for w in range(ctas * W)}
+    nWarps = G * S
     xsLo = nx - 1 if bc[0] else 0
     xsHi = 0 if bc[1] else nx - 1
     perLoY, perHiY = bc[2], bc[3]
@@ -160,8 +167,11 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
         dv = c2[1] if act else 1.0
         return num / dv
 
-    def group(g):
+    def group(g, seg):
         c, warp = g // W, g % W
+        hs0, hs1 = seg * Lseg, min(NH, (seg + 1) * Lseg)
+        nP = hs1 - hs0
+        NS = nP + 31
         gLo = c * W - 1 if c > 0 else -1
         topR = ny
         topG, topB = topR >> 5, topR & 31
@@ -175,13 +185,14 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
             d['low'] = g == 0 and lane == 0
             d['top'] = g == gT and lane == bT and bT >= 1
             d['tAct0'] = lane if d['rowIn'] else NS
-            d['tAct1'] = lane + NH if d['rowIn'] else NS
-            d['tLast'] = lane + ((nx - 1) >> 1)
+            d['tAct1'] = lane + nP if d['rowIn'] else NS
+            hLastX = (nx - 1) >> 1
+            d['tLast'] = lane + hLastX - hs0 if hs0 <= hLastX < hs1 else -1
             ek, elo, ehi = 0, 0, 0
-            if lane == 0 and warp == 0 and g > 0: ek, ehi = 1, NH
-            elif d['low'] and perLoY: ek, ehi = 2, NH
-            elif lane == 31 and hasAbove: ek, elo, ehi = 3, 31, NH + 31
-            elif lane == 31 and g + 1 == gT and bT == 0: ek, elo, ehi = 4, 31, NH + 31
+            if lane == 0 and warp == 0 and g > 0: ek, ehi = 1, nP
+            elif d['low'] and perLoY: ek, ehi = 2, nP
+            elif lane == 31 and hasAbove: ek, elo, ehi = 3, 31, nP + 31
+            elif lane == 31 and g + 1 == gT and bT == 0: ek, elo, ehi = 4, 31, nP + 31
             d['ek'], d['elo'], d['ehi'] = ek, elo, ehi
             d['pLo'] = (max(0, bT - 1) if perHiY else 1) if d['top'] else 0
             d['eWriter'] = lane == 31 and warp < W - 1 and d['rowIn']
@@ -197,9 +208,9 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
 
         def progress_of(h):
             if c * W <= h < c * W + W:
-                return sp[h]
+                return sp[(seg, h)]
             if h in extG:
-                return sp[h]
+                return sp[(seg, h)]
             return -1
 
         for k in range(maxIter):
@@ -207,15 +218,17 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
             kw = k + 1 - nb
             if flags[0]: break
             while True:
-                a = kw < 0 or done[kw] >= G
-                b = not (perHiY and g == G - 1 and g != 0) or sp[0] >= base
-                if a and b: break
+                a = kw < 0 or done[kw] >= nWarps
+                b = not (perHiY and g == G - 1 and g != 0) or sp[(seg, 0)] >= base
+                sl = seg == 0 or sp[(seg - 1, g)] >= (k + 1) * seg_steps(seg - 1)
+                sr = seg == S - 1 or k == 0 or sp[(seg + 1, g)] >= (k - 1) * seg_steps(seg + 1) + 32
+                if a and b and sl and sr: break
                 if flags[0]: break
                 yield
             if flags[0]: break
             go = True
             while KIND == 0 and go and chk < k:
-                if done[chk] < G: break
+                if done[chk] < nWarps: break
                 if res[chk] < tol:
                     flags[0] = 1
                     go = False
@@ -223,29 +236,41 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
             if not go or flags[0]: break
             Qk, Qn = Q[k % nb], Q[(k + 1) % nb]
             rowK = {lane: mq(g, 0, lane) for lane in range(32)}
+            rowKs = {lane: mq(g, hs0, lane) for lane in range(32)}
             stored0 = KIND == 1 and k == 0
             lowFromEdge = perLoY and not stored0
             pP, eP, pLoK = {}, {}, {}
             for lane in range(32):
                 d = L[lane]
-                p = rowK[lane]
+                p = rowKs[lane]
                 pLoK[lane] = 0 if stored0 else d['pLo']
                 if not stored0:
-                    if d['low'] and not perLoY: p = mq(0, 1, 1)
+                    if d['low'] and not perLoY: p = mq(0, hs0 + 1, 1)
                     if d['top']:
-                        p = (mq(0, 1, 1) - 32 * bT) if perHiY else (mq(gT, 0, bT - 1) - 32)
+                        p = (mq(0, hs0 + 1, 1) - 32 * bT) if perHiY else (mq(gT, hs0, bT - 1) - 32)
                 pP[lane] = p
                 ek = d['ek']
-                if ek == 1: e = ('n', mq(g - 1, 31, 31))
-                elif ek == 2: e = ('k', mq(topG, topB, topB))
-                elif ek == 3: e = ('k', mq(g + 1, 0, 0) - 32 * 31)
+                if ek == 1: e = ('n', mq(g - 1, hs0 + 31, 31))
+                elif ek == 2: e = ('k', mq(topG, hs0 + topB, topB))
+                elif ek == 3: e = ('k', mq(g + 1, hs0, 0) - 32 * 31)
                 elif ek == 4:
-                    if stored0: e = ('k', mq(g + 1, 0, 0) - 32 * 31)
-                    else: e = ('k', (mq(0, 1, 1) - 32 * 31) if perHiY else rowK[lane])
-                else: e = ('k', rowK[lane])
+                    if stored0: e = ('k', mq(g + 1, hs0, 0) - 32 * 31)
+                    else: e = ('k', (mq(0, hs0 + 1, 1) - 32 * 31) if perHiY else rowKs[lane])
+                else: e = ('k', rowKs[lane])
                 eP[lane] = e
             gL, gR = {}, {}
             for lane in range(32):
+                if hs0 > 0:   # a later segment starts from the left segment's new last cell
+                    gL[lane] = LD(Qn, mq(g, hs0 - 1 + lane, lane))[1]
+                    gR[lane] = NAN
+                    if L[lane]['tLast'] >= 0 and L[lane]['rowIn']:
+                        if stored0:
+                            n_ = 32 * g + lane - 1
+                            XR, YR = phys(nx, n_)
+                            gR[lane] = p0[YR + 1, XR + 1]
+                        else:
+                            gR[lane] = LD(Qk, rowK[lane] + 32 * ((xsHi >> 1) + lane))[xsHi & 1]
+                    continue
                 if stored0:
                     n_ = 32 * g + lane - 1 if L[lane]['rowIn'] else 0
                     XL, YL = phys(-1, n_)
@@ -267,9 +292,9 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
                 n4 = base + tu - 30 - RE if (warp < W - 1 and hasAbove) else -1
 
                 def met():
-                    return ((n0 < 0 or sp[g - 1] >= n0) and (n1 < 0 or progress_of(g - 1) >= n1) and
+                    return ((n0 < 0 or sp[(seg, g - 1)] >= n0) and (n1 < 0 or progress_of(g - 1) >= n1) and
                             (n2 < 0 or progress_of(topG) >= n2) and (n3 < 0 or progress_of(g + 1) >= n3) and
-                            (n4 < 0 or sp[g + 1] >= n4))
+                            (n4 < 0 or sp[(seg, g + 1)] >= n4))
                 while not met():
                     if flags[0]: return
                     yield
@@ -305,14 +330,16 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
                     tn = t + D
                     for lane in range(32):
                         d = L[lane]
-                        if tn < NS and tn >= pLoK[lane]: pr[lane][u] = LD(Qk, pP[lane] + 32 * tn)
+                        # through step NS before another segment: lane 31's last pair reads its first pair
+                        if tn < NS + (1 if hs1 < NH else 0) and tn >= pLoK[lane]:
+                            pr[lane][u] = LD(Qk, pP[lane] + 32 * tn)
                         if tn < NS and d['elo'] <= tn < d['ehi']: er[lane][u] = ldE(lane, tn)
                     up = {l: newPair[l - 1] if l > 0 else newPair[0] for l in range(32)}
                     down = {l: Pn[l + 1] if l < 31 else Pn[31] for l in range(32)}
                     newNP = dict(newPair)
                     for lane in range(32):
                         d = L[lane]
-                        eb = eRing[g - 1][(eOff + t) & (RE - 1)] if warp > 0 else (NAN, NAN)
+                        eb = eRing[(seg, g - 1)][(eOff + t) & (RE - 1)] if warp > 0 else (NAN, NAN)
                         if lane == 0:
                             pD = eb if warp > 0 else eg[lane]
                         else:
@@ -320,7 +347,7 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
                         pU = eg[lane] if lane == 31 else down[lane]
                         act0 = d['tAct0'] <= t < d['tAct1']
                         act1 = act0 and not (t == d['tLast'] and not lastOdd)
-                        base0 = ((g * SW + t) * 8) * 32 + lane
+                        base0 = ((g * SW + hs0 + t) * 8) * 32 + lane
                         if act0:
                             a = [tuple(rec[base0 + 32 * q]) for q in range(4)]
                             bb = [tuple(rec[base0 + 32 * (4 + q)]) for q in range(4)]
@@ -330,7 +357,7 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
                         pR0 = gR[lane] if (t == d['tLast'] and not lastOdd) else Pt[lane][1]
                         pR1 = gR[lane] if t == d['tLast'] else Pn[lane][0]
                         if KIND == 1:
-                            slot = rowK[lane] + 32 * t
+                            slot = rowKs[lane] + 32 * t
                             pn0 = igr_cell(act0, igrRec.get((slot, 0)), pL0, pR0, pD[0], pU[0])
                             pn1 = igr_cell(act1, igrRec.get((slot, 1)), pn0, pR1, pD[1], pU[1])
                         else:
@@ -343,16 +370,16 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
                             r1 = abs(pn1 - Pt[lane][1])
                             maxRes[lane] = maxRes[lane] if maxRes[lane] >= r1 else r1
                         if act0:
-                            idx = rowK[lane] + 32 * t
+                            idx = rowKs[lane] + 32 * t
                             assert 0 <= idx < qn
                             Qn[idx] = (pn0, pn1 if act1 else 1.0)
                             if d['eWriter']:
-                                eRing[g][(eOff + t - 31) & (RE - 1)] = (pn0, pn1 if act1 else 1.0)
+                                eRing[(seg, g)][(eOff + t - 31) & (RE - 1)] = (pn0, pn1 if act1 else 1.0)
                             newNP[lane] = (pn0, pn1 if act1 else 1.0)
                         elif d['low']:
                             newNP[lane] = eg[lane] if lowFromEdge else Pt[lane]
                     newPair = newNP
-                sp[g] = base + min(t0 + D, NS)
+                sp[(seg, g)] = base + min(t0 + D, NS)
             if aborted: break
             v = 0.0
             for lane in range(32):
@@ -362,9 +389,9 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
             res[k] = max(res[k], v)
             done[k] += 1
             yield
-        sp[g] = FIN
+        sp[(seg, g)] = FIN
 
-    gens = {g: group(g) for g in range(G)}
+    gens = {(s, g): group(g, s) for s in range(S) for g in range(G)}
     alive = set(gens)
     steps = 0
     while alive:

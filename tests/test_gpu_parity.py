@@ -290,6 +290,45 @@ def _check_with_solver(case, nsteps, kind):
     return cg.last_pressure_iterations()
 
 
+@pytest.mark.parametrize("shape,bcs,segs", [((100, 140, 1), (abi.BC_OUTFLOW, abi.BC_SLIPWALL), 2),
+                                            ((130, 70, 1), (abi.BC_SLIPWALL, abi.BC_OUTFLOW), 3),
+                                            ((600, 520, 1), (abi.BC_OUTFLOW, abi.BC_SLIPWALL), 5),
+                                            ((90, 159, 1), (abi.BC_SYMMETRY, abi.BC_OUTFLOW), 0)])
+@pytest.mark.parametrize("max_iter,dt,tol", [(2, 1e-2, 1e-14), (7, 1e-2, 1e-14), (300, 2e-3, 1e-9)])
+def test_gauss_seidel_wavefront_segments(shape, bcs, segs, max_iter, dt, tol, monkeypatch):
+    """The 2D wavefront on meshes without a periodic face, rows cut into
+    segments along the march axis (SIFV_GS_MARCH_SEGMENTS; 0 = the count
+    the solver picks): iteration count and the whole returned array are
+    the oracle's bit for bit."""
+    monkeypatch.setenv("SIFV_GS_MARCH", "1")
+    monkeypatch.setenv("SIFV_GS_MARCH_SEGMENTS", str(segs))
+    cfg, mesh, fields = cases.acoustic_box(*shape)
+    mesh.bc = [bcs[0]] * 2 + [bcs[1]] * 2 + [abi.BC_OUTFLOW] * 2
+    cg = backends.make(backends.cuda(), (cfg, mesh, fields))
+    co = backends.make(backends.oracle(), (cfg, mesh, fields))
+    cg.set_pressure_solver(abi.PRESSURE_GAUSS_SEIDEL)
+    co.set_pressure_solver(abi.PRESSURE_GAUSS_SEIDEL)
+    rng = np.random.default_rng(max_iter + segs)
+    n = cg.ncells
+    args = (1.0 + 0.1 * rng.random(n), 1.4 + 0.2 * rng.random(n), rng.random(n), rng.random(n))
+    pg, ig, _ = cg.pressure_solve(*args, dt, tol, max_iter)
+    po, io, _ = co.pressure_solve(*args, dt, tol, max_iter)
+    assert ig == io, (ig, io)
+    assert np.array_equal(pg.view(np.int64), po.view(np.int64))
+
+
+@pytest.mark.parametrize("shape,bcs,segs", [((100, 140, 1), (abi.BC_OUTFLOW, abi.BC_SLIPWALL), 3),
+                                            ((600, 520, 1), (abi.BC_SLIPWALL, abi.BC_OUTFLOW), 4)])
+def test_igr_wavefront_segments(shape, bcs, segs, monkeypatch):
+    """IGR sweeps (20-sweep warm start, then 5) in the 2D wavefront with
+    rows cut into segments, through two steps: bit-identical to the oracle."""
+    monkeypatch.setenv("SIFV_GS_MARCH", "1")
+    monkeypatch.setenv("SIFV_GS_MARCH_SEGMENTS", str(segs))
+    cfg, mesh, fields = cases.acoustic_box(*shape)
+    mesh.bc = [bcs[0]] * 2 + [bcs[1]] * 2 + [abi.BC_OUTFLOW] * 2
+    check((cfg, mesh, fields), 2)
+
+
 @pytest.mark.parametrize("bcs", [(abi.BC_PERIODIC, abi.BC_PERIODIC), (abi.BC_PERIODIC, abi.BC_SLIPWALL),
                                  (abi.BC_OUTFLOW, abi.BC_PERIODIC)])
 def test_semi_implicit_2d_periodic_wavefront_steps(bcs):

@@ -4,7 +4,7 @@ the plain in-place sweeps' results bit for bit: Gauss-Seidel iterations
 (batch lengths 8 and 4, convergence with speculative sweeps) and IGR sweeps
 (stored ghosts read by sweep 0), walking along x or y, periodic and
 zero-gradient faces, several CTAs, ghost rows that open a new group, odd and
-tiny extents."""
+tiny extents, rows cut into segments along the march axis."""
 import numpy as np
 import pytest
 
@@ -49,5 +49,34 @@ def test_igr_schedule(shape, tr):
     s0 = rs.random((ny + 2, nx + 2))   # stored ghost cells that differ from the interior's images
     ref = ms.ref_igr(nx, ny, bc, cf, s0, 4)
     out, _ = ms.emulate(nx, ny, bc, cf, s0, 0.0, 4, nb=4, seed=ny, tr=tr, D=4, KIND=1)
+    m = _mask(ref.shape)
+    assert np.array_equal(out[m].view(np.int64), ref[m].view(np.int64))
+
+
+@pytest.mark.parametrize("shape,S", [((20, 70), 2), ((37, 64), 3), ((9, 31), 4), ((41, 127), 2)],
+                         ids=lambda v: str(v))
+@pytest.mark.parametrize("tr", [False, True])
+def test_segment_schedule(shape, S, tr):
+    """Rows cut into S segments along the march axis (meshes without a
+    periodic face): Gauss-Seidel (batch 8 and 4) and IGR sweeps."""
+    nx, ny = shape
+    bc = (0, 0, 0, 0)
+    rs = np.random.default_rng(nx * 1000 + ny)
+    cf = [rs.random((ny, nx)) * 0.2 for _ in range(4)] + [np.ones((ny, nx)) * 0.9, 1.0 + rs.random((ny, nx)),
+                                                          rs.random((ny, nx))]
+    p0 = rs.random((ny, nx))
+    for (max_iter, tol), D in (((7, 1e-30), 8), ((40, 1e-4), 4)):
+        pref, prev, itr = ms.ref_gs(nx, ny, bc, cf, p0, tol, max_iter)
+        ref = prev.copy()
+        ref[1:-1, 1:-1] = pref[1:-1, 1:-1]
+        out, it = ms.emulate(nx, ny, bc, cf, p0, tol, max_iter, nb=4, seed=S + nx, tr=tr, D=D, S=S)
+        assert it == itr
+        m = _mask(ref.shape)
+        assert np.array_equal(out[m].view(np.int64), ref[m].view(np.int64))
+    cf2 = [1.0 + rs.random((ny, nx)) for _ in range(4)] + [rs.random((ny, nx)) * 0.3, rs.random((ny, nx)) * 0.3,
+                                                           rs.random((ny, nx)), 2.0 + rs.random((ny, nx))]
+    s0 = rs.random((ny + 2, nx + 2))
+    ref = ms.ref_igr(nx, ny, bc, cf2, s0, 4)
+    out, _ = ms.emulate(nx, ny, bc, cf2, s0, 0.0, 4, nb=4, seed=ny, tr=tr, D=8, KIND=1, S=S)
     m = _mask(ref.shape)
     assert np.array_equal(out[m].view(np.int64), ref[m].view(np.int64))
