@@ -40,6 +40,13 @@
 // axis costs nothing (each row is walked whole before its next sweep); a
 // periodic row axis makes each sweep wait for the far group's previous one.
 //
+// Segments: without a periodic face the rows may be cut into S segments of
+// L pairs along the march axis, a warp per (segment, group).  A segment
+// starts sweep k once the segment to its left finished sweep k (its first
+// pair reads that segment's new last cell) and the one to its right did the
+// first 32 steps of sweep k - 1 (its last pair reads that segment's old
+// first cell), so the segments work on consecutive sweeps at once.
+//
 // Synchronization: each compute warp publishes its progress (steps done,
 // counted across sweeps) in shared memory after each batch of D
 // steps; warp kMarchWarps of the CTA (the helper) turns those into
