@@ -59,8 +59,8 @@ KERNEL_BYTES_PER_CELL_2D = {"march2d": 93.33, "dt": 32.0, "bc_prim": 0.0, "face_
 NCU_KERNEL_SOURCES = ("semiimplicitfv_b200/csrc/sifv_march2d.cuh", "semiimplicitfv_b200/csrc/sifv_sweep.cuh",
                       "semiimplicitfv_b200/csrc/sifv_fastmath.cuh")
 # (precision, kernel) -> {"sha": ..., "dram_bytes_per_cell": ..., "fp64_inst_per_cell": ...}; from
-# profiles/march2d_fp64_2048.md and profiles/march2d_mixed_2048.md (FP64 thread operations: DADD + DMUL +
-# DFMA issued, per interior cell)
+# one ncu capture each of the FP64 and the mixed march kernel on a 2048² four-quadrant Riemann stage
+# (FP64 thread operations: DADD + DMUL + DFMA issued, per interior cell)
 NCU_CAPTURE = {
     (2, "march2d"): {"sha": "32a04e8cb0599297", "dram_bytes_per_cell": 89.50, "fp64_inst_per_cell": 838.1},
     (1, "march2d"): {"sha": "32a04e8cb0599297", "dram_bytes_per_cell": 94.32, "fp64_inst_per_cell": 46.4},
