@@ -83,7 +83,7 @@ struct GsMarch {
     // extents nx (march axis m) and ny (row axis n); x and y when !TR, y and x when TR
     const double2* rec;
     double2* q[kMarchMaxBufs];   // iterate n in q[n % nb]
-    int* prog;                   // [G] device-wide progress per group
+    int* prog;                   // [S][G] device-wide progress per segment and group
     int* done;                   // [maxIter] groups through sweep k
     int* flags;                  // [0] stop, [1] error code (1: a wait timed out)
     const int* slowRecs;
