@@ -7,8 +7,9 @@ register rings of prefetched pairs and edge pairs (a load reads memory at
 its issue step), shuffles between lanes, the shared-memory edge ring, the
 ghost-lane redirects, every wait of the batch and sweep starts, the buffer
 rotation and the convergence rule.  Groups (warps) run as generators that
-yield at each wait, interleaved in a random order, so a wait that does not
-cover a dependency shows up as a wrong value.  Slots the kernel never
+yield at each wait and, at random, after publishing a batch's progress,
+interleaved in a random order, so a wait that does not cover a dependency
+shows up as a wrong value.  Slots the kernel never
 writes hold NaN.  `ref_gs` / `ref_igr` are the plain in-place sweeps
 (GaussSeidelPressureSolver::solve, src/GaussSeidelPressureSolver.cpp:60-100;
 IGR, src/IGR.cpp:110-156, 2D) with one ghost layer; Python floats are IEEE
@@ -380,6 +381,8 @@ def emulate(pnx, pny, pbc, cf, p0, tol, maxIter, nb, seed, tr=False, D=8, W=2, K
                             newNP[lane] = eg[lane] if lowFromEdge else Pt[lane]
                     newPair = newNP
                 sp[(seg, g)] = base + min(t0 + D, NS)
+                if rng.random() < 0.5:   # other warps may see every published progress value
+                    yield
             if aborted: break
             v = 0.0
             for lane in range(32):

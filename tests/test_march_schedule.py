@@ -80,3 +80,44 @@ def test_segment_schedule(shape, S, tr):
     out, _ = ms.emulate(nx, ny, bc, cf2, s0, 0.0, 4, nb=4, seed=ny, tr=tr, D=8, KIND=1, S=S)
     m = _mask(ref.shape)
     assert np.array_equal(out[m].view(np.int64), ref[m].view(np.int64))
+
+
+def _random_case(i):
+    """Configuration i of the randomized schedules: a small mesh, its faces,
+    segments (only without a periodic face; from two up to one pair per
+    segment), batch length, orientation, cell kind and buffer count (down to
+    the minimum of three)."""
+    rs = np.random.default_rng(9000 + i)
+    nx, ny = int(rs.integers(1, 46)), int(rs.integers(1, 100))
+    bc = tuple(int(v) for v in np.repeat(rs.integers(0, 2, 2), 2)) if i % 3 else (0, 0, 0, 0)
+    tr = bool(rs.integers(0, 2))
+    nh = ((ny if tr else nx) + 1) // 2
+    S = 1 if any(bc) else int(rs.choice([1, 2, max(1, nh // 2), nh]))
+    return nx, ny, bc, S, int(rs.choice([4, 8])), tr, int(rs.integers(0, 2)), int(rs.integers(3, 7))
+
+
+@pytest.mark.parametrize("i", range(36))
+def test_random_schedules(i):
+    """Randomized configurations (seeded): the schedule, including
+    one-pair segments and three rotating buffers, still gives the plain
+    sweeps' bits and, for Gauss-Seidel, their iteration count."""
+    nx, ny, bc, S, D, tr, kind, nb = _random_case(i)
+    rs = np.random.default_rng(i)
+    m = _mask((ny + 2, nx + 2))
+    if kind == 0:
+        cf = [rs.random((ny, nx)) * 0.2 for _ in range(4)] + [np.ones((ny, nx)) * 0.9, 1.0 + rs.random((ny, nx)),
+                                                              rs.random((ny, nx))]
+        p0 = rs.random((ny, nx))
+        max_iter, tol = (9, 1e-30) if i % 2 else (30, 1e-3)
+        pref, prev, itr = ms.ref_gs(nx, ny, bc, cf, p0, tol, max_iter)
+        ref = prev.copy()
+        ref[1:-1, 1:-1] = pref[1:-1, 1:-1]
+        out, it = ms.emulate(nx, ny, bc, cf, p0, tol, max_iter, nb=nb, seed=i, tr=tr, D=D, S=S)
+        assert it == itr
+    else:
+        cf = [1.0 + rs.random((ny, nx)) for _ in range(4)] + [rs.random((ny, nx)) * 0.3, rs.random((ny, nx)) * 0.3,
+                                                              rs.random((ny, nx)), 2.0 + rs.random((ny, nx))]
+        s0 = rs.random((ny + 2, nx + 2))
+        ref = ms.ref_igr(nx, ny, bc, cf, s0, 5)
+        out, _ = ms.emulate(nx, ny, bc, cf, s0, 0.0, 5, nb=nb, seed=i, tr=tr, D=D, KIND=1, S=S)
+    assert np.array_equal(out[m].view(np.int64), ref[m].view(np.int64)), (nx, ny, bc, S, D, tr, kind, nb)
