@@ -4,7 +4,8 @@ the plain in-place sweeps' results bit for bit: Gauss-Seidel iterations
 (batch lengths 8 and 4, convergence with speculative sweeps) and IGR sweeps
 (stored ghosts read by sweep 0), walking along x or y, periodic and
 zero-gradient faces, several CTAs, ghost rows that open a new group, odd and
-tiny extents, rows cut into segments along the march axis."""
+tiny extents, rows cut into segments along the march axis, and seeded
+random configurations of all of these."""
 import numpy as np
 import pytest
 
