@@ -694,9 +694,12 @@ int march_run(sifv_ctx* c, int kind, const double* rhs, double tol, int maxIter,
     const int ctas = ctasPerSeg * S, NSs = L + 31;
     const size_t qn = (size_t)GA * SW * 32;   // pairs per iterate
     // buffers: the warps spread over about (G (32 + 2 D + 40) + S NSs) / NSs sweeps, plus the converged
-    // iterate, its predecessor and one sweep of slack; at most 1 GiB
+    // iterate, its predecessor and one sweep of slack; at most 1 GiB together, or 8 buffers where 1 GiB
+    // holds fewer (as many bytes as the Gauss-Seidel records): at 8192² 1 GiB would leave 3 buffers while
+    // the warps spread over about 4 sweeps, and the leading groups would stall on buffers still being read
     int nb = std::min(kMarchMaxBufs, 4 + (G * (32 + 2 * D + 40) + S * NSs + NSs - 1) / NSs);
-    nb = std::max(3, std::min<int>(nb, (int)((size_t(1) << 30) / (qn * sizeof(double2)))));
+    const size_t bufBytes = qn * sizeof(double2);
+    nb = std::max(3, std::min<int>(nb, (int)(std::max<size_t>(size_t(1) << 30, 8 * bufBytes) / bufBytes)));
     int sa = SIFV_OK;
     double*& recBuf = kind ? c->marchRecIgr : c->marchRec;
     if (!recBuf) {
