@@ -11,7 +11,10 @@ steps at a time, one time unit per step.  The waits are the kernel's:
 - before a batch: the group below is 32 steps ahead of what the next batch
   reads (inside a CTA the batch being computed, across CTAs the next one,
   whose prefetch reads it), and the group above did the previous sweep up
-  to 30 steps short of it.
+  to 30 steps short of it;
+- across a periodic row axis: the top group starts a sweep after group 0
+  finished the previous one, and group 0's batches follow the top row's
+  previous sweep.
 
 A warp's progress is seen by warps of its own CTA at once and by others
 `delta` units after its batch ends (the helper warp's relay).  The model
@@ -38,8 +41,12 @@ def buffers(NH, G, GA, S, D):
     return max(3, min(nb, max(1 << 30, 8 * buf) // buf))
 
 
-def run(NH, G, S, sweeps, D=8, nb=32, delta=4.0, W=2):
-    """Times at which all warps finished each sweep (list, in steps)."""
+def run(NH, G, S, sweeps, D=8, nb=32, delta=4.0, W=2, wrap=None):
+    """Times at which all warps finished each sweep (list, in steps).
+    wrap = (group, lane) of the last interior row when the row axis is
+    periodic (one segment): the top group then starts a sweep after group 0
+    finished the previous one (its ghost row above), and group 0 reads its
+    ghost row below from that row's previous sweep."""
     L, S = segments(NH, S)
 
     def steps(s):
@@ -63,6 +70,8 @@ def run(NH, G, S, sweeps, D=8, nb=32, delta=4.0, W=2):
                     t = max(t, seen(s + 1, g, k - 1, 32, False))
                 if k + 1 - nb >= 0:
                     t = max(t, done[k + 1 - nb] + delta)
+                if wrap and g == G - 1 and g != 0 and k > 0:
+                    t = max(t, end[(s, 0, k - 1)] + delta)
                 ns, lst = steps(s), []
                 for t0 in range(0, ns, D):
                     tp = t0 + 2 * D - 1
@@ -72,6 +81,9 @@ def run(NH, G, S, sweeps, D=8, nb=32, delta=4.0, W=2):
                     if g < G - 1 and k > 0 and tp - 30 > 0:
                         same = (g + 1) // W == g // W
                         t = max(t, seen(s, g + 1, k - 1, min(tp - 30, ns), same))
+                    if wrap and g == 0 and k > 0 and wrap[0] != 0:
+                        same = wrap[0] // W == 0
+                        t = max(t, seen(s, wrap[0], k - 1, min(tp + wrap[1] + 1, ns), same))
                     t += min(D, ns - t0)
                     lst.append((min(t0 + D, ns), t))
                 pubs[(s, g, k)] = lst

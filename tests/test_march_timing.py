@@ -2,8 +2,8 @@
 semiimplicitfv_b200/csrc/sifv_capi.cu) never hold its pipeline back in the
 timing model of tests/march_timing.py: with them, the model's period per
 iteration equals the one with unlimited buffers, from 1024² to 8192² and
-with rows cut into segments.  A cap of 1 GiB alone would leave 3 buffers at
-8192² and nearly double the period there."""
+with rows cut into segments, and with every face periodic.  A cap of 1 GiB
+alone would leave 3 buffers at 8192² and nearly double the period there."""
 import pytest
 
 import march_timing as mt
@@ -43,3 +43,16 @@ def test_one_gib_alone_would_stall_at_8192():
     NH, G, GA, S = plan(8192, 8192)
     assert (S, (1 << 30) // (GA * (NH + 32) * 32 * 16), mt.buffers(NH, G, GA, S, 8)) == (1, 1, 8)
     assert period(mt.run(NH, G, S, 10, nb=3), 5, 9) > 1.5 * (NH + 31)
+
+
+@pytest.mark.parametrize("n", [1024, 2048])
+def test_buffers_leave_no_reuse_stall_periodic_rows(n):
+    """Every face periodic (n × n): batch length 4, the period is the climb
+    over all row groups, and the buffers the host picks still leave it as
+    with unlimited buffers."""
+    NH, G, GA = n // 2, n // 32 + 1, (n + 1) // 32 + 1
+    assert G * (32 + 2 * 8 + 10) > NH + 31   # the host's rule for the short batch
+    nb, wrap = mt.buffers(NH, G, GA, 1, 4), (n // 32, n % 32)
+    got = period(mt.run(NH, G, 1, 16, D=4, nb=nb, wrap=wrap), 8, 15)
+    free = period(mt.run(NH, G, 1, 16, D=4, nb=64, wrap=wrap), 8, 15)
+    assert got == free > 2 * (NH + 31), (nb, got, free)
